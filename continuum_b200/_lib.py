@@ -1,0 +1,130 @@
+"""ctypes binding of libcontinuum_cuda.so (include/continuum_cuda.h).
+
+The library is built in-tree by ``python -m continuum_b200.build``; loading
+fails loudly if it is missing. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libcontinuum_cuda.so"
+
+CC_OK = 0
+CC_ERR_INVALID = 1
+CC_ERR_CUDA = 2
+CC_ERR_OOM = 3
+CC_ERR_NO_DEVICE = 4
+CC_ERR_STACK = 5
+CC_ERR_TIMEOUT = 6
+CC_ERR_BUSY = 7
+CC_NONE = 0xFFFFFFFF
+
+CC_DEVICE_POINTERS = 1
+CC_NO_REDO = 2
+
+CC_CONE_CAPPED = 1
+CC_CONE_STACK = 2
+CC_CONE_DIVERGED = 4
+CC_CONE_REWALKED = 8
+CC_CONE_FULL_STOP = 16
+
+#: Every symbol include/continuum_cuda.h declares.
+EXPORTS = (
+    "cc_context_create", "cc_context_destroy", "cc_last_error", "cc_scene_upload", "cc_scene_build",
+    "cc_scene_destroy", "cc_scene_sizes", "cc_scene_arrays", "cc_scene_device_bytes", "cc_options_default",
+    "cc_visibility", "cc_irradiance", "cc_coverage", "cc_scene_primary_hits", "cc_context_kernel_times",
+)
+
+
+class CCError(RuntimeError):
+    """A non-zero status from the library, with its message."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"continuum_cuda error {code}: {message}")
+        self.code = code
+
+
+class FlatScene(C.Structure):
+    _fields_ = [
+        ("tris", C.c_void_p), ("ntris", C.c_uint32),
+        ("ranges", C.c_void_p), ("nmeshes", C.c_uint32),
+        ("blas", C.c_void_p), ("nblas", C.c_uint32),
+        ("blas_items", C.c_void_p), ("nblas_items", C.c_uint32),
+        ("nodes", C.c_void_p), ("nnodes", C.c_uint32),
+        ("items", C.c_void_p), ("nitems", C.c_uint32),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
+        ("wide_cone_cap", C.c_uint32), ("points_per_warp", C.c_uint32), ("flags", C.c_uint32),
+    ]
+
+
+class Outputs(C.Structure):
+    _fields_ = [
+        ("full", C.c_void_p), ("any", C.c_void_p), ("partial", C.c_void_p),
+        ("irradiance", C.c_void_p), ("fraction", C.c_void_p), ("work", C.c_void_p),
+    ]
+
+
+_lib: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m continuum_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, U32, U64, I = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+    sig = {
+        "cc_context_create": (I, [I, C.POINTER(P)]),
+        "cc_context_destroy": (I, [P]),
+        "cc_last_error": (C.c_char_p, []),
+        "cc_scene_upload": (I, [P, C.POINTER(FlatScene), C.POINTER(P)]),
+        "cc_scene_build": (I, [P, P, P, U32, C.POINTER(P)]),
+        "cc_scene_destroy": (I, [P]),
+        "cc_scene_sizes": (I, [P, P]),
+        "cc_scene_arrays": (I, [P, P, P, P, P, P]),
+        "cc_scene_device_bytes": (U64, [P]),
+        "cc_options_default": (None, [C.POINTER(Options)]),
+        "cc_visibility": (I, [P, P, P, U64, P, U32, C.POINTER(Options), C.POINTER(Outputs), P]),
+        "cc_irradiance": (I, [P, P, U64, P, I, P, P, U32, U32, U32, P, C.POINTER(C.c_double)]),
+        "cc_coverage": (I, [P, P, U64, P, I, P, P, U32, P]),
+        "cc_scene_primary_hits": (I, [P, P, U32, U32, P, P]),
+        "cc_context_kernel_times": (I, [P, P, I]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(code: int) -> None:
+    if code != CC_OK:
+        msg = load().cc_last_error()
+        raise CCError(code, msg.decode() if msg else "")
+
+
+def ptr(a: np.ndarray | None) -> int | None:
+    """Host address of a C-contiguous array (None for None)."""
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data
+
+
+def default_options() -> Options:
+    o = Options()
+    load().cc_options_default(C.byref(o))
+    return o

@@ -1,0 +1,265 @@
+// Host hierarchy builder. Follows crates/continuum-gpu/src/hierarchy.rs:
+//   flatten              :29-66
+//   split                :128-179  (median split on the longest centroid axis)
+//   object_hierarchy     :198-253  (two objects per leaf, oversized subtree)
+//   triangle_hierarchy   :527-545  (eight triangles per leaf)
+//   padded               :762-765
+// The reference partitions with select_nth_unstable, whose order among equal
+// keys is unspecified; here the `mid` smallest (key, item) pairs go left and a
+// leaf lists its items in increasing index, so the tree depends only on the
+// input. Meshes build in parallel, and the top levels of a large mesh split
+// their two halves on separate threads; the result is the same tree.
+#include "bvh.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <numeric>
+#include <thread>
+
+namespace cc {
+namespace {
+
+struct Box {
+  float lo[3];
+  float hi[3];
+};
+
+void padded(Box& b) {
+  float m = 0.0f;
+  for (int k = 0; k < 3; ++k) m = std::max(m, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));
+  float pad = 1e-5f * std::max(m, 1.0f);
+  for (int k = 0; k < 3; ++k) {
+    b.lo[k] -= pad;
+    b.hi[k] += pad;
+  }
+}
+
+Box bounds_of(const float* tris12, uint32_t first, uint32_t count) {
+  Box b{{FLT_MAX, FLT_MAX, FLT_MAX}, {-FLT_MAX, -FLT_MAX, -FLT_MAX}};
+  for (uint32_t t = first; t < first + count; ++t)
+    for (int v = 0; v < 3; ++v)
+      for (int k = 0; k < 3; ++k) {
+        float x = tris12[12 * (size_t)t + 4 * v + k];
+        b.lo[k] = std::min(b.lo[k], x);
+        b.hi[k] = std::max(b.hi[k], x);
+      }
+  return b;
+}
+
+// A subtree is built into its own node vector and spliced in afterwards, so
+// two halves can build concurrently; node numbering is fixed up at splice time
+// to the order a serial depth-first build would produce.
+struct Builder {
+  const std::vector<Box>& bounds;
+  uint32_t leaf;
+  uint32_t node_base;
+  uint32_t item_base;
+  int parallel_depth;
+
+  // Builds the subtree over items[0..count) (slots start..start+count) into
+  // `nodes`, root at nodes[root]. Children of a node are allocated as a pair
+  // at the end of `nodes`, left first, in depth-first order.
+  void split(std::vector<NodeGpu>& nodes, size_t root, uint32_t* items, size_t count, size_t start, int depth) {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (size_t i = 0; i < count; ++i) {
+      const Box& b = bounds[items[i]];
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], b.lo[k]);
+        hi[k] = std::max(hi[k], b.hi[k]);
+        float c = (b.lo[k] + b.hi[k]) * 0.5f;
+        clo[k] = std::min(clo[k], c);
+        chi[k] = std::max(chi[k], c);
+      }
+    }
+    NodeGpu& n = nodes[root];
+    std::memset(&n, 0, sizeof(n));
+    for (int k = 0; k < 3; ++k) {
+      n.lo[k] = lo[k];
+      n.hi[k] = hi[k];
+    }
+    if (count <= leaf) {
+      std::sort(items, items + count);
+      n.info[0] = item_base + (uint32_t)start;
+      n.info[1] = (uint32_t)count;
+      return;
+    }
+    float e[3] = {chi[0] - clo[0], chi[1] - clo[1], chi[2] - clo[2]};
+    int axis = (e[0] >= e[1] && e[0] >= e[2]) ? 0 : (e[1] >= e[2] ? 1 : 2);
+    size_t mid = count / 2;
+    const std::vector<Box>& bb = bounds;
+    std::nth_element(items, items + mid, items + count, [&bb, axis](uint32_t a, uint32_t b) {
+      float ka = bb[a].lo[axis] + bb[a].hi[axis];
+      float kb = bb[b].lo[axis] + bb[b].hi[axis];
+      return ka < kb || (ka == kb && a < b);
+    });
+    size_t left = nodes.size();
+    nodes.push_back(NodeGpu{});
+    nodes.push_back(NodeGpu{});
+    nodes[root].info[0] = node_base + (uint32_t)left;
+    if (depth < parallel_depth && count > 65536) {
+      // The right half builds on another thread into a separate vector; its
+      // nodes are appended after the left subtree's, renumbered.
+      std::vector<NodeGpu> right_nodes(1);
+      auto fut = std::async(std::launch::async, [&] {
+        split(right_nodes, 0, items + mid, count - mid, start + mid, depth + 1);
+      });
+      split(nodes, left, items, mid, start, depth + 1);
+      fut.get();
+      splice(nodes, left + 1, right_nodes);
+    } else {
+      split(nodes, left, items, mid, start, depth + 1);
+      split(nodes, left + 1, items + mid, count - mid, start + mid, depth + 1);
+    }
+  }
+
+  // Moves subtree `sub` (root at sub[0], children numbered within `sub` plus
+  // node_base) into `nodes`: its root into nodes[root_slot], the rest
+  // appended, child links shifted by where they land.
+  void splice(std::vector<NodeGpu>& nodes, size_t root_slot, const std::vector<NodeGpu>& sub) {
+    size_t offset = nodes.size() - 1;  // sub index i (i >= 1) lands at offset + i
+    nodes[root_slot] = sub[0];
+    if (sub[0].info[1] == 0) nodes[root_slot].info[0] += (uint32_t)offset;
+    for (size_t i = 1; i < sub.size(); ++i) {
+      NodeGpu n = sub[i];
+      if (n.info[1] == 0) n.info[0] += (uint32_t)offset;
+      nodes.push_back(n);
+    }
+  }
+};
+
+}  // namespace
+
+void build_flat_scene(const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, FlatScene& out,
+                      int threads) {
+  if (threads < 1) threads = 1;
+  out = FlatScene{};
+  out.nmeshes = nmeshes;
+  std::vector<uint64_t> first(nmeshes + 1, 0);
+  for (uint32_t m = 0; m < nmeshes; ++m) first[m + 1] = first[m] + mesh_counts[m];
+  const uint64_t total = first[nmeshes];
+  out.tris.resize(total * 12);
+  for (uint64_t t = 0; t < total; ++t)
+    for (int v = 0; v < 3; ++v) {
+      float* d = &out.tris[12 * t + 4 * v];
+      const float* s = &tri9[9 * t + 3 * v];
+      d[0] = s[0];
+      d[1] = s[1];
+      d[2] = s[2];
+      d[3] = 0.0f;
+    }
+
+  // Per-mesh triangle hierarchies, built concurrently, then concatenated in
+  // mesh order (each numbered from its final position).
+  std::vector<std::vector<NodeGpu>> mesh_nodes(nmeshes);
+  std::vector<std::vector<uint32_t>> mesh_items(nmeshes);
+  std::vector<Box> mesh_box(nmeshes);
+  std::vector<uint32_t> root_of(nmeshes, kNone);
+  // Node numbering needs each mesh's node count before its own; a tree over
+  // n > 0 items with leaves of at most L has a count fixed by n alone, so
+  // the counts are computed first.
+  auto node_count = [](uint64_t n, uint64_t leaf) {
+    // count(n) = 1 if n <= leaf else 1 + count(n/2) + count(n - n/2)
+    struct R {
+      static uint64_t f(uint64_t n, uint64_t leaf) {
+        if (n <= leaf) return 1;
+        return 1 + f(n / 2, leaf) + f(n - n / 2, leaf);
+      }
+    };
+    return R::f(n, leaf);
+  };
+  std::vector<uint64_t> node_first(nmeshes + 1, 0);
+  for (uint32_t m = 0; m < nmeshes; ++m)
+    node_first[m + 1] = node_first[m] + (mesh_counts[m] ? node_count(mesh_counts[m], kLeafTriangles) : 0);
+
+  std::atomic<uint32_t> next{0};
+  auto work = [&] {
+    for (;;) {
+      uint32_t m = next.fetch_add(1);
+      if (m >= nmeshes) break;
+      uint32_t count = mesh_counts[m];
+      mesh_box[m] = bounds_of(out.tris.data(), (uint32_t)first[m], count);
+      padded(mesh_box[m]);
+      if (count == 0) continue;
+      std::vector<Box> bounds(count);
+      for (uint32_t t = 0; t < count; ++t) {
+        bounds[t] = bounds_of(out.tris.data(), (uint32_t)first[m] + t, 1);
+        padded(bounds[t]);
+      }
+      std::vector<uint32_t> items(count);
+      std::iota(items.begin(), items.end(), 0u);
+      std::vector<NodeGpu>& nodes = mesh_nodes[m];
+      nodes.assign(1, NodeGpu{});
+      nodes.reserve(node_first[m + 1] - node_first[m]);
+      uint32_t root = (uint32_t)node_first[m];
+      Builder b{bounds, kLeafTriangles, root, (uint32_t)first[m], count > 1000000 ? 3 : 0};
+      b.split(nodes, 0, items.data(), count, 0, 0);
+      for (uint32_t& t : items) t += (uint32_t)first[m];
+      mesh_items[m] = std::move(items);
+      root_of[m] = root;
+    }
+  };
+  std::vector<std::thread> pool;
+  int nt = std::min<int>(threads, std::max<uint32_t>(1, nmeshes));
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+
+  out.blas.reserve(node_first[nmeshes]);
+  out.blas_items.reserve(total);
+  for (uint32_t m = 0; m < nmeshes; ++m) {
+    out.blas.insert(out.blas.end(), mesh_nodes[m].begin(), mesh_nodes[m].end());
+    out.blas_items.insert(out.blas_items.end(), mesh_items[m].begin(), mesh_items[m].end());
+    out.ranges.insert(out.ranges.end(), {(uint32_t)first[m], mesh_counts[m], root_of[m], kNone});
+  }
+
+  // The object hierarchy over meshes (object_hierarchy, hierarchy.rs:198-253).
+  std::vector<uint32_t> items(nmeshes);
+  std::iota(items.begin(), items.end(), 0u);
+  out.nodes.assign(1, NodeGpu{});
+  if (items.empty()) {
+    out.items = {0};
+    out.nodes[0].info[1] = 1;
+    return;
+  }
+  auto diagonal = [&](uint32_t m) {
+    float d2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      float e = mesh_box[m].hi[k] - mesh_box[m].lo[k];
+      d2 += e * e;
+    }
+    return std::sqrt(d2);
+  };
+  std::vector<float> sizes(nmeshes);
+  for (uint32_t m = 0; m < nmeshes; ++m) sizes[m] = diagonal(m);
+  size_t mid = sizes.size() / 2;
+  std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
+  const float median = sizes[mid];
+  std::vector<uint32_t> big, small;
+  for (uint32_t m : items) (diagonal(m) > kOversized * median ? big : small).push_back(m);
+  Builder ob{mesh_box, kLeafObjects, 0, 0, 0};
+  if (big.empty() || small.empty()) {
+    ob.split(out.nodes, 0, items.data(), items.size(), 0, 0);
+  } else {
+    const size_t nb = big.size();
+    items = big;
+    items.insert(items.end(), small.begin(), small.end());
+    out.nodes.push_back(NodeGpu{});
+    out.nodes.push_back(NodeGpu{});
+    ob.split(out.nodes, 1, items.data(), nb, 0, 0);
+    ob.split(out.nodes, 2, items.data() + nb, items.size() - nb, nb, 0);
+    NodeGpu& r = out.nodes[0];
+    for (int k = 0; k < 3; ++k) {
+      r.lo[k] = std::min(out.nodes[1].lo[k], out.nodes[2].lo[k]);
+      r.hi[k] = std::max(out.nodes[1].hi[k], out.nodes[2].hi[k]);
+    }
+    r.info[0] = 1;
+  }
+  out.items = items;
+}
+
+}  // namespace cc

@@ -1,0 +1,608 @@
+// The C ABI (include/continuum_cuda.h): contexts, resident scenes, and the
+// visibility calls. Host code; the kernels are in visibility.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/continuum_cuda.h"
+#include "bvh.h"
+#include "kernels.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  g_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA;
+}
+
+#define CC_CUDA(call, what)                      \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// A device allocation that grows on demand and is kept for reuse.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t size = 0;
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= size) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    size = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaSuccess) size = want;
+    return e;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    size = 0;
+  }
+};
+
+// The fraction of each bin of a sphere light's window inside the inscribed
+// disk (the reference's DISK table, mask_cones.wgsl:888-897): for the
+// circle of radius 4 bins centred on the 8x8 grid, each cell's area inside
+// it, integrated column by column with the exact chord, rounded to the six
+// decimals the reference's table carries.
+void disk_table(float* out) {
+  const int kSteps = 20000;
+  for (int b = 0; b < 64; ++b) {
+    const int col = b % 8, row = b / 8;
+    double area = 0.0;
+    for (int i = 0; i < kSteps; ++i) {
+      const double x = col + (i + 0.5) / kSteps - 4.0;
+      const double h2 = 16.0 - x * x;
+      if (h2 <= 0.0) continue;
+      const double h = std::sqrt(h2);
+      const double lo = std::max(row - 4.0, -h), hi = std::min(row + 1.0 - 4.0, h);
+      if (hi > lo) area += (hi - lo) / kSteps;
+    }
+    out[b] = (float)(std::round(area * 1e6) / 1e6);
+  }
+}
+
+}  // namespace
+
+struct cc_context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  DevBuf receivers, lights, full, any, partial, irradiance, fraction, work;
+  DevBuf redo;      // redo list
+  DevBuf counters;  // [redo count, error word]
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Kernel timing: three events per visibility call (before the packet pass,
+  // between the passes, after the solo pass) in a ring of kTimingRing calls.
+  static constexpr int kTimingRing = 256;
+  std::vector<cudaEvent_t> marks;  // 3 * kTimingRing
+  int timed_first = 0;             // oldest unread call in the ring
+  int timed_count = 0;             // unread calls
+};
+
+struct cc_scene {
+  cc_context* ctx = nullptr;
+  cc::FlatScene flat;  // host copy of the reference layouts
+  float4* tris = nullptr;
+  uint4* meshes = nullptr;
+  float4* nodes = nullptr;
+  uint32_t* items = nullptr;
+  float4* blas = nullptr;
+  uint32_t* blas_items = nullptr;
+  uint64_t bytes = 0;
+  cc::DevScene dev() const {
+    cc::DevScene s;
+    s.tris = tris;
+    s.meshes = meshes;
+    s.nodes = nodes;
+    s.items = items;
+    s.blas = blas;
+    s.blas_items = blas_items;
+    s.nmeshes = flat.nmeshes;
+    return s;
+  }
+};
+
+namespace {
+
+int set_device(cc_context* ctx) {
+  CC_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  return CC_OK;
+}
+
+// Repacks NodeGpu (48 bytes) into two float4 (lo.xyz | a, hi.xyz | b).
+std::vector<float4> repack(const std::vector<cc::NodeGpu>& nodes) {
+  std::vector<float4> out(2 * nodes.size());
+  for (size_t i = 0; i < nodes.size(); ++i) {
+    const cc::NodeGpu& n = nodes[i];
+    uint32_t a = n.info[0], b = n.info[1];
+    float fa, fb;
+    std::memcpy(&fa, &a, 4);
+    std::memcpy(&fb, &b, 4);
+    out[2 * i] = make_float4(n.lo[0], n.lo[1], n.lo[2], fa);
+    out[2 * i + 1] = make_float4(n.hi[0], n.hi[1], n.hi[2], fb);
+  }
+  return out;
+}
+
+template <class T>
+int upload(const std::vector<T>& host, T** dev, uint64_t& bytes, const char* what) {
+  size_t n = std::max<size_t>(host.size(), 1) * sizeof(T);
+  CC_CUDA(cudaMalloc(dev, n), what);
+  if (!host.empty()) CC_CUDA(cudaMemcpy(*dev, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), what);
+  bytes += n;
+  return CC_OK;
+}
+
+void free_scene_device(cc_scene* s) {
+  cudaFree(s->tris);
+  cudaFree(s->meshes);
+  cudaFree(s->nodes);
+  cudaFree(s->items);
+  cudaFree(s->blas);
+  cudaFree(s->blas_items);
+  s->tris = nullptr;
+  s->meshes = nullptr;
+  s->nodes = nullptr;
+  s->items = nullptr;
+  s->blas = nullptr;
+  s->blas_items = nullptr;
+}
+
+int upload_scene(cc_scene* s) {
+  const cc::FlatScene& f = s->flat;
+  std::vector<float4> tris(f.tris.size() / 4);
+  std::memcpy(tris.data(), f.tris.data(), f.tris.size() * sizeof(float));
+  std::vector<uint4> meshes(f.nmeshes);
+  for (uint32_t m = 0; m < f.nmeshes; ++m)
+    meshes[m] = make_uint4(f.ranges[4 * m], f.ranges[4 * m + 1], f.ranges[4 * m + 2], f.ranges[4 * m + 3]);
+  int rc;
+  if ((rc = upload(tris, &s->tris, s->bytes, "scene triangles"))) return rc;
+  if ((rc = upload(meshes, &s->meshes, s->bytes, "scene meshes"))) return rc;
+  if ((rc = upload(repack(f.nodes), &s->nodes, s->bytes, "scene nodes"))) return rc;
+  if ((rc = upload(f.items, &s->items, s->bytes, "scene items"))) return rc;
+  if ((rc = upload(repack(f.blas), &s->blas, s->bytes, "scene triangle nodes"))) return rc;
+  if ((rc = upload(f.blas_items, &s->blas_items, s->bytes, "scene triangle items"))) return rc;
+  return CC_OK;
+}
+
+int validate_flat(const cc::FlatScene& f) {
+  const uint64_t ntris = f.tris.size() / 12;
+  for (uint32_t m = 0; m < f.nmeshes; ++m) {
+    const uint32_t* r = &f.ranges[4 * m];
+    if ((uint64_t)r[0] + r[1] > ntris) return fail(CC_ERR_INVALID, "mesh range beyond the triangles");
+    if (r[2] != CC_NONE && r[2] >= f.blas.size()) return fail(CC_ERR_INVALID, "mesh hierarchy root out of range");
+    if (r[3] != CC_NONE) return fail(CC_ERR_INVALID, "instancing transforms are not supported by this call");
+  }
+  auto check_nodes = [&](const std::vector<cc::NodeGpu>& nodes, uint64_t nitems, const char* what) {
+    for (size_t i = 0; i < nodes.size(); ++i) {
+      const cc::NodeGpu& n = nodes[i];
+      if (n.info[1] > 0) {
+        if ((uint64_t)n.info[0] + n.info[1] > nitems) return fail(CC_ERR_INVALID, std::string(what) + ": leaf beyond its items");
+      } else if ((uint64_t)n.info[0] + 1 >= nodes.size() || n.info[0] <= i) {
+        return fail(CC_ERR_INVALID, std::string(what) + ": child index out of range");
+      }
+    }
+    return CC_OK;
+  };
+  int rc;
+  if ((rc = check_nodes(f.blas, f.blas_items.size(), "triangle hierarchy"))) return rc;
+  if ((rc = check_nodes(f.nodes, f.items.size(), "object hierarchy"))) return rc;
+  for (uint32_t t : f.blas_items)
+    if (t >= ntris) return fail(CC_ERR_INVALID, "triangle hierarchy item out of range");
+  for (uint32_t m : f.items)
+    if (m >= std::max<uint32_t>(f.nmeshes, 1)) return fail(CC_ERR_INVALID, "object hierarchy item out of range");
+  if (f.nodes.empty()) return fail(CC_ERR_INVALID, "empty object hierarchy");
+  return CC_OK;
+}
+
+int threads_for_build() {
+  unsigned n = std::thread::hardware_concurrency();
+  return n ? (int)std::min(n, 32u) : 4;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cc_last_error(void) { return g_error.c_str(); }
+
+void cc_options_default(cc_options* opt) {
+  if (!opt) return;
+  opt->hierarchy = 2;
+  opt->wide_extent = 8.0f;
+  opt->light_cone_cap = 4096;
+  opt->wide_cone_cap = 512;
+  opt->points_per_warp = 32;
+  opt->flags = 0;
+}
+
+int cc_context_create(int device, cc_context** out) {
+  if (!out) return fail(CC_ERR_INVALID, "null output");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(CC_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= n) return fail(CC_ERR_INVALID, "device index out of range");
+  cc_context* ctx = new cc_context;
+  ctx->device = device;
+  int rc = set_device(ctx);
+  if (rc) {
+    delete ctx;
+    return rc;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) ctx->sm_count = prop.multiProcessorCount;
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  float disk[64];
+  disk_table(disk);
+  if (e == cudaSuccess) e = cc::upload_disk_table(disk);
+  if (e == cudaSuccess) e = ctx->counters.reserve(2 * sizeof(uint32_t));
+  ctx->marks.assign(3 * cc_context::kTimingRing, nullptr);
+  for (auto& ev : ctx->marks)
+    if (e == cudaSuccess) e = cudaEventCreate(&ev);
+  if (e != cudaSuccess) {
+    int code = cuda_fail(e, "context setup");
+    cc_context_destroy(ctx);
+    return code;
+  }
+  *out = ctx;
+  return CC_OK;
+}
+
+int cc_context_destroy(cc_context* ctx) {
+  if (!ctx) return CC_OK;
+  cudaSetDevice(ctx->device);
+  for (DevBuf* b : {&ctx->receivers, &ctx->lights, &ctx->full, &ctx->any, &ctx->partial, &ctx->irradiance,
+                    &ctx->fraction, &ctx->work, &ctx->redo, &ctx->counters})
+    b->release();
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (auto ev : ctx->marks)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return CC_OK;
+}
+
+int cc_scene_upload(cc_context* ctx, const cc_flat_scene* fl, cc_scene** out) {
+  if (!ctx || !fl || !out) return fail(CC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (fl->ntris && !fl->tris) return fail(CC_ERR_INVALID, "null triangles");
+  if (!fl->ranges || !fl->nodes || !fl->items || fl->nnodes == 0)
+    return fail(CC_ERR_INVALID, "a flat scene needs ranges, nodes and items");
+  cc_scene* s = new cc_scene;
+  s->ctx = ctx;
+  cc::FlatScene& f = s->flat;
+  f.nmeshes = fl->nmeshes;
+  f.tris.assign(fl->tris, fl->tris + (size_t)fl->ntris * 12);
+  f.ranges.assign(fl->ranges, fl->ranges + (size_t)fl->nmeshes * 4);
+  const cc::NodeGpu* b = static_cast<const cc::NodeGpu*>(fl->blas);
+  if (fl->nblas && !b) {
+    delete s;
+    return fail(CC_ERR_INVALID, "null triangle hierarchy");
+  }
+  if (b) f.blas.assign(b, b + fl->nblas);
+  if (fl->blas_items) f.blas_items.assign(fl->blas_items, fl->blas_items + fl->nblas_items);
+  const cc::NodeGpu* n = static_cast<const cc::NodeGpu*>(fl->nodes);
+  f.nodes.assign(n, n + fl->nnodes);
+  f.items.assign(fl->items, fl->items + fl->nitems);
+  int rc = validate_flat(f);
+  if (!rc) rc = set_device(ctx);
+  if (!rc) rc = upload_scene(s);
+  if (rc) {
+    free_scene_device(s);
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return CC_OK;
+}
+
+int cc_scene_build(cc_context* ctx, const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes,
+                   cc_scene** out) {
+  if (!out || (nmeshes && !mesh_counts)) return fail(CC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  uint64_t total = 0;
+  for (uint32_t m = 0; m < nmeshes; ++m) total += mesh_counts[m];
+  if (total && !tri9) return fail(CC_ERR_INVALID, "null triangles");
+  if (total >= 0xffffffffull) return fail(CC_ERR_INVALID, "too many triangles");
+  cc_scene* s = new cc_scene;
+  s->ctx = ctx;
+  cc::build_flat_scene(tri9, mesh_counts, nmeshes, s->flat, threads_for_build());
+  if (!ctx) {  // host-only scene
+    *out = s;
+    return CC_OK;
+  }
+  int rc = set_device(ctx);
+  if (!rc) rc = upload_scene(s);
+  if (rc) {
+    free_scene_device(s);
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return CC_OK;
+}
+
+int cc_scene_destroy(cc_scene* s) {
+  if (!s) return CC_OK;
+  if (s->ctx) {
+    cudaSetDevice(s->ctx->device);
+    free_scene_device(s);
+  }
+  delete s;
+  return CC_OK;
+}
+
+int cc_scene_sizes(const cc_scene* s, uint64_t out6[6]) {
+  if (!s || !out6) return fail(CC_ERR_INVALID, "null argument");
+  out6[0] = s->flat.tris.size() / 12;
+  out6[1] = s->flat.nmeshes;
+  out6[2] = s->flat.blas.size();
+  out6[3] = s->flat.blas_items.size();
+  out6[4] = s->flat.nodes.size();
+  out6[5] = s->flat.items.size();
+  return CC_OK;
+}
+
+int cc_scene_arrays(const cc_scene* s, uint32_t* ranges, void* blas, uint32_t* blas_items, void* nodes,
+                    uint32_t* items) {
+  if (!s) return fail(CC_ERR_INVALID, "null scene");
+  const cc::FlatScene& f = s->flat;
+  if (ranges) std::memcpy(ranges, f.ranges.data(), f.ranges.size() * 4);
+  if (blas) std::memcpy(blas, f.blas.data(), f.blas.size() * sizeof(cc::NodeGpu));
+  if (blas_items) std::memcpy(blas_items, f.blas_items.data(), f.blas_items.size() * 4);
+  if (nodes) std::memcpy(nodes, f.nodes.data(), f.nodes.size() * sizeof(cc::NodeGpu));
+  if (items) std::memcpy(items, f.items.data(), f.items.size() * 4);
+  return CC_OK;
+}
+
+uint64_t cc_scene_device_bytes(const cc_scene* s) { return s ? s->bytes : 0; }
+
+int cc_context_kernel_times(cc_context* ctx, float* out2, int max_calls) {
+  if (!ctx || (max_calls > 0 && !out2)) return fail(CC_ERR_INVALID, "null argument");
+  int rc = set_device(ctx);
+  if (rc) return -rc;
+  const int ring = cc_context::kTimingRing;
+  int n = 0;
+  while (ctx->timed_count > 0) {
+    cudaEvent_t* m = &ctx->marks[3 * ctx->timed_first];
+    cudaError_t e = cudaEventSynchronize(m[2]);
+    if (e != cudaSuccess) return -cuda_fail(e, "kernel timing");
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, m[0], m[1]);
+    cudaEventElapsedTime(&b, m[1], m[2]);
+    if (n < max_calls) {
+      out2[2 * n] = a;
+      out2[2 * n + 1] = b;
+      ++n;
+    }
+    ctx->timed_first = (ctx->timed_first + 1) % ring;
+    ctx->timed_count--;
+  }
+  return n;
+}
+
+int cc_scene_primary_hits(const cc_scene* s, const float camera[10], uint32_t width, uint32_t height, float* out8,
+                          uint8_t* hit) {
+  if (!s || !camera || !out8 || !hit) return fail(CC_ERR_INVALID, "null argument");
+  if (s->flat.nodes.empty()) return fail(CC_ERR_INVALID, "scene has no hierarchy");
+  cc::primary_hits(s->flat, camera, width, height, out8, hit, threads_for_build());
+  return CC_OK;
+}
+
+int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                  const float* lights, uint32_t nlights, const cc_options* opt_in, const cc_outputs* out,
+                  void* stream_in) {
+  if (!ctx || !scene || !out) return fail(CC_ERR_INVALID, "null argument");
+  if (scene->ctx != ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
+  if ((npoints && !receivers) || (nlights && !lights)) return fail(CC_ERR_INVALID, "null inputs");
+  cc_options opt;
+  if (opt_in) opt = *opt_in; else cc_options_default(&opt);
+  if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
+  if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
+  const uint64_t ncones = npoints * (uint64_t)nlights;
+  if (ncones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one call");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  cudaStream_t stream = stream_in ? (cudaStream_t)stream_in : ctx->stream;
+  const bool device_ptrs = (opt.flags & CC_DEVICE_POINTERS) != 0;
+
+  cc::DevQuery q;
+  q.npoints = npoints;
+  q.nlights = nlights;
+  q.hierarchy = opt.hierarchy;
+  q.wide_extent = opt.wide_extent;
+  q.light_cone_cap = opt.light_cone_cap;
+  q.wide_cone_cap = opt.wide_cone_cap;
+  cc::DevOut o{};
+  if (device_ptrs) {
+    q.receivers = reinterpret_cast<const float4*>(receivers);
+    q.lights = reinterpret_cast<const float4*>(lights);
+    o.full = reinterpret_cast<uint2*>(out->full);
+    o.any = reinterpret_cast<uint2*>(out->any);
+    o.partial = out->partial;
+    o.irradiance = out->irradiance;
+    o.fraction = out->fraction;
+    o.work = reinterpret_cast<uint4*>(out->work);
+  } else {
+    CC_CUDA(ctx->receivers.reserve(npoints * 32), "receivers buffer");
+    CC_CUDA(ctx->lights.reserve((size_t)nlights * 64), "lights buffer");
+    CC_CUDA(cudaMemcpyAsync(ctx->receivers.ptr, receivers, npoints * 32, cudaMemcpyHostToDevice, stream), "receivers upload");
+    CC_CUDA(cudaMemcpyAsync(ctx->lights.ptr, lights, (size_t)nlights * 64, cudaMemcpyHostToDevice, stream), "lights upload");
+    q.receivers = static_cast<const float4*>(ctx->receivers.ptr);
+    q.lights = static_cast<const float4*>(ctx->lights.ptr);
+    if (out->full) { CC_CUDA(ctx->full.reserve(ncones * 8), "output"); o.full = static_cast<uint2*>(ctx->full.ptr); }
+    if (out->any) { CC_CUDA(ctx->any.reserve(ncones * 8), "output"); o.any = static_cast<uint2*>(ctx->any.ptr); }
+    if (out->partial) { CC_CUDA(ctx->partial.reserve(ncones * 256), "output"); o.partial = static_cast<float*>(ctx->partial.ptr); }
+    if (out->irradiance) { CC_CUDA(ctx->irradiance.reserve(ncones * 4), "output"); o.irradiance = static_cast<float*>(ctx->irradiance.ptr); }
+    if (out->fraction) { CC_CUDA(ctx->fraction.reserve(ncones * 4), "output"); o.fraction = static_cast<float*>(ctx->fraction.ptr); }
+    if (out->work) { CC_CUDA(ctx->work.reserve(ncones * 16), "output"); o.work = static_cast<uint4*>(ctx->work.ptr); }
+  }
+  uint32_t* counters = static_cast<uint32_t*>(ctx->counters.ptr);
+  o.redo_count = counters;
+  o.error = counters + 1;
+  if (!(opt.flags & CC_NO_REDO)) {
+    CC_CUDA(ctx->redo.reserve(std::max<uint64_t>(ncones, 1) * 4), "redo list");
+    o.redo_list = static_cast<uint32_t*>(ctx->redo.ptr);
+    o.redo_capacity = (uint32_t)std::max<uint64_t>(ncones, 1);
+  }
+  CC_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), stream), "counter reset");
+  // The call's slot in the timing ring (the oldest unread call is dropped
+  // when the ring is full).
+  const int ring = cc_context::kTimingRing;
+  if (ctx->timed_count == ring) {
+    ctx->timed_first = (ctx->timed_first + 1) % ring;
+    ctx->timed_count--;
+  }
+  const int slot = (ctx->timed_first + ctx->timed_count) % ring;
+  ctx->timed_count++;
+  CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
+                                &ctx->marks[3 * slot]),
+          "visibility launch");
+  if (device_ptrs) return CC_OK;
+
+  if (out->full) CC_CUDA(cudaMemcpyAsync(out->full, o.full, ncones * 8, cudaMemcpyDeviceToHost, stream), "download");
+  if (out->any) CC_CUDA(cudaMemcpyAsync(out->any, o.any, ncones * 8, cudaMemcpyDeviceToHost, stream), "download");
+  if (out->partial) CC_CUDA(cudaMemcpyAsync(out->partial, o.partial, ncones * 256, cudaMemcpyDeviceToHost, stream), "download");
+  if (out->irradiance) CC_CUDA(cudaMemcpyAsync(out->irradiance, o.irradiance, ncones * 4, cudaMemcpyDeviceToHost, stream), "download");
+  if (out->fraction) CC_CUDA(cudaMemcpyAsync(out->fraction, o.fraction, ncones * 4, cudaMemcpyDeviceToHost, stream), "download");
+  if (out->work) CC_CUDA(cudaMemcpyAsync(out->work, o.work, ncones * 16, cudaMemcpyDeviceToHost, stream), "download");
+  uint32_t host_counters[2] = {0, 0};
+  CC_CUDA(cudaMemcpyAsync(host_counters, counters, sizeof(host_counters), cudaMemcpyDeviceToHost, stream), "status download");
+  CC_CUDA(cudaStreamSynchronize(stream), "visibility");
+  if (host_counters[1] & 2u) return fail(CC_ERR_STACK, "a traversal stack overflowed");
+  if (host_counters[1] & 1u) return fail(CC_ERR_INVALID, "solo re-walk list overflowed");
+  return CC_OK;
+}
+
+static void receivers_from6(const float* r6, uint64_t n, std::vector<float>& out) {
+  out.assign(n * 8, 0.0f);
+  for (uint64_t i = 0; i < n; ++i) {
+    out[8 * i + 0] = r6[6 * i + 0];
+    out[8 * i + 1] = r6[6 * i + 1];
+    out[8 * i + 2] = r6[6 * i + 2];
+    out[8 * i + 4] = r6[6 * i + 3];
+    out[8 * i + 5] = r6[6 * i + 4];
+    out[8 * i + 6] = r6[6 * i + 5];
+  }
+}
+
+// RectLight -> LightGpu (lib.rs:722-728).
+static void light_from9(const float* l9, int one_sided, float* out16) {
+  std::memset(out16, 0, 16 * sizeof(float));
+  for (int k = 0; k < 3; ++k) {
+    out16[k] = l9[k];
+    out16[4 + k] = l9[3 + k];
+    out16[8 + k] = l9[6 + k];
+  }
+  out16[3] = one_sided ? 1.0f : 0.0f;
+  out16[12] = out16[13] = out16[14] = 1.0f;
+}
+
+int cc_irradiance(cc_context* ctx, const float* receivers6, uint64_t npoints, const float* light9, int one_sided,
+                  const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, uint32_t hierarchy,
+                  uint32_t runs, float* out, double* best_seconds) {
+  if (!ctx || !light9 || !out || (npoints && !receivers6)) return fail(CC_ERR_INVALID, "null argument");
+  if (hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
+  cc_scene* scene = nullptr;
+  int rc = cc_scene_build(ctx, tri9, mesh_counts, nmeshes, &scene);
+  if (rc) return rc;
+  std::vector<float> rec;
+  receivers_from6(receivers6, npoints, rec);
+  float light[16];
+  light_from9(light9, one_sided, light);
+  cc_options opt;
+  cc_options_default(&opt);
+  opt.hierarchy = hierarchy;
+  opt.flags = CC_DEVICE_POINTERS;
+  // Inputs and the output on the device, then `runs` timed executions.
+  float4* d_rec = nullptr;
+  float4* d_light = nullptr;
+  float* d_out = nullptr;
+  auto cleanup = [&] {
+    cudaFree(d_rec);
+    cudaFree(d_light);
+    cudaFree(d_out);
+    cc_scene_destroy(scene);
+  };
+  cudaError_t e = cudaMalloc(&d_rec, std::max<uint64_t>(npoints, 1) * 32);
+  if (e == cudaSuccess) e = cudaMalloc(&d_light, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, std::max<uint64_t>(npoints, 1) * 4);
+  if (e == cudaSuccess && npoints) e = cudaMemcpy(d_rec, rec.data(), npoints * 32, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_light, light, 64, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cleanup();
+    return cuda_fail(e, "irradiance inputs");
+  }
+  cc_outputs o{};
+  o.irradiance = d_out;
+  double best = INFINITY;
+  for (uint32_t r = 0; r < std::max(runs, 1u); ++r) {
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    rc = cc_visibility(ctx, scene, reinterpret_cast<const float*>(d_rec), npoints, reinterpret_cast<const float*>(d_light),
+                       1, &opt, &o, ctx->stream);
+    if (rc) {
+      cleanup();
+      return rc;
+    }
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    e = cudaEventSynchronize(ctx->ev1);
+    if (e != cudaSuccess) {
+      cleanup();
+      return cuda_fail(e, "irradiance");
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    best = std::min(best, ms * 1e-3);
+  }
+  uint32_t host_counters[2] = {0, 0};
+  e = cudaMemcpy(host_counters, ctx->counters.ptr, sizeof(host_counters), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && npoints) e = cudaMemcpy(out, d_out, npoints * 4, cudaMemcpyDeviceToHost);
+  cleanup();
+  if (e != cudaSuccess) return cuda_fail(e, "irradiance download");
+  if (host_counters[1] & 2u) return fail(CC_ERR_STACK, "a traversal stack overflowed");
+  if (best_seconds) *best_seconds = best;
+  return CC_OK;
+}
+
+int cc_coverage(cc_context* ctx, const float* receivers6, uint64_t npoints, const float* light9, int one_sided,
+                const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, float* out64) {
+  if (!ctx || !light9 || !out64 || (npoints && !receivers6)) return fail(CC_ERR_INVALID, "null argument");
+  cc_scene* scene = nullptr;
+  int rc = cc_scene_build(ctx, tri9, mesh_counts, nmeshes, &scene);
+  if (rc) return rc;
+  std::vector<float> rec;
+  receivers_from6(receivers6, npoints, rec);
+  float light[16];
+  light_from9(light9, one_sided, light);
+  cc_options opt;
+  cc_options_default(&opt);
+  opt.hierarchy = 0;
+  cc_outputs o{};
+  o.partial = out64;
+  rc = cc_visibility(ctx, scene, rec.data(), npoints, light, 1, &opt, &o, nullptr);
+  cc_scene_destroy(scene);
+  return rc;
+}
+
+}  // extern "C"

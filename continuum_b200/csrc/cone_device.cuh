@@ -1,0 +1,599 @@
+// Device-side cone geometry for the mask-cone visibility kernels (sm_100a).
+//
+// One lane owns one cone. The geometry follows the reference's WGSL light-cone
+// path (crates/continuum-gpu/src/mask_cones.wgsl, cited per function); the
+// per-cone state that the WGSL keeps in private arrays (64 coverages, the
+// 68-cell accumulator) lives here in shared memory, lane-interleaved
+// (cell * 32 + lane), so every access is bank-conflict-free whatever cell
+// each lane touches.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cc {
+
+constexpr int kGrid = 8;
+constexpr int kBins = 64;
+constexpr uint32_t kNoneU = 0xffffffffu;
+constexpr float kNear = 1e-4f;  // NEAR, mask_cones.wgsl:213
+
+// ---- small vector helpers -------------------------------------------------
+struct f3 {
+  float x, y, z;
+};
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ f3 div(f3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ f3 normalize(f3 a) { return div(a, len(a)); }
+__device__ __forceinline__ f3 xyz(float4 v) { return {v.x, v.y, v.z}; }
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+// ---- device scene and query -------------------------------------------------
+// Nodes are two float4: (lo.xyz, a) and (hi.xyz, b) with a, b as bits:
+// leaf: a = first item, b = item count; interior: a = left child, b = 0.
+struct DevScene {
+  const float4* tris;      // 3 per triangle (w unused)
+  const uint4* meshes;     // first, count, blas root, transform
+  const float4* nodes;     // object hierarchy, 2 per node
+  const uint32_t* items;   // mesh per object leaf slot
+  const float4* blas;      // triangle hierarchies, 2 per node
+  const uint32_t* blas_items;
+  uint32_t nmeshes;
+};
+
+struct DevLight {
+  f3 corner;
+  float kind;  // corner.w: 0 two-sided rect, 1 one-sided rect, 2 sphere
+  f3 eu;
+  f3 ev;
+  float evw;   // spot on (sphere)
+};
+
+__device__ __forceinline__ DevLight load_light(const float4* lights, uint32_t l) {
+  float4 a = __ldg(&lights[4 * l + 0]);
+  float4 b = __ldg(&lights[4 * l + 1]);
+  float4 c = __ldg(&lights[4 * l + 2]);
+  DevLight L;
+  L.corner = xyz(a);
+  L.kind = a.w;
+  L.eu = xyz(b);
+  L.ev = xyz(c);
+  L.evw = c.w;
+  return L;
+}
+
+__device__ __forceinline__ bool is_sphere(const DevLight& r) { return r.kind > 1.5f; }
+
+// ---- the cone ----------------------------------------------------------------
+// mask_cones.wgsl:136-155. The far plane's normal is the cone's forward axis
+// for every light cone (:924, :1034), so only its offset is kept; light
+// cones have no horizon.
+struct Cone {
+  f3 apex, right, up, fwd;
+  float u0, v0, u1, v1;
+  float far_offset;
+  f3 baxis;
+  float bcos, bsin;
+};
+
+__device__ __forceinline__ f3 direction(const Cone& c, float s, float t) {  // :203-206
+  return c.fwd + c.right * (c.u0 + s * (c.u1 - c.u0)) + c.up * (c.v0 + t * (c.v1 - c.v0));
+}
+
+__device__ __forceinline__ f3 to_local(const Cone& c, f3 p) {  // :208-211
+  f3 d = p - c.apex;
+  return {dot(c.right, d), dot(c.up, d), dot(c.fwd, d)};
+}
+
+__device__ __forceinline__ bool in_bound(const Cone& c, f3 p, float r) {  // :159-168
+  if (c.bcos < -1.0f) return true;
+  f3 d = p - c.apex;
+  float l = len(d);
+  if (l <= r) return true;
+  float s = r / l;
+  float limit = c.bcos * sqrtf(1.0f - s * s) - c.bsin * s;
+  return dot(c.baxis, d) >= limit * l;
+}
+
+__device__ __forceinline__ void bound_cone(Cone& c, f3 axis) {  // :174-186
+  float cos_half = 1.0f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    f3 d = normalize(direction(c, float(k & 1), float(k >> 1)));
+    cos_half = fminf(cos_half, dot(axis, d));
+  }
+  float cb = clampf(cos_half - 1e-5f, -1.0f, 1.0f);
+  c.baxis = axis;
+  c.bcos = cb;
+  c.bsin = sqrtf(fmaxf(1.0f - cb * cb, 0.0f));
+}
+
+struct LightConeInfo {
+  bool ok;
+  bool wide_clipped;
+  bool wide_window;
+};
+
+// light_cone_sphere (:902-931)
+__device__ __forceinline__ LightConeInfo light_cone_sphere(f3 apex, const DevLight& r, float wide_extent, Cone& c) {
+  LightConeInfo info{false, false, false};
+  f3 to_center = r.corner - apex;
+  float d = len(to_center);
+  float radius = r.eu.x;
+  if (d <= radius * 1.0001f) return info;
+  f3 fwd = div(to_center, d);
+  float s = radius / d;
+  float t = s / sqrtf(fmaxf(1.0f - s * s, 1e-12f));
+  info.wide_clipped = 2.0f * t > wide_extent;
+  info.wide_window = info.wide_clipped;
+  t = fminf(t, 0.5f * wide_extent);
+  f3 helper = fabsf(fwd.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+  f3 right = normalize(cross(helper, fwd));
+  c.apex = apex;
+  c.right = right;
+  c.up = cross(fwd, right);
+  c.fwd = fwd;
+  c.u0 = -t;
+  c.v0 = -t;
+  c.u1 = t;
+  c.v1 = t;
+  c.far_offset = dot(fwd, apex) + (d - radius * s) * (1.0f - 1e-5f);
+  bound_cone(c, fwd);
+  info.ok = true;
+  return info;
+}
+
+// light_cone_rect (:974-1042)
+__device__ __forceinline__ LightConeInfo light_cone(f3 apex, const DevLight& r, float wide_extent, Cone& c) {
+  if (is_sphere(r)) return light_cone_sphere(apex, r, wide_extent, c);
+  LightConeInfo info{false, false, false};
+  f3 fwd = normalize(cross(r.eu, r.ev));
+  if (r.kind > 0.5f && dot(fwd, apex - r.corner) <= 0.0f) return info;
+  if (dot(fwd, r.corner - apex) < 0.0f) fwd = -fwd;
+  float dist = dot(fwd, r.corner - apex);
+  if (dist <= 1e-6f) return info;
+  f3 right = normalize(r.eu);
+  f3 up = cross(fwd, right);
+  f3 rel = r.corner - apex;
+  float lo0 = 3.4e38f, lo1 = 3.4e38f, hi0 = -3.4e38f, hi1 = -3.4e38f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    f3 corner = rel + r.eu * float(k & 1) + r.ev * float((k >> 1) & 1);
+    float u = dot(right, corner) / dist, v = dot(up, corner) / dist;
+    lo0 = fminf(lo0, u);
+    lo1 = fminf(lo1, v);
+    hi0 = fmaxf(hi0, u);
+    hi1 = fmaxf(hi1, v);
+  }
+  float ext0 = hi0 - lo0, ext1 = hi1 - lo1;
+  float foot0 = fminf(fmaxf(0.0f, lo0), hi0), foot1 = fminf(fmaxf(0.0f, lo1), hi1);
+  f3 mid = normalize(mk(0.5f * (lo0 + hi0), 0.5f * (lo1 + hi1), 1.0f));
+  float cos_wide = 1.0f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    f3 q = mk((k & 1) ? hi0 : lo0, (k & 2) ? hi1 : lo1, 1.0f);
+    cos_wide = fminf(cos_wide, dot(mid, normalize(q)));
+  }
+  const float size = wide_extent;
+  info.wide_window = ext0 > size || ext1 > size;
+  info.wide_clipped = info.wide_window && cos_wide < 0.8660254f;
+  if (info.wide_clipped) {
+    if (ext0 > size) {
+      float keep = fminf(fmaxf(foot0 - 0.5f * size, lo0), hi0 - size);
+      lo0 = keep;
+      hi0 = keep + size;
+    }
+    if (ext1 > size) {
+      float keep = fminf(fmaxf(foot1 - 0.5f * size, lo1), hi1 - size);
+      lo1 = keep;
+      hi1 = keep + size;
+    }
+  }
+  c.apex = apex;
+  c.right = right;
+  c.up = up;
+  c.fwd = fwd;
+  c.u0 = lo0;
+  c.v0 = lo1;
+  c.u1 = hi0;
+  c.v1 = hi1;
+  c.far_offset = dot(fwd, apex) + dist * (1.0f - 1e-5f);
+  f3 axis = normalize(rel + (r.eu + r.ev) * 0.5f);
+  if (info.wide_clipped) axis = normalize(direction(c, 0.5f, 0.5f));
+  bound_cone(c, axis);
+  info.ok = true;
+  return info;
+}
+
+// ---- culling ---------------------------------------------------------------
+// may_touch_box (:234-255), which is node_cone_test (:519-574) for exact cones.
+__device__ __forceinline__ bool may_touch_box(const Cone& c, f3 lo, f3 hi) {
+  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    f3 corner = mk((k & 1) ? hi.x : lo.x, (k & 2) ? hi.y : lo.y, (k & 4) ? hi.z : lo.z);
+    if (c.far_offset - dot(c.fwd, corner) >= 0.0f) far_out = false;
+    f3 p = to_local(c, corner);
+    if (p.z >= kNear) near_out = false;
+    if (p.x - c.u0 * p.z >= 0.0f) out_u0 = false;
+    if (c.u1 * p.z - p.x >= 0.0f) out_u1 = false;
+    if (p.y - c.v0 * p.z >= 0.0f) out_v0 = false;
+    if (c.v1 * p.z - p.y >= 0.0f) out_v1 = false;
+  }
+  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1) return false;
+  return in_bound(c, (lo + hi) * 0.5f, 0.5f * len(hi - lo));
+}
+
+// may_touch (:215-232)
+__device__ __forceinline__ bool may_touch(const Cone& c, f3 v0, f3 v1, f3 v2) {
+  float f0 = c.far_offset - dot(c.fwd, v0);
+  float f1 = c.far_offset - dot(c.fwd, v1);
+  float f2 = c.far_offset - dot(c.fwd, v2);
+  if (f0 < 0.0f && f1 < 0.0f && f2 < 0.0f) return false;
+  f3 p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
+  if (p0.z < kNear && p1.z < kNear && p2.z < kNear) return false;
+  if (p0.x - c.u0 * p0.z < 0.0f && p1.x - c.u0 * p1.z < 0.0f && p2.x - c.u0 * p2.z < 0.0f) return false;
+  if (c.u1 * p0.z - p0.x < 0.0f && c.u1 * p1.z - p1.x < 0.0f && c.u1 * p2.z - p2.x < 0.0f) return false;
+  if (p0.y - c.v0 * p0.z < 0.0f && p1.y - c.v0 * p1.z < 0.0f && p2.y - c.v0 * p2.z < 0.0f) return false;
+  if (c.v1 * p0.z - p0.y < 0.0f && c.v1 * p1.z - p1.y < 0.0f && c.v1 * p2.z - p2.y < 0.0f) return false;
+  return true;
+}
+
+// ---- the accumulation rasterizer ------------------------------------------------
+// The lane's 68-cell accumulator (the WGSL's `acc`, :719-760) in shared
+// memory, cell-major with the lane innermost. Cells 64..65 receive writes
+// "one past the last row" that no resolve ever reads, so they are dropped.
+struct LaneAcc {
+  float* base;  // &acc[lane]; cell k at base[32 * k]
+  uint32_t span_lo, span_hi;
+  __device__ __forceinline__ void add(uint32_t cell, float v) {
+    if (cell < (uint32_t)kBins) base[32 * cell] += v;
+  }
+};
+
+// draw_edge (:297-348)
+__device__ __forceinline__ void draw_edge(LaneAcc& acc, float q0x, float q0y, float q1x, float q1y, float weight) {
+  if (fabsf(q0y - q1y) <= 1.1920929e-7f) return;
+  float dir = 1.0f;
+  float p0x = q0x, p0y = q0y, p1x = q1x, p1y = q1y;
+  if (q0y > q1y) {
+    dir = -1.0f;
+    p0x = q1x;
+    p0y = q1y;
+    p1x = q0x;
+    p1y = q0y;
+  }
+  const float dxdy = (p1x - p0x) / (p1y - p0y);
+  float x = p0x;
+  const uint32_t y_end = min((uint32_t)ceilf(p1y), (uint32_t)kGrid);
+  for (uint32_t y = (uint32_t)p0y; y < y_end; ++y) {
+    const uint32_t row = y * kGrid;
+    acc.span_lo = min(acc.span_lo, row);
+    acc.span_hi = max(acc.span_hi, row + kGrid + 1);
+    float dy = fminf(float(y + 1), p1y) - fmaxf(float(y), p0y);
+    float x_next = clampf(x + dxdy * dy, 0.0f, float(kGrid));
+    float d = dy * dir * weight;
+    float x0 = fminf(x, x_next), x1 = fmaxf(x, x_next);
+    float x0_floor = floorf(x0);
+    uint32_t x0i = (uint32_t)x0_floor;
+    float x1_ceil = ceilf(x1);
+    uint32_t x1i = (uint32_t)x1_ceil;
+    if (x1i <= x0i + 1) {
+      float xmf = 0.5f * (x + x_next) - x0_floor;
+      acc.add(row + x0i, d - d * xmf);
+      acc.add(row + x0i + 1, d * xmf);
+    } else {
+      float s = 1.0f / (x1 - x0);
+      float x0f = x0 - x0_floor;
+      float a0 = 0.5f * s * (1.0f - x0f) * (1.0f - x0f);
+      float x1f = x1 - x1_ceil + 1.0f;
+      float am = 0.5f * s * x1f * x1f;
+      acc.add(row + x0i, d * a0);
+      if (x1i == x0i + 2) {
+        acc.add(row + x0i + 1, d * (1.0f - a0 - am));
+      } else {
+        float a1 = s * (1.5f - x0f);
+        acc.add(row + x0i + 1, d * (a1 - a0));
+        for (uint32_t xi = x0i + 2; xi < x1i - 1; ++xi) acc.add(row + xi, d * s);
+        float a2 = a1 + float(x1i - x0i - 3) * s;
+        acc.add(row + x1i - 1, d * (1.0f - a2 - am));
+      }
+      acc.add(row + x1i, d * am);
+    }
+    x = x_next;
+  }
+}
+
+// Polygons of the general clip path. The WGSL holds 10 vertices
+// (mask_cones.wgsl:11); a triangle clipped by the far and near planes has
+// at most 5, the window square clipped by 5 edge planes at most 9, and four
+// rounding-dust clips at the square's sides can add one each, so 16 holds
+// every case.
+constexpr int kPolyCap = 16;
+
+// clip_plane3 (:264-277), in place through a scratch copy.
+__device__ __forceinline__ int clip_plane3(const f3* in, int n, f3* out, f3 normal, float offset) {
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    f3 a = in[i], b = in[(i + 1) % n];
+    float da = offset - dot(normal, a), db = offset - dot(normal, b);
+    if (da >= 0.0f && m < kPolyCap) out[m++] = a;
+    if (da >= 0.0f && db < 0.0f && m < kPolyCap) out[m++] = a + (b - a) * (da / (da - db));
+    if (da < 0.0f && db >= 0.0f && m < kPolyCap) out[m++] = b + (a - b) * (db / (db - da));
+  }
+  return m;
+}
+
+// clip_line2 (:280-294)
+__device__ __forceinline__ int clip_line2(const float2* in, int n, float2* out, float nx, float ny, float offset) {
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    float2 a = in[i], b = in[(i + 1) % n];
+    float da = offset - (nx * a.x + ny * a.y);
+    float db = offset - (nx * b.x + ny * b.y);
+    if (da >= 0.0f && m < kPolyCap) out[m++] = a;
+    if (da >= 0.0f && db < 0.0f && m < kPolyCap) {
+      float f = da / (da - db);
+      out[m++] = make_float2(a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f);
+    }
+    if (da < 0.0f && db >= 0.0f && m < kPolyCap) {
+      float f = db / (db - da);
+      out[m++] = make_float2(b.x + (a.x - b.x) * f, b.y + (a.y - b.y) * f);
+    }
+  }
+  return m;
+}
+
+__device__ __forceinline__ void draw_polygon(LaneAcc& acc, const float2* q, int n) {
+  const float g = float(kGrid);
+  for (int i = 0; i < n; ++i) {
+    float2 a = q[i], b = q[(i + 1) % n];
+    draw_edge(acc, clampf(a.x, 0.f, g), clampf(a.y, 0.f, g), clampf(b.x, 0.f, g), clampf(b.y, 0.f, g), 1.0f);
+  }
+}
+
+// The clipped polygon in bin space, drawn (general path of rasterize,
+// :350-451): far and near clips, then either the projected corners or, for a
+// polygon reaching outside the window, the window square clipped to the
+// planes through the apex and each edge; finally the square's sides.
+static __device__ __noinline__ bool rasterize_general(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2, bool far_clip) {
+  f3 pa[kPolyCap], pb[kPolyCap];
+  pa[0] = v0;
+  pa[1] = v1;
+  pa[2] = v2;
+  int n = 3;
+  f3* p = pa;
+  f3* other = pb;
+  if (far_clip) {
+    n = clip_plane3(p, n, other, c.fwd, c.far_offset);
+    f3* t = p;
+    p = other;
+    other = t;
+  }
+  bool all_near_ok = true, all_in_window = true;
+  for (int i = 0; i < n; ++i) {
+    f3 v = to_local(c, p[i]);
+    p[i] = v;
+    if (v.z < kNear) all_near_ok = false;
+    if (v.x < c.u0 * v.z || v.x > c.u1 * v.z || v.y < c.v0 * v.z || v.y > c.v1 * v.z) all_in_window = false;
+  }
+  if (!all_near_ok) {
+    n = clip_plane3(p, n, other, mk(0.f, 0.f, -1.f), -kNear);
+    f3* t = p;
+    p = other;
+    other = t;
+  }
+  if (n < 3) return false;
+  const float su = float(kGrid) / (c.u1 - c.u0);
+  const float sv = float(kGrid) / (c.v1 - c.v0);
+  const float g = float(kGrid);
+  float2 qa[kPolyCap], qb[kPolyCap];
+  float2* q = qa;
+  float2* q2 = qb;
+  int m;
+  if (all_near_ok && all_in_window) {
+    m = n;
+    for (int i = 0; i < n; ++i) q[i] = make_float2((p[i].x / p[i].z - c.u0) * su, (p[i].y / p[i].z - c.v0) * sv);
+  } else {
+    f3 l0 = to_local(c, v0), l1 = to_local(c, v1), l2 = to_local(c, v2);
+    float d = dot(l0, cross(l1, l2));
+    if (d == 0.0f) return false;
+    float side = d > 0.0f ? 1.0f : -1.0f;
+    m = 4;
+    q[0] = make_float2(0.f, 0.f);
+    q[2] = make_float2(g, g);
+    if (side > 0.0f) {
+      q[1] = make_float2(g, 0.f);
+      q[3] = make_float2(0.f, g);
+    } else {
+      q[1] = make_float2(0.f, g);
+      q[3] = make_float2(g, 0.f);
+    }
+    for (int i = 0; i < n; ++i) {
+      f3 e = cross(p[i], p[(i + 1) % n]);
+      float l = len(e);
+      if (l == 0.0f) continue;
+      f3 k = e * (side / l);
+      m = clip_line2(q, m, q2, -k.x / su, -k.y / sv, k.x * c.u0 + k.y * c.v0 + k.z);
+      float2* t = q;
+      q = q2;
+      q2 = t;
+    }
+  }
+  bool inside = true;
+  for (int i = 0; i < m; ++i)
+    if (q[i].x < 0.f || q[i].y < 0.f || q[i].x > g || q[i].y > g) inside = false;
+  if (!inside) {
+    m = clip_line2(q, m, q2, -1.f, 0.f, 0.f);
+    m = clip_line2(q2, m, q, 1.f, 0.f, g);
+    m = clip_line2(q, m, q2, 0.f, -1.f, 0.f);
+    m = clip_line2(q2, m, q, 0.f, 1.f, g);
+  }
+  if (m < 3) return false;
+  draw_polygon(acc, q, m);
+  return true;
+}
+
+// rasterize (:350-451). The common case — a triangle wholly inside the
+// window between the near and far planes — projects its three corners and
+// draws them from registers; everything else takes the general path.
+__device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2) {
+  float f0 = c.far_offset - dot(c.fwd, v0);
+  float f1 = c.far_offset - dot(c.fwd, v1);
+  float f2 = c.far_offset - dot(c.fwd, v2);
+  bool far_clip = f0 < 0.0f || f1 < 0.0f || f2 < 0.0f;
+  if (!far_clip) {
+    f3 p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
+    auto in_win = [&](f3 v) {
+      return v.z >= kNear && !(v.x < c.u0 * v.z || v.x > c.u1 * v.z || v.y < c.v0 * v.z || v.y > c.v1 * v.z);
+    };
+    if (in_win(p0) && in_win(p1) && in_win(p2)) {
+      const float su = float(kGrid) / (c.u1 - c.u0);
+      const float sv = float(kGrid) / (c.v1 - c.v0);
+      const float g = float(kGrid);
+      float ax = (p0.x / p0.z - c.u0) * su, ay = (p0.y / p0.z - c.v0) * sv;
+      float bx = (p1.x / p1.z - c.u0) * su, by = (p1.y / p1.z - c.v0) * sv;
+      float cx = (p2.x / p2.z - c.u0) * su, cy = (p2.y / p2.z - c.v0) * sv;
+      bool inside = ax >= 0.f && ay >= 0.f && ax <= g && ay <= g && bx >= 0.f && by >= 0.f && bx <= g &&
+                    by <= g && cx >= 0.f && cy >= 0.f && cx <= g && cy <= g;
+      if (inside) {
+        draw_edge(acc, ax, ay, bx, by, 1.0f);
+        draw_edge(acc, bx, by, cx, cy, 1.0f);
+        draw_edge(acc, cx, cy, ax, ay, 1.0f);
+        return true;
+      }
+    }
+  }
+  return rasterize_general(c, acc, v0, v1, v2, far_clip);
+}
+
+// ---- integration --------------------------------------------------------------
+// lambert_edge_unit / lambert_edge (:188-201)
+__device__ __forceinline__ float lambert_edge_unit(f3 n, f3 an, f3 bn) {
+  f3 g = cross(an, bn);
+  float l = len(g);
+  if (l > 1e-12f) return atan2f(l, dot(an, bn)) * dot(n, div(g, l));
+  return 0.0f;
+}
+__device__ __forceinline__ float lambert_edge(f3 n, f3 a, f3 b) { return lambert_edge_unit(n, normalize(a), normalize(b)); }
+
+// The quad d[0..4] clipped to dot(n, x) >= 0 and Lambert-integrated
+// (clipped_bin_weight / clipped_window_weight, :1331-1403; rect_open :2177-2199).
+__device__ __forceinline__ float clipped_quad_weight(f3 n, f3 d0, f3 d1, f3 d2, f3 d3) {
+  f3 d[4] = {d0, d1, d2, d3};
+  f3 poly[6];
+  int k_n = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    f3 a = d[k], e = d[(k + 1) & 3];
+    float sa = dot(n, a), se = dot(n, e);
+    if (sa >= 0.0f) poly[k_n++] = a;
+    if ((sa >= 0.0f) != (se >= 0.0f)) poly[k_n++] = a + (e - a) * (sa / (sa - se));
+  }
+  if (k_n < 3) return 0.0f;
+  float sum = 0.0f;
+  for (int k = 0; k < k_n; ++k) sum += lambert_edge(n, poly[k], poly[(k + 1) % k_n]);
+  return fabsf(0.5f * sum);
+}
+
+// bin_weight (:1232-1242)
+__device__ __forceinline__ float bin_weight(const Cone& c, f3 n, int b) {
+  const float g = float(kGrid);
+  float col = float(b % kGrid), row = float(b / kGrid);
+  f3 d0 = direction(c, col / g, row / g);
+  f3 d1 = direction(c, (col + 1.f) / g, row / g);
+  f3 d2 = direction(c, (col + 1.f) / g, (row + 1.f) / g);
+  f3 d3 = direction(c, col / g, (row + 1.f) / g);
+  return fabsf(0.5f * (lambert_edge(n, d0, d1) + lambert_edge(n, d1, d2) + lambert_edge(n, d2, d3) +
+                       lambert_edge(n, d3, d0)));
+}
+
+__device__ __forceinline__ float clipped_bin_weight(const Cone& c, f3 n, int b) {  // :1331-1369
+  const float g = float(kGrid);
+  float col = float(b % kGrid), row = float(b / kGrid);
+  f3 d0 = direction(c, col / g, row / g);
+  f3 d1 = direction(c, (col + 1.f) / g, row / g);
+  f3 d2 = direction(c, (col + 1.f) / g, (row + 1.f) / g);
+  f3 d3 = direction(c, col / g, (row + 1.f) / g);
+  int above = (dot(n, d0) > 0.f) + (dot(n, d1) > 0.f) + (dot(n, d2) > 0.f) + (dot(n, d3) > 0.f);
+  if (above == 4) return bin_weight(c, n, b);
+  if (above == 0) return 0.0f;
+  return clipped_quad_weight(n, d0, d1, d2, d3);
+}
+
+__device__ __forceinline__ float window_weight(const Cone& c, f3 n, bool* all_above) {
+  f3 d00 = direction(c, 0.f, 0.f), d10 = direction(c, 1.f, 0.f);
+  f3 d11 = direction(c, 1.f, 1.f), d01 = direction(c, 0.f, 1.f);
+  *all_above = dot(n, d00) > 0.f && dot(n, d10) > 0.f && dot(n, d11) > 0.f && dot(n, d01) > 0.f;
+  if (*all_above)
+    return fabsf(0.5f * (lambert_edge(n, d00, d10) + lambert_edge(n, d10, d11) + lambert_edge(n, d11, d01) +
+                         lambert_edge(n, d01, d00)));
+  return clipped_quad_weight(n, d00, d10, d11, d01);
+}
+
+// ---- lights: gating and the unshadowed denominator -------------------------------
+__device__ __forceinline__ f3 light_center(const DevLight& r) {  // :866-869
+  if (is_sphere(r)) return r.corner;
+  return r.corner + (r.eu + r.ev) * 0.5f;
+}
+
+__device__ __forceinline__ float spot_falloff(const DevLight& r, f3 w) {  // :872-876
+  if (!is_sphere(r) || r.evw < 0.5f) return 1.0f;
+  float a = clampf(dot(r.ev, w) * r.eu.y + r.eu.z, 0.0f, 1.0f);
+  return a * a;
+}
+
+__device__ __forceinline__ bool faces_light(const DevLight& r, f3 point, f3 normal) {  // :880-884
+  f3 to_light = light_center(r) - point;
+  if (is_sphere(r)) return dot(normal, to_light) > -r.eu.x;
+  return dot(normal, to_light) > 0.0f;
+}
+
+__device__ __forceinline__ float rect_open(f3 point, f3 normal, const DevLight& r) {  // :2148-2199
+  f3 c0 = r.corner - point;
+  float facing = dot(normalize(cross(r.eu, r.ev)), c0);
+  if ((r.kind > 0.5f && facing >= 0.0f) || fabsf(facing) <= 1e-6f) return 0.0f;
+  f3 d1 = c0 + r.eu, d2 = c0 + r.eu + r.ev, d3 = c0 + r.ev;
+  if (dot(normal, c0) >= 0.f && dot(normal, d1) >= 0.f && dot(normal, d2) >= 0.f && dot(normal, d3) >= 0.f) {
+    f3 a0 = normalize(c0), a1 = normalize(d1), a2 = normalize(d2), a3 = normalize(d3);
+    float sum = 0.0f;
+    sum += lambert_edge_unit(normal, a0, a1);
+    sum += lambert_edge_unit(normal, a1, a2);
+    sum += lambert_edge_unit(normal, a2, a3);
+    sum += lambert_edge_unit(normal, a3, a0);
+    return fabsf(0.5f * sum);
+  }
+  return clipped_quad_weight(normal, c0, d1, d2, d3);
+}
+
+__device__ __forceinline__ float sphere_unshadowed(f3 point, f3 normal, const DevLight& r) {  // :937-952
+  f3 to_center = r.corner - point;
+  float d2 = dot(to_center, to_center);
+  float radius = r.eu.x;
+  if (d2 <= radius * radius) return 0.0f;
+  float sin2 = radius * radius / d2;
+  float cos_t = clampf(dot(normal, to_center) * (1.0f / sqrtf(d2)), -1.0f, 1.0f);
+  if (cos_t * cos_t > sin2) return 3.14159265f * sin2 * fmaxf(cos_t, 0.0f);
+  float sin_t = sqrtf(1.0f - cos_t * cos_t);
+  float x = sqrtf(1.0f / sin2 - 1.0f);
+  float y = clampf(-x * cos_t / sin_t, -1.0f, 1.0f);
+  float q = sin_t * sqrtf(1.0f - y * y);
+  return fmaxf((cos_t * acosf(y) - x * q) * sin2 + atanf(q / x), 0.0f);
+}
+
+// unshadowed_rect (:2135-2141)
+__device__ __forceinline__ float unshadowed(f3 point, f3 normal, const DevLight& r) {
+  if (!faces_light(r, point, normal)) return 0.0f;
+  if (is_sphere(r)) return spot_falloff(r, normalize(point - r.corner)) * sphere_unshadowed(point, normal, r);
+  return rect_open(point, normal, r);
+}
+
+}  // namespace cc

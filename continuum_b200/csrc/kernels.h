@@ -1,0 +1,47 @@
+// Launch interface between the host library and the device kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "cone_device.cuh"
+
+namespace cc {
+
+constexpr int kWarpsPerBlock = 4;
+
+struct DevQuery {
+  const float4* receivers;  // 2 per point: point, normal
+  const float4* lights;     // 4 per light (LightGpu)
+  uint64_t npoints;
+  uint32_t nlights;
+  uint32_t hierarchy;
+  float wide_extent;
+  uint32_t light_cone_cap;
+  uint32_t wide_cone_cap;
+};
+
+struct DevOut {
+  uint2* full;
+  uint2* any;
+  float* partial;
+  float* irradiance;
+  float* fraction;
+  uint4* work;
+  // Scratch: cones to walk again alone, their count, the list's capacity,
+  // and an error word (bit 0: list overflow, bit 1: stack overflow).
+  uint32_t* redo_list;
+  uint32_t* redo_count;
+  uint32_t redo_capacity;
+  uint32_t* error;
+};
+
+cudaError_t upload_disk_table(const float* table64);
+
+// The packet pass over every cone, then (with o.redo_list) the solo pass over
+// the cones it listed. o.redo_count and o.error must be zero on entry.
+// `marks` (nullable): three events recorded before the packet pass, between
+// the passes and after the solo pass.
+cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t points_per_warp,
+                              bool count_work, int sm_count, cudaStream_t stream, const cudaEvent_t* marks);
+
+}  // namespace cc

@@ -1,0 +1,402 @@
+// The plain visibility kernel: one warp walks a packet of up to 32 cones
+// (neighbouring points toward one light) through the scene hierarchy
+// together; each lane tests, rasterizes and integrates its own cone.
+//
+// What the reference does per invocation (mask_cones.wgsl `main` :1513-1520
+// -> hit_irradiance_rect :2125 -> cone_irradiance_rect :1286) is done here
+// per lane, with the packet walk of the reference's PACKETS mode
+// (packet_any, :666-711) built from warp votes:
+//  * the traversal stack is warp-uniform and lives in registers spread over
+//    the lanes (entry i in lane i % 32), so a push is one predicated move and
+//    a pop one shuffle — no shared or local memory;
+//  * each lane keeps a bit per stack entry saying whether its own walk needs
+//    that entry (need_get/need_put, :694-711);
+//  * node and triangle records are loaded by every lane from the same
+//    address, which the load unit serves as one broadcast transaction.
+// Results depend on the walk order only through the walk caps: the packet
+// takes its child order from its first lane that descends; a lane whose own
+// nearest-first order differs somewhere on its walk, and whose walk then
+// stopped early (capped, or every bin full), is listed and walked again
+// alone by a second launch, so every cone's result is the one its own walk
+// gives (the reference's walk without packets, as its view-cache bakes run).
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "cone_device.cuh"
+#include "kernels.h"
+
+namespace cc {
+
+__constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded by the host
+
+constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
+
+struct WarpStack {
+  uint32_t r0 = 0, r1 = 0;  // entry i held by lane i % 32, register i / 32
+  uint32_t need_lo = 0, need_hi = 0;
+  __device__ __forceinline__ void push(int i, uint32_t v, int lane) {
+    if ((i & 31) == lane) {
+      if (i < 32) r0 = v; else r1 = v;
+    }
+  }
+  __device__ __forceinline__ uint32_t get(int i) const {
+    return __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
+  }
+  __device__ __forceinline__ bool need(int i) const {
+    return ((i < 32 ? need_lo : need_hi) >> (i & 31)) & 1u;
+  }
+  __device__ __forceinline__ void set_need(int i, bool v) {
+    uint32_t bit = 1u << (i & 31);
+    if (i < 32) need_lo = v ? (need_lo | bit) : (need_lo & ~bit);
+    else need_hi = v ? (need_hi | bit) : (need_hi & ~bit);
+  }
+};
+
+struct LaneState {
+  Cone cone;
+  f3 d00, d10, d01, d11;  // window corner directions
+  float* cov;             // &cov[lane]; bin b at cov[32 * b]
+  float* acc;             // &acc[lane]
+  uint32_t full;
+  uint32_t cone_work;
+  uint32_t cap;
+  uint32_t status;
+  uint32_t n_obj, n_blas, n_tris;
+};
+
+__device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
+
+template <bool kCount>
+__device__ __forceinline__ bool cover_triangle(const DevScene& s, LaneState& st, LaneAcc& acc, uint32_t t) {
+  if (kCount) st.n_tris++;
+  const Cone& c = st.cone;
+  f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
+  f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
+  f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
+  f3 n = cross(v1 - v0, v2 - v0);
+  if (dot(n, c.apex - v0) <= 0.0f) return false;  // faces away (:600)
+  if (dot(n, st.d00) >= 0.f && dot(n, st.d10) >= 0.f && dot(n, st.d01) >= 0.f && dot(n, st.d11) >= 0.f)
+    return false;  // every window direction leaves its plane (:601-606)
+  if (!may_touch(c, v0, v1, v2)) return false;
+  return rasterize(c, acc, v0, v1, v2);
+}
+
+// add_mesh_coverage_if (:713-829) for the lanes with `on`; the others
+// follow the packet's walk. The triangle hierarchy's stack entries start at
+// `base`, above the object walk's.
+template <bool kCount>
+__device__ __forceinline__ void add_mesh(const DevScene& s, uint32_t hierarchy, LaneState& st, WarpStack& stk,
+                                         bool on, uint32_t m, int base, int lane) {
+  if (!__any_sync(0xffffffffu, on)) return;
+  const uint4 range = __ldg(&s.meshes[m]);
+  LaneAcc acc{st.acc, 68u, 0u};
+  bool touched = false;
+  if (hierarchy == 2) {
+    if (range.z != kNoneU) {
+      int sp = base;
+      stk.push(sp, range.z, lane);
+      stk.set_need(sp, on);
+      ++sp;
+      while (sp > base) {
+        --sp;
+        const uint32_t n = stk.get(sp);
+        const bool mine = stk.need(sp) && st.cone_work < st.cap;
+        if (mine) st.cone_work++;
+        if (!__any_sync(0xffffffffu, mine)) continue;
+        const float4 a = __ldg(&s.blas[2 * (size_t)n + 0]);
+        const float4 b = __ldg(&s.blas[2 * (size_t)n + 1]);
+        bool descend = false;
+        if (mine) {
+          if (kCount) st.n_blas++;
+          descend = may_touch_box(st.cone, node_lo(a), node_lo(b));
+        }
+        if (!__any_sync(0xffffffffu, descend)) continue;
+        const uint32_t ia = __float_as_uint(a.w), ib = __float_as_uint(b.w);
+        if (ib > 0) {
+          if (descend) st.cone_work += ib;
+          for (uint32_t k = ia; k < ia + ib; ++k) {
+            const uint32_t t = __ldg(&s.blas_items[k]);
+            if (descend && cover_triangle<kCount>(s, st, acc, t)) touched = true;
+          }
+        } else {
+          if (sp + 2 > kStack) {
+            if (descend) st.status |= 2u;
+            continue;
+          }
+          // Right child popped first (:783-787).
+          stk.push(sp, ia, lane);
+          stk.push(sp + 1, ia + 1, lane);
+          stk.set_need(sp, descend);
+          stk.set_need(sp + 1, descend);
+          sp += 2;
+        }
+      }
+    }
+  } else {
+    for (uint32_t t = range.x; t < range.x + range.y; ++t)
+      if (on && cover_triangle<kCount>(s, st, acc, t)) touched = true;
+  }
+  // The mesh's coverage: running sum over the touched cells, snapped to
+  // whole within 1e-5, combined into the cone's bins by max (:809-828).
+  const uint32_t end = min(acc.span_hi, (uint32_t)kBins);
+  if (touched) {
+    float running = 0.0f;
+    for (uint32_t b = acc.span_lo; b < end; ++b) {
+      running += st.acc[32 * b];
+      float covered = fabsf(running);
+      if (covered >= 1.0f - 1e-5f) covered = 1.0f;
+      if (covered > 1e-6f) {
+        const float before = st.cov[32 * b];
+        const float after = fmaxf(before, fminf(covered, 1.0f));
+        st.cov[32 * b] = after;
+        if (before < 1.0f && after >= 1.0f) st.full++;
+      }
+    }
+  }
+  for (uint32_t b = acc.span_lo; b < end; ++b) st.acc[32 * b] = 0.0f;
+}
+
+// scene_coverage_if (:1160-1227): the object hierarchy, nearest child first
+// along the bounding cone's axis, until every bin is full or the cap.
+template <bool kCount>
+__device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState& st, bool traced,
+                                           int lane) {
+  WarpStack stk;
+  if (hierarchy >= 1) {
+    int sp = 0;
+    stk.push(0, 0u, lane);
+    stk.set_need(0, traced);
+    sp = 1;
+    while (sp > 0) {
+      --sp;
+      const uint32_t n = stk.get(sp);
+      const bool mine = stk.need(sp) && st.full < (uint32_t)kBins && st.cone_work < st.cap;
+      if (mine) st.cone_work++;
+      if (!__any_sync(0xffffffffu, mine)) continue;
+      const float4 a = __ldg(&s.nodes[2 * (size_t)n + 0]);
+      const float4 b = __ldg(&s.nodes[2 * (size_t)n + 1]);
+      bool descend = false;
+      if (mine) {
+        if (kCount) st.n_obj++;
+        descend = may_touch_box(st.cone, node_lo(a), node_lo(b));
+      }
+      if (!__any_sync(0xffffffffu, descend)) continue;
+      const uint32_t ia = __float_as_uint(a.w), ib = __float_as_uint(b.w);
+      if (ib > 0) {
+        for (uint32_t k = ia; k < ia + ib; ++k) add_mesh<kCount>(s, hierarchy, st, stk, descend, __ldg(&s.items[k]), sp, lane);
+      } else {
+        const float4 la = __ldg(&s.nodes[2 * (size_t)ia + 0]);
+        const float4 lb = __ldg(&s.nodes[2 * (size_t)ia + 1]);
+        const float4 ra = __ldg(&s.nodes[2 * (size_t)ia + 2]);
+        const float4 rb = __ldg(&s.nodes[2 * (size_t)ia + 3]);
+        const Cone& c = st.cone;
+        const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
+        const float db = dot(c.baxis, (node_lo(ra) + node_lo(rb)) * 0.5f - c.apex);
+        const bool pref = db < da;  // this lane's own order: right child nearer
+        const uint32_t voters = __ballot_sync(0xffffffffu, descend);
+        const bool swap = __shfl_sync(0xffffffffu, pref, __ffs(voters) - 1);
+        if (descend && pref != swap) st.status |= 4u;
+        const uint32_t near_ = swap ? ia + 1 : ia, far_ = swap ? ia : ia + 1;
+        if (sp + 2 > kStack) {
+          if (descend) st.status |= 2u;
+          continue;
+        }
+        stk.push(sp, far_, lane);
+        stk.push(sp + 1, near_, lane);
+        stk.set_need(sp, descend);
+        stk.set_need(sp + 1, descend);
+        sp += 2;
+      }
+    }
+  } else {
+    for (uint32_t m = 0; m < s.nmeshes; ++m) add_mesh<kCount>(s, hierarchy, st, stk, traced && st.full < (uint32_t)kBins, m, 0, lane);
+  }
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    visibility_kernel(DevScene s, DevQuery q, DevOut o, const uint32_t* __restrict__ list,
+                      const uint32_t* __restrict__ list_count, uint32_t pw) {
+  extern __shared__ float smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  float* cov_base = smem + (size_t)wib * (2 * kBins * 32);
+  float* acc_base = cov_base + kBins * 32;
+  for (int k = 0; k < kBins; ++k) acc_base[32 * k + lane] = 0.0f;
+
+  const uint64_t ncones = list ? (uint64_t)min(*list_count, o.redo_capacity) : q.npoints * (uint64_t)q.nlights;
+  const uint64_t warps = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t wbase = ((uint64_t)blockIdx.x * kWarpsPerBlock + wib) * pw; wbase < ncones; wbase += warps * pw) {
+    const uint64_t slot = wbase + lane;
+    const bool valid = (uint32_t)lane < pw && slot < ncones;
+    const uint64_t c = valid ? (list ? (uint64_t)list[slot] : slot) : 0;
+    const uint32_t l = (uint32_t)(c / q.npoints);
+    const uint64_t p = c - (uint64_t)l * q.npoints;
+
+    LaneState st;
+    st.cov = cov_base + lane;
+    st.acc = acc_base + lane;
+    st.full = 0;
+    st.cone_work = 0;
+    st.status = 0;
+    st.n_obj = st.n_blas = st.n_tris = 0;
+    for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 0.0f;
+
+    const DevLight L = load_light(q.lights, valid ? l : 0);
+    const float4 pt4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 0]);
+    const float4 nm4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 1]);
+    const f3 point = xyz(pt4), normal = xyz(nm4);
+
+    // hit_irradiance_rect (:2125-2128): spot falloff and the facing test gate
+    // the cone.
+    const float spot = spot_falloff(L, normalize(point - light_center(L)));
+    const bool on = valid && spot > 0.0f && faces_light(L, point, normal);
+    st.cone = Cone{};
+    const LightConeInfo info = light_cone(point, L, q.wide_extent, st.cone);
+    const bool traced = on && info.ok;
+    st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
+    st.d00 = direction(st.cone, 0.f, 0.f);
+    st.d10 = direction(st.cone, 1.f, 0.f);
+    st.d01 = direction(st.cone, 0.f, 1.f);
+    st.d11 = direction(st.cone, 1.f, 1.f);
+
+    scene_walk<kCount>(s, q.hierarchy, st, traced, lane);
+
+    // A grazing sliver stopped at its cap counts as blocked (:1295-1305).
+    const bool capped = traced && st.cone_work >= st.cap;
+    if (capped) st.status |= 1u;
+    if (capped && info.wide_window && !info.wide_clipped) {
+      for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 1.0f;
+      st.full = kBins;
+    }
+    if (traced && st.full >= (uint32_t)kBins) st.status |= 16u;
+
+    uint32_t fw0 = 0, fw1 = 0, aw0 = 0, aw1 = 0;
+    for (int k = 0; k < kBins; ++k) {
+      const float v = st.cov[32 * k];
+      const uint32_t bit = 1u << (k & 31);
+      if (v >= 1.0f) { if (k < 32) fw0 |= bit; else fw1 |= bit; }
+      if (v > 0.0f) { if (k < 32) aw0 |= bit; else aw1 |= bit; }
+    }
+    const bool last_empty = (aw0 | aw1) == 0u;
+    const bool last_full = (fw0 & fw1) == 0xffffffffu;
+
+    float value = 0.0f;
+    if (traced) {
+      const Cone& cn = st.cone;
+      if (is_sphere(L)) {
+        // sphere_open_share (:957-972)
+        float total = 0.0f, open = 0.0f;
+        const float g = float(kGrid);
+        for (int b = 0; b < kBins; ++b) {
+          const float mfrac = info.wide_clipped ? 1.0f : c_disk[b];
+          if (mfrac <= 0.0f) continue;
+          f3 d = direction(cn, (float(b % kGrid) + 0.5f) / g, (float(b / kGrid) + 0.5f) / g);
+          float l2 = dot(d, d);
+          float w = mfrac * fmaxf(dot(normal, d), 0.0f) / (l2 * l2);
+          total += w;
+          open += w * (1.0f - st.cov[32 * b]);
+        }
+        const float share = total <= 0.0f ? 1.0f : open / total;
+        value = sphere_unshadowed(point, normal, L) * share;
+      } else {
+        // cone_visible (:1244-1272) and wide_visible (:1070-1073)
+        bool all_above;
+        const float total = window_weight(cn, normal, &all_above);
+        float blocked = 0.0f;
+        for (int b = 0; b < kBins; ++b) {
+          const float cv = st.cov[32 * b];
+          if (cv > 0.0f) blocked += cv * (all_above ? bin_weight(cn, normal, b) : clipped_bin_weight(cn, normal, b));
+        }
+        float visible = fmaxf(total - blocked, 0.0f);
+        if (info.wide_clipped) visible = (total > 1e-9f ? visible / total : 1.0f) * rect_open(point, normal, L);
+        value = visible;
+      }
+    }
+    value *= spot;
+    // The lighting cache's ratio (vc_bake :3453-3510, static light).
+    const float open = unshadowed(point, normal, L);
+    float ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
+    if (open > 0.0f && last_empty) ratio = 1.0f;
+    if (open > 0.0f && last_full) ratio = 0.0f;
+
+    if (list) st.status |= 8u;
+    const bool redo = !list && o.redo_list && (st.status & 4u) && (st.status & (1u | 16u));
+    if (redo) {
+      const uint32_t at = atomicAdd(o.redo_count, 1u);
+      if (at < o.redo_capacity) o.redo_list[at] = (uint32_t)c;
+      else atomicOr(o.error, 1u);
+    }
+    if (st.status & 2u) atomicOr(o.error, 2u);
+    if (valid && !redo) {
+      if (o.full) o.full[c] = make_uint2(fw0, fw1);
+      if (o.any) o.any[c] = make_uint2(aw0, aw1);
+      if (o.irradiance) o.irradiance[c] = value;
+      if (o.fraction) o.fraction[c] = ratio;
+      if (o.work) o.work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
+      if (o.partial) {
+        float4* dst = reinterpret_cast<float4*>(o.partial + 64 * c);
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k)
+          dst[k] = make_float4(st.cov[32 * (4 * k)], st.cov[32 * (4 * k + 1)], st.cov[32 * (4 * k + 2)],
+                               st.cov[32 * (4 * k + 3)]);
+      }
+    }
+  }
+}
+
+// ---- host-side launchers --------------------------------------------------------
+
+cudaError_t upload_disk_table(const float* table64) {
+  return cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
+}
+
+static bool g_attr_set[2] = {false, false};
+
+template <bool kCount>
+static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const uint32_t* list,
+                              const uint32_t* list_count, uint32_t pw, uint32_t blocks, cudaStream_t stream) {
+  const size_t smem = (size_t)kWarpsPerBlock * 2 * kBins * 32 * sizeof(float);
+  if (!g_attr_set[kCount]) {
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    g_attr_set[kCount] = true;
+  }
+  visibility_kernel<kCount><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, list, list_count, pw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t pw, bool count,
+                              int sm_count, cudaStream_t stream, const cudaEvent_t* marks) {
+  if (pw < 1) pw = 1;
+  if (pw > 32) pw = 32;
+  const uint64_t ncones = q.npoints * (uint64_t)q.nlights;
+  if (marks) cudaEventRecord(marks[0], stream);
+  if (ncones == 0) {
+    if (marks) {
+      cudaEventRecord(marks[1], stream);
+      cudaEventRecord(marks[2], stream);
+    }
+    return cudaSuccess;
+  }
+  const uint64_t packets = (ncones + pw - 1) / pw;
+  // Enough blocks to fill every SM several times over; each warp then strides
+  // over packets.
+  const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const uint64_t cap = (uint64_t)sm_count * 24;
+  const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
+  cudaError_t e = count ? launch_one<true>(s, q, o, nullptr, nullptr, pw, blocks, stream)
+                        : launch_one<false>(s, q, o, nullptr, nullptr, pw, blocks, stream);
+  if (marks) cudaEventRecord(marks[1], stream);
+  if (e != cudaSuccess) return e;
+  if (o.redo_list) {
+    // The listed cones, each walked alone (one lane per warp).
+    const uint32_t solo_blocks = (uint32_t)sm_count * 4;
+    e = count ? launch_one<true>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+              : launch_one<false>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+  }
+  if (marks) cudaEventRecord(marks[2], stream);
+  return e;
+}
+
+}  // namespace cc

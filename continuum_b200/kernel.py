@@ -1,0 +1,395 @@
+"""The reference-facing visibility API over the CUDA library.
+
+Mirrors ``continuum_gpu::MaskConeKernel`` (crates/continuum-gpu/src/lib.rs:65-120)
+for the mask-cone light path: ``irradiance`` / ``irradiance_with``
+(lib.rs:1706-1730), ``coverage`` (lib.rs:3289-3298) and the light types
+``RectLight`` / ``Light`` / ``SphereLight`` / ``Spot`` (lib.rs:552-609), plus
+resident scenes and the multi-light ``visibility`` call with FULL/ANY mask
+words, per-bin coverage and visible fractions.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from enum import IntEnum
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import CCError, check, load, ptr
+
+
+class Hierarchy(IntEnum):
+    """How far cones descend before testing triangles (hierarchy.rs:731-749)."""
+
+    NONE = 0
+    MESHES = 1
+    TRIANGLES = 2
+
+    @staticmethod
+    def of(x) -> "Hierarchy":
+        if isinstance(x, bool):  # impl From<bool> for Hierarchy (hierarchy.rs:751-760)
+            return Hierarchy.TRIANGLES if x else Hierarchy.NONE
+        return Hierarchy(int(x))
+
+
+def _v3(v) -> np.ndarray:
+    a = np.asarray(v, dtype=np.float32).reshape(3)
+    return a
+
+
+@dataclass(frozen=True)
+class RectLight:
+    """A rectangular light: a corner and two perpendicular edges (lib.rs:552-566)."""
+
+    corner: Sequence[float]
+    edge_u: Sequence[float]
+    edge_v: Sequence[float]
+    one_sided: bool = False
+
+
+@dataclass(frozen=True)
+class Spot:
+    """A spot's cone as glTF's: half-angles in radians (lib.rs:588-599)."""
+
+    axis: Sequence[float]
+    inner: float
+    outer: float
+
+
+@dataclass(frozen=True)
+class SphereLight:
+    """A spherical light seen from outside as a disk (lib.rs:576-586)."""
+
+    center: Sequence[float]
+    radius: float
+    spot: Optional[Spot] = None
+
+
+@dataclass(frozen=True)
+class Light:
+    """A light and its RGB radiance (lib.rs:568-574)."""
+
+    emitter: object
+    radiance: Sequence[float] = (1.0, 1.0, 1.0)
+
+    @staticmethod
+    def rect(rect: RectLight, radiance=(1.0, 1.0, 1.0)) -> "Light":
+        return Light(rect, tuple(radiance))
+
+    @staticmethod
+    def white(rect: RectLight, radiance: float) -> "Light":
+        return Light(rect, (radiance,) * 3)
+
+    @staticmethod
+    def point(center, radius: float, intensity=(1.0, 1.0, 1.0)) -> "Light":
+        rad = tuple(float(i) / (math.pi * radius * radius) for i in intensity)
+        return Light(SphereLight(tuple(center), float(radius)), rad)
+
+    @staticmethod
+    def spot(center, radius: float, intensity, spot: Spot) -> "Light":
+        base = Light.point(center, radius, intensity)
+        return Light(SphereLight(tuple(center), float(radius), spot), base.radiance)
+
+    def as_rect(self) -> Optional[RectLight]:
+        return self.emitter if isinstance(self.emitter, RectLight) else None
+
+
+def light_gpu(light) -> np.ndarray:
+    """The 16-float record the kernels read (LightGpu, lib.rs:710-749)."""
+    if isinstance(light, RectLight):
+        light = Light(light)
+    out = np.zeros(16, dtype=np.float32)
+    out[12:15] = np.asarray(light.radiance, dtype=np.float32)
+    e = light.emitter
+    if isinstance(e, RectLight):
+        out[0:3] = _v3(e.corner)
+        out[3] = 1.0 if e.one_sided else 0.0
+        out[4:7] = _v3(e.edge_u)
+        out[8:11] = _v3(e.edge_v)
+    elif isinstance(e, SphereLight):
+        out[0:3] = _v3(e.center)
+        out[3] = 2.0
+        if e.spot is not None:
+            scale = 1.0 / max(math.cos(e.spot.inner) - math.cos(e.spot.outer), 1e-3)
+            axis = np.asarray(e.spot.axis, dtype=np.float64)
+            axis = axis / np.linalg.norm(axis)
+            out[4:7] = (e.radius, scale, -math.cos(e.spot.outer) * scale)
+            out[8:11] = axis
+            out[11] = 1.0
+        else:
+            out[4:7] = (e.radius, 0.0, 1.0)
+            out[8:11] = (0.0, 0.0, 1.0)
+    else:
+        raise TypeError(f"not a light: {light!r}")
+    return out
+
+
+def lights_gpu(lights: Iterable) -> np.ndarray:
+    return np.stack([light_gpu(l) for l in lights]).astype(np.float32)
+
+
+def receivers_gpu(receivers) -> np.ndarray:
+    """(N, 8) float32 from (point, normal) pairs given as (N, 2, 3) or (N, 6)."""
+    r = np.asarray(receivers, dtype=np.float32)
+    if r.ndim == 2 and r.shape[1] == 8:
+        return np.ascontiguousarray(r)
+    r = r.reshape(-1, 6)
+    out = np.zeros((r.shape[0], 8), dtype=np.float32)
+    out[:, 0:3] = r[:, 0:3]
+    out[:, 4:7] = r[:, 3:6]
+    return out
+
+
+def flatten_meshes(meshes) -> tuple[np.ndarray, np.ndarray]:
+    """(tri9 float32 [T, 9], counts uint32 [M]) from a list of (n, 3, 3) arrays."""
+    parts, counts = [], []
+    for m in meshes:
+        a = np.asarray(m, dtype=np.float32).reshape(-1, 9)
+        parts.append(a)
+        counts.append(a.shape[0])
+    tri9 = np.concatenate(parts) if parts else np.zeros((0, 9), np.float32)
+    return np.ascontiguousarray(tri9, dtype=np.float32), np.asarray(counts, dtype=np.uint32)
+
+
+NODE_DTYPE = np.dtype([("lo", "<f4", 4), ("hi", "<f4", 4), ("info", "<u4", 4)])
+
+
+@dataclass
+class Visibility:
+    """Per-cone results, shaped [lights, points]."""
+
+    full: Optional[np.ndarray] = None        # uint64 mask words: bins wholly covered
+    any: Optional[np.ndarray] = None         # uint64 mask words: bins with coverage > 0
+    partial: Optional[np.ndarray] = None     # float32 [..., 64] per-bin coverage
+    irradiance: Optional[np.ndarray] = None  # float32 irradiance per unit radiance
+    fraction: Optional[np.ndarray] = None    # float32 visible fraction of the unshadowed light
+    work: Optional[np.ndarray] = None        # uint32 [..., 4]: object nodes, triangle nodes, triangles, status
+
+
+class Scene:
+    """A scene resident on the device: triangles and both hierarchy levels."""
+
+    def __init__(self, kernel: "MaskConeKernel", handle: int):
+        self._kernel = kernel
+        self._h = C.c_void_p(handle)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("scene is closed")
+        return self._h
+
+    def sizes(self) -> dict:
+        out = np.zeros(6, dtype=np.uint64)
+        check(load().cc_scene_sizes(self.handle, ptr(out)))
+        keys = ("ntris", "nmeshes", "nblas", "nblas_items", "nnodes", "nitems")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def arrays(self) -> dict:
+        """The host layouts (hierarchy.rs Flat + mesh_hierarchy), for checking the builder."""
+        sz = self.sizes()
+        ranges = np.zeros((sz["nmeshes"], 4), np.uint32)
+        blas = np.zeros(sz["nblas"], NODE_DTYPE)
+        blas_items = np.zeros(sz["nblas_items"], np.uint32)
+        nodes = np.zeros(sz["nnodes"], NODE_DTYPE)
+        items = np.zeros(sz["nitems"], np.uint32)
+        check(load().cc_scene_arrays(self.handle, ptr(ranges), ptr(blas), ptr(blas_items), ptr(nodes), ptr(items)))
+        return dict(ranges=ranges, blas=blas, blas_items=blas_items, nodes=nodes, items=items)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(load().cc_scene_device_bytes(self.handle))
+
+    def primary_hits(self, camera, width: int, height: int):
+        """Receivers (H*W, 8) at a pinhole camera's primary hits, and the hit mask."""
+        cam = np.ascontiguousarray(np.asarray(camera, np.float32).reshape(10))
+        out = np.zeros((width * height, 8), np.float32)
+        hit = np.zeros(width * height, np.uint8)
+        check(load().cc_scene_primary_hits(self.handle, ptr(cam), int(width), int(height), ptr(out), ptr(hit)))
+        return out, hit
+
+    def close(self) -> None:
+        if self._h:
+            load().cc_scene_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def host_scene(meshes=None, tri9=None, counts=None) -> Scene:
+    """A scene built on the host only (no device needed): hierarchies to
+    inspect and ray cast, not to pass to ``visibility``."""
+    if meshes is not None:
+        tri9, counts = flatten_meshes(meshes)
+    tri9 = np.ascontiguousarray(tri9, dtype=np.float32)
+    counts = np.ascontiguousarray(counts, dtype=np.uint32)
+    h = C.c_void_p()
+    check(load().cc_scene_build(None, ptr(tri9), ptr(counts), len(counts), C.byref(h)))
+    return Scene(None, h.value)
+
+
+class MaskConeKernel:
+    """Mask-cone visibility on one CUDA device (MaskConeKernel, lib.rs:65-120).
+
+    Like the reference's kernel it is used from one thread at a time. The walk
+    parameters the reference keeps in cells (``wide_extent``,
+    ``light_cone_cap``, ``wide_cone_cap``; lib.rs:1211-1213) are attributes.
+    """
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = C.c_void_p()
+        check(lib.cc_context_create(int(device), C.byref(h)))
+        self._h = h
+        self.device = device
+        self.wide_extent = 8.0
+        self.light_cone_cap = 4096
+        self.wide_cone_cap = 512
+        self.points_per_warp = 32
+
+    @classmethod
+    def new(cls, device: int = 0) -> Optional["MaskConeKernel"]:
+        """None without a CUDA device, as MaskConeKernel::new (lib.rs:1155-1175)."""
+        try:
+            return cls(device)
+        except CCError as e:
+            if e.code == _lib.CC_ERR_NO_DEVICE:
+                return None
+            raise
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("kernel is closed")
+        return self._h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().cc_context_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the reference's calls ---------------------------------------------------
+    def irradiance(self, receivers, light: RectLight, meshes, runs: int = 1):
+        """Irradiance per unit radiance at each receiver and the best of `runs`
+        kernel times in seconds; every receiver tests every mesh (lib.rs:1706-1715)."""
+        return self.irradiance_with(receivers, light, meshes, Hierarchy.NONE, runs)
+
+    def irradiance_with(self, receivers, light: RectLight, meshes, hierarchy, runs: int = 1):
+        """`irradiance` culling through the hierarchy (lib.rs:1718-1730)."""
+        rec = np.ascontiguousarray(np.asarray(receivers, dtype=np.float32).reshape(-1, 6))
+        l9 = np.concatenate([_v3(light.corner), _v3(light.edge_u), _v3(light.edge_v)]).astype(np.float32)
+        tri9, counts = flatten_meshes(meshes)
+        out = np.zeros(rec.shape[0], dtype=np.float32)
+        best = C.c_double(0.0)
+        check(load().cc_irradiance(self.handle, ptr(rec), rec.shape[0], ptr(l9), int(bool(light.one_sided)),
+                                   ptr(tri9), ptr(counts), len(counts), int(Hierarchy.of(hierarchy)), int(runs),
+                                   ptr(out), C.byref(best)))
+        return out, best.value
+
+    def coverage(self, receivers, light: RectLight, meshes) -> np.ndarray:
+        """Per-bin coverage (64 per receiver), every triangle tested (lib.rs:3289-3298)."""
+        rec = np.ascontiguousarray(np.asarray(receivers, dtype=np.float32).reshape(-1, 6))
+        l9 = np.concatenate([_v3(light.corner), _v3(light.edge_u), _v3(light.edge_v)]).astype(np.float32)
+        tri9, counts = flatten_meshes(meshes)
+        out = np.zeros((rec.shape[0], 64), dtype=np.float32)
+        check(load().cc_coverage(self.handle, ptr(rec), rec.shape[0], ptr(l9), int(bool(light.one_sided)),
+                                 ptr(tri9), ptr(counts), len(counts), ptr(out)))
+        return out
+
+    # -- resident scenes and the multi-light call -----------------------------------
+    def scene(self, meshes) -> Scene:
+        """Builds the hierarchies on the host and uploads the scene."""
+        tri9, counts = flatten_meshes(meshes)
+        return self.scene_from_tri9(tri9, counts)
+
+    def scene_from_tri9(self, tri9: np.ndarray, counts: np.ndarray) -> Scene:
+        tri9 = np.ascontiguousarray(tri9, dtype=np.float32)
+        counts = np.ascontiguousarray(counts, dtype=np.uint32)
+        h = C.c_void_p()
+        check(load().cc_scene_build(self.handle, ptr(tri9), ptr(counts), len(counts), C.byref(h)))
+        return Scene(self, h.value)
+
+    def scene_from_flat(self, tris12, ranges, blas, blas_items, nodes, items) -> Scene:
+        """A scene from the reference's own flattened arrays (Flat + mesh_hierarchy)."""
+        arrs = [np.ascontiguousarray(tris12, np.float32), np.ascontiguousarray(ranges, np.uint32),
+                np.ascontiguousarray(blas), np.ascontiguousarray(blas_items, np.uint32),
+                np.ascontiguousarray(nodes), np.ascontiguousarray(items, np.uint32)]
+        f = _lib.FlatScene(ptr(arrs[0]), arrs[0].size // 12, ptr(arrs[1]), arrs[1].size // 4, ptr(arrs[2]),
+                           len(arrs[2]), ptr(arrs[3]), arrs[3].size, ptr(arrs[4]), len(arrs[4]), ptr(arrs[5]),
+                           arrs[5].size)
+        h = C.c_void_p()
+        check(load().cc_scene_upload(self.handle, C.byref(f), C.byref(h)))
+        return Scene(self, h.value)
+
+    def options(self, hierarchy=Hierarchy.TRIANGLES, flags: int = 0, points_per_warp: Optional[int] = None):
+        o = _lib.default_options()
+        o.hierarchy = int(Hierarchy.of(hierarchy))
+        o.wide_extent = float(self.wide_extent)
+        o.light_cone_cap = int(self.light_cone_cap)
+        o.wide_cone_cap = int(self.wide_cone_cap)
+        o.points_per_warp = int(points_per_warp or self.points_per_warp)
+        o.flags = int(flags)
+        return o
+
+    def visibility(self, scene: Scene, receivers, lights, hierarchy=Hierarchy.TRIANGLES,
+                   outputs: Sequence[str] = ("full", "any", "irradiance", "fraction"),
+                   points_per_warp: Optional[int] = None, flags: int = 0) -> Visibility:
+        """Every (light, point) cone through a resident scene; results [L, P]."""
+        rec = receivers_gpu(receivers)
+        lig = lights if isinstance(lights, np.ndarray) else lights_gpu(lights)
+        lig = np.ascontiguousarray(lig, dtype=np.float32).reshape(-1, 16)
+        P, L = rec.shape[0], lig.shape[0]
+        res = Visibility()
+        bufs = {}
+        if "full" in outputs:
+            bufs["full"] = np.zeros((L, P), np.uint64)
+        if "any" in outputs:
+            bufs["any"] = np.zeros((L, P), np.uint64)
+        if "partial" in outputs:
+            bufs["partial"] = np.zeros((L, P, 64), np.float32)
+        if "irradiance" in outputs:
+            bufs["irradiance"] = np.zeros((L, P), np.float32)
+        if "fraction" in outputs:
+            bufs["fraction"] = np.zeros((L, P), np.float32)
+        if "work" in outputs:
+            bufs["work"] = np.zeros((L, P, 4), np.uint32)
+        o = _lib.Outputs(*(ptr(bufs.get(k)) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.options(hierarchy, flags, points_per_warp)
+        check(load().cc_visibility(self.handle, scene.handle, ptr(rec), P, ptr(lig), L, C.byref(opt), C.byref(o),
+                                   None))
+        for k, v in bufs.items():
+            setattr(res, k, v)
+        return res
+
+    def visibility_device(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int,
+                          outputs: dict, stream: int = 0, hierarchy=Hierarchy.TRIANGLES,
+                          points_per_warp: Optional[int] = None, flags: int = 0) -> None:
+        """The same with device pointers (ints), asynchronous on `stream`."""
+        o = _lib.Outputs(*(outputs.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.options(hierarchy, flags | _lib.CC_DEVICE_POINTERS, points_per_warp)
+        check(load().cc_visibility(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints),
+                                   C.c_void_p(d_lights), int(nlights), C.byref(opt), C.byref(o),
+                                   C.c_void_p(stream) if stream else None))
+
+
+def kernel_times(kernel: MaskConeKernel, max_calls: int = 256) -> np.ndarray:
+    """(calls, 2) milliseconds of the packet and solo passes of the
+    visibility calls since the last query (waits for them)."""
+    out = np.zeros((max_calls, 2), np.float32)
+    n = load().cc_context_kernel_times(kernel.handle, ptr(out), int(max_calls))
+    if n < 0:
+        check(-n)
+    return out[:n]

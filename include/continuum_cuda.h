@@ -1,0 +1,195 @@
+/* continuum_cuda.h — C ABI of the B200-native mask-cone visibility path.
+ *
+ * One cone per (shading point, area light) is traversed through the scene's
+ * bounding volume hierarchy; the occluding triangles are rasterized as exact
+ * areas into the cone's 8x8 bins, and the bins are integrated into the
+ * irradiance per unit radiance and the visible fraction of the light.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (CC_OK = 0). No exception or
+ *    abort crosses the ABI; cc_last_error() gives a message for the calling
+ *    thread's last failure.
+ *  - Buffers are owned by the caller. Unless a call says otherwise, pointers
+ *    are host pointers; with CC_DEVICE_POINTERS in cc_options.flags the
+ *    receivers, lights and every output of cc_visibility are device pointers
+ *    and the call is asynchronous on the given stream.
+ *  - A context is used from one host thread at a time (the reference's
+ *    MaskConeKernel is !Sync for the same reason); scenes belong to the
+ *    context that built them.
+ *  - Cone c = light * npoints + point (light-major). Mask words: bin b of a
+ *    cone is bit (b % 32) of word (b / 32); bin b = row * 8 + col.
+ *
+ * Layouts match the reference's GPU buffers:
+ *  receivers: 8 floats each, point.xyz w, normal.xyz w  (ReceiverGpu,
+ *             crates/continuum-gpu/src/lib.rs:54-60)
+ *  lights:    16 floats each (LightGpu, crates/continuum-gpu/src/lib.rs:710-749):
+ *             rect:   corner.xyz, w = 0 two-sided / 1 one-sided; edge_u.xyz 0;
+ *                     edge_v.xyz 0; radiance.xyz 0
+ *             sphere: center.xyz, w = 2; (radius, spot scale, spot offset, 0);
+ *                     (spot axis.xyz, 1 if spot else 0); radiance.xyz 0
+ *  triangles: 12 floats each in flat scenes (three vec4 vertices,
+ *             crates/continuum-gpu/src/hierarchy.rs:12-13), 9 floats each
+ *             where a call builds the hierarchy itself.
+ */
+#ifndef CONTINUUM_CUDA_H
+#define CONTINUUM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CC_API __attribute__((visibility("default")))
+#else
+#define CC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CC_OK 0
+#define CC_ERR_INVALID 1      /* bad argument or layout */
+#define CC_ERR_CUDA 2         /* a CUDA call failed (message in cc_last_error) */
+#define CC_ERR_OOM 3          /* device memory exhausted */
+#define CC_ERR_NO_DEVICE 4    /* no CUDA device (MaskConeKernel::new() -> None) */
+#define CC_ERR_STACK 5        /* a traversal stack overflowed: flagged cones are not exact */
+#define CC_ERR_TIMEOUT 6      /* a bounded device wait gave up */
+#define CC_ERR_BUSY 7         /* a batch or server queue is full */
+
+#define CC_NONE 0xffffffffu
+
+/* cc_options.flags */
+#define CC_DEVICE_POINTERS 1u /* receivers, lights and outputs are device pointers */
+#define CC_NO_REDO 2u         /* skip the solo re-walk of order-diverged cones (diagnostic) */
+
+/* Status bits in cc_outputs.work[4 * c + 3] */
+#define CC_CONE_CAPPED 1u     /* the walk stopped at its cap (LIGHT_CONE_CAP / WIDE_CONE_CAP) */
+#define CC_CONE_STACK 2u      /* the traversal stack overflowed */
+#define CC_CONE_DIVERGED 4u   /* its packet's child order differed from its own */
+#define CC_CONE_REWALKED 8u   /* recomputed walking alone */
+#define CC_CONE_FULL_STOP 16u /* the walk stopped early with every bin full */
+
+typedef struct cc_context cc_context;
+typedef struct cc_scene cc_scene;
+
+/* Replaces MaskConeKernel::new / with_device
+ * (crates/continuum-gpu/src/lib.rs:1145-1190): a context on CUDA device
+ * `device`. CC_ERR_NO_DEVICE where the reference returns None. */
+CC_API int cc_context_create(int device, cc_context** out);
+CC_API int cc_context_destroy(cc_context* ctx);
+
+/* The calling thread's last error message ("" if none). */
+CC_API const char* cc_last_error(void);
+
+/* A scene from the reference's flattened layout: Flat (hierarchy.rs:11-25,
+ * flatten :29-66) plus the object hierarchy (mesh_hierarchy :183-194).
+ * NodeGpu records are 48 bytes: lo.xyzw, hi.xyzw, info.xyzw (hierarchy.rs:68-76).
+ * The library repacks nodes into its own 32-byte device records. */
+typedef struct cc_flat_scene {
+  const float* tris;          /* 12 floats per triangle */
+  uint32_t ntris;
+  const uint32_t* ranges;     /* 4 per mesh: first, count, blas root or CC_NONE, transform (CC_NONE) */
+  uint32_t nmeshes;
+  const void* blas;           /* NodeGpu per triangle-hierarchy node */
+  uint32_t nblas;
+  const uint32_t* blas_items; /* triangle index per leaf slot */
+  uint32_t nblas_items;
+  const void* nodes;          /* NodeGpu per object-hierarchy node */
+  uint32_t nnodes;
+  const uint32_t* items;      /* mesh index per object leaf slot */
+  uint32_t nitems;
+} cc_flat_scene;
+
+CC_API int cc_scene_upload(cc_context* ctx, const cc_flat_scene* flat, cc_scene** out);
+
+/* A scene from meshes, with the hierarchies built on the host exactly as the
+ * reference builds them (flatten, triangle_hierarchy, mesh_hierarchy:
+ * hierarchy.rs:29-66, 128-253, 527-571, 762-765). tri9: 9 floats per
+ * triangle, meshes consecutive, mesh_counts[m] triangles in mesh m.
+ * With ctx NULL the scene stays on the host (no device is needed): it can be
+ * inspected and ray cast, but not passed to cc_visibility. */
+CC_API int cc_scene_build(cc_context* ctx, const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes,
+                   cc_scene** out);
+CC_API int cc_scene_destroy(cc_scene* scene);
+
+/* Sizes of the scene's flattened host arrays: ntris, nmeshes, nblas,
+ * nblas_items, nnodes, nitems; and copies of them (NodeGpu layout, any
+ * pointer may be NULL). For checking the host builder. */
+CC_API int cc_scene_sizes(const cc_scene* scene, uint64_t out6[6]);
+CC_API int cc_scene_arrays(const cc_scene* scene, uint32_t* ranges, void* blas, uint32_t* blas_items, void* nodes,
+                    uint32_t* items);
+/* Device bytes the scene holds. */
+CC_API uint64_t cc_scene_device_bytes(const cc_scene* scene);
+
+/* Shading points of a pinhole camera: for each pixel (row-major) the nearest
+ * hit's point lifted off the surface and its geometric normal facing the
+ * camera, as the reference's camera pass forms them (camera_dir, primary_hit,
+ * surface_offset: mask_cones.wgsl:1724-1760, 2062-2064, 2275-2277). Host
+ * threads; for preparing inputs. camera: eye.xyz, target.xyz, up.xyz,
+ * vertical fov in degrees. out8: 8 floats per pixel (receiver layout);
+ * hit: 1 per pixel, 0 where the ray misses (its receiver is zero). */
+CC_API int cc_scene_primary_hits(const cc_scene* scene, const float camera[10], uint32_t width, uint32_t height,
+                                 float* out8, uint8_t* hit);
+
+typedef struct cc_options {
+  uint32_t hierarchy;        /* 0: every triangle; 1: mesh hierarchy; 2: + triangle hierarchies (Hierarchy, hierarchy.rs:731-749) */
+  float wide_extent;         /* WIDE_EXTENT, mask_cones.wgsl:1048 (8.0) */
+  uint32_t light_cone_cap;   /* LIGHT_CONE_CAP, mask_cones.wgsl:1052 (4096) */
+  uint32_t wide_cone_cap;    /* WIDE_CONE_CAP, mask_cones.wgsl:1056 (512) */
+  uint32_t points_per_warp;  /* cones walked together per warp: 1..32 (32); results do not depend on it */
+  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO */
+} cc_options;
+
+/* Defaults: hierarchy 2, 8.0, 4096, 512, 32, 0. */
+CC_API void cc_options_default(cc_options* opt);
+
+typedef struct cc_outputs {
+  uint32_t* full;        /* 2 words per cone: bins wholly covered (nullable) */
+  uint32_t* any;         /* 2 words per cone: bins with coverage > 0 (nullable) */
+  float* partial;        /* 64 per cone: per-bin coverage in [0, 1] (nullable) */
+  float* irradiance;     /* 1 per cone: irradiance per unit radiance (nullable) */
+  float* fraction;       /* 1 per cone: visible fraction of the unshadowed light (nullable) */
+  uint32_t* work;        /* 4 per cone: object nodes, triangle-hierarchy nodes, triangles tested; status bits (nullable) */
+} cc_outputs;
+
+/* Visibility of every (point, light) cone. Replaces the reference's light
+ * cones as traced by hit_irradiance_rect (mask_cones.wgsl:2125-2128) for each
+ * light of the `lights` list, with the lighting cache's ratio
+ * (vc_bake, mask_cones.wgsl:3453-3510) as `fraction`. `stream` is a
+ * cudaStream_t (NULL: the context's stream). With host pointers the call
+ * returns when the results are in the host buffers. */
+CC_API int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                  const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
+                  void* stream);
+
+/* Kernel times of the cc_visibility calls made on this context since the
+ * last query, oldest first (the last 256 calls at most): per call, the packet
+ * pass and the solo re-walk pass in milliseconds, from CUDA events recorded
+ * on the call's stream around each launch. The reference's counterpart is its
+ * GPU timestamp queries (crates/continuum-gpu/src/lib.rs:1081-1090). Waits
+ * for those calls to finish. Returns the number of calls written to out2
+ * (2 floats each, at most max_calls), or minus a status code. */
+CC_API int cc_context_kernel_times(cc_context* ctx, float* out2, int max_calls);
+
+/* Replaces MaskConeKernel::irradiance / irradiance_with
+ * (crates/continuum-gpu/src/lib.rs:1706-1730): irradiance per unit radiance
+ * at each receiver (6 floats: point.xyz, normal.xyz) from a rect light
+ * (9 floats: corner, edge_u, edge_v; one_sided 0/1) over meshes given as
+ * 9 floats per triangle. The hierarchy is built and the scene uploaded on
+ * every call, as the reference does; `best_seconds` (nullable) receives the
+ * fastest of `runs` kernel executions (upload and readback excluded, as in
+ * lib.rs:3496-3512). hierarchy: 0 (irradiance), 1 or 2 (irradiance_with). */
+CC_API int cc_irradiance(cc_context* ctx, const float* receivers6, uint64_t npoints, const float* light9, int one_sided,
+                  const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, uint32_t hierarchy,
+                  uint32_t runs, float* out, double* best_seconds);
+
+/* Replaces MaskConeKernel::coverage (crates/continuum-gpu/src/lib.rs:3289-3298):
+ * 64 per-bin coverages per receiver, every triangle tested (hierarchy 0). */
+CC_API int cc_coverage(cc_context* ctx, const float* receivers6, uint64_t npoints, const float* light9, int one_sided,
+                const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, float* out64);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CONTINUUM_CUDA_H */

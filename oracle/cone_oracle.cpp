@@ -1,0 +1,1532 @@
+// ORACLE — test infrastructure only. Nothing in the product links or calls this
+// file; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do,
+// as the checker.
+//
+// A plain CPU restatement of Continuum's mask-cone area-light visibility path
+// (reference v0.3.2), templated on the scalar type so the same code runs in
+// FP32 (parity) and FP64 (error report). It follows, function by function:
+//   crates/continuum-gpu/src/mask_cones.wgsl   (the GPU path the CUDA kernels replace)
+//   crates/continuum-gpu/src/hierarchy.rs      (host BVH layouts)
+//   crates/continuum/src/cone3.rs, coverage.rs, bvh.rs (the reference CPU path,
+//                                               used to pin the restatement)
+// Parity pins: the reference's own known-answer tests (cones_match_the_cpu,
+// the large-wall test, cone3/coverage/bvh unit tests) are re-run against this
+// file in tests/test_oracle_kat.py. Per-bin coverage has no golden vector in the
+// reference; beyond the 1e-4-of-light-weight KAT bound it is pinned only by
+// this restatement.
+//
+// Deliberate simplifications (all outside the exact light-cone path):
+//   * prefilter threshold 0 (exact cones): node_cone_test reduces to
+//     may_touch_box, splat_object_node never splats;
+//   * light cones carry no horizon (the WGSL zero-initialises it), so the
+//     horizon tests never cull and are left out;
+//   * meshes are in world space (no instancing transforms), tri_weight 1.
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+namespace oracle {
+
+constexpr uint32_t GRID = 8;
+constexpr uint32_t BINS = 64;
+constexpr uint32_t NONE = 0xffffffffu;
+constexpr int POLY_CAP = 16;  // the WGSL's is 10 (mask_cones.wgsl:11); see clip counts
+
+template <class R> struct V3 {
+  R x, y, z;
+};
+template <class R> inline V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R> inline V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R> inline V3<R> operator-(V3<R> a) { return {-a.x, -a.y, -a.z}; }
+template <class R> inline V3<R> operator*(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class R> inline V3<R> operator/(V3<R> a, R s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class R> inline R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> inline V3<R> cross(V3<R> a, V3<R> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class R> inline R length(V3<R> a) { return std::sqrt(dot(a, a)); }
+template <class R> inline V3<R> normalize(V3<R> a) { return a / length(a); }
+template <class R> inline V3<R> vmin(V3<R> a, V3<R> b) {
+  return {std::min(a.x, b.x), std::min(a.y, b.y), std::min(a.z, b.z)};
+}
+template <class R> inline V3<R> vmax(V3<R> a, V3<R> b) {
+  return {std::max(a.x, b.x), std::max(a.y, b.y), std::max(a.z, b.z)};
+}
+template <class R> inline R clampv(R x, R lo, R hi) { return std::min(std::max(x, lo), hi); }
+
+template <class R> struct V2 {
+  R x, y;
+};
+
+// ---------------------------------------------------------------------------
+// Host hierarchy (hierarchy.rs). Built in FP32 as the reference builds it.
+// ---------------------------------------------------------------------------
+
+struct Node {  // NodeGpu (hierarchy.rs:68-76): lo, hi, info = [first/left, count, 0, 0]
+  float lo[4];
+  float hi[4];
+  uint32_t info[4];
+};
+
+using F3 = V3<float>;
+
+// padded (hierarchy.rs:762-765)
+static void padded(F3& lo, F3& hi) {
+  float m = std::max(std::max(std::fabs(lo.x), std::fabs(hi.x)),
+                     std::max(std::max(std::fabs(lo.y), std::fabs(hi.y)),
+                              std::max(std::fabs(lo.z), std::fabs(hi.z))));
+  float pad = 1e-5f * std::max(m, 1.0f);
+  lo = lo - F3{pad, pad, pad};
+  hi = hi + F3{pad, pad, pad};
+}
+
+// split (hierarchy.rs:128-179). The median partition puts the `mid` smallest
+// keys on the left (ties broken by item id), and each leaf lists its items in
+// increasing id, so the tree is fully determined by its inputs.
+static void split(std::vector<Node>& nodes, size_t node, uint32_t* items, size_t count,
+                  size_t start, const std::vector<std::pair<F3, F3>>& bounds, size_t leaf,
+                  uint32_t node_base, uint32_t item_base) {
+  F3 lo{FLT_MAX, FLT_MAX, FLT_MAX}, hi{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  F3 clo = lo, chi = hi;
+  for (size_t i = 0; i < count; ++i) {
+    const auto& b = bounds[items[i]];
+    lo = vmin(lo, b.first);
+    hi = vmax(hi, b.second);
+    F3 c = (b.first + b.second) * 0.5f;
+    clo = vmin(clo, c);
+    chi = vmax(chi, c);
+  }
+  Node& n = nodes[node];
+  n.lo[0] = lo.x; n.lo[1] = lo.y; n.lo[2] = lo.z; n.lo[3] = 0;
+  n.hi[0] = hi.x; n.hi[1] = hi.y; n.hi[2] = hi.z; n.hi[3] = 0;
+  if (count <= leaf) {
+    std::sort(items, items + count);
+    n.info[0] = item_base + (uint32_t)start;
+    n.info[1] = (uint32_t)count;
+    n.info[2] = n.info[3] = 0;
+    return;
+  }
+  F3 e = chi - clo;
+  int axis = (e.x >= e.y && e.x >= e.z) ? 0 : (e.y >= e.z ? 1 : 2);
+  auto key = [&](uint32_t m) {
+    const auto& b = bounds[m];
+    const float* a = &b.first.x;
+    const float* c = &b.second.x;
+    return a[axis] + c[axis];
+  };
+  size_t mid = count / 2;
+  std::nth_element(items, items + mid, items + count, [&](uint32_t a, uint32_t b) {
+    float ka = key(a), kb = key(b);
+    return ka < kb || (ka == kb && a < b);
+  });
+  size_t left = nodes.size();
+  nodes.push_back(Node{});
+  nodes.push_back(Node{});
+  nodes[node].info[0] = node_base + (uint32_t)left;
+  nodes[node].info[1] = nodes[node].info[2] = nodes[node].info[3] = 0;
+  split(nodes, left, items, mid, start, bounds, leaf, node_base, item_base);
+  split(nodes, left + 1, items + mid, count - mid, start + mid, bounds, leaf, node_base, item_base);
+}
+
+struct Scene {
+  std::vector<float> tris;       // 12 floats per triangle: three vec4 (hierarchy.rs:12-13)
+  std::vector<uint32_t> ranges;  // 4 per mesh: first, count, blas root, xform (NONE)
+  std::vector<Node> blas;
+  std::vector<uint32_t> blas_items;
+  std::vector<Node> nodes;       // object hierarchy (mesh_hierarchy)
+  std::vector<uint32_t> items;
+  uint32_t nmeshes = 0;
+};
+
+static void mesh_bounds(const float* tris, uint32_t first, uint32_t count, F3& lo, F3& hi) {
+  lo = {FLT_MAX, FLT_MAX, FLT_MAX};
+  hi = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (uint32_t t = first; t < first + count; ++t)
+    for (int k = 0; k < 3; ++k) {
+      const float* v = tris + 12 * t + 4 * k;
+      F3 p{v[0], v[1], v[2]};
+      lo = vmin(lo, p);
+      hi = vmax(hi, p);
+    }
+}
+
+// flatten + triangle_hierarchy + mesh_hierarchy/object_hierarchy
+// (hierarchy.rs:29-66, 527-545, 183-253). Coverage samples (prefiltering) are
+// not built: exact cones never read them.
+static Scene* build_scene(const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes) {
+  Scene* s = new Scene;
+  s->nmeshes = nmeshes;
+  uint64_t total = 0;
+  for (uint32_t m = 0; m < nmeshes; ++m) total += mesh_counts[m];
+  s->tris.resize(total * 12);
+  for (uint64_t t = 0; t < total; ++t)
+    for (int k = 0; k < 3; ++k) {
+      s->tris[12 * t + 4 * k + 0] = tri9[9 * t + 3 * k + 0];
+      s->tris[12 * t + 4 * k + 1] = tri9[9 * t + 3 * k + 1];
+      s->tris[12 * t + 4 * k + 2] = tri9[9 * t + 3 * k + 2];
+      s->tris[12 * t + 4 * k + 3] = 0.0f;
+    }
+  uint32_t first = 0;
+  std::vector<std::pair<F3, F3>> mesh_box(nmeshes);
+  for (uint32_t m = 0; m < nmeshes; ++m) {
+    uint32_t count = mesh_counts[m];
+    uint32_t root = NONE;
+    if (count > 0) {
+      root = (uint32_t)s->blas.size();
+      std::vector<std::pair<F3, F3>> bounds(count);
+      for (uint32_t t = 0; t < count; ++t) {
+        F3 lo, hi;
+        mesh_bounds(s->tris.data(), first + t, 1, lo, hi);
+        padded(lo, hi);
+        bounds[t] = {lo, hi};
+      }
+      std::vector<uint32_t> items(count);
+      std::iota(items.begin(), items.end(), 0u);
+      std::vector<Node> nodes(1);
+      split(nodes, 0, items.data(), count, 0, bounds, 8, root, first);
+      s->blas.insert(s->blas.end(), nodes.begin(), nodes.end());
+      for (uint32_t t : items) s->blas_items.push_back(first + t);
+    }
+    s->ranges.insert(s->ranges.end(), {first, count, root, NONE});
+    F3 lo, hi;
+    mesh_bounds(s->tris.data(), first, count, lo, hi);
+    padded(lo, hi);
+    mesh_box[m] = {lo, hi};
+    first += count;
+  }
+  // object_hierarchy (hierarchy.rs:198-253): at most two meshes per leaf,
+  // oversized meshes (diagonal > 64 x median) in their own subtree.
+  std::vector<uint32_t> items(nmeshes);
+  std::iota(items.begin(), items.end(), 0u);
+  s->nodes.assign(1, Node{});
+  if (items.empty()) {
+    s->items = {0};
+    s->nodes[0].info[1] = 1;
+    return s;
+  }
+  auto diagonal = [&](uint32_t m) { return length(mesh_box[m].second - mesh_box[m].first); };
+  std::vector<float> sizes(nmeshes);
+  for (uint32_t i = 0; i < nmeshes; ++i) sizes[i] = diagonal(i);
+  size_t mid = sizes.size() / 2;
+  std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
+  float median = sizes[mid];
+  std::vector<uint32_t> big, small;
+  for (uint32_t m : items) (diagonal(m) > 64.0f * median ? big : small).push_back(m);
+  if (big.empty() || small.empty()) {
+    split(s->nodes, 0, items.data(), items.size(), 0, mesh_box, 2, 0, 0);
+  } else {
+    size_t nb = big.size();
+    items = big;
+    items.insert(items.end(), small.begin(), small.end());
+    s->nodes.push_back(Node{});
+    s->nodes.push_back(Node{});
+    split(s->nodes, 1, items.data(), nb, 0, mesh_box, 2, 0, 0);
+    split(s->nodes, 2, items.data() + nb, items.size() - nb, nb, mesh_box, 2, 0, 0);
+    Node& r = s->nodes[0];
+    const Node &a = s->nodes[1], &b = s->nodes[2];
+    for (int k = 0; k < 3; ++k) {
+      r.lo[k] = std::min(a.lo[k], b.lo[k]);
+      r.hi[k] = std::max(a.hi[k], b.hi[k]);
+    }
+    r.info[0] = 1;
+  }
+  s->items = items;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// The light cone (mask_cones.wgsl:136-1042).
+// ---------------------------------------------------------------------------
+
+template <class R> struct Cone {  // mask_cones.wgsl:136-155 (horizon left out: zero)
+  V3<R> apex, right, up, forward;
+  R window[4];  // u0, v0, u1, v1
+  V3<R> far_normal;
+  R far_offset;
+  V3<R> bound_axis;
+  R bound_cos;
+  R bound_sin;
+};
+
+template <class R> struct Light {  // LightRect (mask_cones.wgsl:843-848), LightGpu (lib.rs:710-749)
+  V3<R> corner;
+  R corner_w;  // 0 two-sided rect, 1 one-sided rect, 2 sphere
+  V3<R> edge_u;
+  R edge_u_w;
+  V3<R> edge_v;
+  R edge_v_w;
+};
+
+template <class R> struct Params {
+  uint32_t hierarchy;  // 0 every triangle, 1 mesh hierarchy, 2 + triangle hierarchies
+  R wide_extent;
+  uint32_t light_cone_cap;
+  uint32_t wide_cone_cap;
+};
+
+template <class R> constexpr R NEAR = R(1e-4);
+
+template <class R> inline V3<R> direction(const Cone<R>& c, R s, R t) {  // :203-206
+  return c.forward + c.right * (c.window[0] + s * (c.window[2] - c.window[0])) +
+         c.up * (c.window[1] + t * (c.window[3] - c.window[1]));
+}
+
+template <class R> inline V3<R> to_local(const Cone<R>& c, V3<R> p) {  // :208-211
+  V3<R> d = p - c.apex;
+  return {dot(c.right, d), dot(c.up, d), dot(c.forward, d)};
+}
+
+template <class R> bool in_bound(const Cone<R>& c, V3<R> p, R r) {  // :159-168
+  if (c.bound_cos < R(-1)) return true;
+  V3<R> d = p - c.apex;
+  R len = length(d);
+  if (len <= r) return true;
+  R s = r / len;
+  R limit = c.bound_cos * std::sqrt(R(1) - s * s) - c.bound_sin * s;
+  return dot(c.bound_axis, d) >= limit * len;
+}
+
+template <class R> void bound_cone(Cone<R>& c, V3<R> axis) {  // :174-186
+  R cos_half = 1;
+  for (uint32_t k = 0; k < 4; ++k) {
+    V3<R> d = normalize(direction(c, R(k & 1u), R(k >> 1u)));
+    cos_half = std::min(cos_half, dot(axis, d));
+  }
+  R cos_b = clampv(cos_half - R(1e-5), R(-1), R(1));
+  c.bound_axis = axis;
+  c.bound_cos = cos_b;
+  c.bound_sin = std::sqrt(std::max(R(1) - cos_b * cos_b, R(0)));
+}
+
+template <class R> R lambert_edge_unit(V3<R> n, V3<R> an, V3<R> bn) {  // :193-201
+  V3<R> g = cross(an, bn);
+  R len = length(g);
+  if (len > R(1e-12)) return std::atan2(len, dot(an, bn)) * dot(n, g / len);
+  return 0;
+}
+
+template <class R> R lambert_edge(V3<R> n, V3<R> a, V3<R> b) {  // :188-190
+  return lambert_edge_unit(n, normalize(a), normalize(b));
+}
+
+template <class R> bool may_touch(const Cone<R>& c, V3<R> v0, V3<R> v1, V3<R> v2) {  // :215-232
+  R f0 = c.far_offset - dot(c.far_normal, v0);
+  R f1 = c.far_offset - dot(c.far_normal, v1);
+  R f2 = c.far_offset - dot(c.far_normal, v2);
+  if (f0 < 0 && f1 < 0 && f2 < 0) return false;
+  V3<R> p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
+  const R NR = NEAR<R>;
+  if (p0.z < NR && p1.z < NR && p2.z < NR) return false;
+  const R* w = c.window;
+  if (p0.x - w[0] * p0.z < 0 && p1.x - w[0] * p1.z < 0 && p2.x - w[0] * p2.z < 0) return false;
+  if (w[2] * p0.z - p0.x < 0 && w[2] * p1.z - p1.x < 0 && w[2] * p2.z - p2.x < 0) return false;
+  if (p0.y - w[1] * p0.z < 0 && p1.y - w[1] * p1.z < 0 && p2.y - w[1] * p2.z < 0) return false;
+  if (w[3] * p0.z - p0.y < 0 && w[3] * p1.z - p1.y < 0 && w[3] * p2.z - p2.y < 0) return false;
+  return true;
+}
+
+template <class R> bool may_touch_box(const Cone<R>& c, V3<R> lo, V3<R> hi) {  // :234-255
+  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true;
+  for (uint32_t k = 0; k < 8; ++k) {
+    V3<R> corner{(k & 1u) ? hi.x : lo.x, (k & 2u) ? hi.y : lo.y, (k & 4u) ? hi.z : lo.z};
+    if (c.far_offset - dot(c.far_normal, corner) >= 0) far_out = false;
+    V3<R> p = to_local(c, corner);
+    if (p.z >= NEAR<R>) near_out = false;
+    if (p.x - c.window[0] * p.z >= 0) out_u0 = false;
+    if (c.window[2] * p.z - p.x >= 0) out_u1 = false;
+    if (p.y - c.window[1] * p.z >= 0) out_v0 = false;
+    if (c.window[3] * p.z - p.y >= 0) out_v1 = false;
+  }
+  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1) return false;
+  return in_bound(c, (lo + hi) * R(0.5), R(0.5) * length(hi - lo));
+}
+
+template <class R> struct Poly3 {
+  V3<R> v[POLY_CAP];
+  int n = 0;
+};
+template <class R> struct Poly2 {
+  V2<R> v[POLY_CAP];
+  int n = 0;
+};
+
+// Diagnostic: polygons that would have exceeded the WGSL's 10-vertex arrays.
+static std::atomic<uint64_t> g_poly_overflow{0};
+
+template <class P, class T> inline void poly_push(P& out, const T& x) {
+  if (out.n >= 10) g_poly_overflow.fetch_add(1, std::memory_order_relaxed);
+  if (out.n < POLY_CAP) out.v[out.n++] = x;
+}
+
+// clip_plane3 (:264-277): keeps dot(normal, x) <= offset; crossings found from
+// the kept end.
+template <class R> Poly3<R> clip_plane3(const Poly3<R>& p, V3<R> normal, R offset) {
+  Poly3<R> out;
+  for (int i = 0; i < p.n; ++i) {
+    V3<R> a = p.v[i], b = p.v[(i + 1) % p.n];
+    R da = offset - dot(normal, a), db = offset - dot(normal, b);
+    if (da >= 0) poly_push(out, a);
+    if (da >= 0 && db < 0) poly_push(out, a + (b - a) * (da / (da - db)));
+    if (da < 0 && db >= 0) poly_push(out, b + (a - b) * (db / (db - da)));
+  }
+  return out;
+}
+
+// clip_line2 (:280-294)
+template <class R> Poly2<R> clip_line2(const Poly2<R>& p, V2<R> normal, R offset) {
+  Poly2<R> out;
+  for (int i = 0; i < p.n; ++i) {
+    V2<R> a = p.v[i], b = p.v[(i + 1) % p.n];
+    R da = offset - (normal.x * a.x + normal.y * a.y);
+    R db = offset - (normal.x * b.x + normal.y * b.y);
+    if (da >= 0) poly_push(out, a);
+    if (da >= 0 && db < 0) {
+      R f = da / (da - db);
+      poly_push(out, V2<R>{a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f});
+    }
+    if (da < 0 && db >= 0) {
+      R f = db / (db - da);
+      poly_push(out, V2<R>{b.x + (a.x - b.x) * f, b.y + (a.y - b.y) * f});
+    }
+  }
+  return out;
+}
+
+template <class R> struct Acc {
+  R cell[68];
+  uint32_t span_lo, span_hi;
+  void reset() {
+    std::fill(cell, cell + 68, R(0));
+    span_lo = 68;
+    span_hi = 0;
+  }
+};
+
+// draw_edge (:297-348): an edge's signed swept area added to the cells it
+// crosses (accumulation rasterizer).
+template <class R> void draw_edge(Acc<R>& acc, V2<R> q0, V2<R> q1, R weight) {
+  if (std::fabs(q0.y - q1.y) <= R(1.1920929e-7)) return;
+  R dir = 1;
+  V2<R> p0 = q0, p1 = q1;
+  if (q0.y > q1.y) {
+    dir = -1;
+    p0 = q1;
+    p1 = q0;
+  }
+  R dxdy = (p1.x - p0.x) / (p1.y - p0.y);
+  R x = p0.x;
+  uint32_t y_end = std::min((uint32_t)std::ceil(p1.y), GRID);
+  for (uint32_t y = (uint32_t)p0.y; y < y_end; ++y) {
+    uint32_t row = y * GRID;
+    acc.span_lo = std::min(acc.span_lo, row);
+    acc.span_hi = std::max(acc.span_hi, row + GRID + 1);
+    R dy = std::min(R(y + 1), p1.y) - std::max(R(y), p0.y);
+    R x_next = clampv(x + dxdy * dy, R(0), R(GRID));
+    R d = dy * dir * weight;
+    R x0 = std::min(x, x_next), x1 = std::max(x, x_next);
+    R x0_floor = std::floor(x0);
+    uint32_t x0i = (uint32_t)x0_floor;
+    R x1_ceil = std::ceil(x1);
+    uint32_t x1i = (uint32_t)x1_ceil;
+    if (x1i <= x0i + 1) {
+      R xmf = R(0.5) * (x + x_next) - x0_floor;
+      acc.cell[row + x0i] += d - d * xmf;
+      acc.cell[row + x0i + 1] += d * xmf;
+    } else {
+      R s = R(1) / (x1 - x0);
+      R x0f = x0 - x0_floor;
+      R a0 = R(0.5) * s * (R(1) - x0f) * (R(1) - x0f);
+      R x1f = x1 - x1_ceil + R(1);
+      R am = R(0.5) * s * x1f * x1f;
+      acc.cell[row + x0i] += d * a0;
+      if (x1i == x0i + 2) {
+        acc.cell[row + x0i + 1] += d * (R(1) - a0 - am);
+      } else {
+        R a1 = s * (R(1.5) - x0f);
+        acc.cell[row + x0i + 1] += d * (a1 - a0);
+        for (uint32_t xi = x0i + 2; xi < x1i - 1; ++xi) acc.cell[row + xi] += d * s;
+        R a2 = a1 + R(x1i - x0i - 3) * s;
+        acc.cell[row + x1i - 1] += d * (R(1) - a2 - am);
+      }
+      acc.cell[row + x1i] += d * am;
+    }
+    x = x_next;
+  }
+}
+
+// rasterize (:350-451)
+template <class R> bool rasterize(const Cone<R>& c, Acc<R>& acc, V3<R> v0, V3<R> v1, V3<R> v2) {
+  Poly3<R> p;
+  p.v[0] = v0;
+  p.v[1] = v1;
+  p.v[2] = v2;
+  p.n = 3;
+  R f0 = c.far_offset - dot(c.far_normal, v0);
+  R f1 = c.far_offset - dot(c.far_normal, v1);
+  R f2 = c.far_offset - dot(c.far_normal, v2);
+  if (f0 < 0 || f1 < 0 || f2 < 0) p = clip_plane3(p, c.far_normal, c.far_offset);
+  bool all_near_ok = true, all_in_window = true;
+  const R* w = c.window;
+  for (int i = 0; i < p.n; ++i) {
+    p.v[i] = to_local(c, p.v[i]);
+    V3<R> v = p.v[i];
+    if (v.z < NEAR<R>) all_near_ok = false;
+    if (v.x < w[0] * v.z || v.x > w[2] * v.z || v.y < w[1] * v.z || v.y > w[3] * v.z) all_in_window = false;
+  }
+  if (!all_near_ok) p = clip_plane3(p, V3<R>{0, 0, -1}, -NEAR<R>);
+  if (p.n < 3) return false;
+  R su = R(GRID) / (w[2] - w[0]);
+  R sv = R(GRID) / (w[3] - w[1]);
+  R g = R(GRID);
+  Poly2<R> q;
+  if (all_near_ok && all_in_window) {
+    q.n = p.n;
+    for (int i = 0; i < p.n; ++i)
+      q.v[i] = V2<R>{(p.v[i].x / p.v[i].z - w[0]) * su, (p.v[i].y / p.v[i].z - w[1]) * sv};
+  } else {
+    // The window's square clipped to the directions through the polygon
+    // (the apex-plane clip, :376-425).
+    R d = dot(to_local(c, v0), cross(to_local(c, v1), to_local(c, v2)));
+    if (d == 0) return false;
+    R side = d > 0 ? R(1) : R(-1);
+    q.n = 4;
+    q.v[0] = {0, 0};
+    q.v[2] = {g, g};
+    if (side > 0) {
+      q.v[1] = {g, 0};
+      q.v[3] = {0, g};
+    } else {
+      q.v[1] = {0, g};
+      q.v[3] = {g, 0};
+    }
+    for (int i = 0; i < p.n; ++i) {
+      V3<R> e = cross(p.v[i], p.v[(i + 1) % p.n]);
+      R len = length(e);
+      if (len == 0) continue;
+      V3<R> k = e * (side / len);
+      q = clip_line2(q, V2<R>{-k.x / su, -k.y / sv}, k.x * w[0] + k.y * w[1] + k.z);
+    }
+  }
+  bool inside = true;
+  for (int i = 0; i < q.n; ++i)
+    if (q.v[i].x < 0 || q.v[i].y < 0 || q.v[i].x > g || q.v[i].y > g) inside = false;
+  if (!inside) {
+    q = clip_line2(q, V2<R>{-1, 0}, R(0));
+    q = clip_line2(q, V2<R>{1, 0}, g);
+    q = clip_line2(q, V2<R>{0, -1}, R(0));
+    q = clip_line2(q, V2<R>{0, 1}, g);
+  }
+  if (q.n < 3) return false;
+  for (int i = 0; i < q.n; ++i) {
+    V2<R> a = q.v[i], b = q.v[(i + 1) % q.n];
+    a = {clampv(a.x, R(0), g), clampv(a.y, R(0), g)};
+    b = {clampv(b.x, R(0), g), clampv(b.y, R(0), g)};
+    draw_edge(acc, a, b, R(1));
+  }
+  return true;
+}
+
+template <class R> inline V3<R> tri_vertex(const Scene& s, uint32_t t, int k) {
+  const float* v = s.tris.data() + 12 * (size_t)t + 4 * k;
+  return {R(v[0]), R(v[1]), R(v[2])};
+}
+
+struct Work {  // the reference's work counters (mask_cones.wgsl:655-665), per cone
+  uint32_t object_nodes = 0;  // object-hierarchy nodes tested
+  uint32_t blas_nodes = 0;    // triangle-hierarchy nodes tested
+  uint32_t tris = 0;          // triangles tested
+  uint32_t flags = 0;         // bit 0: walk capped; bit 1: stack overflow
+};
+
+// cover_triangle (:594-616)
+template <class R> bool cover_triangle(const Scene& s, const Cone<R>& c, Acc<R>& acc, uint32_t t, Work& wk) {
+  wk.tris++;
+  V3<R> v0 = tri_vertex<R>(s, t, 0), v1 = tri_vertex<R>(s, t, 1), v2 = tri_vertex<R>(s, t, 2);
+  V3<R> n = cross(v1 - v0, v2 - v0);
+  if (dot(n, c.apex - v0) <= 0) return false;
+  if (dot(n, direction(c, R(0), R(0))) >= 0 && dot(n, direction(c, R(1), R(0))) >= 0 &&
+      dot(n, direction(c, R(0), R(1))) >= 0 && dot(n, direction(c, R(1), R(1))) >= 0)
+    return false;
+  if (!may_touch(c, v0, v1, v2)) return false;
+  return rasterize(c, acc, v0, v1, v2);
+}
+
+template <class R> inline V3<R> node_lo(const Node& n) { return {R(n.lo[0]), R(n.lo[1]), R(n.lo[2])}; }
+template <class R> inline V3<R> node_hi(const Node& n) { return {R(n.hi[0]), R(n.hi[1]), R(n.hi[2])}; }
+
+template <class R> struct Walk {
+  R cov[BINS];
+  uint32_t full = 0;
+  uint32_t cone_work = 0;
+  uint32_t cone_cap = NONE;
+  Work work;
+};
+
+constexpr int STACK = 64;
+
+// add_mesh_coverage_if for one cone walking alone (:713-829).
+template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& c, uint32_t m, Walk<R>& wk,
+                                          uint32_t hierarchy) {
+  Acc<R> acc;
+  acc.reset();
+  bool touched = false;
+  const uint32_t* range = s.ranges.data() + 4 * m;
+  if (hierarchy == 2) {
+    if (range[2] != NONE) {
+      uint32_t stack[STACK];
+      int sp = 0;
+      stack[sp++] = range[2];
+      while (sp > 0) {
+        uint32_t n = stack[--sp];
+        if (!(wk.cone_work < wk.cone_cap)) continue;
+        wk.cone_work++;
+        const Node& node = s.blas[n];
+        wk.work.blas_nodes++;
+        if (!may_touch_box(c, node_lo<R>(node), node_hi<R>(node))) continue;
+        if (node.info[1] > 0) {
+          wk.cone_work += node.info[1];
+          for (uint32_t k = node.info[0]; k < node.info[0] + node.info[1]; ++k)
+            if (cover_triangle(s, c, acc, s.blas_items[k], wk.work)) touched = true;
+        } else {
+          if (sp + 2 > STACK) {
+            wk.work.flags |= 2;
+            continue;
+          }
+          stack[sp++] = node.info[0];
+          stack[sp++] = node.info[0] + 1;
+        }
+      }
+    }
+  } else {
+    for (uint32_t t = range[0]; t < range[0] + range[1]; ++t)
+      if (cover_triangle(s, c, acc, t, wk.work)) touched = true;
+  }
+  if (touched) {
+    R running = 0;
+    for (uint32_t b = acc.span_lo; b < std::min(acc.span_hi, BINS); ++b) {
+      running += acc.cell[b];
+      R covered = std::fabs(running);
+      if (covered >= R(1) - R(1e-5)) covered = 1;
+      if (covered > R(1e-6)) {
+        R before = wk.cov[b];
+        wk.cov[b] = std::max(before, std::min(covered, R(1)));
+        if (before < R(1) && wk.cov[b] >= R(1)) wk.full++;
+      }
+    }
+  }
+}
+
+// scene_coverage_if for one cone walking alone (:1160-1227): nearest child
+// first along the bounding cone's axis, stop once every bin is full or at
+// the walk cap.
+template <class R> void scene_coverage(const Scene& s, const Cone<R>& c, Walk<R>& wk, uint32_t hierarchy) {
+  wk.cone_work = 0;
+  if (hierarchy >= 1) {
+    uint32_t stack[STACK];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+      uint32_t n = stack[--sp];
+      if (!(wk.full < BINS && wk.cone_work < wk.cone_cap)) continue;
+      wk.cone_work++;
+      const Node& node = s.nodes[n];
+      wk.work.object_nodes++;
+      if (!may_touch_box(c, node_lo<R>(node), node_hi<R>(node))) continue;
+      if (node.info[1] > 0) {
+        for (uint32_t k = node.info[0]; k < node.info[0] + node.info[1]; ++k)
+          add_mesh_coverage(s, c, s.items[k], wk, hierarchy);
+      } else {
+        uint32_t near_ = node.info[0], far_ = node.info[0] + 1;
+        const Node& a = s.nodes[near_];
+        const Node& b = s.nodes[far_];
+        V3<R> axis = c.bound_axis;  // a light cone's bound is always set
+        R da = dot(axis, (node_lo<R>(a) + node_hi<R>(a)) * R(0.5) - c.apex);
+        R db = dot(axis, (node_lo<R>(b) + node_hi<R>(b)) * R(0.5) - c.apex);
+        if (db < da) std::swap(near_, far_);
+        if (sp + 2 > STACK) {
+          wk.work.flags |= 2;
+          continue;
+        }
+        stack[sp++] = far_;
+        stack[sp++] = near_;
+      }
+    }
+  } else {
+    for (uint32_t m = 0; m < s.nmeshes; ++m)
+      if (wk.full < BINS) add_mesh_coverage(s, c, m, wk, hierarchy);
+  }
+}
+
+// bin_weight (:1232-1242)
+template <class R> R bin_weight(const Cone<R>& c, V3<R> n, uint32_t b) {
+  R col = R(b % GRID), row = R(b / GRID), g = R(GRID);
+  V3<R> d0 = direction(c, col / g, row / g);
+  V3<R> d1 = direction(c, (col + 1) / g, row / g);
+  V3<R> d2 = direction(c, (col + 1) / g, (row + 1) / g);
+  V3<R> d3 = direction(c, col / g, (row + 1) / g);
+  return std::fabs(R(0.5) * (lambert_edge(n, d0, d1) + lambert_edge(n, d1, d2) + lambert_edge(n, d2, d3) +
+                             lambert_edge(n, d3, d0)));
+}
+
+// The quad d[0..4] clipped to dot(n, x) >= 0, Lambert-integrated (:1331-1403).
+template <class R> R clipped_quad_weight(V3<R> n, const V3<R> d[4]) {
+  V3<R> poly[6];
+  int k_n = 0;
+  for (int k = 0; k < 4; ++k) {
+    V3<R> a = d[k], e = d[(k + 1) % 4];
+    R sa = dot(n, a), se = dot(n, e);
+    if (sa >= 0) poly[k_n++] = a;
+    if ((sa >= 0) != (se >= 0)) poly[k_n++] = a + (e - a) * (sa / (sa - se));
+  }
+  if (k_n < 3) return 0;
+  R sum = 0;
+  for (int k = 0; k < k_n; ++k) sum += lambert_edge(n, poly[k], poly[(k + 1) % k_n]);
+  return std::fabs(R(0.5) * sum);
+}
+
+template <class R> R clipped_bin_weight(const Cone<R>& c, V3<R> n, uint32_t b) {  // :1331-1369
+  R col = R(b % GRID), row = R(b / GRID), g = R(GRID);
+  V3<R> d[4] = {direction(c, col / g, row / g), direction(c, (col + 1) / g, row / g),
+                direction(c, (col + 1) / g, (row + 1) / g), direction(c, col / g, (row + 1) / g)};
+  int above = 0;
+  for (int k = 0; k < 4; ++k)
+    if (dot(n, d[k]) > 0) above++;
+  if (above == 4) return bin_weight(c, n, b);
+  if (above == 0) return 0;
+  return clipped_quad_weight(n, d);
+}
+
+template <class R> R clipped_window_weight(const Cone<R>& c, V3<R> n) {  // :1375-1403
+  V3<R> d[4] = {direction(c, R(0), R(0)), direction(c, R(1), R(0)), direction(c, R(1), R(1)),
+                direction(c, R(0), R(1))};
+  return clipped_quad_weight(n, d);
+}
+
+// cone_visible (:1244-1272)
+template <class R> R cone_visible(const Cone<R>& c, V3<R> n, const R* cov) {
+  V3<R> d00 = direction(c, R(0), R(0)), d10 = direction(c, R(1), R(0));
+  V3<R> d11 = direction(c, R(1), R(1)), d01 = direction(c, R(0), R(1));
+  if (dot(n, d00) > 0 && dot(n, d10) > 0 && dot(n, d11) > 0 && dot(n, d01) > 0) {
+    R blocked = 0;
+    for (uint32_t b = 0; b < BINS; ++b)
+      if (cov[b] > 0) blocked += cov[b] * bin_weight(c, n, b);
+    R total = std::fabs(R(0.5) * (lambert_edge(n, d00, d10) + lambert_edge(n, d10, d11) +
+                                  lambert_edge(n, d11, d01) + lambert_edge(n, d01, d00)));
+    return std::max(total - blocked, R(0));
+  }
+  R blocked = 0;
+  for (uint32_t b = 0; b < BINS; ++b)
+    if (cov[b] > 0) blocked += cov[b] * clipped_bin_weight(c, n, b);
+  return std::max(clipped_window_weight(c, n) - blocked, R(0));
+}
+
+template <class R> R window_open(const Cone<R>& c, V3<R> n) {  // :1074-1085
+  V3<R> d00 = direction(c, R(0), R(0)), d10 = direction(c, R(1), R(0));
+  V3<R> d11 = direction(c, R(1), R(1)), d01 = direction(c, R(0), R(1));
+  if (dot(n, d00) > 0 && dot(n, d10) > 0 && dot(n, d11) > 0 && dot(n, d01) > 0)
+    return std::fabs(R(0.5) * (lambert_edge(n, d00, d10) + lambert_edge(n, d10, d11) +
+                               lambert_edge(n, d11, d01) + lambert_edge(n, d01, d00)));
+  return clipped_window_weight(c, n);
+}
+
+template <class R> inline bool is_sphere(const Light<R>& r) { return r.corner_w > R(1.5); }
+
+template <class R> V3<R> light_center(const Light<R>& r) {  // :866-869
+  if (is_sphere(r)) return r.corner;
+  return r.corner + (r.edge_u + r.edge_v) * R(0.5);
+}
+
+template <class R> R spot_falloff(const Light<R>& r, V3<R> w) {  // :872-876
+  if (!is_sphere(r) || r.edge_v_w < R(0.5)) return 1;
+  R a = clampv(dot(r.edge_v, w) * r.edge_u.y + r.edge_u.z, R(0), R(1));
+  return a * a;
+}
+
+template <class R> bool faces_light(const Light<R>& r, V3<R> point, V3<R> normal) {  // :880-884
+  V3<R> to_light = light_center(r) - point;
+  if (is_sphere(r)) return dot(normal, to_light) > -r.edge_u.x;
+  return dot(normal, to_light) > 0;
+}
+
+// rect_open (:2148-2199)
+template <class R> R rect_open(V3<R> point, V3<R> normal, const Light<R>& r) {
+  V3<R> u = r.edge_u, v = r.edge_v, c0 = r.corner - point;
+  R facing = dot(normalize(cross(u, v)), c0);
+  if ((r.corner_w > R(0.5) && facing >= 0) || std::fabs(facing) <= R(1e-6)) return 0;
+  V3<R> d1 = c0 + u, d2 = c0 + u + v, d3 = c0 + v;
+  if (dot(normal, c0) >= 0 && dot(normal, d1) >= 0 && dot(normal, d2) >= 0 && dot(normal, d3) >= 0) {
+    V3<R> a0 = normalize(c0), a1 = normalize(d1), a2 = normalize(d2), a3 = normalize(d3);
+    R sum = 0;
+    sum += lambert_edge_unit(normal, a0, a1);
+    sum += lambert_edge_unit(normal, a1, a2);
+    sum += lambert_edge_unit(normal, a2, a3);
+    sum += lambert_edge_unit(normal, a3, a0);
+    return std::fabs(R(0.5) * sum);
+  }
+  V3<R> d[4] = {c0, c0 + u, c0 + u + v, c0 + v};
+  return clipped_quad_weight(normal, d);
+}
+
+// sphere_unshadowed (:937-952)
+template <class R> R sphere_unshadowed(V3<R> point, V3<R> normal, const Light<R>& r) {
+  V3<R> to_center = r.corner - point;
+  R d2 = dot(to_center, to_center);
+  R radius = r.edge_u.x;
+  if (d2 <= radius * radius) return 0;
+  R sin2 = radius * radius / d2;
+  R cos_t = clampv(dot(normal, to_center) * (R(1) / std::sqrt(d2)), R(-1), R(1));
+  const R PI = R(3.14159265);
+  if (cos_t * cos_t > sin2) return PI * sin2 * std::max(cos_t, R(0));
+  R sin_t = std::sqrt(R(1) - cos_t * cos_t);
+  R x = std::sqrt(R(1) / sin2 - R(1));
+  R y = clampv(-x * cos_t / sin_t, R(-1), R(1));
+  R q = sin_t * std::sqrt(R(1) - y * y);
+  return std::max((cos_t * std::acos(y) - x * q) * sin2 + std::atan(q / x), R(0));
+}
+
+// unshadowed_rect (:2135-2141): the fraction's denominator.
+template <class R> R unshadowed_rect(V3<R> point, V3<R> normal, const Light<R>& r) {
+  if (!faces_light(r, point, normal)) return 0;
+  if (is_sphere(r)) return spot_falloff(r, normalize(point - r.corner)) * sphere_unshadowed(point, normal, r);
+  return rect_open(point, normal, r);
+}
+
+// The fraction of each bin inside the disk inscribed in a sphere light's
+// window (the WGSL's DISK table, mask_cones.wgsl:888-897): computed here
+// from the geometry (circle of radius 4 bins centred on the 8x8 grid, each
+// cell's covered area by fine quadrature) and rounded to the table's six
+// decimals.
+static const double* disk_table() {
+  static double table[BINS];
+  static bool init = false;
+  if (!init) {
+    const int S = 2000;  // samples per cell side (midpoint rule on the circle's chord)
+    for (uint32_t b = 0; b < BINS; ++b) {
+      int col = b % 8, row = b / 8;
+      double area = 0;
+      for (int i = 0; i < S; ++i) {
+        // Exact chord length in y at this x: the integral over x of the
+        // vertical overlap of [row, row+1] with the circle at x.
+        double x = col + (i + 0.5) / S - 4.0;
+        double h2 = 16.0 - x * x;
+        if (h2 <= 0) continue;
+        double h = std::sqrt(h2);
+        double y0 = std::max((double)row - 4.0, -h), y1 = std::min((double)row + 1 - 4.0, h);
+        if (y1 > y0) area += (y1 - y0) / S;
+      }
+      table[b] = std::round(area * 1e6) / 1e6;
+    }
+    init = true;
+  }
+  return table;
+}
+
+// sphere_open_share (:957-972)
+template <class R> R sphere_open_share(const Cone<R>& c, V3<R> normal, const R* cov, bool wide_clipped) {
+  const double* disk = disk_table();
+  R total = 0, open = 0, g = R(GRID);
+  for (uint32_t b = 0; b < BINS; ++b) {
+    R m = wide_clipped ? R(1) : R(float(disk[b]));
+    if (m <= 0) continue;
+    V3<R> d = direction(c, (R(b % GRID) + R(0.5)) / g, (R(b / GRID) + R(0.5)) / g);
+    R l2 = dot(d, d);
+    R w = m * std::max(dot(normal, d), R(0)) / (l2 * l2);
+    total += w;
+    open += w * (R(1) - cov[b]);
+  }
+  if (total <= 0) return 1;
+  return open / total;
+}
+
+template <class R> struct LightCone {
+  Cone<R> c;
+  bool ok = false;
+  bool wide_clipped = false;
+  bool wide_window = false;
+};
+
+// light_cone_sphere (:902-931)
+template <class R> LightCone<R> light_cone_sphere(V3<R> apex, const Light<R>& r, R wide_extent) {
+  LightCone<R> out;
+  V3<R> to_center = r.corner - apex;
+  R d = length(to_center);
+  R radius = r.edge_u.x;
+  if (d <= radius * R(1.0001)) return out;
+  V3<R> forward = to_center / d;
+  R s = radius / d;
+  R t = s / std::sqrt(std::max(R(1) - s * s, R(1e-12)));
+  out.wide_clipped = R(2) * t > wide_extent;
+  out.wide_window = out.wide_clipped;
+  t = std::min(t, R(0.5) * wide_extent);
+  V3<R> helper = std::fabs(forward.x) > R(0.9) ? V3<R>{0, 1, 0} : V3<R>{1, 0, 0};
+  V3<R> right = normalize(cross(helper, forward));
+  Cone<R>& c = out.c;
+  c.apex = apex;
+  c.right = right;
+  c.up = cross(forward, right);
+  c.forward = forward;
+  c.window[0] = -t;
+  c.window[1] = -t;
+  c.window[2] = t;
+  c.window[3] = t;
+  c.far_normal = forward;
+  c.far_offset = dot(forward, apex) + (d - radius * s) * (R(1) - R(1e-5));
+  bound_cone(c, forward);
+  out.ok = true;
+  return out;
+}
+
+// light_cone_rect (:974-1042)
+template <class R> LightCone<R> light_cone_rect(V3<R> apex, const Light<R>& r, R wide_extent) {
+  if (is_sphere(r)) return light_cone_sphere(apex, r, wide_extent);
+  LightCone<R> out;
+  V3<R> corner0 = r.corner, edge_u = r.edge_u, edge_v = r.edge_v;
+  V3<R> forward = normalize(cross(edge_u, edge_v));
+  if (r.corner_w > R(0.5) && dot(forward, apex - corner0) <= 0) return out;
+  if (dot(forward, corner0 - apex) < 0) forward = -forward;
+  R dist = dot(forward, corner0 - apex);
+  if (dist <= R(1e-6)) return out;
+  V3<R> right = normalize(edge_u);
+  V3<R> up = cross(forward, right);
+  V3<R> rel = corner0 - apex;
+  R lo[2] = {R(3.4e38), R(3.4e38)}, hi[2] = {R(-3.4e38), R(-3.4e38)};
+  for (uint32_t k = 0; k < 4; ++k) {
+    V3<R> corner = rel + edge_u * R(k & 1u) + edge_v * R((k >> 1u) & 1u);
+    R u = dot(right, corner) / dist, v = dot(up, corner) / dist;
+    lo[0] = std::min(lo[0], u);
+    lo[1] = std::min(lo[1], v);
+    hi[0] = std::max(hi[0], u);
+    hi[1] = std::max(hi[1], v);
+  }
+  R extent[2] = {hi[0] - lo[0], hi[1] - lo[1]};
+  R foot[2] = {std::min(std::max(R(0), lo[0]), hi[0]), std::min(std::max(R(0), lo[1]), hi[1])};
+  V3<R> mid = normalize(V3<R>{R(0.5) * (lo[0] + hi[0]), R(0.5) * (lo[1] + hi[1]), R(1)});
+  R cos_wide = 1;
+  for (uint32_t k = 0; k < 4; ++k) {
+    V3<R> q{(k & 1u) ? hi[0] : lo[0], (k & 2u) ? hi[1] : lo[1], R(1)};
+    cos_wide = std::min(cos_wide, dot(mid, normalize(q)));
+  }
+  R size = wide_extent;
+  out.wide_window = extent[0] > size || extent[1] > size;
+  out.wide_clipped = out.wide_window && cos_wide < R(0.8660254);
+  if (out.wide_clipped) {
+    for (int i = 0; i < 2; ++i) {
+      if (extent[i] > size) {
+        R keep = std::min(std::max(foot[i] - R(0.5) * size, lo[i]), hi[i] - size);
+        lo[i] = keep;
+        hi[i] = keep + size;
+      }
+    }
+  }
+  Cone<R>& c = out.c;
+  c.apex = apex;
+  c.right = right;
+  c.up = up;
+  c.forward = forward;
+  c.window[0] = lo[0];
+  c.window[1] = lo[1];
+  c.window[2] = hi[0];
+  c.window[3] = hi[1];
+  c.far_normal = forward;
+  c.far_offset = dot(forward, apex) + dist * (R(1) - R(1e-5));
+  V3<R> axis = normalize(rel + (edge_u + edge_v) * R(0.5));
+  if (out.wide_clipped) axis = normalize(direction(c, R(0.5), R(0.5)));
+  bound_cone(c, axis);
+  out.ok = true;
+  return out;
+}
+
+template <class R> struct ConeResult {
+  R cov[BINS];
+  R irradiance;
+  R fraction;
+  R unshadowed;
+  Work work;
+};
+
+// hit_irradiance_rect (:2125-2128) through cone_irradiance_rect (:1286-1321),
+// plus the lighting cache's ratio (vc_bake, :3453-3510, static light): the
+// visible fraction of the unshadowed light, exactly 1 for an empty cone and 0
+// for a full one.
+template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> normal, const Light<R>& r,
+                                        const Params<R>& prm, ConeResult<R>& out) {
+  R spot = spot_falloff(r, normalize(point - light_center(r)));
+  bool on = spot > 0 && faces_light(r, point, normal);
+  LightCone<R> lc = light_cone_rect(point, r, prm.wide_extent);
+  bool traced = on && lc.ok;
+  Walk<R> wk;
+  std::fill(wk.cov, wk.cov + BINS, R(0));
+  wk.cone_cap = lc.wide_window ? prm.wide_cone_cap : prm.light_cone_cap;
+  if (traced) scene_coverage(s, lc.c, wk, prm.hierarchy);
+  if (wk.cone_work >= wk.cone_cap && traced) wk.work.flags |= 1;
+  if (traced && wk.cone_work >= wk.cone_cap && lc.wide_window && !lc.wide_clipped) {
+    std::fill(wk.cov, wk.cov + BINS, R(1));
+    wk.full = BINS;
+  }
+  bool last_empty = true, last_full = true;
+  for (uint32_t b = 0; b < BINS; ++b) {
+    if (wk.cov[b] > 0) last_empty = false;
+    if (wk.cov[b] < 1) last_full = false;
+  }
+  R value = 0;
+  if (traced) {
+    if (is_sphere(r)) {
+      value = sphere_unshadowed(point, normal, r) * sphere_open_share(lc.c, normal, wk.cov, lc.wide_clipped);
+    } else {
+      R visible = cone_visible(lc.c, normal, wk.cov);
+      if (lc.wide_clipped) {  // wide_visible (:1070-1073)
+        R kept = window_open(lc.c, normal);
+        visible = (kept > R(1e-9) ? visible / kept : R(1)) * rect_open(point, normal, r);
+      }
+      value = visible;
+    }
+  }
+  value *= spot;
+  R open = unshadowed_rect(point, normal, r);
+  R ratio = open > 0 ? clampv(value / open, R(0), R(1)) : R(1);
+  if (open > 0 && last_empty) ratio = 1;
+  if (open > 0 && last_full) ratio = 0;
+  std::copy(wk.cov, wk.cov + BINS, out.cov);
+  out.irradiance = value;
+  out.fraction = ratio;
+  out.unshadowed = open;
+  out.work = wk.work;
+}
+
+// ---------------------------------------------------------------------------
+// The reference CPU path: cone3.rs, coverage.rs, bvh.rs (FP32).
+// ---------------------------------------------------------------------------
+
+namespace cpu {
+using V = V3<float>;
+
+struct Plane {
+  V normal;
+  float offset;
+  float signed_distance(V p) const { return offset - dot(normal, p); }
+};
+
+struct PyramidCone {  // cone3.rs:46-64
+  V apex, right, up, forward;
+  float window[4];
+  float near_;
+  Plane far_;
+  float weights[BINS];
+  V direction(float s, float t) const {
+    return forward + right * (window[0] + s * (window[2] - window[0])) + up * (window[1] + t * (window[3] - window[1]));
+  }
+  V to_local(V p) const {
+    V d = p - apex;
+    return {dot(right, d), dot(up, d), dot(forward, d)};
+  }
+};
+
+// projected_solid_angle (cone3.rs:69-82)
+static float projected_solid_angle(V n, const V* verts, int count) {
+  float sum = 0;
+  for (int i = 0; i < count; ++i) {
+    V a = normalize(verts[i]), b = normalize(verts[(i + 1) % count]);
+    V g = cross(a, b);
+    float len = length(g);
+    if (len > 1e-12f) sum += std::atan2(len, dot(a, b)) * dot(n, g / len);
+  }
+  return std::fabs(0.5f * sum);
+}
+
+// toward_rect_light (cone3.rs:197-247)
+static bool toward_rect_light(V apex, V corner, V edge_u, V edge_v, V receiver_normal, PyramidCone& cone) {
+  V forward = normalize(cross(edge_u, edge_v));
+  if (dot(forward, corner - apex) < 0) forward = -forward;
+  float dist = dot(forward, corner - apex);
+  if (dist <= 1e-6f) return false;
+  V right = normalize(edge_u), up = cross(forward, right), rel = corner - apex;
+  V corners[4] = {rel, rel + edge_u, rel + edge_v, rel + edge_u + edge_v};
+  float u0 = FLT_MAX, v0 = FLT_MAX, u1 = -FLT_MAX, v1 = -FLT_MAX;
+  for (V c : corners) {
+    float u = dot(right, c) / dist, v = dot(up, c) / dist;
+    u0 = std::min(u0, u);
+    v0 = std::min(v0, v);
+    u1 = std::max(u1, u);
+    v1 = std::max(v1, v);
+  }
+  cone.apex = apex;
+  cone.right = right;
+  cone.up = up;
+  cone.forward = forward;
+  cone.window[0] = u0;
+  cone.window[1] = v0;
+  cone.window[2] = u1;
+  cone.window[3] = v1;
+  cone.near_ = 1e-4f;
+  cone.far_ = {forward, dot(forward, apex) + dist * (1.0f - 1e-5f)};
+  for (uint32_t bin = 0; bin < BINS; ++bin) {
+    float col = float(bin % GRID), row = float(bin / GRID), g = float(GRID);
+    V quad[4] = {cone.direction(col / g, row / g), cone.direction((col + 1) / g, row / g),
+                 cone.direction((col + 1) / g, (row + 1) / g), cone.direction(col / g, (row + 1) / g)};
+    cone.weights[bin] = projected_solid_angle(receiver_normal, quad, 4);
+  }
+  return true;
+}
+
+static float total_weight(const PyramidCone& c) {
+  float s = 0;
+  for (float w : c.weights) s += w;
+  return s;
+}
+
+// may_touch / may_touch_box (cone3.rs:267-307)
+template <int N> static bool may_touch_points(const PyramidCone& c, const V (&pts)[N]) {
+  bool all_far = true;
+  for (const V& p : pts)
+    if (!(c.far_.signed_distance(p) < 0)) all_far = false;
+  if (all_far) return false;
+  V local[N];
+  bool all_near = true;
+  for (int i = 0; i < N; ++i) {
+    local[i] = c.to_local(pts[i]);
+    if (!(local[i].z < c.near_)) all_near = false;
+  }
+  if (all_near) return false;
+  const float* w = c.window;
+  auto outside = [&](auto f) {
+    for (int i = 0; i < N; ++i)
+      if (!(f(local[i]) < 0)) return false;
+    return true;
+  };
+  return !(outside([&](V p) { return p.x - w[0] * p.z; }) || outside([&](V p) { return w[2] * p.z - p.x; }) ||
+           outside([&](V p) { return p.y - w[1] * p.z; }) || outside([&](V p) { return w[3] * p.z - p.y; }));
+}
+
+static bool may_touch(const PyramidCone& c, const V (&tri)[3]) { return may_touch_points<3>(c, tri); }
+
+static bool may_touch_box(const PyramidCone& c, V mn, V mx) {
+  V corners[8];
+  for (int i = 0; i < 8; ++i)
+    corners[i] = {(i & 1) ? mx.x : mn.x, (i & 2) ? mx.y : mn.y, (i & 4) ? mx.z : mn.z};
+  return may_touch_points<8>(c, corners);
+}
+
+template <class P, class D> static int clip_poly(const P* in, int n, P* out, D d) {  // Poly::clip (cone3.rs:110-126)
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    P a = in[i], b = in[(i + 1) % n];
+    float da = d(a), db = d(b);
+    if (da >= 0 && m < POLY_CAP) out[m++] = a;
+    if ((da >= 0) != (db >= 0) && m < POLY_CAP) {
+      float f = da / (da - db);
+      out[m++] = P{a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f};
+    }
+  }
+  return m;
+}
+
+// draw_edge (cone3.rs:140-190), weight 1
+static void draw_edge(float* buf, V2<float> p0, V2<float> p1) {
+  if (std::fabs(p0.y - p1.y) <= FLT_EPSILON) return;
+  float dir = 1;
+  if (!(p0.y < p1.y)) {
+    dir = -1;
+    std::swap(p0, p1);
+  }
+  float dxdy = (p1.x - p0.x) / (p1.y - p0.y);
+  float x = p0.x;
+  size_t y_end = std::min((size_t)std::ceil(p1.y), (size_t)GRID);
+  for (size_t y = (size_t)p0.y; y < y_end; ++y) {
+    size_t row = y * GRID;
+    float dy = std::min(float(y + 1), p1.y) - std::max(float(y), p0.y);
+    float x_next = clampv(x + dxdy * dy, 0.0f, float(GRID));
+    float d = dy * dir;
+    float x0 = x < x_next ? x : x_next, x1 = x < x_next ? x_next : x;
+    float x0_floor = std::floor(x0);
+    size_t x0i = (size_t)x0_floor;
+    float x1_ceil = std::ceil(x1);
+    size_t x1i = (size_t)x1_ceil;
+    if (x1i <= x0i + 1) {
+      float xmf = 0.5f * (x + x_next) - x0_floor;
+      buf[row + x0i] += d - d * xmf;
+      buf[row + x0i + 1] += d * xmf;
+    } else {
+      float s = 1.0f / (x1 - x0);
+      float x0f = x0 - x0_floor;
+      float a0 = 0.5f * s * (1.0f - x0f) * (1.0f - x0f);
+      float x1f = x1 - x1_ceil + 1.0f;
+      float am = 0.5f * s * x1f * x1f;
+      buf[row + x0i] += d * a0;
+      if (x1i == x0i + 2) {
+        buf[row + x0i + 1] += d * (1.0f - a0 - am);
+      } else {
+        float a1 = s * (1.5f - x0f);
+        buf[row + x0i + 1] += d * (a1 - a0);
+        for (size_t xi = x0i + 2; xi < x1i - 1; ++xi) buf[row + xi] += d * s;
+        float a2 = a1 + float(x1i - x0i - 3) * s;
+        buf[row + x1i - 1] += d * (1.0f - a2 - am);
+      }
+      buf[row + x1i] += d * am;
+    }
+    x = x_next;
+  }
+}
+
+// rasterize (cone3.rs:360-393)
+static bool rasterize(const PyramidCone& c, float* buf, const V (&tri)[3]) {
+  V a[POLY_CAP], b[POLY_CAP];
+  int n = 0;
+  {  // far clip: keep signed_distance >= 0
+    for (int i = 0; i < 3; ++i) {
+      V p = tri[i], q = tri[(i + 1) % 3];
+      float da = c.far_.signed_distance(p), db = c.far_.signed_distance(q);
+      if (da >= 0) a[n++] = p;
+      if ((da >= 0) != (db >= 0)) a[n++] = p + (q - p) * (da / (da - db));
+    }
+  }
+  for (int i = 0; i < n; ++i) a[i] = c.to_local(a[i]);
+  int m = 0;
+  for (int i = 0; i < n; ++i) {  // near clip: keep z - near >= 0
+    V p = a[i], q = a[(i + 1) % n];
+    float da = p.z - c.near_, db = q.z - c.near_;
+    if (da >= 0 && m < POLY_CAP) b[m++] = p;
+    if ((da >= 0) != (db >= 0) && m < POLY_CAP) b[m++] = p + (q - p) * (da / (da - db));
+  }
+  if (m < 3) return false;
+  const float* w = c.window;
+  float su = float(GRID) / (w[2] - w[0]), sv = float(GRID) / (w[3] - w[1]), g = float(GRID);
+  V2<float> q0[POLY_CAP], q1[POLY_CAP];
+  for (int i = 0; i < m; ++i) q0[i] = {(b[i].x / b[i].z - w[0]) * su, (b[i].y / b[i].z - w[1]) * sv};
+  int k = m;
+  k = clip_poly(q0, k, q1, [](V2<float> p) { return p.x; });
+  k = clip_poly(q1, k, q0, [g](V2<float> p) { return g - p.x; });
+  k = clip_poly(q0, k, q1, [](V2<float> p) { return p.y; });
+  k = clip_poly(q1, k, q0, [g](V2<float> p) { return g - p.y; });
+  if (k < 3) return false;
+  auto at = [&](int i) {
+    V2<float> p = q0[i % k];
+    return V2<float>{clampv(p.x, 0.0f, g), clampv(p.y, 0.0f, g)};
+  };
+  for (int i = 0; i < k; ++i) draw_edge(buf, at(i), at(i + 1));
+  return true;
+}
+
+struct CoverageMask {  // coverage.rs:22-126
+  uint64_t full = 0;
+  float partial[BINS] = {};
+  void add_bin(uint32_t bin, float fraction) {
+    if (fraction >= 1.0f)
+      full |= 1ull << bin;
+    else if (fraction > partial[bin])
+      partial[bin] = fraction;
+  }
+  bool is_full() const { return full == ~0ull; }
+  float visible_weighted(const float* weights) const {
+    float visible = 0;
+    for (uint32_t bin = 0; bin < BINS; ++bin)
+      if (!((full >> bin) & 1)) visible += (1.0f - partial[bin]) * weights[bin];
+    return visible;
+  }
+};
+
+// add_mesh (cone3.rs:317-341): front-facing triangles of one mesh summed.
+static void add_mesh(const PyramidCone& c, CoverageMask& mask, const std::vector<const float*>& tris) {
+  float buf[BINS + 4] = {};
+  bool touched = false;
+  for (const float* t : tris) {
+    V tri[3] = {{t[0], t[1], t[2]}, {t[4], t[5], t[6]}, {t[8], t[9], t[10]}};
+    V normal = cross(tri[1] - tri[0], tri[2] - tri[0]);
+    if (dot(normal, c.apex - tri[0]) <= 0) continue;
+    touched |= rasterize(c, buf, tri);
+  }
+  if (touched) {
+    float running = 0;
+    for (uint32_t bin = 0; bin < BINS; ++bin) {
+      running += buf[bin];
+      float covered = std::fabs(running);
+      if (covered > 1e-6f) mask.add_bin(bin, std::min(covered, 1.0f));
+    }
+  }
+}
+
+// bvh.rs: leaf-4 median BVH over all triangles of all meshes.
+struct Bvh {
+  struct N {
+    V mn, mx;
+    uint32_t start, count;
+  };
+  std::vector<N> nodes;
+  std::vector<uint32_t> tri;  // triangle index (into the scene) per slot
+  std::vector<uint32_t> mesh_of;
+};
+
+static void bvh_split(const Scene& s, Bvh& b, size_t node, std::vector<uint32_t>& items, size_t start, size_t end) {
+  V mn{FLT_MAX, FLT_MAX, FLT_MAX}, mx{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  V cmin = mn, cmax = mx;
+  for (size_t i = start; i < end; ++i) {
+    V t[3];
+    for (int k = 0; k < 3; ++k) t[k] = tri_vertex<float>(s, items[i], k);
+    for (int k = 0; k < 3; ++k) {
+      mn = vmin(mn, t[k]);
+      mx = vmax(mx, t[k]);
+    }
+    V c = (t[0] + t[1] + t[2]) / 3.0f;
+    cmin = vmin(cmin, c);
+    cmax = vmax(cmax, c);
+  }
+  b.nodes[node].mn = mn;
+  b.nodes[node].mx = mx;
+  if (end - start <= 4) {
+    b.nodes[node].start = (uint32_t)start;
+    b.nodes[node].count = (uint32_t)(end - start);
+    return;
+  }
+  V e = cmax - cmin;
+  int axis = (e.x >= e.y && e.x >= e.z) ? 0 : (e.y >= e.z ? 1 : 2);
+  size_t mid = (start + end) / 2;
+  auto key = [&](uint32_t t) {
+    float k = 0;
+    for (int j = 0; j < 3; ++j) k += (&s.tris[12 * (size_t)t + 4 * j])[axis];
+    return k;
+  };
+  std::nth_element(items.begin() + start, items.begin() + mid, items.begin() + end, [&](uint32_t a, uint32_t c) {
+    float ka = key(a), kc = key(c);
+    return ka < kc || (ka == kc && a < c);
+  });
+  size_t left = b.nodes.size();
+  b.nodes.push_back({});
+  b.nodes.push_back({});
+  b.nodes[node].start = (uint32_t)left;
+  b.nodes[node].count = 0;
+  bvh_split(s, b, left, items, start, mid);
+  bvh_split(s, b, left + 1, items, mid, end);
+}
+
+static Bvh* build_bvh(const Scene& s) {
+  Bvh* b = new Bvh;
+  size_t total = s.tris.size() / 12;
+  std::vector<uint32_t> items(total);
+  std::iota(items.begin(), items.end(), 0u);
+  b->nodes.assign(1, {});
+  if (total) bvh_split(s, *b, 0, items, 0, total);
+  b->tri = items;
+  std::vector<uint32_t> mesh_of_tri(total);
+  for (uint32_t m = 0; m < s.nmeshes; ++m)
+    for (uint32_t t = s.ranges[4 * m]; t < s.ranges[4 * m] + s.ranges[4 * m + 1]; ++t) mesh_of_tri[t] = m;
+  for (uint32_t t : items) b->mesh_of.push_back(mesh_of_tri[t]);
+  return b;
+}
+
+// Receiver::new / with_bvh + Receiver::masked (experiments/room3d/src/lib.rs:180-243):
+// irradiance per unit radiance and the cone's total weight.
+static void receiver_masked(const Scene& s, const Bvh* bvh, V point, V normal, V corner, V eu, V ev, float& visible,
+                            float& total, uint32_t& visited) {
+  PyramidCone cone;
+  visited = 0;
+  if (!toward_rect_light(point, corner, eu, ev, normal, cone)) {
+    visible = 0;
+    total = 1;  // m2_gate1.rs:42: (0, 1) for receivers without a cone
+    return;
+  }
+  std::vector<std::pair<uint32_t, const float*>> found;
+  if (bvh) {
+    std::vector<uint32_t> stack{0};
+    while (!stack.empty()) {
+      uint32_t i = stack.back();
+      stack.pop_back();
+      visited++;
+      const auto& n = bvh->nodes[i];
+      if (!may_touch_box(cone, n.mn, n.mx)) continue;
+      if (n.count > 0) {
+        for (uint32_t t = n.start; t < n.start + n.count; ++t) {
+          const float* p = s.tris.data() + 12 * (size_t)bvh->tri[t];
+          V tri[3] = {{p[0], p[1], p[2]}, {p[4], p[5], p[6]}, {p[8], p[9], p[10]}};
+          if (may_touch(cone, tri)) found.push_back({bvh->mesh_of[t], p});
+        }
+      } else {
+        stack.push_back(n.start);
+        stack.push_back(n.start + 1);
+      }
+    }
+    std::stable_sort(found.begin(), found.end(), [](auto& a, auto& b) { return a.first < b.first; });
+  } else {
+    for (uint32_t m = 0; m < s.nmeshes; ++m)
+      for (uint32_t t = s.ranges[4 * m]; t < s.ranges[4 * m] + s.ranges[4 * m + 1]; ++t) {
+        const float* p = s.tris.data() + 12 * (size_t)t;
+        V tri[3] = {{p[0], p[1], p[2]}, {p[4], p[5], p[6]}, {p[8], p[9], p[10]}};
+        if (may_touch(cone, tri)) found.push_back({m, p});
+      }
+  }
+  CoverageMask mask;
+  size_t i = 0;
+  while (i < found.size()) {
+    size_t j = i;
+    std::vector<const float*> tris;
+    while (j < found.size() && found[j].first == found[i].first) tris.push_back(found[j++].second);
+    add_mesh(cone, mask, tris);
+    if (mask.is_full()) break;
+    i = j;
+  }
+  visible = mask.visible_weighted(cone.weights);
+  total = total_weight(cone);
+}
+}  // namespace cpu
+
+// Run `fn(i)` for i in [0, n) on `threads` threads, static contiguous chunks
+// (the reference's par_map partitions rows among threads the same way).
+template <class F> static void parallel_for(uint64_t n, int threads, F fn) {
+  if (threads <= 1 || n < 2) {
+    for (uint64_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<uint64_t> next{0};
+  const uint64_t chunk = 64;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&] {
+      for (;;) {
+        uint64_t start = next.fetch_add(chunk);
+        if (start >= n) break;
+        uint64_t end = std::min(n, start + chunk);
+        for (uint64_t i = start; i < end; ++i) fn(i);
+      }
+    });
+  for (auto& th : pool) th.join();
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+
+extern "C" {
+
+// Builds the reference's host layouts from meshes given as 9 floats per
+// triangle, `mesh_counts[m]` triangles each, consecutive.
+void* oracle_scene_create(const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes) {
+  return build_scene(tri9, mesh_counts, nmeshes);
+}
+
+void oracle_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+// Sizes of the flattened arrays: ntris, nmeshes, nblas, nblas_items, nnodes, nitems.
+void oracle_scene_sizes(void* sp, uint64_t* out6) {
+  Scene* s = static_cast<Scene*>(sp);
+  out6[0] = s->tris.size() / 12;
+  out6[1] = s->nmeshes;
+  out6[2] = s->blas.size();
+  out6[3] = s->blas_items.size();
+  out6[4] = s->nodes.size();
+  out6[5] = s->items.size();
+}
+
+// Copies of the flattened arrays (NodeGpu = 12 x 4 bytes).
+void oracle_scene_arrays(void* sp, uint32_t* ranges, void* blas, uint32_t* blas_items, void* nodes, uint32_t* items) {
+  Scene* s = static_cast<Scene*>(sp);
+  if (ranges) std::memcpy(ranges, s->ranges.data(), s->ranges.size() * 4);
+  if (blas) std::memcpy(blas, s->blas.data(), s->blas.size() * sizeof(Node));
+  if (blas_items) std::memcpy(blas_items, s->blas_items.data(), s->blas_items.size() * 4);
+  if (nodes) std::memcpy(nodes, s->nodes.data(), s->nodes.size() * sizeof(Node));
+  if (items) std::memcpy(items, s->items.data(), s->items.size() * 4);
+}
+
+struct OracleParams {
+  uint32_t hierarchy;
+  float wide_extent;
+  uint32_t light_cone_cap;
+  uint32_t wide_cone_cap;
+};
+
+// Visibility of cones (light l, receiver p), cone id c = l * npoints + p,
+// in the scalar type `precision` (4: float, 8: double). `cone_ids` (nullable)
+// selects a subset; outputs are indexed by position in that subset.
+// receivers: 8 floats each (point.xyzw, normal.xyzw); lights: 16 floats each.
+// full/any: 2 u32 words per cone (bin b in word b/32, bit b%32).
+int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const float* lights, uint32_t nlights,
+                      const OracleParams* prm_in, const uint64_t* cone_ids, uint64_t ncones, int precision,
+                      uint32_t* full, uint32_t* any, float* partial, float* irradiance, float* fraction,
+                      uint32_t* work, float* unshadowed, int threads) {
+  Scene* s = static_cast<Scene*>(sp);
+  if (!s || !prm_in) return 1;
+  uint64_t total = npoints * nlights;
+  uint64_t n = cone_ids ? ncones : total;
+  auto run = [&](auto zero) {
+    using R = decltype(zero);
+    Params<R> prm{prm_in->hierarchy, R(prm_in->wide_extent), prm_in->light_cone_cap, prm_in->wide_cone_cap};
+    parallel_for(n, threads, [&](uint64_t i) {
+      uint64_t c = cone_ids ? cone_ids[i] : i;
+      uint64_t l = c / npoints, p = c % npoints;
+      const float* rc = receivers + 8 * p;
+      const float* lt = lights + 16 * l;
+      Light<R> L{{R(lt[0]), R(lt[1]), R(lt[2])}, R(lt[3]), {R(lt[4]), R(lt[5]), R(lt[6])}, R(lt[7]),
+                 {R(lt[8]), R(lt[9]), R(lt[10])}, R(lt[11])};
+      ConeResult<R> res;
+      visibility_cone<R>(*s, V3<R>{R(rc[0]), R(rc[1]), R(rc[2])}, V3<R>{R(rc[4]), R(rc[5]), R(rc[6])}, L, prm, res);
+      uint32_t f[2] = {0, 0}, a[2] = {0, 0};
+      for (uint32_t b = 0; b < BINS; ++b) {
+        if (res.cov[b] >= R(1)) f[b >> 5] |= 1u << (b & 31);
+        if (res.cov[b] > R(0)) a[b >> 5] |= 1u << (b & 31);
+      }
+      if (full) { full[2 * i] = f[0]; full[2 * i + 1] = f[1]; }
+      if (any) { any[2 * i] = a[0]; any[2 * i + 1] = a[1]; }
+      if (partial)
+        for (uint32_t b = 0; b < BINS; ++b) partial[64 * i + b] = float(res.cov[b]);
+      if (irradiance) irradiance[i] = float(res.irradiance);
+      if (fraction) fraction[i] = float(res.fraction);
+      if (unshadowed) unshadowed[i] = float(res.unshadowed);
+      if (work) {
+        work[4 * i + 0] = res.work.object_nodes;
+        work[4 * i + 1] = res.work.blas_nodes;
+        work[4 * i + 2] = res.work.tris;
+        work[4 * i + 3] = res.work.flags;
+      }
+    });
+  };
+  if (precision == 8)
+    run(double(0));
+  else
+    run(float(0));
+  return 0;
+}
+
+// The reference CPU path (Receiver::masked over cone3 + coverage), FP32:
+// irradiance per unit radiance and each cone's total weight, for a rect light
+// (corner, edge_u, edge_v: 9 floats). use_bvh: 0 brute-force may_touch per
+// triangle (Receiver::new), 1 the leaf-4 BVH (Receiver::with_bvh).
+int oracle_cpu_masked(void* sp, const float* receivers, uint64_t npoints, const float* light9, int use_bvh,
+                      float* visible, float* total, uint32_t* visited, int threads) {
+  Scene* s = static_cast<Scene*>(sp);
+  cpu::Bvh* bvh = use_bvh ? cpu::build_bvh(*s) : nullptr;
+  cpu::V corner{light9[0], light9[1], light9[2]}, eu{light9[3], light9[4], light9[5]}, ev{light9[6], light9[7], light9[8]};
+  parallel_for(npoints, threads, [&](uint64_t p) {
+    const float* rc = receivers + 8 * p;
+    float v, t;
+    uint32_t vis;
+    cpu::receiver_masked(*s, bvh, cpu::V{rc[0], rc[1], rc[2]}, cpu::V{rc[4], rc[5], rc[6]}, corner, eu, ev, v, t, vis);
+    visible[p] = v;
+    if (total) total[p] = t;
+    if (visited) visited[p] = vis;
+  });
+  delete bvh;
+  return 0;
+}
+
+// The DISK table as this file computes it (64 doubles).
+void oracle_disk_table(double* out) {
+  const double* d = disk_table();
+  std::copy(d, d + BINS, out);
+}
+
+// Bin weights of the reference CPU cone (cone3.rs weights), 64 floats; 0 if no cone.
+int oracle_cpu_weights(const float* point, const float* normal, const float* light9, float* weights) {
+  cpu::PyramidCone cone;
+  if (!cpu::toward_rect_light(cpu::V{point[0], point[1], point[2]}, cpu::V{light9[0], light9[1], light9[2]},
+                              cpu::V{light9[3], light9[4], light9[5]}, cpu::V{light9[6], light9[7], light9[8]},
+                              cpu::V{normal[0], normal[1], normal[2]}, cone))
+    return 1;
+  std::copy(cone.weights, cone.weights + BINS, weights);
+  return 0;
+}
+
+uint64_t oracle_poly_overflows() { return g_poly_overflow.load(); }
+}

@@ -1,0 +1,150 @@
+"""ORACLE — test infrastructure. ctypes wrapper of oracle/cone_oracle.cpp.
+
+Used only by tests/, __graft_entry__.smoke() and bench.py's CPU baseline, as
+the checker of the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .build import OUT, build
+
+_lib = None
+
+NODE_DTYPE = np.dtype([("lo", "<f4", 4), ("hi", "<f4", 4), ("info", "<u4", 4)])
+
+
+class _Params(C.Structure):
+    _fields_ = [("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
+                ("wide_cone_cap", C.c_uint32)]
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not OUT.exists():
+            build()
+        lib = C.CDLL(str(OUT))
+        P, U32, U64, I = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+        lib.oracle_scene_create.restype = P
+        lib.oracle_scene_create.argtypes = [P, P, U32]
+        lib.oracle_scene_destroy.argtypes = [P]
+        lib.oracle_scene_sizes.argtypes = [P, P]
+        lib.oracle_scene_arrays.argtypes = [P, P, P, P, P, P]
+        lib.oracle_visibility.restype = I
+        lib.oracle_visibility.argtypes = [P, P, U64, P, U32, C.POINTER(_Params), P, U64, I, P, P, P, P, P, P, P, I]
+        lib.oracle_cpu_masked.restype = I
+        lib.oracle_cpu_masked.argtypes = [P, P, U64, P, I, P, P, P, I]
+        lib.oracle_disk_table.argtypes = [P]
+        lib.oracle_cpu_weights.restype = I
+        lib.oracle_cpu_weights.argtypes = [P, P, P, P]
+        lib.oracle_poly_overflows.restype = U64
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def default_threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
+
+
+class OracleScene:
+    """The reference's host layouts built by the oracle's own restatement."""
+
+    def __init__(self, meshes=None, tri9=None, counts=None):
+        if meshes is not None:
+            parts = [np.asarray(m, np.float32).reshape(-1, 9) for m in meshes]
+            tri9 = np.concatenate(parts) if parts else np.zeros((0, 9), np.float32)
+            counts = np.array([len(p) for p in parts], np.uint32)
+        self.tri9 = np.ascontiguousarray(tri9, np.float32)
+        self.counts = np.ascontiguousarray(counts, np.uint32)
+        self._h = C.c_void_p(load().oracle_scene_create(_p(self.tri9), _p(self.counts), len(self.counts)))
+
+    def sizes(self) -> dict:
+        out = np.zeros(6, np.uint64)
+        load().oracle_scene_sizes(self._h, _p(out))
+        keys = ("ntris", "nmeshes", "nblas", "nblas_items", "nnodes", "nitems")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def arrays(self) -> dict:
+        sz = self.sizes()
+        ranges = np.zeros((sz["nmeshes"], 4), np.uint32)
+        blas = np.zeros(sz["nblas"], NODE_DTYPE)
+        blas_items = np.zeros(sz["nblas_items"], np.uint32)
+        nodes = np.zeros(sz["nnodes"], NODE_DTYPE)
+        items = np.zeros(sz["nitems"], np.uint32)
+        load().oracle_scene_arrays(self._h, _p(ranges), _p(blas), _p(blas_items), _p(nodes), _p(items))
+        return dict(ranges=ranges, blas=blas, blas_items=blas_items, nodes=nodes, items=items)
+
+    def visibility(self, receivers: np.ndarray, lights: np.ndarray, hierarchy: int = 2, precision: int = 4,
+                   cone_ids: np.ndarray | None = None, threads: int | None = None, wide_extent: float = 8.0,
+                   light_cone_cap: int = 4096, wide_cone_cap: int = 512, partial: bool = True) -> dict:
+        """Per-cone results (cone c = light * npoints + point), for all cones or
+        the `cone_ids` subset (outputs in subset order)."""
+        rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
+        lig = np.ascontiguousarray(lights, np.float32).reshape(-1, 16)
+        n = rec.shape[0] * lig.shape[0] if cone_ids is None else len(cone_ids)
+        ids = None if cone_ids is None else np.ascontiguousarray(cone_ids, np.uint64)
+        full = np.zeros((n, 2), np.uint32)
+        any_ = np.zeros((n, 2), np.uint32)
+        part = np.zeros((n, 64), np.float32) if partial else None
+        irr = np.zeros(n, np.float32)
+        frac = np.zeros(n, np.float32)
+        work = np.zeros((n, 4), np.uint32)
+        unsh = np.zeros(n, np.float32)
+        prm = _Params(hierarchy, wide_extent, light_cone_cap, wide_cone_cap)
+        rc = load().oracle_visibility(self._h, _p(rec), rec.shape[0], _p(lig), lig.shape[0], C.byref(prm), _p(ids),
+                                      0 if ids is None else len(ids), precision, _p(full), _p(any_), _p(part),
+                                      _p(irr), _p(frac), _p(work), _p(unsh), threads or default_threads())
+        if rc != 0:
+            raise RuntimeError(f"oracle_visibility failed: {rc}")
+        return dict(full=full.view(np.uint64).reshape(n), any=any_.view(np.uint64).reshape(n), partial=part,
+                    irradiance=irr, fraction=frac, work=work, unshadowed=unsh)
+
+    def cpu_masked(self, receivers: np.ndarray, light9, use_bvh: bool = False, threads: int | None = None):
+        """The reference CPU path (cone3 + coverage, Receiver::masked): (visible, total weight)."""
+        rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
+        l9 = np.ascontiguousarray(light9, np.float32).reshape(9)
+        vis = np.zeros(rec.shape[0], np.float32)
+        tot = np.zeros(rec.shape[0], np.float32)
+        visited = np.zeros(rec.shape[0], np.uint32)
+        load().oracle_cpu_masked(self._h, _p(rec), rec.shape[0], _p(l9), int(use_bvh), _p(vis), _p(tot),
+                                 _p(visited), threads or default_threads())
+        return vis, tot
+
+    def close(self):
+        if self._h:
+            load().oracle_scene_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def disk_table() -> np.ndarray:
+    out = np.zeros(64, np.float64)
+    load().oracle_disk_table(_p(out))
+    return out
+
+
+def cpu_weights(point, normal, light9) -> np.ndarray:
+    p = np.ascontiguousarray(point, np.float32)
+    n = np.ascontiguousarray(normal, np.float32)
+    l9 = np.ascontiguousarray(light9, np.float32)
+    w = np.zeros(64, np.float32)
+    if load().oracle_cpu_weights(_p(p), _p(n), _p(l9), _p(w)) != 0:
+        raise ValueError("no cone")
+    return w
+
+
+def poly_overflows() -> int:
+    return int(load().oracle_poly_overflows())
