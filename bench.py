@@ -43,10 +43,21 @@ NODE_BYTES = 48  # reference NodeGpu (hierarchy.rs:68-76)
 TRI_BYTES = 48   # three vec4 vertices (hierarchy.rs:12-13)
 
 
-def workload():
+def workload(points: int = 0):
     from continuum_b200 import scenes
 
-    return scenes.icosphere_field(seed=2)
+    w = scenes.icosphere_field(seed=2)
+    if points and points < w.receivers.shape[0]:
+        width, height = w.size
+        if w.receivers.shape[0] == width * height:
+            # Whole image rows, evenly spaced: neighbours stay neighbours.
+            rows = max(1, points // width)
+            img = w.receivers.reshape(height, width, 8)
+            w.receivers = np.ascontiguousarray(img[:: max(1, height // rows)][:rows].reshape(-1, 8))
+        else:
+            stride = w.receivers.shape[0] // points
+            w.receivers = np.ascontiguousarray(w.receivers[::stride][:points])
+    return w
 
 
 def config(n_gpus: int, w) -> dict:
@@ -184,7 +195,7 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    w = workload()
+    w = workload(args.points)
     P, L = w.receivers.shape[0], w.lights.shape[0]
     C = P * L
     kernel = MaskConeKernel(local_rank)
@@ -194,7 +205,10 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
     outs = {"full": torch.empty(C, dtype=torch.int64, device=dev), "any": torch.empty(C, dtype=torch.int64, device=dev),
             "irradiance": torch.empty(C, device=dev), "fraction": torch.empty(C, device=dev)}
     ptrs = {k: v.data_ptr() for k, v in outs.items()}
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated stream for every timed launch (torch's default stream has
+    # handle 0, which the library reads as "the context's own stream").
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def step():
@@ -260,13 +274,14 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         _lib.check(_lib.load().cc_visibility(kernel.handle, scene.handle, rec_h.ctypes.data, P, lig_h.ctypes.data, L,
                                              Cc.byref(opt), Cc.byref(o), None))
 
-    e2e_step()
+    if not args.no_e2e:
+        e2e_step()
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(0 if args.no_e2e else e2e_steps):
         e2e_step()
-    e2e_time = time.perf_counter() - t0
+    e2e_time = max(time.perf_counter() - t0, 1e-9)
     if world > 1:
         t = torch.tensor([e2e_time], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -331,6 +346,9 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=3.0)
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--points", type=int, default=0,
+                    help="keep a strided subset of this many receivers (profiling runs; not a bench line)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

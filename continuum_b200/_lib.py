@@ -24,6 +24,7 @@ CC_NONE = 0xFFFFFFFF
 
 CC_DEVICE_POINTERS = 1
 CC_NO_REDO = 2
+CC_KEEP_ORDER = 4
 
 CC_CONE_CAPPED = 1
 CC_CONE_STACK = 2

@@ -84,6 +84,8 @@ struct cc_context {
   cudaStream_t stream = nullptr;
   DevBuf receivers, lights, full, any, partial, irradiance, fraction, work;
   DevBuf redo;      // redo list
+  DevBuf order;     // walk order of the points
+  DevBuf sort_scratch;
   DevBuf counters;  // [redo count, error word]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Kernel timing: three events per visibility call (before the packet pass,
@@ -102,7 +104,6 @@ struct cc_scene {
   float4* nodes = nullptr;
   uint32_t* items = nullptr;
   float4* blas = nullptr;
-  uint32_t* blas_items = nullptr;
   uint64_t bytes = 0;
   cc::DevScene dev() const {
     cc::DevScene s;
@@ -111,7 +112,6 @@ struct cc_scene {
     s.nodes = nodes;
     s.items = items;
     s.blas = blas;
-    s.blas_items = blas_items;
     s.nmeshes = flat.nmeshes;
     return s;
   }
@@ -154,29 +154,39 @@ void free_scene_device(cc_scene* s) {
   cudaFree(s->nodes);
   cudaFree(s->items);
   cudaFree(s->blas);
-  cudaFree(s->blas_items);
   s->tris = nullptr;
   s->meshes = nullptr;
   s->nodes = nullptr;
   s->items = nullptr;
   s->blas = nullptr;
-  s->blas_items = nullptr;
 }
 
 int upload_scene(cc_scene* s) {
   const cc::FlatScene& f = s->flat;
-  std::vector<float4> tris(f.tris.size() / 4);
-  std::memcpy(tris.data(), f.tris.data(), f.tris.size() * sizeof(float));
+  // Triangles in leaf order: slot k holds triangle blas_items[k], so a
+  // triangle-hierarchy leaf's items are slots. Each mesh's items permute its
+  // own range, so a mesh's range of slots still holds exactly its triangles.
+  const size_t ntris = f.tris.size() / 12;
+  std::vector<float4> tris(3 * ntris);
+  for (size_t k = 0; k < ntris; ++k) {
+    const size_t t = (!f.blas.empty() && k < f.blas_items.size()) ? f.blas_items[k] : k;
+    for (int v = 0; v < 3; ++v) {
+      const float* p = &f.tris[12 * t + 4 * v];
+      tris[3 * k + v] = make_float4(p[0], p[1], p[2], p[3]);
+    }
+  }
   std::vector<uint4> meshes(f.nmeshes);
   for (uint32_t m = 0; m < f.nmeshes; ++m)
     meshes[m] = make_uint4(f.ranges[4 * m], f.ranges[4 * m + 1], f.ranges[4 * m + 2], f.ranges[4 * m + 3]);
+  // Without meshes the object hierarchy is one leaf holding mesh 0, which
+  // must then be an empty range (as flatten pads it, hierarchy.rs:57-59).
+  if (meshes.empty()) meshes.push_back(make_uint4(0u, 0u, CC_NONE, CC_NONE));
   int rc;
   if ((rc = upload(tris, &s->tris, s->bytes, "scene triangles"))) return rc;
   if ((rc = upload(meshes, &s->meshes, s->bytes, "scene meshes"))) return rc;
   if ((rc = upload(repack(f.nodes), &s->nodes, s->bytes, "scene nodes"))) return rc;
   if ((rc = upload(f.items, &s->items, s->bytes, "scene items"))) return rc;
   if ((rc = upload(repack(f.blas), &s->blas, s->bytes, "scene triangle nodes"))) return rc;
-  if ((rc = upload(f.blas_items, &s->blas_items, s->bytes, "scene triangle items"))) return rc;
   return CC_OK;
 }
 
@@ -204,6 +214,26 @@ int validate_flat(const cc::FlatScene& f) {
   if ((rc = check_nodes(f.nodes, f.items.size(), "object hierarchy"))) return rc;
   for (uint32_t t : f.blas_items)
     if (t >= ntris) return fail(CC_ERR_INVALID, "triangle hierarchy item out of range");
+  // Each mesh's leaf items must permute its own triangle range (as flatten
+  // lays them out, hierarchy.rs:38-45); the device stores triangles in that
+  // order.
+  if (!f.blas.empty()) {
+    if (f.blas_items.size() != ntris) return fail(CC_ERR_INVALID, "triangle hierarchy items must cover every triangle");
+    std::vector<uint8_t> seen(ntris, 0);
+    for (uint32_t m = 0; m < f.nmeshes; ++m) {
+      const uint32_t first = f.ranges[4 * m], count = f.ranges[4 * m + 1];
+      for (uint64_t k = first; k < (uint64_t)first + count; ++k) {
+        const uint32_t t = f.blas_items[k];
+        if (t < first || t >= (uint64_t)first + count || seen[t])
+          return fail(CC_ERR_INVALID, "a mesh's triangle hierarchy items must permute its triangle range");
+        seen[t] = 1;
+      }
+    }
+  }
+  for (const auto* nodes : {&f.blas, &f.nodes})
+    for (const cc::NodeGpu& n : *nodes)
+      if (n.info[1] > 15 || n.info[0] >= (1u << 28))
+        return fail(CC_ERR_INVALID, "hierarchy leaves hold at most 15 items and indices stay below 2^28");
   for (uint32_t m : f.items)
     if (m >= std::max<uint32_t>(f.nmeshes, 1)) return fail(CC_ERR_INVALID, "object hierarchy item out of range");
   if (f.nodes.empty()) return fail(CC_ERR_INVALID, "empty object hierarchy");
@@ -422,6 +452,7 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
   if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
   const uint64_t ncones = npoints * (uint64_t)nlights;
   if (ncones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one call");
+  if (npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one call");
   int rc = set_device(ctx);
   if (rc) return rc;
   cudaStream_t stream = stream_in ? (cudaStream_t)stream_in : ctx->stream;
@@ -436,6 +467,12 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
   q.wide_cone_cap = opt.wide_cone_cap;
   cc::DevOut o{};
   if (device_ptrs) {
+    // The kernels read and write these with vector accesses.
+    auto misaligned = [](const void* p, uintptr_t a) { return p && (reinterpret_cast<uintptr_t>(p) % a) != 0; };
+    if (misaligned(receivers, 16) || misaligned(lights, 16) || misaligned(out->partial, 16) ||
+        misaligned(out->work, 16) || misaligned(out->full, 8) || misaligned(out->any, 8) ||
+        misaligned(out->irradiance, 4) || misaligned(out->fraction, 4))
+      return fail(CC_ERR_INVALID, "device buffers must be aligned (receivers, lights, partial, work: 16 B; full, any: 8 B)");
     q.receivers = reinterpret_cast<const float4*>(receivers);
     q.lights = reinterpret_cast<const float4*>(lights);
     o.full = reinterpret_cast<uint2*>(out->full);
@@ -467,6 +504,18 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
     o.redo_capacity = (uint32_t)std::max<uint64_t>(ncones, 1);
   }
   CC_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), stream), "counter reset");
+  // Walk the points in Morton order of their positions (coherent packets).
+  q.order = nullptr;
+  if (!(opt.flags & CC_KEEP_ORDER) && npoints > 64 && !scene->flat.nodes.empty()) {
+    CC_CUDA(ctx->order.reserve(npoints * sizeof(uint32_t)), "walk order");
+    const size_t need = cc::walk_order_scratch_bytes(npoints);
+    CC_CUDA(ctx->sort_scratch.reserve(need), "walk order scratch");
+    CC_CUDA(cc::walk_order(q.receivers, npoints, scene->flat.nodes[0].lo, scene->flat.nodes[0].hi,
+                           ctx->sort_scratch.ptr, ctx->sort_scratch.size, static_cast<uint32_t*>(ctx->order.ptr),
+                           stream),
+            "walk order");
+    q.order = static_cast<const uint32_t*>(ctx->order.ptr);
+  }
   // The call's slot in the timing ring (the oldest unread call is dropped
   // when the ring is full).
   const int ring = cc_context::kTimingRing;

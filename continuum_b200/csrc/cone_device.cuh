@@ -40,12 +40,11 @@ __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fm
 // Nodes are two float4: (lo.xyz, a) and (hi.xyz, b) with a, b as bits:
 // leaf: a = first item, b = item count; interior: a = left child, b = 0.
 struct DevScene {
-  const float4* tris;      // 3 per triangle (w unused)
+  const float4* tris;      // 3 per triangle (w unused), in triangle-hierarchy leaf order
   const uint4* meshes;     // first, count, blas root, transform
   const float4* nodes;     // object hierarchy, 2 per node
   const uint32_t* items;   // mesh per object leaf slot
-  const float4* blas;      // triangle hierarchies, 2 per node
-  const uint32_t* blas_items;
+  const float4* blas;      // triangle hierarchies, 2 per node; leaf items are triangle slots
   uint32_t nmeshes;
 };
 

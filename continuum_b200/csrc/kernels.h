@@ -8,6 +8,7 @@
 namespace cc {
 
 constexpr int kWarpsPerBlock = 4;
+constexpr int kBlocksPerSm = 3;  // resident blocks per SM the shared memory allows
 
 struct DevQuery {
   const float4* receivers;  // 2 per point: point, normal
@@ -18,7 +19,17 @@ struct DevQuery {
   float wide_extent;
   uint32_t light_cone_cap;
   uint32_t wide_cone_cap;
+  // The walk order of the points (a permutation; null: as given). Slot s
+  // walks cone (s / npoints) * npoints + order[s % npoints].
+  const uint32_t* order;
 };
+
+// Scratch bytes walk_order needs for `npoints` receivers.
+size_t walk_order_scratch_bytes(uint64_t npoints);
+// Morton order of the receivers' positions in the scene's bounds, into
+// `order` (npoints entries), on `stream`.
+cudaError_t walk_order(const float4* receivers, uint64_t npoints, const float* scene_lo, const float* scene_hi,
+                       void* scratch, size_t scratch_bytes, uint32_t* order, cudaStream_t stream);
 
 struct DevOut {
   uint2* full;

@@ -31,12 +31,34 @@ __constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded b
 
 constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
 
+// A stack entry is a node reference packed in one word: the node's item
+// count in the top 4 bits (0: interior) and its first item (leaf) or left
+// child (interior) below. Each lane keeps two bits per entry: whether its
+// own walk needs the entry, and whether its cone passed the entry's box
+// test, which is done when the parent is visited (the two children of a
+// node are adjacent, so one 64-byte load serves both tests and the
+// nearest-first choice).
+constexpr uint32_t kRefIndexBits = 28;
+constexpr uint32_t kRefIndexMask = (1u << kRefIndexBits) - 1u;
+__device__ __forceinline__ uint32_t node_ref(float4 a, float4 b) {
+  return (__float_as_uint(b.w) << kRefIndexBits) | (__float_as_uint(a.w) & kRefIndexMask);
+}
+
 struct WarpStack {
   uint32_t r0 = 0, r1 = 0;  // entry i held by lane i % 32, register i / 32
   uint32_t need_lo = 0, need_hi = 0;
-  __device__ __forceinline__ void push(int i, uint32_t v, int lane) {
+  uint32_t pass_lo = 0, pass_hi = 0;
+  __device__ __forceinline__ void push(int i, uint32_t v, bool need, bool pass, int lane) {
     if ((i & 31) == lane) {
       if (i < 32) r0 = v; else r1 = v;
+    }
+    const uint32_t bit = 1u << (i & 31);
+    if (i < 32) {
+      need_lo = need ? (need_lo | bit) : (need_lo & ~bit);
+      pass_lo = pass ? (pass_lo | bit) : (pass_lo & ~bit);
+    } else {
+      need_hi = need ? (need_hi | bit) : (need_hi & ~bit);
+      pass_hi = pass ? (pass_hi | bit) : (pass_hi & ~bit);
     }
   }
   __device__ __forceinline__ uint32_t get(int i) const {
@@ -45,10 +67,8 @@ struct WarpStack {
   __device__ __forceinline__ bool need(int i) const {
     return ((i < 32 ? need_lo : need_hi) >> (i & 31)) & 1u;
   }
-  __device__ __forceinline__ void set_need(int i, bool v) {
-    uint32_t bit = 1u << (i & 31);
-    if (i < 32) need_lo = v ? (need_lo | bit) : (need_lo & ~bit);
-    else need_hi = v ? (need_hi | bit) : (need_hi & ~bit);
+  __device__ __forceinline__ bool pass(int i) const {
+    return ((i < 32 ? pass_lo : pass_hi) >> (i & 31)) & 1u;
   }
 };
 
@@ -83,7 +103,10 @@ __device__ __forceinline__ bool cover_triangle(const DevScene& s, LaneState& st,
 
 // add_mesh_coverage_if (:713-829) for the lanes with `on`; the others
 // follow the packet's walk. The triangle hierarchy's stack entries start at
-// `base`, above the object walk's.
+// `base`, above the object walk's. A node still counts toward the walk cap
+// when it is popped, as in the reference, though its box was tested when its
+// parent was visited. Triangles are stored in leaf order, so a leaf's items
+// are the triangle slots themselves.
 template <bool kCount>
 __device__ __forceinline__ void add_mesh(const DevScene& s, uint32_t hierarchy, LaneState& st, WarpStack& stk,
                                          bool on, uint32_t m, int base, int lane) {
@@ -93,48 +116,51 @@ __device__ __forceinline__ void add_mesh(const DevScene& s, uint32_t hierarchy, 
   bool touched = false;
   if (hierarchy == 2) {
     if (range.z != kNoneU) {
+      const float4 ra = __ldg(&s.blas[2 * (size_t)range.z + 0]);
+      const float4 rb = __ldg(&s.blas[2 * (size_t)range.z + 1]);
+      const bool root_pass = on && may_touch_box(st.cone, node_lo(ra), node_lo(rb));
       int sp = base;
-      stk.push(sp, range.z, lane);
-      stk.set_need(sp, on);
+      stk.push(sp, node_ref(ra, rb), on, root_pass, lane);
       ++sp;
       while (sp > base) {
         --sp;
-        const uint32_t n = stk.get(sp);
+        const uint32_t ref = stk.get(sp);
         const bool mine = stk.need(sp) && st.cone_work < st.cap;
         if (mine) st.cone_work++;
-        if (!__any_sync(0xffffffffu, mine)) continue;
-        const float4 a = __ldg(&s.blas[2 * (size_t)n + 0]);
-        const float4 b = __ldg(&s.blas[2 * (size_t)n + 1]);
-        bool descend = false;
-        if (mine) {
-          if (kCount) st.n_blas++;
-          descend = may_touch_box(st.cone, node_lo(a), node_lo(b));
-        }
+        if (kCount && mine) st.n_blas++;
+        const bool descend = mine && stk.pass(sp);
         if (!__any_sync(0xffffffffu, descend)) continue;
-        const uint32_t ia = __float_as_uint(a.w), ib = __float_as_uint(b.w);
+        const uint32_t ia = ref & kRefIndexMask, ib = ref >> kRefIndexBits;
         if (ib > 0) {
-          if (descend) st.cone_work += ib;
-          for (uint32_t k = ia; k < ia + ib; ++k) {
-            const uint32_t t = __ldg(&s.blas_items[k]);
-            if (descend && cover_triangle<kCount>(s, st, acc, t)) touched = true;
+          if (descend) {
+            st.cone_work += ib;
+            for (uint32_t k = ia; k < ia + ib; ++k)
+              if (cover_triangle<kCount>(s, st, acc, k)) touched = true;
           }
         } else {
+          const float4 la = __ldg(&s.blas[2 * (size_t)ia + 0]);
+          const float4 lb = __ldg(&s.blas[2 * (size_t)ia + 1]);
+          const float4 xa = __ldg(&s.blas[2 * (size_t)ia + 2]);
+          const float4 xb = __ldg(&s.blas[2 * (size_t)ia + 3]);
+          bool pl = false, pr = false;
+          if (descend) {
+            pl = may_touch_box(st.cone, node_lo(la), node_lo(lb));
+            pr = may_touch_box(st.cone, node_lo(xa), node_lo(xb));
+          }
           if (sp + 2 > kStack) {
             if (descend) st.status |= 2u;
             continue;
           }
           // Right child popped first (:783-787).
-          stk.push(sp, ia, lane);
-          stk.push(sp + 1, ia + 1, lane);
-          stk.set_need(sp, descend);
-          stk.set_need(sp + 1, descend);
+          stk.push(sp, node_ref(la, lb), descend, pl, lane);
+          stk.push(sp + 1, node_ref(xa, xb), descend, pr, lane);
           sp += 2;
         }
       }
     }
-  } else {
+  } else if (on) {
     for (uint32_t t = range.x; t < range.x + range.y; ++t)
-      if (on && cover_triangle<kCount>(s, st, acc, t)) touched = true;
+      if (cover_triangle<kCount>(s, st, acc, t)) touched = true;
   }
   // The mesh's coverage: running sum over the touched cells, snapped to
   // whole within 1e-5, combined into the cone's bins by max (:809-828).
@@ -163,58 +189,61 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
                                            int lane) {
   WarpStack stk;
   if (hierarchy >= 1) {
-    int sp = 0;
-    stk.push(0, 0u, lane);
-    stk.set_need(0, traced);
-    sp = 1;
+    const float4 ra = __ldg(&s.nodes[0]);
+    const float4 rb = __ldg(&s.nodes[1]);
+    const bool root_pass = traced && may_touch_box(st.cone, node_lo(ra), node_lo(rb));
+    stk.push(0, node_ref(ra, rb), traced, root_pass, lane);
+    int sp = 1;
     while (sp > 0) {
       --sp;
-      const uint32_t n = stk.get(sp);
+      const uint32_t ref = stk.get(sp);
       const bool mine = stk.need(sp) && st.full < (uint32_t)kBins && st.cone_work < st.cap;
       if (mine) st.cone_work++;
-      if (!__any_sync(0xffffffffu, mine)) continue;
-      const float4 a = __ldg(&s.nodes[2 * (size_t)n + 0]);
-      const float4 b = __ldg(&s.nodes[2 * (size_t)n + 1]);
-      bool descend = false;
-      if (mine) {
-        if (kCount) st.n_obj++;
-        descend = may_touch_box(st.cone, node_lo(a), node_lo(b));
-      }
+      if (kCount && mine) st.n_obj++;
+      const bool descend = mine && stk.pass(sp);
       if (!__any_sync(0xffffffffu, descend)) continue;
-      const uint32_t ia = __float_as_uint(a.w), ib = __float_as_uint(b.w);
+      const uint32_t ia = ref & kRefIndexMask, ib = ref >> kRefIndexBits;
       if (ib > 0) {
-        for (uint32_t k = ia; k < ia + ib; ++k) add_mesh<kCount>(s, hierarchy, st, stk, descend, __ldg(&s.items[k]), sp, lane);
+        for (uint32_t k = ia; k < ia + ib; ++k)
+          add_mesh<kCount>(s, hierarchy, st, stk, descend, __ldg(&s.items[k]), sp, lane);
       } else {
         const float4 la = __ldg(&s.nodes[2 * (size_t)ia + 0]);
         const float4 lb = __ldg(&s.nodes[2 * (size_t)ia + 1]);
-        const float4 ra = __ldg(&s.nodes[2 * (size_t)ia + 2]);
-        const float4 rb = __ldg(&s.nodes[2 * (size_t)ia + 3]);
+        const float4 xa = __ldg(&s.nodes[2 * (size_t)ia + 2]);
+        const float4 xb = __ldg(&s.nodes[2 * (size_t)ia + 3]);
         const Cone& c = st.cone;
+        bool pl = false, pr = false;
+        if (descend) {
+          pl = may_touch_box(c, node_lo(la), node_lo(lb));
+          pr = may_touch_box(c, node_lo(xa), node_lo(xb));
+        }
         const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
-        const float db = dot(c.baxis, (node_lo(ra) + node_lo(rb)) * 0.5f - c.apex);
+        const float db = dot(c.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - c.apex);
         const bool pref = db < da;  // this lane's own order: right child nearer
         const uint32_t voters = __ballot_sync(0xffffffffu, descend);
         const bool swap = __shfl_sync(0xffffffffu, pref, __ffs(voters) - 1);
         if (descend && pref != swap) st.status |= 4u;
-        const uint32_t near_ = swap ? ia + 1 : ia, far_ = swap ? ia : ia + 1;
         if (sp + 2 > kStack) {
           if (descend) st.status |= 2u;
           continue;
         }
-        stk.push(sp, far_, lane);
-        stk.push(sp + 1, near_, lane);
-        stk.set_need(sp, descend);
-        stk.set_need(sp + 1, descend);
+        const uint32_t rl = node_ref(la, lb), rr = node_ref(xa, xb);
+        // The far child below the near one: the near child is popped first.
+        stk.push(sp, swap ? rl : rr, descend, swap ? pl : pr, lane);
+        stk.push(sp + 1, swap ? rr : rl, descend, swap ? pr : pl, lane);
         sp += 2;
       }
     }
   } else {
-    for (uint32_t m = 0; m < s.nmeshes; ++m) add_mesh<kCount>(s, hierarchy, st, stk, traced && st.full < (uint32_t)kBins, m, 0, lane);
+    for (uint32_t m = 0; m < s.nmeshes; ++m)
+      add_mesh<kCount>(s, hierarchy, st, stk, traced && st.full < (uint32_t)kBins, m, 0, lane);
   }
 }
 
 template <bool kCount>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+// Three blocks per SM fit the shared memory (3 x 64 KB); saying so lets the
+// register allocator use up to 170 registers a thread instead of spilling.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     visibility_kernel(DevScene s, DevQuery q, DevOut o, const uint32_t* __restrict__ list,
                       const uint32_t* __restrict__ list_count, uint32_t pw) {
   extern __shared__ float smem[];
@@ -229,7 +258,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
   for (uint64_t wbase = ((uint64_t)blockIdx.x * kWarpsPerBlock + wib) * pw; wbase < ncones; wbase += warps * pw) {
     const uint64_t slot = wbase + lane;
     const bool valid = (uint32_t)lane < pw && slot < ncones;
-    const uint64_t c = valid ? (list ? (uint64_t)list[slot] : slot) : 0;
+    uint64_t c = 0;
+    if (valid) {
+      if (list) {
+        c = list[slot];
+      } else if (q.order) {
+        const uint64_t light_base = (slot / q.npoints) * q.npoints;
+        c = light_base + __ldg(&q.order[slot - light_base]);
+      } else {
+        c = slot;
+      }
+    }
     const uint32_t l = (uint32_t)(c / q.npoints);
     const uint64_t p = c - (uint64_t)l * q.npoints;
 
@@ -351,16 +390,21 @@ cudaError_t upload_disk_table(const float* table64) {
   return cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
 }
 
-static bool g_attr_set[2] = {false, false};
+// Whether the large dynamic shared memory size was allowed, per device and
+// kernel variant (the attribute is set per device).
+static uint64_t g_attr_set[2] = {0, 0};
 
 template <bool kCount>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const uint32_t* list,
                               const uint32_t* list_count, uint32_t pw, uint32_t blocks, cudaStream_t stream) {
   const size_t smem = (size_t)kWarpsPerBlock * 2 * kBins * 32 * sizeof(float);
-  if (!g_attr_set[kCount]) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(g_attr_set[kCount] & bit)) {
     cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    g_attr_set[kCount] = true;
+    g_attr_set[kCount] |= bit;
   }
   visibility_kernel<kCount><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, list, list_count, pw);
   return cudaGetLastError();

@@ -61,6 +61,7 @@ extern "C" {
 /* cc_options.flags */
 #define CC_DEVICE_POINTERS 1u /* receivers, lights and outputs are device pointers */
 #define CC_NO_REDO 2u         /* skip the solo re-walk of order-diverged cones (diagnostic) */
+#define CC_KEEP_ORDER 4u      /* walk points in the given order (default: Morton order of their positions) */
 
 /* Status bits in cc_outputs.work[4 * c + 3] */
 #define CC_CONE_CAPPED 1u     /* the walk stopped at its cap (LIGHT_CONE_CAP / WIDE_CONE_CAP) */
@@ -137,7 +138,7 @@ typedef struct cc_options {
   uint32_t light_cone_cap;   /* LIGHT_CONE_CAP, mask_cones.wgsl:1052 (4096) */
   uint32_t wide_cone_cap;    /* WIDE_CONE_CAP, mask_cones.wgsl:1056 (512) */
   uint32_t points_per_warp;  /* cones walked together per warp: 1..32 (32); results do not depend on it */
-  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO */
+  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO, CC_KEEP_ORDER */
 } cc_options;
 
 /* Defaults: hierarchy 2, 8.0, 4096, 512, 32, 0. */
