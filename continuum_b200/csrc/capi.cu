@@ -285,7 +285,7 @@ int cc_context_create(int device, cc_context** out) {
   float disk[64];
   disk_table(disk);
   if (e == cudaSuccess) e = cc::upload_disk_table(disk);
-  if (e == cudaSuccess) e = ctx->counters.reserve(2 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = ctx->counters.reserve(cc::kCounterWords * sizeof(uint32_t));
   ctx->marks.assign(3 * cc_context::kTimingRing, nullptr);
   for (auto& ev : ctx->marks)
     if (e == cudaSuccess) e = cudaEventCreate(&ev);
@@ -498,12 +498,14 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
   uint32_t* counters = static_cast<uint32_t*>(ctx->counters.ptr);
   o.redo_count = counters;
   o.error = counters + 1;
+  o.next_packet = counters + 2;
+  o.next_solo = counters + 3;
   if (!(opt.flags & CC_NO_REDO)) {
     CC_CUDA(ctx->redo.reserve(std::max<uint64_t>(ncones, 1) * 4), "redo list");
     o.redo_list = static_cast<uint32_t*>(ctx->redo.ptr);
     o.redo_capacity = (uint32_t)std::max<uint64_t>(ncones, 1);
   }
-  CC_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), stream), "counter reset");
+  CC_CUDA(cudaMemsetAsync(counters, 0, cc::kCounterWords * sizeof(uint32_t), stream), "counter reset");
   // Walk the points in Morton order of their positions (coherent packets).
   q.order = nullptr;
   if (!(opt.flags & CC_KEEP_ORDER) && npoints > 64 && !scene->flat.nodes.empty()) {

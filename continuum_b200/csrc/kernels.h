@@ -44,7 +44,13 @@ struct DevOut {
   uint32_t* redo_count;
   uint32_t redo_capacity;
   uint32_t* error;
+  // Work counters: the next packet of the packet pass and of the solo pass.
+  uint32_t* next_packet;
+  uint32_t* next_solo;
 };
+
+// Scratch words per call: redo count, error word, packet and solo counters.
+constexpr int kCounterWords = 4;
 
 cudaError_t upload_disk_table(const float* table64);
 

@@ -30,6 +30,10 @@ namespace cc {
 __constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded by the host
 
 constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
+// Shared memory per warp: the lanes' coverages (64 x 32), accumulators
+// (64 x 32) and the cooperative integration's corners and edges (387).
+constexpr int kScratchFloats = 416;
+constexpr int kWarpFloats = 2 * kBins * 32 + kScratchFloats;
 
 // A stack entry is a node reference packed in one word: the node's item
 // count in the top 4 bits (0: interior) and its first item (leaf) or left
@@ -86,19 +90,27 @@ struct LaneState {
 
 __device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
 
-template <bool kCount>
-__device__ __forceinline__ bool cover_triangle(const DevScene& s, LaneState& st, LaneAcc& acc, uint32_t t) {
-  if (kCount) st.n_tris++;
+// The cheap tests of cover_triangle (:594-612): faces the apex, some window
+// direction enters its plane, may touch the cone.
+__device__ __forceinline__ bool cull_triangle(const LaneState& st, f3 v0, f3 v1, f3 v2) {
   const Cone& c = st.cone;
-  f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
-  f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
-  f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
   f3 n = cross(v1 - v0, v2 - v0);
   if (dot(n, c.apex - v0) <= 0.0f) return false;  // faces away (:600)
   if (dot(n, st.d00) >= 0.f && dot(n, st.d10) >= 0.f && dot(n, st.d01) >= 0.f && dot(n, st.d11) >= 0.f)
     return false;  // every window direction leaves its plane (:601-606)
-  if (!may_touch(c, v0, v1, v2)) return false;
-  return rasterize(c, acc, v0, v1, v2);
+  return may_touch(c, v0, v1, v2);
+}
+
+// cover_triangle (:594-616): triangle slot t rasterized into `acc` if it
+// faces the apex and may touch the cone.
+template <bool kCount>
+__device__ __forceinline__ bool cover_triangle(const DevScene& s, LaneState& st, LaneAcc& acc, uint32_t t) {
+  if (kCount) st.n_tris++;
+  f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
+  f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
+  f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
+  if (!cull_triangle(st, v0, v1, v2)) return false;
+  return rasterize(st.cone, acc, v0, v1, v2);
 }
 
 // add_mesh_coverage_if (:713-829) for the lanes with `on`; the others
@@ -240,6 +252,80 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
   }
 }
 
+__device__ __forceinline__ f3 shfl3(f3 v, int src) {
+  return mk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src), __shfl_sync(0xffffffffu, v.z, src));
+}
+
+// The blocked light of lane j's cone, Σ coverage × bin weight (cone_visible,
+// :1244-1272), computed by the whole warp. With the window above the
+// horizon every bin weight is Lambert's formula over its quad
+// (bin_weight, :1232-1242); the 64 quads share 81 corner directions and 144
+// edges, so the warp normalizes each corner once and integrates each edge
+// once (a quad's edges are its neighbours' reversed, exact negatives in
+// IEEE arithmetic) and each lane combines two bins. A window crossing the
+// horizon clips each bin on its own (clipped_bin_weight, :1331-1369).
+// `cov_j` is lane j's coverage column (bin b at cov_j[32 * b]); `scratch`
+// holds 387 floats. Every lane returns the sum.
+__device__ __noinline__ float warp_blocked(const Cone& mine, f3 my_normal, bool my_all_above, const float* cov_j,
+                                           float* scratch, int j, int lane) {
+  Cone c;
+  c.fwd = shfl3(mine.fwd, j);
+  c.right = shfl3(mine.right, j);
+  c.up = shfl3(mine.up, j);
+  c.u0 = __shfl_sync(0xffffffffu, mine.u0, j);
+  c.v0 = __shfl_sync(0xffffffffu, mine.v0, j);
+  c.u1 = __shfl_sync(0xffffffffu, mine.u1, j);
+  c.v1 = __shfl_sync(0xffffffffu, mine.v1, j);
+  const f3 n = shfl3(my_normal, j);
+  const bool all_above = __shfl_sync(0xffffffffu, my_all_above, j);
+  float sum = 0.0f;
+  if (all_above) {
+    const float g = float(kGrid);
+    float* corner = scratch;       // 81 unit directions, point (col, row) at 3 * (row * 9 + col)
+    float* edge = scratch + 243;   // 72 row edges (col, row)->(col+1, row), then 72 column edges (col, row)->(col, row+1)
+    for (int p = lane; p < 81; p += 32) {
+      const f3 u = normalize(direction(c, float(p % 9) / g, float(p / 9) / g));
+      corner[3 * p] = u.x;
+      corner[3 * p + 1] = u.y;
+      corner[3 * p + 2] = u.z;
+    }
+    __syncwarp();
+    for (int e = lane; e < 144; e += 32) {
+      int a, b;
+      if (e < 72) {
+        a = (e / 8) * 9 + e % 8;
+        b = a + 1;
+      } else {
+        a = ((e - 72) / 9) * 9 + (e - 72) % 9;
+        b = a + 9;
+      }
+      edge[e] = lambert_edge_unit(n, mk(corner[3 * a], corner[3 * a + 1], corner[3 * a + 2]),
+                                  mk(corner[3 * b], corner[3 * b + 1], corner[3 * b + 2]));
+    }
+    __syncwarp();
+    for (int b = lane; b < kBins; b += 32) {
+      const float cv = cov_j[32 * b];
+      if (cv > 0.0f) {
+        const int col = b % kGrid, row = b / kGrid;
+        const float e01 = edge[row * 8 + col];                 // d0 -> d1
+        const float e12 = edge[72 + row * 9 + col + 1];        // d1 -> d2
+        const float e23 = -edge[(row + 1) * 8 + col];          // d2 -> d3
+        const float e30 = -edge[72 + row * 9 + col];           // d3 -> d0
+        sum += cv * fabsf(0.5f * (e01 + e12 + e23 + e30));
+      }
+    }
+    __syncwarp();
+  } else {
+    for (int b = lane; b < kBins; b += 32) {
+      const float cv = cov_j[32 * b];
+      if (cv > 0.0f) sum += cv * clipped_bin_weight(c, n, b);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  return sum;
+}
+
 template <bool kCount>
 // Three blocks per SM fit the shared memory (3 x 64 KB); saying so lets the
 // register allocator use up to 170 registers a thread instead of spilling.
@@ -249,13 +335,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  float* cov_base = smem + (size_t)wib * (2 * kBins * 32);
+  float* cov_base = smem + (size_t)wib * kWarpFloats;
   float* acc_base = cov_base + kBins * 32;
+  float* scratch = acc_base + kBins * 32;
   for (int k = 0; k < kBins; ++k) acc_base[32 * k + lane] = 0.0f;
 
   const uint64_t ncones = list ? (uint64_t)min(*list_count, o.redo_capacity) : q.npoints * (uint64_t)q.nlights;
-  const uint64_t warps = (uint64_t)gridDim.x * kWarpsPerBlock;
-  for (uint64_t wbase = ((uint64_t)blockIdx.x * kWarpsPerBlock + wib) * pw; wbase < ncones; wbase += warps * pw) {
+  const uint64_t npackets = (ncones + pw - 1) / pw;
+  // Packets are taken from a shared counter as warps finish: their costs
+  // differ by two orders of magnitude, so a fixed assignment leaves most
+  // warps idle behind the slowest.
+  uint32_t* next = list ? o.next_solo : o.next_packet;
+  for (;;) {
+    uint32_t packet = 0;
+    if (lane == 0) packet = atomicAdd(next, 1u);
+    packet = __shfl_sync(0xffffffffu, packet, 0);
+    if (packet >= npackets) break;
+    const uint64_t wbase = (uint64_t)packet * pw;
     const uint64_t slot = wbase + lane;
     const bool valid = (uint32_t)lane < pw && slot < ncones;
     uint64_t c = 0;
@@ -320,6 +416,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const bool last_empty = (aw0 | aw1) == 0u;
     const bool last_full = (fw0 & fw1) == 0xffffffffu;
 
+    // Rect light cones with coverage: the bins' Lambert weights, one cone at
+    // a time across the warp.
+    const bool rect_traced = traced && !is_sphere(L);
+    bool all_above = true;
+    float total = 0.0f;
+    if (rect_traced) total = window_weight(st.cone, normal, &all_above);
+    float blocked = 0.0f;
+    uint32_t todo = __ballot_sync(0xffffffffu, rect_traced && !last_empty);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const float b = warp_blocked(st.cone, normal, all_above, cov_base + j, scratch, j, lane);
+      if (lane == j) blocked = b;
+    }
     float value = 0.0f;
     if (traced) {
       const Cone& cn = st.cone;
@@ -340,13 +450,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
         value = sphere_unshadowed(point, normal, L) * share;
       } else {
         // cone_visible (:1244-1272) and wide_visible (:1070-1073)
-        bool all_above;
-        const float total = window_weight(cn, normal, &all_above);
-        float blocked = 0.0f;
-        for (int b = 0; b < kBins; ++b) {
-          const float cv = st.cov[32 * b];
-          if (cv > 0.0f) blocked += cv * (all_above ? bin_weight(cn, normal, b) : clipped_bin_weight(cn, normal, b));
-        }
         float visible = fmaxf(total - blocked, 0.0f);
         if (info.wide_clipped) visible = (total > 1e-9f ? visible / total : 1.0f) * rect_open(point, normal, L);
         value = visible;
@@ -397,7 +500,7 @@ static uint64_t g_attr_set[2] = {0, 0};
 template <bool kCount>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const uint32_t* list,
                               const uint32_t* list_count, uint32_t pw, uint32_t blocks, cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * 2 * kBins * 32 * sizeof(float);
+  const size_t smem = (size_t)kWarpsPerBlock * kWarpFloats * sizeof(float);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
@@ -427,7 +530,8 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   // Enough blocks to fill every SM several times over; each warp then strides
   // over packets.
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  const uint64_t cap = (uint64_t)sm_count * 24;
+  // One resident wave: warps take packets from the shared counter.
+  const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
   cudaError_t e = count ? launch_one<true>(s, q, o, nullptr, nullptr, pw, blocks, stream)
                         : launch_one<false>(s, q, o, nullptr, nullptr, pw, blocks, stream);
@@ -435,7 +539,7 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   if (e != cudaSuccess) return e;
   if (o.redo_list) {
     // The listed cones, each walked alone (one lane per warp).
-    const uint32_t solo_blocks = (uint32_t)sm_count * 4;
+    const uint32_t solo_blocks = (uint32_t)sm_count * kBlocksPerSm;
     e = count ? launch_one<true>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream)
               : launch_one<false>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream);
   }

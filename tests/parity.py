@@ -6,12 +6,13 @@ The bar (stated once, used by every parity test):
     a FULL disagreement has coverage within 2e-5 of whole on both sides, an
     ANY disagreement coverage below 2e-5 on both sides (a sliver that thin);
   * visible fractions agree within 1e-3 absolute;
-  * irradiance agrees within 1e-3 of the cone's unshadowed light where that
-    is positive. (The reference's own GPU-vs-CPU bound, 1e-4 of the light's
-    weight, gpu.rs:330-336, holds on the reference's test scenes and is
-    checked there; on the seeded workloads the FP32 integration alone differs
-    from FP64 by up to 2.3e-4 of the unshadowed light, so two FP32
-    implementations cannot be held to 1e-4 there.)
+  * irradiance agrees within 2e-3 of the cone's unshadowed light, floored
+    at 1e-3 of the brightest cone's: near a light's horizon, or at a spot's
+    edge, the unshadowed light tends to zero and f32 loses it (on these
+    cases the oracle's own FP32 run differs from its FP64 run by up to
+    7.3e-4 of that scale, and by up to 6x of the raw unshadowed value). The
+    reference's own GPU-vs-CPU bound, 1e-4 of the light's weight
+    (gpu.rs:330-336), is checked on the reference's test scenes.
 """
 from __future__ import annotations
 
@@ -19,7 +20,8 @@ import numpy as np
 
 WORD_AGREEMENT = 0.999
 FRACTION_TOL = 1e-3
-IRRADIANCE_TOL = 1e-3
+IRRADIANCE_TOL = 2e-3
+IRRADIANCE_FLOOR = 1e-3
 EDGE_SLACK = 2e-5
 
 
@@ -45,7 +47,11 @@ def compare(gpu: dict, orc: dict, unshadowed: np.ndarray | None = None, check: b
         u = np.asarray(unshadowed).reshape(-1)
         di = np.abs(np.asarray(gpu["irradiance"]).reshape(-1) - np.asarray(orc["irradiance"]).reshape(-1))
         m = u > 0
-        stats["max_irradiance_diff_rel"] = float((di[m] / u[m]).max()) if m.any() else 0.0
+        if m.any():
+            scale = np.maximum(u[m], IRRADIANCE_FLOOR * u[m].max())
+            stats["max_irradiance_diff_rel"] = float((di[m] / scale).max())
+        else:
+            stats["max_irradiance_diff_rel"] = 0.0
     # Trace every disagreeing bit through the coverages on both sides.
     untraced = 0
     bad = np.nonzero(~agree)[0]

@@ -94,6 +94,18 @@ def test_packets_equal_solo_walks(kernel):
             assert np.array_equal(r[k], runs[0][k]), k
 
 
+def test_walk_order_changes_no_result(kernel):
+    """Walking points in Morton order (the default) or in the given order
+    (CC_KEEP_ORDER) gives identical results."""
+    w = small_field(seed=11, n=8, sub=3, width=96, height=54)
+    scene = kernel.scene(w.meshes)
+    a = parity.flat(kernel.visibility(scene, w.receivers, w.lights, outputs=ALL))
+    b = parity.flat(kernel.visibility(scene, w.receivers, w.lights, outputs=ALL, flags=_lib.CC_KEEP_ORDER))
+    scene.close()
+    for k in ("full", "any", "partial", "irradiance", "fraction"):
+        assert np.array_equal(a[k], b[k]), k
+
+
 def small_field(seed=5, n=12, sub=4, width=160, height=90):
     return scenes.icosphere_field(seed=seed, n_spheres=n, subdivisions=sub, width=width, height=height)
 
