@@ -232,8 +232,8 @@ int validate_flat(const cc::FlatScene& f) {
   }
   for (const auto* nodes : {&f.blas, &f.nodes})
     for (const cc::NodeGpu& n : *nodes)
-      if (n.info[1] > 15 || n.info[0] >= (1u << 28))
-        return fail(CC_ERR_INVALID, "hierarchy leaves hold at most 15 items and indices stay below 2^28");
+      if (n.info[1] > 15 || n.info[0] >= (1u << 26))
+        return fail(CC_ERR_INVALID, "hierarchy leaves hold at most 15 items and indices stay below 2^26");
   for (uint32_t m : f.items)
     if (m >= std::max<uint32_t>(f.nmeshes, 1)) return fail(CC_ERR_INVALID, "object hierarchy item out of range");
   if (f.nodes.empty()) return fail(CC_ERR_INVALID, "empty object hierarchy");
@@ -358,6 +358,10 @@ int cc_scene_build(cc_context* ctx, const float* tri9, const uint32_t* mesh_coun
   cc_scene* s = new cc_scene;
   s->ctx = ctx;
   cc::build_flat_scene(tri9, mesh_counts, nmeshes, s->flat, threads_for_build());
+  if (s->flat.blas.size() >= (1u << 26) || s->flat.nodes.size() >= (1u << 26) || total >= (1u << 26)) {
+    delete s;
+    return fail(CC_ERR_INVALID, "a scene holds fewer than 2^26 triangles and hierarchy nodes");
+  }
   if (!ctx) {  // host-only scene
     *out = s;
     return CC_OK;

@@ -247,14 +247,22 @@ __device__ __forceinline__ bool may_touch(const Cone& c, f3 v0, f3 v1, f3 v2) {
 }
 
 // ---- the accumulation rasterizer ------------------------------------------------
-// The lane's 68-cell accumulator (the WGSL's `acc`, :719-760) in shared
-// memory, cell-major with the lane innermost. Cells 64..65 receive writes
-// "one past the last row" that no resolve ever reads, so they are dropped.
+// A cone's 68-cell accumulator (the WGSL's `acc`, :719-760) in shared
+// memory, cell-major with the cone's lane innermost, in 64-bit fixed point
+// (units of 2^-40 of a bin). Any lane may add to any cone's cells: integer
+// addition is exact and order-free, so the sum — and every result — is the
+// same whichever lanes draw which triangles in whatever order. (The
+// reference sums in f32 in walk order; the exact sum differs from that by
+// f32 rounding only.) Cells 64..65 receive writes "one past the last row"
+// that no resolve ever reads, so they are dropped.
+constexpr float kFixScale = 1099511627776.0f;        // 2^40
+constexpr float kFixUnit = 1.0f / 1099511627776.0f;  // 2^-40
+
 struct LaneAcc {
-  float* base;  // &acc[lane]; cell k at base[32 * k]
-  uint32_t span_lo, span_hi;
+  unsigned long long* base;  // &acc[cone]; cell k at base[32 * k]
+  uint32_t span_lo, span_hi; // rows this triangle wrote (the WGSL's span, :758-760)
   __device__ __forceinline__ void add(uint32_t cell, float v) {
-    if (cell < (uint32_t)kBins) base[32 * cell] += v;
+    if (cell < (uint32_t)kBins) atomicAdd(base + 32 * cell, (unsigned long long)__float2ll_rn(v * kFixScale));
   }
 };
 
@@ -398,14 +406,16 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, LaneAcc& ac
   float2* q = qa;
   float2* q2 = qb;
   int m;
-  if (all_near_ok && all_in_window) {
+  const bool projected = all_near_ok && all_in_window;
+  float side = 1.0f;
+  if (projected) {
     m = n;
     for (int i = 0; i < n; ++i) q[i] = make_float2((p[i].x / p[i].z - c.u0) * su, (p[i].y / p[i].z - c.v0) * sv);
   } else {
     f3 l0 = to_local(c, v0), l1 = to_local(c, v1), l2 = to_local(c, v2);
     float d = dot(l0, cross(l1, l2));
     if (d == 0.0f) return false;
-    float side = d > 0.0f ? 1.0f : -1.0f;
+    side = d > 0.0f ? 1.0f : -1.0f;
     m = 4;
     q[0] = make_float2(0.f, 0.f);
     q[2] = make_float2(g, g);
@@ -416,25 +426,47 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, LaneAcc& ac
       q[1] = make_float2(0.f, g);
       q[3] = make_float2(g, 0.f);
     }
-    for (int i = 0; i < n; ++i) {
-      f3 e = cross(p[i], p[(i + 1) % n]);
-      float l = len(e);
-      if (l == 0.0f) continue;
-      f3 k = e * (side / l);
-      m = clip_line2(q, m, q2, -k.x / su, -k.y / sv, k.x * c.u0 + k.y * c.v0 + k.z);
-      float2* t = q;
-      q = q2;
-      q2 = t;
-    }
   }
-  bool inside = true;
-  for (int i = 0; i < m; ++i)
-    if (q[i].x < 0.f || q[i].y < 0.f || q[i].x > g || q[i].y > g) inside = false;
-  if (!inside) {
-    m = clip_line2(q, m, q2, -1.f, 0.f, 0.f);
-    m = clip_line2(q2, m, q, 1.f, 0.f, g);
-    m = clip_line2(q, m, q2, 0.f, -1.f, 0.f);
-    m = clip_line2(q2, m, q, 0.f, 1.f, g);
+  // Every 2D clip from one call site: first the planes through the apex and
+  // each edge (the apex-plane case), then, if some vertex lies outside the
+  // grid, the square's four sides — the reference's sequence of clips.
+  int stage = projected ? 1 : 0;  // 0: edge planes, 1: the inside check, 2: the square's sides
+  int i = 0;
+#pragma unroll 1
+  for (;;) {
+    float nx, ny, off;
+    if (stage == 0) {
+      if (i == n) {
+        stage = 1;
+        continue;
+      }
+      const f3 e = cross(p[i], p[(i + 1) % n]);
+      ++i;
+      const float l = len(e);
+      if (l == 0.0f) continue;
+      const f3 k = e * (side / l);
+      nx = -k.x / su;
+      ny = -k.y / sv;
+      off = k.x * c.u0 + k.y * c.v0 + k.z;
+    } else if (stage == 1) {
+      bool inside = true;
+      for (int j = 0; j < m; ++j)
+        if (q[j].x < 0.f || q[j].y < 0.f || q[j].x > g || q[j].y > g) inside = false;
+      if (inside) break;
+      stage = 2;
+      i = 0;
+      continue;
+    } else {
+      if (i == 4) break;
+      nx = i == 0 ? -1.f : (i == 1 ? 1.f : 0.f);
+      ny = i == 2 ? -1.f : (i == 3 ? 1.f : 0.f);
+      off = (i & 1) ? g : 0.f;
+      ++i;
+    }
+    m = clip_line2(q, m, q2, nx, ny, off);
+    float2* t = q;
+    q = q2;
+    q2 = t;
   }
   if (m < 3) return false;
   draw_polygon(acc, q, m);
@@ -464,9 +496,14 @@ __device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3
       bool inside = ax >= 0.f && ay >= 0.f && ax <= g && ay <= g && bx >= 0.f && by >= 0.f && bx <= g &&
                     by <= g && cx >= 0.f && cy >= 0.f && cx <= g && cy <= g;
       if (inside) {
-        draw_edge(acc, ax, ay, bx, by, 1.0f);
-        draw_edge(acc, bx, by, cx, cy, 1.0f);
-        draw_edge(acc, cx, cy, ax, ay, 1.0f);
+        // The three edges from one call site (a rolled loop keeps the hot
+        // code small enough for the instruction caches).
+#pragma unroll 1
+        for (int e = 0; e < 3; ++e) {
+          const float sx = e == 0 ? ax : (e == 1 ? bx : cx), sy = e == 0 ? ay : (e == 1 ? by : cy);
+          const float tx = e == 0 ? bx : (e == 1 ? cx : ax), ty = e == 0 ? by : (e == 1 ? cy : ay);
+          draw_edge(acc, sx, sy, tx, ty, 1.0f);
+        }
         return true;
       }
     }

@@ -7,8 +7,8 @@
 
 namespace cc {
 
-constexpr int kWarpsPerBlock = 4;
-constexpr int kBlocksPerSm = 3;  // resident blocks per SM the shared memory allows
+constexpr int kWarpsPerBlock = 2;
+constexpr int kBlocksPerSm = 4;  // resident blocks per SM the shared memory allows (4 x 54 KB)
 
 struct DevQuery {
   const float4* receivers;  // 2 per point: point, normal

@@ -1,10 +1,11 @@
 // The plain visibility kernel: one warp walks a packet of up to 32 cones
 // (neighbouring points toward one light) through the scene hierarchy
-// together; each lane tests, rasterizes and integrates its own cone.
+// together; the lanes share the rasterization of every leaf the packet
+// visits, and each lane integrates its own cone.
 //
 // What the reference does per invocation (mask_cones.wgsl `main` :1513-1520
 // -> hit_irradiance_rect :2125 -> cone_irradiance_rect :1286) is done here
-// per lane, with the packet walk of the reference's PACKETS mode
+// per cone, with the packet walk of the reference's PACKETS mode
 // (packet_any, :666-711) built from warp votes:
 //  * the traversal stack is warp-uniform and lives in registers spread over
 //    the lanes (entry i in lane i % 32), so a push is one predicated move and
@@ -12,7 +13,11 @@
 //  * each lane keeps a bit per stack entry saying whether its own walk needs
 //    that entry (need_get/need_put, :694-711);
 //  * node and triangle records are loaded by every lane from the same
-//    address, which the load unit serves as one broadcast transaction.
+//    address, which the load unit serves as one broadcast transaction;
+//  * at a triangle-hierarchy leaf, the (triangle, cone) pairs of every cone
+//    that descends into it are dealt out over all 32 lanes, which cull and
+//    rasterize them into the owning cone's accumulator — cones whose
+//    triangles take the long clip path no longer hold 31 lanes idle.
 // Results depend on the walk order only through the walk caps: the packet
 // takes its child order from its first lane that descends; a lane whose own
 // nearest-first order differs somewhere on its walk, and whose walk then
@@ -30,23 +35,36 @@ namespace cc {
 __constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded by the host
 
 constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
-// Shared memory per warp: the lanes' coverages (64 x 32), accumulators
-// (64 x 32) and the cooperative integration's corners and edges (387).
-constexpr int kScratchFloats = 416;
-constexpr int kWarpFloats = 2 * kBins * 32 + kScratchFloats;
+constexpr int kConeFields = 17;    // apex, right, up, forward, window, far offset
 
-// A stack entry is a node reference packed in one word: the node's item
-// count in the top 4 bits (0: interior) and its first item (leaf) or left
-// child (interior) below. Each lane keeps two bits per entry: whether its
-// own walk needs the entry, and whether its cone passed the entry's box
-// test, which is done when the parent is visited (the two children of a
-// node are adjacent, so one 64-byte load serves both tests and the
-// nearest-first choice).
-constexpr uint32_t kRefIndexBits = 28;
+// Shared memory of one warp.
+struct WarpShared {
+  float cov[kBins * 32];                // each cone's 64 coverages, bin-major, lane innermost
+  unsigned long long acc[kBins * 32];   // each cone's accumulator (64-bit fixed point)
+  float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
+  uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
+};
+static_assert(sizeof(WarpShared) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
+
+// A stack entry packed in one word: its kind in the top 2 bits (an
+// object-hierarchy node, a triangle-hierarchy node, or a mesh's resolve
+// marker), then a node's item count in 4 bits (0: interior), then its first
+// item (leaf) or left child (interior) in 26 bits. Each lane keeps two bits
+// per entry: whether its own walk needs the entry, and whether its cone
+// passed the entry's box test, which is done when the parent is visited (the
+// two children of a node are adjacent, so one 64-byte load serves both
+// tests and the nearest-first choice).
+constexpr uint32_t kRefIndexBits = 26;
 constexpr uint32_t kRefIndexMask = (1u << kRefIndexBits) - 1u;
-__device__ __forceinline__ uint32_t node_ref(float4 a, float4 b) {
-  return (__float_as_uint(b.w) << kRefIndexBits) | (__float_as_uint(a.w) & kRefIndexMask);
+constexpr uint32_t kRefKindShift = 30;
+__device__ __forceinline__ uint32_t node_ref(float4 a, float4 b, uint32_t kind) {
+  return (kind << kRefKindShift) | ((__float_as_uint(b.w) & 15u) << kRefIndexBits) |
+         (__float_as_uint(a.w) & kRefIndexMask);
 }
+__device__ __forceinline__ uint32_t ref_kind(uint32_t r) { return r >> kRefKindShift; }
+__device__ __forceinline__ uint32_t ref_count(uint32_t r) { return (r >> kRefIndexBits) & 15u; }
+__device__ __forceinline__ uint32_t ref_index(uint32_t r) { return r & kRefIndexMask; }
 
 struct WarpStack {
   uint32_t r0 = 0, r1 = 0;  // entry i held by lane i % 32, register i / 32
@@ -78,9 +96,8 @@ struct WarpStack {
 
 struct LaneState {
   Cone cone;
-  f3 d00, d10, d01, d11;  // window corner directions
-  float* cov;             // &cov[lane]; bin b at cov[32 * b]
-  float* acc;             // &acc[lane]
+  WarpShared* ws;
+  float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
   uint32_t full;
   uint32_t cone_work;
   uint32_t cap;
@@ -90,165 +107,219 @@ struct LaneState {
 
 __device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
 
-// The cheap tests of cover_triangle (:594-612): faces the apex, some window
-// direction enters its plane, may touch the cone.
-__device__ __forceinline__ bool cull_triangle(const LaneState& st, f3 v0, f3 v1, f3 v2) {
-  const Cone& c = st.cone;
-  f3 n = cross(v1 - v0, v2 - v0);
-  if (dot(n, c.apex - v0) <= 0.0f) return false;  // faces away (:600)
-  if (dot(n, st.d00) >= 0.f && dot(n, st.d10) >= 0.f && dot(n, st.d01) >= 0.f && dot(n, st.d11) >= 0.f)
-    return false;  // every window direction leaves its plane (:601-606)
-  return may_touch(c, v0, v1, v2);
+__device__ __forceinline__ void store_cone(WarpShared* ws, const Cone& c, int lane) {
+  float* t = ws->cone + lane;
+  const float f[kConeFields] = {c.apex.x, c.apex.y, c.apex.z, c.right.x, c.right.y, c.right.z, c.up.x, c.up.y,
+                                c.up.z,   c.fwd.x,  c.fwd.y,  c.fwd.z,   c.u0,      c.v0,      c.u1,   c.v1,
+                                c.far_offset};
+#pragma unroll
+  for (int k = 0; k < kConeFields; ++k) t[32 * k] = f[k];
 }
 
-// cover_triangle (:594-616): triangle slot t rasterized into `acc` if it
-// faces the apex and may touch the cone.
-template <bool kCount>
-__device__ __forceinline__ bool cover_triangle(const DevScene& s, LaneState& st, LaneAcc& acc, uint32_t t) {
-  if (kCount) st.n_tris++;
-  f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
-  f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
-  f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
-  if (!cull_triangle(st, v0, v1, v2)) return false;
-  return rasterize(st.cone, acc, v0, v1, v2);
+__device__ __forceinline__ Cone load_cone(const WarpShared* ws, int owner) {
+  const float* t = ws->cone + owner;
+  Cone c;
+  c.apex = mk(t[0], t[32], t[64]);
+  c.right = mk(t[96], t[128], t[160]);
+  c.up = mk(t[192], t[224], t[256]);
+  c.fwd = mk(t[288], t[320], t[352]);
+  c.u0 = t[384];
+  c.v0 = t[416];
+  c.u1 = t[448];
+  c.v1 = t[480];
+  c.far_offset = t[512];
+  c.baxis = mk(0.f, 0.f, 0.f);
+  c.bcos = c.bsin = 0.f;
+  return c;
 }
 
-// add_mesh_coverage_if (:713-829) for the lanes with `on`; the others
-// follow the packet's walk. The triangle hierarchy's stack entries start at
-// `base`, above the object walk's. A node still counts toward the walk cap
-// when it is popped, as in the reference, though its box was tested when its
-// parent was visited. Triangles are stored in leaf order, so a leaf's items
-// are the triangle slots themselves.
+// cover_triangle (:594-616) for one (triangle, cone) pair: back face, the
+// window-direction test, may_touch, then rasterization into the cone's
+// accumulator.
+__device__ __forceinline__ void cover_pair(const DevScene& s, WarpShared* ws, int owner, uint32_t t) {
+  const Cone c = load_cone(ws, owner);
+  const f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
+  const f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
+  const f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
+  const f3 n = cross(v1 - v0, v2 - v0);
+  if (dot(n, c.apex - v0) <= 0.0f) return;  // faces away (:600)
+  if (dot(n, direction(c, 0.f, 0.f)) >= 0.f && dot(n, direction(c, 1.f, 0.f)) >= 0.f &&
+      dot(n, direction(c, 0.f, 1.f)) >= 0.f && dot(n, direction(c, 1.f, 1.f)) >= 0.f)
+    return;  // every window direction leaves its plane (:601-606)
+  if (!may_touch(c, v0, v1, v2)) return;
+  LaneAcc acc{ws->acc + owner, 68u, 0u};
+  rasterize(c, acc, v0, v1, v2);
+  if (acc.span_lo < acc.span_hi) {
+    atomicMin(&ws->span_lo[owner], acc.span_lo);
+    atomicMax(&ws->span_hi[owner], acc.span_hi);
+  }
+}
+
+// Triangles t0 .. t0+nt, each to be tested against the cones of the lanes
+// in `owners`: the pairs, triangle-major (consecutive lanes read the same
+// triangle), dealt out over the warp.
+__device__ __noinline__ void cover_leaf(const DevScene& s, WarpShared* ws, uint32_t owners, uint32_t t0,
+                                           uint32_t nt, int lane) {
+  const uint32_t n_owners = __popc(owners);
+  const uint32_t n_pairs = n_owners * nt;
+  for (uint32_t base = 0; base < n_pairs; base += 32) {
+    const uint32_t pair = base + lane;
+    if (pair < n_pairs) {
+      const uint32_t k = pair / n_owners;
+      const uint32_t r = pair - k * n_owners;
+      cover_pair(s, ws, __fns(owners, 0, r + 1), t0 + k);
+    }
+  }
+  __syncwarp();
+}
+
+// The mesh's coverage for the lane's own cone: running sum over the touched
+// cells (exact), snapped to whole within 1e-5, combined into the cone's bins
+// by max (:809-828); then the cells are cleared for the next mesh.
+__device__ __forceinline__ void resolve_mesh(LaneState& st, int lane) {
+  WarpShared* ws = st.ws;
+  const uint32_t lo = ws->span_lo[lane];
+  const uint32_t end = min(ws->span_hi[lane], (uint32_t)kBins);
+  long long running = 0;
+  for (uint32_t b = lo; b < end; ++b) {
+    unsigned long long* cell = &ws->acc[32 * b + lane];
+    running += (long long)*cell;
+    *cell = 0ull;
+    float covered = fabsf(__ll2float_rn(running) * kFixUnit);
+    if (covered >= 1.0f - 1e-5f) covered = 1.0f;
+    if (covered > 1e-6f) {
+      const float before = st.cov[32 * b];
+      const float after = fmaxf(before, fminf(covered, 1.0f));
+      st.cov[32 * b] = after;
+      if (before < 1.0f && after >= 1.0f) st.full++;
+    }
+  }
+  ws->span_lo[lane] = 68u;
+  ws->span_hi[lane] = 0u;
+  __syncwarp();
+}
+
+// Stack entry kinds for the walk of both hierarchy levels in one loop.
+constexpr uint32_t kObjNode = 0;   // an object-hierarchy node
+constexpr uint32_t kTriNode = 1;   // a node of the current mesh's triangle hierarchy
+constexpr uint32_t kResolve = 2;   // the current mesh is done: resolve its coverage
+
+// add_mesh_coverage_if (:713-829) for hierarchy levels 0 and 1: every
+// triangle of mesh m for the lanes with `on`, in leaf-sized groups, then the
+// mesh's resolve.
 template <bool kCount>
-__device__ __forceinline__ void add_mesh(const DevScene& s, uint32_t hierarchy, LaneState& st, WarpStack& stk,
-                                         bool on, uint32_t m, int base, int lane) {
-  if (!__any_sync(0xffffffffu, on)) return;
+__device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState& st, bool on, uint32_t m, int lane) {
+  const uint32_t owners = __ballot_sync(0xffffffffu, on);
+  if (!owners) return;
   const uint4 range = __ldg(&s.meshes[m]);
-  LaneAcc acc{st.acc, 68u, 0u};
-  bool touched = false;
-  if (hierarchy == 2) {
-    if (range.z != kNoneU) {
-      const float4 ra = __ldg(&s.blas[2 * (size_t)range.z + 0]);
-      const float4 rb = __ldg(&s.blas[2 * (size_t)range.z + 1]);
-      const bool root_pass = on && may_touch_box(st.cone, node_lo(ra), node_lo(rb));
-      int sp = base;
-      stk.push(sp, node_ref(ra, rb), on, root_pass, lane);
-      ++sp;
-      while (sp > base) {
-        --sp;
-        const uint32_t ref = stk.get(sp);
-        const bool mine = stk.need(sp) && st.cone_work < st.cap;
-        if (mine) st.cone_work++;
-        if (kCount && mine) st.n_blas++;
-        const bool descend = mine && stk.pass(sp);
-        if (!__any_sync(0xffffffffu, descend)) continue;
-        const uint32_t ia = ref & kRefIndexMask, ib = ref >> kRefIndexBits;
-        if (ib > 0) {
-          if (descend) {
-            st.cone_work += ib;
-            for (uint32_t k = ia; k < ia + ib; ++k)
-              if (cover_triangle<kCount>(s, st, acc, k)) touched = true;
-          }
-        } else {
-          const float4 la = __ldg(&s.blas[2 * (size_t)ia + 0]);
-          const float4 lb = __ldg(&s.blas[2 * (size_t)ia + 1]);
-          const float4 xa = __ldg(&s.blas[2 * (size_t)ia + 2]);
-          const float4 xb = __ldg(&s.blas[2 * (size_t)ia + 3]);
-          bool pl = false, pr = false;
-          if (descend) {
-            pl = may_touch_box(st.cone, node_lo(la), node_lo(lb));
-            pr = may_touch_box(st.cone, node_lo(xa), node_lo(xb));
-          }
-          if (sp + 2 > kStack) {
-            if (descend) st.status |= 2u;
-            continue;
-          }
-          // Right child popped first (:783-787).
-          stk.push(sp, node_ref(la, lb), descend, pl, lane);
-          stk.push(sp + 1, node_ref(xa, xb), descend, pr, lane);
-          sp += 2;
-        }
-      }
-    }
-  } else if (on) {
-    for (uint32_t t = range.x; t < range.x + range.y; ++t)
-      if (cover_triangle<kCount>(s, st, acc, t)) touched = true;
-  }
-  // The mesh's coverage: running sum over the touched cells, snapped to
-  // whole within 1e-5, combined into the cone's bins by max (:809-828).
-  const uint32_t end = min(acc.span_hi, (uint32_t)kBins);
-  if (touched) {
-    float running = 0.0f;
-    for (uint32_t b = acc.span_lo; b < end; ++b) {
-      running += st.acc[32 * b];
-      float covered = fabsf(running);
-      if (covered >= 1.0f - 1e-5f) covered = 1.0f;
-      if (covered > 1e-6f) {
-        const float before = st.cov[32 * b];
-        const float after = fmaxf(before, fminf(covered, 1.0f));
-        st.cov[32 * b] = after;
-        if (before < 1.0f && after >= 1.0f) st.full++;
-      }
-    }
-  }
-  for (uint32_t b = acc.span_lo; b < end; ++b) st.acc[32 * b] = 0.0f;
+  if (kCount && on) st.n_tris += range.y;
+  for (uint32_t t = range.x; t < range.x + range.y; t += 8)
+    cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), lane);
+  resolve_mesh(st, lane);
 }
 
-// scene_coverage_if (:1160-1227): the object hierarchy, nearest child first
-// along the bounding cone's axis, until every bin is full or the cap.
+// The cone walk (scene_coverage_if, :1160-1227, with add_mesh_coverage_if,
+// :713-829, for each mesh it reaches). Hierarchy level 2 walks both levels in
+// one loop: an object leaf that a lane descends into pushes, for each of its
+// meshes (first mesh on top), a resolve marker under the mesh's triangle
+// hierarchy root, so each mesh is walked and then resolved in the reference's
+// order. Object nodes are visited nearest child first along the bounding
+// cone's axis while some bin is open; triangle-hierarchy nodes right child
+// first (:783-787) with no full check, as in the reference; every popped node
+// a lane needs counts toward its walk cap, though its box was tested when its
+// parent was visited. Levels 0 and 1 keep the reference's loops over meshes
+// and triangles.
 template <bool kCount>
 __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState& st, bool traced,
                                            int lane) {
+  const Cone& c = st.cone;
+  if (hierarchy == 0) {
+    for (uint32_t m = 0; m < s.nmeshes; ++m) add_mesh_flat<kCount>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
+    return;
+  }
   WarpStack stk;
-  if (hierarchy >= 1) {
-    const float4 ra = __ldg(&s.nodes[0]);
-    const float4 rb = __ldg(&s.nodes[1]);
-    const bool root_pass = traced && may_touch_box(st.cone, node_lo(ra), node_lo(rb));
-    stk.push(0, node_ref(ra, rb), traced, root_pass, lane);
-    int sp = 1;
-    while (sp > 0) {
-      --sp;
-      const uint32_t ref = stk.get(sp);
-      const bool mine = stk.need(sp) && st.full < (uint32_t)kBins && st.cone_work < st.cap;
-      if (mine) st.cone_work++;
-      if (kCount && mine) st.n_obj++;
-      const bool descend = mine && stk.pass(sp);
-      if (!__any_sync(0xffffffffu, descend)) continue;
-      const uint32_t ia = ref & kRefIndexMask, ib = ref >> kRefIndexBits;
-      if (ib > 0) {
-        for (uint32_t k = ia; k < ia + ib; ++k)
-          add_mesh<kCount>(s, hierarchy, st, stk, descend, __ldg(&s.items[k]), sp, lane);
-      } else {
-        const float4 la = __ldg(&s.nodes[2 * (size_t)ia + 0]);
-        const float4 lb = __ldg(&s.nodes[2 * (size_t)ia + 1]);
-        const float4 xa = __ldg(&s.nodes[2 * (size_t)ia + 2]);
-        const float4 xb = __ldg(&s.nodes[2 * (size_t)ia + 3]);
-        const Cone& c = st.cone;
-        bool pl = false, pr = false;
-        if (descend) {
-          pl = may_touch_box(c, node_lo(la), node_lo(lb));
-          pr = may_touch_box(c, node_lo(xa), node_lo(xb));
-        }
-        const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
-        const float db = dot(c.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - c.apex);
-        const bool pref = db < da;  // this lane's own order: right child nearer
-        const uint32_t voters = __ballot_sync(0xffffffffu, descend);
-        const bool swap = __shfl_sync(0xffffffffu, pref, __ffs(voters) - 1);
-        if (descend && pref != swap) st.status |= 4u;
+  const float4 ra = __ldg(&s.nodes[0]);
+  const float4 rb = __ldg(&s.nodes[1]);
+  const bool root_pass = traced && may_touch_box(c, node_lo(ra), node_lo(rb));
+  stk.push(0, node_ref(ra, rb, kObjNode), traced, root_pass, lane);
+  int sp = 1;
+  while (sp > 0) {
+    --sp;
+    const uint32_t ref = stk.get(sp);
+    const uint32_t kind = ref_kind(ref);
+    if (kind == kResolve) {
+      resolve_mesh(st, lane);
+      continue;
+    }
+    const bool is_obj = kind == kObjNode;
+    const bool mine = stk.need(sp) && st.cone_work < st.cap && (!is_obj || st.full < (uint32_t)kBins);
+    if (mine) st.cone_work++;
+    if (kCount && mine) {
+      if (is_obj) st.n_obj++; else st.n_blas++;
+    }
+    const bool descend = mine && stk.pass(sp);
+    const uint32_t owners = __ballot_sync(0xffffffffu, descend);
+    if (!owners) continue;
+    const uint32_t ia = ref_index(ref), ib = ref_count(ref);
+    if (ib > 0 && !is_obj) {
+      // A triangle-hierarchy leaf: its triangles against every descending cone.
+      if (descend) {
+        st.cone_work += ib;
+        if (kCount) st.n_tris += ib;
+      }
+      cover_leaf(s, st.ws, owners, ia, ib, lane);
+    } else if (ib > 0) {
+      // An object leaf: its meshes.
+      if (hierarchy == 1) {
+        for (uint32_t k = ia; k < ia + ib; ++k) add_mesh_flat<kCount>(s, st, descend, __ldg(&s.items[k]), lane);
+        continue;
+      }
+      for (int k = (int)(ia + ib) - 1; k >= (int)ia; --k) {
+        const uint4 range = __ldg(&s.meshes[__ldg(&s.items[k])]);
+        if (range.z == kNoneU) continue;  // no triangles: nothing to draw or resolve
         if (sp + 2 > kStack) {
           if (descend) st.status |= 2u;
           continue;
         }
-        const uint32_t rl = node_ref(la, lb), rr = node_ref(xa, xb);
-        // The far child below the near one: the near child is popped first.
-        stk.push(sp, swap ? rl : rr, descend, swap ? pl : pr, lane);
-        stk.push(sp + 1, swap ? rr : rl, descend, swap ? pr : pl, lane);
+        const float4 ma = __ldg(&s.blas[2 * (size_t)range.z + 0]);
+        const float4 mb = __ldg(&s.blas[2 * (size_t)range.z + 1]);
+        const bool mesh_pass = descend && may_touch_box(c, node_lo(ma), node_lo(mb));
+        stk.push(sp, kResolve << kRefKindShift, false, false, lane);
+        stk.push(sp + 1, node_ref(ma, mb, kTriNode), descend, mesh_pass, lane);
         sp += 2;
       }
+    } else {
+      // An interior node: both children's boxes tested now.
+      const float4* base = (is_obj ? s.nodes : s.blas) + 2 * (size_t)ia;
+      const float4 la = __ldg(base + 0), lb = __ldg(base + 1), xa = __ldg(base + 2), xb = __ldg(base + 3);
+      bool pl = false, pr = false;
+      if (descend) {
+#pragma unroll 1
+        for (int ch = 0; ch < 2; ++ch) {
+          const bool t = may_touch_box(c, node_lo(ch ? xa : la), node_lo(ch ? xb : lb));
+          if (ch) pr = t; else pl = t;
+        }
+      }
+      bool swap = false;  // left child popped first (object level: when it is the nearer)
+      if (is_obj) {
+        const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
+        const float db = dot(c.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - c.apex);
+        const bool pref = db < da;  // this lane's own order: right child nearer
+        swap = __shfl_sync(0xffffffffu, pref, __ffs(owners) - 1);
+        if (descend && pref != swap) st.status |= 4u;
+      } else {
+        swap = true;  // triangle hierarchies pop the right child first (:783-787)
+      }
+      if (sp + 2 > kStack) {
+        if (descend) st.status |= 2u;
+        continue;
+      }
+      const uint32_t rl = node_ref(la, lb, kind), rr = node_ref(xa, xb, kind);
+      // The child popped second below the one popped first.
+      stk.push(sp, swap ? rl : rr, descend, swap ? pl : pr, lane);
+      stk.push(sp + 1, swap ? rr : rl, descend, swap ? pr : pl, lane);
+      sp += 2;
     }
-  } else {
-    for (uint32_t m = 0; m < s.nmeshes; ++m)
-      add_mesh<kCount>(s, hierarchy, st, stk, traced && st.full < (uint32_t)kBins, m, 0, lane);
   }
 }
 
@@ -327,18 +398,18 @@ __device__ __noinline__ float warp_blocked(const Cone& mine, f3 my_normal, bool 
 }
 
 template <bool kCount>
-// Three blocks per SM fit the shared memory (3 x 64 KB); saying so lets the
-// register allocator use up to 170 registers a thread instead of spilling.
+// kBlocksPerSm blocks fit the shared memory; saying so bounds the registers
+// per thread the allocator may use without lowering occupancy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     visibility_kernel(DevScene s, DevQuery q, DevOut o, const uint32_t* __restrict__ list,
                       const uint32_t* __restrict__ list_count, uint32_t pw) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  float* cov_base = smem + (size_t)wib * kWarpFloats;
-  float* acc_base = cov_base + kBins * 32;
-  float* scratch = acc_base + kBins * 32;
-  for (int k = 0; k < kBins; ++k) acc_base[32 * k + lane] = 0.0f;
+  WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw) + wib;
+  for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0ull;
+  ws->span_lo[lane] = 68u;
+  ws->span_hi[lane] = 0u;
 
   const uint64_t ncones = list ? (uint64_t)min(*list_count, o.redo_capacity) : q.npoints * (uint64_t)q.nlights;
   const uint64_t npackets = (ncones + pw - 1) / pw;
@@ -369,8 +440,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const uint64_t p = c - (uint64_t)l * q.npoints;
 
     LaneState st;
-    st.cov = cov_base + lane;
-    st.acc = acc_base + lane;
+    st.ws = ws;
+    st.cov = ws->cov + lane;
     st.full = 0;
     st.cone_work = 0;
     st.status = 0;
@@ -390,10 +461,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const LightConeInfo info = light_cone(point, L, q.wide_extent, st.cone);
     const bool traced = on && info.ok;
     st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
-    st.d00 = direction(st.cone, 0.f, 0.f);
-    st.d10 = direction(st.cone, 1.f, 0.f);
-    st.d01 = direction(st.cone, 0.f, 1.f);
-    st.d11 = direction(st.cone, 1.f, 1.f);
+    store_cone(ws, st.cone, lane);
+    __syncwarp();
 
     scene_walk<kCount>(s, q.hierarchy, st, traced, lane);
 
@@ -417,7 +486,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const bool last_full = (fw0 & fw1) == 0xffffffffu;
 
     // Rect light cones with coverage: the bins' Lambert weights, one cone at
-    // a time across the warp.
+    // a time across the warp (the cone table is free now: it is the scratch).
     const bool rect_traced = traced && !is_sphere(L);
     bool all_above = true;
     float total = 0.0f;
@@ -427,7 +496,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     while (todo) {
       const int j = __ffs(todo) - 1;
       todo &= todo - 1;
-      const float b = warp_blocked(st.cone, normal, all_above, cov_base + j, scratch, j, lane);
+      const float b = warp_blocked(st.cone, normal, all_above, ws->cov + j, ws->cone, j, lane);
       if (lane == j) blocked = b;
     }
     float value = 0.0f;
@@ -484,6 +553,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
                                st.cov[32 * (4 * k + 3)]);
       }
     }
+    __syncwarp();
   }
 }
 
@@ -500,7 +570,7 @@ static uint64_t g_attr_set[2] = {0, 0};
 template <bool kCount>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const uint32_t* list,
                               const uint32_t* list_count, uint32_t pw, uint32_t blocks, cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * kWarpFloats * sizeof(float);
+  const size_t smem = (size_t)kWarpsPerBlock * sizeof(WarpShared);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
@@ -527,8 +597,6 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
     return cudaSuccess;
   }
   const uint64_t packets = (ncones + pw - 1) / pw;
-  // Enough blocks to fill every SM several times over; each warp then strides
-  // over packets.
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
   // One resident wave: warps take packets from the shared counter.
   const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
@@ -538,7 +606,8 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   if (marks) cudaEventRecord(marks[1], stream);
   if (e != cudaSuccess) return e;
   if (o.redo_list) {
-    // The listed cones, each walked alone (one lane per warp).
+    // The listed cones, each walked alone (one cone per warp; the warp still
+    // shares its leaves' triangles).
     const uint32_t solo_blocks = (uint32_t)sm_count * kBlocksPerSm;
     e = count ? launch_one<true>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream)
               : launch_one<false>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream);
