@@ -32,7 +32,10 @@ __device__ __forceinline__ f3 cross(f3 a, f3 b) {
 }
 __device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
 __device__ __forceinline__ f3 div(f3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
-__device__ __forceinline__ f3 normalize(f3 a) { return div(a, len(a)); }
+// Out of line (like the integration helpers below): the kernel is limited by
+// instruction fetch, and inline copies of the division and square root at
+// every call site cost more than the calls.
+static __device__ __noinline__ f3 normalize(f3 a) { return div(a, len(a)); }
 __device__ __forceinline__ f3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 
@@ -512,8 +515,9 @@ __device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3
 }
 
 // ---- integration --------------------------------------------------------------
-// lambert_edge_unit / lambert_edge (:188-201)
-__device__ __forceinline__ float lambert_edge_unit(f3 n, f3 an, f3 bn) {
+// lambert_edge_unit / lambert_edge (:188-201). Out of line: an inline copy
+// of atan2f at each of its many call sites made up a quarter of the kernel.
+static __device__ __noinline__ float lambert_edge_unit(f3 n, f3 an, f3 bn) {
   f3 g = cross(an, bn);
   float l = len(g);
   if (l > 1e-12f) return atan2f(l, dot(an, bn)) * dot(n, div(g, l));
@@ -523,7 +527,7 @@ __device__ __forceinline__ float lambert_edge(f3 n, f3 a, f3 b) { return lambert
 
 // The quad d[0..4] clipped to dot(n, x) >= 0 and Lambert-integrated
 // (clipped_bin_weight / clipped_window_weight, :1331-1403; rect_open :2177-2199).
-__device__ __forceinline__ float clipped_quad_weight(f3 n, f3 d0, f3 d1, f3 d2, f3 d3) {
+static __device__ __noinline__ float clipped_quad_weight(f3 n, f3 d0, f3 d1, f3 d2, f3 d3) {
   f3 d[4] = {d0, d1, d2, d3};
   f3 poly[6];
   int k_n = 0;
@@ -593,7 +597,7 @@ __device__ __forceinline__ bool faces_light(const DevLight& r, f3 point, f3 norm
   return dot(normal, to_light) > 0.0f;
 }
 
-__device__ __forceinline__ float rect_open(f3 point, f3 normal, const DevLight& r) {  // :2148-2199
+static __device__ __noinline__ float rect_open(f3 point, f3 normal, const DevLight& r) {  // :2148-2199
   f3 c0 = r.corner - point;
   float facing = dot(normalize(cross(r.eu, r.ev)), c0);
   if ((r.kind > 0.5f && facing >= 0.0f) || fabsf(facing) <= 1e-6f) return 0.0f;
