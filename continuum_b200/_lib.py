@@ -25,6 +25,7 @@ CC_NONE = 0xFFFFFFFF
 CC_DEVICE_POINTERS = 1
 CC_NO_REDO = 2
 CC_KEEP_ORDER = 4
+CC_STATIC_MAX_CONES = 131072
 
 CC_CONE_CAPPED = 1
 CC_CONE_STACK = 2
@@ -37,6 +38,7 @@ EXPORTS = (
     "cc_context_create", "cc_context_destroy", "cc_last_error", "cc_scene_upload", "cc_scene_build",
     "cc_scene_destroy", "cc_scene_sizes", "cc_scene_arrays", "cc_scene_device_bytes", "cc_options_default",
     "cc_visibility", "cc_irradiance", "cc_coverage", "cc_scene_primary_hits", "cc_context_kernel_times",
+    "cc_visibility_static",
 )
 
 
@@ -101,6 +103,7 @@ def load() -> C.CDLL:
         "cc_coverage": (I, [P, P, U64, P, I, P, P, U32, P]),
         "cc_scene_primary_hits": (I, [P, P, U32, U32, P, P]),
         "cc_context_kernel_times": (I, [P, P, I]),
+        "cc_visibility_static": (I, [P, P, U64, P, U32, C.POINTER(Options), C.POINTER(Outputs), P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

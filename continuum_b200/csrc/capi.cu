@@ -550,6 +550,76 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
   return CC_OK;
 }
 
+int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
+                         uint32_t nlights, const cc_options* opt_in, const cc_outputs* out, void* stream_in) {
+  static_assert(cc::kStaticMaxCones == CC_STATIC_MAX_CONES, "header and library disagree on the limit");
+  if (!scene || !out) return fail(CC_ERR_INVALID, "null argument");
+  if (!scene->ctx) return fail(CC_ERR_INVALID, "scene is not on a device");
+  if ((npoints && !receivers) || (nlights && !lights)) return fail(CC_ERR_INVALID, "null inputs");
+  cc_options opt;
+  if (opt_in) opt = *opt_in; else cc_options_default(&opt);
+  if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
+  if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
+  if (npoints > CC_STATIC_MAX_CONES || npoints * (uint64_t)nlights > CC_STATIC_MAX_CONES)
+    return fail(CC_ERR_INVALID, "more than CC_STATIC_MAX_CONES cones (or points) in one cc_visibility_static call");
+  const uint64_t ncones = npoints * (uint64_t)nlights;
+  auto misaligned = [](const void* p, uintptr_t a) { return p && (reinterpret_cast<uintptr_t>(p) % a) != 0; };
+  if (misaligned(receivers, 16) || misaligned(lights, 16) || misaligned(out->partial, 16) ||
+      misaligned(out->work, 16) || misaligned(out->full, 8) || misaligned(out->any, 8) ||
+      misaligned(out->irradiance, 4) || misaligned(out->fraction, 4))
+    return fail(CC_ERR_INVALID, "device buffers must be aligned (receivers, lights, partial, work: 16 B; full, any: 8 B)");
+  cc_context* ctx = scene->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  cudaStream_t stream = stream_in ? (cudaStream_t)stream_in : ctx->stream;
+  void* base = nullptr;
+  CC_CUDA(cc::static_scratch(ctx->device, &base), "static scratch address");
+  uint8_t* scratch = static_cast<uint8_t*>(base);
+
+  cc::DevQuery q;
+  q.receivers = reinterpret_cast<const float4*>(receivers);
+  q.lights = reinterpret_cast<const float4*>(lights);
+  q.npoints = npoints;
+  q.nlights = nlights;
+  q.hierarchy = opt.hierarchy;
+  q.wide_extent = opt.wide_extent;
+  q.light_cone_cap = opt.light_cone_cap;
+  q.wide_cone_cap = opt.wide_cone_cap;
+  q.order = nullptr;
+  cc::DevOut o{};
+  o.full = reinterpret_cast<uint2*>(out->full);
+  o.any = reinterpret_cast<uint2*>(out->any);
+  o.partial = out->partial;
+  o.irradiance = out->irradiance;
+  o.fraction = out->fraction;
+  o.work = reinterpret_cast<uint4*>(out->work);
+  uint32_t* counters = reinterpret_cast<uint32_t*>(scratch);
+  o.redo_count = counters;
+  o.error = counters + 1;
+  o.next_packet = counters + 2;
+  o.next_solo = counters + 3;
+  if (!(opt.flags & CC_NO_REDO)) {
+    o.redo_list = reinterpret_cast<uint32_t*>(scratch + cc::kStaticRedoOffset);
+    o.redo_capacity = (uint32_t)std::max<uint64_t>(ncones, 1);
+  }
+  // The counters are the only scratch that must start at zero.
+  CC_CUDA(cudaMemsetAsync(counters, 0, cc::kCounterWords * sizeof(uint32_t), stream), "counter reset");
+  if (!(opt.flags & CC_KEEP_ORDER) && npoints > 64 && !scene->flat.nodes.empty()) {
+    const size_t sort_bytes = cc::kStaticScratchBytes - cc::kStaticSortOffset;
+    if (cc::walk_order_scratch_bytes(npoints) > sort_bytes)
+      return fail(CC_ERR_INVALID, "walk order scratch exceeds the static scratch");
+    uint32_t* order = reinterpret_cast<uint32_t*>(scratch + cc::kStaticOrderOffset);
+    CC_CUDA(cc::walk_order(q.receivers, npoints, scene->flat.nodes[0].lo, scene->flat.nodes[0].hi,
+                           scratch + cc::kStaticSortOffset, sort_bytes, order, stream),
+            "walk order");
+    q.order = order;
+  }
+  CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
+                                nullptr),
+          "visibility launch");
+  return CC_OK;
+}
+
 static void receivers_from6(const float* r6, uint64_t n, std::vector<float>& out) {
   out.assign(n * 8, 0.0f);
   for (uint64_t i = 0; i < n; ++i) {

@@ -52,6 +52,19 @@ struct DevOut {
 // Scratch words per call: redo count, error word, packet and solo counters.
 constexpr int kCounterWords = 4;
 
+// Scratch of cc_visibility_static: a file-scope device array of
+// kStaticScratchBytes per device, laid out as the counters (256 bytes), the
+// redo list (4 bytes per cone), the walk order (4 bytes per point) and the
+// walk order's sort scratch (the rest).
+constexpr uint32_t kStaticMaxCones = 1u << 17;  // cones (and points) per call: 131,072
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;
+constexpr size_t kStaticRedoOffset = 256;
+constexpr size_t kStaticOrderOffset = kStaticRedoOffset + 4 * size_t(kStaticMaxCones);
+constexpr size_t kStaticSortOffset = kStaticOrderOffset + 4 * size_t(kStaticMaxCones);
+// The array's device address on `device` (the current device). The first
+// call per device looks it up; later calls return the cached address.
+cudaError_t static_scratch(int device, void** ptr);
+
 cudaError_t upload_disk_table(const float* table64);
 
 // The packet pass over every cone, then (with o.redo_list) the solo pass over

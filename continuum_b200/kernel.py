@@ -384,6 +384,17 @@ class MaskConeKernel:
                                    C.c_void_p(d_lights), int(nlights), C.byref(opt), C.byref(o),
                                    C.c_void_p(stream) if stream else None))
 
+    def visibility_static(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int,
+                          outputs: dict, stream: int = 0, hierarchy=Hierarchy.TRIANGLES,
+                          points_per_warp: Optional[int] = None, flags: int = 0) -> None:
+        """visibility_device through cc_visibility_static: no allocation, at
+        most CC_STATIC_MAX_CONES cones, one call in flight per device."""
+        o = _lib.Outputs(*(outputs.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.options(hierarchy, flags | _lib.CC_DEVICE_POINTERS, points_per_warp)
+        check(load().cc_visibility_static(scene.handle, C.c_void_p(d_receivers), int(npoints), C.c_void_p(d_lights),
+                                          int(nlights), C.byref(opt), C.byref(o),
+                                          C.c_void_p(stream) if stream else None))
+
 
 def kernel_times(kernel: MaskConeKernel, max_calls: int = 256) -> np.ndarray:
     """(calls, 2) milliseconds of the packet and solo passes of the

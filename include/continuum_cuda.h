@@ -163,6 +163,34 @@ CC_API int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* re
                   const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                   void* stream);
 
+/* No counterpart in the reference (whose kernel owns its wgpu buffers).
+ * cc_visibility without allocation: the same results as cc_visibility with
+ * CC_DEVICE_POINTERS, for at most CC_STATIC_MAX_CONES cones and as many points
+ * per call (larger calls are rejected with CC_ERR_INVALID), with its scratch
+ * (the work counters, the re-walk list, the walk order and its sort space) in
+ * one fixed 8 MiB device array of the library per device instead of context
+ * buffers. It calls no cudaMalloc, cudaFree or allocating library routine, so
+ * it suits callers that cannot let the library allocate: a server that admits
+ * scenes against a fixed device-memory budget or whose memory a caching
+ * allocator owns (cc_visibility grows its context's buffers with cudaMalloc
+ * to the largest call seen and keeps them), a loop that overlaps work on other
+ * streams (cudaFree waits for the whole device), and a caller that must keep
+ * working when device memory is exhausted.
+ *  - Every pointer is a device pointer (CC_DEVICE_POINTERS is implied); the
+ *    call is asynchronous on `stream` (NULL: the scene's context's stream).
+ *  - The first call on a device looks up the array's address
+ *    (cudaGetSymbolAddress, which loads the array's module) and may set the
+ *    kernel's shared-memory attribute; make it before any stream capture.
+ *  - The call zeroes the array's four counter words on the stream before its
+ *    kernels run; nothing else in it needs a starting value.
+ *  - All calls on one device share the array: calls whose work can overlap on
+ *    the device (on different streams, or from several host threads) race and
+ *    corrupt each other's results. Issue them on one stream, or order them.
+ *  - No kernel times are recorded (cc_context_kernel_times does not see it). */
+#define CC_STATIC_MAX_CONES 131072u
+CC_API int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
+                                uint32_t nlights, const cc_options* opt, const cc_outputs* out, void* stream);
+
 /* Kernel times of the cc_visibility calls made on this context since the
  * last query, oldest first (the last 256 calls at most): per call, the packet
  * pass and the solo re-walk pass in milliseconds, from CUDA events recorded
