@@ -80,7 +80,7 @@ def cpu_sample(w, target_seconds: float, offset: int = 0):
     threads = cpu_threads()
     scene = OracleScene(w.meshes)
     total = w.receivers.shape[0] * w.lights.shape[0]
-    probe = np.arange(offset % 97, total, max(1, total // 2048), dtype=np.uint64)[:2048]
+    probe = np.arange(offset % 97, total, max(1, total // 16384), dtype=np.uint64)[:16384]
     t0 = time.perf_counter()
     scene.visibility(w.receivers, w.lights, cone_ids=probe, threads=threads, partial=False)
     rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
@@ -214,6 +214,11 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
     def step():
         kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, ptrs, stream=stream.cuda_stream)
 
+    # This library's kernels per step: morton_keys (Morton walk order, when
+    # there are more than 64 points), the packet pass and the solo pass.
+    morton = P > 64
+    launches_per_step = 2 + (1 if morton else 0)
+
     # Work counters (an untimed counted run): the algorithmic bytes per cone.
     work = torch.empty(C, 4, dtype=torch.int32, device=dev)
     kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, {**ptrs, "work": work.data_ptr()},
@@ -321,7 +326,8 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
                      "work_per_cone": {"object_nodes": n_obj / C, "triangle_nodes": n_blas / C,
                                        "triangles": n_tri / C},
                      "note": "most node and triangle reads hit L1/L2; the kernel is issue-bound, see profiles/"},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
+        "library_launches": {"cub_radix_sort": 6 * args.steps if morton else 0},
         "clocks": clk.summary(),
         "status": {"capped": int(((status & L_.CC_CONE_CAPPED) != 0).sum()),
                    "rewalked": int(((status & L_.CC_CONE_REWALKED) != 0).sum()),
@@ -343,7 +349,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--cpu-seconds", type=float, default=3.0)
+    ap.add_argument("--cpu-seconds", type=float, default=1.5)
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
