@@ -159,6 +159,198 @@ def traffic_per_cone():
     return None
 
 
+def timed_steps(torch, dev, stream, flush, fn, warmup, steps):
+    """Device milliseconds of `steps` calls of fn on `stream` (CUDA events,
+    L2 flushed before each), after `warmup` untimed calls."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return [e0.elapsed_time(e1) for e0, e1 in ev]
+
+
+def batched_leg(args, kernel, dev, stream, flush) -> dict:
+    """The batching workload (64 jobs of uneven scene, light and point counts):
+    cones/s of one batched submission (autotuned, replayed from a CUDA graph)
+    beside the plain path called once per job, both device-timed with CUDA
+    events and the L2 flushed between steps."""
+    import torch
+
+    from continuum_b200 import Batch, _lib, scenes
+    from continuum_b200.kernel import kernel_times
+
+    jobs = scenes.batch_jobs(seed=3, njobs=args.batch_jobs)
+    sc = [kernel.scene(w.meshes) for w in jobs]
+    rec = [torch.from_numpy(w.receivers).to(dev) for w in jobs]
+    lig = [torch.from_numpy(w.lights).to(dev) for w in jobs]
+    cones = [r.shape[0] * l.shape[0] for r, l in zip(rec, lig)]
+    outs = [{"full": torch.empty(n, dtype=torch.int64, device=dev), "any": torch.empty(n, dtype=torch.int64, device=dev),
+             "irradiance": torch.empty(n, device=dev), "fraction": torch.empty(n, device=dev)} for n in cones]
+    ptrs = [{k: v.data_ptr() for k, v in o.items()} for o in outs]
+    total = int(sum(cones))
+
+    # The autotuner runs on a sample of the same jobs (every 16th point).
+    sample_rec = [r[::16].contiguous() for r in rec]
+    sample_out = [{k: torch.empty(max(1, sr.shape[0] * l.shape[0]), dtype=v.dtype, device=dev) for k, v in o.items()}
+                  for sr, l, o in zip(sample_rec, lig, outs)]
+    tb = Batch(kernel)
+    for s_, sr, l, so in zip(sc, sample_rec, lig, sample_out):
+        tb.add(s_, sr.data_ptr(), sr.shape[0], l.data_ptr(), l.shape[0], {k: v.data_ptr() for k, v in so.items()})
+    best, tune_ms = tb.tune(reps=2)
+    tb.close()
+    del sample_rec, sample_out
+
+    b = Batch(kernel)
+    for s_, r, l, p in zip(sc, rec, lig, ptrs):
+        b.add(s_, r.data_ptr(), r.shape[0], l.data_ptr(), l.shape[0], p)
+
+    def batched():
+        b.submit(best, stream=stream.cuda_stream)
+
+    def plain():
+        for s_, r, l, p in zip(sc, rec, lig, ptrs):
+            kernel.visibility_device(s_, r.data_ptr(), r.shape[0], l.data_ptr(), l.shape[0], p,
+                                     stream=stream.cuda_stream)
+
+    steps = max(1, min(args.steps, args.batch_steps))
+    # The first submission runs directly and captures the graph; later ones replay it.
+    batched_ms = timed_steps(torch, dev, stream, flush, batched, 2, steps)
+    b.wait()
+    plain_ms = timed_steps(torch, dev, stream, flush, plain, 1, steps)
+    kernel_times(kernel)
+    b.close()
+    for s_ in sc:
+        s_.close()
+    bt, pt = float(np.mean(batched_ms)), float(np.mean(plain_ms))
+    return {"workload": f"{len(jobs)} jobs: displaced-icosphere fields of 10k-2M triangles (log-uniform), 1-16 rect "
+                        "and disk lights, 4k-1M primary hits (log-uniform)",
+            "jobs": len(jobs), "triangles": int(sum(w.ntris for w in jobs)),
+            "points": int(sum(r.shape[0] for r in rec)), "cones_per_step": total,
+            "value": total / (bt * 1e-3), "unit": UNIT, "ms_per_step": bt, "steps": steps,
+            "plain_per_job": {"value": total / (pt * 1e-3), "ms_per_step": pt,
+                              "path": "cc_visibility with device pointers, once per job, same stream"},
+            "speedup_vs_plain_per_job": pt / bt,
+            "tuned": {"points_per_warp": best.points_per_warp, "blocks_per_sm": best.blocks_per_sm,
+                      "walk_order": "given" if best.flags & _lib.CC_KEEP_ORDER else "morton",
+                      "graph_replay": bool(best.flags & _lib.CC_BATCH_GRAPH)},
+            "tune_ms_per_candidate": [round(float(x), 3) for x in tune_ms],
+            "tune_sample": "every 16th point of every job",
+            "l2": "flushed between timed steps (256 MB write)"}
+
+
+def served_leg(args, kernel) -> dict:
+    """The serving workload: 8 resident scenes, requests of 1-8 moved or
+    recoloured lights over seeded camera poses, Poisson arrivals at each rate.
+    A client thread submits each request at its arrival time with pinned host
+    buffers; latency is submission to results in the host buffers. Beside it,
+    the plain per-request path (cc_visibility with host buffers, one request
+    at a time, first come first served) under the same arrivals, from each
+    request's measured time alone."""
+    import threading
+
+    import torch
+
+    from continuum_b200 import Server, scenes
+
+    pool = scenes.served_scenes(seed=4)
+    sc = [kernel.scene(p.meshes) for p in pool]
+    poses = [[torch.from_numpy(r).pin_memory() for r in p.poses] for p in pool]
+    reqs = scenes.served_requests(pool, args.serve_requests, seed=5)
+    cones = [poses[si][pi].shape[0] * l.shape[0] for si, pi, l in reqs]
+    pts = [poses[si][pi].shape[0] for si, pi, _ in reqs]
+    outs = []
+    for (si, pi, l), c in zip(reqs, cones):
+        P, L = poses[si][pi].shape[0], l.shape[0]
+        outs.append({"full": torch.empty((L, P), dtype=torch.int64).pin_memory().numpy(),
+                     "any": torch.empty((L, P), dtype=torch.int64).pin_memory().numpy(),
+                     "irradiance": torch.empty((L, P), dtype=torch.float32).pin_memory().numpy(),
+                     "fraction": torch.empty((L, P), dtype=torch.float32).pin_memory().numpy()})
+
+    # The plain per-request path: each request alone through cc_visibility.
+    for si, pi, l in reqs[:2]:
+        kernel.visibility(sc[si], poses[si][pi].numpy(), l)
+    service = []
+    for (si, pi, l), o in zip(reqs, outs):
+        t0 = time.perf_counter()
+        kernel.visibility(sc[si], poses[si][pi].numpy(), l)
+        service.append(time.perf_counter() - t0)
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x) * 1e3, q)) if len(x) else None
+
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    results = []
+    for ri, rate in enumerate(rates):
+        rng = np.random.default_rng(100 + ri)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        arrivals -= arrivals[0]
+        # Plain, first come first served: each request waits for the previous.
+        done_at, lat_plain = 0.0, []
+        for a, s_ in zip(arrivals, service):
+            done_at = max(done_at, a) + s_
+            lat_plain.append(done_at - a)
+        plain_span = done_at
+        srv = Server(kernel, hbm_budget=args.serve_budget_gib << 30, max_inflight=4)
+        ids = [srv.add_scene(s_) for s_ in sc]
+        tickets = [None] * len(reqs)
+        refused = [False] * len(reqs)
+
+        def client():
+            t0 = time.perf_counter()
+            for i, ((si, pi, l), o) in enumerate(zip(reqs, outs)):
+                wait = arrivals[i] - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                try:
+                    tickets[i] = srv.submit(ids[si], poses[si][pi].numpy(), l, o, cache_key=1 + si * 16 + pi)
+                except Exception:
+                    refused[i] = True
+
+        t_start = time.perf_counter()
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        stats = []
+        for t in tickets:
+            if t is not None:
+                stats.append(srv.wait(t))
+        span = time.perf_counter() - t_start
+        st = srv.stats()
+        srv.close()
+        lat = [x["total_ms"] / 1e3 for x in stats]
+        big = [x["total_ms"] / 1e3 for x, p in zip(stats, [p for p, t in zip(pts, tickets) if t is not None])
+               if p >= 1_000_000]
+        served_cones = sum(c for c, t in zip(cones, tickets) if t is not None)
+        results.append({
+            "rate_req_s": rate, "requests": len(reqs), "completed": len(stats), "refused": int(sum(refused)),
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+            "p99_ms_requests_of_1M_points_or_more": pct(big, 99) if big else None,
+            "queries_per_s": served_cones / span, "requests_per_s": len(stats) / span,
+            "launches": st["launches"], "lights_from_cache": st["cached_lights"], "lights_traced": st["traced_lights"],
+            "peak_device_bytes": st["peak_bytes"],
+            "plain_per_request": {"p50_ms": pct(lat_plain, 50), "p99_ms": pct(lat_plain, 99),
+                                  "queries_per_s": sum(cones) / plain_span},
+        })
+    for s_ in sc:
+        s_.close()
+    return {"workload": "8 resident displaced-icosphere scenes (50k-3M triangles, log-uniform), 3 seeded camera poses "
+                        "each (16k-2M primary hits, log-uniform); requests of 1-8 lights, each a base light recoloured "
+                        "or a moved light (1:1)",
+            "scene_triangles": [p.ntris for p in pool], "requests_per_rate": len(reqs),
+            "mean_cones_per_request": float(np.mean(cones)),
+            "server": {"hbm_budget_gib": args.serve_budget_gib, "max_inflight": 4,
+                       "cache_key": "scene and camera pose (recoloured lights are served from the lighting cache)"},
+            "plain_per_request_path": "cc_visibility with pinned host buffers, one request at a time; latency under "
+                                      "the same arrivals from each request's measured time alone, first come first served",
+            "rates": results}
+
+
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
@@ -313,7 +505,7 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded)", "impl": "cuda", "config": config(world, w),
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.nbytes + lig_h.nbytes),
+        "e2e": None if args.no_e2e else {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.nbytes + lig_h.nbytes),
                 "d2h_bytes_per_step": int(sum(v.nbytes for v in host_out.values()) + 8),
                 "steps": e2e_steps, "path": "cc_visibility with host buffers (pinned), scene resident"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -333,6 +525,11 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
                    "rewalked": int(((status & L_.CC_CONE_REWALKED) != 0).sum()),
                    "diverged": int(((status & L_.CC_CONE_DIVERGED) != 0).sum())},
     }
+    forms = set(args.forms.split(",")) if args.forms else set()
+    if "batched" in forms:
+        line["batched"] = batched_leg(args, kernel, dev, stream, flush)
+    if "served" in forms:
+        line["served"] = served_leg(args, kernel)
     if world == 1 and not args.no_cpu_baseline:
         rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
@@ -353,6 +550,13 @@ def main() -> None:
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--forms", default="batched,served",
+                    help="systems forms measured beside the plain line (comma list of batched, served; none)")
+    ap.add_argument("--batch-jobs", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=3, help="timed steps of the batched leg (at most --steps)")
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-rates", default="50,200,2000", help="Poisson arrival rates (requests/s)")
+    ap.add_argument("--serve-budget-gib", type=int, default=16)
     ap.add_argument("--points", type=int, default=0,
                     help="keep a strided subset of this many receivers (profiling runs; not a bench line)")
     args = ap.parse_args()

@@ -4,10 +4,10 @@ The product is libcontinuum_cuda.so (hand-written sm_100a CUDA behind a C
 ABI, include/continuum_cuda.h); this package binds it and mirrors the
 reference's visibility API.
 """
-from .kernel import (Hierarchy, Light, MaskConeKernel, RectLight, Scene, SphereLight, Spot, Visibility,
+from .kernel import (Batch, Hierarchy, Light, MaskConeKernel, RectLight, Scene, Server, SphereLight, Spot, Visibility,
                      flatten_meshes, host_scene, light_gpu, lights_gpu, receivers_gpu)
 
 __all__ = [
-    "Hierarchy", "Light", "MaskConeKernel", "RectLight", "Scene", "SphereLight", "Spot", "Visibility",
+    "Batch", "Hierarchy", "Light", "MaskConeKernel", "RectLight", "Scene", "Server", "SphereLight", "Spot", "Visibility",
     "flatten_meshes", "host_scene", "light_gpu", "lights_gpu", "receivers_gpu",
 ]

@@ -26,6 +26,7 @@ CC_DEVICE_POINTERS = 1
 CC_NO_REDO = 2
 CC_KEEP_ORDER = 4
 CC_STATIC_MAX_CONES = 131072
+CC_BATCH_GRAPH = 8
 
 CC_CONE_CAPPED = 1
 CC_CONE_STACK = 2
@@ -38,7 +39,10 @@ EXPORTS = (
     "cc_context_create", "cc_context_destroy", "cc_last_error", "cc_scene_upload", "cc_scene_build",
     "cc_scene_destroy", "cc_scene_sizes", "cc_scene_arrays", "cc_scene_device_bytes", "cc_options_default",
     "cc_visibility", "cc_irradiance", "cc_coverage", "cc_scene_primary_hits", "cc_context_kernel_times",
-    "cc_visibility_static",
+    "cc_visibility_static", "cc_batch_options_default", "cc_batch_create", "cc_batch_destroy", "cc_batch_clear",
+    "cc_batch_add", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
+    "cc_server_options_default", "cc_server_create", "cc_server_destroy", "cc_server_add_scene", "cc_server_submit",
+    "cc_server_wait", "cc_server_stats",
 )
 
 
@@ -66,6 +70,26 @@ class Options(C.Structure):
         ("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
         ("wide_cone_cap", C.c_uint32), ("points_per_warp", C.c_uint32), ("flags", C.c_uint32),
     ]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("points_per_warp", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("flags", C.c_uint32)]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_budget", C.c_uint64), ("max_inflight", C.c_uint32), ("max_queue", C.c_uint32),
+                ("max_launch_cones", C.c_uint64), ("points_per_warp", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", C.c_uint32), ("receivers", C.c_void_p), ("npoints", C.c_uint64), ("lights", C.c_void_p),
+                ("nlights", C.c_uint32), ("hierarchy", C.c_uint32), ("cache_key", C.c_uint64),
+                ("full", C.c_void_p), ("any", C.c_void_p), ("irradiance", C.c_void_p), ("fraction", C.c_void_p)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("queued_ms", C.c_double), ("total_ms", C.c_double), ("launch_requests", C.c_uint32),
+                ("cached_lights", C.c_uint32)]
 
 
 class Outputs(C.Structure):
@@ -104,6 +128,22 @@ def load() -> C.CDLL:
         "cc_scene_primary_hits": (I, [P, P, U32, U32, P, P]),
         "cc_context_kernel_times": (I, [P, P, I]),
         "cc_visibility_static": (I, [P, P, U64, P, U32, C.POINTER(Options), C.POINTER(Outputs), P]),
+        "cc_batch_options_default": (None, [C.POINTER(BatchOptions)]),
+        "cc_batch_create": (I, [P, C.POINTER(P)]),
+        "cc_batch_destroy": (I, [P]),
+        "cc_batch_clear": (I, [P]),
+        "cc_batch_add": (I, [P, P, P, U64, P, U32, C.POINTER(Options), C.POINTER(Outputs), C.POINTER(U32)]),
+        "cc_batch_submit": (I, [P, C.POINTER(BatchOptions), P]),
+        "cc_batch_wait": (I, [P, U32]),
+        "cc_batch_tune": (I, [P, C.POINTER(BatchOptions), U32, C.POINTER(BatchOptions), P, U32]),
+        "cc_batch_sizes": (I, [P, P]),
+        "cc_server_options_default": (None, [C.POINTER(ServerOptions)]),
+        "cc_server_create": (I, [P, C.POINTER(ServerOptions), C.POINTER(P)]),
+        "cc_server_destroy": (I, [P]),
+        "cc_server_add_scene": (I, [P, P, C.POINTER(U32)]),
+        "cc_server_submit": (I, [P, C.POINTER(Request), C.POINTER(U64)]),
+        "cc_server_wait": (I, [P, U64, U32, C.POINTER(RequestStats)]),
+        "cc_server_stats": (I, [P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -9,11 +9,9 @@
 #include <thread>
 #include <vector>
 
-#include "../../include/continuum_cuda.h"
-#include "bvh.h"
-#include "kernels.h"
+#include "capi_internal.h"
 
-namespace {
+namespace cc_host {
 
 thread_local std::string g_error;
 
@@ -27,32 +25,16 @@ int cuda_fail(cudaError_t e, const char* what) {
   return e == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA;
 }
 
-#define CC_CUDA(call, what)                      \
-  do {                                           \
-    cudaError_t e_ = (call);                     \
-    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-  } while (0)
+int set_device(cc_context* ctx) {
+  CC_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  return CC_OK;
+}
 
-// A device allocation that grows on demand and is kept for reuse.
-struct DevBuf {
-  void* ptr = nullptr;
-  size_t size = 0;
-  cudaError_t reserve(size_t bytes) {
-    if (bytes <= size) return cudaSuccess;
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    size = 0;
-    size_t want = std::max<size_t>(bytes, 256);
-    cudaError_t e = cudaMalloc(&ptr, want);
-    if (e == cudaSuccess) size = want;
-    return e;
-  }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    size = 0;
-  }
-};
+}  // namespace cc_host
+
+using namespace cc_host;
+
+namespace {
 
 // The fraction of each bin of a sphere light's window inside the inscribed
 // disk (the reference's DISK table, mask_cones.wgsl:888-897): for the
@@ -74,54 +56,6 @@ void disk_table(float* out) {
     }
     out[b] = (float)(std::round(area * 1e6) / 1e6);
   }
-}
-
-}  // namespace
-
-struct cc_context {
-  int device = 0;
-  int sm_count = 148;
-  cudaStream_t stream = nullptr;
-  DevBuf receivers, lights, full, any, partial, irradiance, fraction, work;
-  DevBuf redo;      // redo list
-  DevBuf order;     // walk order of the points
-  DevBuf sort_scratch;
-  DevBuf counters;  // [redo count, error word]
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  // Kernel timing: three events per visibility call (before the packet pass,
-  // between the passes, after the solo pass) in a ring of kTimingRing calls.
-  static constexpr int kTimingRing = 256;
-  std::vector<cudaEvent_t> marks;  // 3 * kTimingRing
-  int timed_first = 0;             // oldest unread call in the ring
-  int timed_count = 0;             // unread calls
-};
-
-struct cc_scene {
-  cc_context* ctx = nullptr;
-  cc::FlatScene flat;  // host copy of the reference layouts
-  float4* tris = nullptr;
-  uint4* meshes = nullptr;
-  float4* nodes = nullptr;
-  uint32_t* items = nullptr;
-  float4* blas = nullptr;
-  uint64_t bytes = 0;
-  cc::DevScene dev() const {
-    cc::DevScene s;
-    s.tris = tris;
-    s.meshes = meshes;
-    s.nodes = nodes;
-    s.items = items;
-    s.blas = blas;
-    s.nmeshes = flat.nmeshes;
-    return s;
-  }
-};
-
-namespace {
-
-int set_device(cc_context* ctx) {
-  CC_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-  return CC_OK;
 }
 
 // Repacks NodeGpu (48 bytes) into two float4 (lo.xyz | a, hi.xyz | b).
@@ -302,7 +236,7 @@ int cc_context_destroy(cc_context* ctx) {
   if (!ctx) return CC_OK;
   cudaSetDevice(ctx->device);
   for (DevBuf* b : {&ctx->receivers, &ctx->lights, &ctx->full, &ctx->any, &ctx->partial, &ctx->irradiance,
-                    &ctx->fraction, &ctx->work, &ctx->redo, &ctx->counters})
+                    &ctx->fraction, &ctx->work, &ctx->redo, &ctx->order, &ctx->sort_scratch, &ctx->counters})
     b->release();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);

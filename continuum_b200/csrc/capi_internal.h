@@ -1,0 +1,91 @@
+// Host-side state shared by the C ABI's files: contexts, scenes, growable
+// device buffers and the error helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/continuum_cuda.h"
+#include "bvh.h"
+#include "kernels.h"
+
+namespace cc_host {
+
+// Records the calling thread's error message and returns `code`.
+int fail(int code, const std::string& msg);
+// The same for a failed CUDA call (CC_ERR_OOM for an allocation failure).
+int cuda_fail(cudaError_t e, const char* what);
+
+#define CC_CUDA(call, what)                      \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// A device allocation that grows on demand and is kept for reuse.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t size = 0;
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= size) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    size = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaSuccess) size = want;
+    return e;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    size = 0;
+  }
+};
+
+int set_device(cc_context* ctx);
+
+}  // namespace cc_host
+
+struct cc_context {
+  using DevBuf = cc_host::DevBuf;
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  DevBuf receivers, lights, full, any, partial, irradiance, fraction, work;
+  DevBuf redo;      // redo list
+  DevBuf order;     // walk order of the points
+  DevBuf sort_scratch;
+  DevBuf counters;  // [redo count, error word]
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Kernel timing: three events per visibility call (before the packet pass,
+  // between the passes, after the solo pass) in a ring of kTimingRing calls.
+  static constexpr int kTimingRing = 256;
+  std::vector<cudaEvent_t> marks;  // 3 * kTimingRing
+  int timed_first = 0;             // oldest unread call in the ring
+  int timed_count = 0;             // unread calls
+};
+
+struct cc_scene {
+  cc_context* ctx = nullptr;
+  cc::FlatScene flat;  // host copy of the reference layouts
+  float4* tris = nullptr;
+  uint4* meshes = nullptr;
+  float4* nodes = nullptr;
+  uint32_t* items = nullptr;
+  float4* blas = nullptr;
+  uint64_t bytes = 0;
+  cc::DevScene dev() const {
+    cc::DevScene s;
+    s.tris = tris;
+    s.meshes = meshes;
+    s.nodes = nodes;
+    s.items = items;
+    s.blas = blas;
+    s.nmeshes = flat.nmeshes;
+    return s;
+  }
+};
+

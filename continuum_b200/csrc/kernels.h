@@ -52,6 +52,51 @@ struct DevOut {
 // Scratch words per call: redo count, error word, packet and solo counters.
 constexpr int kCounterWords = 4;
 
+// One job of a batch: its scene, query and outputs, and where its packets,
+// cones and points start in the batch's numbering. A batch's packets never
+// straddle two jobs.
+struct JobGpu {
+  DevScene scene;
+  DevQuery query;  // query.order is unused: the batch's order array holds every job's
+  uint2* full;
+  uint2* any;
+  float* partial;
+  float* irradiance;
+  float* fraction;
+  uint4* work;
+  uint64_t packet_start;
+  uint64_t cone_start;
+  uint64_t point_start;
+  float lo[3], hi[3];  // the scene's bounds (Morton quantization)
+};
+
+// A batch launch: the job table and the batch's sizes. The redo list and
+// counters are DevOut's scratch fields (its output pointers are unused).
+struct BatchLaunch {
+  const JobGpu* jobs;
+  uint32_t njobs;
+  uint64_t packets;  // packets of all jobs at `pw` cones per packet
+  uint64_t points;   // points of all jobs
+  uint32_t pw;
+  // The walk order of every job's points (job j's at order + point_start,
+  // job-local indices), or null: each job's points in their given order.
+  const uint32_t* order;
+};
+
+// Morton walk order of every job's points in one sort: keys are the job index
+// above each point's 30-bit code, values the job-local point index; job j's
+// order lands at order + jobs[j].point_start.
+size_t batch_order_scratch_bytes(uint64_t points);
+cudaError_t batch_order(const BatchLaunch& b, void* scratch, size_t scratch_bytes, uint32_t* order,
+                        cudaStream_t stream);
+
+// The packet pass over every job's cones, then the solo pass over the cones
+// it listed (batch cone numbers). o.redo_count, o.error and the two packet
+// counters must be zero on entry. blocks_per_sm: resident blocks per SM to
+// launch (1..kBlocksPerSm).
+cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count_work, int sm_count, int blocks_per_sm,
+                         cudaStream_t stream);
+
 // Scratch of cc_visibility_static: a file-scope device array of
 // kStaticScratchBytes per device, laid out as the counters (256 bytes), the
 // redo list (4 bytes per cone), the walk order (4 bytes per point) and the

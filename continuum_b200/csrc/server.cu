@@ -1,0 +1,624 @@
+// The served form of the C ABI (include/continuum_cuda.h, cc_server_*): a
+// request loop on its own host thread with continuous batching over several
+// streams, admission against a device-memory budget, and a lighting cache of
+// per-light results kept on the device.
+//
+// Each launch slot owns a stream, an event and pinned host staging for its
+// job table and status words. The loop retires finished launches (results
+// become cache entries or are freed), then builds the next launch from the
+// queue's front: cache lookups first, then device memory for the traced
+// lights (evicting unused cache entries least recently used), one job per
+// (request, traced light), the copies in, one batched launch, and the copies
+// out. Device memory comes from a pool owned by the server, allocated and
+// freed in stream order.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "capi_internal.h"
+
+using namespace cc_host;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// Per-point bytes of one light's results: full and any words, irradiance, fraction.
+constexpr uint64_t kResultBytes = 8 + 8 + 4 + 4;
+
+struct CacheEntry {
+  uint64_t key = 0;
+  float geometry[12] = {};  // the light record without its radiance
+  uint64_t npoints = 0;
+  uint32_t scene = 0, hierarchy = 0;
+  uint8_t* dev = nullptr;   // npoints x (full | any | irradiance | fraction)
+  uint64_t bytes = 0;
+  int refs = 0;             // launches in flight reading it
+  std::list<CacheEntry*>::iterator lru;
+};
+
+struct Request {
+  uint64_t ticket = 0;
+  cc_request req{};
+  std::vector<float> lights;  // copied at submission
+  Clock::time_point t_submit, t_admit, t_done;
+  bool done = false;
+  int status = CC_OK;
+  std::string error;
+  cc_request_stats stats{};
+  // Set while in a launch.
+  std::vector<CacheEntry*> hit;      // per light: the entry serving it, or null
+  std::vector<uint8_t*> result;      // per light: the traced result block, or null
+  std::vector<float> traced;         // the traced lights' records, compacted (the copy's source)
+  float4* d_receivers = nullptr;
+  float4* d_lights = nullptr;
+  const cc_scene* scene = nullptr;
+};
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool busy = false;
+  std::vector<Request*> reqs;
+  std::vector<void*> scratch;        // freed when the launch retires
+  uint64_t scratch_bytes = 0;        // in_use held by the launch besides result blocks
+  cc::JobGpu* host_jobs = nullptr;   // pinned
+  size_t host_jobs_cap = 0;
+  uint32_t* status = nullptr;        // pinned, kCounterWords
+};
+
+}  // namespace
+
+struct cc_server {
+  cc_context* ctx = nullptr;
+  cc_server_options opt{};
+  cudaMemPool_t pool = nullptr;
+  std::vector<const cc_scene*> scenes;
+  std::vector<Slot> slots;
+
+  std::mutex mu;                     // guards everything below
+  std::condition_variable wake;      // the loop: new requests or stop
+  std::condition_variable finished;  // waiters: a request completed
+  std::deque<Request*> queue;
+  std::unordered_map<uint64_t, std::unique_ptr<Request>> requests;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  std::thread loop;
+
+  std::list<CacheEntry*> lru;        // front: least recently used
+  std::multimap<uint64_t, std::unique_ptr<CacheEntry>> cache;  // by key
+  uint64_t in_use = 0, peak = 0;
+
+  uint64_t completed = 0, refused = 0, launches = 0, cached_lights = 0, traced_lights = 0;
+};
+
+namespace {
+
+uint64_t request_cones(const cc_request& r) { return r.npoints * (uint64_t)r.nlights; }
+
+// Device bytes a request needs while in flight when `traced` of its lights
+// are traced: inputs, results, and its share of the launch's scratch.
+uint64_t request_bytes(const cc_request& r, uint64_t traced) {
+  const uint64_t P = r.npoints;
+  return P * 32 + traced * 64 + traced * P * kResultBytes + traced * P * 4 /* redo */ + P * 4 /* order */ +
+         cc::batch_order_scratch_bytes(std::max<uint64_t>(P, 1)) + traced * sizeof(cc::JobGpu) + 4096;
+}
+
+void* pool_alloc(cc_server* s, uint64_t bytes, cudaStream_t stream, cudaError_t* e) {
+  void* p = nullptr;
+  *e = cudaMallocFromPoolAsync(&p, std::max<uint64_t>(bytes, 256), s->pool, stream);
+  return *e == cudaSuccess ? p : nullptr;
+}
+
+CacheEntry* find_entry(cc_server* s, const cc_request& r, const float* light) {
+  auto range = s->cache.equal_range(r.cache_key);
+  for (auto it = range.first; it != range.second; ++it) {
+    CacheEntry* e = it->second.get();
+    if (e->npoints == r.npoints && e->scene == r.scene && e->hierarchy == r.hierarchy &&
+        std::memcmp(e->geometry, light, sizeof(e->geometry)) == 0)
+      return e;
+  }
+  return nullptr;
+}
+
+void touch(cc_server* s, CacheEntry* e) {
+  s->lru.erase(e->lru);
+  e->lru = s->lru.insert(s->lru.end(), e);
+}
+
+// Frees unused cache entries, least recently used first, until `need` more
+// bytes fit the budget. Returns whether they fit. (s->mu held.)
+bool make_room(cc_server* s, uint64_t need, cudaStream_t stream) {
+  auto it = s->lru.begin();
+  while (s->in_use + need > s->opt.hbm_budget && it != s->lru.end()) {
+    CacheEntry* e = *it;
+    if (e->refs > 0) {
+      ++it;
+      continue;
+    }
+    it = s->lru.erase(it);
+    cudaFreeAsync(e->dev, stream);
+    s->in_use -= e->bytes;
+    auto range = s->cache.equal_range(e->key);
+    for (auto c = range.first; c != range.second; ++c)
+      if (c->second.get() == e) {
+        s->cache.erase(c);
+        break;
+      }
+  }
+  return s->in_use + need <= s->opt.hbm_budget;
+}
+
+// Marks a request done. (s->mu held.)
+void complete_locked(cc_server* s, Request* r, int status, const std::string& error) {
+  r->status = status;
+  r->error = error;
+  r->done = true;
+  r->t_done = Clock::now();
+  r->stats.queued_ms = ms_between(r->t_submit, r->t_admit);
+  r->stats.total_ms = ms_between(r->t_submit, r->t_done);
+  if (status == CC_OK) s->completed++;
+  s->finished.notify_all();
+}
+
+void release_slot(cc_server* s, Slot& slot) {
+  for (void* p : slot.scratch) cudaFreeAsync(p, slot.stream);
+  s->in_use -= slot.scratch_bytes;
+  slot.scratch.clear();
+  slot.scratch_bytes = 0;
+  slot.reqs.clear();
+  slot.busy = false;
+}
+
+// Retires a finished launch: traced results become cache entries (or are
+// freed), inputs and scratch are freed, and its requests complete. (s->mu held.)
+void retire(cc_server* s, Slot& slot) {
+  const bool stack = (slot.status[1] & 2u) != 0;
+  for (Request* r : slot.reqs) {
+    for (size_t l = 0; l < r->result.size(); ++l) {
+      if (r->hit[l]) r->hit[l]->refs--;
+      uint8_t* block = r->result[l];
+      if (!block) continue;
+      const uint64_t bytes = r->req.npoints * kResultBytes;
+      const float* light = r->lights.data() + 16 * l;
+      if (r->req.cache_key && !stack && !find_entry(s, r->req, light)) {
+        auto e = std::make_unique<CacheEntry>();
+        e->key = r->req.cache_key;
+        std::memcpy(e->geometry, light, sizeof(e->geometry));
+        e->npoints = r->req.npoints;
+        e->scene = r->req.scene;
+        e->hierarchy = r->req.hierarchy;
+        e->dev = block;
+        e->bytes = bytes;
+        e->lru = s->lru.insert(s->lru.end(), e.get());
+        s->cache.emplace(e->key, std::move(e));
+      } else {
+        cudaFreeAsync(block, slot.stream);
+        s->in_use -= bytes;
+      }
+    }
+    cudaFreeAsync(r->d_receivers, slot.stream);
+    if (r->d_lights) cudaFreeAsync(r->d_lights, slot.stream);
+    complete_locked(s, r, stack ? CC_ERR_STACK : CC_OK, stack ? "a traversal stack overflowed" : "");
+  }
+  release_slot(s, slot);
+}
+
+// Undoes a launch that failed while being built: its requests fail. (Called
+// without s->mu.)
+void abandon(cc_server* s, Slot& slot, int status, const std::string& error) {
+  cudaStreamSynchronize(slot.stream);
+  std::lock_guard<std::mutex> g(s->mu);
+  for (Request* r : slot.reqs) {
+    for (size_t l = 0; l < r->result.size(); ++l) {
+      if (r->hit[l]) r->hit[l]->refs--;
+      if (r->result[l]) {
+        cudaFreeAsync(r->result[l], slot.stream);
+        s->in_use -= r->req.npoints * kResultBytes;
+      }
+    }
+    if (r->d_receivers) cudaFreeAsync(r->d_receivers, slot.stream);
+    if (r->d_lights) cudaFreeAsync(r->d_lights, slot.stream);
+    complete_locked(s, r, status, error);
+  }
+  release_slot(s, slot);
+}
+
+#define SRV_CUDA(call, what)                                                       \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      abandon(s, slot, e_ == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA, \
+              std::string(what) + ": " + cudaGetErrorString(e_));                  \
+      return;                                                                      \
+    }                                                                              \
+  } while (0)
+
+// Builds and enqueues one launch on `slot` from the requests admitted to it
+// (their memory already counted in in_use). Called without s->mu: the
+// requests and the slot belong to the loop thread until the launch retires.
+void launch(cc_server* s, Slot& slot) {
+  cudaStream_t st = slot.stream;
+  std::vector<cc::JobGpu> jobs;
+  uint64_t points = 0, cones = 0, packet = 0;
+  const uint32_t pw = s->opt.points_per_warp;
+  cc_options d;
+  cc_options_default(&d);
+  for (Request* r : slot.reqs) {
+    const cc_request& q = r->req;
+    const uint64_t P = q.npoints;
+    cudaError_t e = cudaSuccess;
+    r->d_receivers = static_cast<float4*>(pool_alloc(s, P * 32, st, &e));
+    SRV_CUDA(e, "request receivers");
+    SRV_CUDA(cudaMemcpyAsync(r->d_receivers, q.receivers, P * 32, cudaMemcpyHostToDevice, st), "request receivers");
+    r->traced.clear();
+    for (size_t l = 0; l < r->result.size(); ++l)
+      if (!r->hit[l]) r->traced.insert(r->traced.end(), r->lights.begin() + 16 * l, r->lights.begin() + 16 * (l + 1));
+    if (!r->traced.empty()) {
+      r->d_lights = static_cast<float4*>(pool_alloc(s, r->traced.size() * 4, st, &e));
+      SRV_CUDA(e, "request lights");
+      SRV_CUDA(cudaMemcpyAsync(r->d_lights, r->traced.data(), r->traced.size() * 4, cudaMemcpyHostToDevice, st),
+               "request lights");
+    }
+    const cc_scene* sc = r->scene;
+    uint32_t t = 0;
+    for (size_t l = 0; l < r->result.size(); ++l) {
+      if (r->hit[l]) continue;
+      uint8_t* block = static_cast<uint8_t*>(pool_alloc(s, P * kResultBytes, st, &e));
+      SRV_CUDA(e, "request results");
+      r->result[l] = block;
+      cc::JobGpu j{};
+      j.scene = sc->dev();
+      j.query.receivers = r->d_receivers;
+      j.query.lights = r->d_lights + 4 * t;
+      j.query.npoints = P;
+      j.query.nlights = 1;
+      j.query.hierarchy = q.hierarchy;
+      j.query.wide_extent = d.wide_extent;
+      j.query.light_cone_cap = d.light_cone_cap;
+      j.query.wide_cone_cap = d.wide_cone_cap;
+      j.full = reinterpret_cast<uint2*>(block);
+      j.any = reinterpret_cast<uint2*>(block + 8 * P);
+      j.irradiance = reinterpret_cast<float*>(block + 16 * P);
+      j.fraction = reinterpret_cast<float*>(block + 20 * P);
+      if (!sc->flat.nodes.empty())
+        for (int k = 0; k < 3; ++k) {
+          j.lo[k] = sc->flat.nodes[0].lo[k];
+          j.hi[k] = sc->flat.nodes[0].hi[k];
+        }
+      j.packet_start = packet;
+      j.cone_start = cones;
+      j.point_start = points;
+      packet += (P + pw - 1) / pw;
+      cones += P;
+      points += P;
+      jobs.push_back(j);
+      ++t;
+    }
+  }
+  // Launch scratch: job table, redo list, walk order and its sort, counters.
+  if (!jobs.empty()) {
+    cudaError_t e = cudaSuccess;
+    if (slot.host_jobs_cap < jobs.size()) {
+      if (slot.host_jobs) cudaFreeHost(slot.host_jobs);
+      slot.host_jobs = nullptr;
+      slot.host_jobs_cap = 0;
+      SRV_CUDA(cudaMallocHost(&slot.host_jobs, jobs.size() * 2 * sizeof(cc::JobGpu)), "job table staging");
+      slot.host_jobs_cap = jobs.size() * 2;
+    }
+    std::memcpy(slot.host_jobs, jobs.data(), jobs.size() * sizeof(cc::JobGpu));
+    const uint64_t sort_bytes = cc::batch_order_scratch_bytes(points);
+    void* d_jobs = pool_alloc(s, jobs.size() * sizeof(cc::JobGpu), st, &e);
+    SRV_CUDA(e, "job table");
+    slot.scratch.push_back(d_jobs);
+    void* d_redo = pool_alloc(s, cones * 4, st, &e);
+    SRV_CUDA(e, "redo list");
+    slot.scratch.push_back(d_redo);
+    void* d_order = pool_alloc(s, points * 4, st, &e);
+    SRV_CUDA(e, "walk order");
+    slot.scratch.push_back(d_order);
+    void* d_sort = pool_alloc(s, sort_bytes, st, &e);
+    SRV_CUDA(e, "sort scratch");
+    slot.scratch.push_back(d_sort);
+    void* d_counters = pool_alloc(s, cc::kCounterWords * 4, st, &e);
+    SRV_CUDA(e, "counters");
+    slot.scratch.push_back(d_counters);
+    SRV_CUDA(cudaMemcpyAsync(d_jobs, slot.host_jobs, jobs.size() * sizeof(cc::JobGpu), cudaMemcpyHostToDevice, st),
+             "job table upload");
+    SRV_CUDA(cudaMemsetAsync(d_counters, 0, cc::kCounterWords * 4, st), "counter reset");
+    cc::BatchLaunch L{};
+    L.jobs = static_cast<const cc::JobGpu*>(d_jobs);
+    L.njobs = (uint32_t)jobs.size();
+    L.packets = packet;
+    L.points = points;
+    L.pw = pw;
+    SRV_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
+    L.order = static_cast<const uint32_t*>(d_order);
+    uint32_t* counters = static_cast<uint32_t*>(d_counters);
+    cc::DevOut o{};
+    o.redo_count = counters;
+    o.error = counters + 1;
+    o.next_packet = counters + 2;
+    o.next_solo = counters + 3;
+    o.redo_list = static_cast<uint32_t*>(d_redo);
+    o.redo_capacity = (uint32_t)std::max<uint64_t>(cones, 1);
+    SRV_CUDA(cc::launch_batch(L, o, false, s->ctx->sm_count, (int)s->opt.blocks_per_sm, st), "launch");
+    SRV_CUDA(cudaMemcpyAsync(slot.status, counters, cc::kCounterWords * 4, cudaMemcpyDeviceToHost, st), "status");
+  } else {
+    std::fill(slot.status, slot.status + cc::kCounterWords, 0u);
+  }
+  // Results to the requests' host buffers, light-major.
+  for (Request* r : slot.reqs) {
+    const cc_request& q = r->req;
+    const uint64_t P = q.npoints;
+    for (size_t l = 0; l < r->result.size(); ++l) {
+      const uint8_t* src = r->result[l] ? r->result[l] : r->hit[l]->dev;
+      if (q.full) SRV_CUDA(cudaMemcpyAsync(q.full + 2 * P * l, src, 8 * P, cudaMemcpyDeviceToHost, st), "results");
+      if (q.any) SRV_CUDA(cudaMemcpyAsync(q.any + 2 * P * l, src + 8 * P, 8 * P, cudaMemcpyDeviceToHost, st), "results");
+      if (q.irradiance)
+        SRV_CUDA(cudaMemcpyAsync(q.irradiance + P * l, src + 16 * P, 4 * P, cudaMemcpyDeviceToHost, st), "results");
+      if (q.fraction)
+        SRV_CUDA(cudaMemcpyAsync(q.fraction + P * l, src + 20 * P, 4 * P, cudaMemcpyDeviceToHost, st), "results");
+    }
+  }
+  SRV_CUDA(cudaEventRecord(slot.done, st), "launch event");
+  std::lock_guard<std::mutex> g(s->mu);
+  s->launches++;
+}
+
+// Takes requests off the queue's front for a launch while they fit: the
+// budget (after evicting unused cache entries) and the launch's cone limit.
+// Returns the requests taken and the bytes their results hold. (s->mu held.)
+std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_bytes, uint64_t* total_bytes) {
+  std::vector<Request*> taken;
+  uint64_t cones = 0;
+  *result_bytes = *total_bytes = 0;
+  while (!s->queue.empty()) {
+    Request* r = s->queue.front();
+    const cc_request& q = r->req;
+    // Lighting-cache lookups (entries found stay referenced by this launch).
+    std::vector<CacheEntry*> hit(q.nlights, nullptr);
+    uint64_t traced = 0;
+    for (uint32_t l = 0; l < q.nlights; ++l) {
+      if (q.cache_key) hit[l] = find_entry(s, q, r->lights.data() + 16 * l);
+      if (!hit[l]) ++traced;
+    }
+    const uint64_t c = traced * q.npoints;
+    if (!taken.empty() && cones + c > s->opt.max_launch_cones) break;
+    for (CacheEntry* e : hit)
+      if (e) e->refs++;  // keep them through make_room
+    const uint64_t need = request_bytes(q, traced);
+    if (!make_room(s, need, stream)) {
+      for (CacheEntry* e : hit)
+        if (e) e->refs--;
+      break;
+    }
+    for (CacheEntry* e : hit)
+      if (e) touch(s, e);
+    s->queue.pop_front();
+    r->hit = std::move(hit);
+    r->result.assign(q.nlights, nullptr);
+    r->t_admit = Clock::now();
+    r->scene = s->scenes[q.scene];
+    r->stats.cached_lights = (uint32_t)(q.nlights - traced);
+    s->cached_lights += q.nlights - traced;
+    s->traced_lights += traced;
+    s->in_use += need;
+    s->peak = std::max(s->peak, s->in_use);
+    *result_bytes += traced * q.npoints * kResultBytes;
+    *total_bytes += need;
+    taken.push_back(r);
+    cones += c;
+  }
+  for (Request* r : taken) r->stats.launch_requests = (uint32_t)taken.size();
+  return taken;
+}
+
+void run_loop(cc_server* s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    bool any_busy = false;
+    for (Slot& slot : s->slots) {
+      if (!slot.busy) continue;
+      if (cudaEventQuery(slot.done) == cudaSuccess) retire(s, slot);
+      else any_busy = true;
+    }
+    if (s->stop && s->queue.empty() && !any_busy) break;
+    Slot* free_slot = nullptr;
+    for (Slot& slot : s->slots)
+      if (!slot.busy) {
+        free_slot = &slot;
+        break;
+      }
+    if (free_slot && !s->queue.empty()) {
+      uint64_t result_bytes = 0, total_bytes = 0;
+      std::vector<Request*> taken = admit(s, free_slot->stream, &result_bytes, &total_bytes);
+      if (!taken.empty()) {
+        // Result blocks are released one by one (or kept as cache entries);
+        // the rest of the admitted bytes are released with the launch.
+        free_slot->scratch_bytes = total_bytes - result_bytes;
+        free_slot->reqs = std::move(taken);
+        free_slot->busy = true;
+        lk.unlock();
+        launch(s, *free_slot);
+        lk.lock();
+        continue;
+      }
+      if (!any_busy) {
+        // Nothing in flight and the cache emptied, yet the front request does
+        // not fit: it never will.
+        Request* r = s->queue.front();
+        s->queue.pop_front();
+        s->refused++;
+        r->t_admit = Clock::now();
+        complete_locked(s, r, CC_ERR_BUSY, "the request does not fit the server's memory budget");
+        continue;
+      }
+    }
+    if (any_busy) {
+      lk.unlock();
+      std::this_thread::sleep_for(std::chrono::microseconds(100));
+      lk.lock();
+    } else if (s->queue.empty() && !s->stop) {
+      s->wake.wait_for(lk, std::chrono::milliseconds(50));
+    }
+  }
+}
+
+}  // namespace
+
+void cc_server_options_default(cc_server_options* opt) {
+  if (!opt) return;
+  opt->hbm_budget = 8ull << 30;
+  opt->max_inflight = 4;
+  opt->max_queue = 256;
+  opt->max_launch_cones = 8ull << 20;
+  opt->points_per_warp = 32;
+  opt->blocks_per_sm = cc::kBlocksPerSm;
+}
+
+int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server** out) {
+  if (!ctx || !out) return fail(CC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  cc_server_options opt;
+  if (opt_in) opt = *opt_in; else cc_server_options_default(&opt);
+  if (opt.max_inflight < 1 || opt.max_inflight > 8) return fail(CC_ERR_INVALID, "max_inflight must be 1..8");
+  if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
+  if (opt.blocks_per_sm < 1 || opt.blocks_per_sm > (uint32_t)cc::kBlocksPerSm)
+    return fail(CC_ERR_INVALID, "blocks_per_sm must be 1..4");
+  if (opt.max_queue < 1 || opt.hbm_budget == 0 || opt.max_launch_cones == 0)
+    return fail(CC_ERR_INVALID, "zero queue, budget or launch size");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  cc_server* s = new cc_server;
+  s->ctx = ctx;
+  s->opt = opt;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
+  if (e == cudaSuccess) {
+    uint64_t keep = ~0ull;  // keep freed memory in the pool for reuse
+    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  s->slots.resize(opt.max_inflight);
+  for (Slot& slot : s->slots) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&slot.status, cc::kCounterWords * sizeof(uint32_t));
+  }
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "server setup");
+    cc_server_destroy(s);
+    return rc;
+  }
+  s->loop = std::thread(run_loop, s);
+  *out = s;
+  return CC_OK;
+}
+
+int cc_server_destroy(cc_server* s) {
+  if (!s) return CC_OK;
+  if (s->loop.joinable()) {
+    {
+      std::lock_guard<std::mutex> g(s->mu);
+      s->stop = true;
+    }
+    s->wake.notify_all();
+    s->loop.join();
+  }
+  cudaSetDevice(s->ctx->device);
+  if (!s->slots.empty() && s->slots[0].stream)
+    for (auto& kv : s->cache) cudaFreeAsync(kv.second->dev, s->slots[0].stream);
+  for (Slot& slot : s->slots) {
+    if (slot.stream) cudaStreamSynchronize(slot.stream);
+    if (slot.host_jobs) cudaFreeHost(slot.host_jobs);
+    if (slot.status) cudaFreeHost(slot.status);
+    if (slot.done) cudaEventDestroy(slot.done);
+    if (slot.stream) cudaStreamDestroy(slot.stream);
+  }
+  if (s->pool) cudaMemPoolDestroy(s->pool);
+  delete s;
+  return CC_OK;
+}
+
+int cc_server_add_scene(cc_server* s, const cc_scene* scene, uint32_t* id) {
+  if (!s || !scene) return fail(CC_ERR_INVALID, "null argument");
+  if (scene->ctx != s->ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
+  std::lock_guard<std::mutex> g(s->mu);
+  if (id) *id = (uint32_t)s->scenes.size();
+  s->scenes.push_back(scene);
+  return CC_OK;
+}
+
+int cc_server_submit(cc_server* s, const cc_request* req, uint64_t* ticket) {
+  if (!s || !req) return fail(CC_ERR_INVALID, "null argument");
+  if ((req->npoints && !req->receivers) || (req->nlights && !req->lights))
+    return fail(CC_ERR_INVALID, "null inputs");
+  if (req->hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
+  if (req->npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one request");
+  if (request_cones(*req) >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one request");
+  auto r = std::make_unique<Request>();
+  r->req = *req;
+  r->lights.assign(req->lights, req->lights + 16 * (size_t)req->nlights);
+  r->t_submit = Clock::now();
+  std::lock_guard<std::mutex> g(s->mu);
+  if (req->scene >= s->scenes.size()) return fail(CC_ERR_INVALID, "unknown scene");
+  if (s->queue.size() >= s->opt.max_queue) {
+    s->refused++;
+    return fail(CC_ERR_BUSY, "the server's queue is full");
+  }
+  if (request_bytes(*req, req->nlights) > s->opt.hbm_budget) {
+    s->refused++;
+    return fail(CC_ERR_BUSY, "the request alone exceeds the server's memory budget");
+  }
+  r->ticket = s->next_ticket++;
+  if (ticket) *ticket = r->ticket;
+  s->queue.push_back(r.get());
+  s->requests.emplace(r->ticket, std::move(r));
+  s->wake.notify_all();
+  return CC_OK;
+}
+
+int cc_server_wait(cc_server* s, uint64_t ticket, uint32_t timeout_ms, cc_request_stats* stats) {
+  if (!s) return fail(CC_ERR_INVALID, "null argument");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->requests.find(ticket);
+  if (it == s->requests.end()) return fail(CC_ERR_INVALID, "unknown ticket");
+  Request* r = it->second.get();
+  if (!s->finished.wait_for(lk, std::chrono::milliseconds(timeout_ms), [r] { return r->done; }))
+    return fail(CC_ERR_TIMEOUT, "the request has not finished");
+  const int status = r->status;
+  const std::string error = r->error;
+  if (stats) *stats = r->stats;
+  s->requests.erase(it);
+  if (status != CC_OK) return fail(status, error);
+  return CC_OK;
+}
+
+int cc_server_stats(cc_server* s, uint64_t out8[8]) {
+  if (!s || !out8) return fail(CC_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(s->mu);
+  out8[0] = s->completed;
+  out8[1] = s->refused;
+  out8[2] = s->launches;
+  out8[3] = s->cached_lights;
+  out8[4] = s->traced_lights;
+  out8[5] = s->in_use;
+  out8[6] = s->peak;
+  out8[7] = s->cache.size();
+  return CC_OK;
+}

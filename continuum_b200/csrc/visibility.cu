@@ -397,12 +397,27 @@ __device__ __noinline__ float warp_blocked(const Cone& mine, f3 my_normal, bool 
   return sum;
 }
 
-template <bool kCount>
+// The job of a batch that holds `key` (a packet or a cone number): the last
+// job whose start is at most `key`. Warp-uniform.
+__device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, uint32_t njobs, uint64_t key,
+                                             bool by_cone) {
+  uint32_t lo = 0, hi = njobs;  // jobs[lo].start <= key < jobs[hi].start
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const uint64_t start = by_cone ? __ldg(&jobs[mid].cone_start) : __ldg(&jobs[mid].packet_start);
+    if (start <= key) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// kBatch: the cones of every job of a batch (BatchLaunch); each packet's job
+// is looked up in the job table, and the redo list holds batch cone numbers.
+template <bool kCount, bool kBatch>
 // kBlocksPerSm blocks fit the shared memory; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
-    visibility_kernel(DevScene s, DevQuery q, DevOut o, const uint32_t* __restrict__ list,
-                      const uint32_t* __restrict__ list_count, uint32_t pw) {
+    visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
+                      const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -411,8 +426,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
   ws->span_lo[lane] = 68u;
   ws->span_hi[lane] = 0u;
 
-  const uint64_t ncones = list ? (uint64_t)min(*list_count, o.redo_capacity) : q.npoints * (uint64_t)q.nlights;
-  const uint64_t npackets = (ncones + pw - 1) / pw;
+  const uint64_t plain_cones = q_plain.npoints * (uint64_t)q_plain.nlights;
+  uint64_t npackets;
+  if (list) npackets = (uint64_t)min(*list_count, o.redo_capacity);  // one cone per packet
+  else npackets = kBatch ? batch.packets : (plain_cones + pw - 1) / pw;
   // Packets are taken from a shared counter as warps finish: their costs
   // differ by two orders of magnitude, so a fixed assignment leaves most
   // warps idle behind the slowest.
@@ -422,13 +439,43 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     if (lane == 0) packet = atomicAdd(next, 1u);
     packet = __shfl_sync(0xffffffffu, packet, 0);
     if (packet >= npackets) break;
-    const uint64_t wbase = (uint64_t)packet * pw;
+    // The packet's job: its scene, query and outputs.
+    DevScene s = s_plain;
+    DevQuery q = q_plain;
+    uint2* out_full = o.full;
+    uint2* out_any = o.any;
+    float* out_partial = o.partial;
+    float* out_irradiance = o.irradiance;
+    float* out_fraction = o.fraction;
+    uint4* out_work = o.work;
+    uint64_t cone_start = 0;  // the job's first cone in the batch's numbering
+    uint64_t ncones = plain_cones;
+    uint64_t wbase = (uint64_t)packet * pw;
+    uint64_t listed = 0;
+    if (list) listed = list[packet];
+    if constexpr (kBatch) {
+      const uint32_t j = list ? find_job(batch.jobs, batch.njobs, listed, true)
+                              : find_job(batch.jobs, batch.njobs, packet, false);
+      const JobGpu* J = batch.jobs + j;
+      s = J->scene;
+      q = J->query;
+      q.order = batch.order ? batch.order + J->point_start : nullptr;
+      out_full = J->full;
+      out_any = J->any;
+      out_partial = J->partial;
+      out_irradiance = J->irradiance;
+      out_fraction = J->fraction;
+      out_work = J->work;
+      cone_start = J->cone_start;
+      ncones = q.npoints * (uint64_t)q.nlights;
+      if (!list) wbase = (packet - J->packet_start) * (uint64_t)pw;
+    }
     const uint64_t slot = wbase + lane;
-    const bool valid = (uint32_t)lane < pw && slot < ncones;
+    const bool valid = list ? lane == 0 : ((uint32_t)lane < pw && slot < ncones);
     uint64_t c = 0;
     if (valid) {
       if (list) {
-        c = list[slot];
+        c = listed - cone_start;
       } else if (q.order) {
         const uint64_t light_base = (slot / q.npoints) * q.npoints;
         c = light_base + __ldg(&q.order[slot - light_base]);
@@ -535,18 +582,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const bool redo = !list && o.redo_list && (st.status & 4u) && (st.status & (1u | 16u));
     if (redo) {
       const uint32_t at = atomicAdd(o.redo_count, 1u);
-      if (at < o.redo_capacity) o.redo_list[at] = (uint32_t)c;
+      if (at < o.redo_capacity) o.redo_list[at] = (uint32_t)(cone_start + c);
       else atomicOr(o.error, 1u);
     }
     if (st.status & 2u) atomicOr(o.error, 2u);
     if (valid && !redo) {
-      if (o.full) o.full[c] = make_uint2(fw0, fw1);
-      if (o.any) o.any[c] = make_uint2(aw0, aw1);
-      if (o.irradiance) o.irradiance[c] = value;
-      if (o.fraction) o.fraction[c] = ratio;
-      if (o.work) o.work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
-      if (o.partial) {
-        float4* dst = reinterpret_cast<float4*>(o.partial + 64 * c);
+      if (out_full) out_full[c] = make_uint2(fw0, fw1);
+      if (out_any) out_any[c] = make_uint2(aw0, aw1);
+      if (out_irradiance) out_irradiance[c] = value;
+      if (out_fraction) out_fraction[c] = ratio;
+      if (out_work) out_work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
+      if (out_partial) {
+        float4* dst = reinterpret_cast<float4*>(out_partial + 64 * c);
 #pragma unroll 4
         for (int k = 0; k < 16; ++k)
           dst[k] = make_float4(st.cov[32 * (4 * k)], st.cov[32 * (4 * k + 1)], st.cov[32 * (4 * k + 2)],
@@ -565,21 +612,24 @@ cudaError_t upload_disk_table(const float* table64) {
 
 // Whether the large dynamic shared memory size was allowed, per device and
 // kernel variant (the attribute is set per device).
-static uint64_t g_attr_set[2] = {0, 0};
+static uint64_t g_attr_set[4] = {0, 0, 0, 0};
 
-template <bool kCount>
-static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const uint32_t* list,
-                              const uint32_t* list_count, uint32_t pw, uint32_t blocks, cudaStream_t stream) {
+template <bool kCount, bool kBatch>
+static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
+                              const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
+                              cudaStream_t stream) {
   const size_t smem = (size_t)kWarpsPerBlock * sizeof(WarpShared);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
-  if (!(g_attr_set[kCount] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0);
+  if (!(g_attr_set[variant] & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    g_attr_set[kCount] |= bit;
+    g_attr_set[variant] |= bit;
   }
-  visibility_kernel<kCount><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, list, list_count, pw);
+  visibility_kernel<kCount, kBatch><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
   return cudaGetLastError();
 }
 
@@ -601,19 +651,38 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   // One resident wave: warps take packets from the shared counter.
   const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-  cudaError_t e = count ? launch_one<true>(s, q, o, nullptr, nullptr, pw, blocks, stream)
-                        : launch_one<false>(s, q, o, nullptr, nullptr, pw, blocks, stream);
+  const BatchLaunch none{};
+  cudaError_t e = count ? launch_one<true, false>(s, q, o, none, nullptr, nullptr, pw, blocks, stream)
+                        : launch_one<false, false>(s, q, o, none, nullptr, nullptr, pw, blocks, stream);
   if (marks) cudaEventRecord(marks[1], stream);
   if (e != cudaSuccess) return e;
   if (o.redo_list) {
     // The listed cones, each walked alone (one cone per warp; the warp still
     // shares its leaves' triangles).
     const uint32_t solo_blocks = (uint32_t)sm_count * kBlocksPerSm;
-    e = count ? launch_one<true>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream)
-              : launch_one<false>(s, q, o, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+    e = count ? launch_one<true, false>(s, q, o, none, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+              : launch_one<false, false>(s, q, o, none, o.redo_list, o.redo_count, 1, solo_blocks, stream);
   }
   if (marks) cudaEventRecord(marks[2], stream);
   return e;
+}
+
+cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count, int sm_count, int blocks_per_sm,
+                         cudaStream_t stream) {
+  if (b.njobs == 0 || b.packets == 0) return cudaSuccess;
+  if (blocks_per_sm < 1) blocks_per_sm = 1;
+  if (blocks_per_sm > kBlocksPerSm) blocks_per_sm = kBlocksPerSm;
+  const DevScene s{};
+  const DevQuery q{};
+  const uint64_t want = (b.packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const uint64_t cap = (uint64_t)sm_count * blocks_per_sm;
+  const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
+  cudaError_t e = count ? launch_one<true, true>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
+                        : launch_one<false, true>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+  if (e != cudaSuccess || !o.redo_list) return e;
+  const uint32_t solo_blocks = (uint32_t)cap;
+  return count ? launch_one<true, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+               : launch_one<false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
 }
 
 }  // namespace cc

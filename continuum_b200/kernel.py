@@ -396,6 +396,155 @@ class MaskConeKernel:
                                           C.c_void_p(stream) if stream else None))
 
 
+class Batch:
+    """Many visibility jobs solved by one persistent launch (cc_batch_*).
+
+    Jobs take device pointers (ints) for their receivers, lights and outputs,
+    which must stay valid while the batch is submitted. Each job's results
+    equal a visibility_device call for that job alone.
+    """
+
+    def __init__(self, kernel: MaskConeKernel):
+        h = C.c_void_p()
+        check(load().cc_batch_create(kernel.handle, C.byref(h)))
+        self._h = h
+        self.kernel = kernel
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("batch is closed")
+        return self._h
+
+    def add(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int, outputs: dict,
+            hierarchy=Hierarchy.TRIANGLES) -> int:
+        o = _lib.Outputs(*(outputs.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.kernel.options(hierarchy)
+        job = C.c_uint32()
+        check(load().cc_batch_add(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints),
+                                  C.c_void_p(d_lights), int(nlights), C.byref(opt), C.byref(o), C.byref(job)))
+        return int(job.value)
+
+    @staticmethod
+    def options(points_per_warp: int = 32, blocks_per_sm: int = 4, flags: int = _lib.CC_BATCH_GRAPH):
+        return _lib.BatchOptions(int(points_per_warp), int(blocks_per_sm), int(flags))
+
+    def submit(self, options=None, stream: int = 0) -> None:
+        opt = options if options is not None else self.options()
+        check(load().cc_batch_submit(self.handle, C.byref(opt), C.c_void_p(stream) if stream else None))
+
+    def wait(self, timeout_ms: int = 600_000) -> None:
+        check(load().cc_batch_wait(self.handle, int(timeout_ms)))
+
+    def tune(self, reps: int = 2, flags: int = _lib.CC_BATCH_GRAPH):
+        """The autotuner: (best options, each candidate's milliseconds)."""
+        base = self.options(flags=flags)
+        best = _lib.BatchOptions()
+        ms = np.zeros(64, np.float32)
+        n = load().cc_batch_tune(self.handle, C.byref(base), int(reps), C.byref(best), ptr(ms), 64)
+        if n < 0:
+            check(-n)
+        return best, ms[:n]
+
+    def sizes(self) -> dict:
+        out = np.zeros(4, np.uint64)
+        check(load().cc_batch_sizes(self.handle, ptr(out)))
+        return {"jobs": int(out[0]), "points": int(out[1]), "cones": int(out[2]), "device_bytes": int(out[3])}
+
+    def clear(self) -> None:
+        check(load().cc_batch_clear(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().cc_batch_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The served form (cc_server_*): a native request loop with continuous
+    batching, admission against a device-memory budget and a resident
+    lighting cache. Requests take host arrays, which the server's thread
+    reads and writes until the request completes (pinned memory lets the
+    copies overlap with other launches)."""
+
+    def __init__(self, kernel: MaskConeKernel, hbm_budget: int = 8 << 30, max_inflight: int = 4,
+                 max_queue: int = 256, max_launch_cones: int = 8 << 20, points_per_warp: int = 32,
+                 blocks_per_sm: int = 4):
+        opt = _lib.ServerOptions(int(hbm_budget), int(max_inflight), int(max_queue), int(max_launch_cones),
+                                 int(points_per_warp), int(blocks_per_sm))
+        h = C.c_void_p()
+        check(load().cc_server_create(kernel.handle, C.byref(opt), C.byref(h)))
+        self._h = h
+        self.kernel = kernel
+        self._live = {}  # ticket -> the arrays the request reads and writes
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("server is closed")
+        return self._h
+
+    def add_scene(self, scene: Scene) -> int:
+        i = C.c_uint32()
+        check(load().cc_server_add_scene(self.handle, scene.handle, C.byref(i)))
+        return int(i.value)
+
+    def submit(self, scene_id: int, receivers: np.ndarray, lights: np.ndarray, outputs: dict,
+               hierarchy=Hierarchy.TRIANGLES, cache_key: int = 0) -> int:
+        """Queues a request; outputs maps full/any (uint64 [L, P]) and
+        irradiance/fraction (float32 [L, P]) to host arrays. Raises CCError
+        (CC_ERR_BUSY) when the queue is full."""
+        rec = np.ascontiguousarray(receivers, np.float32)
+        lig = np.ascontiguousarray(lights, np.float32).reshape(-1, 16)
+        for k, v in outputs.items():
+            if not v.flags["C_CONTIGUOUS"] or v.size < rec.shape[0] * lig.shape[0]:
+                raise ValueError(f"output {k} must be C-contiguous with a value per cone")
+        req = _lib.Request(int(scene_id), ptr(rec), rec.shape[0], ptr(lig), lig.shape[0],
+                           int(Hierarchy.of(hierarchy)), int(cache_key),
+                           *(ptr(outputs.get(k)) for k in ("full", "any", "irradiance", "fraction")))
+        t = C.c_uint64()
+        check(load().cc_server_submit(self.handle, C.byref(req), C.byref(t)))
+        self._live[int(t.value)] = (rec, lig, outputs)
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_ms: int = 600_000) -> dict:
+        st = _lib.RequestStats()
+        try:
+            check(load().cc_server_wait(self.handle, int(ticket), int(timeout_ms), C.byref(st)))
+        except CCError as e:
+            if e.code != _lib.CC_ERR_TIMEOUT:
+                self._live.pop(int(ticket), None)
+            raise
+        self._live.pop(int(ticket), None)
+        return {"queued_ms": st.queued_ms, "total_ms": st.total_ms, "launch_requests": st.launch_requests,
+                "cached_lights": st.cached_lights}
+
+    def stats(self) -> dict:
+        out = np.zeros(8, np.uint64)
+        check(load().cc_server_stats(self.handle, ptr(out)))
+        keys = ("completed", "refused", "launches", "cached_lights", "traced_lights", "bytes_in_use", "peak_bytes",
+                "cache_entries")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().cc_server_destroy(self._h)
+            self._h = C.c_void_p(None)
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def kernel_times(kernel: MaskConeKernel, max_calls: int = 256) -> np.ndarray:
     """(calls, 2) milliseconds of the packet and solo passes of the
     visibility calls since the last query (waits for them)."""

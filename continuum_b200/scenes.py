@@ -300,3 +300,142 @@ def primary_hits(w: Workload, width: int, height: int, camera: Optional[np.ndarr
     finally:
         s.close()
     return np.ascontiguousarray(rec[hit.astype(bool)])
+
+
+def _shape_pool(subdivisions: int, count: int, seed: int) -> list:
+    """`count` unit displaced icospheres (radius 1, centred at the origin)."""
+    return [displaced_icosphere((0.0, 0.0, 0.0), 1.0, seed=seed * 7919 + k, subdivisions=subdivisions)
+            for k in range(count)]
+
+
+def _field(rng: Pcg32, target_tris: float, pools: dict, pool: int, seed: int):
+    """A field of displaced icospheres with about `target_tris` triangles on a
+    ground quad; its area grows with the sphere count, so the density stays
+    near icosphere_field's. Returns (meshes, half extent)."""
+    sub = 5 if target_tris >= 150_000 else (4 if target_tris >= 20_000 else 3)
+    per = 20 * 4 ** sub
+    n = max(1, int(round((target_tris - 2) / per)))
+    if sub not in pools:
+        pools[sub] = _shape_pool(sub, pool, seed * 100 + sub)
+    half = max(10.0, 50.0 * math.sqrt(n / 150.0))
+    meshes = [ground_quad(max(1000.0, 20.0 * half))]
+    for _ in range(n):
+        r = rng.uniform(0.5, 3.0)
+        cx, cz = rng.uniform(-half, half), rng.uniform(-half, half)
+        shape = pools[sub][rng.next_u32() % pool]
+        meshes.append((shape * np.float32(r) + np.array([cx, r, cz], np.float32)).astype(np.float32))
+    return meshes, half
+
+
+def _random_light(rng: Pcg32, half: float) -> Light:
+    """A rect or disk light of size U[0.25, 4] m, 8-20 m up, tilted up to 30
+    degrees from straight down, over the middle of a field."""
+    h = rng.uniform(8.0, 20.0)
+    x, z = rng.uniform(-0.8 * half, 0.8 * half), rng.uniform(-0.8 * half, 0.8 * half)
+    nrm, u, v = _tilted_frame(rng, 30.0)
+    centre = np.array([x, h, z])
+    if rng.next_u32() & 1:
+        eu, ev = u * rng.uniform(0.25, 4.0), v * rng.uniform(0.25, 4.0)
+        if np.dot(np.cross(eu, ev), nrm) < 0:
+            ev = -ev
+        corner = centre - 0.5 * (eu + ev)
+        return Light.rect(RectLight(tuple(corner), tuple(eu), tuple(ev), one_sided=True))
+    spot = Spot(axis=tuple(nrm), inner=math.radians(89.0), outer=math.radians(90.0))
+    return Light(SphereLight(tuple(centre), 0.5 * rng.uniform(0.25, 4.0), spot))
+
+
+def _camera(rng: Pcg32, half: float) -> np.ndarray:
+    az = 2.0 * math.pi * rng.next_f32()
+    d = 1.5 * half
+    return np.array([d * math.sin(az), 1.4 * half, -d * math.cos(az), 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 60.0], np.float32)
+
+
+def _image(points: float):
+    width = max(8, int(round(math.sqrt(points * 16.0 / 9.0))))
+    return width, max(8, int(round(points / width)))
+
+
+def batch_jobs(seed: int = 3, njobs: int = 64, tris=(10_000, 2_000_000), points=(4_000, 1_000_000),
+               lights=(1, 16), pool: int = 16) -> list:
+    """The batching workload: `njobs` jobs, each its own field of displaced
+    icospheres (value-noise displacement of 0.15 r, as icosphere_field) with a
+    triangle count log-uniform in `tris`, a light count uniform in `lights`
+    (rects and disks of sizes U[0.25, 4] m), and the primary hits of a seeded
+    camera with a point count log-uniform in `points` (misses dropped).
+    Spheres are drawn from a pool of `pool` displaced shapes per subdivision
+    level, scaled and placed per sphere."""
+    rng = Pcg32(seed, 33)
+    pools = {}
+    jobs = []
+    for i in range(njobs):
+        t = math.exp(rng.uniform(math.log(tris[0]), math.log(tris[1])))
+        meshes, half = _field(rng, t, pools, pool, seed)
+        nl = lights[0] + rng.next_u32() % (lights[1] - lights[0] + 1)
+        objs = [_random_light(rng, half) for _ in range(nl)]
+        width, height = _image(math.exp(rng.uniform(math.log(points[0]), math.log(points[1]))))
+        w = Workload(f"job{i}", meshes, np.stack([light_gpu(l) for l in objs]), None, objs, _camera(rng, half),
+                     (width, height))
+        w.receivers = primary_hits(w, width, height)
+        jobs.append(w)
+    return jobs
+
+
+@dataclass
+class ServedScene:
+    """A resident scene of the serving workload: its meshes, its 8 base
+    lights (16-float records) and the receivers of its seeded camera poses."""
+
+    meshes: list
+    lights: np.ndarray
+    poses: list
+    half: float = 0.0  # the field's half extent
+
+    @property
+    def ntris(self) -> int:
+        return int(sum(len(m) for m in self.meshes))
+
+
+def served_scenes(seed: int = 4, nscenes: int = 8, tris=(50_000, 3_000_000), poses: int = 3,
+                  points=(16_000, 2_000_000), pool: int = 16) -> list:
+    """The serving workload's resident scenes: `nscenes` displaced-icosphere
+    fields with triangle counts log-uniform in `tris`, 8 base lights each (as
+    batch_jobs'), and `poses` seeded camera poses per scene whose primary hits
+    number log-uniform in `points`."""
+    rng = Pcg32(seed, 44)
+    pools = {}
+    out = []
+    for i in range(nscenes):
+        t = math.exp(rng.uniform(math.log(tris[0]), math.log(tris[1])))
+        meshes, half = _field(rng, t, pools, pool, seed)
+        lights = np.stack([light_gpu(_random_light(rng, half)) for _ in range(8)])
+        sc = ServedScene(meshes, lights, [], half)
+        for _ in range(poses):
+            width, height = _image(math.exp(rng.uniform(math.log(points[0]), math.log(points[1]))))
+            w = Workload(f"scene{i}", meshes, lights, None, None, _camera(rng, half), (width, height))
+            sc.poses.append(primary_hits(w, width, height))
+        out.append(sc)
+    return out
+
+
+def served_requests(scenes_: list, n: int, seed: int = 5, moved: float = 0.5) -> list:
+    """`n` requests over `scenes_`: (scene index, pose index, lights [k, 16])
+    with k uniform in 1..8; each light is either one of the scene's base
+    lights recoloured (same geometry, new radiance) or, with probability
+    `moved`, a light moved to a new seeded place."""
+    rng = Pcg32(seed, 55)
+    reqs = []
+    for _ in range(n):
+        si = rng.next_u32() % len(scenes_)
+        sc = scenes_[si]
+        pi = rng.next_u32() % len(sc.poses)
+        k = 1 + rng.next_u32() % 8
+        recs = []
+        for j in range(k):
+            if rng.next_f32() < moved:
+                recs.append(light_gpu(_random_light(rng, sc.half)))
+            else:
+                rec = sc.lights[(j + rng.next_u32()) % 8].copy()
+                rec[12:15] = (rng.uniform(0.2, 5.0), rng.uniform(0.2, 5.0), rng.uniform(0.2, 5.0))
+                recs.append(rec)
+        reqs.append((si, pi, np.ascontiguousarray(np.stack(recs).astype(np.float32))))
+    return reqs

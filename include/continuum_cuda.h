@@ -191,6 +191,133 @@ CC_API int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* re
 CC_API int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
                                 uint32_t nlights, const cc_options* opt, const cc_outputs* out, void* stream);
 
+/* ---- Batched form -------------------------------------------------------
+ * Many visibility jobs (each its own scene, receivers, lights, options and
+ * outputs) solved by one persistent launch: a job table on the device, one
+ * Morton sort over every job's points, then warps take packets of any job
+ * from one device counter (a packet never straddles two jobs), so small and
+ * uneven jobs share the GPU instead of each leaving it idle behind its own
+ * tail. Each job's results equal cc_visibility's for that job alone.
+ * The reference's counterpart is its bake job list (vc_bake's job packing,
+ * mask_cones.wgsl:3433-3443), which packs many cache entries into one
+ * dispatch; it has no general batch of scenes. */
+typedef struct cc_batch cc_batch;
+
+#define CC_BATCH_GRAPH 8u /* replay submissions from a captured CUDA graph (cc_batch_options.flags) */
+
+typedef struct cc_batch_options {
+  uint32_t points_per_warp; /* cones per packet: 1..32 (32) */
+  uint32_t blocks_per_sm;   /* resident blocks per SM launched: 1..4 (4) */
+  uint32_t flags;           /* CC_KEEP_ORDER, CC_NO_REDO, CC_BATCH_GRAPH */
+} cc_batch_options;
+
+/* Defaults: 32 cones per packet, 4 blocks per SM, CC_BATCH_GRAPH. */
+CC_API void cc_batch_options_default(cc_batch_options* opt);
+
+CC_API int cc_batch_create(cc_context* ctx, cc_batch** out);
+CC_API int cc_batch_destroy(cc_batch* batch);
+/* Removes every job (the batch's device buffers are kept for reuse). */
+CC_API int cc_batch_clear(cc_batch* batch);
+/* Appends a job. Receivers, lights and outputs are device pointers that must
+ * stay valid while the batch is submitted; opt gives the job's hierarchy,
+ * wide extent and walk caps (its points_per_warp and flags are ignored: the
+ * batch's options apply). `job` (nullable) receives the job's index. At most
+ * 2^32 - 1 cones over all jobs. */
+CC_API int cc_batch_add(cc_batch* batch, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                        const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
+                        uint32_t* job);
+/* Enqueues the whole batch on `stream` (NULL: the context's stream) and
+ * returns. The first submission after a change of jobs or options sizes the
+ * batch's buffers and uploads the job table; with CC_BATCH_GRAPH it runs the
+ * work directly and captures it into a CUDA graph, and later submissions with
+ * the same jobs and options launch that graph. */
+CC_API int cc_batch_submit(cc_batch* batch, const cc_batch_options* opt, void* stream);
+/* Waits at most timeout_ms for the last submission: CC_ERR_TIMEOUT if it has
+ * not finished, CC_ERR_STACK if a traversal stack overflowed, else CC_OK. */
+CC_API int cc_batch_wait(cc_batch* batch, uint32_t timeout_ms);
+/* The autotuner: times every candidate launch configuration (cones per
+ * packet 8, 16, 32 x Morton or given walk order x 2 or 4 blocks per SM) on
+ * this batch, `reps` runs each, and writes the fastest to *best (keeping
+ * base->flags' CC_BATCH_GRAPH and CC_NO_REDO; base nullable). ms_out
+ * (nullable, max_candidates entries) receives each candidate's best time in
+ * candidate order. Returns the number of candidates, or minus a status.
+ * Results do not depend on the configuration. */
+CC_API int cc_batch_tune(cc_batch* batch, const cc_batch_options* base, uint32_t reps, cc_batch_options* best,
+                         float* ms_out, uint32_t max_candidates);
+/* jobs, points, cones, and device bytes the batch holds. */
+CC_API int cc_batch_sizes(const cc_batch* batch, uint64_t out4[4]);
+
+/* ---- Served form --------------------------------------------------------
+ * A request loop on its own host thread. Scenes stay resident; requests
+ * (a scene, receivers, 1 or more lights) queue on submission and are admitted
+ * in arrival order while launch slots and device memory under the server's
+ * budget allow. Each launch takes every admitted request (continuous
+ * batching: requests that arrive while earlier launches run join the next
+ * one, and up to max_inflight launches overlap on the device on their own
+ * streams); every (request, light) pair is one job of a batched launch.
+ * Results of a request with a nonzero cache_key stay on the device as a
+ * lighting cache, one entry per (cache_key, light geometry): a later request
+ * with the same key and a light of the same geometry (a recoloured light:
+ * only the radiance differs) is served from the entry without tracing.
+ * Entries are evicted least recently used when admission needs the memory.
+ * Each result equals cc_visibility's for that request alone.
+ * The reference has no request server; its nearest counterpart is the
+ * lighting cache's frame-budgeted bake (CacheOptions.bake_budget and
+ * frame_target_ms, crates/continuum/src/vcache.rs:183-207). */
+typedef struct cc_server cc_server;
+
+typedef struct cc_server_options {
+  uint64_t hbm_budget;       /* device bytes for requests in flight and cached results */
+  uint32_t max_inflight;     /* launches in flight at once: 1..8 (4) */
+  uint32_t max_queue;        /* queued requests before submissions are refused with CC_ERR_BUSY (256) */
+  uint64_t max_launch_cones; /* cones one launch takes at most (8M); one larger request runs alone */
+  uint32_t points_per_warp;  /* 1..32 (32) */
+  uint32_t blocks_per_sm;    /* 1..4 (4) */
+} cc_server_options;
+
+/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 8M cones per launch, 32, 4. */
+CC_API void cc_server_options_default(cc_server_options* opt);
+
+typedef struct cc_request {
+  uint32_t scene;            /* an index from cc_server_add_scene */
+  const float* receivers;    /* host, 8 floats per point (pinned memory lets the copies overlap) */
+  uint64_t npoints;
+  const float* lights;       /* host, 16 floats per light */
+  uint32_t nlights;
+  uint32_t hierarchy;        /* 0, 1 or 2 */
+  uint64_t cache_key;        /* 0: no caching; else names this receiver set for the lighting cache */
+  uint32_t* full;            /* host outputs, light-major as cc_visibility's (nullable); written when done */
+  uint32_t* any;
+  float* irradiance;
+  float* fraction;
+} cc_request;
+
+typedef struct cc_request_stats {
+  double queued_ms;          /* submission to admission */
+  double total_ms;           /* submission to completion (results in the host buffers) */
+  uint32_t launch_requests;  /* requests in the launch that served it */
+  uint32_t cached_lights;    /* lights served from the lighting cache */
+} cc_request_stats;
+
+CC_API int cc_server_create(cc_context* ctx, const cc_server_options* opt, cc_server** out);
+/* Finishes every queued and running request, then stops the loop. */
+CC_API int cc_server_destroy(cc_server* server);
+/* Makes a scene of the server's context resident for requests; `id`
+ * receives its index. The scene must outlive the server. */
+CC_API int cc_server_add_scene(cc_server* server, const cc_scene* scene, uint32_t* id);
+/* Queues a request (its receivers are read, and its outputs written, by the
+ * server's thread: they must stay valid until the request completes; its
+ * lights are copied). CC_ERR_BUSY when the queue is full or the request alone
+ * exceeds the budget. */
+CC_API int cc_server_submit(cc_server* server, const cc_request* req, uint64_t* ticket);
+/* Waits at most timeout_ms for a request: CC_OK with its stats (nullable)
+ * when done, CC_ERR_TIMEOUT if not, or the status it failed with. A ticket is
+ * forgotten once its wait returns anything but CC_ERR_TIMEOUT. */
+CC_API int cc_server_wait(cc_server* server, uint64_t ticket, uint32_t timeout_ms, cc_request_stats* stats);
+/* Counters: completed, refused, launches, cached lights served, lights
+ * traced, device bytes in use, peak device bytes, cache entries. */
+CC_API int cc_server_stats(cc_server* server, uint64_t out8[8]);
+
 /* Kernel times of the cc_visibility calls made on this context since the
  * last query, oldest first (the last 256 calls at most): per call, the packet
  * pass and the solo re-walk pass in milliseconds, from CUDA events recorded

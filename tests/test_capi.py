@@ -141,4 +141,30 @@ def test_invalid_arguments_are_errors_not_crashes():
     s = host_scene([kat.box_mesh((0, 0, 0), (1, 1, 1))])
     out = _lib.Outputs()
     assert lib.cc_visibility(None, s.handle, None, 0, None, 0, None, C.byref(out), None) == _lib.CC_ERR_INVALID
+    # Nor for the entry point without allocation, nor in a batch.
+    assert lib.cc_visibility_static(s.handle, None, 0, None, 0, None, C.byref(out), None) == _lib.CC_ERR_INVALID
+    assert lib.cc_batch_create(None, C.byref(h)) == _lib.CC_ERR_INVALID
+    assert lib.cc_batch_add(None, s.handle, None, 0, None, 0, None, C.byref(out), None) == _lib.CC_ERR_INVALID
+    assert lib.cc_batch_submit(None, None, None) == _lib.CC_ERR_INVALID
+    assert lib.cc_batch_wait(None, 0) == _lib.CC_ERR_INVALID
+    assert lib.cc_batch_tune(None, None, 1, None, None, 0) == -_lib.CC_ERR_INVALID
     s.close()
+
+
+def test_batch_options_defaults():
+    o = _lib.BatchOptions()
+    _lib.load().cc_batch_options_default(C.byref(o))
+    assert (o.points_per_warp, o.blocks_per_sm, o.flags) == (32, 4, _lib.CC_BATCH_GRAPH)
+
+
+def test_server_options_and_invalid_arguments():
+    lib = _lib.load()
+    o = _lib.ServerOptions()
+    lib.cc_server_options_default(C.byref(o))
+    assert (o.hbm_budget, o.max_inflight, o.max_queue, o.max_launch_cones, o.points_per_warp, o.blocks_per_sm) == \
+        (8 << 30, 4, 256, 8 << 20, 32, 4)
+    h = C.c_void_p()
+    assert lib.cc_server_create(None, C.byref(o), C.byref(h)) == _lib.CC_ERR_INVALID
+    assert lib.cc_server_submit(None, None, None) == _lib.CC_ERR_INVALID
+    assert lib.cc_server_wait(None, 1, 0, None) == _lib.CC_ERR_INVALID
+    assert lib.cc_server_destroy(None) == _lib.CC_OK

@@ -1,0 +1,120 @@
+"""The served form (cc_server_*) on a B200: every request's results are the
+same alone and in the mix, the lighting cache serves recoloured lights, and
+admission keeps device memory under the budget."""
+import numpy as np
+import pytest
+
+from continuum_b200 import Server, _lib, scenes
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("full", "any", "irradiance", "fraction")
+
+
+def host_outputs(P, L):
+    return {"full": np.zeros((L, P), np.uint64), "any": np.zeros((L, P), np.uint64),
+            "irradiance": np.zeros((L, P), np.float32), "fraction": np.zeros((L, P), np.float32)}
+
+
+def alone(kernel, scene, rec, lights):
+    v = kernel.visibility(scene, rec, lights, outputs=KEYS)
+    return {k: getattr(v, k).reshape(lights.shape[0], rec.shape[0]) for k in KEYS}
+
+
+def recolour(light, rgb):
+    out = light.copy()
+    out[12:15] = rgb
+    return out
+
+
+@pytest.fixture(scope="module")
+def fields(kernel):
+    ws = [scenes.icosphere_field(seed=5, n_spheres=12, subdivisions=4, width=160, height=90),
+          scenes.icosphere_field(seed=8, n_spheres=6, subdivisions=3, width=96, height=54),
+          scenes.box_field(grid=96)]
+    sc = [kernel.scene(w.meshes) for w in ws]
+    yield ws, sc
+    for s in sc:
+        s.close()
+
+
+def test_each_request_is_the_same_alone_and_in_the_mix(kernel, fields):
+    ws, sc = fields
+    srv = Server(kernel, max_inflight=3, max_launch_cones=40_000)
+    ids = [srv.add_scene(s) for s in sc]
+    rng = np.random.default_rng(4)
+    reqs = []
+    for i in range(12):
+        k = i % 3
+        w = ws[k]
+        n = int(rng.integers(500, w.receivers.shape[0]))
+        start = int(rng.integers(0, w.receivers.shape[0] - n + 1))
+        rec = np.ascontiguousarray(w.receivers[start:start + n])
+        pick = rng.permutation(w.lights.shape[0])[: int(rng.integers(1, w.lights.shape[0] + 1))]
+        lig = np.ascontiguousarray(w.lights[pick])
+        reqs.append((k, rec, lig, host_outputs(n, lig.shape[0])))
+    tickets = [srv.submit(ids[k], rec, lig, out) for k, rec, lig, out in reqs]
+    stats = [srv.wait(t) for t in tickets]
+    s = srv.stats()
+    assert s["completed"] == 12 and s["launches"] >= 2
+    assert max(st["launch_requests"] for st in stats) >= 2  # requests shared launches
+    for (k, rec, lig, out) in reqs:
+        ref = alone(kernel, sc[k], rec, lig)
+        for key in KEYS:
+            assert np.array_equal(out[key], ref[key]), key
+    srv.close()
+
+
+def test_the_lighting_cache_serves_recoloured_lights(kernel, fields):
+    ws, sc = fields
+    w = ws[0]
+    srv = Server(kernel)
+    sid = srv.add_scene(sc[0])
+    rec = w.receivers
+    first = np.ascontiguousarray(w.lights[:2])
+    out1 = host_outputs(rec.shape[0], 2)
+    st1 = srv.wait(srv.submit(sid, rec, first, out1, cache_key=77))
+    assert st1["cached_lights"] == 0
+    # Light 0 recoloured (same geometry: served from the cache), light 3 new.
+    second = np.ascontiguousarray(np.stack([recolour(w.lights[0], (5.0, 0.5, 0.1)), w.lights[3]]))
+    out2 = host_outputs(rec.shape[0], 2)
+    st2 = srv.wait(srv.submit(sid, rec, second, out2, cache_key=77))
+    assert st2["cached_lights"] == 1
+    ref = alone(kernel, sc[0], rec, second)
+    for key in KEYS:
+        assert np.array_equal(out2[key], ref[key]), key
+    # Without the key nothing is served from the cache.
+    out3 = host_outputs(rec.shape[0], 2)
+    assert srv.wait(srv.submit(sid, rec, second, out3))["cached_lights"] == 0
+    assert srv.stats()["cache_entries"] >= 3
+    srv.close()
+
+
+def test_admission_stays_under_the_budget(kernel, fields):
+    ws, sc = fields
+    w = ws[0]
+    rec, lig = w.receivers, w.lights
+    P, L = rec.shape[0], lig.shape[0]
+    # Room for two or three requests in flight, but not for every request's
+    # cached results besides: admission must evict cache entries.
+    budget = P * 32 + L * 64 + L * P * 28 + P * 4 + 64 * P + (4 << 20)
+    srv = Server(kernel, hbm_budget=budget, max_inflight=4)
+    sid = srv.add_scene(sc[0])
+    outs = [host_outputs(P, L) for _ in range(4)]
+    tickets = [srv.submit(sid, rec, lig, o, cache_key=i + 1) for i, o in enumerate(outs)]
+    for t in tickets:
+        srv.wait(t)
+    s = srv.stats()
+    assert s["completed"] == 4
+    assert s["peak_bytes"] <= budget
+    ref = alone(kernel, sc[0], rec, lig)
+    for o in outs:
+        for key in KEYS:
+            assert np.array_equal(o[key], ref[key]), key
+    # A request larger than the whole budget is refused at submission.
+    big = np.ascontiguousarray(np.concatenate([rec] * 4))
+    with pytest.raises(_lib.CCError) as e:
+        srv.submit(sid, big, lig, host_outputs(big.shape[0], L))
+    assert e.value.code == _lib.CC_ERR_BUSY
+    assert srv.stats()["refused"] == 1
+    srv.close()
