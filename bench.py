@@ -159,6 +159,25 @@ def traffic_per_cone():
     return None
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest of every rank's `x` (all ranks call it, in the same order);
+    x itself with one rank. Each rank of a multi-GPU run solves its own replica
+    of the workload, so the job's time is its slowest rank's."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(cones_per_rank: int, steps: int, world: int, slowest_seconds: float) -> float:
+    """Whole-job cones/s: every rank's cones over the slowest rank's time."""
+    return world * cones_per_rank * steps / slowest_seconds
+
+
 def timed_steps(torch, dev, stream, flush, fn, warmup, steps):
     """Device milliseconds of `steps` calls of fn on `stream` (CUDA events,
     L2 flushed before each), after `warmup` untimed calls."""
@@ -443,14 +462,11 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize(dev)
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     kt = kernel_times(kernel)
-    elapsed = float(sum(step_ms)) / 1e3
+    elapsed = max_over_ranks(float(sum(step_ms)) / 1e3, world, dev)
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
         dist.barrier()
-    value = world * C * args.steps / elapsed
+    value = replica_value(C, args.steps, world, elapsed)
     packet_ms = float(np.mean(kt[:, 0])) if len(kt) else None
     solo_ms = float(np.mean(kt[:, 1])) if len(kt) else None
 
@@ -478,12 +494,8 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
     t0 = time.perf_counter()
     for _ in range(0 if args.no_e2e else e2e_steps):
         e2e_step()
-    e2e_time = max(time.perf_counter() - t0, 1e-9)
-    if world > 1:
-        t = torch.tensor([e2e_time], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_time = float(t.item())
-    e2e_value = world * C * e2e_steps / e2e_time
+    e2e_time = max_over_ranks(max(time.perf_counter() - t0, 1e-9), world, dev)
+    e2e_value = replica_value(C, e2e_steps, world, e2e_time)
     kernel_times(kernel)
 
     if rank != 0:
