@@ -36,6 +36,10 @@ __constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded b
 
 constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
 constexpr int kConeFields = 17;    // apex, right, up, forward, window, far offset
+// Pairs passed to rasterization wait in a per-warp queue until 32 are ready:
+// a cull round adds at most 32 to at most 31 waiting.
+constexpr int kQueueCap = 64;
+constexpr uint32_t kQueueOwnerShift = 26;  // entry: cone lane << 26 | triangle slot (< 2^26)
 
 // Shared memory of one warp.
 struct WarpShared {
@@ -43,6 +47,7 @@ struct WarpShared {
   unsigned long long acc[kBins * 32];   // each cone's accumulator (64-bit fixed point)
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
   uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
+  uint32_t queue[kQueueCap];            // (cone, triangle) pairs that passed the cull, waiting to be rasterized
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
@@ -99,6 +104,7 @@ struct LaneState {
   WarpShared* ws;
   float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
   uint32_t full;
+  uint32_t queued;  // entries waiting in ws->queue (the same in every lane)
   uint32_t cone_work;
   uint32_t cap;
   uint32_t status;
@@ -133,51 +139,83 @@ __device__ __forceinline__ Cone load_cone(const WarpShared* ws, int owner) {
   return c;
 }
 
-// cover_triangle (:594-616) for one (triangle, cone) pair: back face, the
-// window-direction test, may_touch, then rasterization into the cone's
-// accumulator.
-__device__ __forceinline__ void cover_pair(const DevScene& s, WarpShared* ws, int owner, uint32_t t) {
+// The tests of cover_triangle (:594-616) for one (triangle, cone) pair: back
+// face, the window-direction test, may_touch. A pair that passes is
+// rasterized.
+__device__ __forceinline__ bool pair_survives(const DevScene& s, const WarpShared* ws, int owner, uint32_t t) {
   const Cone c = load_cone(ws, owner);
   const f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
   const f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
   const f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
   const f3 n = cross(v1 - v0, v2 - v0);
-  if (dot(n, c.apex - v0) <= 0.0f) return;  // faces away (:600)
+  if (dot(n, c.apex - v0) <= 0.0f) return false;  // faces away (:600)
   if (dot(n, direction(c, 0.f, 0.f)) >= 0.f && dot(n, direction(c, 1.f, 0.f)) >= 0.f &&
       dot(n, direction(c, 0.f, 1.f)) >= 0.f && dot(n, direction(c, 1.f, 1.f)) >= 0.f)
-    return;  // every window direction leaves its plane (:601-606)
-  if (!may_touch(c, v0, v1, v2)) return;
-  LaneAcc acc{ws->acc + owner, 68u, 0u};
-  rasterize(c, acc, v0, v1, v2);
-  if (acc.span_lo < acc.span_hi) {
-    atomicMin(&ws->span_lo[owner], acc.span_lo);
-    atomicMax(&ws->span_hi[owner], acc.span_hi);
-  }
+    return false;  // every window direction leaves its plane (:601-606)
+  return may_touch(c, v0, v1, v2);
 }
 
-// Triangles t0 .. t0+nt, each to be tested against the cones of the lanes
-// in `owners`: the pairs, triangle-major (consecutive lanes read the same
-// triangle), dealt out over the warp.
-__device__ __noinline__ void cover_leaf(const DevScene& s, WarpShared* ws, uint32_t owners, uint32_t t0,
-                                           uint32_t nt, int lane) {
-  const uint32_t n_owners = __popc(owners);
-  const uint32_t n_pairs = n_owners * nt;
-  for (uint32_t base = 0; base < n_pairs; base += 32) {
-    const uint32_t pair = base + lane;
-    if (pair < n_pairs) {
-      const uint32_t k = pair / n_owners;
-      const uint32_t r = pair - k * n_owners;
-      cover_pair(s, ws, __fns(owners, 0, r + 1), t0 + k);
+// Rasterizes queue entries first .. first+n (n <= 32), one per lane, each
+// into its cone's accumulator.
+__device__ __noinline__ void raster_queue(const DevScene& s, WarpShared* ws, uint32_t first, uint32_t n, int lane) {
+  if ((uint32_t)lane < n) {
+    const uint32_t e = ws->queue[first + lane];
+    const int owner = (int)(e >> kQueueOwnerShift);
+    const uint32_t t = e & ((1u << kQueueOwnerShift) - 1u);
+    const Cone c = load_cone(ws, owner);
+    const f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
+    const f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
+    const f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
+    LaneAcc acc{ws->acc + owner, 68u, 0u};
+    rasterize(c, acc, v0, v1, v2);
+    if (acc.span_lo < acc.span_hi) {
+      atomicMin(&ws->span_lo[owner], acc.span_lo);
+      atomicMax(&ws->span_hi[owner], acc.span_hi);
     }
   }
   __syncwarp();
 }
 
+// Triangles t0 .. t0+nt, each tested against the cones of the lanes in
+// `owners`: the pairs, triangle-major (consecutive lanes read the same
+// triangle), are dealt out over the warp for the cull tests; the survivors
+// join the warp's queue, and every 32 queued pairs are rasterized by the
+// whole warp at once, so lanes whose pair was culled do not sit idle while
+// the others rasterize. Returns the new queue length (below 32).
+__device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WarpShared* ws, uint32_t owners, uint32_t t0,
+                                            uint32_t nt, uint32_t queued, int lane) {
+  const uint32_t n_owners = __popc(owners);
+  const uint32_t n_pairs = n_owners * nt;
+  for (uint32_t base = 0; base < n_pairs; base += 32) {
+    const uint32_t pair = base + lane;
+    bool pass = false;
+    uint32_t entry = 0;
+    if (pair < n_pairs) {
+      const uint32_t k = pair / n_owners;
+      const uint32_t r = pair - k * n_owners;
+      const int owner = (int)__fns(owners, 0, r + 1);
+      pass = pair_survives(s, ws, owner, t0 + k);
+      entry = ((uint32_t)owner << kQueueOwnerShift) | (t0 + k);
+    }
+    const uint32_t m = __ballot_sync(0xffffffffu, pass);
+    if (pass) ws->queue[queued + __popc(m & ((1u << lane) - 1u))] = entry;
+    queued += __popc(m);
+    __syncwarp();
+    if (queued >= 32) {
+      queued -= 32;
+      raster_queue(s, ws, queued, 32, lane);
+    }
+  }
+  return queued;
+}
+
 // The mesh's coverage for the lane's own cone: running sum over the touched
 // cells (exact), snapped to whole within 1e-5, combined into the cone's bins
 // by max (:809-828); then the cells are cleared for the next mesh.
-__device__ __forceinline__ void resolve_mesh(LaneState& st, int lane) {
+__device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState& st, int lane) {
   WarpShared* ws = st.ws;
+  if (st.queued) raster_queue(s, ws, 0, st.queued, lane);  // the mesh's last pairs
+  st.queued = 0;
   const uint32_t lo = ws->span_lo[lane];
   const uint32_t end = min(ws->span_hi[lane], (uint32_t)kBins);
   long long running = 0;
@@ -214,8 +252,8 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState& st, 
   const uint4 range = __ldg(&s.meshes[m]);
   if (kCount && on) st.n_tris += range.y;
   for (uint32_t t = range.x; t < range.x + range.y; t += 8)
-    cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), lane);
-  resolve_mesh(st, lane);
+    st.queued = cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), st.queued, lane);
+  resolve_mesh(s, st, lane);
 }
 
 // The cone walk (scene_coverage_if, :1160-1227, with add_mesh_coverage_if,
@@ -248,7 +286,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
     const uint32_t ref = stk.get(sp);
     const uint32_t kind = ref_kind(ref);
     if (kind == kResolve) {
-      resolve_mesh(st, lane);
+      resolve_mesh(s, st, lane);
       continue;
     }
     const bool is_obj = kind == kObjNode;
@@ -267,7 +305,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
         st.cone_work += ib;
         if (kCount) st.n_tris += ib;
       }
-      cover_leaf(s, st.ws, owners, ia, ib, lane);
+      st.queued = cover_leaf(s, st.ws, owners, ia, ib, st.queued, lane);
     } else if (ib > 0) {
       // An object leaf: its meshes.
       if (hierarchy == 1) {
@@ -490,6 +528,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     st.ws = ws;
     st.cov = ws->cov + lane;
     st.full = 0;
+    st.queued = 0;
     st.cone_work = 0;
     st.status = 0;
     st.n_obj = st.n_blas = st.n_tris = 0;
