@@ -476,15 +476,20 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, LaneAcc& ac
   return true;
 }
 
-// rasterize (:350-451). The common case — a triangle wholly inside the
-// window between the near and far planes — projects its three corners and
-// draws them from registers; everything else takes the general path.
-__device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2) {
-  float f0 = c.far_offset - dot(c.fwd, v0);
-  float f1 = c.far_offset - dot(c.fwd, v1);
-  float f2 = c.far_offset - dot(c.fwd, v2);
-  bool far_clip = f0 < 0.0f || f1 < 0.0f || f2 < 0.0f;
-  if (!far_clip) {
+// Whether the triangle reaches past the far plane (rasterize's far clip, :356-362).
+__device__ __forceinline__ bool crosses_far(const Cone& c, f3 v0, f3 v1, f3 v2) {
+  const float f0 = c.far_offset - dot(c.fwd, v0);
+  const float f1 = c.far_offset - dot(c.fwd, v1);
+  const float f2 = c.far_offset - dot(c.fwd, v2);
+  return f0 < 0.0f || f1 < 0.0f || f2 < 0.0f;
+}
+
+// rasterize (:350-451), its common case: a triangle wholly inside the window
+// between the near and far planes projects its three corners and draws them
+// from registers. Returns false, having drawn nothing, for every other
+// triangle: those take rasterize_general.
+__device__ __forceinline__ bool rasterize_fast(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2) {
+  if (!crosses_far(c, v0, v1, v2)) {
     f3 p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
     auto in_win = [&](f3 v) {
       return v.z >= kNear && !(v.x < c.u0 * v.z || v.x > c.u1 * v.z || v.y < c.v0 * v.z || v.y > c.v1 * v.z);
@@ -511,7 +516,13 @@ __device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3
       }
     }
   }
-  return rasterize_general(c, acc, v0, v1, v2, far_clip);
+  return false;
+}
+
+// rasterize (:350-451): the common case, else the general path.
+__device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2) {
+  if (rasterize_fast(c, acc, v0, v1, v2)) return true;
+  return rasterize_general(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2));
 }
 
 // ---- integration --------------------------------------------------------------

@@ -37,9 +37,15 @@ __constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded b
 constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
 constexpr int kConeFields = 17;    // apex, right, up, forward, window, far offset
 // Pairs passed to rasterization wait in a per-warp queue until 32 are ready:
-// a cull round adds at most 32 to at most 31 waiting.
+// a cull round adds at most 32 to at most 31 waiting. Pairs that need the
+// general clip path wait in a second queue of the same size.
 constexpr int kQueueCap = 64;
 constexpr uint32_t kQueueOwnerShift = 26;  // entry: cone lane << 26 | triangle slot (< 2^26)
+// Both queues' lengths in one word: fast queue in the low byte, general
+// queue in the next (each below 32 between rounds).
+__device__ __forceinline__ uint32_t fast_len(uint32_t q) { return q & 255u; }
+__device__ __forceinline__ uint32_t general_len(uint32_t q) { return q >> 8; }
+__device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) { return fast | (general << 8); }
 
 // Shared memory of one warp.
 struct WarpShared {
@@ -48,6 +54,7 @@ struct WarpShared {
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
   uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
   uint32_t queue[kQueueCap];            // (cone, triangle) pairs that passed the cull, waiting to be rasterized
+  uint32_t general[kQueueCap];          // pairs that need rasterize's general path, waiting for it
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
@@ -104,7 +111,7 @@ struct LaneState {
   WarpShared* ws;
   float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
   uint32_t full;
-  uint32_t queued;  // entries waiting in ws->queue (the same in every lane)
+  uint32_t queued;  // both queues' lengths (queue_lens; the same in every lane)
   uint32_t cone_work;
   uint32_t cap;
   uint32_t status;
@@ -155,25 +162,65 @@ __device__ __forceinline__ bool pair_survives(const DevScene& s, const WarpShare
   return may_touch(c, v0, v1, v2);
 }
 
-// Rasterizes queue entries first .. first+n (n <= 32), one per lane, each
-// into its cone's accumulator.
-__device__ __noinline__ void raster_queue(const DevScene& s, WarpShared* ws, uint32_t first, uint32_t n, int lane) {
+__device__ __forceinline__ void load_pair(const DevScene& s, const WarpShared* ws, uint32_t e, int& owner, Cone& c,
+                                          f3& v0, f3& v1, f3& v2) {
+  owner = (int)(e >> kQueueOwnerShift);
+  const uint32_t t = e & ((1u << kQueueOwnerShift) - 1u);
+  c = load_cone(ws, owner);
+  v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
+  v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
+  v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
+}
+
+__device__ __forceinline__ void note_span(WarpShared* ws, int owner, const LaneAcc& acc) {
+  if (acc.span_lo < acc.span_hi) {
+    atomicMin(&ws->span_lo[owner], acc.span_lo);
+    atomicMax(&ws->span_hi[owner], acc.span_hi);
+  }
+}
+
+// The general path for general-queue entries first .. first+n (n <= 32),
+// one per lane.
+__device__ __noinline__ void raster_general(const DevScene& s, WarpShared* ws, uint32_t first, uint32_t n, int lane) {
   if ((uint32_t)lane < n) {
-    const uint32_t e = ws->queue[first + lane];
-    const int owner = (int)(e >> kQueueOwnerShift);
-    const uint32_t t = e & ((1u << kQueueOwnerShift) - 1u);
-    const Cone c = load_cone(ws, owner);
-    const f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
-    const f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
-    const f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
+    int owner;
+    Cone c;
+    f3 v0, v1, v2;
+    load_pair(s, ws, ws->general[first + lane], owner, c, v0, v1, v2);
     LaneAcc acc{ws->acc + owner, 68u, 0u};
-    rasterize(c, acc, v0, v1, v2);
-    if (acc.span_lo < acc.span_hi) {
-      atomicMin(&ws->span_lo[owner], acc.span_lo);
-      atomicMax(&ws->span_hi[owner], acc.span_hi);
-    }
+    rasterize_general(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2));
+    note_span(ws, owner, acc);
   }
   __syncwarp();
+}
+
+// Rasterizes queue entries first .. first+n (n <= 32), one per lane, each
+// into its cone's accumulator by the common case; pairs that need the
+// general path join the general queue, which is run whenever 32 wait.
+// Returns the general queue's new length (below 32).
+__device__ __noinline__ uint32_t raster_queue(const DevScene& s, WarpShared* ws, uint32_t first, uint32_t n,
+                                              uint32_t general, int lane) {
+  bool defer = false;
+  uint32_t e = 0;
+  if ((uint32_t)lane < n) {
+    e = ws->queue[first + lane];
+    int owner;
+    Cone c;
+    f3 v0, v1, v2;
+    load_pair(s, ws, e, owner, c, v0, v1, v2);
+    LaneAcc acc{ws->acc + owner, 68u, 0u};
+    defer = !rasterize_fast(c, acc, v0, v1, v2);
+    note_span(ws, owner, acc);
+  }
+  const uint32_t m = __ballot_sync(0xffffffffu, defer);
+  if (defer) ws->general[general + __popc(m & ((1u << lane) - 1u))] = e;
+  general += __popc(m);
+  __syncwarp();
+  if (general >= 32) {
+    general -= 32;
+    raster_general(s, ws, general, 32, lane);
+  }
+  return general;
 }
 
 // Triangles t0 .. t0+nt, each tested against the cones of the lanes in
@@ -181,9 +228,10 @@ __device__ __noinline__ void raster_queue(const DevScene& s, WarpShared* ws, uin
 // triangle), are dealt out over the warp for the cull tests; the survivors
 // join the warp's queue, and every 32 queued pairs are rasterized by the
 // whole warp at once, so lanes whose pair was culled do not sit idle while
-// the others rasterize. Returns the new queue length (below 32).
+// the others rasterize. `queues` and the result are both queues' lengths.
 __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WarpShared* ws, uint32_t owners, uint32_t t0,
-                                            uint32_t nt, uint32_t queued, int lane) {
+                                            uint32_t nt, uint32_t queues, int lane) {
+  uint32_t queued = fast_len(queues), general = general_len(queues);
   const uint32_t n_owners = __popc(owners);
   const uint32_t n_pairs = n_owners * nt;
   for (uint32_t base = 0; base < n_pairs; base += 32) {
@@ -203,10 +251,10 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WarpShared* ws, u
     __syncwarp();
     if (queued >= 32) {
       queued -= 32;
-      raster_queue(s, ws, queued, 32, lane);
+      general = raster_queue(s, ws, queued, 32, general, lane);
     }
   }
-  return queued;
+  return queue_lens(queued, general);
 }
 
 // The mesh's coverage for the lane's own cone: running sum over the touched
@@ -214,7 +262,10 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WarpShared* ws, u
 // by max (:809-828); then the cells are cleared for the next mesh.
 __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState& st, int lane) {
   WarpShared* ws = st.ws;
-  if (st.queued) raster_queue(s, ws, 0, st.queued, lane);  // the mesh's last pairs
+  // The mesh's last pairs: the common case, then the general path.
+  uint32_t general = general_len(st.queued);
+  if (fast_len(st.queued)) general = raster_queue(s, ws, 0, fast_len(st.queued), general, lane);
+  if (general) raster_general(s, ws, 0, general, lane);
   st.queued = 0;
   const uint32_t lo = ws->span_lo[lane];
   const uint32_t end = min(ws->span_hi[lane], (uint32_t)kBins);
