@@ -5,9 +5,9 @@ ABI, include/continuum_cuda.h); this package binds it and mirrors the
 reference's visibility API.
 """
 from .kernel import (Batch, Hierarchy, Light, MaskConeKernel, RectLight, Scene, Server, SphereLight, Spot, Visibility,
-                     flatten_meshes, host_scene, light_gpu, lights_gpu, receivers_gpu)
+                     flatten_meshes, host_scene, host_scene_instanced, light_gpu, lights_gpu, receivers_gpu)
 
 __all__ = [
     "Batch", "Hierarchy", "Light", "MaskConeKernel", "RectLight", "Scene", "Server", "SphereLight", "Spot", "Visibility",
-    "flatten_meshes", "host_scene", "light_gpu", "lights_gpu", "receivers_gpu",
+    "flatten_meshes", "host_scene", "host_scene_instanced", "light_gpu", "lights_gpu", "receivers_gpu",
 ]

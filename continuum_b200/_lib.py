@@ -42,8 +42,11 @@ EXPORTS = (
     "cc_visibility_static", "cc_batch_options_default", "cc_batch_create", "cc_batch_destroy", "cc_batch_clear",
     "cc_batch_add", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
     "cc_server_options_default", "cc_server_create", "cc_server_destroy", "cc_server_add_scene", "cc_server_submit",
-    "cc_server_wait", "cc_server_stats",
+    "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms",
 )
+
+# cc_instance: an object placing a geometry (world = scale * rotation * p + translation).
+INSTANCE_DTYPE = np.dtype([("geometry", "<u4"), ("rotation", "<f4", 9), ("scale", "<f4"), ("translation", "<f4", 3)])
 
 
 class CCError(RuntimeError):
@@ -62,6 +65,7 @@ class FlatScene(C.Structure):
         ("blas_items", C.c_void_p), ("nblas_items", C.c_uint32),
         ("nodes", C.c_void_p), ("nnodes", C.c_uint32),
         ("items", C.c_void_p), ("nitems", C.c_uint32),
+        ("xforms", C.c_void_p), ("nxforms", C.c_uint32),
     ]
 
 
@@ -144,6 +148,8 @@ def load() -> C.CDLL:
         "cc_server_submit": (I, [P, C.POINTER(Request), C.POINTER(U64)]),
         "cc_server_wait": (I, [P, U64, U32, C.POINTER(RequestStats)]),
         "cc_server_stats": (I, [P, P]),
+        "cc_scene_build_instanced": (I, [P, P, P, U32, P, U32, C.POINTER(P)]),
+        "cc_scene_transforms": (U64, [P, P, U64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

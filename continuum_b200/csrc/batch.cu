@@ -219,6 +219,7 @@ int cc_batch_add(cc_batch* b, const cc_scene* scene, const float* receivers, uin
                  uint32_t nlights, const cc_options* opt_in, const cc_outputs* out, uint32_t* job) {
   if (!b || !scene || !out) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != b->ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
+  if (scene->xforms) return fail(CC_ERR_INVALID, "instanced scenes are solved by cc_visibility, not in batches");
   if ((npoints && !receivers) || (nlights && !lights)) return fail(CC_ERR_INVALID, "null inputs");
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);

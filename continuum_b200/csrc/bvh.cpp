@@ -132,6 +132,56 @@ struct Builder {
   }
 };
 
+// object_hierarchy (hierarchy.rs:198-253): two objects per leaf over the
+// objects' padded world bounds, with oversized objects in a subtree of their
+// own under the root.
+void object_hierarchy(const std::vector<Box>& mesh_box, std::vector<NodeGpu>& nodes_out, std::vector<uint32_t>& items_out) {
+  const uint32_t nmeshes = (uint32_t)mesh_box.size();
+  std::vector<uint32_t> items(nmeshes);
+  std::iota(items.begin(), items.end(), 0u);
+  std::vector<NodeGpu>& nodes = nodes_out;
+  nodes.assign(1, NodeGpu{});
+  if (items.empty()) {
+    items_out = {0};
+    nodes[0].info[1] = 1;
+    return;
+  }
+  auto diagonal = [&](uint32_t m) {
+    float d2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      float e = mesh_box[m].hi[k] - mesh_box[m].lo[k];
+      d2 += e * e;
+    }
+    return std::sqrt(d2);
+  };
+  std::vector<float> sizes(nmeshes);
+  for (uint32_t m = 0; m < nmeshes; ++m) sizes[m] = diagonal(m);
+  size_t mid = sizes.size() / 2;
+  std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
+  const float median = sizes[mid];
+  std::vector<uint32_t> big, small;
+  for (uint32_t m : items) (diagonal(m) > kOversized * median ? big : small).push_back(m);
+  Builder ob{mesh_box, kLeafObjects, 0, 0, 0};
+  if (big.empty() || small.empty()) {
+    ob.split(nodes, 0, items.data(), items.size(), 0, 0);
+  } else {
+    const size_t nb = big.size();
+    items = big;
+    items.insert(items.end(), small.begin(), small.end());
+    nodes.push_back(NodeGpu{});
+    nodes.push_back(NodeGpu{});
+    ob.split(nodes, 1, items.data(), nb, 0, 0);
+    ob.split(nodes, 2, items.data() + nb, items.size() - nb, nb, 0);
+    NodeGpu& r = nodes[0];
+    for (int k = 0; k < 3; ++k) {
+      r.lo[k] = std::min(nodes[1].lo[k], nodes[2].lo[k]);
+      r.hi[k] = std::max(nodes[1].hi[k], nodes[2].hi[k]);
+    }
+    r.info[0] = 1;
+  }
+  items_out = items;
+}
+
 }  // namespace
 
 void build_flat_scene(const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, FlatScene& out,
@@ -218,48 +268,50 @@ void build_flat_scene(const float* tri9, const uint32_t* mesh_counts, uint32_t n
   }
 
   // The object hierarchy over meshes (object_hierarchy, hierarchy.rs:198-253).
-  std::vector<uint32_t> items(nmeshes);
-  std::iota(items.begin(), items.end(), 0u);
-  out.nodes.assign(1, NodeGpu{});
-  if (items.empty()) {
-    out.items = {0};
-    out.nodes[0].info[1] = 1;
-    return;
-  }
-  auto diagonal = [&](uint32_t m) {
-    float d2 = 0;
-    for (int k = 0; k < 3; ++k) {
-      float e = mesh_box[m].hi[k] - mesh_box[m].lo[k];
-      d2 += e * e;
+  object_hierarchy(mesh_box, out.nodes, out.items);
+}
+
+void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
+                           const Instance* instances, uint32_t ninstances, FlatScene& out, int threads) {
+  // Each geometry's triangles and hierarchy once (flatten, triangle_hierarchy).
+  build_flat_scene(tri9, geometry_counts, ngeometries, out, threads);
+  const std::vector<uint32_t> geometry_ranges = out.ranges;
+  std::vector<Box> local(ngeometries);
+  for (uint32_t g = 0; g < ngeometries; ++g)
+    local[g] = bounds_of(out.tris.data(), geometry_ranges[4 * g], geometry_ranges[4 * g + 1]);
+  // Per object: its geometry's range with its transform, the transform's
+  // rows, and its padded world bounds (flatten_instanced, hierarchy.rs:464-522;
+  // Placement::rows and world_bounds, :272-303).
+  out.ranges.clear();
+  out.xforms.clear();
+  std::vector<Box> bounds(ninstances);
+  for (uint32_t k = 0; k < ninstances; ++k) {
+    const Instance& o = instances[k];
+    const uint32_t* r = &geometry_ranges[4 * o.geometry];
+    out.ranges.insert(out.ranges.end(), {r[0], r[1], r[2], k});
+    const float* R = o.rotation;  // row-major
+    const float* t = o.translation;
+    out.xforms.insert(out.xforms.end(), {R[0], R[1], R[2], t[0], R[3], R[4], R[5], t[1], R[6], R[7], R[8], t[2],
+                                         o.scale, 1.0f / o.scale, 0.0f, 0.0f});
+    Box w{{FLT_MAX, FLT_MAX, FLT_MAX}, {-FLT_MAX, -FLT_MAX, -FLT_MAX}};
+    const Box& b = local[o.geometry];
+    for (int c = 0; c < 8; ++c) {
+      const float p[3] = {(c & 1) ? b.hi[0] : b.lo[0], (c & 2) ? b.hi[1] : b.lo[1], (c & 4) ? b.hi[2] : b.lo[2]};
+      for (int i = 0; i < 3; ++i) {
+        // rotation * p (columns scaled by p's components, summed in order),
+        // then * scale + translation.
+        const float v = (R[3 * i] * p[0] + R[3 * i + 1] * p[1] + R[3 * i + 2] * p[2]) * o.scale + t[i];
+        w.lo[i] = std::min(w.lo[i], v);
+        w.hi[i] = std::max(w.hi[i], v);
+      }
     }
-    return std::sqrt(d2);
-  };
-  std::vector<float> sizes(nmeshes);
-  for (uint32_t m = 0; m < nmeshes; ++m) sizes[m] = diagonal(m);
-  size_t mid = sizes.size() / 2;
-  std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
-  const float median = sizes[mid];
-  std::vector<uint32_t> big, small;
-  for (uint32_t m : items) (diagonal(m) > kOversized * median ? big : small).push_back(m);
-  Builder ob{mesh_box, kLeafObjects, 0, 0, 0};
-  if (big.empty() || small.empty()) {
-    ob.split(out.nodes, 0, items.data(), items.size(), 0, 0);
-  } else {
-    const size_t nb = big.size();
-    items = big;
-    items.insert(items.end(), small.begin(), small.end());
-    out.nodes.push_back(NodeGpu{});
-    out.nodes.push_back(NodeGpu{});
-    ob.split(out.nodes, 1, items.data(), nb, 0, 0);
-    ob.split(out.nodes, 2, items.data() + nb, items.size() - nb, nb, 0);
-    NodeGpu& r = out.nodes[0];
-    for (int k = 0; k < 3; ++k) {
-      r.lo[k] = std::min(out.nodes[1].lo[k], out.nodes[2].lo[k]);
-      r.hi[k] = std::max(out.nodes[1].hi[k], out.nodes[2].hi[k]);
-    }
-    r.info[0] = 1;
+    padded(w);
+    bounds[k] = w;
   }
-  out.items = items;
+  if (out.ranges.empty()) out.ranges.insert(out.ranges.end(), {0u, 0u, kNone, kNone});
+  if (out.xforms.empty()) out.xforms.assign(16, 0.0f);
+  out.nmeshes = (uint32_t)(out.ranges.size() / 4);
+  object_hierarchy(bounds, out.nodes, out.items);
 }
 
 }  // namespace cc

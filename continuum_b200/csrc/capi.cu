@@ -88,6 +88,8 @@ void free_scene_device(cc_scene* s) {
   cudaFree(s->nodes);
   cudaFree(s->items);
   cudaFree(s->blas);
+  cudaFree(s->xforms);
+  s->xforms = nullptr;
   s->tris = nullptr;
   s->meshes = nullptr;
   s->nodes = nullptr;
@@ -121,6 +123,12 @@ int upload_scene(cc_scene* s) {
   if ((rc = upload(repack(f.nodes), &s->nodes, s->bytes, "scene nodes"))) return rc;
   if ((rc = upload(f.items, &s->items, s->bytes, "scene items"))) return rc;
   if ((rc = upload(repack(f.blas), &s->blas, s->bytes, "scene triangle nodes"))) return rc;
+  if (!f.xforms.empty()) {
+    std::vector<float4> x(f.xforms.size() / 4);
+    for (size_t i = 0; i < x.size(); ++i)
+      x[i] = make_float4(f.xforms[4 * i], f.xforms[4 * i + 1], f.xforms[4 * i + 2], f.xforms[4 * i + 3]);
+    if ((rc = upload(x, &s->xforms, s->bytes, "scene transforms"))) return rc;
+  }
   return CC_OK;
 }
 
@@ -130,7 +138,12 @@ int validate_flat(const cc::FlatScene& f) {
     const uint32_t* r = &f.ranges[4 * m];
     if ((uint64_t)r[0] + r[1] > ntris) return fail(CC_ERR_INVALID, "mesh range beyond the triangles");
     if (r[2] != CC_NONE && r[2] >= f.blas.size()) return fail(CC_ERR_INVALID, "mesh hierarchy root out of range");
-    if (r[3] != CC_NONE) return fail(CC_ERR_INVALID, "instancing transforms are not supported by this call");
+    if (r[3] != CC_NONE) {
+      if ((uint64_t)r[3] * 16 + 16 > f.xforms.size()) return fail(CC_ERR_INVALID, "object transform out of range");
+      const float* x = &f.xforms[16 * (size_t)r[3]];
+      if (!(x[12] > 0.0f) || !std::isfinite(x[12]) || !std::isfinite(x[13]))
+        return fail(CC_ERR_INVALID, "object transforms need a positive finite scale");
+    }
   }
   auto check_nodes = [&](const std::vector<cc::NodeGpu>& nodes, uint64_t nitems, const char* what) {
     for (size_t i = 0; i < nodes.size(); ++i) {
@@ -154,8 +167,11 @@ int validate_flat(const cc::FlatScene& f) {
   if (!f.blas.empty()) {
     if (f.blas_items.size() != ntris) return fail(CC_ERR_INVALID, "triangle hierarchy items must cover every triangle");
     std::vector<uint8_t> seen(ntris, 0);
+    std::vector<uint8_t> checked(ntris + 1, 0);  // objects placing one geometry share its range
     for (uint32_t m = 0; m < f.nmeshes; ++m) {
       const uint32_t first = f.ranges[4 * m], count = f.ranges[4 * m + 1];
+      if (count == 0 || checked[first]) continue;
+      checked[first] = 1;
       for (uint64_t k = first; k < (uint64_t)first + count; ++k) {
         const uint32_t t = f.blas_items[k];
         if (t < first || t >= (uint64_t)first + count || seen[t])
@@ -269,6 +285,13 @@ int cc_scene_upload(cc_context* ctx, const cc_flat_scene* fl, cc_scene** out) {
   const cc::NodeGpu* n = static_cast<const cc::NodeGpu*>(fl->nodes);
   f.nodes.assign(n, n + fl->nnodes);
   f.items.assign(fl->items, fl->items + fl->nitems);
+  if (fl->nxforms) {
+    if (!fl->xforms) {
+      delete s;
+      return fail(CC_ERR_INVALID, "null transforms");
+    }
+    f.xforms.assign(fl->xforms, fl->xforms + (size_t)fl->nxforms * 16);
+  }
   int rc = validate_flat(f);
   if (!rc) rc = set_device(ctx);
   if (!rc) rc = upload_scene(s);
@@ -309,6 +332,58 @@ int cc_scene_build(cc_context* ctx, const float* tri9, const uint32_t* mesh_coun
   }
   *out = s;
   return CC_OK;
+}
+
+int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const uint32_t* geometry_counts,
+                             uint32_t ngeometries, const cc_instance* instances, uint32_t ninstances, cc_scene** out) {
+  static_assert(sizeof(cc_instance) == sizeof(cc::Instance), "cc_instance is cc::Instance");
+  if (!out || (ngeometries && !geometry_counts) || (ninstances && !instances)) return fail(CC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  uint64_t total = 0;
+  for (uint32_t g = 0; g < ngeometries; ++g) total += geometry_counts[g];
+  if (total && !tri9) return fail(CC_ERR_INVALID, "null triangles");
+  if (ninstances >= (1u << 26)) return fail(CC_ERR_INVALID, "fewer than 2^26 instances");
+  for (uint32_t k = 0; k < ninstances; ++k) {
+    const cc_instance& o = instances[k];
+    if (o.geometry >= ngeometries) return fail(CC_ERR_INVALID, "instance geometry out of range");
+    if (!(o.scale > 0.0f) || !std::isfinite(o.scale)) return fail(CC_ERR_INVALID, "instance scale must be positive");
+    // The rotation must be orthonormal (Placement, hierarchy.rs:258-270).
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const float d = o.rotation[3 * i] * o.rotation[3 * j] + o.rotation[3 * i + 1] * o.rotation[3 * j + 1] +
+                        o.rotation[3 * i + 2] * o.rotation[3 * j + 2];
+        if (!(std::fabs(d - (i == j ? 1.0f : 0.0f)) < 1e-4f)) return fail(CC_ERR_INVALID, "instance rotation is not orthonormal");
+      }
+  }
+  if (total >= (1u << 26)) return fail(CC_ERR_INVALID, "a scene holds fewer than 2^26 triangles and hierarchy nodes");
+  cc_scene* s = new cc_scene;
+  s->ctx = ctx;
+  cc::build_instanced_scene(tri9, geometry_counts, ngeometries, reinterpret_cast<const cc::Instance*>(instances),
+                            ninstances, s->flat, threads_for_build());
+  if (s->flat.blas.size() >= (1u << 26) || s->flat.nodes.size() >= (1u << 26)) {
+    delete s;
+    return fail(CC_ERR_INVALID, "a scene holds fewer than 2^26 triangles and hierarchy nodes");
+  }
+  if (!ctx) {  // host-only scene
+    *out = s;
+    return CC_OK;
+  }
+  int rc = set_device(ctx);
+  if (!rc) rc = upload_scene(s);
+  if (rc) {
+    free_scene_device(s);
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return CC_OK;
+}
+
+uint64_t cc_scene_transforms(const cc_scene* s, float* out16, uint64_t max_transforms) {
+  if (!s) return 0;
+  const uint64_t n = s->flat.xforms.size() / 16;
+  if (out16) std::memcpy(out16, s->flat.xforms.data(), std::min(n, max_transforms) * 16 * sizeof(float));
+  return n;
 }
 
 int cc_scene_destroy(cc_scene* s) {

@@ -76,6 +76,7 @@ struct cc_scene {
   float4* nodes = nullptr;
   uint32_t* items = nullptr;
   float4* blas = nullptr;
+  float4* xforms = nullptr;  // instanced scenes: 4 per transform
   uint64_t bytes = 0;
   cc::DevScene dev() const {
     cc::DevScene s;
@@ -85,6 +86,7 @@ struct cc_scene {
     s.items = items;
     s.blas = blas;
     s.nmeshes = flat.nmeshes;
+    s.xforms = xforms;
     return s;
   }
 };

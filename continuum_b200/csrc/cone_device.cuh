@@ -49,6 +49,10 @@ struct DevScene {
   const uint32_t* items;   // mesh per object leaf slot
   const float4* blas;      // triangle hierarchies, 2 per node; leaf items are triangle slots
   uint32_t nmeshes;
+  // Instanced scenes: 4 per transform (rows 0-2 of the rotation with the
+  // translation in w, then scale, 1 / scale); meshes[m].w names object m's.
+  // Null when every object's triangles are in world space.
+  const float4* xforms;
 };
 
 struct DevLight {
@@ -85,6 +89,32 @@ struct Cone {
   f3 baxis;
   float bcos, bsin;
 };
+
+// cone_to_object (:623-638): the cone in the space of the object placed by
+// transform X (world = scale * rotation * p + translation): the apex moved and
+// scaled, the frame and the bounding axis rotated (rotate_to_object, :61-63),
+// the far plane moved; the window is a set of directions, which a rotation
+// and a uniform scale keep.
+__device__ __forceinline__ Cone cone_to_object(const Cone& c, const float4* __restrict__ X) {
+  const float4 r0 = __ldg(X), r1 = __ldg(X + 1), r2 = __ldg(X + 2), r3 = __ldg(X + 3);
+  const f3 a = {r0.x, r0.y, r0.z}, b = {r1.x, r1.y, r1.z}, d = {r2.x, r2.y, r2.z};
+  auto rot = [&](f3 v) { return a * v.x + b * v.y + d * v.z; };
+  const f3 t = {r0.w, r1.w, r2.w};
+  Cone o;
+  o.apex = rot(c.apex - t) * r3.y;
+  o.right = rot(c.right);
+  o.up = rot(c.up);
+  o.fwd = rot(c.fwd);
+  o.u0 = c.u0;
+  o.v0 = c.v0;
+  o.u1 = c.u1;
+  o.v1 = c.v1;
+  o.far_offset = (c.far_offset - dot(c.fwd, t)) * r3.y;  // the far plane's normal is the forward axis
+  o.baxis = rot(c.baxis);
+  o.bcos = c.bcos;
+  o.bsin = c.bsin;
+  return o;
+}
 
 __device__ __forceinline__ f3 direction(const Cone& c, float s, float t) {  // :203-206
   return c.fwd + c.right * (c.u0 + s * (c.u1 - c.u0)) + c.up * (c.v0 + t * (c.v1 - c.v0));

@@ -66,6 +66,7 @@ inline float ray_tri(V o, V d, V v0, V v1, V v2) {
 struct Hit {
   float t = FLT_MAX;
   uint32_t tri = kNone;
+  uint32_t xform = kNone;  // the hit object's transform (instanced scenes)
 };
 
 void trace(const FlatScene& s, V o, V d, Hit& hit) {
@@ -81,19 +82,32 @@ void trace(const FlatScene& s, V o, V d, Hit& hit) {
       for (uint32_t k = n.info[0]; k < n.info[0] + n.info[1]; ++k) {
         const uint32_t* r = &s.ranges[4 * s.items[k]];
         if (r[2] == kNone) continue;
+        // A placed object: the ray in its space, o' = R^T (o - t) / s and
+        // d' = R^T d / s, so distances along it stay the world's.
+        V ob = o, db = d, ib = inv;
+        if (r[3] != kNone) {
+          const float* x = &s.xforms[16 * (size_t)r[3]];
+          const V a{x[0], x[1], x[2]}, b{x[4], x[5], x[6]}, c{x[8], x[9], x[10]}, t{x[3], x[7], x[11]};
+          const float is = x[13];
+          const V q = o - t;
+          ob = (a * q.x + b * q.y + c * q.z) * is;
+          db = (a * d.x + b * d.y + c * d.z) * is;
+          ib = V{1.0f / db.x, 1.0f / db.y, 1.0f / db.z};
+        }
         int bp = 0;
         bstack[bp++] = r[2];
         while (bp > 0) {
           const NodeGpu& b = s.blas[bstack[--bp]];
-          if (!ray_box(o, inv, b, hit.t)) continue;
+          if (!ray_box(ob, ib, b, hit.t)) continue;
           if (b.info[1] > 0) {
             for (uint32_t j = b.info[0]; j < b.info[0] + b.info[1]; ++j) {
               uint32_t t = s.blas_items[j];
               const float* p = &s.tris[12 * (size_t)t];
-              float dist = ray_tri(o, d, V{p[0], p[1], p[2]}, V{p[4], p[5], p[6]}, V{p[8], p[9], p[10]});
+              float dist = ray_tri(ob, db, V{p[0], p[1], p[2]}, V{p[4], p[5], p[6]}, V{p[8], p[9], p[10]});
               if (dist > 0.0f && dist < hit.t) {
                 hit.t = dist;
                 hit.tri = t;
+                hit.xform = r[3];
               }
             }
           } else if (bp + 2 <= 128) {
@@ -142,6 +156,11 @@ void primary_hits(const FlatScene& s, const float* camera, uint32_t width, uint3
         const float* p = &s.tris[12 * (size_t)h.tri];
         V v0{p[0], p[1], p[2]}, v1{p[4], p[5], p[6]}, v2{p[8], p[9], p[10]};
         V n = normalize(cross(v1 - v0, v2 - v0));
+        if (h.xform != kNone) {  // the object's normal in world space: R n
+          const float* x = &s.xforms[16 * (size_t)h.xform];
+          n = normalize(V{x[0] * n.x + x[1] * n.y + x[2] * n.z, x[4] * n.x + x[5] * n.y + x[6] * n.z,
+                          x[8] * n.x + x[9] * n.y + x[10] * n.z});
+        }
         if (dot(n, d) > 0.0f) n = n * -1.0f;
         V surface = eye + d * h.t;
         V point = surface + n * std::max(1e-4f, 2e-6f * h.t);

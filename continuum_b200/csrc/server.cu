@@ -558,6 +558,7 @@ int cc_server_destroy(cc_server* s) {
 int cc_server_add_scene(cc_server* s, const cc_scene* scene, uint32_t* id) {
   if (!s || !scene) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != s->ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
+  if (scene->xforms) return fail(CC_ERR_INVALID, "instanced scenes are solved by cc_visibility, not by the server");
   std::lock_guard<std::mutex> g(s->mu);
   if (id) *id = (uint32_t)s->scenes.size();
   s->scenes.push_back(scene);

@@ -107,7 +107,8 @@ struct WarpStack {
 };
 
 struct LaneState {
-  Cone cone;
+  Cone cone;   // the cone in the space of the object being walked (the world's elsewhere)
+  Cone world;  // instanced scenes: the cone in world space
   WarpShared* ws;
   float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
   uint32_t full;
@@ -291,20 +292,32 @@ __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState& st, i
 // Stack entry kinds for the walk of both hierarchy levels in one loop.
 constexpr uint32_t kObjNode = 0;   // an object-hierarchy node
 constexpr uint32_t kTriNode = 1;   // a node of the current mesh's triangle hierarchy
-constexpr uint32_t kResolve = 2;   // the current mesh is done: resolve its coverage
+constexpr uint32_t kResolve = 2;   // the current mesh is done: resolve its coverage (index 1: and return to world space)
+constexpr uint32_t kObjRoot = 3;   // instanced scenes: the root of object `index`'s triangle hierarchy
 
 // add_mesh_coverage_if (:713-829) for hierarchy levels 0 and 1: every
 // triangle of mesh m for the lanes with `on`, in leaf-sized groups, then the
 // mesh's resolve.
-template <bool kCount>
+template <bool kCount, bool kInst>
 __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState& st, bool on, uint32_t m, int lane) {
   const uint32_t owners = __ballot_sync(0xffffffffu, on);
   if (!owners) return;
   const uint4 range = __ldg(&s.meshes[m]);
+  const bool placed = kInst && range.w != kNoneU;
+  if (placed) {
+    st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);  // cone_to_object (:623-638)
+    store_cone(st.ws, st.cone, lane);
+    __syncwarp();
+  }
   if (kCount && on) st.n_tris += range.y;
   for (uint32_t t = range.x; t < range.x + range.y; t += 8)
     st.queued = cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), st.queued, lane);
   resolve_mesh(s, st, lane);
+  if (placed) {
+    st.cone = st.world;
+    store_cone(st.ws, st.cone, lane);
+    __syncwarp();
+  }
 }
 
 // The cone walk (scene_coverage_if, :1160-1227, with add_mesh_coverage_if,
@@ -318,12 +331,13 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState& st, 
 // a lane needs counts toward its walk cap, though its box was tested when its
 // parent was visited. Levels 0 and 1 keep the reference's loops over meshes
 // and triangles.
-template <bool kCount>
+template <bool kCount, bool kInst>
 __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState& st, bool traced,
                                            int lane) {
   const Cone& c = st.cone;
   if (hierarchy == 0) {
-    for (uint32_t m = 0; m < s.nmeshes; ++m) add_mesh_flat<kCount>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
+    for (uint32_t m = 0; m < s.nmeshes; ++m)
+      add_mesh_flat<kCount, kInst>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
     return;
   }
   WarpStack stk;
@@ -334,11 +348,26 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
   int sp = 1;
   while (sp > 0) {
     --sp;
-    const uint32_t ref = stk.get(sp);
-    const uint32_t kind = ref_kind(ref);
+    uint32_t ref = stk.get(sp);
+    uint32_t kind = ref_kind(ref);
     if (kind == kResolve) {
       resolve_mesh(s, st, lane);
+      if (kInst && ref_index(ref) == 1) {  // back to world space
+        st.cone = st.world;
+        store_cone(st.ws, st.cone, lane);
+        __syncwarp();
+      }
       continue;
+    }
+    if (kInst && kind == kObjRoot) {
+      // Entering a placed object: the cone in its space (cone_to_object,
+      // :623-638), then its triangle hierarchy's root.
+      const uint4 range = __ldg(&s.meshes[ref_index(ref)]);
+      st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
+      store_cone(st.ws, st.cone, lane);
+      __syncwarp();
+      ref = node_ref(__ldg(&s.blas[2 * (size_t)range.z + 0]), __ldg(&s.blas[2 * (size_t)range.z + 1]), kTriNode);
+      kind = kTriNode;
     }
     const bool is_obj = kind == kObjNode;
     const bool mine = stk.need(sp) && st.cone_work < st.cap && (!is_obj || st.full < (uint32_t)kBins);
@@ -360,7 +389,8 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
     } else if (ib > 0) {
       // An object leaf: its meshes.
       if (hierarchy == 1) {
-        for (uint32_t k = ia; k < ia + ib; ++k) add_mesh_flat<kCount>(s, st, descend, __ldg(&s.items[k]), lane);
+        for (uint32_t k = ia; k < ia + ib; ++k)
+          add_mesh_flat<kCount, kInst>(s, st, descend, __ldg(&s.items[k]), lane);
         continue;
       }
       for (int k = (int)(ia + ib) - 1; k >= (int)ia; --k) {
@@ -372,9 +402,19 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
         }
         const float4 ma = __ldg(&s.blas[2 * (size_t)range.z + 0]);
         const float4 mb = __ldg(&s.blas[2 * (size_t)range.z + 1]);
-        const bool mesh_pass = descend && may_touch_box(c, node_lo(ma), node_lo(mb));
-        stk.push(sp, kResolve << kRefKindShift, false, false, lane);
-        stk.push(sp + 1, node_ref(ma, mb, kTriNode), descend, mesh_pass, lane);
+        const uint32_t m = __ldg(&s.items[k]);
+        if (kInst && range.w != kNoneU) {
+          // A placed object: its root's box in its own space; the entry names
+          // the object, whose cone is set up when the entry is popped.
+          const Cone oc = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
+          const bool mesh_pass = descend && may_touch_box(oc, node_lo(ma), node_lo(mb));
+          stk.push(sp, (kResolve << kRefKindShift) | 1u, false, false, lane);
+          stk.push(sp + 1, (kObjRoot << kRefKindShift) | m, descend, mesh_pass, lane);
+        } else {
+          const bool mesh_pass = descend && may_touch_box(c, node_lo(ma), node_lo(mb));
+          stk.push(sp, kResolve << kRefKindShift, false, false, lane);
+          stk.push(sp + 1, node_ref(ma, mb, kTriNode), descend, mesh_pass, lane);
+        }
         sp += 2;
       }
     } else {
@@ -501,7 +541,8 @@ __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, ui
 
 // kBatch: the cones of every job of a batch (BatchLaunch); each packet's job
 // is looked up in the job table, and the redo list holds batch cone numbers.
-template <bool kCount, bool kBatch>
+// kInst: the scene's objects place shared geometry with transforms.
+template <bool kCount, bool kBatch, bool kInst>
 // kBlocksPerSm blocks fit the shared memory; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
@@ -598,10 +639,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const LightConeInfo info = light_cone(point, L, q.wide_extent, st.cone);
     const bool traced = on && info.ok;
     st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
+    if (kInst) st.world = st.cone;
     store_cone(ws, st.cone, lane);
     __syncwarp();
 
-    scene_walk<kCount>(s, q.hierarchy, st, traced, lane);
+    scene_walk<kCount, kInst>(s, q.hierarchy, st, traced, lane);
 
     // A grazing sliver stopped at its cap counts as blocked (:1295-1305).
     const bool capped = traced && st.cone_work >= st.cap;
@@ -702,9 +744,9 @@ cudaError_t upload_disk_table(const float* table64) {
 
 // Whether the large dynamic shared memory size was allowed, per device and
 // kernel variant (the attribute is set per device).
-static uint64_t g_attr_set[4] = {0, 0, 0, 0};
+static uint64_t g_attr_set[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
-template <bool kCount, bool kBatch>
+template <bool kCount, bool kBatch, bool kInst>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
@@ -712,14 +754,14 @@ static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
-  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0);
+  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0);
   if (!(g_attr_set[variant] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch>,
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     g_attr_set[variant] |= bit;
   }
-  visibility_kernel<kCount, kBatch><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
+  visibility_kernel<kCount, kBatch, kInst><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
   return cudaGetLastError();
 }
 
@@ -742,16 +784,22 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
   const BatchLaunch none{};
-  cudaError_t e = count ? launch_one<true, false>(s, q, o, none, nullptr, nullptr, pw, blocks, stream)
-                        : launch_one<false, false>(s, q, o, none, nullptr, nullptr, pw, blocks, stream);
+  const bool inst = s.xforms != nullptr;
+  auto one = [&](const uint32_t* list, const uint32_t* list_count, uint32_t p, uint32_t nb) {
+    if (inst)
+      return count ? launch_one<true, false, true>(s, q, o, none, list, list_count, p, nb, stream)
+                   : launch_one<false, false, true>(s, q, o, none, list, list_count, p, nb, stream);
+    return count ? launch_one<true, false, false>(s, q, o, none, list, list_count, p, nb, stream)
+                 : launch_one<false, false, false>(s, q, o, none, list, list_count, p, nb, stream);
+  };
+  cudaError_t e = one(nullptr, nullptr, pw, blocks);
   if (marks) cudaEventRecord(marks[1], stream);
   if (e != cudaSuccess) return e;
   if (o.redo_list) {
     // The listed cones, each walked alone (one cone per warp; the warp still
     // shares its leaves' triangles).
     const uint32_t solo_blocks = (uint32_t)sm_count * kBlocksPerSm;
-    e = count ? launch_one<true, false>(s, q, o, none, o.redo_list, o.redo_count, 1, solo_blocks, stream)
-              : launch_one<false, false>(s, q, o, none, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+    e = one(o.redo_list, o.redo_count, 1, solo_blocks);
   }
   if (marks) cudaEventRecord(marks[2], stream);
   return e;
@@ -767,12 +815,12 @@ cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count, int 
   const uint64_t want = (b.packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
   const uint64_t cap = (uint64_t)sm_count * blocks_per_sm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-  cudaError_t e = count ? launch_one<true, true>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
-                        : launch_one<false, true>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+  cudaError_t e = count ? launch_one<true, true, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
+                        : launch_one<false, true, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
   if (e != cudaSuccess || !o.redo_list) return e;
   const uint32_t solo_blocks = (uint32_t)cap;
-  return count ? launch_one<true, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
-               : launch_one<false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+  return count ? launch_one<true, true, false>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+               : launch_one<false, true, false>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
 }
 
 }  // namespace cc

@@ -199,6 +199,14 @@ class Scene:
         check(load().cc_scene_arrays(self.handle, ptr(ranges), ptr(blas), ptr(blas_items), ptr(nodes), ptr(items)))
         return dict(ranges=ranges, blas=blas, blas_items=blas_items, nodes=nodes, items=items)
 
+    def transforms(self) -> np.ndarray:
+        """The objects' transforms, 16 floats each (instanced scenes; else empty)."""
+        n = int(load().cc_scene_transforms(self.handle, None, 0))
+        out = np.zeros((n, 16), np.float32)
+        if n:
+            load().cc_scene_transforms(self.handle, ptr(out), n)
+        return out
+
     @property
     def device_bytes(self) -> int:
         return int(load().cc_scene_device_bytes(self.handle))
@@ -233,6 +241,32 @@ def host_scene(meshes=None, tri9=None, counts=None) -> Scene:
     h = C.c_void_p()
     check(load().cc_scene_build(None, ptr(tri9), ptr(counts), len(counts), C.byref(h)))
     return Scene(None, h.value)
+
+
+def instances_array(instances) -> np.ndarray:
+    """cc_instance records from an INSTANCE_DTYPE array or (geometry, rotation
+    3x3, scale, translation) tuples."""
+    if isinstance(instances, np.ndarray) and instances.dtype == _lib.INSTANCE_DTYPE:
+        return np.ascontiguousarray(instances)
+    out = np.zeros(len(instances), _lib.INSTANCE_DTYPE)
+    for i, (g, rot, scale, t) in enumerate(instances):
+        out[i] = (g, np.asarray(rot, np.float32).reshape(9), scale, np.asarray(t, np.float32).reshape(3))
+    return out
+
+
+def _build_instanced(handle, geometries, instances) -> int:
+    tri9, counts = flatten_meshes(geometries)
+    inst = instances_array(instances)
+    h = C.c_void_p()
+    check(load().cc_scene_build_instanced(handle, ptr(tri9), ptr(counts), len(counts), ptr(inst), len(inst),
+                                          C.byref(h)))
+    return h.value
+
+
+def host_scene_instanced(geometries, instances) -> Scene:
+    """An instanced scene built on the host only (hierarchies to inspect and
+    ray cast)."""
+    return Scene(None, _build_instanced(None, geometries, instances))
 
 
 class MaskConeKernel:
@@ -315,6 +349,11 @@ class MaskConeKernel:
         tri9, counts = flatten_meshes(meshes)
         return self.scene_from_tri9(tri9, counts)
 
+    def scene_instanced(self, geometries, instances) -> Scene:
+        """An instanced scene: shared geometries (object space) placed by
+        transforms (flatten_instanced, hierarchy.rs:464-522)."""
+        return Scene(self, _build_instanced(self.handle, geometries, instances))
+
     def scene_from_tri9(self, tri9: np.ndarray, counts: np.ndarray) -> Scene:
         tri9 = np.ascontiguousarray(tri9, dtype=np.float32)
         counts = np.ascontiguousarray(counts, dtype=np.uint32)
@@ -329,7 +368,7 @@ class MaskConeKernel:
                 np.ascontiguousarray(nodes), np.ascontiguousarray(items, np.uint32)]
         f = _lib.FlatScene(ptr(arrs[0]), arrs[0].size // 12, ptr(arrs[1]), arrs[1].size // 4, ptr(arrs[2]),
                            len(arrs[2]), ptr(arrs[3]), arrs[3].size, ptr(arrs[4]), len(arrs[4]), ptr(arrs[5]),
-                           arrs[5].size)
+                           arrs[5].size, None, 0)
         h = C.c_void_p()
         check(load().cc_scene_upload(self.handle, C.byref(f), C.byref(h)))
         return Scene(self, h.value)

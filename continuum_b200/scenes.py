@@ -439,3 +439,96 @@ def served_requests(scenes_: list, n: int, seed: int = 5, moved: float = 0.5) ->
                 recs.append(rec)
         reqs.append((si, pi, np.ascontiguousarray(np.stack(recs).astype(np.float32))))
     return reqs
+
+
+def displaced_uv_sphere(seed: int, segments: int = 80, rings: int = 65, amplitude: float = 0.15,
+                        frequency: float = 2.0) -> np.ndarray:
+    """A unit UV sphere (segments x (2 rings - 2) triangles: 10,240 for 80 x 65)
+    with vertices moved radially by seeded value noise of amplitude
+    `amplitude`, centred at the origin, +Z poles, outward winding."""
+    base = sphere_mesh((0.0, 0.0, 0.0), 1.0, segments, rings).astype(np.float64)
+    flat = base.reshape(-1, 3)
+    unit = flat / np.linalg.norm(flat, axis=1, keepdims=True)
+    scale = 1.0 + amplitude * value_noise(unit * frequency, seed)
+    return (unit * scale[:, None]).reshape(-1, 3, 3).astype(np.float32)
+
+
+@dataclass
+class InstancedWorld:
+    """Shared geometries (object space), cc_instance records placing them, lights
+    and receivers."""
+
+    geometries: list
+    instances: np.ndarray
+    lights: np.ndarray
+    receivers: Optional[np.ndarray] = None
+    camera: Optional[np.ndarray] = None
+    size: Optional[tuple] = None
+
+    @property
+    def instanced_tris(self) -> int:
+        counts = np.array([len(g) for g in self.geometries])
+        return int(counts[self.instances["geometry"]].sum())
+
+
+def yaw_rotation(angle: float) -> np.ndarray:
+    """Rotation about +Y by `angle`, row-major."""
+    c, s = math.cos(angle), math.sin(angle)
+    return np.array([[c, 0.0, s], [0.0, 1.0, 0.0], [-s, 0.0, c]], np.float32)
+
+
+def instanced_world(seed: int = 5, n_instances: int = 1_000_000, n_boulders: int = 10, half: float = 2000.0,
+                    n_lights: int = 8, width: int = 1280, height: int = 720, segments: int = 80, rings: int = 65,
+                    with_receivers: bool = True) -> InstancedWorld:
+    """The instanced large world: `n_boulders` displaced UV-sphere boulders
+    (10,240 triangles each at 80 x 65) placed as `n_instances` instances with
+    scale U[0.5, 4], yaw U[0, 2 pi] and positions U[-half, half]^2 resting on a
+    ground quad (itself one more instance); `n_lights` rect and disk lights
+    (as batch_jobs') over the camera's view; the primary hits of a seeded
+    camera (misses dropped)."""
+    rng = Pcg32(seed, 66)
+    geometries = [displaced_uv_sphere(seed * 100 + k, segments, rings) for k in range(n_boulders)]
+    geometries.append(ground_quad(1.0))
+    ground = len(geometries) - 1
+    inst = np.zeros(n_instances + 1, _lib_instance_dtype())
+    eye_r = np.random.default_rng(seed)  # placements: vectorized, seeded
+    g = eye_r.integers(0, n_boulders, n_instances)
+    scale = eye_r.uniform(0.5, 4.0, n_instances).astype(np.float32)
+    yaw = eye_r.uniform(0.0, 2.0 * math.pi, n_instances)
+    x = eye_r.uniform(-half, half, n_instances).astype(np.float32)
+    z = eye_r.uniform(-half, half, n_instances).astype(np.float32)
+    c, s = np.cos(yaw).astype(np.float32), np.sin(yaw).astype(np.float32)
+    rot = np.zeros((n_instances, 9), np.float32)
+    rot[:, 0], rot[:, 2], rot[:, 4], rot[:, 6], rot[:, 8] = c, s, 1.0, -s, c
+    inst["geometry"][:n_instances] = g
+    inst["rotation"][:n_instances] = rot
+    inst["scale"][:n_instances] = scale
+    inst["translation"][:n_instances] = np.stack([x, scale, z], 1)
+    inst[n_instances] = (ground, np.eye(3, dtype=np.float32).reshape(9), half * 1.05, (0.0, 0.0, 0.0))
+    # The camera looks at a seeded spot; the lights hang over what it sees.
+    cx, cz = rng.uniform(-0.5 * half, 0.5 * half), rng.uniform(-0.5 * half, 0.5 * half)
+    az = 2.0 * math.pi * rng.next_f32()
+    camera = np.array([cx + 60.0 * math.sin(az), 35.0, cz - 60.0 * math.cos(az), cx, 0.0, cz, 0.0, 1.0, 0.0, 60.0],
+                      np.float32)
+    objs = []
+    for _ in range(n_lights):
+        l = _random_light(rng, 40.0)
+        objs.append(l)
+    lights = np.stack([light_gpu(l) for l in objs])
+    lights[:, 0] += cx  # over the view (corner / centre x and z)
+    lights[:, 2] += cz
+    w = InstancedWorld(geometries, inst, lights, None, camera, (width, height))
+    if with_receivers:
+        from .kernel import host_scene_instanced
+        hs = host_scene_instanced(geometries, inst)
+        try:
+            rec, hit = hs.primary_hits(camera, width, height)
+        finally:
+            hs.close()
+        w.receivers = np.ascontiguousarray(rec[hit.astype(bool)])
+    return w
+
+
+def _lib_instance_dtype():
+    from ._lib import INSTANCE_DTYPE
+    return INSTANCE_DTYPE

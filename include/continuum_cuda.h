@@ -89,7 +89,7 @@ CC_API const char* cc_last_error(void);
 typedef struct cc_flat_scene {
   const float* tris;          /* 12 floats per triangle */
   uint32_t ntris;
-  const uint32_t* ranges;     /* 4 per mesh: first, count, blas root or CC_NONE, transform (CC_NONE) */
+  const uint32_t* ranges;     /* 4 per mesh: first, count, blas root or CC_NONE, transform index or CC_NONE */
   uint32_t nmeshes;
   const void* blas;           /* NodeGpu per triangle-hierarchy node */
   uint32_t nblas;
@@ -99,6 +99,8 @@ typedef struct cc_flat_scene {
   uint32_t nnodes;
   const uint32_t* items;      /* mesh index per object leaf slot */
   uint32_t nitems;
+  const float* xforms;        /* instanced scenes: 16 floats per transform (nullable), see cc_scene_build_instanced */
+  uint32_t nxforms;
 } cc_flat_scene;
 
 CC_API int cc_scene_upload(cc_context* ctx, const cc_flat_scene* flat, cc_scene** out);
@@ -112,6 +114,32 @@ CC_API int cc_scene_upload(cc_context* ctx, const cc_flat_scene* flat, cc_scene*
 CC_API int cc_scene_build(cc_context* ctx, const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes,
                    cc_scene** out);
 CC_API int cc_scene_destroy(cc_scene* scene);
+
+/* An object placing a geometry: world = scale * rotation * p + translation,
+ * rotation orthonormal (row-major), scale positive (Placement,
+ * crates/continuum-gpu/src/hierarchy.rs:258-270; opaque objects). */
+typedef struct cc_instance {
+  uint32_t geometry;
+  float rotation[9];
+  float scale;
+  float translation[3];
+} cc_instance;
+
+/* An instanced scene (flatten_instanced, hierarchy.rs:464-522): each
+ * geometry's triangles (9 floats each, object space) and triangle hierarchy
+ * once, one object per instance pointing at its geometry with a transform,
+ * and the object hierarchy over the objects' padded world bounds
+ * (object_hierarchy, :198-253). Cones are walked into each object's space as
+ * the reference's cone_to_object does (mask_cones.wgsl:623-638). The
+ * transforms are stored as the reference's shader reads them: rows 0-2 of the
+ * rotation with the translation in w, then (scale, 1 / scale, 0, 0). With ctx
+ * NULL the scene stays on the host. */
+CC_API int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const uint32_t* geometry_counts,
+                                    uint32_t ngeometries, const cc_instance* instances, uint32_t ninstances,
+                                    cc_scene** out);
+/* The scene's transforms (16 floats each) into out16 (nullable, at most
+ * max_transforms); returns their count (0 for a scene without instancing). */
+CC_API uint64_t cc_scene_transforms(const cc_scene* scene, float* out16, uint64_t max_transforms);
 
 /* Sizes of the scene's flattened host arrays: ntris, nmeshes, nblas,
  * nblas_items, nnodes, nitems; and copies of them (NodeGpu layout, any

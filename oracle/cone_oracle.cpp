@@ -142,6 +142,10 @@ struct Scene {
   std::vector<Node> nodes;       // object hierarchy (mesh_hierarchy)
   std::vector<uint32_t> items;
   uint32_t nmeshes = 0;
+  // Instanced scenes: per transform, rows 0-2 of the rotation with the
+  // translation in w, then (scale, 1 / scale, 0, 0) (Placement::rows,
+  // hierarchy.rs:272-285); ranges[4 * m + 3] names object m's.
+  std::vector<float> xforms;
 };
 
 static void mesh_bounds(const float* tris, uint32_t first, uint32_t count, F3& lo, F3& hi) {
@@ -154,6 +158,47 @@ static void mesh_bounds(const float* tris, uint32_t first, uint32_t count, F3& l
       lo = vmin(lo, p);
       hi = vmax(hi, p);
     }
+}
+
+// object_hierarchy (hierarchy.rs:198-253): at most two objects per leaf,
+// oversized objects (diagonal > 64 x median) in their own subtree.
+static void object_hierarchy(Scene* s, const std::vector<std::pair<F3, F3>>& mesh_box) {
+  const uint32_t nmeshes = (uint32_t)mesh_box.size();
+  std::vector<uint32_t> items(nmeshes);
+  std::iota(items.begin(), items.end(), 0u);
+  s->nodes.assign(1, Node{});
+  if (items.empty()) {
+    s->items = {0};
+    s->nodes[0].info[1] = 1;
+    return;
+  }
+  auto diagonal = [&](uint32_t m) { return length(mesh_box[m].second - mesh_box[m].first); };
+  std::vector<float> sizes(nmeshes);
+  for (uint32_t i = 0; i < nmeshes; ++i) sizes[i] = diagonal(i);
+  size_t mid = sizes.size() / 2;
+  std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
+  float median = sizes[mid];
+  std::vector<uint32_t> big, small;
+  for (uint32_t m : items) (diagonal(m) > 64.0f * median ? big : small).push_back(m);
+  if (big.empty() || small.empty()) {
+    split(s->nodes, 0, items.data(), items.size(), 0, mesh_box, 2, 0, 0);
+  } else {
+    size_t nb = big.size();
+    items = big;
+    items.insert(items.end(), small.begin(), small.end());
+    s->nodes.push_back(Node{});
+    s->nodes.push_back(Node{});
+    split(s->nodes, 1, items.data(), nb, 0, mesh_box, 2, 0, 0);
+    split(s->nodes, 2, items.data() + nb, items.size() - nb, nb, mesh_box, 2, 0, 0);
+    Node& r = s->nodes[0];
+    const Node &a = s->nodes[1], &b = s->nodes[2];
+    for (int k = 0; k < 3; ++k) {
+      r.lo[k] = std::min(a.lo[k], b.lo[k]);
+      r.hi[k] = std::max(a.hi[k], b.hi[k]);
+    }
+    r.info[0] = 1;
+  }
+  s->items = items;
 }
 
 // flatten + triangle_hierarchy + mesh_hierarchy/object_hierarchy
@@ -200,43 +245,56 @@ static Scene* build_scene(const float* tri9, const uint32_t* mesh_counts, uint32
     mesh_box[m] = {lo, hi};
     first += count;
   }
-  // object_hierarchy (hierarchy.rs:198-253): at most two meshes per leaf,
-  // oversized meshes (diagonal > 64 x median) in their own subtree.
-  std::vector<uint32_t> items(nmeshes);
-  std::iota(items.begin(), items.end(), 0u);
-  s->nodes.assign(1, Node{});
-  if (items.empty()) {
-    s->items = {0};
-    s->nodes[0].info[1] = 1;
-    return s;
-  }
-  auto diagonal = [&](uint32_t m) { return length(mesh_box[m].second - mesh_box[m].first); };
-  std::vector<float> sizes(nmeshes);
-  for (uint32_t i = 0; i < nmeshes; ++i) sizes[i] = diagonal(i);
-  size_t mid = sizes.size() / 2;
-  std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
-  float median = sizes[mid];
-  std::vector<uint32_t> big, small;
-  for (uint32_t m : items) (diagonal(m) > 64.0f * median ? big : small).push_back(m);
-  if (big.empty() || small.empty()) {
-    split(s->nodes, 0, items.data(), items.size(), 0, mesh_box, 2, 0, 0);
-  } else {
-    size_t nb = big.size();
-    items = big;
-    items.insert(items.end(), small.begin(), small.end());
-    s->nodes.push_back(Node{});
-    s->nodes.push_back(Node{});
-    split(s->nodes, 1, items.data(), nb, 0, mesh_box, 2, 0, 0);
-    split(s->nodes, 2, items.data() + nb, items.size() - nb, nb, mesh_box, 2, 0, 0);
-    Node& r = s->nodes[0];
-    const Node &a = s->nodes[1], &b = s->nodes[2];
-    for (int k = 0; k < 3; ++k) {
-      r.lo[k] = std::min(a.lo[k], b.lo[k]);
-      r.hi[k] = std::max(a.hi[k], b.hi[k]);
+  object_hierarchy(s, mesh_box);
+  return s;
+}
+
+// One object placing a geometry (cc_instance's layout): world = scale *
+// rotation * p + translation, rotation row-major.
+struct Instance {
+  uint32_t geometry;
+  float rotation[9];
+  float scale;
+  float translation[3];
+};
+
+// flatten_instanced (hierarchy.rs:464-522) + object_hierarchy over the
+// objects' padded world bounds (Placement::world_bounds, :287-303).
+static Scene* build_instanced(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
+                              const Instance* inst, uint32_t ninstances) {
+  Scene* s = build_scene(tri9, geometry_counts, ngeometries);
+  const std::vector<uint32_t> geometry = s->ranges;
+  std::vector<std::pair<F3, F3>> local(ngeometries);
+  for (uint32_t g = 0; g < ngeometries; ++g) mesh_bounds(s->tris.data(), geometry[4 * g], geometry[4 * g + 1], local[g].first, local[g].second);
+  s->ranges.clear();
+  std::vector<std::pair<F3, F3>> box(ninstances);
+  for (uint32_t k = 0; k < ninstances; ++k) {
+    const Instance& o = inst[k];
+    const uint32_t* r = &geometry[4 * o.geometry];
+    s->ranges.insert(s->ranges.end(), {r[0], r[1], r[2], k});
+    const float* R = o.rotation;
+    const float* t = o.translation;
+    s->xforms.insert(s->xforms.end(), {R[0], R[1], R[2], t[0], R[3], R[4], R[5], t[1], R[6], R[7], R[8], t[2],
+                                       o.scale, 1.0f / o.scale, 0.0f, 0.0f});
+    F3 lo{FLT_MAX, FLT_MAX, FLT_MAX}, hi{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    const F3 a = local[o.geometry].first, b = local[o.geometry].second;
+    for (int c = 0; c < 8; ++c) {
+      const F3 p{(c & 1) ? b.x : a.x, (c & 2) ? b.y : a.y, (c & 4) ? b.z : a.z};
+      const F3 w{(R[0] * p.x + R[1] * p.y + R[2] * p.z) * o.scale + t[0],
+                 (R[3] * p.x + R[4] * p.y + R[5] * p.z) * o.scale + t[1],
+                 (R[6] * p.x + R[7] * p.y + R[8] * p.z) * o.scale + t[2]};
+      lo = vmin(lo, w);
+      hi = vmax(hi, w);
     }
-    r.info[0] = 1;
+    padded(lo, hi);
+    box[k] = {lo, hi};
   }
-  s->items = items;
+  if (s->ranges.empty()) s->ranges.insert(s->ranges.end(), {0u, 0u, NONE, NONE});
+  if (s->xforms.empty()) s->xforms.assign(16, 0.0f);
+  s->nmeshes = (uint32_t)(s->ranges.size() / 4);
+  s->nodes.clear();
+  s->items.clear();
+  object_hierarchy(s, box);
   return s;
 }
 
@@ -570,13 +628,34 @@ template <class R> struct Walk {
 
 constexpr int STACK = 64;
 
+// cone_to_object (:623-638) with rotate_to_object, translation and
+// point_to_object (:61-78): the cone in the space of the object placed by
+// transform x.
+template <class R> Cone<R> cone_to_object(const Scene& s, const Cone<R>& c, uint32_t x) {
+  const float* X = s.xforms.data() + 16 * (size_t)x;
+  const V3<R> r0{R(X[0]), R(X[1]), R(X[2])}, r1{R(X[4]), R(X[5]), R(X[6])}, r2{R(X[8]), R(X[9]), R(X[10])};
+  const V3<R> t{R(X[3]), R(X[7]), R(X[11])};
+  const R inv_scale = R(X[13]);
+  auto rot = [&](V3<R> d) { return r0 * d.x + r1 * d.y + r2 * d.z; };
+  Cone<R> o = c;
+  o.apex = rot(c.apex - t) * inv_scale;
+  o.right = rot(c.right);
+  o.up = rot(c.up);
+  o.forward = rot(c.forward);
+  o.far_normal = rot(c.far_normal);
+  o.far_offset = (c.far_offset - dot(c.far_normal, t)) * inv_scale;
+  o.bound_axis = rot(c.bound_axis);
+  return o;
+}
+
 // add_mesh_coverage_if for one cone walking alone (:713-829).
-template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& c, uint32_t m, Walk<R>& wk,
+template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, uint32_t m, Walk<R>& wk,
                                           uint32_t hierarchy) {
   Acc<R> acc;
   acc.reset();
   bool touched = false;
   const uint32_t* range = s.ranges.data() + 4 * m;
+  const Cone<R> c = range[3] != NONE ? cone_to_object(s, world, range[3]) : world;
   if (hierarchy == 2) {
     if (range[2] != NONE) {
       uint32_t stack[STACK];
@@ -1405,6 +1484,20 @@ extern "C" {
 // triangle, `mesh_counts[m]` triangles each, consecutive.
 void* oracle_scene_create(const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes) {
   return build_scene(tri9, mesh_counts, nmeshes);
+}
+
+// An instanced scene: geometries given as 9 floats per triangle (object
+// space), instances as cc_instance records.
+void* oracle_scene_create_instanced(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
+                                    const void* instances, uint32_t ninstances) {
+  return build_instanced(tri9, geometry_counts, ngeometries, static_cast<const Instance*>(instances), ninstances);
+}
+
+// The scene's transforms (16 floats each) into out (nullable); returns their count.
+uint64_t oracle_scene_transforms(void* sp, float* out) {
+  Scene* s = static_cast<Scene*>(sp);
+  if (out) std::memcpy(out, s->xforms.data(), s->xforms.size() * sizeof(float));
+  return s->xforms.size() / 16;
 }
 
 void oracle_scene_destroy(void* s) { delete static_cast<Scene*>(s); }

@@ -42,6 +42,10 @@ def load():
         lib.oracle_cpu_weights.restype = I
         lib.oracle_cpu_weights.argtypes = [P, P, P, P]
         lib.oracle_poly_overflows.restype = U64
+        lib.oracle_scene_create_instanced.restype = P
+        lib.oracle_scene_create_instanced.argtypes = [P, P, U32, P, U32]
+        lib.oracle_scene_transforms.restype = U64
+        lib.oracle_scene_transforms.argtypes = [P, P]
         _lib = lib
     return _lib
 
@@ -65,6 +69,26 @@ class OracleScene:
         self.tri9 = np.ascontiguousarray(tri9, np.float32)
         self.counts = np.ascontiguousarray(counts, np.uint32)
         self._h = C.c_void_p(load().oracle_scene_create(_p(self.tri9), _p(self.counts), len(self.counts)))
+
+    @classmethod
+    def instanced(cls, geometries, instances: np.ndarray) -> "OracleScene":
+        """An instanced scene: geometries (object space) placed by cc_instance
+        records (flatten_instanced, hierarchy.rs:464-522)."""
+        self = cls.__new__(cls)
+        parts = [np.asarray(m, np.float32).reshape(-1, 9) for m in geometries]
+        self.tri9 = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros((0, 9), np.float32))
+        self.counts = np.array([len(p) for p in parts], np.uint32)
+        self.instances = np.ascontiguousarray(instances)
+        self._h = C.c_void_p(load().oracle_scene_create_instanced(_p(self.tri9), _p(self.counts), len(self.counts),
+                                                                  _p(self.instances), len(self.instances)))
+        return self
+
+    def transforms(self) -> np.ndarray:
+        n = int(load().oracle_scene_transforms(self._h, None))
+        out = np.zeros((n, 16), np.float32)
+        if n:
+            load().oracle_scene_transforms(self._h, _p(out))
+        return out
 
     def sizes(self) -> dict:
         out = np.zeros(6, np.uint64)
