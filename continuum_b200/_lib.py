@@ -42,7 +42,8 @@ EXPORTS = (
     "cc_visibility_static", "cc_batch_options_default", "cc_batch_create", "cc_batch_destroy", "cc_batch_clear",
     "cc_batch_add", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
     "cc_server_options_default", "cc_server_create", "cc_server_destroy", "cc_server_add_scene", "cc_server_submit",
-    "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms",
+    "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms", "cc_scene_move",
+    "cc_stale_cones", "cc_visibility_update",
 )
 
 # cc_instance: an object placing a geometry (world = scale * rotation * p + translation).
@@ -148,7 +149,10 @@ def load() -> C.CDLL:
         "cc_server_submit": (I, [P, C.POINTER(Request), C.POINTER(U64)]),
         "cc_server_wait": (I, [P, U64, U32, C.POINTER(RequestStats)]),
         "cc_server_stats": (I, [P, P]),
-        "cc_scene_build_instanced": (I, [P, P, P, U32, P, U32, C.POINTER(P)]),
+        "cc_scene_build_instanced": (I, [P, P, P, U32, P, U32, P, U32, C.POINTER(P)]),
+        "cc_scene_move": (I, [P, P, U32, P]),
+        "cc_stale_cones": (I, [P, P, P, U64, P, U32, P, U32, P, C.POINTER(U64), P]),
+        "cc_visibility_update": (I, [P, P, P, U64, P, U32, P, C.POINTER(Options), C.POINTER(Outputs), C.POINTER(U64), P]),
         "cc_scene_transforms": (U64, [P, P, U64]),
     }
     for name, (res, args) in sig.items():

@@ -38,6 +38,12 @@ void padded(Box& b) {
   }
 }
 
+// Nodes of a tree over n > 0 items with at most `leaf` per leaf: fixed by n.
+uint64_t node_count_for(uint64_t n, uint64_t leaf) {
+  if (n <= leaf) return 1;
+  return 1 + node_count_for(n / 2, leaf) + node_count_for(n - n / 2, leaf);
+}
+
 Box bounds_of(const float* tris12, uint32_t first, uint32_t count) {
   Box b{{FLT_MAX, FLT_MAX, FLT_MAX}, {-FLT_MAX, -FLT_MAX, -FLT_MAX}};
   for (uint32_t t = first; t < first + count; ++t)
@@ -135,10 +141,10 @@ struct Builder {
 // object_hierarchy (hierarchy.rs:198-253): two objects per leaf over the
 // objects' padded world bounds, with oversized objects in a subtree of their
 // own under the root.
-void object_hierarchy(const std::vector<Box>& mesh_box, std::vector<NodeGpu>& nodes_out, std::vector<uint32_t>& items_out) {
-  const uint32_t nmeshes = (uint32_t)mesh_box.size();
-  std::vector<uint32_t> items(nmeshes);
-  std::iota(items.begin(), items.end(), 0u);
+void object_hierarchy(const std::vector<Box>& mesh_box, const std::vector<uint32_t>& keep,
+                      std::vector<NodeGpu>& nodes_out, std::vector<uint32_t>& items_out) {
+  std::vector<uint32_t> items = keep;
+  const size_t nmeshes = items.size();
   std::vector<NodeGpu>& nodes = nodes_out;
   nodes.assign(1, NodeGpu{});
   if (items.empty()) {
@@ -155,7 +161,7 @@ void object_hierarchy(const std::vector<Box>& mesh_box, std::vector<NodeGpu>& no
     return std::sqrt(d2);
   };
   std::vector<float> sizes(nmeshes);
-  for (uint32_t m = 0; m < nmeshes; ++m) sizes[m] = diagonal(m);
+  for (size_t i = 0; i < nmeshes; ++i) sizes[i] = diagonal(items[i]);
   size_t mid = sizes.size() / 2;
   std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
   const float median = sizes[mid];
@@ -268,11 +274,76 @@ void build_flat_scene(const float* tri9, const uint32_t* mesh_counts, uint32_t n
   }
 
   // The object hierarchy over meshes (object_hierarchy, hierarchy.rs:198-253).
-  object_hierarchy(mesh_box, out.nodes, out.items);
+  std::vector<uint32_t> all(nmeshes);
+  std::iota(all.begin(), all.end(), 0u);
+  object_hierarchy(mesh_box, all, out.nodes, out.items);
 }
 
+namespace {
+
+// The padded world bounds of an object-space box placed by `o`
+// (Placement::world_bounds, hierarchy.rs:287-303).
+Box world_bounds(const Box& b, const Instance& o) {
+  const float* R = o.rotation;
+  const float* t = o.translation;
+  Box w{{FLT_MAX, FLT_MAX, FLT_MAX}, {-FLT_MAX, -FLT_MAX, -FLT_MAX}};
+  for (int c = 0; c < 8; ++c) {
+    const float p[3] = {(c & 1) ? b.hi[0] : b.lo[0], (c & 2) ? b.hi[1] : b.lo[1], (c & 4) ? b.hi[2] : b.lo[2]};
+    for (int i = 0; i < 3; ++i) {
+      // rotation * p (columns scaled by p's components, summed in order),
+      // then * scale + translation.
+      const float v = (R[3 * i] * p[0] + R[3 * i + 1] * p[1] + R[3 * i + 2] * p[2]) * o.scale + t[i];
+      w.lo[i] = std::min(w.lo[i], v);
+      w.hi[i] = std::max(w.hi[i], v);
+    }
+  }
+  padded(w);
+  return w;
+}
+
+void to_node_bounds(const Box& b, NodeGpu& n) {
+  for (int k = 0; k < 3; ++k) {
+    n.lo[k] = b.lo[k];
+    n.hi[k] = b.hi[k];
+  }
+}
+
+// The root over the static subtree (node 1) and the movers' (node 2)
+// (union_root, hierarchy.rs:372-381).
+NodeGpu union_root(const NodeGpu& a, const NodeGpu& b) {
+  NodeGpu r{};
+  for (int k = 0; k < 3; ++k) {
+    r.lo[k] = std::min(a.lo[k], b.lo[k]);
+    r.hi[k] = std::max(a.hi[k], b.hi[k]);
+  }
+  r.info[0] = 1;
+  r.info[2] = kNoSplat;
+  return r;
+}
+
+// mover_subtree (hierarchy.rs:383-410): the movers' subtree over their
+// current bounds, in the movers' order; its shape depends only on their
+// count. Writes its root to nodes[2], its other nodes from first_node and
+// its items from first_item.
+void mover_subtree(FlatScene& s, const std::vector<Box>& mover_bounds) {
+  const MoverTree& t = s.movers;
+  std::vector<NodeGpu> local(1);
+  std::vector<uint32_t> order(mover_bounds.size());
+  std::iota(order.begin(), order.end(), 0u);
+  Builder b{mover_bounds, kLeafObjects, t.first_node - 1, t.first_item, 0};
+  b.split(local, 0, order.data(), order.size(), 0, 0);
+  for (NodeGpu& n : local) n.info[2] = kNoSplat;
+  s.nodes[2] = local[0];
+  for (size_t i = 1; i < local.size(); ++i) s.nodes[t.first_node + i - 1] = local[i];
+  for (size_t k = 0; k < order.size(); ++k) s.items[t.first_item + k] = t.objects[order[k]];
+  s.nodes[0] = union_root(s.nodes[1], s.nodes[2]);
+}
+
+}  // namespace
+
 void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
-                           const Instance* instances, uint32_t ninstances, FlatScene& out, int threads) {
+                           const Instance* instances, uint32_t ninstances, const uint32_t* movable,
+                           uint32_t nmovable, FlatScene& out, int threads) {
   // Each geometry's triangles and hierarchy once (flatten, triangle_hierarchy).
   build_flat_scene(tri9, geometry_counts, ngeometries, out, threads);
   const std::vector<uint32_t> geometry_ranges = out.ranges;
@@ -285,6 +356,7 @@ void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, u
   out.ranges.clear();
   out.xforms.clear();
   std::vector<Box> bounds(ninstances);
+  out.object_geometry.assign(ninstances, 0);
   for (uint32_t k = 0; k < ninstances; ++k) {
     const Instance& o = instances[k];
     const uint32_t* r = &geometry_ranges[4 * o.geometry];
@@ -293,25 +365,95 @@ void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, u
     const float* t = o.translation;
     out.xforms.insert(out.xforms.end(), {R[0], R[1], R[2], t[0], R[3], R[4], R[5], t[1], R[6], R[7], R[8], t[2],
                                          o.scale, 1.0f / o.scale, 0.0f, 0.0f});
-    Box w{{FLT_MAX, FLT_MAX, FLT_MAX}, {-FLT_MAX, -FLT_MAX, -FLT_MAX}};
-    const Box& b = local[o.geometry];
-    for (int c = 0; c < 8; ++c) {
-      const float p[3] = {(c & 1) ? b.hi[0] : b.lo[0], (c & 2) ? b.hi[1] : b.lo[1], (c & 4) ? b.hi[2] : b.lo[2]};
-      for (int i = 0; i < 3; ++i) {
-        // rotation * p (columns scaled by p's components, summed in order),
-        // then * scale + translation.
-        const float v = (R[3 * i] * p[0] + R[3 * i + 1] * p[1] + R[3 * i + 2] * p[2]) * o.scale + t[i];
-        w.lo[i] = std::min(w.lo[i], v);
-        w.hi[i] = std::max(w.hi[i], v);
-      }
-    }
-    padded(w);
-    bounds[k] = w;
+    out.object_geometry[k] = o.geometry;
+    bounds[k] = world_bounds(local[o.geometry], o);
   }
+  out.geometry_bounds.resize(6 * (size_t)ngeometries);
+  for (uint32_t g = 0; g < ngeometries; ++g)
+    for (int k = 0; k < 3; ++k) {
+      out.geometry_bounds[6 * g + k] = local[g].lo[k];
+      out.geometry_bounds[6 * g + 3 + k] = local[g].hi[k];
+    }
   if (out.ranges.empty()) out.ranges.insert(out.ranges.end(), {0u, 0u, kNone, kNone});
   if (out.xforms.empty()) out.xforms.assign(16, 0.0f);
   out.nmeshes = (uint32_t)(out.ranges.size() / 4);
-  object_hierarchy(bounds, out.nodes, out.items);
+  out.movers = MoverTree{};
+  if (nmovable == 0) {
+    std::vector<uint32_t> all(ninstances);
+    std::iota(all.begin(), all.end(), 0u);
+    object_hierarchy(bounds, all, out.nodes, out.items);
+    return;
+  }
+  // object_hierarchy_with_movers (hierarchy.rs:331-369): the static objects'
+  // hierarchy under node 1 (its node i >= 1 at i + 2), the movers' subtree
+  // under node 2, the root over both.
+  std::vector<uint8_t> is_movable(ninstances, 0);
+  for (uint32_t i = 0; i < nmovable; ++i) is_movable[movable[i]] = 1;
+  std::vector<uint32_t> fixed_items;
+  for (uint32_t m = 0; m < ninstances; ++m)
+    if (!is_movable[m]) fixed_items.push_back(m);
+  std::vector<NodeGpu> fixed;
+  std::vector<uint32_t> items;
+  object_hierarchy(bounds, fixed_items, fixed, items);
+  auto place = [](uint32_t i) { return i == 0 ? 1u : i + 2u; };
+  MoverTree& t = out.movers;
+  t.first_node = (uint32_t)fixed.size() + 2;
+  t.first_item = (uint32_t)items.size();
+  t.objects.assign(movable, movable + nmovable);
+  const uint64_t mover_nodes = node_count_for(nmovable, kLeafObjects);
+  t.nodes = (uint32_t)(mover_nodes - 1);
+  out.nodes.assign(t.first_node + t.nodes, NodeGpu{});
+  for (size_t i = 0; i < fixed.size(); ++i) {
+    NodeGpu n = fixed[i];
+    if (n.info[1] == 0) n.info[0] = place(n.info[0]);
+    out.nodes[place((uint32_t)i)] = n;
+  }
+  out.items = items;
+  out.items.resize(items.size() + nmovable);
+  std::vector<Box> mover_bounds(nmovable);
+  for (uint32_t i = 0; i < nmovable; ++i) mover_bounds[i] = bounds[movable[i]];
+  mover_subtree(out, mover_bounds);
+}
+
+void move_instances(FlatScene& s, const Instance* placements, float* boxes12) {
+  const MoverTree& t = s.movers;
+  std::vector<Box> mover_bounds(t.objects.size());
+  for (size_t i = 0; i < t.objects.size(); ++i) {
+    const uint32_t m = t.objects[i];
+    const uint32_t x = s.ranges[4 * m + 3];
+    float* X = &s.xforms[16 * (size_t)x];
+    const uint32_t g = s.object_geometry[m];
+    Box local;
+    for (int k = 0; k < 3; ++k) {
+      local.lo[k] = s.geometry_bounds[6 * g + k];
+      local.hi[k] = s.geometry_bounds[6 * g + 3 + k];
+    }
+    // The old place: the transform as stored.
+    Instance old{};
+    old.geometry = g;
+    for (int r = 0; r < 3; ++r) {
+      for (int c = 0; c < 3; ++c) old.rotation[3 * r + c] = X[4 * r + c];
+      old.translation[r] = X[4 * r + 3];
+    }
+    old.scale = X[12];
+    const Box before = world_bounds(local, old);
+    const Instance& o = placements[i];
+    const float* R = o.rotation;
+    const float* tr = o.translation;
+    const float row[16] = {R[0], R[1], R[2], tr[0], R[3], R[4], R[5], tr[1], R[6], R[7], R[8], tr[2],
+                           o.scale, 1.0f / o.scale, 0.0f, 0.0f};
+    std::memcpy(X, row, sizeof(row));
+    mover_bounds[i] = world_bounds(local, o);
+    if (boxes12) {
+      for (int k = 0; k < 3; ++k) {
+        boxes12[12 * i + k] = before.lo[k];
+        boxes12[12 * i + 3 + k] = before.hi[k];
+        boxes12[12 * i + 6 + k] = mover_bounds[i].lo[k];
+        boxes12[12 * i + 9 + k] = mover_bounds[i].hi[k];
+      }
+    }
+  }
+  mover_subtree(s, mover_bounds);
 }
 
 }  // namespace cc

@@ -22,6 +22,17 @@ constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kLeafTriangles = 8;  // LEAF_TRIANGLES, hierarchy.rs:727
 constexpr uint32_t kLeafObjects = 2;    // object_hierarchy leaves, hierarchy.rs:198
 constexpr float kOversized = 64.0f;     // OVERSIZED, hierarchy.rs:257
+constexpr uint32_t kNoSplat = 1;        // NO_SPLAT (info.z of the movers' nodes and the root), hierarchy.rs:307
+
+// Where the movable objects' subtree lives (MoverTree, hierarchy.rs:309-327):
+// its root is node 2 (node 1 roots the static objects), its other nodes are
+// `nodes` from `first_node`, its items the movers' count from `first_item`.
+struct MoverTree {
+  uint32_t first_node = 0;
+  uint32_t nodes = 0;
+  uint32_t first_item = 0;
+  std::vector<uint32_t> objects;  // the movable objects, in the order their placements are given
+};
 
 struct FlatScene {
   std::vector<float> tris;          // 12 floats per triangle
@@ -36,6 +47,9 @@ struct FlatScene {
   // object's range points at its geometry and ranges[4 * m + 3] at its
   // transform. Empty for scenes whose triangles are in world space.
   std::vector<float> xforms;
+  std::vector<uint32_t> object_geometry;  // instanced scenes: each object's geometry
+  std::vector<float> geometry_bounds;     // instanced scenes: each geometry's object-space box (lo, hi)
+  MoverTree movers;                       // instanced scenes built with movable objects
 };
 
 // An object placing a geometry: world = scale * rotation * p + translation
@@ -55,8 +69,17 @@ void build_flat_scene(const float* tri9, const uint32_t* mesh_counts, uint32_t n
 // flatten_instanced (hierarchy.rs:464-522) + object_hierarchy over the
 // objects' world bounds: each geometry's triangles and triangle hierarchy
 // once, one object per instance.
+// With `nmovable` > 0 the object hierarchy keeps the movable objects in a
+// subtree of their own (object_hierarchy_with_movers, hierarchy.rs:331-369).
 void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
-                           const Instance* instances, uint32_t ninstances, FlatScene& out, int threads);
+                           const Instance* instances, uint32_t ninstances, const uint32_t* movable,
+                           uint32_t nmovable, FlatScene& out, int threads);
+
+// Places the movable objects anew (placements in MoverTree::objects order,
+// same geometries) and rebuilds their subtree and the root (mover_subtree,
+// hierarchy.rs:383-410). boxes12 (nullable): per mover, the padded world
+// bounds before and after (lo.xyz, hi.xyz each).
+void move_instances(FlatScene& s, const Instance* placements, float* boxes12);
 
 // Primary hits of a pinhole camera (raycast.cpp).
 void primary_hits(const FlatScene& s, const float* camera, uint32_t width, uint32_t height, float* out8,

@@ -335,7 +335,8 @@ int cc_scene_build(cc_context* ctx, const float* tri9, const uint32_t* mesh_coun
 }
 
 int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const uint32_t* geometry_counts,
-                             uint32_t ngeometries, const cc_instance* instances, uint32_t ninstances, cc_scene** out) {
+                             uint32_t ngeometries, const cc_instance* instances, uint32_t ninstances,
+                             const uint32_t* movable, uint32_t nmovable, cc_scene** out) {
   static_assert(sizeof(cc_instance) == sizeof(cc::Instance), "cc_instance is cc::Instance");
   if (!out || (ngeometries && !geometry_counts) || (ninstances && !instances)) return fail(CC_ERR_INVALID, "null argument");
   *out = nullptr;
@@ -356,10 +357,19 @@ int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const uint32_t*
       }
   }
   if (total >= (1u << 26)) return fail(CC_ERR_INVALID, "a scene holds fewer than 2^26 triangles and hierarchy nodes");
+  if (nmovable) {
+    if (!movable) return fail(CC_ERR_INVALID, "null movable list");
+    if (nmovable >= ninstances) return fail(CC_ERR_INVALID, "a scene with movers needs a static object");
+    std::vector<uint8_t> seen(ninstances, 0);
+    for (uint32_t i = 0; i < nmovable; ++i) {
+      if (movable[i] >= ninstances || seen[movable[i]]) return fail(CC_ERR_INVALID, "movable objects must be distinct objects");
+      seen[movable[i]] = 1;
+    }
+  }
   cc_scene* s = new cc_scene;
   s->ctx = ctx;
   cc::build_instanced_scene(tri9, geometry_counts, ngeometries, reinterpret_cast<const cc::Instance*>(instances),
-                            ninstances, s->flat, threads_for_build());
+                            ninstances, movable, nmovable, s->flat, threads_for_build());
   if (s->flat.blas.size() >= (1u << 26) || s->flat.nodes.size() >= (1u << 26)) {
     delete s;
     return fail(CC_ERR_INVALID, "a scene holds fewer than 2^26 triangles and hierarchy nodes");

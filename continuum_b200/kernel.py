@@ -199,6 +199,14 @@ class Scene:
         check(load().cc_scene_arrays(self.handle, ptr(ranges), ptr(blas), ptr(blas_items), ptr(nodes), ptr(items)))
         return dict(ranges=ranges, blas=blas, blas_items=blas_items, nodes=nodes, items=items)
 
+    def move(self, placements) -> np.ndarray:
+        """Places the movable objects anew (in their order); returns per mover
+        its padded world bounds before and after (12 floats)."""
+        inst = instances_array(placements)
+        boxes = np.zeros((len(inst), 12), np.float32)
+        check(load().cc_scene_move(self.handle, ptr(inst), len(inst), ptr(boxes)))
+        return boxes
+
     def transforms(self) -> np.ndarray:
         """The objects' transforms, 16 floats each (instanced scenes; else empty)."""
         n = int(load().cc_scene_transforms(self.handle, None, 0))
@@ -254,19 +262,20 @@ def instances_array(instances) -> np.ndarray:
     return out
 
 
-def _build_instanced(handle, geometries, instances) -> int:
+def _build_instanced(handle, geometries, instances, movable=None) -> int:
     tri9, counts = flatten_meshes(geometries)
     inst = instances_array(instances)
+    mov = None if movable is None else np.ascontiguousarray(movable, np.uint32)
     h = C.c_void_p()
-    check(load().cc_scene_build_instanced(handle, ptr(tri9), ptr(counts), len(counts), ptr(inst), len(inst),
-                                          C.byref(h)))
+    check(load().cc_scene_build_instanced(handle, ptr(tri9), ptr(counts), len(counts), ptr(inst), len(inst), ptr(mov),
+                                          0 if mov is None else len(mov), C.byref(h)))
     return h.value
 
 
-def host_scene_instanced(geometries, instances) -> Scene:
+def host_scene_instanced(geometries, instances, movable=None) -> Scene:
     """An instanced scene built on the host only (hierarchies to inspect and
     ray cast)."""
-    return Scene(None, _build_instanced(None, geometries, instances))
+    return Scene(None, _build_instanced(None, geometries, instances, movable))
 
 
 class MaskConeKernel:
@@ -349,10 +358,35 @@ class MaskConeKernel:
         tri9, counts = flatten_meshes(meshes)
         return self.scene_from_tri9(tri9, counts)
 
-    def scene_instanced(self, geometries, instances) -> Scene:
+    def scene_instanced(self, geometries, instances, movable=None) -> Scene:
         """An instanced scene: shared geometries (object space) placed by
-        transforms (flatten_instanced, hierarchy.rs:464-522)."""
-        return Scene(self, _build_instanced(self.handle, geometries, instances))
+        transforms (flatten_instanced, hierarchy.rs:464-522); `movable`
+        objects keep a subtree of their own (Scene.move places them anew)."""
+        return Scene(self, _build_instanced(self.handle, geometries, instances, movable))
+
+    def stale_cones(self, scene: Scene, d_receivers: int, npoints: int, lights: np.ndarray, boxes: np.ndarray,
+                    d_stale: int, stream: int = 0) -> int:
+        """Marks (1 byte per cone, device) the cones the moved boxes may have
+        changed; returns their count. lights and boxes are host arrays."""
+        lig = np.ascontiguousarray(lights, np.float32).reshape(-1, 16)
+        b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 12)
+        n = C.c_uint64()
+        check(load().cc_stale_cones(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints), ptr(lig),
+                                    lig.shape[0], ptr(b), b.shape[0], C.c_void_p(d_stale), C.byref(n),
+                                    C.c_void_p(stream) if stream else None))
+        return int(n.value)
+
+    def visibility_update(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int,
+                          d_stale: int, outputs: dict, hierarchy=Hierarchy.TRIANGLES, stream: int = 0) -> int:
+        """Recomputes the stale cones of device result arrays in place;
+        returns the cones solved."""
+        o = _lib.Outputs(*(outputs.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.options(hierarchy)
+        n = C.c_uint64()
+        check(load().cc_visibility_update(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints),
+                                          C.c_void_p(d_lights), int(nlights), C.c_void_p(d_stale), C.byref(opt),
+                                          C.byref(o), C.byref(n), C.c_void_p(stream) if stream else None))
+        return int(n.value)
 
     def scene_from_tri9(self, tri9: np.ndarray, counts: np.ndarray) -> Scene:
         tri9 = np.ascontiguousarray(tri9, dtype=np.float32)

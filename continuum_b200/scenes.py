@@ -532,3 +532,22 @@ def instanced_world(seed: int = 5, n_instances: int = 1_000_000, n_boulders: int
 def _lib_instance_dtype():
     from ._lib import INSTANCE_DTYPE
     return INSTANCE_DTYPE
+
+
+def moved_placements(world: InstancedWorld, movable: np.ndarray, frame: int, step: float = 3.0) -> np.ndarray:
+    """New cc_instance records for the movable objects (in their order) at
+    `frame`: each moved by a seeded offset of up to `step` metres in x and z
+    and turned by a seeded yaw; geometry and scale kept."""
+    rng = np.random.default_rng(10_000 + frame)
+    base = world.instances[np.asarray(movable)]
+    out = base.copy()
+    n = len(out)
+    off = rng.uniform(-step, step, (n, 2)).astype(np.float32) * np.float32(frame)
+    out["translation"][:, 0] += off[:, 0]
+    out["translation"][:, 2] += off[:, 1]
+    yaw = rng.uniform(0.0, 2.0 * math.pi, n)
+    c, s = np.cos(yaw).astype(np.float32), np.sin(yaw).astype(np.float32)
+    rot = np.zeros((n, 9), np.float32)
+    rot[:, 0], rot[:, 2], rot[:, 4], rot[:, 6], rot[:, 8] = c, s, 1.0, -s, c
+    out["rotation"] = rot
+    return out

@@ -136,7 +136,24 @@ typedef struct cc_instance {
  * NULL the scene stays on the host. */
 CC_API int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const uint32_t* geometry_counts,
                                     uint32_t ngeometries, const cc_instance* instances, uint32_t ninstances,
-                                    cc_scene** out);
+                                    const uint32_t* movable, uint32_t nmovable, cc_scene** out);
+/* With `movable` objects (nmovable > 0, some object staying static) the
+ * object hierarchy keeps them in a subtree of their own under the root
+ * (object_hierarchy_with_movers, hierarchy.rs:331-369); cc_scene_move places
+ * them anew (placements in `movable` order, same geometries), rebuilds that
+ * subtree (mover_subtree, :383-410) and updates the device copy. boxes12
+ * (nullable) receives per mover its padded world bounds before and after
+ * (lo.xyz, hi.xyz each): the input of cc_stale_cones. */
+CC_API int cc_scene_move(cc_scene* scene, const cc_instance* placements, uint32_t nplacements, float* boxes12);
+/* The cones that moved objects may have changed: cone (light l, point p) is
+ * stale when a mover's box, old or new, meets the convex hull of p and the
+ * light's box (hull_meets, mask_cones.wgsl:3903-3917, after the shadow-region
+ * prefilter of hierarchy.rs:418-457). receivers and stale (1 byte per cone,
+ * light-major) are device pointers; lights (16 floats each) and boxes12 are
+ * host arrays. Waits for the result; *count receives the stale cones. */
+CC_API int cc_stale_cones(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                          const float* lights, uint32_t nlights, const float* boxes12, uint32_t nmovers,
+                          uint8_t* stale, uint64_t* count, void* stream);
 /* The scene's transforms (16 floats each) into out16 (nullable, at most
  * max_transforms); returns their count (0 for a scene without instancing). */
 CC_API uint64_t cc_scene_transforms(const cc_scene* scene, float* out16, uint64_t max_transforms);
@@ -190,6 +207,15 @@ typedef struct cc_outputs {
 CC_API int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
                   const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                   void* stream);
+
+/* Recomputes the stale cones of a cache of results (device arrays, as
+ * cc_visibility with CC_DEVICE_POINTERS writes them; full, any, irradiance
+ * and fraction) and leaves every other cone's results as they are. receivers,
+ * lights and stale are device pointers. *recomputed (nullable) receives the
+ * cones solved. Waits for the result. */
+CC_API int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                                const float* lights, uint32_t nlights, const uint8_t* stale, const cc_options* opt,
+                                const cc_outputs* out, uint64_t* recomputed, void* stream);
 
 /* No counterpart in the reference (whose kernel owns its wgpu buffers).
  * cc_visibility without allocation: the same results as cc_visibility with

@@ -146,6 +146,12 @@ struct Scene {
   // translation in w, then (scale, 1 / scale, 0, 0) (Placement::rows,
   // hierarchy.rs:272-285); ranges[4 * m + 3] names object m's.
   std::vector<float> xforms;
+  std::vector<uint32_t> object_geometry;  // instanced scenes: each object's geometry
+  std::vector<std::pair<F3, F3>> geometry_box;  // instanced scenes: each geometry's object-space box
+  // The movers' subtree (MoverTree, hierarchy.rs:309-327): root node 2, other
+  // nodes from first_node, items from first_item, in `movers` order.
+  uint32_t first_node = 0, mover_nodes = 0, first_item = 0;
+  std::vector<uint32_t> movers;
 };
 
 static void mesh_bounds(const float* tris, uint32_t first, uint32_t count, F3& lo, F3& hi) {
@@ -162,10 +168,16 @@ static void mesh_bounds(const float* tris, uint32_t first, uint32_t count, F3& l
 
 // object_hierarchy (hierarchy.rs:198-253): at most two objects per leaf,
 // oversized objects (diagonal > 64 x median) in their own subtree.
-static void object_hierarchy(Scene* s, const std::vector<std::pair<F3, F3>>& mesh_box) {
-  const uint32_t nmeshes = (uint32_t)mesh_box.size();
-  std::vector<uint32_t> items(nmeshes);
-  std::iota(items.begin(), items.end(), 0u);
+static void object_hierarchy(Scene* s, const std::vector<std::pair<F3, F3>>& mesh_box,
+                             const std::vector<uint32_t>* keep = nullptr) {
+  std::vector<uint32_t> items;
+  if (keep) {
+    items = *keep;
+  } else {
+    items.resize(mesh_box.size());
+    std::iota(items.begin(), items.end(), 0u);
+  }
+  const size_t nmeshes = items.size();
   s->nodes.assign(1, Node{});
   if (items.empty()) {
     s->items = {0};
@@ -174,7 +186,7 @@ static void object_hierarchy(Scene* s, const std::vector<std::pair<F3, F3>>& mes
   }
   auto diagonal = [&](uint32_t m) { return length(mesh_box[m].second - mesh_box[m].first); };
   std::vector<float> sizes(nmeshes);
-  for (uint32_t i = 0; i < nmeshes; ++i) sizes[i] = diagonal(i);
+  for (size_t i = 0; i < nmeshes; ++i) sizes[i] = diagonal(items[i]);
   size_t mid = sizes.size() / 2;
   std::nth_element(sizes.begin(), sizes.begin() + mid, sizes.end());
   float median = sizes[mid];
@@ -260,42 +272,142 @@ struct Instance {
 
 // flatten_instanced (hierarchy.rs:464-522) + object_hierarchy over the
 // objects' padded world bounds (Placement::world_bounds, :287-303).
+// Placement::world_bounds (hierarchy.rs:287-303): the padded world bounds of
+// an object-space box placed by `o`.
+static std::pair<F3, F3> world_bounds(const std::pair<F3, F3>& box, const Instance& o) {
+  const float* R = o.rotation;
+  const float* t = o.translation;
+  F3 lo{FLT_MAX, FLT_MAX, FLT_MAX}, hi{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  const F3 a = box.first, b = box.second;
+  for (int c = 0; c < 8; ++c) {
+    const F3 p{(c & 1) ? b.x : a.x, (c & 2) ? b.y : a.y, (c & 4) ? b.z : a.z};
+    const F3 w{(R[0] * p.x + R[1] * p.y + R[2] * p.z) * o.scale + t[0],
+               (R[3] * p.x + R[4] * p.y + R[5] * p.z) * o.scale + t[1],
+               (R[6] * p.x + R[7] * p.y + R[8] * p.z) * o.scale + t[2]};
+    lo = vmin(lo, w);
+    hi = vmax(hi, w);
+  }
+  padded(lo, hi);
+  return {lo, hi};
+}
+
+// mover_subtree (hierarchy.rs:383-410): the movers' subtree over their
+// current bounds (root at node 2, the rest from first_node, items from
+// first_item), marked NO_SPLAT (1), and the root over both subtrees
+// (union_root, :372-381).
+static void mover_subtree(Scene* s, const std::vector<std::pair<F3, F3>>& bounds) {
+  std::vector<Node> local(1);
+  std::vector<uint32_t> order(bounds.size());
+  std::iota(order.begin(), order.end(), 0u);
+  split(local, 0, order.data(), order.size(), 0, bounds, 2, s->first_node - 1, s->first_item);
+  for (Node& n : local) n.info[2] = 1;
+  s->nodes[2] = local[0];
+  for (size_t i = 1; i < local.size(); ++i) s->nodes[s->first_node + i - 1] = local[i];
+  for (size_t k = 0; k < order.size(); ++k) s->items[s->first_item + k] = s->movers[order[k]];
+  Node& r = s->nodes[0];
+  r = Node{};
+  for (int k = 0; k < 3; ++k) {
+    r.lo[k] = std::min(s->nodes[1].lo[k], s->nodes[2].lo[k]);
+    r.hi[k] = std::max(s->nodes[1].hi[k], s->nodes[2].hi[k]);
+  }
+  r.info[0] = 1;
+  r.info[2] = 1;
+}
+
+static uint32_t tree_nodes(uint32_t n, uint32_t leaf) {
+  return n <= leaf ? 1 : 1 + tree_nodes(n / 2, leaf) + tree_nodes(n - n / 2, leaf);
+}
+
 static Scene* build_instanced(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
-                              const Instance* inst, uint32_t ninstances) {
+                              const Instance* inst, uint32_t ninstances, const uint32_t* movable = nullptr,
+                              uint32_t nmovable = 0) {
   Scene* s = build_scene(tri9, geometry_counts, ngeometries);
   const std::vector<uint32_t> geometry = s->ranges;
   std::vector<std::pair<F3, F3>> local(ngeometries);
   for (uint32_t g = 0; g < ngeometries; ++g) mesh_bounds(s->tris.data(), geometry[4 * g], geometry[4 * g + 1], local[g].first, local[g].second);
   s->ranges.clear();
+  s->geometry_box = local;
+  s->object_geometry.assign(ninstances, 0);
   std::vector<std::pair<F3, F3>> box(ninstances);
   for (uint32_t k = 0; k < ninstances; ++k) {
     const Instance& o = inst[k];
+    s->object_geometry[k] = o.geometry;
     const uint32_t* r = &geometry[4 * o.geometry];
     s->ranges.insert(s->ranges.end(), {r[0], r[1], r[2], k});
     const float* R = o.rotation;
     const float* t = o.translation;
     s->xforms.insert(s->xforms.end(), {R[0], R[1], R[2], t[0], R[3], R[4], R[5], t[1], R[6], R[7], R[8], t[2],
                                        o.scale, 1.0f / o.scale, 0.0f, 0.0f});
-    F3 lo{FLT_MAX, FLT_MAX, FLT_MAX}, hi{-FLT_MAX, -FLT_MAX, -FLT_MAX};
-    const F3 a = local[o.geometry].first, b = local[o.geometry].second;
-    for (int c = 0; c < 8; ++c) {
-      const F3 p{(c & 1) ? b.x : a.x, (c & 2) ? b.y : a.y, (c & 4) ? b.z : a.z};
-      const F3 w{(R[0] * p.x + R[1] * p.y + R[2] * p.z) * o.scale + t[0],
-                 (R[3] * p.x + R[4] * p.y + R[5] * p.z) * o.scale + t[1],
-                 (R[6] * p.x + R[7] * p.y + R[8] * p.z) * o.scale + t[2]};
-      lo = vmin(lo, w);
-      hi = vmax(hi, w);
-    }
-    padded(lo, hi);
-    box[k] = {lo, hi};
+    box[k] = world_bounds(local[o.geometry], o);
   }
   if (s->ranges.empty()) s->ranges.insert(s->ranges.end(), {0u, 0u, NONE, NONE});
   if (s->xforms.empty()) s->xforms.assign(16, 0.0f);
   s->nmeshes = (uint32_t)(s->ranges.size() / 4);
   s->nodes.clear();
   s->items.clear();
-  object_hierarchy(s, box);
+  if (nmovable == 0) {
+    object_hierarchy(s, box);
+    return s;
+  }
+  // object_hierarchy_with_movers (hierarchy.rs:331-369).
+  std::vector<uint8_t> is_movable(ninstances, 0);
+  for (uint32_t i = 0; i < nmovable; ++i) is_movable[movable[i]] = 1;
+  std::vector<uint32_t> keep;
+  for (uint32_t m = 0; m < ninstances; ++m)
+    if (!is_movable[m]) keep.push_back(m);
+  object_hierarchy(s, box, &keep);
+  std::vector<Node> fixed = s->nodes;
+  std::vector<uint32_t> items = s->items;
+  auto place = [](uint32_t i) { return i == 0 ? 1u : i + 2u; };
+  s->first_node = (uint32_t)fixed.size() + 2;
+  s->first_item = (uint32_t)items.size();
+  s->movers.assign(movable, movable + nmovable);
+  s->mover_nodes = tree_nodes(nmovable, 2) - 1;
+  s->nodes.assign(s->first_node + s->mover_nodes, Node{});
+  for (size_t i = 0; i < fixed.size(); ++i) {
+    Node n = fixed[i];
+    if (n.info[1] == 0) n.info[0] = place(n.info[0]);
+    s->nodes[place((uint32_t)i)] = n;
+  }
+  s->items = items;
+  s->items.resize(items.size() + nmovable);
+  std::vector<std::pair<F3, F3>> mb(nmovable);
+  for (uint32_t i = 0; i < nmovable; ++i) mb[i] = box[movable[i]];
+  mover_subtree(s, mb);
   return s;
+}
+
+// The movers placed anew (in `movers` order): transforms replaced, their
+// subtree rebuilt; boxes12 (nullable) receives the bounds before and after.
+static void move_objects(Scene* s, const Instance* placements, float* boxes12) {
+  std::vector<std::pair<F3, F3>> mb(s->movers.size());
+  for (size_t i = 0; i < s->movers.size(); ++i) {
+    const uint32_t m = s->movers[i];
+    const uint32_t x = s->ranges[4 * m + 3];
+    float* X = &s->xforms[16 * (size_t)x];
+    Instance old{};
+    old.geometry = s->object_geometry[m];
+    for (int r = 0; r < 3; ++r) {
+      for (int c = 0; c < 3; ++c) old.rotation[3 * r + c] = X[4 * r + c];
+      old.translation[r] = X[4 * r + 3];
+    }
+    old.scale = X[12];
+    const auto before = world_bounds(s->geometry_box[old.geometry], old);
+    const Instance& o = placements[i];
+    const float* R = o.rotation;
+    const float* t = o.translation;
+    const float row[16] = {R[0], R[1], R[2], t[0], R[3], R[4], R[5], t[1], R[6], R[7], R[8], t[2],
+                           o.scale, 1.0f / o.scale, 0.0f, 0.0f};
+    std::memcpy(X, row, sizeof(row));
+    mb[i] = world_bounds(s->geometry_box[old.geometry], o);
+    if (boxes12) {
+      const float v[12] = {before.first.x, before.first.y, before.first.z, before.second.x, before.second.y,
+                           before.second.z, mb[i].first.x, mb[i].first.y, mb[i].first.z, mb[i].second.x,
+                           mb[i].second.y, mb[i].second.z};
+      std::memcpy(boxes12 + 12 * i, v, sizeof(v));
+    }
+  }
+  mover_subtree(s, mb);
 }
 
 // ---------------------------------------------------------------------------
@@ -1489,8 +1601,108 @@ void* oracle_scene_create(const float* tri9, const uint32_t* mesh_counts, uint32
 // An instanced scene: geometries given as 9 floats per triangle (object
 // space), instances as cc_instance records.
 void* oracle_scene_create_instanced(const float* tri9, const uint32_t* geometry_counts, uint32_t ngeometries,
-                                    const void* instances, uint32_t ninstances) {
-  return build_instanced(tri9, geometry_counts, ngeometries, static_cast<const Instance*>(instances), ninstances);
+                                    const void* instances, uint32_t ninstances, const uint32_t* movable,
+                                    uint32_t nmovable) {
+  return build_instanced(tri9, geometry_counts, ngeometries, static_cast<const Instance*>(instances), ninstances,
+                         movable, nmovable);
+}
+
+void oracle_scene_move(void* sp, const void* placements, float* boxes12) {
+  move_objects(static_cast<Scene*>(sp), static_cast<const Instance*>(placements), boxes12);
+}
+
+// The cones moved objects may have changed (may_be_shadowed, mask_cones.wgsl:
+// 3961-3974, for a point's box): for each (light, point), some mover box, old
+// or new, whose shadow region (hierarchy.rs:418-457) holds the point and
+// which meets the hull of the point and the light's box (hull_meets,
+// :3903-3917). 1 byte per cone, light-major.
+void oracle_stale_cones(void* sp, const float* rec8, uint64_t npoints, const float* lights16, uint32_t nlights,
+                        const float* boxes12, uint32_t nmovers, uint8_t* out, int threads) {
+  const Scene* s = static_cast<const Scene*>(sp);
+  typedef std::pair<F3, F3> B;
+  const B scene_box{F3{s->nodes[0].lo[0], s->nodes[0].lo[1], s->nodes[0].lo[2]},
+                    F3{s->nodes[0].hi[0], s->nodes[0].hi[1], s->nodes[0].hi[2]}};
+  auto light_box = [](const float* L) {  // :3887-3898
+    F3 c;
+    float radius;
+    if (L[3] > 1.5f) {
+      c = F3{L[0], L[1], L[2]};
+      radius = 1.5f * L[4];
+    } else {
+      c = F3{L[0], L[1], L[2]} + (F3{L[4], L[5], L[6]} + F3{L[8], L[9], L[10]}) * 0.5f;
+      radius = 0.5f * (length(F3{L[4], L[5], L[6]}) + length(F3{L[8], L[9], L[10]}));
+    }
+    const float far = std::max(std::max(std::fabs(c.x), 1.0f), std::max(std::max(std::fabs(c.y), 1.0f), std::max(std::fabs(c.z), 1.0f)));
+    radius = radius * 1.001f + 1e-5f * far + 1e-4f;
+    return B{c - F3{radius, radius, radius}, c + F3{radius, radius, radius}};
+  };
+  auto comp = [](const F3& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); };
+  auto region = [&](const B& m, const B& l, const B& sb, B& out) {  // shadow_region
+    const F3 d_lo = m.first - l.second, d_hi = m.second - l.first;
+    float t0 = 0.0f, t1 = INFINITY;
+    for (int a = 0; a < 3; ++a) {
+      float b = comp(d_lo, a), c = comp(sb.second, a) - comp(m.first, a);
+      if (b > 0.0f) t1 = std::min(t1, c / b);
+      else if (b < 0.0f) t0 = std::max(t0, c / b);
+      else if (c < 0.0f) return false;
+      b = comp(d_hi, a);
+      c = comp(sb.first, a) - comp(m.second, a);
+      if (b > 0.0f) t0 = std::max(t0, c / b);
+      else if (b < 0.0f) t1 = std::min(t1, c / b);
+      else if (c > 0.0f) return false;
+    }
+    if (t0 > t1 * (1.0f + 1e-6f) + 1e-6f) return false;
+    if (!std::isfinite(t1)) {
+      out = sb;
+      return true;
+    }
+    const F3 lo = vmax(vmin(m.first + d_lo * t0, m.first + d_lo * t1), sb.first);
+    const F3 hi = vmin(vmax(m.second + d_hi * t0, m.second + d_hi * t1), sb.second);
+    const float pad = 1e-4f * std::max(std::max(std::max(std::fabs(lo.x), std::fabs(hi.x)),
+                                                std::max(std::fabs(lo.y), std::fabs(hi.y))),
+                                       std::max(std::max(std::fabs(lo.z), std::fabs(hi.z)), 1.0f));
+    out = B{lo - F3{pad, pad, pad}, hi + F3{pad, pad, pad}};
+    return true;
+  };
+  auto hull_meets = [&](const F3& p, const B& l, const B& m) {
+    float s0 = 0.0f, s1 = 1.0f;
+    for (int a = 0; a < 3; ++a) {
+      const float b0 = comp(l.first, a) - comp(p, a), c0 = comp(m.second, a) - comp(p, a);
+      if (b0 > 0.0f) s1 = std::min(s1, c0 / b0);
+      else if (b0 < 0.0f) s0 = std::max(s0, c0 / b0);
+      else if (c0 < 0.0f) return false;
+      const float b1 = comp(l.second, a) - comp(p, a), c1 = comp(m.first, a) - comp(p, a);
+      if (b1 > 0.0f) s0 = std::max(s0, c1 / b1);
+      else if (b1 < 0.0f) s1 = std::min(s1, c1 / b1);
+      else if (c1 > 0.0f) return false;
+    }
+    return s0 <= s1 + 1e-6f;
+  };
+  for (uint32_t l = 0; l < nlights; ++l) {
+    const B lb = light_box(lights16 + 16 * (size_t)l);
+    std::vector<B> boxes, regions;
+    for (uint32_t b = 0; b < 2 * nmovers; ++b) {
+      const float* v = boxes12 + 6 * (size_t)b;
+      const B m{F3{v[0], v[1], v[2]}, F3{v[3], v[4], v[5]}};
+      B r;
+      if (region(m, lb, scene_box, r)) {
+        boxes.push_back(m);
+        regions.push_back(r);
+      }
+    }
+    parallel_for(npoints, threads, [&](uint64_t p) {
+      const F3 pt{rec8[8 * p], rec8[8 * p + 1], rec8[8 * p + 2]};
+      uint8_t hit = 0;
+      for (size_t k = 0; k < boxes.size() && !hit; ++k) {
+        const B& r = regions[k];
+        if (pt.x < r.first.x || pt.y < r.first.y || pt.z < r.first.z || pt.x > r.second.x || pt.y > r.second.y ||
+            pt.z > r.second.z)
+          continue;
+        if (hull_meets(pt, lb, boxes[k])) hit = 1;
+      }
+      out[(size_t)l * npoints + p] = hit;
+    });
+  }
 }
 
 // The scene's transforms (16 floats each) into out (nullable); returns their count.

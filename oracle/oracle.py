@@ -43,7 +43,9 @@ def load():
         lib.oracle_cpu_weights.argtypes = [P, P, P, P]
         lib.oracle_poly_overflows.restype = U64
         lib.oracle_scene_create_instanced.restype = P
-        lib.oracle_scene_create_instanced.argtypes = [P, P, U32, P, U32]
+        lib.oracle_scene_create_instanced.argtypes = [P, P, U32, P, U32, P, U32]
+        lib.oracle_scene_move.argtypes = [P, P, P]
+        lib.oracle_stale_cones.argtypes = [P, P, U64, P, U32, P, U32, P, I]
         lib.oracle_scene_transforms.restype = U64
         lib.oracle_scene_transforms.argtypes = [P, P]
         _lib = lib
@@ -71,7 +73,7 @@ class OracleScene:
         self._h = C.c_void_p(load().oracle_scene_create(_p(self.tri9), _p(self.counts), len(self.counts)))
 
     @classmethod
-    def instanced(cls, geometries, instances: np.ndarray) -> "OracleScene":
+    def instanced(cls, geometries, instances: np.ndarray, movable=None) -> "OracleScene":
         """An instanced scene: geometries (object space) placed by cc_instance
         records (flatten_instanced, hierarchy.rs:464-522)."""
         self = cls.__new__(cls)
@@ -79,9 +81,27 @@ class OracleScene:
         self.tri9 = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros((0, 9), np.float32))
         self.counts = np.array([len(p) for p in parts], np.uint32)
         self.instances = np.ascontiguousarray(instances)
-        self._h = C.c_void_p(load().oracle_scene_create_instanced(_p(self.tri9), _p(self.counts), len(self.counts),
-                                                                  _p(self.instances), len(self.instances)))
+        self.movable = None if movable is None else np.ascontiguousarray(movable, np.uint32)
+        self._h = C.c_void_p(load().oracle_scene_create_instanced(
+            _p(self.tri9), _p(self.counts), len(self.counts), _p(self.instances), len(self.instances),
+            _p(self.movable), 0 if self.movable is None else len(self.movable)))
         return self
+
+    def move(self, placements: np.ndarray) -> np.ndarray:
+        """Places the movers anew (in their order); per mover its bounds before and after."""
+        pl = np.ascontiguousarray(placements)
+        boxes = np.zeros((len(pl), 12), np.float32)
+        load().oracle_scene_move(self._h, _p(pl), _p(boxes))
+        return boxes
+
+    def stale_cones(self, receivers: np.ndarray, lights: np.ndarray, boxes: np.ndarray, threads=None) -> np.ndarray:
+        rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
+        lig = np.ascontiguousarray(lights, np.float32).reshape(-1, 16)
+        b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 12)
+        out = np.zeros(rec.shape[0] * lig.shape[0], np.uint8)
+        load().oracle_stale_cones(self._h, _p(rec), rec.shape[0], _p(lig), lig.shape[0], _p(b), b.shape[0], _p(out),
+                                  int(threads or default_threads()))
+        return out
 
     def transforms(self) -> np.ndarray:
         n = int(load().oracle_scene_transforms(self._h, None))

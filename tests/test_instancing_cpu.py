@@ -78,3 +78,39 @@ def test_invalid_instances_are_rejected():
         with pytest.raises(_lib.CCError) as e:
             host_scene_instanced(g, inst)
         assert e.value.code == _lib.CC_ERR_INVALID
+
+
+def test_movers_subtree_matches_the_oracle_before_and_after_a_move():
+    w = small_world(n=300)
+    movable = np.arange(0, 300, 10, dtype=np.uint32)
+    lib = host_scene_instanced(w.geometries, w.instances, movable)
+    orc = OracleScene.instanced(w.geometries, w.instances, movable)
+
+    def same():
+        a, b = lib.arrays(), orc.arrays()
+        for k in ("ranges", "blas_items", "items"):
+            assert np.array_equal(a[k], b[k]), k
+        for k in ("blas", "nodes"):
+            assert a[k].tobytes() == b[k].tobytes(), k
+        assert np.array_equal(lib.transforms(), orc.transforms())
+        return a
+
+    a = same()
+    assert a["nodes"][0]["info"][0] == 1 and a["nodes"][0]["info"][2] == 1  # root over the two subtrees
+    for frame in (1, 2):
+        pl = scenes.moved_placements(w, movable, frame)
+        ba, bb = lib.move(pl), orc.move(pl)
+        assert np.array_equal(ba, bb)
+        a = same()
+        # The movers' new bounds are inside the root's.
+        assert np.all(ba[:, 6:9] >= a["nodes"][0]["lo"][:3]) and np.all(ba[:, 9:12] <= a["nodes"][0]["hi"][:3])
+    lib.close()
+    orc.close()
+
+
+def test_moving_without_movers_is_an_error():
+    w = small_world(n=20)
+    s = host_scene_instanced(w.geometries, w.instances)
+    with pytest.raises(_lib.CCError):
+        s.move(w.instances[:1])
+    s.close()

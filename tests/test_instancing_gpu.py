@@ -41,3 +41,50 @@ def test_instanced_packets_equal_solo_walks(kernel, world):
     scene.close()
     for k in ("full", "any", "partial", "irradiance", "fraction"):
         assert np.array_equal(runs[0][k], runs[1][k]), k
+
+
+def test_moved_objects_mark_the_oracle_stale_cones_and_the_update_equals_a_full_solve(kernel, world):
+    """Move every tenth boulder; the device's stale cones are the oracle's,
+    the incremental update leaves every uncapped cone as a full solve of the
+    moved scene gives it, and the moved scene meets the parity bar."""
+    import torch
+
+    from continuum_b200 import _lib
+
+    movable = np.arange(0, len(world.instances) - 1, 10, dtype=np.uint32)
+    scene = kernel.scene_instanced(world.geometries, world.instances, movable)
+    orc = OracleScene.instanced(world.geometries, world.instances, movable)
+    dev = torch.device("cuda:0")
+    rec = torch.from_numpy(world.receivers).to(dev)
+    lig = torch.from_numpy(world.lights).to(dev)
+    P, L = rec.shape[0], lig.shape[0]
+    n = P * L
+    cache = {"full": torch.zeros(n, dtype=torch.int64, device=dev), "any": torch.zeros(n, dtype=torch.int64, device=dev),
+             "irradiance": torch.zeros(n, device=dev), "fraction": torch.zeros(n, device=dev)}
+    ptrs = {k: v.data_ptr() for k, v in cache.items()}
+    kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, ptrs)
+    torch.cuda.synchronize()
+
+    pl = scenes.moved_placements(world, movable, 1)
+    boxes = scene.move(pl)
+    assert np.array_equal(boxes, orc.move(pl))
+    stale = torch.zeros(n, dtype=torch.uint8, device=dev)
+    count = kernel.stale_cones(scene, rec.data_ptr(), P, world.lights, boxes, stale.data_ptr())
+    want = orc.stale_cones(world.receivers, world.lights, boxes)
+    assert np.array_equal(stale.cpu().numpy(), want)
+    assert count == int(want.sum()) and 0 < count < n
+
+    solved = kernel.visibility_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(), ptrs)
+    assert solved == count
+    full = parity.flat(kernel.visibility(scene, world.receivers, world.lights, outputs=ALL))
+    capped = (full["work"][:, 3] & _lib.CC_CONE_CAPPED) != 0
+    got = {k: v.cpu().numpy() for k, v in cache.items()}
+    for k in ("full", "any", "irradiance", "fraction"):
+        a, b = got[k].reshape(-1), np.asarray(full[k]).reshape(-1)
+        if k in ("full", "any"):
+            a = a.view(np.uint64)
+        assert np.array_equal(a[~capped], b[~capped]), k
+    o = orc.visibility(world.receivers, world.lights)
+    parity.compare(full, o, o["unshadowed"])
+    scene.close()
+    orc.close()
