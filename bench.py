@@ -370,6 +370,63 @@ def served_leg(args, kernel) -> dict:
             "rates": results}
 
 
+def instanced_leg(args, kernel, dev, stream, flush) -> dict:
+    """The instanced large world: 10 displaced UV-sphere boulders (10,240
+    triangles each) placed as 1,000,000 instances (10.24 billion instanced
+    triangles) on a ground quad, 8 lights, 1280x720 primary hits. A full solve
+    (device-timed, L2 flushed), then frames in which 1% of the instances (a
+    fixed movable set) move: each frame's move (host subtree rebuild and
+    upload), stale-cone marking and incremental recompute, wall-clock timed
+    as one update of the cached results."""
+    import torch
+
+    from continuum_b200 import scenes
+
+    w = scenes.instanced_world(seed=5, n_instances=args.instances)
+    n_obj = len(w.instances)
+    movable = np.arange(0, n_obj - 1, 100, dtype=np.uint32)  # 1%, the ground stays
+    scene = kernel.scene_instanced(w.geometries, w.instances, movable)
+    rec = torch.from_numpy(w.receivers).to(dev)
+    lig = torch.from_numpy(w.lights).to(dev)
+    P, L = rec.shape[0], lig.shape[0]
+    C = P * L
+    cache = {"full": torch.empty(C, dtype=torch.int64, device=dev), "any": torch.empty(C, dtype=torch.int64, device=dev),
+             "irradiance": torch.empty(C, device=dev), "fraction": torch.empty(C, device=dev)}
+    ptrs = {k: v.data_ptr() for k, v in cache.items()}
+
+    def full():
+        kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, ptrs, stream=stream.cuda_stream)
+
+    steps = max(1, min(args.steps, 2))
+    full_ms = float(np.mean(timed_steps(torch, dev, stream, flush, full, 1, steps)))
+    stale = torch.empty(C, dtype=torch.uint8, device=dev)
+    frames = []
+    for f in range(1, args.frames + 1):
+        pl = scenes.moved_placements(w, movable, f)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        boxes = scene.move(pl)
+        count = kernel.stale_cones(scene, rec.data_ptr(), P, w.lights, boxes, stale.data_ptr(),
+                                   stream=stream.cuda_stream)
+        solved = kernel.visibility_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(), ptrs,
+                                          stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        ms = (time.perf_counter() - t0) * 1e3
+        frames.append({"ms": ms, "stale_cones": count, "recomputed": solved, "stale_share": count / C})
+    scene.close()
+    upd = float(np.mean([fr["ms"] for fr in frames])) if frames else None
+    return {"workload": f"{n_obj - 1} boulder instances (10 displaced UV spheres, 10,240 triangles each) on a ground "
+                        f"quad, {L} lights, 1280x720 primary hits; 1% of the instances move per frame",
+            "instanced_triangles": w.instanced_tris, "points": P, "cones": C,
+            "full_solve": {"value": C / (full_ms * 1e-3), "unit": UNIT, "ms": full_ms, "steps": steps,
+                           "timing": "CUDA events, L2 flushed"},
+            "frames": frames,
+            "update": {"ms_per_frame": upd, "cones_per_s_served": (C / (upd * 1e-3)) if upd else None,
+                       "timing": "wall clock: host move of the movers' subtree and upload, stale-cone marking, "
+                                 "recompute of the stale cones",
+                       "speedup_vs_full_solve": (full_ms / upd) if upd else None}}
+
+
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
@@ -542,6 +599,8 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         line["batched"] = batched_leg(args, kernel, dev, stream, flush)
     if "served" in forms:
         line["served"] = served_leg(args, kernel)
+    if "instanced" in forms:
+        line["instanced"] = instanced_leg(args, kernel, dev, stream, flush)
     if world == 1 and not args.no_cpu_baseline:
         rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
@@ -562,8 +621,10 @@ def main() -> None:
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--forms", default="batched,served",
-                    help="systems forms measured beside the plain line (comma list of batched, served; none)")
+    ap.add_argument("--forms", default="batched,served,instanced",
+                    help="systems forms measured beside the plain line (comma list of batched, served, instanced; none)")
+    ap.add_argument("--instances", type=int, default=1_000_000)
+    ap.add_argument("--frames", type=int, default=3, help="moving frames of the instanced leg")
     ap.add_argument("--batch-jobs", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3, help="timed steps of the batched leg (at most --steps)")
     ap.add_argument("--serve-requests", type=int, default=48)
