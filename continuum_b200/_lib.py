@@ -33,6 +33,7 @@ CC_CONE_STACK = 2
 CC_CONE_DIVERGED = 4
 CC_CONE_REWALKED = 8
 CC_CONE_FULL_STOP = 16
+CC_CONE_ACC_WIDE = 32
 
 #: Every symbol include/continuum_cuda.h declares.
 EXPORTS = (

@@ -281,26 +281,55 @@ __device__ __forceinline__ bool may_touch(const Cone& c, f3 v0, f3 v1, f3 v2) {
 
 // ---- the accumulation rasterizer ------------------------------------------------
 // A cone's 68-cell accumulator (the WGSL's `acc`, :719-760) in shared
-// memory, cell-major with the cone's lane innermost, in 64-bit fixed point
-// (units of 2^-40 of a bin). Any lane may add to any cone's cells: integer
-// addition is exact and order-free, so the sum — and every result — is the
-// same whichever lanes draw which triangles in whatever order. (The
-// reference sums in f32 in walk order; the exact sum differs from that by
-// f32 rounding only.) Cells 64..65 receive writes "one past the last row"
-// that no resolve ever reads, so they are dropped.
-constexpr float kFixScale = 1099511627776.0f;        // 2^40
-constexpr float kFixUnit = 1.0f / 1099511627776.0f;  // 2^-40
+// memory, cell-major with the cone's lane innermost, in fixed point (units of
+// 2^-24 of a bin: an f32's resolution at 1). Any lane may add to any cone's
+// cells: integer addition is exact and order-free, so the sum — and every
+// result — is the same whichever lanes draw which triangles in whatever
+// order. (The reference sums in f32 in walk order; the exact sum differs from
+// that by f32 rounding only.) The packet pass keeps 32-bit cells, so more
+// warps fit an SM; an add that overflows one (a mesh piling 128 bins' worth
+// of coverage into a cell) flags its cone, which the solo pass walks again
+// with 64-bit cells of the same unit — the same result, never a wrapped one.
+// Cells 64..65 receive writes "one past the last row" that no resolve ever
+// reads, so they are dropped.
+constexpr float kFixScale = 16777216.0f;        // 2^24
+constexpr float kFixUnit = 1.0f / 16777216.0f;  // 2^-24
 
-struct LaneAcc {
+template <class Cell>
+struct LaneAcc;
+
+// 64-bit cells: no overflow is possible (each add is at most one bin).
+template <>
+struct LaneAcc<unsigned long long> {
   unsigned long long* base;  // &acc[cone]; cell k at base[32 * k]
   uint32_t span_lo, span_hi; // rows this triangle wrote (the WGSL's span, :758-760)
+  uint32_t* overflow;        // unused
+  uint32_t bit;
   __device__ __forceinline__ void add(uint32_t cell, float v) {
     if (cell < (uint32_t)kBins) atomicAdd(base + 32 * cell, (unsigned long long)__float2ll_rn(v * kFixScale));
   }
 };
 
+// 32-bit cells: a signed overflow of any add sets the cone's bit in *overflow.
+template <>
+struct LaneAcc<unsigned int> {
+  unsigned int* base;
+  uint32_t span_lo, span_hi;
+  uint32_t* overflow;
+  uint32_t bit;
+  __device__ __forceinline__ void add(uint32_t cell, float v) {
+    if (cell < (uint32_t)kBins) {
+      const int a = __float2int_rn(v * kFixScale);
+      const int old = (int)atomicAdd(base + 32 * cell, (unsigned int)a);
+      const int sum = (int)((unsigned int)old + (unsigned int)a);
+      if (((old ^ sum) & (a ^ sum)) < 0) atomicOr(overflow, bit);
+    }
+  }
+};
+
 // draw_edge (:297-348)
-__device__ __forceinline__ void draw_edge(LaneAcc& acc, float q0x, float q0y, float q1x, float q1y, float weight) {
+template <class Acc>
+__device__ __forceinline__ void draw_edge(Acc& acc, float q0x, float q0y, float q1x, float q1y, float weight) {
   if (fabsf(q0y - q1y) <= 1.1920929e-7f) return;
   float dir = 1.0f;
   float p0x = q0x, p0y = q0y, p1x = q1x, p1y = q1y;
@@ -392,7 +421,8 @@ __device__ __forceinline__ int clip_line2(const float2* in, int n, float2* out, 
   return m;
 }
 
-__device__ __forceinline__ void draw_polygon(LaneAcc& acc, const float2* q, int n) {
+template <class Acc>
+__device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n) {
   const float g = float(kGrid);
   for (int i = 0; i < n; ++i) {
     float2 a = q[i], b = q[(i + 1) % n];
@@ -404,7 +434,8 @@ __device__ __forceinline__ void draw_polygon(LaneAcc& acc, const float2* q, int 
 // :350-451): far and near clips, then either the projected corners or, for a
 // polygon reaching outside the window, the window square clipped to the
 // planes through the apex and each edge; finally the square's sides.
-static __device__ __noinline__ bool rasterize_general(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2, bool far_clip) {
+template <class Acc>
+static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2, bool far_clip) {
   f3 pa[kPolyCap], pb[kPolyCap];
   pa[0] = v0;
   pa[1] = v1;
@@ -518,7 +549,8 @@ __device__ __forceinline__ bool crosses_far(const Cone& c, f3 v0, f3 v1, f3 v2) 
 // between the near and far planes projects its three corners and draws them
 // from registers. Returns false, having drawn nothing, for every other
 // triangle: those take rasterize_general.
-__device__ __forceinline__ bool rasterize_fast(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2) {
+template <class Acc>
+__device__ __forceinline__ bool rasterize_fast(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2) {
   if (!crosses_far(c, v0, v1, v2)) {
     f3 p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
     auto in_win = [&](f3 v) {
@@ -550,7 +582,8 @@ __device__ __forceinline__ bool rasterize_fast(const Cone& c, LaneAcc& acc, f3 v
 }
 
 // rasterize (:350-451): the common case, else the general path.
-__device__ __forceinline__ bool rasterize(const Cone& c, LaneAcc& acc, f3 v0, f3 v1, f3 v2) {
+template <class Acc>
+__device__ __forceinline__ bool rasterize(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2) {
   if (rasterize_fast(c, acc, v0, v1, v2)) return true;
   return rasterize_general(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2));
 }

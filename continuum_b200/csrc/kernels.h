@@ -8,7 +8,11 @@
 namespace cc {
 
 constexpr int kWarpsPerBlock = 2;
-constexpr int kBlocksPerSm = 4;  // resident blocks per SM the shared memory allows (4 x 54 KB)
+// Resident blocks per SM the shared memory allows: the packet pass (32-bit
+// accumulator cells, 38 KB per block) fits 5, the solo pass (64-bit cells,
+// 55 KB) 4.
+constexpr int kBlocksPerSm = 5;
+constexpr int kSoloBlocksPerSm = 4;
 
 struct DevQuery {
   const float4* receivers;  // 2 per point: point, normal

@@ -25,6 +25,7 @@
 // alone by a second launch, so every cone's result is the one its own walk
 // gives (the reference's walk without packets, as its view-cache bakes run).
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "cone_device.cuh"
@@ -47,16 +48,28 @@ __device__ __forceinline__ uint32_t fast_len(uint32_t q) { return q & 255u; }
 __device__ __forceinline__ uint32_t general_len(uint32_t q) { return q >> 8; }
 __device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) { return fast | (general << 8); }
 
-// Shared memory of one warp.
+// Shared memory of one warp; Cell is the accumulator's cell: 32 bits in the
+// packet pass, 64 in the solo pass.
+template <class CellT>
 struct WarpShared {
+  using Cell = CellT;
   float cov[kBins * 32];                // each cone's 64 coverages, bin-major, lane innermost
-  unsigned long long acc[kBins * 32];   // each cone's accumulator (64-bit fixed point)
+  Cell acc[kBins * 32];                 // each cone's accumulator (fixed point, units of kFixUnit)
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
   uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
   uint32_t queue[kQueueCap];            // (cone, triangle) pairs that passed the cull, waiting to be rasterized
   uint32_t general[kQueueCap];          // pairs that need rasterize's general path, waiting for it
+  uint32_t overflow[4];                 // word 0: cones whose 32-bit accumulation overflowed in the current mesh
 };
-static_assert(sizeof(WarpShared) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned int>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned long long>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+using NarrowShared = WarpShared<unsigned int>;
+using WideShared = WarpShared<unsigned long long>;
+// Resident blocks per SM the shared memory allows: 5 x 38 KB with 32-bit
+// cells, 4 x 55 KB with 64-bit ones.
+template <class WS>
+constexpr int blocks_per_sm() { return sizeof(typename WS::Cell) == 4 ? 5 : 4; }
+constexpr uint32_t kStatusAccOverflow = 32u;
 static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
 
 // A stack entry packed in one word: its kind in the top 2 bits (an
@@ -106,10 +119,11 @@ struct WarpStack {
   }
 };
 
+template <class WS>
 struct LaneState {
   Cone cone;   // the cone in the space of the object being walked (the world's elsewhere)
   Cone world;  // instanced scenes: the cone in world space
-  WarpShared* ws;
+  WS* ws;
   float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
   uint32_t full;
   uint32_t queued;  // both queues' lengths (queue_lens; the same in every lane)
@@ -121,7 +135,8 @@ struct LaneState {
 
 __device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
 
-__device__ __forceinline__ void store_cone(WarpShared* ws, const Cone& c, int lane) {
+template <class WS>
+__device__ __forceinline__ void store_cone(WS* ws, const Cone& c, int lane) {
   float* t = ws->cone + lane;
   const float f[kConeFields] = {c.apex.x, c.apex.y, c.apex.z, c.right.x, c.right.y, c.right.z, c.up.x, c.up.y,
                                 c.up.z,   c.fwd.x,  c.fwd.y,  c.fwd.z,   c.u0,      c.v0,      c.u1,   c.v1,
@@ -130,7 +145,8 @@ __device__ __forceinline__ void store_cone(WarpShared* ws, const Cone& c, int la
   for (int k = 0; k < kConeFields; ++k) t[32 * k] = f[k];
 }
 
-__device__ __forceinline__ Cone load_cone(const WarpShared* ws, int owner) {
+template <class WS>
+__device__ __forceinline__ Cone load_cone(const WS* ws, int owner) {
   const float* t = ws->cone + owner;
   Cone c;
   c.apex = mk(t[0], t[32], t[64]);
@@ -150,7 +166,8 @@ __device__ __forceinline__ Cone load_cone(const WarpShared* ws, int owner) {
 // The tests of cover_triangle (:594-616) for one (triangle, cone) pair: back
 // face, the window-direction test, may_touch. A pair that passes is
 // rasterized.
-__device__ __forceinline__ bool pair_survives(const DevScene& s, const WarpShared* ws, int owner, uint32_t t) {
+template <class WS>
+__device__ __forceinline__ bool pair_survives(const DevScene& s, const WS* ws, int owner, uint32_t t) {
   const Cone c = load_cone(ws, owner);
   const f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
   const f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
@@ -163,7 +180,8 @@ __device__ __forceinline__ bool pair_survives(const DevScene& s, const WarpShare
   return may_touch(c, v0, v1, v2);
 }
 
-__device__ __forceinline__ void load_pair(const DevScene& s, const WarpShared* ws, uint32_t e, int& owner, Cone& c,
+template <class WS>
+__device__ __forceinline__ void load_pair(const DevScene& s, const WS* ws, uint32_t e, int& owner, Cone& c,
                                           f3& v0, f3& v1, f3& v2) {
   owner = (int)(e >> kQueueOwnerShift);
   const uint32_t t = e & ((1u << kQueueOwnerShift) - 1u);
@@ -173,7 +191,8 @@ __device__ __forceinline__ void load_pair(const DevScene& s, const WarpShared* w
   v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
 }
 
-__device__ __forceinline__ void note_span(WarpShared* ws, int owner, const LaneAcc& acc) {
+template <class WS, class Acc>
+__device__ __forceinline__ void note_span(WS* ws, int owner, const Acc& acc) {
   if (acc.span_lo < acc.span_hi) {
     atomicMin(&ws->span_lo[owner], acc.span_lo);
     atomicMax(&ws->span_hi[owner], acc.span_hi);
@@ -182,13 +201,14 @@ __device__ __forceinline__ void note_span(WarpShared* ws, int owner, const LaneA
 
 // The general path for general-queue entries first .. first+n (n <= 32),
 // one per lane.
-__device__ __noinline__ void raster_general(const DevScene& s, WarpShared* ws, uint32_t first, uint32_t n, int lane) {
+template <class WS>
+__device__ __noinline__ void raster_general(const DevScene& s, WS* ws, uint32_t first, uint32_t n, int lane) {
   if ((uint32_t)lane < n) {
     int owner;
     Cone c;
     f3 v0, v1, v2;
     load_pair(s, ws, ws->general[first + lane], owner, c, v0, v1, v2);
-    LaneAcc acc{ws->acc + owner, 68u, 0u};
+    LaneAcc<typename WS::Cell> acc{ws->acc + owner, 68u, 0u, &ws->overflow[0], 1u << owner};
     rasterize_general(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2));
     note_span(ws, owner, acc);
   }
@@ -199,7 +219,8 @@ __device__ __noinline__ void raster_general(const DevScene& s, WarpShared* ws, u
 // into its cone's accumulator by the common case; pairs that need the
 // general path join the general queue, which is run whenever 32 wait.
 // Returns the general queue's new length (below 32).
-__device__ __noinline__ uint32_t raster_queue(const DevScene& s, WarpShared* ws, uint32_t first, uint32_t n,
+template <class WS>
+__device__ __noinline__ uint32_t raster_queue(const DevScene& s, WS* ws, uint32_t first, uint32_t n,
                                               uint32_t general, int lane) {
   bool defer = false;
   uint32_t e = 0;
@@ -209,7 +230,7 @@ __device__ __noinline__ uint32_t raster_queue(const DevScene& s, WarpShared* ws,
     Cone c;
     f3 v0, v1, v2;
     load_pair(s, ws, e, owner, c, v0, v1, v2);
-    LaneAcc acc{ws->acc + owner, 68u, 0u};
+    LaneAcc<typename WS::Cell> acc{ws->acc + owner, 68u, 0u, &ws->overflow[0], 1u << owner};
     defer = !rasterize_fast(c, acc, v0, v1, v2);
     note_span(ws, owner, acc);
   }
@@ -230,7 +251,8 @@ __device__ __noinline__ uint32_t raster_queue(const DevScene& s, WarpShared* ws,
 // join the warp's queue, and every 32 queued pairs are rasterized by the
 // whole warp at once, so lanes whose pair was culled do not sit idle while
 // the others rasterize. `queues` and the result are both queues' lengths.
-__device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WarpShared* ws, uint32_t owners, uint32_t t0,
+template <class WS>
+__device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t owners, uint32_t t0,
                                             uint32_t nt, uint32_t queues, int lane) {
   uint32_t queued = fast_len(queues), general = general_len(queues);
   const uint32_t n_owners = __popc(owners);
@@ -261,8 +283,9 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WarpShared* ws, u
 // The mesh's coverage for the lane's own cone: running sum over the touched
 // cells (exact), snapped to whole within 1e-5, combined into the cone's bins
 // by max (:809-828); then the cells are cleared for the next mesh.
-__device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState& st, int lane) {
-  WarpShared* ws = st.ws;
+template <class WS>
+__device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState<WS>& st, int lane) {
+  WS* ws = st.ws;
   // The mesh's last pairs: the common case, then the general path.
   uint32_t general = general_len(st.queued);
   if (fast_len(st.queued)) general = raster_queue(s, ws, 0, fast_len(st.queued), general, lane);
@@ -270,11 +293,19 @@ __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState& st, i
   st.queued = 0;
   const uint32_t lo = ws->span_lo[lane];
   const uint32_t end = min(ws->span_hi[lane], (uint32_t)kBins);
+  // 32-bit cells: a cone whose adds overflowed in this mesh is walked again
+  // with 64-bit cells (its result here is discarded).
+  if (sizeof(typename WS::Cell) == 4) {
+    if ((ws->overflow[0] >> lane) & 1u) st.status |= kStatusAccOverflow;
+    __syncwarp();
+    if (lane == 0) ws->overflow[0] = 0u;
+  }
   long long running = 0;
   for (uint32_t b = lo; b < end; ++b) {
-    unsigned long long* cell = &ws->acc[32 * b + lane];
-    running += (long long)*cell;
-    *cell = 0ull;
+    typename WS::Cell* cell = &ws->acc[32 * b + lane];
+    if (sizeof(typename WS::Cell) == 4) running += (long long)(int)*cell;
+    else running += (long long)*cell;
+    *cell = 0;
     float covered = fabsf(__ll2float_rn(running) * kFixUnit);
     if (covered >= 1.0f - 1e-5f) covered = 1.0f;
     if (covered > 1e-6f) {
@@ -298,8 +329,8 @@ constexpr uint32_t kObjRoot = 3;   // instanced scenes: the root of object `inde
 // add_mesh_coverage_if (:713-829) for hierarchy levels 0 and 1: every
 // triangle of mesh m for the lanes with `on`, in leaf-sized groups, then the
 // mesh's resolve.
-template <bool kCount, bool kInst>
-__device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState& st, bool on, uint32_t m, int lane) {
+template <bool kCount, bool kInst, class WS>
+__device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& st, bool on, uint32_t m, int lane) {
   const uint32_t owners = __ballot_sync(0xffffffffu, on);
   if (!owners) return;
   const uint4 range = __ldg(&s.meshes[m]);
@@ -331,13 +362,13 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState& st, 
 // a lane needs counts toward its walk cap, though its box was tested when its
 // parent was visited. Levels 0 and 1 keep the reference's loops over meshes
 // and triangles.
-template <bool kCount, bool kInst>
-__device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState& st, bool traced,
+template <bool kCount, bool kInst, class WS>
+__device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState<WS>& st, bool traced,
                                            int lane) {
   const Cone& c = st.cone;
   if (hierarchy == 0) {
     for (uint32_t m = 0; m < s.nmeshes; ++m)
-      add_mesh_flat<kCount, kInst>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
+      add_mesh_flat<kCount, kInst, WS>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
     return;
   }
   WarpStack stk;
@@ -390,7 +421,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       // An object leaf: its meshes.
       if (hierarchy == 1) {
         for (uint32_t k = ia; k < ia + ib; ++k)
-          add_mesh_flat<kCount, kInst>(s, st, descend, __ldg(&s.items[k]), lane);
+          add_mesh_flat<kCount, kInst, WS>(s, st, descend, __ldg(&s.items[k]), lane);
         continue;
       }
       for (int k = (int)(ia + ib) - 1; k >= (int)ia; --k) {
@@ -542,17 +573,21 @@ __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, ui
 // kBatch: the cones of every job of a batch (BatchLaunch); each packet's job
 // is looked up in the job table, and the redo list holds batch cone numbers.
 // kInst: the scene's objects place shared geometry with transforms.
-template <bool kCount, bool kBatch, bool kInst>
-// kBlocksPerSm blocks fit the shared memory; saying so bounds the registers
+// kWide: 64-bit accumulator cells (the solo pass); else 32-bit ones (the
+// packet pass), whose overflowed cones the solo pass walks again.
+template <bool kCount, bool kBatch, bool kInst, bool kWide>
+// The blocks the shared memory fits per SM; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm : kBlocksPerSm)
     visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
                       const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
+  using WS = typename std::conditional<kWide, WideShared, NarrowShared>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw) + wib;
-  for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0ull;
+  WS* ws = reinterpret_cast<WS*>(smem_raw) + wib;
+  for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0;
+  if (lane == 0) ws->overflow[0] = 0u;
   ws->span_lo[lane] = 68u;
   ws->span_hi[lane] = 0u;
 
@@ -616,7 +651,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     const uint32_t l = (uint32_t)(c / q.npoints);
     const uint64_t p = c - (uint64_t)l * q.npoints;
 
-    LaneState st;
+    LaneState<WS> st;
     st.ws = ws;
     st.cov = ws->cov + lane;
     st.full = 0;
@@ -711,7 +746,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kBlocksPerSm)
     if (open > 0.0f && last_full) ratio = 0.0f;
 
     if (list) st.status |= 8u;
-    const bool redo = !list && o.redo_list && (st.status & 4u) && (st.status & (1u | 16u));
+    const bool redo = !list && o.redo_list &&
+                      (((st.status & 4u) && (st.status & (1u | 16u))) || (st.status & kStatusAccOverflow));
     if (redo) {
       const uint32_t at = atomicAdd(o.redo_count, 1u);
       if (at < o.redo_capacity) o.redo_list[at] = (uint32_t)(cone_start + c);
@@ -744,24 +780,24 @@ cudaError_t upload_disk_table(const float* table64) {
 
 // Whether the large dynamic shared memory size was allowed, per device and
 // kernel variant (the attribute is set per device).
-static uint64_t g_attr_set[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+static uint64_t g_attr_set[16] = {};
 
-template <bool kCount, bool kBatch, bool kInst>
+template <bool kCount, bool kBatch, bool kInst, bool kWide>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * sizeof(WarpShared);
+  const size_t smem = (size_t)kWarpsPerBlock * (kWide ? sizeof(WideShared) : sizeof(NarrowShared));
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
-  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0);
+  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0);
   if (!(g_attr_set[variant] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst>,
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     g_attr_set[variant] |= bit;
   }
-  visibility_kernel<kCount, kBatch, kInst><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
+  visibility_kernel<kCount, kBatch, kInst, kWide><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
   return cudaGetLastError();
 }
 
@@ -785,21 +821,28 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
   const BatchLaunch none{};
   const bool inst = s.xforms != nullptr;
-  auto one = [&](const uint32_t* list, const uint32_t* list_count, uint32_t p, uint32_t nb) {
+  // The packet pass with 32-bit accumulator cells, the solo pass with 64-bit.
+  auto packets_pass = [&](uint32_t p, uint32_t nb) {
     if (inst)
-      return count ? launch_one<true, false, true>(s, q, o, none, list, list_count, p, nb, stream)
-                   : launch_one<false, false, true>(s, q, o, none, list, list_count, p, nb, stream);
-    return count ? launch_one<true, false, false>(s, q, o, none, list, list_count, p, nb, stream)
-                 : launch_one<false, false, false>(s, q, o, none, list, list_count, p, nb, stream);
+      return count ? launch_one<true, false, true, false>(s, q, o, none, nullptr, nullptr, p, nb, stream)
+                   : launch_one<false, false, true, false>(s, q, o, none, nullptr, nullptr, p, nb, stream);
+    return count ? launch_one<true, false, false, false>(s, q, o, none, nullptr, nullptr, p, nb, stream)
+                 : launch_one<false, false, false, false>(s, q, o, none, nullptr, nullptr, p, nb, stream);
   };
-  cudaError_t e = one(nullptr, nullptr, pw, blocks);
+  auto solo_pass = [&](uint32_t nb) {
+    if (inst)
+      return count ? launch_one<true, false, true, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream)
+                   : launch_one<false, false, true, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream);
+    return count ? launch_one<true, false, false, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream)
+                 : launch_one<false, false, false, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream);
+  };
+  cudaError_t e = packets_pass(pw, blocks);
   if (marks) cudaEventRecord(marks[1], stream);
   if (e != cudaSuccess) return e;
   if (o.redo_list) {
     // The listed cones, each walked alone (one cone per warp; the warp still
     // shares its leaves' triangles).
-    const uint32_t solo_blocks = (uint32_t)sm_count * kBlocksPerSm;
-    e = one(o.redo_list, o.redo_count, 1, solo_blocks);
+    e = solo_pass((uint32_t)sm_count * kSoloBlocksPerSm);
   }
   if (marks) cudaEventRecord(marks[2], stream);
   return e;
@@ -815,12 +858,12 @@ cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count, int 
   const uint64_t want = (b.packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
   const uint64_t cap = (uint64_t)sm_count * blocks_per_sm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-  cudaError_t e = count ? launch_one<true, true, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
-                        : launch_one<false, true, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+  cudaError_t e = count ? launch_one<true, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
+                        : launch_one<false, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
   if (e != cudaSuccess || !o.redo_list) return e;
-  const uint32_t solo_blocks = (uint32_t)cap;
-  return count ? launch_one<true, true, false>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
-               : launch_one<false, true, false>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+  const uint32_t solo_blocks = (uint32_t)sm_count * kSoloBlocksPerSm;
+  return count ? launch_one<true, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+               : launch_one<false, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
 }
 
 }  // namespace cc

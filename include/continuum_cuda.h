@@ -60,7 +60,7 @@ extern "C" {
 
 /* cc_options.flags */
 #define CC_DEVICE_POINTERS 1u /* receivers, lights and outputs are device pointers */
-#define CC_NO_REDO 2u         /* skip the solo re-walk of order-diverged cones (diagnostic) */
+#define CC_NO_REDO 2u         /* skip the solo re-walk (diagnostic): order-diverged and overflowed cones keep their packet results */
 #define CC_KEEP_ORDER 4u      /* walk points in the given order (default: Morton order of their positions) */
 
 /* Status bits in cc_outputs.work[4 * c + 3] */
@@ -69,6 +69,7 @@ extern "C" {
 #define CC_CONE_DIVERGED 4u   /* its packet's child order differed from its own */
 #define CC_CONE_REWALKED 8u   /* recomputed walking alone */
 #define CC_CONE_FULL_STOP 16u /* the walk stopped early with every bin full */
+#define CC_CONE_ACC_WIDE 32u  /* its 32-bit accumulation overflowed: recomputed with 64-bit cells */
 
 typedef struct cc_context cc_context;
 typedef struct cc_scene cc_scene;
@@ -261,11 +262,11 @@ typedef struct cc_batch cc_batch;
 
 typedef struct cc_batch_options {
   uint32_t points_per_warp; /* cones per packet: 1..32 (32) */
-  uint32_t blocks_per_sm;   /* resident blocks per SM launched: 1..4 (4) */
+  uint32_t blocks_per_sm;   /* resident blocks per SM launched: 1..5 (5) */
   uint32_t flags;           /* CC_KEEP_ORDER, CC_NO_REDO, CC_BATCH_GRAPH */
 } cc_batch_options;
 
-/* Defaults: 32 cones per packet, 4 blocks per SM, CC_BATCH_GRAPH. */
+/* Defaults: 32 cones per packet, 5 blocks per SM, CC_BATCH_GRAPH. */
 CC_API void cc_batch_options_default(cc_batch_options* opt);
 
 CC_API int cc_batch_create(cc_context* ctx, cc_batch** out);
@@ -290,7 +291,7 @@ CC_API int cc_batch_submit(cc_batch* batch, const cc_batch_options* opt, void* s
  * not finished, CC_ERR_STACK if a traversal stack overflowed, else CC_OK. */
 CC_API int cc_batch_wait(cc_batch* batch, uint32_t timeout_ms);
 /* The autotuner: times every candidate launch configuration (cones per
- * packet 8, 16, 32 x Morton or given walk order x 2 or 4 blocks per SM) on
+ * packet 8, 16, 32 x Morton or given walk order x 3 or 5 blocks per SM) on
  * this batch, `reps` runs each, and writes the fastest to *best (keeping
  * base->flags' CC_BATCH_GRAPH and CC_NO_REDO; base nullable). ms_out
  * (nullable, max_candidates entries) receives each candidate's best time in
@@ -326,10 +327,10 @@ typedef struct cc_server_options {
   uint32_t max_queue;        /* queued requests before submissions are refused with CC_ERR_BUSY (256) */
   uint64_t max_launch_cones; /* cones one launch takes at most (8M); one larger request runs alone */
   uint32_t points_per_warp;  /* 1..32 (32) */
-  uint32_t blocks_per_sm;    /* 1..4 (4) */
+  uint32_t blocks_per_sm;    /* 1..5 (5) */
 } cc_server_options;
 
-/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 8M cones per launch, 32, 4. */
+/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 8M cones per launch, 32, 5. */
 CC_API void cc_server_options_default(cc_server_options* opt);
 
 typedef struct cc_request {

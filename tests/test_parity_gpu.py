@@ -223,3 +223,25 @@ def test_golden_fixtures(kernel):
     from golden_fixtures import check_all
 
     check_all(kernel)
+
+
+def test_stacked_layers_overflow_to_wide_accumulators(kernel):
+    """One mesh of 200 stacked quads over the receivers piles 200 bins' worth
+    of coverage into each cell: the packet pass's 32-bit accumulators
+    overflow, the cones are walked again with 64-bit ones (status
+    CC_CONE_ACC_WIDE), and the results are the oracle's."""
+    quads = []
+    for k in range(200):
+        y = 1.0 + 0.01 * k
+        quads.append(np.array([[[-2, y, -2], [-2, y, 2], [2, y, 2]], [[-2, y, -2], [2, y, 2], [2, y, -2]]],
+                              np.float32))
+    stack = np.concatenate(quads)
+    light = RectLight((-0.5, 4.0, -0.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0))
+    xs = np.linspace(-1.0, 1.0, 16, dtype=np.float32)
+    pts = np.stack(np.meshgrid(xs, [0.0], xs, indexing="ij"), -1).reshape(-1, 3)
+    rec = kat.receivers(pts, (0.0, 1.0, 0.0))
+    g, o = run_both(kernel, [stack], rec, kat.lights16(light))
+    wide = (g["work"][:, 3] & _lib.CC_CONE_ACC_WIDE) != 0
+    assert wide.mean() > 0.5
+    parity.compare(g, o, o["unshadowed"])
+    assert np.all(g["full"] == np.uint64(0xFFFFFFFFFFFFFFFF))
