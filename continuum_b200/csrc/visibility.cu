@@ -745,6 +745,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     if (open > 0.0f && last_empty) ratio = 1.0f;
     if (open > 0.0f && last_full) ratio = 0.0f;
 
+    // A walk again keeps the reasons its packet pass listed the cone for.
+    if (valid && list && out_work) st.status |= out_work[c].w & (4u | kStatusAccOverflow);
     if (list) st.status |= 8u;
     const bool redo = !list && o.redo_list &&
                       (((st.status & 4u) && (st.status & (1u | 16u))) || (st.status & kStatusAccOverflow));
@@ -754,6 +756,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
       else atomicOr(o.error, 1u);
     }
     if (st.status & 2u) atomicOr(o.error, 2u);
+    if (valid && redo && out_work) out_work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
     if (valid && !redo) {
       if (out_full) out_full[c] = make_uint2(fw0, fw1);
       if (out_any) out_any[c] = make_uint2(aw0, aw1);

@@ -233,7 +233,8 @@ def test_stacked_layers_overflow_to_wide_accumulators(kernel):
     quads = []
     for k in range(200):
         y = 1.0 + 0.01 * k
-        quads.append(np.array([[[-2, y, -2], [-2, y, 2], [2, y, 2]], [[-2, y, -2], [2, y, 2], [2, y, -2]]],
+        # Wound to face the receivers below (a triangle facing away is culled).
+        quads.append(np.array([[[-2, y, -2], [2, y, 2], [-2, y, 2]], [[-2, y, -2], [2, y, -2], [2, y, 2]]],
                               np.float32))
     stack = np.concatenate(quads)
     light = RectLight((-0.5, 4.0, -0.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0))
