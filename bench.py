@@ -436,6 +436,65 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
                        "speedup_vs_full_solve": (full_ms / upd) if upd else None}}
 
 
+def bake_leg(args, kernel, scene, w) -> dict:
+    """The lighting cache's bake over the plain workload's view: pages of 8 x 8
+    texels (stored 9 x 9) over the camera's 1280 x 720 hit grid (a stand-in
+    for the cache's charts: one page per 8 x 8 pixels), 4 lights, nearest the
+    image centre first. With a fixed budget of `--bake-budget` cones a frame
+    the view warms in a few frames: device cones/s from the bake's CUDA events,
+    wall time per frame with planning and staging. Then with a 14 ms frame
+    target and 4 ms of camera passes: the budget the bake model settles on,
+    and the bake time it gives."""
+    from continuum_b200 import LightingCache, scenes
+    from continuum_b200.kernel import prepare_requests
+
+    width, height = 1280, 720
+    rec, hit = scene.primary_hits(w.camera, width, height)
+    pages = scenes.grid_pages(rec.reshape(height, width, 8), hit.reshape(height, width).astype(bool))
+    for p in pages:
+        _, py, px = p.key
+        p.priority = int(abs(py * 8 + 4 - height / 2) + abs(px * 8 + 4 - width / 2))
+    prepared = prepare_requests(pages)
+    out = {"workload": f"{len(pages)} pages over the {width}x{height} hit grid of the plain workload, "
+                       f"{w.lights.shape[0]} lights, visible fraction (light_ratio)", "pages": len(pages)}
+
+    def run(frames_max, **opt):
+        cache = LightingCache(kernel, scene, w.lights, pages=16384, **opt)
+        rows, jobs_prev = [], 0
+        for f in range(frames_max):
+            t0 = time.perf_counter()
+            st = cache.frame(prepared, period_ms=16.0, render_ms=4.0)
+            rows.append({"frame": f, "budget": st["budget"], "pages": st["pages_planned"], "cones": st["jobs"],
+                         "host_ms": (time.perf_counter() - t0) * 1e3, "prev_bake_ms": st["last_bake_ms"]})
+            if st["pages_planned"] == 0:
+                break
+        cache.frame(prepared)  # reads the last bake's time
+        last = cache.frame(prepared)
+        for i in range(len(rows) - 1):
+            rows[i]["bake_ms"] = rows[i + 1]["prev_bake_ms"]
+        rows[-1]["bake_ms"] = last["last_bake_ms"] if rows[-1]["cones"] else 0.0
+        resident = last["resident"]
+        cache.close()
+        return rows, resident
+
+    run(2, bake_budget=args.bake_budget)  # warm-up (untimed): first use of the bake's kernels and buffers
+    rows, resident = run(200, bake_budget=args.bake_budget)
+    baked = [r for r in rows if r["cones"]]
+    cones = sum(r["cones"] for r in baked)
+    dev_ms = sum(r["bake_ms"] for r in baked)
+    out["fixed_budget"] = {"bake_budget": args.bake_budget, "frames_to_warm": len(baked), "resident": resident,
+                           "cones": cones, "value": cones / (dev_ms * 1e-3) if dev_ms > 0 else None, "unit": UNIT,
+                           "bake_ms_per_frame": [round(r["bake_ms"], 3) for r in baked],
+                           "host_ms_per_frame": [round(r["host_ms"], 3) for r in baked],
+                           "timing": "CUDA events around each bake (texel upload, visibility, pool scatter)"}
+    rows, resident = run(60, bake_budget=1 << 22, frame_target_ms=14.0)
+    out["adaptive"] = {"frame_target_ms": 14.0, "render_ms": 4.0,
+                       "budget": [round(r["budget"]) for r in rows if r["cones"]],
+                       "bake_ms": [round(r["bake_ms"], 3) for r in rows if r["cones"]],
+                       "frames_to_warm": sum(1 for r in rows if r["cones"])}
+    return out
+
+
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
@@ -610,6 +669,8 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         line["served"] = served_leg(args, kernel)
     if "instanced" in forms:
         line["instanced"] = instanced_leg(args, kernel, dev, stream, flush)
+    if "bake" in forms:
+        line["bake"] = bake_leg(args, kernel, scene, w)
     if world == 1 and not args.no_cpu_baseline:
         rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
@@ -630,8 +691,10 @@ def main() -> None:
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--forms", default="batched,served,instanced",
-                    help="systems forms measured beside the plain line (comma list of batched, served, instanced; none)")
+    ap.add_argument("--forms", default="batched,served,instanced,bake",
+                    help="systems forms measured beside the plain line (comma list of batched, served, instanced, "
+                         "bake; none)")
+    ap.add_argument("--bake-budget", type=int, default=1 << 20, help="cones a frame of the bake leg's fixed budget")
     ap.add_argument("--instances", type=int, default=1_000_000)
     ap.add_argument("--frames", type=int, default=3, help="moving frames of the instanced leg")
     ap.add_argument("--batch-jobs", type=int, default=64)

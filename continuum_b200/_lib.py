@@ -44,7 +44,9 @@ EXPORTS = (
     "cc_batch_add", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
     "cc_server_options_default", "cc_server_create", "cc_server_destroy", "cc_server_add_scene", "cc_server_submit",
     "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms", "cc_scene_move",
-    "cc_stale_cones", "cc_visibility_update",
+    "cc_stale_cones", "cc_visibility_update", "cc_cache_options_default", "cc_cache_create", "cc_cache_destroy",
+    "cc_cache_frame", "cc_cache_read", "cc_cache_pool", "cc_cache_jobs", "cc_planner_create", "cc_planner_destroy",
+    "cc_planner_frame", "cc_planner_jobs", "cc_planner_slot",
 )
 
 # cc_instance: an object placing a geometry (world = scale * rotation * p + translation).
@@ -85,6 +87,24 @@ class BatchOptions(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget", C.c_uint64), ("max_inflight", C.c_uint32), ("max_queue", C.c_uint32),
                 ("max_launch_cones", C.c_uint64), ("points_per_warp", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+
+
+class CacheOptions(C.Structure):
+    _fields_ = [("pages", C.c_uint32), ("bake_budget", C.c_uint32), ("frame_target_ms", C.c_float),
+                ("frame_budget_ms", C.c_float), ("floor_overrun", C.c_float), ("light_ratio", C.c_uint32)]
+
+
+class PageRequest(C.Structure):
+    _fields_ = [("key", C.c_uint32 * 3), ("priority", C.c_uint32), ("inside", C.c_uint32 * 2), ("texels", C.c_void_p)]
+
+
+class CacheFrameInfo(C.Structure):
+    _fields_ = [("period_ms", C.c_float), ("render_ms", C.c_float), ("gpu_waited", C.c_uint32)]
+
+
+class CacheStats(C.Structure):
+    _fields_ = [("budget", C.c_float), ("frame", C.c_uint32), ("pages_planned", C.c_uint32), ("jobs", C.c_uint32),
+                ("spent", C.c_uint32), ("resident", C.c_uint32), ("evicted", C.c_uint32), ("last_bake_ms", C.c_float)]
 
 
 class Request(C.Structure):
@@ -155,6 +175,18 @@ def load() -> C.CDLL:
         "cc_stale_cones": (I, [P, P, P, U64, P, U32, P, U32, P, C.POINTER(U64), P]),
         "cc_visibility_update": (I, [P, P, P, U64, P, U32, P, C.POINTER(Options), C.POINTER(Outputs), C.POINTER(U64), P]),
         "cc_scene_transforms": (U64, [P, P, U64]),
+        "cc_cache_options_default": (None, [C.POINTER(CacheOptions)]),
+        "cc_cache_create": (I, [P, P, P, U32, C.POINTER(CacheOptions), C.POINTER(P)]),
+        "cc_cache_destroy": (I, [P]),
+        "cc_cache_frame": (I, [P, P, U32, C.POINTER(CacheFrameInfo), C.POINTER(CacheStats)]),
+        "cc_cache_read": (I, [P, P, P]),
+        "cc_cache_pool": (I, [P, C.POINTER(P), C.POINTER(U32)]),
+        "cc_cache_jobs": (C.c_int64, [P, P, U64, P, U32]),
+        "cc_planner_create": (I, [C.POINTER(CacheOptions), U32, C.POINTER(P)]),
+        "cc_planner_destroy": (I, [P]),
+        "cc_planner_frame": (I, [P, P, U32, C.POINTER(CacheFrameInfo), C.c_float, C.POINTER(CacheStats)]),
+        "cc_planner_jobs": (C.c_int64, [P, P, U64, P, U32]),
+        "cc_planner_slot": (C.c_int64, [P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

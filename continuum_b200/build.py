@@ -15,7 +15,8 @@ LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libcontinuum_cuda.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["visibility.cu", "order.cu", "capi.cu", "batch.cu", "server.cu", "movers.cu", "static_scratch.cu", "bvh.cpp", "raycast.cpp"]
+SOURCES = ["visibility.cu", "order.cu", "capi.cu", "batch.cu", "server.cu", "movers.cu", "cache.cu", "static_scratch.cu", "bvh.cpp",
+           "raycast.cpp", "cache_plan.cpp"]
 # The cone geometry is evaluated without fused multiply-adds: the reference's
 # clip and cull decisions are ill-conditioned in f32 for receivers lifted
 # 1e-4 off curved surfaces (the plane through the apex and a near edge),

@@ -626,3 +626,180 @@ def kernel_times(kernel: MaskConeKernel, max_calls: int = 256) -> np.ndarray:
     if n < 0:
         check(-n)
     return out[:n]
+
+
+# ---- the lighting cache's bake ---------------------------------------------------
+
+PAGE_TEXELS = 81  # 8 x 8 texels stored 9 x 9 (vcache.rs:32-35)
+#: Texel flags (the w of a texel record's point): outside the chart's grid,
+#: inside without a surface, a surface to bake.
+TEXEL_OUTSIDE, TEXEL_EMPTY, TEXEL_SURFACE = 0.0, 1.0, 2.0
+
+
+@dataclass
+class PageRequest:
+    """A page a view wants (vcache.rs: a request with its priority): `key` of
+    3 u32, `priority` (lower first), `inside` texels per axis (0..9) and
+    `texels`, 81 x 8 floats (point.xyz, flag, normal.xyz, 0), row-major 9 x 9,
+    needed only when the page is not resident."""
+
+    key: Sequence[int]
+    priority: int
+    inside: Sequence[int] = (8, 8)
+    texels: Optional[np.ndarray] = None
+
+
+def cache_options(pages: int = 1 << 16, bake_budget: int = 1 << 20, frame_target_ms: float = 0.0,
+                  frame_budget_ms: float = 0.0, floor_overrun: float = 0.25, light_ratio: bool = True):
+    return _lib.CacheOptions(int(pages), int(bake_budget), float(frame_target_ms), float(frame_budget_ms),
+                             float(floor_overrun), 1 if light_ratio else 0)
+
+
+class PreparedRequests:
+    """Page requests converted once for the C ABI, for a view that asks for
+    the same pages frame after frame."""
+
+    def __init__(self, reqs: Sequence[PageRequest]):
+        self.arr, self.keep = _requests(reqs)
+        self.n = len(reqs)
+
+
+def prepare_requests(reqs: Sequence[PageRequest]) -> PreparedRequests:
+    return PreparedRequests(reqs)
+
+
+def _requests(reqs):
+    if isinstance(reqs, PreparedRequests):
+        return reqs.arr, reqs.keep
+    arr = (_lib.PageRequest * max(len(reqs), 1))()
+    keep = []
+    for i, r in enumerate(reqs):
+        arr[i].key[:] = [int(x) for x in r.key]
+        arr[i].priority = int(r.priority)
+        arr[i].inside[:] = [int(x) for x in r.inside]
+        if r.texels is not None:
+            t = np.ascontiguousarray(r.texels, dtype=np.float32).reshape(PAGE_TEXELS, 8)
+            keep.append(t)
+            arr[i].texels = t.ctypes.data
+        else:
+            arr[i].texels = None
+    return arr, keep
+
+
+def _count(reqs) -> int:
+    return reqs.n if isinstance(reqs, PreparedRequests) else len(reqs)
+
+
+def _stats(s: _lib.CacheStats) -> dict:
+    return {k: getattr(s, k) for k, _ in _lib.CacheStats._fields_}
+
+
+def _frame_info(period_ms: float, render_ms: float, gpu_waited: bool):
+    return _lib.CacheFrameInfo(float(period_ms), float(render_ms), 1 if gpu_waited else 0)
+
+
+def _jobs(fn, handle, max_pages: int = 1 << 20):
+    n = fn(handle, None, 0, None, 0)
+    if n < 0:
+        check(int(-n))
+    jobs = np.zeros((max(n, 1), 2), np.uint32)
+    slots = np.zeros(max_pages, np.uint32)
+    fn(handle, ptr(jobs), int(n), ptr(slots), int(max_pages))
+    return jobs[:n], slots
+
+
+class Planner:
+    """The lighting cache's page manager alone, on the host (cc_planner_*):
+    each frame plans the requested pages within the bake budget, adapts the
+    budget to the frame time from the bake's measured GPU time, and lists the
+    bake jobs [bake-list index, texel | light << 8]."""
+
+    def __init__(self, nlights: int = 1, **options):
+        h = C.c_void_p()
+        opt = cache_options(**options)
+        check(load().cc_planner_create(C.byref(opt), int(nlights), C.byref(h)))
+        self._h = h
+        self.nlights = nlights
+
+    def frame(self, requests: Sequence[PageRequest], period_ms: float = 0.0, render_ms: float = 0.0,
+              gpu_waited: bool = False, bake_ms: float = -1.0) -> dict:
+        arr, _keep = _requests(requests)
+        st = _lib.CacheStats()
+        info = _frame_info(period_ms, render_ms, gpu_waited)
+        check(load().cc_planner_frame(self._h, arr, _count(requests), C.byref(info), float(bake_ms), C.byref(st)))
+        return _stats(st)
+
+    def jobs(self):
+        """(jobs (n, 2) u32, slot per planned page) of the last frame."""
+        jobs, slots = _jobs(load().cc_planner_jobs, self._h)
+        return jobs, slots[: (int(jobs[:, 0].max()) + 1) if len(jobs) else 0]
+
+    def slot(self, key) -> int:
+        k = np.asarray(key, np.uint32)
+        return int(load().cc_planner_slot(self._h, ptr(k)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().cc_planner_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LightingCache:
+    """The lighting cache's direct-light bake on the device (cc_cache_*): a
+    pool of pages, one channel per light, baked frame by frame from the
+    view's page requests within the bake budget."""
+
+    def __init__(self, kernel: MaskConeKernel, scene: Scene, lights, **options):
+        self.kernel, self.scene = kernel, scene
+        self.lights = np.ascontiguousarray(lights_gpu(lights) if not isinstance(lights, np.ndarray) else lights,
+                                           dtype=np.float32).reshape(-1, 16)
+        h = C.c_void_p()
+        opt = cache_options(**options)
+        check(load().cc_cache_create(kernel.handle, scene.handle, ptr(self.lights), self.lights.shape[0],
+                                     C.byref(opt), C.byref(h)))
+        self._h = h
+
+    @property
+    def nlights(self) -> int:
+        return self.lights.shape[0]
+
+    def frame(self, requests: Sequence[PageRequest], period_ms: float = 0.0, render_ms: float = 0.0,
+              gpu_waited: bool = False) -> dict:
+        arr, _keep = _requests(requests)
+        st = _lib.CacheStats()
+        info = _frame_info(period_ms, render_ms, gpu_waited)
+        check(load().cc_cache_frame(self._h, arr, _count(requests), C.byref(info), C.byref(st)))
+        return _stats(st)
+
+    def read(self, key) -> np.ndarray:
+        """A resident page's (81, nlights) pool values."""
+        k = np.asarray(key, np.uint32)
+        out = np.zeros((PAGE_TEXELS, self.nlights), np.float32)
+        check(load().cc_cache_read(self._h, ptr(k), ptr(out)))
+        return out
+
+    def jobs(self):
+        jobs, slots = _jobs(load().cc_cache_jobs, self._h)
+        return jobs, slots[: (int(jobs[:, 0].max()) + 1) if len(jobs) else 0]
+
+    def pool(self) -> tuple[int, int]:
+        p, ch = C.c_void_p(), C.c_uint32()
+        check(load().cc_cache_pool(self._h, C.byref(p), C.byref(ch)))
+        return int(p.value or 0), int(ch.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().cc_cache_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

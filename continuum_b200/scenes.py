@@ -551,3 +551,28 @@ def moved_placements(world: InstancedWorld, movable: np.ndarray, frame: int, ste
     rot[:, 0], rot[:, 2], rot[:, 4], rot[:, 6], rot[:, 8] = c, s, 1.0, -s, c
     out["rotation"] = rot
     return out
+
+
+def grid_pages(grid: np.ndarray, surface: Optional[np.ndarray] = None, object_id: int = 0) -> list:
+    """Lighting-cache pages over a (rows, cols) grid of receivers, a stand-in
+    for one chart at one mip (the cache's charts are not part of this
+    library): page (px, py) holds the grid points [py * 8 + y, px * 8 + x]
+    for x, y in 0..8 (8 x 8 texels stored 9 x 9, vcache.rs:32-35); `inside`
+    counts those within the grid; a texel's flag is 2 where `surface` is true
+    (all by default), 1 where it is not, 0 past the grid. Keys are
+    (object_id, py, px); priorities 0."""
+    from .kernel import PageRequest
+    rows, cols = grid.shape[:2]
+    if surface is None:
+        surface = np.ones((rows, cols), bool)
+    pages = []
+    for py in range((rows - 1) // 8 + 1 if rows > 1 else 1):
+        for px in range((cols - 1) // 8 + 1 if cols > 1 else 1):
+            t = np.zeros((9, 9, 8), np.float32)
+            r0, c0 = py * 8, px * 8
+            ins = (min(9, cols - c0), min(9, rows - r0))
+            t[: ins[1], : ins[0]] = grid[r0:r0 + ins[1], c0:c0 + ins[0]]
+            t[: ins[1], : ins[0], 3] = np.where(surface[r0:r0 + ins[1], c0:c0 + ins[0]], 2.0, 1.0)
+            t[: ins[1], : ins[0], 7] = 0.0
+            pages.append(PageRequest((object_id, py, px), 0, ins, t.reshape(81, 8)))
+    return pages

@@ -399,6 +399,102 @@ CC_API int cc_irradiance(cc_context* ctx, const float* receivers6, uint64_t npoi
 CC_API int cc_coverage(cc_context* ctx, const float* receivers6, uint64_t npoints, const float* light9, int one_sided,
                 const float* tri9, const uint32_t* mesh_counts, uint32_t nmeshes, float* out64);
 
+/* ---- The lighting cache's bake (the consumer of the visible fraction) ------
+ * Replaces the direct-light bake of crates/continuum-gpu/src/vcache.rs
+ * (`VirtualCache`: the page manager `plan` :3704, `plan_page` :3928, the
+ * adaptive budget of `begin_frame` :2976-3080) and the `vc_bake` pass
+ * (mask_cones.wgsl:3433-3554) for static lights. Pages are 8 x 8 texels
+ * stored 9 x 9 (81, row-major); the pool holds one channel per light:
+ * pool[(slot * 81 + texel) * nlights + light]. Each frame the page requests
+ * are planned in priority order within the bake budget (cones: a page costs
+ * its inside texels x lights; the first page always fits), new pages take
+ * free slots (pages unused for 64 frames are evicted once a quarter of the
+ * pool is resident; when the pool is full, pages unused for 2 frames), and
+ * the planned pages' listed texels (inside + 1 per axis, at most 9) are baked
+ * for every light: one cone per job [bake-list index, texel | light << 8].
+ * The pool receives the visible fraction of the unshadowed light (the
+ * reference's `light_ratio`) or the shadowed light; a texel without a
+ * surface receives 0, one outside the chart's grid nothing. Not built: sky
+ * samples, bounce light, moving lights (lattice, ledger), lighting levels and
+ * the light-below-the-horizon estimator (such texels take ratio 1, as the
+ * reference gives moving lights). */
+typedef struct cc_cache cc_cache;
+typedef struct cc_planner cc_planner;
+
+typedef struct cc_cache_options {
+  uint32_t pages;          /* pool slots (CacheOptions::pages, vcache.rs:218) */
+  uint32_t bake_budget;    /* the most cones a frame (CacheOptions::bake_budget, :183) */
+  float frame_target_ms;   /* the frame period the bake aims for; 0: always bake_budget (:194) */
+  float frame_budget_ms;   /* frames are capped to this period (0: no cap; :196-207) */
+  float floor_overrun;     /* CacheOptions::floor_overrun (:208-213) */
+  uint32_t light_ratio;    /* 1: the pool keeps the visible fraction; 0: the shadowed light */
+} cc_cache_options;
+
+/* Defaults: 65,536 pages, 1,048,576 cones, 0 ms, 0 ms, 0.25, light_ratio 1. */
+CC_API void cc_cache_options_default(cc_cache_options* opt);
+
+typedef struct cc_page_request {
+  uint32_t key[3];        /* the page's identity (object, chart and mip, page coordinates: the caller's packing) */
+  uint32_t priority;      /* lower first */
+  uint32_t inside[2];     /* texels of the page inside its chart's grid along x and y (0..9) */
+  const float* texels;    /* 81 receiver records of 8 floats (point.xyz, flag, normal.xyz, 0), row-major 9 x 9;
+                             flag 0: outside the chart's grid, 1: inside without a surface, 2: a surface to bake.
+                             Host memory, read during cc_cache_frame; may be null for pages that are resident */
+} cc_page_request;
+
+typedef struct cc_cache_frame_info {
+  float period_ms;        /* the previous frame's period (<= 0: not known) */
+  float render_ms;        /* the previous frame's camera passes on the GPU (ms) */
+  uint32_t gpu_waited;    /* 1 if the CPU waited more than 1 ms for the GPU in the previous frame */
+} cc_cache_frame_info;
+
+typedef struct cc_cache_stats {
+  float budget;           /* this frame's bake budget (cones) */
+  uint32_t frame;         /* this frame's number */
+  uint32_t pages_planned; /* pages baked this frame */
+  uint32_t jobs;          /* cones baked this frame (listed texels x lights) */
+  uint32_t spent;         /* budget spent (inside texels x lights) */
+  uint32_t resident;      /* pages resident after planning */
+  uint32_t evicted;       /* pages evicted so far */
+  float last_bake_ms;     /* the previous frame's bake on the GPU (ms; < 0: none) */
+} cc_cache_stats;
+
+/* A cache of `scene` (which must outlive it) lit by `nlights` static lights
+ * (16 floats each, copied). */
+CC_API int cc_cache_create(cc_context* ctx, const cc_scene* scene, const float* lights, uint32_t nlights,
+                           const cc_cache_options* opt, cc_cache** out);
+CC_API int cc_cache_destroy(cc_cache* cache);
+/* One frame: the previous bake's GPU time feeds the budget, the requests are
+ * planned, and the planned pages are baked on the context's stream (not
+ * waited for). A request for a resident page counts as its use this frame.
+ * `info` and `stats` are nullable. */
+CC_API int cc_cache_frame(cc_cache* cache, const cc_page_request* requests, uint32_t nrequests,
+                          const cc_cache_frame_info* info, cc_cache_stats* stats);
+/* A resident page's 81 x nlights pool values (texel-major), after its bake:
+ * CC_OK, or CC_ERR_INVALID if the page is not resident. */
+CC_API int cc_cache_read(cc_cache* cache, const uint32_t key[3], float* out);
+/* The device pool and its channel count (lights). */
+CC_API int cc_cache_pool(cc_cache* cache, float** pool, uint32_t* channels);
+/* The last frame's bake job list: pairs [bake-list index, texel | light << 8]
+ * (at most max_jobs written), and per planned page its slot. Returns the job
+ * count, or minus a status code. */
+CC_API int64_t cc_cache_jobs(cc_cache* cache, uint32_t* jobs2, uint64_t max_jobs, uint32_t* page_slots,
+                             uint32_t max_pages);
+
+/* The page manager alone, on the host (no device work): the same planning
+ * and budget as cc_cache_frame, with the bake's GPU time supplied. */
+CC_API int cc_planner_create(const cc_cache_options* opt, uint32_t nlights, cc_planner** out);
+CC_API int cc_planner_destroy(cc_planner* planner);
+/* begin the frame (bake_ms < 0: no timing of the previous bake, else its GPU
+ * time over the previous frame's spent budget), plan it, end it. */
+CC_API int cc_planner_frame(cc_planner* planner, const cc_page_request* requests, uint32_t nrequests,
+                            const cc_cache_frame_info* info, float bake_ms, cc_cache_stats* stats);
+/* The last planned frame's jobs and page slots, as cc_cache_jobs. */
+CC_API int64_t cc_planner_jobs(cc_planner* planner, uint32_t* jobs2, uint64_t max_jobs, uint32_t* page_slots,
+                               uint32_t max_pages);
+/* The slot of a resident page, or -1. */
+CC_API int64_t cc_planner_slot(cc_planner* planner, const uint32_t key[3]);
+
 #ifdef __cplusplus
 }
 #endif
