@@ -495,6 +495,40 @@ def bake_leg(args, kernel, scene, w) -> dict:
     return out
 
 
+def sky_leg(args, kernel, dev, stream, flush) -> dict:
+    """Sky cones on the small plain workload (the ground and 64 boxes, 770
+    triangles; its 256 x 256 receivers lifted 1e-4 off the ground): six
+    cube-face cones per receiver (393,216 cones), the irradiance per unit
+    uniform sky radiance per receiver, device-timed with CUDA events (L2
+    flushed between steps). Exact sky cones reach 1e7 past each receiver over
+    a 90-degree face, so their cost grows with the whole scene in view (the
+    reference prefilters them, which this library does not build)."""
+    import torch
+
+    from continuum_b200 import scenes
+
+    w = scenes.box_field()
+    rec_h = w.receivers.copy()
+    rec_h[:, 1] = 1e-4
+    scene = kernel.scene(w.meshes)
+    P = rec_h.shape[0]
+    rec = torch.from_numpy(rec_h).to(dev)
+    out = torch.empty(P, device=dev)
+    faces = torch.empty(6 * P, device=dev)
+
+    def step():
+        kernel.sky_visibility_device(scene, rec.data_ptr(), P, out.data_ptr(), faces={"irradiance": faces.data_ptr()},
+                                     stream=stream.cuda_stream)
+
+    steps = max(1, min(args.steps, 5))
+    ms = float(np.mean(timed_steps(torch, dev, stream, flush, step, 2, steps)))
+    mean = float(out.mean().item())
+    scene.close()
+    return {"workload": f"sky cones: 6 cube faces x {P} receivers of the small plain workload (770 triangles)",
+            "cones": 6 * P, "value": 6 * P / (ms * 1e-3), "unit": UNIT, "ms": ms, "steps": steps,
+            "mean_irradiance_per_unit_sky": mean, "timing": "CUDA events, L2 flushed"}
+
+
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
@@ -671,6 +705,8 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         line["instanced"] = instanced_leg(args, kernel, dev, stream, flush)
     if "bake" in forms:
         line["bake"] = bake_leg(args, kernel, scene, w)
+    if "sky" in forms:
+        line["sky"] = sky_leg(args, kernel, dev, stream, flush)
     if world == 1 and not args.no_cpu_baseline:
         rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
@@ -691,9 +727,9 @@ def main() -> None:
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--forms", default="batched,served,instanced,bake",
+    ap.add_argument("--forms", default="batched,served,instanced,bake,sky",
                     help="systems forms measured beside the plain line (comma list of batched, served, instanced, "
-                         "bake; none)")
+                         "bake, sky; none)")
     ap.add_argument("--bake-budget", type=int, default=1 << 20, help="cones a frame of the bake leg's fixed budget")
     ap.add_argument("--instances", type=int, default=1_000_000)
     ap.add_argument("--frames", type=int, default=3, help="moving frames of the instanced leg")

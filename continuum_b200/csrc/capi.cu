@@ -463,12 +463,16 @@ int cc_scene_primary_hits(const cc_scene* s, const float camera[10], uint32_t wi
   return CC_OK;
 }
 
-int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
-                  const float* lights, uint32_t nlights, const cc_options* opt_in, const cc_outputs* out,
-                  void* stream_in) {
+}  // extern "C"
+
+// cc_visibility's body; `sky` (kSkyCones and its flags) makes the cones the
+// receivers' six sky faces (nlights = 6, no lights).
+static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                           const float* lights, uint32_t nlights, const cc_options* opt_in, const cc_outputs* out,
+                           void* stream_in, uint32_t sky) {
   if (!ctx || !scene || !out) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
-  if ((npoints && !receivers) || (nlights && !lights)) return fail(CC_ERR_INVALID, "null inputs");
+  if ((npoints && !receivers) || (nlights && !lights && !sky)) return fail(CC_ERR_INVALID, "null inputs");
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
@@ -488,6 +492,7 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
   q.wide_extent = opt.wide_extent;
   q.light_cone_cap = opt.light_cone_cap;
   q.wide_cone_cap = opt.wide_cone_cap;
+  q.sky = sky;
   cc::DevOut o{};
   if (device_ptrs) {
     // The kernels read and write these with vector accesses.
@@ -506,11 +511,15 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
     o.work = reinterpret_cast<uint4*>(out->work);
   } else {
     CC_CUDA(ctx->receivers.reserve(npoints * 32), "receivers buffer");
-    CC_CUDA(ctx->lights.reserve((size_t)nlights * 64), "lights buffer");
     CC_CUDA(cudaMemcpyAsync(ctx->receivers.ptr, receivers, npoints * 32, cudaMemcpyHostToDevice, stream), "receivers upload");
-    CC_CUDA(cudaMemcpyAsync(ctx->lights.ptr, lights, (size_t)nlights * 64, cudaMemcpyHostToDevice, stream), "lights upload");
     q.receivers = static_cast<const float4*>(ctx->receivers.ptr);
-    q.lights = static_cast<const float4*>(ctx->lights.ptr);
+    q.lights = nullptr;
+    if (!sky) {
+      CC_CUDA(ctx->lights.reserve((size_t)nlights * 64), "lights buffer");
+      CC_CUDA(cudaMemcpyAsync(ctx->lights.ptr, lights, (size_t)nlights * 64, cudaMemcpyHostToDevice, stream),
+              "lights upload");
+      q.lights = static_cast<const float4*>(ctx->lights.ptr);
+    }
     if (out->full) { CC_CUDA(ctx->full.reserve(ncones * 8), "output"); o.full = static_cast<uint2*>(ctx->full.ptr); }
     if (out->any) { CC_CUDA(ctx->any.reserve(ncones * 8), "output"); o.any = static_cast<uint2*>(ctx->any.ptr); }
     if (out->partial) { CC_CUDA(ctx->partial.reserve(ncones * 256), "output"); o.partial = static_cast<float*>(ctx->partial.ptr); }
@@ -564,6 +573,98 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
   uint32_t host_counters[2] = {0, 0};
   CC_CUDA(cudaMemcpyAsync(host_counters, counters, sizeof(host_counters), cudaMemcpyDeviceToHost, stream), "status download");
   CC_CUDA(cudaStreamSynchronize(stream), "visibility");
+  if (host_counters[1] & 2u) return fail(CC_ERR_STACK, "a traversal stack overflowed");
+  if (host_counters[1] & 1u) return fail(CC_ERR_INVALID, "solo re-walk list overflowed");
+  return CC_OK;
+}
+
+namespace {
+// sky_irradiance (:1411-1426): the six faces' light summed in face order.
+__global__ void sum_sky_faces(const float* __restrict__ faces, uint64_t npoints, float* __restrict__ out) {
+  const uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (p >= npoints) return;
+  float total = 0.0f;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) total += faces[f * npoints + p];
+  out[p] = total;
+}
+}  // namespace
+
+extern "C" {
+
+int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                  const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
+                  void* stream) {
+  return visibility_impl(ctx, scene, receivers, npoints, lights, nlights, opt, out, stream, 0u);
+}
+
+int cc_sky_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                      const cc_options* opt_in, uint32_t sky_flags, float* irradiance, const cc_outputs* faces,
+                      void* stream_in) {
+  if (!ctx || !scene || !irradiance) return fail(CC_ERR_INVALID, "null argument");
+  if (scene->ctx != ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
+  if (npoints && !receivers) return fail(CC_ERR_INVALID, "null inputs");
+  if (sky_flags & ~(CC_SKY_COMBINE_MAX | CC_SKY_NO_HORIZON_CULL)) return fail(CC_ERR_INVALID, "unknown sky flags");
+  if (npoints >= (0xffffffffull / 6)) return fail(CC_ERR_INVALID, "too many receivers in one call");
+  cc_options opt;
+  if (opt_in) opt = *opt_in; else cc_options_default(&opt);
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  cudaStream_t stream = stream_in ? (cudaStream_t)stream_in : ctx->stream;
+  const bool device_ptrs = (opt.flags & CC_DEVICE_POINTERS) != 0;
+  const uint64_t ncones = 6 * npoints;
+  uint32_t sky = cc::kSkyCones;
+  if (sky_flags & CC_SKY_COMBINE_MAX) sky |= cc::kSkyCombineMax;
+  if (sky_flags & CC_SKY_NO_HORIZON_CULL) sky |= cc::kSkyNoHorizonCull;
+  // The face cones run on device buffers: the caller's with device pointers,
+  // else the context's.
+  cc_outputs fo{};
+  if (device_ptrs && faces) fo = *faces;
+  const float* d_rec = receivers;
+  if (!device_ptrs) {
+    CC_CUDA(ctx->receivers.reserve(npoints * 32), "receivers buffer");
+    CC_CUDA(cudaMemcpyAsync(ctx->receivers.ptr, receivers, npoints * 32, cudaMemcpyHostToDevice, stream),
+            "receivers upload");
+    d_rec = static_cast<const float*>(ctx->receivers.ptr);
+    if (faces) {
+      if (faces->full) { CC_CUDA(ctx->full.reserve(ncones * 8), "output"); fo.full = static_cast<uint32_t*>(ctx->full.ptr); }
+      if (faces->any) { CC_CUDA(ctx->any.reserve(ncones * 8), "output"); fo.any = static_cast<uint32_t*>(ctx->any.ptr); }
+      if (faces->partial) { CC_CUDA(ctx->partial.reserve(ncones * 256), "output"); fo.partial = static_cast<float*>(ctx->partial.ptr); }
+      if (faces->fraction) { CC_CUDA(ctx->fraction.reserve(ncones * 4), "output"); fo.fraction = static_cast<float*>(ctx->fraction.ptr); }
+      if (faces->work) { CC_CUDA(ctx->work.reserve(ncones * 16), "output"); fo.work = static_cast<uint32_t*>(ctx->work.ptr); }
+    }
+  }
+  if (!fo.irradiance) {
+    CC_CUDA(ctx->irradiance.reserve(std::max<uint64_t>(ncones, 1) * 4), "sky faces");
+    fo.irradiance = static_cast<float*>(ctx->irradiance.ptr);
+  }
+  float* d_sum = irradiance;
+  if (!device_ptrs) {
+    CC_CUDA(ctx->sky_sum.reserve(std::max<uint64_t>(npoints, 1) * 4), "sky sum");
+    d_sum = static_cast<float*>(ctx->sky_sum.ptr);
+  }
+  cc_options vo = opt;
+  vo.flags |= CC_DEVICE_POINTERS;
+  rc = visibility_impl(ctx, scene, d_rec, npoints, nullptr, 6, &vo, &fo, stream, sky);
+  if (rc) return rc;
+  if (npoints) {
+    sum_sky_faces<<<(unsigned)((npoints + 255) / 256), 256, 0, stream>>>(fo.irradiance, npoints, d_sum);
+    CC_CUDA(cudaGetLastError(), "sky sum");
+  }
+  if (device_ptrs) return CC_OK;
+  CC_CUDA(cudaMemcpyAsync(irradiance, d_sum, npoints * 4, cudaMemcpyDeviceToHost, stream), "download");
+  if (faces) {
+    if (faces->irradiance) CC_CUDA(cudaMemcpyAsync(faces->irradiance, fo.irradiance, ncones * 4, cudaMemcpyDeviceToHost, stream), "download");
+    if (faces->full) CC_CUDA(cudaMemcpyAsync(faces->full, fo.full, ncones * 8, cudaMemcpyDeviceToHost, stream), "download");
+    if (faces->any) CC_CUDA(cudaMemcpyAsync(faces->any, fo.any, ncones * 8, cudaMemcpyDeviceToHost, stream), "download");
+    if (faces->partial) CC_CUDA(cudaMemcpyAsync(faces->partial, fo.partial, ncones * 256, cudaMemcpyDeviceToHost, stream), "download");
+    if (faces->fraction) CC_CUDA(cudaMemcpyAsync(faces->fraction, fo.fraction, ncones * 4, cudaMemcpyDeviceToHost, stream), "download");
+    if (faces->work) CC_CUDA(cudaMemcpyAsync(faces->work, fo.work, ncones * 16, cudaMemcpyDeviceToHost, stream), "download");
+  }
+  uint32_t host_counters[2] = {0, 0};
+  CC_CUDA(cudaMemcpyAsync(host_counters, ctx->counters.ptr, sizeof(host_counters), cudaMemcpyDeviceToHost, stream),
+          "status download");
+  CC_CUDA(cudaStreamSynchronize(stream), "sky visibility");
   if (host_counters[1] & 2u) return fail(CC_ERR_STACK, "a traversal stack overflowed");
   if (host_counters[1] & 1u) return fail(CC_ERR_INVALID, "solo re-walk list overflowed");
   return CC_OK;

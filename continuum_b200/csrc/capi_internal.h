@@ -55,6 +55,7 @@ struct cc_context {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   DevBuf receivers, lights, full, any, partial, irradiance, fraction, work;
+  DevBuf sky_sum;   // sky irradiance per receiver before its download
   DevBuf redo;      // redo list
   DevBuf order;     // walk order of the points
   DevBuf sort_scratch;

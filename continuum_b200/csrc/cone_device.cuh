@@ -246,13 +246,27 @@ __device__ __forceinline__ LightConeInfo light_cone(f3 apex, const DevLight& r, 
 }
 
 // ---- culling ---------------------------------------------------------------
+// rotate_to_object (:61-63): a direction in the space of the object placed by
+// transform X.
+__device__ __forceinline__ f3 rotate_to_object(f3 v, const float4* __restrict__ X) {
+  const float4 r0 = __ldg(X), r1 = __ldg(X + 1), r2 = __ldg(X + 2);
+  return mk(r0.x, r0.y, r0.z) * v.x + mk(r1.x, r1.y, r1.z) * v.y + mk(r2.x, r2.y, r2.z) * v.z;
+}
+
 // may_touch_box (:234-255), which is node_cone_test (:519-574) for exact cones.
-__device__ __forceinline__ bool may_touch_box(const Cone& c, f3 lo, f3 hi) {
-  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true;
+// kHorizon: sky cones, whose horizon `horizon` (the receiver's normal, in the
+// cone's space) also culls a box wholly below it (:245); a light cone's
+// horizon is zero (:146-147), which culls nothing, so light cones skip it.
+template <bool kHorizon = false>
+__device__ __forceinline__ bool may_touch_box(const Cone& c, f3 lo, f3 hi, f3 horizon = f3{0.f, 0.f, 0.f}) {
+  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true, below = kHorizon;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     f3 corner = mk((k & 1) ? hi.x : lo.x, (k & 2) ? hi.y : lo.y, (k & 4) ? hi.z : lo.z);
     if (c.far_offset - dot(c.fwd, corner) >= 0.0f) far_out = false;
+    if constexpr (kHorizon) {
+      if (dot(horizon, corner - c.apex) >= 0.0f) below = false;
+    }
     f3 p = to_local(c, corner);
     if (p.z >= kNear) near_out = false;
     if (p.x - c.u0 * p.z >= 0.0f) out_u0 = false;
@@ -260,16 +274,21 @@ __device__ __forceinline__ bool may_touch_box(const Cone& c, f3 lo, f3 hi) {
     if (p.y - c.v0 * p.z >= 0.0f) out_v0 = false;
     if (c.v1 * p.z - p.y >= 0.0f) out_v1 = false;
   }
-  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1) return false;
+  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1 || below) return false;
   return in_bound(c, (lo + hi) * 0.5f, 0.5f * len(hi - lo));
 }
 
-// may_touch (:215-232)
-__device__ __forceinline__ bool may_touch(const Cone& c, f3 v0, f3 v1, f3 v2) {
+// may_touch (:215-232); kHorizon as in may_touch_box (:220-221).
+template <bool kHorizon = false>
+__device__ __forceinline__ bool may_touch(const Cone& c, f3 v0, f3 v1, f3 v2, f3 horizon = f3{0.f, 0.f, 0.f}) {
   float f0 = c.far_offset - dot(c.fwd, v0);
   float f1 = c.far_offset - dot(c.fwd, v1);
   float f2 = c.far_offset - dot(c.fwd, v2);
   if (f0 < 0.0f && f1 < 0.0f && f2 < 0.0f) return false;
+  if constexpr (kHorizon) {
+    if (dot(horizon, v0 - c.apex) < 0.0f && dot(horizon, v1 - c.apex) < 0.0f && dot(horizon, v2 - c.apex) < 0.0f)
+      return false;
+  }
   f3 p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
   if (p0.z < kNear && p1.z < kNear && p2.z < kNear) return false;
   if (p0.x - c.u0 * p0.z < 0.0f && p1.x - c.u0 * p1.z < 0.0f && p2.x - c.u0 * p2.z < 0.0f) return false;
@@ -651,6 +670,45 @@ __device__ __forceinline__ float window_weight(const Cone& c, f3 n, bool* all_ab
     return fabsf(0.5f * (lambert_edge(n, d00, d10) + lambert_edge(n, d10, d11) + lambert_edge(n, d11, d01) +
                          lambert_edge(n, d01, d00)));
   return clipped_quad_weight(n, d00, d10, d11, d01);
+}
+
+// ---- sky cones (:1323-1511) --------------------------------------------------------
+// Far enough that every scene lies inside a sky cone (SKY_FAR, :1326).
+constexpr float kSkyFar = 1e7f;
+
+// clipped_window_weight (:1375-1403): the window's quad of directions clipped
+// to the horizon of `n`, Lambert-integrated.
+__device__ __forceinline__ float clipped_window_weight(const Cone& c, f3 n) {
+  return clipped_quad_weight(n, direction(c, 0.f, 0.f), direction(c, 1.f, 0.f), direction(c, 1.f, 1.f),
+                             direction(c, 0.f, 1.f));
+}
+
+// sky_face (:1444-1478) in world axes: cube face f (axis f / 2, negative for
+// odd f) around `apex`, reaching kSkyFar past it (its horizon, the
+// receiver's normal or zero, is the caller's). Returns whether any of its
+// directions lies above the horizon of `normal`.
+__device__ __forceinline__ bool sky_face(uint32_t f, f3 apex, f3 normal, Cone& c) {
+  const uint32_t axis = f / 2u;
+  const float sign = (f & 1u) ? -1.0f : 1.0f;
+  f3 forward = mk(0.f, 0.f, 0.f), right = mk(0.f, 0.f, 0.f);
+  if (axis == 0u) forward.x = sign; else if (axis == 1u) forward.y = sign; else forward.z = sign;
+  const uint32_t r = (axis + 1u) % 3u;
+  if (r == 0u) right.x = 1.0f; else if (r == 1u) right.y = 1.0f; else right.z = 1.0f;
+  c.apex = apex;
+  c.right = right;
+  c.up = cross(forward, right);
+  c.fwd = forward;
+  c.u0 = -1.0f;
+  c.v0 = -1.0f;
+  c.u1 = 1.0f;
+  c.v1 = 1.0f;
+  c.far_offset = dot(forward, apex) + kSkyFar;
+  bound_cone(c, forward);
+  bool above = false;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (dot(normal, direction(c, float(k & 1), float(k >> 1))) > 0.0f) above = true;
+  return above;
 }
 
 // ---- lights: gating and the unshadowed denominator -------------------------------

@@ -26,7 +26,13 @@ struct DevQuery {
   // The walk order of the points (a permutation; null: as given). Slot s
   // walks cone (s / npoints) * npoints + order[s % npoints].
   const uint32_t* order;
+  // kSkyCones: the query's cones are sky cones, the six cube faces around
+  // each receiver (nlights = 6, lights unused), with the flags below.
+  uint32_t sky = 0;
 };
+constexpr uint32_t kSkyCones = 1u;
+constexpr uint32_t kSkyCombineMax = 2u;      // combine meshes by the maximum, as light cones do (a diagnostic)
+constexpr uint32_t kSkyNoHorizonCull = 4u;   // walk geometry below the receiver's horizon too
 
 // Scratch bytes walk_order needs for `npoints` receivers.
 size_t walk_order_scratch_bytes(uint64_t npoints);

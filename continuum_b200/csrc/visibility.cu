@@ -49,10 +49,12 @@ __device__ __forceinline__ uint32_t general_len(uint32_t q) { return q >> 8; }
 __device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) { return fast | (general << 8); }
 
 // Shared memory of one warp; Cell is the accumulator's cell: 32 bits in the
-// packet pass, 64 in the solo pass.
-template <class CellT>
+// packet pass, 64 in the solo pass. Sky: the warp walks sky cones, whose
+// horizons are kept beside their frames.
+template <class CellT, bool Sky>
 struct WarpShared {
   using Cell = CellT;
+  static constexpr bool kSky = Sky;
   float cov[kBins * 32];                // each cone's 64 coverages, bin-major, lane innermost
   Cell acc[kBins * 32];                 // each cone's accumulator (fixed point, units of kFixUnit)
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
@@ -60,11 +62,15 @@ struct WarpShared {
   uint32_t queue[kQueueCap];            // (cone, triangle) pairs that passed the cull, waiting to be rasterized
   uint32_t general[kQueueCap];          // pairs that need rasterize's general path, waiting for it
   uint32_t overflow[4];                 // word 0: cones whose 32-bit accumulation overflowed in the current mesh
+  float horizon[Sky ? 3 * 32 : 4];      // sky cones: each cone's horizon, field-major
 };
-static_assert(sizeof(WarpShared<unsigned int>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-static_assert(sizeof(WarpShared<unsigned long long>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-using NarrowShared = WarpShared<unsigned int>;
-using WideShared = WarpShared<unsigned long long>;
+static_assert(sizeof(WarpShared<unsigned int, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned long long, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned int, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+template <bool kSky>
+using NarrowShared = WarpShared<unsigned int, kSky>;
+template <bool kSky>
+using WideShared = WarpShared<unsigned long long, kSky>;
 // Resident blocks per SM the shared memory allows: 5 x 38 KB with 32-bit
 // cells, 4 x 55 KB with 64-bit ones.
 template <class WS>
@@ -131,6 +137,9 @@ struct LaneState {
   uint32_t cap;
   uint32_t status;
   uint32_t n_obj, n_blas, n_tris;
+  bool independent;  // sky cones: meshes combine as independent occluders (else by the maximum)
+  f3 horizon;        // sky cones: the horizon in the space of the object being walked (the world's elsewhere)
+  f3 world_horizon;  // sky cones in instanced scenes: the horizon in world space
 };
 
 __device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
@@ -143,6 +152,16 @@ __device__ __forceinline__ void store_cone(WS* ws, const Cone& c, int lane) {
                                 c.far_offset};
 #pragma unroll
   for (int k = 0; k < kConeFields; ++k) t[32 * k] = f[k];
+}
+
+// Sky cones: the lane's horizon beside its cone (the cull reads both).
+template <class WS>
+__device__ __forceinline__ void store_horizon(WS* ws, f3 h, int lane) {
+  if constexpr (WS::kSky) {
+    ws->horizon[lane] = h.x;
+    ws->horizon[32 + lane] = h.y;
+    ws->horizon[64 + lane] = h.z;
+  }
 }
 
 template <class WS>
@@ -177,7 +196,10 @@ __device__ __forceinline__ bool pair_survives(const DevScene& s, const WS* ws, i
   if (dot(n, direction(c, 0.f, 0.f)) >= 0.f && dot(n, direction(c, 1.f, 0.f)) >= 0.f &&
       dot(n, direction(c, 0.f, 1.f)) >= 0.f && dot(n, direction(c, 1.f, 1.f)) >= 0.f)
     return false;  // every window direction leaves its plane (:601-606)
-  return may_touch(c, v0, v1, v2);
+  if constexpr (WS::kSky)
+    return may_touch<true>(c, v0, v1, v2, mk(ws->horizon[owner], ws->horizon[32 + owner], ws->horizon[64 + owner]));
+  else
+    return may_touch(c, v0, v1, v2);
 }
 
 template <class WS>
@@ -282,7 +304,9 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t 
 
 // The mesh's coverage for the lane's own cone: running sum over the touched
 // cells (exact), snapped to whole within 1e-5, combined into the cone's bins
-// by max (:809-828); then the cells are cleared for the next mesh.
+// by max (:809-828), or for sky cones as independent occluders
+// (1 - (1 - before)(1 - covered), :819-821); then the cells are cleared for
+// the next mesh.
 template <class WS>
 __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState<WS>& st, int lane) {
   WS* ws = st.ws;
@@ -310,7 +334,13 @@ __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState<WS>& s
     if (covered >= 1.0f - 1e-5f) covered = 1.0f;
     if (covered > 1e-6f) {
       const float before = st.cov[32 * b];
-      const float after = fmaxf(before, fminf(covered, 1.0f));
+      float after;
+      if constexpr (WS::kSky) {
+        after = st.independent ? 1.0f - (1.0f - before) * (1.0f - fminf(covered, 1.0f))
+                               : fmaxf(before, fminf(covered, 1.0f));
+      } else {
+        after = fmaxf(before, fminf(covered, 1.0f));
+      }
       st.cov[32 * b] = after;
       if (before < 1.0f && after >= 1.0f) st.full++;
     }
@@ -338,6 +368,10 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& 
   if (placed) {
     st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);  // cone_to_object (:623-638)
     store_cone(st.ws, st.cone, lane);
+    if constexpr (WS::kSky) {
+      st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
+      store_horizon(st.ws, st.horizon, lane);
+    }
     __syncwarp();
   }
   if (kCount && on) st.n_tris += range.y;
@@ -347,6 +381,10 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& 
   if (placed) {
     st.cone = st.world;
     store_cone(st.ws, st.cone, lane);
+    if constexpr (WS::kSky) {
+      st.horizon = st.world_horizon;
+      store_horizon(st.ws, st.horizon, lane);
+    }
     __syncwarp();
   }
 }
@@ -374,7 +412,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
   WarpStack stk;
   const float4 ra = __ldg(&s.nodes[0]);
   const float4 rb = __ldg(&s.nodes[1]);
-  const bool root_pass = traced && may_touch_box(c, node_lo(ra), node_lo(rb));
+  const bool root_pass = traced && may_touch_box<WS::kSky>(c, node_lo(ra), node_lo(rb), st.horizon);
   stk.push(0, node_ref(ra, rb, kObjNode), traced, root_pass, lane);
   int sp = 1;
   while (sp > 0) {
@@ -386,6 +424,10 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       if (kInst && ref_index(ref) == 1) {  // back to world space
         st.cone = st.world;
         store_cone(st.ws, st.cone, lane);
+        if constexpr (WS::kSky) {
+          st.horizon = st.world_horizon;
+          store_horizon(st.ws, st.horizon, lane);
+        }
         __syncwarp();
       }
       continue;
@@ -396,6 +438,11 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       const uint4 range = __ldg(&s.meshes[ref_index(ref)]);
       st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
       store_cone(st.ws, st.cone, lane);
+      if constexpr (WS::kSky) {
+        // The horizon turns with the cone (:634).
+        st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
+        store_horizon(st.ws, st.horizon, lane);
+      }
       __syncwarp();
       ref = node_ref(__ldg(&s.blas[2 * (size_t)range.z + 0]), __ldg(&s.blas[2 * (size_t)range.z + 1]), kTriNode);
       kind = kTriNode;
@@ -438,11 +485,13 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
           // A placed object: its root's box in its own space; the entry names
           // the object, whose cone is set up when the entry is popped.
           const Cone oc = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
-          const bool mesh_pass = descend && may_touch_box(oc, node_lo(ma), node_lo(mb));
+          f3 oh = st.horizon;
+          if constexpr (WS::kSky) oh = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
+          const bool mesh_pass = descend && may_touch_box<WS::kSky>(oc, node_lo(ma), node_lo(mb), oh);
           stk.push(sp, (kResolve << kRefKindShift) | 1u, false, false, lane);
           stk.push(sp + 1, (kObjRoot << kRefKindShift) | m, descend, mesh_pass, lane);
         } else {
-          const bool mesh_pass = descend && may_touch_box(c, node_lo(ma), node_lo(mb));
+          const bool mesh_pass = descend && may_touch_box<WS::kSky>(c, node_lo(ma), node_lo(mb), st.horizon);
           stk.push(sp, kResolve << kRefKindShift, false, false, lane);
           stk.push(sp + 1, node_ref(ma, mb, kTriNode), descend, mesh_pass, lane);
         }
@@ -456,7 +505,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       if (descend) {
 #pragma unroll 1
         for (int ch = 0; ch < 2; ++ch) {
-          const bool t = may_touch_box(c, node_lo(ch ? xa : la), node_lo(ch ? xb : lb));
+          const bool t = may_touch_box<WS::kSky>(c, node_lo(ch ? xa : la), node_lo(ch ? xb : lb), st.horizon);
           if (ch) pr = t; else pl = t;
         }
       }
@@ -575,13 +624,15 @@ __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, ui
 // kInst: the scene's objects place shared geometry with transforms.
 // kWide: 64-bit accumulator cells (the solo pass); else 32-bit ones (the
 // packet pass), whose overflowed cones the solo pass walks again.
-template <bool kCount, bool kBatch, bool kInst, bool kWide>
+// kSky: sky cones, the six cube faces around each receiver in place of its
+// lights (cone c = face * npoints + point).
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky>
 // The blocks the shared memory fits per SM; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm : kBlocksPerSm)
     visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
                       const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
-  using WS = typename std::conditional<kWide, WideShared, NarrowShared>::type;
+  using WS = typename std::conditional<kWide, WideShared<kSky>, NarrowShared<kSky>>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -659,23 +710,39 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     st.cone_work = 0;
     st.status = 0;
     st.n_obj = st.n_blas = st.n_tris = 0;
+    st.independent = false;
+    st.horizon = st.world_horizon = mk(0.f, 0.f, 0.f);
     for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 0.0f;
 
-    const DevLight L = load_light(q.lights, valid ? l : 0);
     const float4 pt4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 0]);
     const float4 nm4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 1]);
     const f3 point = xyz(pt4), normal = xyz(nm4);
-
-    // hit_irradiance_rect (:2125-2128): spot falloff and the facing test gate
-    // the cone.
-    const float spot = spot_falloff(L, normalize(point - light_center(L)));
-    const bool on = valid && spot > 0.0f && faces_light(L, point, normal);
     st.cone = Cone{};
-    const LightConeInfo info = light_cone(point, L, q.wide_extent, st.cone);
-    const bool traced = on && info.ok;
-    st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
+    DevLight L{};
+    float spot = 1.0f;
+    LightConeInfo info{true, false, false};
+    bool traced;
+    if constexpr (WS::kSky) {
+      // Sky face l of the receiver (sky_face, :1444-1478); walked without a
+      // cap (:1059, :1305).
+      traced = valid && sky_face(l, point, normal, st.cone);
+      st.cap = 0xffffffffu;
+      st.independent = (q.sky & kSkyCombineMax) == 0u;
+      st.horizon = (q.sky & kSkyNoHorizonCull) == 0u ? normal : mk(0.f, 0.f, 0.f);
+      st.world_horizon = st.horizon;
+    } else {
+      L = load_light(q.lights, valid ? l : 0);
+      // hit_irradiance_rect (:2125-2128): spot falloff and the facing test
+      // gate the cone.
+      spot = spot_falloff(L, normalize(point - light_center(L)));
+      const bool on = valid && spot > 0.0f && faces_light(L, point, normal);
+      info = light_cone(point, L, q.wide_extent, st.cone);
+      traced = on && info.ok;
+      st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
+    }
     if (kInst) st.world = st.cone;
     store_cone(ws, st.cone, lane);
+    store_horizon(ws, st.horizon, lane);
     __syncwarp();
 
     scene_walk<kCount, kInst>(s, q.hierarchy, st, traced, lane);
@@ -699,6 +766,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     const bool last_empty = (aw0 | aw1) == 0u;
     const bool last_full = (fw0 & fw1) == 0xffffffffu;
 
+    float value = 0.0f, ratio = 1.0f;
+    if constexpr (WS::kSky) {
+      // sky_face_light (:1489-1498): the face's window clipped to the
+      // horizon, less its covered bins' clipped weights.
+      if (traced) {
+        float blocked = 0.0f;
+        for (int b = 0; b < kBins; ++b) {
+          const float cv = st.cov[32 * b];
+          if (cv > 0.0f) blocked += cv * clipped_bin_weight(st.cone, normal, b);
+        }
+        const float open = clipped_window_weight(st.cone, normal);
+        value = fmaxf(open - blocked, 0.0f);
+        ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
+      }
+    } else {
     // Rect light cones with coverage: the bins' Lambert weights, one cone at
     // a time across the warp (the cone table is free now: it is the scratch).
     const bool rect_traced = traced && !is_sphere(L);
@@ -713,7 +795,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
       const float b = warp_blocked(st.cone, normal, all_above, ws->cov + j, ws->cone, j, lane);
       if (lane == j) blocked = b;
     }
-    float value = 0.0f;
     if (traced) {
       const Cone& cn = st.cone;
       if (is_sphere(L)) {
@@ -741,9 +822,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     value *= spot;
     // The lighting cache's ratio (vc_bake :3453-3510, static light).
     const float open = unshadowed(point, normal, L);
-    float ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
+    ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
     if (open > 0.0f && last_empty) ratio = 1.0f;
     if (open > 0.0f && last_full) ratio = 0.0f;
+    }
 
     // A walk again keeps the reasons its packet pass listed the cone for.
     if (valid && list && out_work) st.status |= out_work[c].w & (4u | kStatusAccOverflow);
@@ -783,25 +865,39 @@ cudaError_t upload_disk_table(const float* table64) {
 
 // Whether the large dynamic shared memory size was allowed, per device and
 // kernel variant (the attribute is set per device).
-static uint64_t g_attr_set[16] = {};
+static uint64_t g_attr_set[32] = {};
 
-template <bool kCount, bool kBatch, bool kInst, bool kWide>
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * (kWide ? sizeof(WideShared) : sizeof(NarrowShared));
+  const size_t smem = (size_t)kWarpsPerBlock * (kWide ? sizeof(WideShared<kSky>) : sizeof(NarrowShared<kSky>));
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
-  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0);
+  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0) + (kSky ? 16 : 0);
   if (!(g_attr_set[variant] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide>,
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide, kSky>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     g_attr_set[variant] |= bit;
   }
-  visibility_kernel<kCount, kBatch, kInst, kWide><<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
+  visibility_kernel<kCount, kBatch, kInst, kWide, kSky>
+      <<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
   return cudaGetLastError();
+}
+
+// A plain (not batched) pass of the variant the flags pick.
+template <bool kWide, bool kSky>
+static cudaError_t plain_pass(bool count, bool inst, const DevScene& s, const DevQuery& q, const DevOut& o,
+                              const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
+                              cudaStream_t stream) {
+  const BatchLaunch none{};
+  if (inst)
+    return count ? launch_one<true, false, true, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream)
+                 : launch_one<false, false, true, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream);
+  return count ? launch_one<true, false, false, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream)
+               : launch_one<false, false, false, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream);
 }
 
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t pw, bool count,
@@ -822,22 +918,16 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   // One resident wave: warps take packets from the shared counter.
   const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-  const BatchLaunch none{};
   const bool inst = s.xforms != nullptr;
+  const bool sky = (q.sky & kSkyCones) != 0u;
   // The packet pass with 32-bit accumulator cells, the solo pass with 64-bit.
   auto packets_pass = [&](uint32_t p, uint32_t nb) {
-    if (inst)
-      return count ? launch_one<true, false, true, false>(s, q, o, none, nullptr, nullptr, p, nb, stream)
-                   : launch_one<false, false, true, false>(s, q, o, none, nullptr, nullptr, p, nb, stream);
-    return count ? launch_one<true, false, false, false>(s, q, o, none, nullptr, nullptr, p, nb, stream)
-                 : launch_one<false, false, false, false>(s, q, o, none, nullptr, nullptr, p, nb, stream);
+    return sky ? plain_pass<false, true>(count, inst, s, q, o, nullptr, nullptr, p, nb, stream)
+               : plain_pass<false, false>(count, inst, s, q, o, nullptr, nullptr, p, nb, stream);
   };
   auto solo_pass = [&](uint32_t nb) {
-    if (inst)
-      return count ? launch_one<true, false, true, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream)
-                   : launch_one<false, false, true, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream);
-    return count ? launch_one<true, false, false, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream)
-                 : launch_one<false, false, false, true>(s, q, o, none, o.redo_list, o.redo_count, 1, nb, stream);
+    return sky ? plain_pass<true, true>(count, inst, s, q, o, o.redo_list, o.redo_count, 1, nb, stream)
+               : plain_pass<true, false>(count, inst, s, q, o, o.redo_list, o.redo_count, 1, nb, stream);
   };
   cudaError_t e = packets_pass(pw, blocks);
   if (marks) cudaEventRecord(marks[1], stream);

@@ -457,6 +457,41 @@ class MaskConeKernel:
                                    C.c_void_p(d_lights), int(nlights), C.byref(opt), C.byref(o),
                                    C.c_void_p(stream) if stream else None))
 
+    def sky_visibility(self, scene: Scene, receivers, hierarchy=Hierarchy.TRIANGLES, sky_flags: int = 0,
+                       outputs: Sequence[str] = (), points_per_warp: Optional[int] = None, flags: int = 0):
+        """Sky cones (cc_sky_visibility): the irradiance per unit uniform sky
+        radiance per receiver, and with `outputs` the six face cones' results
+        [6, P] (face-major) in a Visibility."""
+        rec = receivers_gpu(receivers)
+        P = rec.shape[0]
+        irr = np.zeros(P, np.float32)
+        faces = Visibility()
+        bufs = {}
+        shapes = {"full": ((6, P), np.uint64), "any": ((6, P), np.uint64), "partial": ((6, P, 64), np.float32),
+                  "irradiance": ((6, P), np.float32), "fraction": ((6, P), np.float32), "work": ((6, P, 4), np.uint32)}
+        for k in outputs:
+            shape, dt = shapes[k]
+            bufs[k] = np.zeros(shape, dt)
+        o = _lib.Outputs(*(ptr(bufs.get(k)) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.options(hierarchy, flags, points_per_warp)
+        check(load().cc_sky_visibility(self.handle, scene.handle, ptr(rec), P, C.byref(opt), int(sky_flags), ptr(irr),
+                                       C.byref(o) if bufs else None, None))
+        for k, v in bufs.items():
+            setattr(faces, k, v)
+        return irr, faces
+
+    def sky_visibility_device(self, scene: Scene, d_receivers: int, npoints: int, d_irradiance: int,
+                              faces: Optional[dict] = None, stream: int = 0, hierarchy=Hierarchy.TRIANGLES,
+                              sky_flags: int = 0, points_per_warp: Optional[int] = None, flags: int = 0) -> None:
+        """The same with device pointers (ints), asynchronous on `stream`."""
+        o = None
+        if faces:
+            o = _lib.Outputs(*(faces.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.options(hierarchy, flags | _lib.CC_DEVICE_POINTERS, points_per_warp)
+        check(load().cc_sky_visibility(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints), C.byref(opt),
+                                       int(sky_flags), C.c_void_p(d_irradiance), C.byref(o) if o else None,
+                                       C.c_void_p(stream) if stream else None))
+
     def visibility_static(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int,
                           outputs: dict, stream: int = 0, hierarchy=Hierarchy.TRIANGLES,
                           points_per_warp: Optional[int] = None, flags: int = 0) -> None:

@@ -209,6 +209,26 @@ CC_API int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* re
                   const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                   void* stream);
 
+/* cc_sky_visibility flags */
+#define CC_SKY_COMBINE_MAX 1u      /* meshes combine by the maximum, as light cones do (MaskConeKernel::set_sky_combination_max) */
+#define CC_SKY_NO_HORIZON_CULL 2u  /* walk geometry below the receiver's horizon too (set_sky_horizon_cull(false)) */
+
+/* A uniform sky through six cube-face mask cones per receiver (the sky light
+ * of mask_cones.wgsl:1323-1511, sky_irradiance :1411-1426, for a uniform sky
+ * in world axes without prefiltering): `irradiance` receives per receiver the
+ * irradiance per unit sky radiance, Σ over faces of the face's window clipped
+ * to the receiver's horizon less its covered bins' clipped weights. Each face
+ * (axis f / 2, negative for odd f) is a cone with a [-1, 1]^2 window reaching
+ * 1e7 past the receiver, walked without a cap; meshes combine as independent
+ * occluders, and geometry wholly below the receiver's tangent plane is
+ * skipped (both as the reference defaults). `faces` (nullable) receives the
+ * face cones' outputs as cc_visibility's, cone c = face * npoints + point.
+ * opt->flags: CC_DEVICE_POINTERS (receivers, irradiance and faces on the
+ * device; asynchronous), CC_NO_REDO, CC_KEEP_ORDER; the walk caps are unused. */
+CC_API int cc_sky_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                             const cc_options* opt, uint32_t sky_flags, float* irradiance, const cc_outputs* faces,
+                             void* stream);
+
 /* Recomputes the stale cones of a cache of results (device arrays, as
  * cc_visibility with CC_DEVICE_POINTERS writes them; full, any, irradiance
  * and fraction) and leaves every other cone's results as they are. receivers,

@@ -414,7 +414,7 @@ static void move_objects(Scene* s, const Instance* placements, float* boxes12) {
 // The light cone (mask_cones.wgsl:136-1042).
 // ---------------------------------------------------------------------------
 
-template <class R> struct Cone {  // mask_cones.wgsl:136-155 (horizon left out: zero)
+template <class R> struct Cone {  // mask_cones.wgsl:136-155
   V3<R> apex, right, up, forward;
   R window[4];  // u0, v0, u1, v1
   V3<R> far_normal;
@@ -422,6 +422,10 @@ template <class R> struct Cone {  // mask_cones.wgsl:136-155 (horizon left out: 
   V3<R> bound_axis;
   R bound_cos;
   R bound_sin;
+  // Geometry wholly below the plane through the apex with this normal is
+  // skipped: sky cones' receiver normal; zero (nothing skipped) for light
+  // cones (:146-147).
+  V3<R> horizon{R(0), R(0), R(0)};
 };
 
 template <class R> struct Light {  // LightRect (mask_cones.wgsl:843-848), LightGpu (lib.rs:710-749)
@@ -490,6 +494,8 @@ template <class R> bool may_touch(const Cone<R>& c, V3<R> v0, V3<R> v1, V3<R> v2
   R f1 = c.far_offset - dot(c.far_normal, v1);
   R f2 = c.far_offset - dot(c.far_normal, v2);
   if (f0 < 0 && f1 < 0 && f2 < 0) return false;
+  if (dot(c.horizon, v0 - c.apex) < 0 && dot(c.horizon, v1 - c.apex) < 0 && dot(c.horizon, v2 - c.apex) < 0)
+    return false;
   V3<R> p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
   const R NR = NEAR<R>;
   if (p0.z < NR && p1.z < NR && p2.z < NR) return false;
@@ -502,10 +508,11 @@ template <class R> bool may_touch(const Cone<R>& c, V3<R> v0, V3<R> v1, V3<R> v2
 }
 
 template <class R> bool may_touch_box(const Cone<R>& c, V3<R> lo, V3<R> hi) {  // :234-255
-  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true;
+  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true, below = true;
   for (uint32_t k = 0; k < 8; ++k) {
     V3<R> corner{(k & 1u) ? hi.x : lo.x, (k & 2u) ? hi.y : lo.y, (k & 4u) ? hi.z : lo.z};
     if (c.far_offset - dot(c.far_normal, corner) >= 0) far_out = false;
+    if (dot(c.horizon, corner - c.apex) >= 0) below = false;
     V3<R> p = to_local(c, corner);
     if (p.z >= NEAR<R>) near_out = false;
     if (p.x - c.window[0] * p.z >= 0) out_u0 = false;
@@ -513,7 +520,7 @@ template <class R> bool may_touch_box(const Cone<R>& c, V3<R> lo, V3<R> hi) {  /
     if (p.y - c.window[1] * p.z >= 0) out_v0 = false;
     if (c.window[3] * p.z - p.y >= 0) out_v1 = false;
   }
-  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1) return false;
+  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1 || below) return false;
   return in_bound(c, (lo + hi) * R(0.5), R(0.5) * length(hi - lo));
 }
 
@@ -735,6 +742,7 @@ template <class R> struct Walk {
   uint32_t full = 0;
   uint32_t cone_work = 0;
   uint32_t cone_cap = NONE;
+  bool independent = false;  // sky cones: meshes combine as independent occluders (:819-821)
   Work work;
 };
 
@@ -757,6 +765,7 @@ template <class R> Cone<R> cone_to_object(const Scene& s, const Cone<R>& c, uint
   o.far_normal = rot(c.far_normal);
   o.far_offset = (c.far_offset - dot(c.far_normal, t)) * inv_scale;
   o.bound_axis = rot(c.bound_axis);
+  o.horizon = rot(c.horizon);
   return o;
 }
 
@@ -806,7 +815,10 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
       if (covered >= R(1) - R(1e-5)) covered = 1;
       if (covered > R(1e-6)) {
         R before = wk.cov[b];
-        wk.cov[b] = std::max(before, std::min(covered, R(1)));
+        if (wk.independent)
+          wk.cov[b] = R(1) - (R(1) - before) * (R(1) - std::min(covered, R(1)));
+        else
+          wk.cov[b] = std::max(before, std::min(covered, R(1)));
         if (before < R(1) && wk.cov[b] >= R(1)) wk.full++;
       }
     }
@@ -1188,6 +1200,56 @@ template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> norma
   out.fraction = ratio;
   out.unshadowed = open;
   out.work = wk.work;
+}
+
+// Sky light (:1323-1511), a uniform sky in world axes without prefiltering.
+constexpr float SKY_FAR = 1e7f;  // :1326
+
+// sky_face (:1444-1478): cube face f around `apex`; returns whether any of its
+// window's corner directions lies above the horizon of `normal`.
+template <class R> bool sky_face(uint32_t f, V3<R> apex, V3<R> normal, bool horizon_cull, Cone<R>& c) {
+  const uint32_t axis = f / 2;
+  const R sign = (f & 1u) ? R(-1) : R(1);
+  R fw[3] = {0, 0, 0}, rt[3] = {0, 0, 0};
+  fw[axis] = sign;
+  rt[(axis + 1) % 3] = 1;
+  const V3<R> forward{fw[0], fw[1], fw[2]}, right{rt[0], rt[1], rt[2]};
+  c.apex = apex;
+  c.right = right;
+  c.up = cross(forward, right);
+  c.forward = forward;
+  c.window[0] = -1;
+  c.window[1] = -1;
+  c.window[2] = 1;
+  c.window[3] = 1;
+  c.far_normal = forward;
+  c.far_offset = dot(forward, apex) + R(SKY_FAR);
+  c.horizon = horizon_cull ? normal : V3<R>{0, 0, 0};
+  bound_cone(c, forward);
+  bool above = false;
+  for (uint32_t k = 0; k < 4; ++k)
+    if (dot(normal, direction(c, R(k & 1u), R(k >> 1))) > 0) above = true;
+  return above;
+}
+
+// sky_face_coverage and sky_face_light (:1482-1498) for face f: the face's
+// coverage (no walk cap; independent occluders unless `combine_max`) and its
+// light per unit sky radiance.
+template <class R> R sky_face_irradiance(const Scene& s, uint32_t f, V3<R> point, V3<R> normal, uint32_t hierarchy,
+                                         bool combine_max, bool horizon_cull, R* cov_out, Work* work) {
+  Cone<R> c;
+  const bool above = sky_face(f, point, normal, horizon_cull, c);
+  Walk<R> wk;
+  std::fill(wk.cov, wk.cov + BINS, R(0));
+  wk.independent = !combine_max;
+  if (above) scene_coverage(s, c, wk, hierarchy);
+  if (cov_out) std::copy(wk.cov, wk.cov + BINS, cov_out);
+  if (work) *work = wk.work;
+  if (!above) return 0;
+  R blocked = 0;
+  for (uint32_t b = 0; b < BINS; ++b)
+    if (wk.cov[b] > 0) blocked += wk.cov[b] * clipped_bin_weight(c, normal, b);
+  return std::max(clipped_window_weight(c, normal) - blocked, R(0));
 }
 
 // ---------------------------------------------------------------------------
@@ -1785,6 +1847,54 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
         work[4 * i + 2] = res.work.tris;
         work[4 * i + 3] = res.work.flags;
       }
+    });
+  };
+  if (precision == 8)
+    run(double(0));
+  else
+    run(float(0));
+  return 0;
+}
+
+// Sky irradiance per unit radiance per receiver (sky_irradiance, :1411-1426:
+// the six faces summed in order) and, nullable, per face cone c = face *
+// npoints + point: its light, FULL/ANY words, coverage and work counters.
+// flags: 1 combine by the maximum, 2 no horizon cull.
+int oracle_sky_visibility(void* sp, const float* receivers, uint64_t npoints, uint32_t hierarchy, uint32_t flags,
+                          int precision, float* irradiance, float* face_light, uint32_t* full, uint32_t* any,
+                          float* partial, uint32_t* work, int threads) {
+  Scene* s = static_cast<Scene*>(sp);
+  if (!s || !irradiance) return 1;
+  auto run = [&](auto zero) {
+    using R = decltype(zero);
+    parallel_for(npoints, threads, [&](uint64_t p) {
+      const float* rc = receivers + 8 * p;
+      const V3<R> point{R(rc[0]), R(rc[1]), R(rc[2])}, normal{R(rc[4]), R(rc[5]), R(rc[6])};
+      R total = 0;
+      for (uint32_t f = 0; f < 6; ++f) {
+        R cov[BINS];
+        Work wk;
+        const R v = sky_face_irradiance(*s, f, point, normal, hierarchy, (flags & 1u) != 0, (flags & 2u) == 0, cov, &wk);
+        total += v;
+        const uint64_t c = f * npoints + p;
+        if (face_light) face_light[c] = float(v);
+        uint32_t fw[2] = {0, 0}, aw[2] = {0, 0};
+        for (uint32_t b = 0; b < BINS; ++b) {
+          if (cov[b] >= R(1)) fw[b >> 5] |= 1u << (b & 31);
+          if (cov[b] > R(0)) aw[b >> 5] |= 1u << (b & 31);
+        }
+        if (full) { full[2 * c] = fw[0]; full[2 * c + 1] = fw[1]; }
+        if (any) { any[2 * c] = aw[0]; any[2 * c + 1] = aw[1]; }
+        if (partial)
+          for (uint32_t b = 0; b < BINS; ++b) partial[64 * c + b] = float(cov[b]);
+        if (work) {
+          work[4 * c + 0] = wk.object_nodes;
+          work[4 * c + 1] = wk.blas_nodes;
+          work[4 * c + 2] = wk.tris;
+          work[4 * c + 3] = wk.flags;
+        }
+      }
+      irradiance[p] = float(total);
     });
   };
   if (precision == 8)

@@ -36,6 +36,8 @@ def load():
         lib.oracle_scene_arrays.argtypes = [P, P, P, P, P, P]
         lib.oracle_visibility.restype = I
         lib.oracle_visibility.argtypes = [P, P, U64, P, U32, C.POINTER(_Params), P, U64, I, P, P, P, P, P, P, P, I]
+        lib.oracle_sky_visibility.restype = I
+        lib.oracle_sky_visibility.argtypes = [P, P, U64, U32, U32, I, P, P, P, P, P, P, I]
         lib.oracle_cpu_masked.restype = I
         lib.oracle_cpu_masked.argtypes = [P, P, U64, P, I, P, P, P, I]
         lib.oracle_disk_table.argtypes = [P]
@@ -150,6 +152,31 @@ class OracleScene:
             raise RuntimeError(f"oracle_visibility failed: {rc}")
         return dict(full=full.view(np.uint64).reshape(n), any=any_.view(np.uint64).reshape(n), partial=part,
                     irradiance=irr, fraction=frac, work=work, unshadowed=unsh)
+
+    def sky_visibility(self, receivers: np.ndarray, hierarchy: int = 2, flags: int = 0, precision: int = 4,
+                       threads: int | None = None, faces: bool = True) -> dict:
+        """Sky cones (six cube faces per receiver): irradiance per unit sky
+        radiance per receiver, and per face cone c = face * npoints + point its
+        light, FULL/ANY words, coverage and work counters. flags: 1 combine
+        meshes by the maximum, 2 walk geometry below the horizon too."""
+        rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
+        n = rec.shape[0]
+        irr = np.zeros(n, np.float32)
+        out = dict(irradiance=irr)
+        if faces:
+            out.update(face_light=np.zeros(6 * n, np.float32), full=np.zeros((6 * n, 2), np.uint32),
+                       any=np.zeros((6 * n, 2), np.uint32), partial=np.zeros((6 * n, 64), np.float32),
+                       work=np.zeros((6 * n, 4), np.uint32))
+        g = out.get
+        rc = load().oracle_sky_visibility(self._h, _p(rec), n, hierarchy, flags, precision, _p(irr), _p(g("face_light")),
+                                          _p(g("full")), _p(g("any")), _p(g("partial")), _p(g("work")),
+                                          threads or default_threads())
+        if rc != 0:
+            raise RuntimeError(f"oracle_sky_visibility failed: {rc}")
+        if faces:
+            out["full"] = out["full"].view(np.uint64).reshape(6 * n)
+            out["any"] = out["any"].view(np.uint64).reshape(6 * n)
+        return out
 
     def cpu_masked(self, receivers: np.ndarray, light9, use_bvh: bool = False, threads: int | None = None):
         """The reference CPU path (cone3 + coverage, Receiver::masked): (visible, total weight)."""
