@@ -510,13 +510,18 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
         }
       }
       bool swap = false;  // left child popped first (object level: when it is the nearer)
-      if (is_obj) {
+      // Nearest child first where meshes combine by the maximum; sky cones
+      // combining as independent occluders keep the left child first, as
+      // their products would round differently in another order (:1188-1207).
+      bool nearest = is_obj;
+      if constexpr (WS::kSky) nearest = nearest && !st.independent;
+      if (nearest) {
         const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
         const float db = dot(c.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - c.apex);
         const bool pref = db < da;  // this lane's own order: right child nearer
         swap = __shfl_sync(0xffffffffu, pref, __ffs(owners) - 1);
         if (descend && pref != swap) st.status |= 4u;
-      } else {
+      } else if (!is_obj) {
         swap = true;  // triangle hierarchies pop the right child first (:783-787)
       }
       if (sp + 2 > kStack) {

@@ -848,10 +848,14 @@ template <class R> void scene_coverage(const Scene& s, const Cone<R>& c, Walk<R>
         uint32_t near_ = node.info[0], far_ = node.info[0] + 1;
         const Node& a = s.nodes[near_];
         const Node& b = s.nodes[far_];
-        V3<R> axis = c.bound_axis;  // a light cone's bound is always set
-        R da = dot(axis, (node_lo<R>(a) + node_hi<R>(a)) * R(0.5) - c.apex);
-        R db = dot(axis, (node_lo<R>(b) + node_hi<R>(b)) * R(0.5) - c.apex);
-        if (db < da) std::swap(near_, far_);
+        // Nearest child first where meshes combine by the maximum; independent
+        // occluders (sky cones) keep the left child first (:1188-1207).
+        if (!wk.independent) {
+          V3<R> axis = c.bound_axis;  // a light cone's bound is always set
+          R da = dot(axis, (node_lo<R>(a) + node_hi<R>(a)) * R(0.5) - c.apex);
+          R db = dot(axis, (node_lo<R>(b) + node_hi<R>(b)) * R(0.5) - c.apex);
+          if (db < da) std::swap(near_, far_);
+        }
         if (sp + 2 > STACK) {
           wk.work.flags |= 2;
           continue;
