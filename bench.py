@@ -495,14 +495,15 @@ def bake_leg(args, kernel, scene, w) -> dict:
     return out
 
 
-def sky_leg(args, kernel, dev, stream, flush) -> dict:
+def sky_leg(args, kernel, dev, stream, flush, prefiltered_scene) -> dict:
     """Sky cones on the small plain workload (the ground and 64 boxes, 770
     triangles; its 256 x 256 receivers lifted 1e-4 off the ground): six
     cube-face cones per receiver (393,216 cones), the irradiance per unit
     uniform sky radiance per receiver, device-timed with CUDA events (L2
     flushed between steps). Exact sky cones reach 1e7 past each receiver over
-    a 90-degree face, so their cost grows with the whole scene in view (the
-    reference prefilters them, which this library does not build)."""
+    a 90-degree face, so their cost grows with the whole scene in view; the
+    reference prefilters them, as the second measurement does on the plain
+    workload at scale."""
     import torch
 
     from continuum_b200 import scenes
@@ -524,9 +525,31 @@ def sky_leg(args, kernel, dev, stream, flush) -> dict:
     ms = float(np.mean(timed_steps(torch, dev, stream, flush, step, 2, steps)))
     mean = float(out.mean().item())
     scene.close()
-    return {"workload": f"sky cones: 6 cube faces x {P} receivers of the small plain workload (770 triangles)",
-            "cones": 6 * P, "value": 6 * P / (ms * 1e-3), "unit": UNIT, "ms": ms, "steps": steps,
-            "mean_irradiance_per_unit_sky": mean, "timing": "CUDA events, L2 flushed"}
+    exact = {"workload": f"sky cones: 6 cube faces x {P} receivers of the small plain workload (770 triangles)",
+             "cones": 6 * P, "value": 6 * P / (ms * 1e-3), "unit": UNIT, "ms": ms, "steps": steps,
+             "mean_irradiance_per_unit_sky": mean, "timing": "CUDA events, L2 flushed"}
+    # Prefiltered (1 bin, the reference renderer's default) on the plain
+    # workload at scale: 6 faces x 921,600 primary hits over 3.07 M triangles.
+    big_scene, big = prefiltered_scene
+    P2 = big.receivers.shape[0]
+    rec2 = torch.from_numpy(big.receivers).to(dev)
+    out2 = torch.empty(P2, device=dev)
+    faces2 = torch.empty(6 * P2, device=dev)
+    kernel.prefilter = 1.0
+
+    def step2():
+        kernel.sky_visibility_device(big_scene, rec2.data_ptr(), P2, out2.data_ptr(),
+                                     faces={"irradiance": faces2.data_ptr()}, stream=stream.cuda_stream)
+
+    try:
+        ms2 = float(np.mean(timed_steps(torch, dev, stream, flush, step2, 1, steps)))
+    finally:
+        kernel.prefilter = 0.0
+    pre = {"workload": f"prefiltered sky cones (1 bin): 6 cube faces x {P2} primary hits of the plain workload at "
+                       "scale (3.07 M triangles)", "cones": 6 * P2, "value": 6 * P2 / (ms2 * 1e-3), "unit": UNIT,
+           "ms": ms2, "steps": steps, "mean_irradiance_per_unit_sky": float(out2.mean().item()),
+           "timing": "CUDA events, L2 flushed"}
+    return {"exact": exact, "prefiltered": pre}
 
 
 def reference_arm(args, rank: int) -> None:
@@ -706,7 +729,7 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
     if "bake" in forms:
         line["bake"] = bake_leg(args, kernel, scene, w)
     if "sky" in forms:
-        line["sky"] = sky_leg(args, kernel, dev, stream, flush)
+        line["sky"] = sky_leg(args, kernel, dev, stream, flush, (scene, w))
     if world == 1 and not args.no_cpu_baseline:
         rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",

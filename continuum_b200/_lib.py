@@ -34,6 +34,7 @@ CC_CONE_DIVERGED = 4
 CC_CONE_REWALKED = 8
 CC_CONE_FULL_STOP = 16
 CC_CONE_ACC_WIDE = 32
+CC_NO_OBJECT_PREFILTER = 8
 CC_SKY_COMBINE_MAX = 1
 CC_SKY_NO_HORIZON_CULL = 2
 
@@ -48,7 +49,7 @@ EXPORTS = (
     "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms", "cc_scene_move",
     "cc_stale_cones", "cc_visibility_update", "cc_cache_options_default", "cc_cache_create", "cc_cache_destroy",
     "cc_cache_frame", "cc_cache_read", "cc_cache_pool", "cc_cache_jobs", "cc_planner_create", "cc_planner_destroy",
-    "cc_planner_frame", "cc_planner_jobs", "cc_planner_slot", "cc_sky_visibility",
+    "cc_planner_frame", "cc_planner_jobs", "cc_planner_slot", "cc_sky_visibility", "cc_scene_coverage",
 )
 
 # cc_instance: an object placing a geometry (world = scale * rotation * p + translation).
@@ -79,6 +80,7 @@ class Options(C.Structure):
     _fields_ = [
         ("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
         ("wide_cone_cap", C.c_uint32), ("points_per_warp", C.c_uint32), ("flags", C.c_uint32),
+        ("prefilter", C.c_float),
     ]
 
 
@@ -190,6 +192,7 @@ def load() -> C.CDLL:
         "cc_planner_jobs": (C.c_int64, [P, P, U64, P, U32]),
         "cc_planner_slot": (C.c_int64, [P, P]),
         "cc_sky_visibility": (I, [P, P, P, U64, C.POINTER(Options), U32, P, C.POINTER(Outputs), P]),
+        "cc_scene_coverage": (C.c_int64, [P, P, U64, P, U64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -224,6 +224,7 @@ int cc_batch_add(cc_batch* b, const cc_scene* scene, const float* receivers, uin
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
+  if (opt.prefilter != 0.0f) return fail(CC_ERR_INVALID, "batched jobs take exact cones only (prefilter 0)");
   if (npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one job");
   const uint64_t cones = npoints * (uint64_t)nlights;
   if (b->cones + cones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one batch");

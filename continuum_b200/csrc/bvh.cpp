@@ -456,4 +456,112 @@ void move_instances(FlatScene& s, const Instance* placements, float* boxes12) {
   mover_subtree(s, mover_bounds);
 }
 
+// coverage_directions (hierarchy.rs:714-723): (i, j, k) normalized, the zero
+// direction kept zero (glam's normalize_or_zero: v times 1 / |v|).
+static void coverage_directions(float d[kCoverageSamples][3]) {
+  for (uint32_t n = 0; n < kCoverageSamples; ++n) {
+    const float v[3] = {float(n / 9) - 1.0f, float(n / 3 % 3) - 1.0f, float(n % 3) - 1.0f};
+    const float len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const float rcp = 1.0f / len;
+    const bool ok = std::isfinite(rcp) && rcp > 0.0f;
+    for (int k = 0; k < 3; ++k) d[n][k] = ok ? v[k] * rcp : 0.0f;
+  }
+}
+
+std::vector<float> blas_coverage(const FlatScene& s) {
+  float dirs[kCoverageSamples][3];
+  coverage_directions(dirs);
+  const size_t n = s.blas.size();
+  std::vector<float> cov(n * kCoverageSamples, 0.0f);
+  // Children always follow their parent: a reverse sweep sees them first.
+  for (size_t i = n; i-- > 0;) {
+    float* out = cov.data() + i * kCoverageSamples;
+    const uint32_t x = s.blas[i].info[0], count = s.blas[i].info[1];
+    if (count > 0) {
+      for (uint32_t k = x; k < x + count; ++k) {
+        const float* t = s.tris.data() + 12 * (size_t)s.blas_items[k];
+        const float e1[3] = {t[4] - t[0], t[5] - t[1], t[6] - t[2]};
+        const float e2[3] = {t[8] - t[0], t[9] - t[1], t[10] - t[2]};
+        const float an[3] = {(e1[1] * e2[2] - e2[1] * e1[2]) * 0.5f, (e1[2] * e2[0] - e2[2] * e1[0]) * 0.5f,
+                             (e1[0] * e2[1] - e2[0] * e1[1]) * 0.5f};
+        for (uint32_t d = 0; d < kCoverageSamples; ++d)
+          out[d] += std::max(an[0] * dirs[d][0] + an[1] * dirs[d][1] + an[2] * dirs[d][2], 0.0f);
+      }
+    } else {
+      const float* a = cov.data() + (size_t)x * kCoverageSamples;
+      const float* b = a + kCoverageSamples;
+      for (uint32_t d = 0; d < kCoverageSamples; ++d) out[d] = a[d] + b[d];
+    }
+  }
+  return cov;
+}
+
+// front_area (hierarchy.rs:625-652): a node's coverage seen along v,
+// bilinear on the face of the cube of sample directions v points through.
+static float front_area(const float* cov, const float v[3]) {
+  const float a[3] = {std::fabs(v[0]), std::fabs(v[1]), std::fabs(v[2])};
+  int axis = 0;
+  if (a[1] > a[0] && a[1] >= a[2]) axis = 1;
+  else if (a[2] > a[0] && a[2] > a[1]) axis = 2;
+  float main, s, t;
+  if (axis == 0) main = v[0], s = v[1] / a[0], t = v[2] / a[0];
+  else if (axis == 1) main = v[1], s = v[0] / a[1], t = v[2] / a[1];
+  else main = v[2], s = v[0] / a[2], t = v[1] / a[2];
+  const int m = main >= 0.0f ? 1 : -1;
+  const int s0 = s < 0.0f ? -1 : 0, t0 = t < 0.0f ? -1 : 0;
+  const float fs = s - float(s0), ft = t - float(t0);
+  auto sample = [&](int i, int j, int k) { return cov[9 * (i + 1) + 3 * (j + 1) + (k + 1)]; };
+  float f[4];
+  for (int c = 0; c < 4; ++c) {
+    const int gs = s0 + (c & 1), gt = t0 + (c >> 1);
+    f[c] = axis == 0 ? sample(m, gs, gt) : axis == 1 ? sample(gs, m, gt) : sample(gs, gt, m);
+  }
+  auto lerp = [](float x, float y, float u) { return x + (y - x) * u; };
+  return lerp(lerp(f[0], f[1], fs), lerp(f[2], f[3], fs), ft);
+}
+
+std::vector<float> object_coverage(const FlatScene& s, const std::vector<float>& blas_cov) {
+  float dirs[kCoverageSamples][3];
+  coverage_directions(dirs);
+  const uint32_t nobj = s.nmeshes;
+  std::vector<float> per_object((size_t)nobj * kCoverageSamples, 0.0f);
+  for (uint32_t m = 0; m < nobj; ++m) {
+    const uint32_t root = s.ranges[4 * m + 2];
+    const uint32_t x = s.ranges[4 * m + 3];
+    if (root == kNone || x == kNone) continue;
+    const float* cov = blas_cov.data() + (size_t)root * kCoverageSamples;
+    const float* X = s.xforms.data() + 16 * (size_t)x;
+    const float scale = X[12];
+    float* out = per_object.data() + (size_t)m * kCoverageSamples;
+    for (uint32_t n = 0; n < kCoverageSamples; ++n) {
+      const float* d = dirs[n];
+      if (d[0] == 0.0f && d[1] == 0.0f && d[2] == 0.0f) continue;
+      // The direction turned into the object: the rotation's transpose (its
+      // rows as columns) times d.
+      const float v[3] = {X[0] * d[0] + X[4] * d[1] + X[8] * d[2], X[1] * d[0] + X[5] * d[1] + X[9] * d[2],
+                          X[2] * d[0] + X[6] * d[1] + X[10] * d[2]};
+      out[n] = scale * scale * front_area(cov, v);
+    }
+  }
+  const size_t nn = s.nodes.size();
+  std::vector<float> cov(nn * kCoverageSamples, 0.0f);
+  for (size_t i = nn; i-- > 0;) {
+    float* out = cov.data() + i * kCoverageSamples;
+    const uint32_t x = s.nodes[i].info[0], count = s.nodes[i].info[1];
+    if (count > 0) {
+      for (uint32_t k = x; k < x + count; ++k) {
+        const float* po = per_object.data() + (size_t)s.items[k] * kCoverageSamples;
+        for (uint32_t d = 0; d < kCoverageSamples; ++d) out[d] += po[d];
+      }
+    } else {
+      const float* a = cov.data() + (size_t)x * kCoverageSamples;
+      const float* b = a + kCoverageSamples;
+      for (uint32_t d = 0; d < kCoverageSamples; ++d) out[d] = a[d] + b[d];
+    }
+  }
+  for (size_t i = 0; i < nn; ++i)
+    if (s.nodes[i].info[2] == kNoSplat) cov[i * kCoverageSamples + 13] = 1.0f;
+  return cov;
+}
+
 }  // namespace cc

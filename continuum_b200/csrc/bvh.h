@@ -81,6 +81,22 @@ void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, u
 // bounds before and after (lo.xyz, hi.xyz each).
 void move_instances(FlatScene& s, const Instance* placements, float* boxes12);
 
+// Coverage samples per hierarchy node for prefiltered cones
+// (COVERAGE_SAMPLES, hierarchy.rs:710-723): the projected front area of the
+// node's triangles from the 26 directions (i, j, k) in {-1, 0, 1}^3 \ 0
+// (normalized), at index 9(i+1) + 3(j+1) + (k+1); index 13 is unused.
+constexpr uint32_t kCoverageSamples = 27;
+// triangle_hierarchy's coverage (hierarchy.rs:546-569), for every node of
+// every mesh's triangle hierarchy: a leaf sums its triangles' max(0,
+// area-normal . d), an interior node its children's.
+std::vector<float> blas_coverage(const FlatScene& s);
+// object_coverage (hierarchy.rs:661-707) for an instanced scene: per object
+// node, its objects' projected front areas, each its geometry root's
+// coverage seen along the direction turned into the object, times scale^2.
+// Sample 13 of a node without prefiltered coverage (NO_SPLAT: the root over
+// movers and the movers' subtree) is set to 1 as its flag.
+std::vector<float> object_coverage(const FlatScene& s, const std::vector<float>& blas_cov);
+
 // Primary hits of a pinhole camera (raycast.cpp).
 void primary_hits(const FlatScene& s, const float* camera, uint32_t width, uint32_t height, float* out8,
                   uint8_t* hit_mask, int threads);

@@ -89,6 +89,11 @@ void free_scene_device(cc_scene* s) {
   cudaFree(s->items);
   cudaFree(s->blas);
   cudaFree(s->xforms);
+  cudaFree(s->blas_cov);
+  cudaFree(s->obj_cov);
+  s->blas_cov = nullptr;
+  s->obj_cov = nullptr;
+  s->coverage_ready = false;
   s->xforms = nullptr;
   s->tris = nullptr;
   s->meshes = nullptr;
@@ -129,6 +134,22 @@ int upload_scene(cc_scene* s) {
       x[i] = make_float4(f.xforms[4 * i], f.xforms[4 * i + 1], f.xforms[4 * i + 2], f.xforms[4 * i + 3]);
     if ((rc = upload(x, &s->xforms, s->bytes, "scene transforms"))) return rc;
   }
+  return CC_OK;
+}
+
+// The prefiltered cones' coverage samples of every triangle-hierarchy node
+// and, for instanced scenes, every object-hierarchy node (built on the host
+// from the scene's own arrays as the reference builds them, then uploaded).
+int ensure_coverage(cc_scene* s) {
+  if (s->coverage_ready) return CC_OK;
+  const std::vector<float> blas = cc::blas_coverage(s->flat);
+  int rc;
+  if (!blas.empty() && (rc = upload(blas, &s->blas_cov, s->bytes, "triangle-node coverage"))) return rc;
+  if (!s->flat.xforms.empty()) {
+    const std::vector<float> obj = cc::object_coverage(s->flat, blas);
+    if (!obj.empty() && (rc = upload(obj, &s->obj_cov, s->bytes, "object-node coverage"))) return rc;
+  }
+  s->coverage_ready = true;
   return CC_OK;
 }
 
@@ -209,6 +230,7 @@ void cc_options_default(cc_options* opt) {
   opt->wide_cone_cap = 512;
   opt->points_per_warp = 32;
   opt->flags = 0;
+  opt->prefilter = 0.0f;
 }
 
 int cc_context_create(int device, cc_context** out) {
@@ -477,6 +499,8 @@ static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* 
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
   if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
+  if (!(opt.prefilter >= 0.0f)) return fail(CC_ERR_INVALID, "prefilter must be >= 0");
+  if (opt.prefilter > 0.0f && opt.hierarchy != 2) return fail(CC_ERR_INVALID, "prefiltered cones need hierarchy 2");
   const uint64_t ncones = npoints * (uint64_t)nlights;
   if (ncones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one call");
   if (npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one call");
@@ -493,6 +517,14 @@ static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* 
   q.light_cone_cap = opt.light_cone_cap;
   q.wide_cone_cap = opt.wide_cone_cap;
   q.sky = sky;
+  q.prefilter = opt.prefilter;
+  cc::DevScene sd = scene->dev();
+  if (opt.prefilter > 0.0f) {
+    int rc2 = ensure_coverage(const_cast<cc_scene*>(scene));
+    if (rc2) return rc2;
+    sd = scene->dev();
+    if (opt.flags & CC_NO_OBJECT_PREFILTER) sd.obj_cov = nullptr;
+  }
   cc::DevOut o{};
   if (device_ptrs) {
     // The kernels read and write these with vector accesses.
@@ -559,7 +591,7 @@ static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* 
   }
   const int slot = (ctx->timed_first + ctx->timed_count) % ring;
   ctx->timed_count++;
-  CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
+  CC_CUDA(cc::launch_visibility(sd, q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
                                 &ctx->marks[3 * slot]),
           "visibility launch");
   if (device_ptrs) return CC_OK;
@@ -596,6 +628,19 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
                   const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                   void* stream) {
   return visibility_impl(ctx, scene, receivers, npoints, lights, nlights, opt, out, stream, 0u);
+}
+
+int64_t cc_scene_coverage(const cc_scene* scene, float* blas27, uint64_t max_blas, float* obj27, uint64_t max_obj) {
+  if (!scene) return -(int64_t)fail(CC_ERR_INVALID, "null scene");
+  const std::vector<float> blas = cc::blas_coverage(scene->flat);
+  const uint64_t nb = blas.size() / cc::kCoverageSamples;
+  if (blas27) std::copy(blas.begin(), blas.begin() + std::min(nb, max_blas) * cc::kCoverageSamples, blas27);
+  if (obj27 && !scene->flat.xforms.empty()) {
+    const std::vector<float> obj = cc::object_coverage(scene->flat, blas);
+    const uint64_t no = obj.size() / cc::kCoverageSamples;
+    std::copy(obj.begin(), obj.begin() + std::min(no, max_obj) * cc::kCoverageSamples, obj27);
+  }
+  return (int64_t)nb;
 }
 
 int cc_sky_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
@@ -680,6 +725,7 @@ int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
   if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
+  if (opt.prefilter != 0.0f) return fail(CC_ERR_INVALID, "cc_visibility_static takes exact cones only (prefilter 0)");
   if (npoints > CC_STATIC_MAX_CONES || npoints * (uint64_t)nlights > CC_STATIC_MAX_CONES)
     return fail(CC_ERR_INVALID, "more than CC_STATIC_MAX_CONES cones (or points) in one cc_visibility_static call");
   const uint64_t ncones = npoints * (uint64_t)nlights;

@@ -78,6 +78,10 @@ struct cc_scene {
   uint32_t* items = nullptr;
   float4* blas = nullptr;
   float4* xforms = nullptr;  // instanced scenes: 4 per transform
+  // Prefiltered cones' coverage samples, computed and uploaded on first use.
+  float* blas_cov = nullptr;
+  float* obj_cov = nullptr;
+  bool coverage_ready = false;
   uint64_t bytes = 0;
   cc::DevScene dev() const {
     cc::DevScene s;
@@ -88,6 +92,8 @@ struct cc_scene {
     s.blas = blas;
     s.nmeshes = flat.nmeshes;
     s.xforms = xforms;
+    s.blas_cov = blas_cov;
+    s.obj_cov = obj_cov;
     return s;
   }
 };

@@ -53,6 +53,12 @@ struct DevScene {
   // translation in w, then scale, 1 / scale); meshes[m].w names object m's.
   // Null when every object's triangles are in world space.
   const float4* xforms;
+  // Prefiltered cones: 27 coverage samples per triangle-hierarchy node and
+  // per object-hierarchy node (an object node's sample 13, unused as a
+  // direction, is 1 where the node has no prefiltered coverage); null where
+  // the scene has none on the device.
+  const float* blas_cov;
+  const float* obj_cov;
 };
 
 struct DevLight {

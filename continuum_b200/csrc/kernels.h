@@ -29,6 +29,9 @@ struct DevQuery {
   // kSkyCones: the query's cones are sky cones, the six cube faces around
   // each receiver (nlights = 6, lights unused), with the flags below.
   uint32_t sky = 0;
+  // Prefiltering cones: nodes projecting to at most this many bins are
+  // splatted (0: exact cones). Hierarchy level 2 only.
+  float prefilter = 0.0f;
 };
 constexpr uint32_t kSkyCones = 1u;
 constexpr uint32_t kSkyCombineMax = 2u;      // combine meshes by the maximum, as light cones do (a diagnostic)
@@ -121,6 +124,12 @@ constexpr size_t kStaticSortOffset = kStaticOrderOffset + 4 * size_t(kStaticMaxC
 cudaError_t static_scratch(int device, void** ptr);
 
 cudaError_t upload_disk_table(const float* table64);
+// The prefiltering unit's copy of the table, and its plain passes (packet
+// pass with 32-bit cells, or solo pass with 64-bit ones when `wide`).
+cudaError_t upload_disk_table_splat(const float* table64);
+cudaError_t launch_splat_pass(bool wide, bool count, bool inst, bool sky, const DevScene& s, const DevQuery& q,
+                              const DevOut& o, const uint32_t* list, const uint32_t* list_count, uint32_t pw,
+                              uint32_t blocks, cudaStream_t stream);
 
 // The packet pass over every cone, then (with o.redo_list) the solo pass over
 // the cones it listed. o.redo_count and o.error must be zero on entry.

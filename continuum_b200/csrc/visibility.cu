@@ -24,885 +24,26 @@
 // stopped early (capped, or every bin full), is listed and walked again
 // alone by a second launch, so every cone's result is the one its own walk
 // gives (the reference's walk without packets, as its view-cache bakes run).
-#include <cstdint>
-#include <type_traits>
-#include <cuda_runtime.h>
-
-#include "cone_device.cuh"
-#include "kernels.h"
+#include "visibility_kernel.cuh"
 
 namespace cc {
-
-__constant__ float c_disk[kBins];  // DISK (mask_cones.wgsl:888-897), uploaded by the host
-
-constexpr int kStack = 64;         // entries; the reference's is 48 (mask_cones.wgsl:111)
-constexpr int kConeFields = 17;    // apex, right, up, forward, window, far offset
-// Pairs passed to rasterization wait in a per-warp queue until 32 are ready:
-// a cull round adds at most 32 to at most 31 waiting. Pairs that need the
-// general clip path wait in a second queue of the same size.
-constexpr int kQueueCap = 64;
-constexpr uint32_t kQueueOwnerShift = 26;  // entry: cone lane << 26 | triangle slot (< 2^26)
-// Both queues' lengths in one word: fast queue in the low byte, general
-// queue in the next (each below 32 between rounds).
-__device__ __forceinline__ uint32_t fast_len(uint32_t q) { return q & 255u; }
-__device__ __forceinline__ uint32_t general_len(uint32_t q) { return q >> 8; }
-__device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) { return fast | (general << 8); }
-
-// Shared memory of one warp; Cell is the accumulator's cell: 32 bits in the
-// packet pass, 64 in the solo pass. Sky: the warp walks sky cones, whose
-// horizons are kept beside their frames.
-template <class CellT, bool Sky>
-struct WarpShared {
-  using Cell = CellT;
-  static constexpr bool kSky = Sky;
-  float cov[kBins * 32];                // each cone's 64 coverages, bin-major, lane innermost
-  Cell acc[kBins * 32];                 // each cone's accumulator (fixed point, units of kFixUnit)
-  float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
-  uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
-  uint32_t queue[kQueueCap];            // (cone, triangle) pairs that passed the cull, waiting to be rasterized
-  uint32_t general[kQueueCap];          // pairs that need rasterize's general path, waiting for it
-  uint32_t overflow[4];                 // word 0: cones whose 32-bit accumulation overflowed in the current mesh
-  float horizon[Sky ? 3 * 32 : 4];      // sky cones: each cone's horizon, field-major
-};
-static_assert(sizeof(WarpShared<unsigned int, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-static_assert(sizeof(WarpShared<unsigned long long, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-static_assert(sizeof(WarpShared<unsigned int, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-template <bool kSky>
-using NarrowShared = WarpShared<unsigned int, kSky>;
-template <bool kSky>
-using WideShared = WarpShared<unsigned long long, kSky>;
-// Resident blocks per SM the shared memory allows: 5 x 38 KB with 32-bit
-// cells, 4 x 55 KB with 64-bit ones.
-template <class WS>
-constexpr int blocks_per_sm() { return sizeof(typename WS::Cell) == 4 ? 5 : 4; }
-constexpr uint32_t kStatusAccOverflow = 32u;
-static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
-
-// A stack entry packed in one word: its kind in the top 2 bits (an
-// object-hierarchy node, a triangle-hierarchy node, or a mesh's resolve
-// marker), then a node's item count in 4 bits (0: interior), then its first
-// item (leaf) or left child (interior) in 26 bits. Each lane keeps two bits
-// per entry: whether its own walk needs the entry, and whether its cone
-// passed the entry's box test, which is done when the parent is visited (the
-// two children of a node are adjacent, so one 64-byte load serves both
-// tests and the nearest-first choice).
-constexpr uint32_t kRefIndexBits = 26;
-constexpr uint32_t kRefIndexMask = (1u << kRefIndexBits) - 1u;
-constexpr uint32_t kRefKindShift = 30;
-__device__ __forceinline__ uint32_t node_ref(float4 a, float4 b, uint32_t kind) {
-  return (kind << kRefKindShift) | ((__float_as_uint(b.w) & 15u) << kRefIndexBits) |
-         (__float_as_uint(a.w) & kRefIndexMask);
-}
-__device__ __forceinline__ uint32_t ref_kind(uint32_t r) { return r >> kRefKindShift; }
-__device__ __forceinline__ uint32_t ref_count(uint32_t r) { return (r >> kRefIndexBits) & 15u; }
-__device__ __forceinline__ uint32_t ref_index(uint32_t r) { return r & kRefIndexMask; }
-
-struct WarpStack {
-  uint32_t r0 = 0, r1 = 0;  // entry i held by lane i % 32, register i / 32
-  uint32_t need_lo = 0, need_hi = 0;
-  uint32_t pass_lo = 0, pass_hi = 0;
-  __device__ __forceinline__ void push(int i, uint32_t v, bool need, bool pass, int lane) {
-    if ((i & 31) == lane) {
-      if (i < 32) r0 = v; else r1 = v;
-    }
-    const uint32_t bit = 1u << (i & 31);
-    if (i < 32) {
-      need_lo = need ? (need_lo | bit) : (need_lo & ~bit);
-      pass_lo = pass ? (pass_lo | bit) : (pass_lo & ~bit);
-    } else {
-      need_hi = need ? (need_hi | bit) : (need_hi & ~bit);
-      pass_hi = pass ? (pass_hi | bit) : (pass_hi & ~bit);
-    }
-  }
-  __device__ __forceinline__ uint32_t get(int i) const {
-    return __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
-  }
-  __device__ __forceinline__ bool need(int i) const {
-    return ((i < 32 ? need_lo : need_hi) >> (i & 31)) & 1u;
-  }
-  __device__ __forceinline__ bool pass(int i) const {
-    return ((i < 32 ? pass_lo : pass_hi) >> (i & 31)) & 1u;
-  }
-};
-
-template <class WS>
-struct LaneState {
-  Cone cone;   // the cone in the space of the object being walked (the world's elsewhere)
-  Cone world;  // instanced scenes: the cone in world space
-  WS* ws;
-  float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
-  uint32_t full;
-  uint32_t queued;  // both queues' lengths (queue_lens; the same in every lane)
-  uint32_t cone_work;
-  uint32_t cap;
-  uint32_t status;
-  uint32_t n_obj, n_blas, n_tris;
-  bool independent;  // sky cones: meshes combine as independent occluders (else by the maximum)
-  f3 horizon;        // sky cones: the horizon in the space of the object being walked (the world's elsewhere)
-  f3 world_horizon;  // sky cones in instanced scenes: the horizon in world space
-};
-
-__device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
-
-template <class WS>
-__device__ __forceinline__ void store_cone(WS* ws, const Cone& c, int lane) {
-  float* t = ws->cone + lane;
-  const float f[kConeFields] = {c.apex.x, c.apex.y, c.apex.z, c.right.x, c.right.y, c.right.z, c.up.x, c.up.y,
-                                c.up.z,   c.fwd.x,  c.fwd.y,  c.fwd.z,   c.u0,      c.v0,      c.u1,   c.v1,
-                                c.far_offset};
-#pragma unroll
-  for (int k = 0; k < kConeFields; ++k) t[32 * k] = f[k];
-}
-
-// Sky cones: the lane's horizon beside its cone (the cull reads both).
-template <class WS>
-__device__ __forceinline__ void store_horizon(WS* ws, f3 h, int lane) {
-  if constexpr (WS::kSky) {
-    ws->horizon[lane] = h.x;
-    ws->horizon[32 + lane] = h.y;
-    ws->horizon[64 + lane] = h.z;
-  }
-}
-
-template <class WS>
-__device__ __forceinline__ Cone load_cone(const WS* ws, int owner) {
-  const float* t = ws->cone + owner;
-  Cone c;
-  c.apex = mk(t[0], t[32], t[64]);
-  c.right = mk(t[96], t[128], t[160]);
-  c.up = mk(t[192], t[224], t[256]);
-  c.fwd = mk(t[288], t[320], t[352]);
-  c.u0 = t[384];
-  c.v0 = t[416];
-  c.u1 = t[448];
-  c.v1 = t[480];
-  c.far_offset = t[512];
-  c.baxis = mk(0.f, 0.f, 0.f);
-  c.bcos = c.bsin = 0.f;
-  return c;
-}
-
-// The tests of cover_triangle (:594-616) for one (triangle, cone) pair: back
-// face, the window-direction test, may_touch. A pair that passes is
-// rasterized.
-template <class WS>
-__device__ __forceinline__ bool pair_survives(const DevScene& s, const WS* ws, int owner, uint32_t t) {
-  const Cone c = load_cone(ws, owner);
-  const f3 v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
-  const f3 v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
-  const f3 v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
-  const f3 n = cross(v1 - v0, v2 - v0);
-  if (dot(n, c.apex - v0) <= 0.0f) return false;  // faces away (:600)
-  if (dot(n, direction(c, 0.f, 0.f)) >= 0.f && dot(n, direction(c, 1.f, 0.f)) >= 0.f &&
-      dot(n, direction(c, 0.f, 1.f)) >= 0.f && dot(n, direction(c, 1.f, 1.f)) >= 0.f)
-    return false;  // every window direction leaves its plane (:601-606)
-  if constexpr (WS::kSky)
-    return may_touch<true>(c, v0, v1, v2, mk(ws->horizon[owner], ws->horizon[32 + owner], ws->horizon[64 + owner]));
-  else
-    return may_touch(c, v0, v1, v2);
-}
-
-template <class WS>
-__device__ __forceinline__ void load_pair(const DevScene& s, const WS* ws, uint32_t e, int& owner, Cone& c,
-                                          f3& v0, f3& v1, f3& v2) {
-  owner = (int)(e >> kQueueOwnerShift);
-  const uint32_t t = e & ((1u << kQueueOwnerShift) - 1u);
-  c = load_cone(ws, owner);
-  v0 = xyz(__ldg(&s.tris[3 * (size_t)t + 0]));
-  v1 = xyz(__ldg(&s.tris[3 * (size_t)t + 1]));
-  v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
-}
-
-template <class WS, class Acc>
-__device__ __forceinline__ void note_span(WS* ws, int owner, const Acc& acc) {
-  if (acc.span_lo < acc.span_hi) {
-    atomicMin(&ws->span_lo[owner], acc.span_lo);
-    atomicMax(&ws->span_hi[owner], acc.span_hi);
-  }
-}
-
-// The general path for general-queue entries first .. first+n (n <= 32),
-// one per lane.
-template <class WS>
-__device__ __noinline__ void raster_general(const DevScene& s, WS* ws, uint32_t first, uint32_t n, int lane) {
-  if ((uint32_t)lane < n) {
-    int owner;
-    Cone c;
-    f3 v0, v1, v2;
-    load_pair(s, ws, ws->general[first + lane], owner, c, v0, v1, v2);
-    LaneAcc<typename WS::Cell> acc{ws->acc + owner, 68u, 0u, &ws->overflow[0], 1u << owner};
-    rasterize_general(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2));
-    note_span(ws, owner, acc);
-  }
-  __syncwarp();
-}
-
-// Rasterizes queue entries first .. first+n (n <= 32), one per lane, each
-// into its cone's accumulator by the common case; pairs that need the
-// general path join the general queue, which is run whenever 32 wait.
-// Returns the general queue's new length (below 32).
-template <class WS>
-__device__ __noinline__ uint32_t raster_queue(const DevScene& s, WS* ws, uint32_t first, uint32_t n,
-                                              uint32_t general, int lane) {
-  bool defer = false;
-  uint32_t e = 0;
-  if ((uint32_t)lane < n) {
-    e = ws->queue[first + lane];
-    int owner;
-    Cone c;
-    f3 v0, v1, v2;
-    load_pair(s, ws, e, owner, c, v0, v1, v2);
-    LaneAcc<typename WS::Cell> acc{ws->acc + owner, 68u, 0u, &ws->overflow[0], 1u << owner};
-    defer = !rasterize_fast(c, acc, v0, v1, v2);
-    note_span(ws, owner, acc);
-  }
-  const uint32_t m = __ballot_sync(0xffffffffu, defer);
-  if (defer) ws->general[general + __popc(m & ((1u << lane) - 1u))] = e;
-  general += __popc(m);
-  __syncwarp();
-  if (general >= 32) {
-    general -= 32;
-    raster_general(s, ws, general, 32, lane);
-  }
-  return general;
-}
-
-// Triangles t0 .. t0+nt, each tested against the cones of the lanes in
-// `owners`: the pairs, triangle-major (consecutive lanes read the same
-// triangle), are dealt out over the warp for the cull tests; the survivors
-// join the warp's queue, and every 32 queued pairs are rasterized by the
-// whole warp at once, so lanes whose pair was culled do not sit idle while
-// the others rasterize. `queues` and the result are both queues' lengths.
-template <class WS>
-__device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t owners, uint32_t t0,
-                                            uint32_t nt, uint32_t queues, int lane) {
-  uint32_t queued = fast_len(queues), general = general_len(queues);
-  const uint32_t n_owners = __popc(owners);
-  const uint32_t n_pairs = n_owners * nt;
-  for (uint32_t base = 0; base < n_pairs; base += 32) {
-    const uint32_t pair = base + lane;
-    bool pass = false;
-    uint32_t entry = 0;
-    if (pair < n_pairs) {
-      const uint32_t k = pair / n_owners;
-      const uint32_t r = pair - k * n_owners;
-      const int owner = (int)__fns(owners, 0, r + 1);
-      pass = pair_survives(s, ws, owner, t0 + k);
-      entry = ((uint32_t)owner << kQueueOwnerShift) | (t0 + k);
-    }
-    const uint32_t m = __ballot_sync(0xffffffffu, pass);
-    if (pass) ws->queue[queued + __popc(m & ((1u << lane) - 1u))] = entry;
-    queued += __popc(m);
-    __syncwarp();
-    if (queued >= 32) {
-      queued -= 32;
-      general = raster_queue(s, ws, queued, 32, general, lane);
-    }
-  }
-  return queue_lens(queued, general);
-}
-
-// The mesh's coverage for the lane's own cone: running sum over the touched
-// cells (exact), snapped to whole within 1e-5, combined into the cone's bins
-// by max (:809-828), or for sky cones as independent occluders
-// (1 - (1 - before)(1 - covered), :819-821); then the cells are cleared for
-// the next mesh.
-template <class WS>
-__device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState<WS>& st, int lane) {
-  WS* ws = st.ws;
-  // The mesh's last pairs: the common case, then the general path.
-  uint32_t general = general_len(st.queued);
-  if (fast_len(st.queued)) general = raster_queue(s, ws, 0, fast_len(st.queued), general, lane);
-  if (general) raster_general(s, ws, 0, general, lane);
-  st.queued = 0;
-  const uint32_t lo = ws->span_lo[lane];
-  const uint32_t end = min(ws->span_hi[lane], (uint32_t)kBins);
-  // 32-bit cells: a cone whose adds overflowed in this mesh is walked again
-  // with 64-bit cells (its result here is discarded).
-  if (sizeof(typename WS::Cell) == 4) {
-    if ((ws->overflow[0] >> lane) & 1u) st.status |= kStatusAccOverflow;
-    __syncwarp();
-    if (lane == 0) ws->overflow[0] = 0u;
-  }
-  long long running = 0;
-  for (uint32_t b = lo; b < end; ++b) {
-    typename WS::Cell* cell = &ws->acc[32 * b + lane];
-    if (sizeof(typename WS::Cell) == 4) running += (long long)(int)*cell;
-    else running += (long long)*cell;
-    *cell = 0;
-    float covered = fabsf(__ll2float_rn(running) * kFixUnit);
-    if (covered >= 1.0f - 1e-5f) covered = 1.0f;
-    if (covered > 1e-6f) {
-      const float before = st.cov[32 * b];
-      float after;
-      if constexpr (WS::kSky) {
-        after = st.independent ? 1.0f - (1.0f - before) * (1.0f - fminf(covered, 1.0f))
-                               : fmaxf(before, fminf(covered, 1.0f));
-      } else {
-        after = fmaxf(before, fminf(covered, 1.0f));
-      }
-      st.cov[32 * b] = after;
-      if (before < 1.0f && after >= 1.0f) st.full++;
-    }
-  }
-  ws->span_lo[lane] = 68u;
-  ws->span_hi[lane] = 0u;
-  __syncwarp();
-}
-
-// Stack entry kinds for the walk of both hierarchy levels in one loop.
-constexpr uint32_t kObjNode = 0;   // an object-hierarchy node
-constexpr uint32_t kTriNode = 1;   // a node of the current mesh's triangle hierarchy
-constexpr uint32_t kResolve = 2;   // the current mesh is done: resolve its coverage (index 1: and return to world space)
-constexpr uint32_t kObjRoot = 3;   // instanced scenes: the root of object `index`'s triangle hierarchy
-
-// add_mesh_coverage_if (:713-829) for hierarchy levels 0 and 1: every
-// triangle of mesh m for the lanes with `on`, in leaf-sized groups, then the
-// mesh's resolve.
-template <bool kCount, bool kInst, class WS>
-__device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& st, bool on, uint32_t m, int lane) {
-  const uint32_t owners = __ballot_sync(0xffffffffu, on);
-  if (!owners) return;
-  const uint4 range = __ldg(&s.meshes[m]);
-  const bool placed = kInst && range.w != kNoneU;
-  if (placed) {
-    st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);  // cone_to_object (:623-638)
-    store_cone(st.ws, st.cone, lane);
-    if constexpr (WS::kSky) {
-      st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
-      store_horizon(st.ws, st.horizon, lane);
-    }
-    __syncwarp();
-  }
-  if (kCount && on) st.n_tris += range.y;
-  for (uint32_t t = range.x; t < range.x + range.y; t += 8)
-    st.queued = cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), st.queued, lane);
-  resolve_mesh(s, st, lane);
-  if (placed) {
-    st.cone = st.world;
-    store_cone(st.ws, st.cone, lane);
-    if constexpr (WS::kSky) {
-      st.horizon = st.world_horizon;
-      store_horizon(st.ws, st.horizon, lane);
-    }
-    __syncwarp();
-  }
-}
-
-// The cone walk (scene_coverage_if, :1160-1227, with add_mesh_coverage_if,
-// :713-829, for each mesh it reaches). Hierarchy level 2 walks both levels in
-// one loop: an object leaf that a lane descends into pushes, for each of its
-// meshes (first mesh on top), a resolve marker under the mesh's triangle
-// hierarchy root, so each mesh is walked and then resolved in the reference's
-// order. Object nodes are visited nearest child first along the bounding
-// cone's axis while some bin is open; triangle-hierarchy nodes right child
-// first (:783-787) with no full check, as in the reference; every popped node
-// a lane needs counts toward its walk cap, though its box was tested when its
-// parent was visited. Levels 0 and 1 keep the reference's loops over meshes
-// and triangles.
-template <bool kCount, bool kInst, class WS>
-__device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState<WS>& st, bool traced,
-                                           int lane) {
-  const Cone& c = st.cone;
-  if (hierarchy == 0) {
-    for (uint32_t m = 0; m < s.nmeshes; ++m)
-      add_mesh_flat<kCount, kInst, WS>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
-    return;
-  }
-  WarpStack stk;
-  const float4 ra = __ldg(&s.nodes[0]);
-  const float4 rb = __ldg(&s.nodes[1]);
-  const bool root_pass = traced && may_touch_box<WS::kSky>(c, node_lo(ra), node_lo(rb), st.horizon);
-  stk.push(0, node_ref(ra, rb, kObjNode), traced, root_pass, lane);
-  int sp = 1;
-  while (sp > 0) {
-    --sp;
-    uint32_t ref = stk.get(sp);
-    uint32_t kind = ref_kind(ref);
-    if (kind == kResolve) {
-      resolve_mesh(s, st, lane);
-      if (kInst && ref_index(ref) == 1) {  // back to world space
-        st.cone = st.world;
-        store_cone(st.ws, st.cone, lane);
-        if constexpr (WS::kSky) {
-          st.horizon = st.world_horizon;
-          store_horizon(st.ws, st.horizon, lane);
-        }
-        __syncwarp();
-      }
-      continue;
-    }
-    if (kInst && kind == kObjRoot) {
-      // Entering a placed object: the cone in its space (cone_to_object,
-      // :623-638), then its triangle hierarchy's root.
-      const uint4 range = __ldg(&s.meshes[ref_index(ref)]);
-      st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
-      store_cone(st.ws, st.cone, lane);
-      if constexpr (WS::kSky) {
-        // The horizon turns with the cone (:634).
-        st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
-        store_horizon(st.ws, st.horizon, lane);
-      }
-      __syncwarp();
-      ref = node_ref(__ldg(&s.blas[2 * (size_t)range.z + 0]), __ldg(&s.blas[2 * (size_t)range.z + 1]), kTriNode);
-      kind = kTriNode;
-    }
-    const bool is_obj = kind == kObjNode;
-    const bool mine = stk.need(sp) && st.cone_work < st.cap && (!is_obj || st.full < (uint32_t)kBins);
-    if (mine) st.cone_work++;
-    if (kCount && mine) {
-      if (is_obj) st.n_obj++; else st.n_blas++;
-    }
-    const bool descend = mine && stk.pass(sp);
-    const uint32_t owners = __ballot_sync(0xffffffffu, descend);
-    if (!owners) continue;
-    const uint32_t ia = ref_index(ref), ib = ref_count(ref);
-    if (ib > 0 && !is_obj) {
-      // A triangle-hierarchy leaf: its triangles against every descending cone.
-      if (descend) {
-        st.cone_work += ib;
-        if (kCount) st.n_tris += ib;
-      }
-      st.queued = cover_leaf(s, st.ws, owners, ia, ib, st.queued, lane);
-    } else if (ib > 0) {
-      // An object leaf: its meshes.
-      if (hierarchy == 1) {
-        for (uint32_t k = ia; k < ia + ib; ++k)
-          add_mesh_flat<kCount, kInst, WS>(s, st, descend, __ldg(&s.items[k]), lane);
-        continue;
-      }
-      for (int k = (int)(ia + ib) - 1; k >= (int)ia; --k) {
-        const uint4 range = __ldg(&s.meshes[__ldg(&s.items[k])]);
-        if (range.z == kNoneU) continue;  // no triangles: nothing to draw or resolve
-        if (sp + 2 > kStack) {
-          if (descend) st.status |= 2u;
-          continue;
-        }
-        const float4 ma = __ldg(&s.blas[2 * (size_t)range.z + 0]);
-        const float4 mb = __ldg(&s.blas[2 * (size_t)range.z + 1]);
-        const uint32_t m = __ldg(&s.items[k]);
-        if (kInst && range.w != kNoneU) {
-          // A placed object: its root's box in its own space; the entry names
-          // the object, whose cone is set up when the entry is popped.
-          const Cone oc = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
-          f3 oh = st.horizon;
-          if constexpr (WS::kSky) oh = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
-          const bool mesh_pass = descend && may_touch_box<WS::kSky>(oc, node_lo(ma), node_lo(mb), oh);
-          stk.push(sp, (kResolve << kRefKindShift) | 1u, false, false, lane);
-          stk.push(sp + 1, (kObjRoot << kRefKindShift) | m, descend, mesh_pass, lane);
-        } else {
-          const bool mesh_pass = descend && may_touch_box<WS::kSky>(c, node_lo(ma), node_lo(mb), st.horizon);
-          stk.push(sp, kResolve << kRefKindShift, false, false, lane);
-          stk.push(sp + 1, node_ref(ma, mb, kTriNode), descend, mesh_pass, lane);
-        }
-        sp += 2;
-      }
-    } else {
-      // An interior node: both children's boxes tested now.
-      const float4* base = (is_obj ? s.nodes : s.blas) + 2 * (size_t)ia;
-      const float4 la = __ldg(base + 0), lb = __ldg(base + 1), xa = __ldg(base + 2), xb = __ldg(base + 3);
-      bool pl = false, pr = false;
-      if (descend) {
-#pragma unroll 1
-        for (int ch = 0; ch < 2; ++ch) {
-          const bool t = may_touch_box<WS::kSky>(c, node_lo(ch ? xa : la), node_lo(ch ? xb : lb), st.horizon);
-          if (ch) pr = t; else pl = t;
-        }
-      }
-      bool swap = false;  // left child popped first (object level: when it is the nearer)
-      // Nearest child first where meshes combine by the maximum; sky cones
-      // combining as independent occluders keep the left child first, as
-      // their products would round differently in another order (:1188-1207).
-      bool nearest = is_obj;
-      if constexpr (WS::kSky) nearest = nearest && !st.independent;
-      if (nearest) {
-        const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
-        const float db = dot(c.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - c.apex);
-        const bool pref = db < da;  // this lane's own order: right child nearer
-        swap = __shfl_sync(0xffffffffu, pref, __ffs(owners) - 1);
-        if (descend && pref != swap) st.status |= 4u;
-      } else if (!is_obj) {
-        swap = true;  // triangle hierarchies pop the right child first (:783-787)
-      }
-      if (sp + 2 > kStack) {
-        if (descend) st.status |= 2u;
-        continue;
-      }
-      const uint32_t rl = node_ref(la, lb, kind), rr = node_ref(xa, xb, kind);
-      // The child popped second below the one popped first.
-      stk.push(sp, swap ? rl : rr, descend, swap ? pl : pr, lane);
-      stk.push(sp + 1, swap ? rr : rl, descend, swap ? pr : pl, lane);
-      sp += 2;
-    }
-  }
-}
-
-__device__ __forceinline__ f3 shfl3(f3 v, int src) {
-  return mk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src), __shfl_sync(0xffffffffu, v.z, src));
-}
-
-// The blocked light of lane j's cone, Σ coverage × bin weight (cone_visible,
-// :1244-1272), computed by the whole warp. With the window above the
-// horizon every bin weight is Lambert's formula over its quad
-// (bin_weight, :1232-1242); the 64 quads share 81 corner directions and 144
-// edges, so the warp normalizes each corner once and integrates each edge
-// once (a quad's edges are its neighbours' reversed, exact negatives in
-// IEEE arithmetic) and each lane combines two bins. A window crossing the
-// horizon clips each bin on its own (clipped_bin_weight, :1331-1369).
-// `cov_j` is lane j's coverage column (bin b at cov_j[32 * b]); `scratch`
-// holds 387 floats. Every lane returns the sum.
-__device__ __noinline__ float warp_blocked(const Cone& mine, f3 my_normal, bool my_all_above, const float* cov_j,
-                                           float* scratch, int j, int lane) {
-  Cone c;
-  c.fwd = shfl3(mine.fwd, j);
-  c.right = shfl3(mine.right, j);
-  c.up = shfl3(mine.up, j);
-  c.u0 = __shfl_sync(0xffffffffu, mine.u0, j);
-  c.v0 = __shfl_sync(0xffffffffu, mine.v0, j);
-  c.u1 = __shfl_sync(0xffffffffu, mine.u1, j);
-  c.v1 = __shfl_sync(0xffffffffu, mine.v1, j);
-  const f3 n = shfl3(my_normal, j);
-  const bool all_above = __shfl_sync(0xffffffffu, my_all_above, j);
-  float sum = 0.0f;
-  if (all_above) {
-    const float g = float(kGrid);
-    float* corner = scratch;       // 81 unit directions, point (col, row) at 3 * (row * 9 + col)
-    float* edge = scratch + 243;   // 72 row edges (col, row)->(col+1, row), then 72 column edges (col, row)->(col, row+1)
-    for (int p = lane; p < 81; p += 32) {
-      const f3 u = normalize(direction(c, float(p % 9) / g, float(p / 9) / g));
-      corner[3 * p] = u.x;
-      corner[3 * p + 1] = u.y;
-      corner[3 * p + 2] = u.z;
-    }
-    __syncwarp();
-    for (int e = lane; e < 144; e += 32) {
-      int a, b;
-      if (e < 72) {
-        a = (e / 8) * 9 + e % 8;
-        b = a + 1;
-      } else {
-        a = ((e - 72) / 9) * 9 + (e - 72) % 9;
-        b = a + 9;
-      }
-      edge[e] = lambert_edge_unit(n, mk(corner[3 * a], corner[3 * a + 1], corner[3 * a + 2]),
-                                  mk(corner[3 * b], corner[3 * b + 1], corner[3 * b + 2]));
-    }
-    __syncwarp();
-    for (int b = lane; b < kBins; b += 32) {
-      const float cv = cov_j[32 * b];
-      if (cv > 0.0f) {
-        const int col = b % kGrid, row = b / kGrid;
-        const float e01 = edge[row * 8 + col];                 // d0 -> d1
-        const float e12 = edge[72 + row * 9 + col + 1];        // d1 -> d2
-        const float e23 = -edge[(row + 1) * 8 + col];          // d2 -> d3
-        const float e30 = -edge[72 + row * 9 + col];           // d3 -> d0
-        sum += cv * fabsf(0.5f * (e01 + e12 + e23 + e30));
-      }
-    }
-    __syncwarp();
-  } else {
-    for (int b = lane; b < kBins; b += 32) {
-      const float cv = cov_j[32 * b];
-      if (cv > 0.0f) sum += cv * clipped_bin_weight(c, n, b);
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-  return sum;
-}
-
-// The job of a batch that holds `key` (a packet or a cone number): the last
-// job whose start is at most `key`. Warp-uniform.
-__device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, uint32_t njobs, uint64_t key,
-                                             bool by_cone) {
-  uint32_t lo = 0, hi = njobs;  // jobs[lo].start <= key < jobs[hi].start
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    const uint64_t start = by_cone ? __ldg(&jobs[mid].cone_start) : __ldg(&jobs[mid].packet_start);
-    if (start <= key) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-// kBatch: the cones of every job of a batch (BatchLaunch); each packet's job
-// is looked up in the job table, and the redo list holds batch cone numbers.
-// kInst: the scene's objects place shared geometry with transforms.
-// kWide: 64-bit accumulator cells (the solo pass); else 32-bit ones (the
-// packet pass), whose overflowed cones the solo pass walks again.
-// kSky: sky cones, the six cube faces around each receiver in place of its
-// lights (cone c = face * npoints + point).
-template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky>
-// The blocks the shared memory fits per SM; saying so bounds the registers
-// per thread the allocator may use without lowering occupancy.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm : kBlocksPerSm)
-    visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
-                      const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
-  using WS = typename std::conditional<kWide, WideShared<kSky>, NarrowShared<kSky>>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  WS* ws = reinterpret_cast<WS*>(smem_raw) + wib;
-  for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0;
-  if (lane == 0) ws->overflow[0] = 0u;
-  ws->span_lo[lane] = 68u;
-  ws->span_hi[lane] = 0u;
-
-  const uint64_t plain_cones = q_plain.npoints * (uint64_t)q_plain.nlights;
-  uint64_t npackets;
-  if (list) npackets = (uint64_t)min(*list_count, o.redo_capacity);  // one cone per packet
-  else npackets = kBatch ? batch.packets : (plain_cones + pw - 1) / pw;
-  // Packets are taken from a shared counter as warps finish: their costs
-  // differ by two orders of magnitude, so a fixed assignment leaves most
-  // warps idle behind the slowest.
-  uint32_t* next = list ? o.next_solo : o.next_packet;
-  for (;;) {
-    uint32_t packet = 0;
-    if (lane == 0) packet = atomicAdd(next, 1u);
-    packet = __shfl_sync(0xffffffffu, packet, 0);
-    if (packet >= npackets) break;
-    // The packet's job: its scene, query and outputs.
-    DevScene s = s_plain;
-    DevQuery q = q_plain;
-    uint2* out_full = o.full;
-    uint2* out_any = o.any;
-    float* out_partial = o.partial;
-    float* out_irradiance = o.irradiance;
-    float* out_fraction = o.fraction;
-    uint4* out_work = o.work;
-    uint64_t cone_start = 0;  // the job's first cone in the batch's numbering
-    uint64_t ncones = plain_cones;
-    uint64_t wbase = (uint64_t)packet * pw;
-    uint64_t listed = 0;
-    if (list) listed = list[packet];
-    if constexpr (kBatch) {
-      const uint32_t j = list ? find_job(batch.jobs, batch.njobs, listed, true)
-                              : find_job(batch.jobs, batch.njobs, packet, false);
-      const JobGpu* J = batch.jobs + j;
-      s = J->scene;
-      q = J->query;
-      q.order = batch.order ? batch.order + J->point_start : nullptr;
-      out_full = J->full;
-      out_any = J->any;
-      out_partial = J->partial;
-      out_irradiance = J->irradiance;
-      out_fraction = J->fraction;
-      out_work = J->work;
-      cone_start = J->cone_start;
-      ncones = q.npoints * (uint64_t)q.nlights;
-      if (!list) wbase = (packet - J->packet_start) * (uint64_t)pw;
-    }
-    const uint64_t slot = wbase + lane;
-    const bool valid = list ? lane == 0 : ((uint32_t)lane < pw && slot < ncones);
-    uint64_t c = 0;
-    if (valid) {
-      if (list) {
-        c = listed - cone_start;
-      } else if (q.order) {
-        const uint64_t light_base = (slot / q.npoints) * q.npoints;
-        c = light_base + __ldg(&q.order[slot - light_base]);
-      } else {
-        c = slot;
-      }
-    }
-    const uint32_t l = (uint32_t)(c / q.npoints);
-    const uint64_t p = c - (uint64_t)l * q.npoints;
-
-    LaneState<WS> st;
-    st.ws = ws;
-    st.cov = ws->cov + lane;
-    st.full = 0;
-    st.queued = 0;
-    st.cone_work = 0;
-    st.status = 0;
-    st.n_obj = st.n_blas = st.n_tris = 0;
-    st.independent = false;
-    st.horizon = st.world_horizon = mk(0.f, 0.f, 0.f);
-    for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 0.0f;
-
-    const float4 pt4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 0]);
-    const float4 nm4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 1]);
-    const f3 point = xyz(pt4), normal = xyz(nm4);
-    st.cone = Cone{};
-    DevLight L{};
-    float spot = 1.0f;
-    LightConeInfo info{true, false, false};
-    bool traced;
-    if constexpr (WS::kSky) {
-      // Sky face l of the receiver (sky_face, :1444-1478); walked without a
-      // cap (:1059, :1305).
-      traced = valid && sky_face(l, point, normal, st.cone);
-      st.cap = 0xffffffffu;
-      st.independent = (q.sky & kSkyCombineMax) == 0u;
-      st.horizon = (q.sky & kSkyNoHorizonCull) == 0u ? normal : mk(0.f, 0.f, 0.f);
-      st.world_horizon = st.horizon;
-    } else {
-      L = load_light(q.lights, valid ? l : 0);
-      // hit_irradiance_rect (:2125-2128): spot falloff and the facing test
-      // gate the cone.
-      spot = spot_falloff(L, normalize(point - light_center(L)));
-      const bool on = valid && spot > 0.0f && faces_light(L, point, normal);
-      info = light_cone(point, L, q.wide_extent, st.cone);
-      traced = on && info.ok;
-      st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
-    }
-    if (kInst) st.world = st.cone;
-    store_cone(ws, st.cone, lane);
-    store_horizon(ws, st.horizon, lane);
-    __syncwarp();
-
-    scene_walk<kCount, kInst>(s, q.hierarchy, st, traced, lane);
-
-    // A grazing sliver stopped at its cap counts as blocked (:1295-1305).
-    const bool capped = traced && st.cone_work >= st.cap;
-    if (capped) st.status |= 1u;
-    if (capped && info.wide_window && !info.wide_clipped) {
-      for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 1.0f;
-      st.full = kBins;
-    }
-    if (traced && st.full >= (uint32_t)kBins) st.status |= 16u;
-
-    uint32_t fw0 = 0, fw1 = 0, aw0 = 0, aw1 = 0;
-    for (int k = 0; k < kBins; ++k) {
-      const float v = st.cov[32 * k];
-      const uint32_t bit = 1u << (k & 31);
-      if (v >= 1.0f) { if (k < 32) fw0 |= bit; else fw1 |= bit; }
-      if (v > 0.0f) { if (k < 32) aw0 |= bit; else aw1 |= bit; }
-    }
-    const bool last_empty = (aw0 | aw1) == 0u;
-    const bool last_full = (fw0 & fw1) == 0xffffffffu;
-
-    float value = 0.0f, ratio = 1.0f;
-    if constexpr (WS::kSky) {
-      // sky_face_light (:1489-1498): the face's window clipped to the
-      // horizon, less its covered bins' clipped weights.
-      if (traced) {
-        float blocked = 0.0f;
-        for (int b = 0; b < kBins; ++b) {
-          const float cv = st.cov[32 * b];
-          if (cv > 0.0f) blocked += cv * clipped_bin_weight(st.cone, normal, b);
-        }
-        const float open = clipped_window_weight(st.cone, normal);
-        value = fmaxf(open - blocked, 0.0f);
-        ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
-      }
-    } else {
-    // Rect light cones with coverage: the bins' Lambert weights, one cone at
-    // a time across the warp (the cone table is free now: it is the scratch).
-    const bool rect_traced = traced && !is_sphere(L);
-    bool all_above = true;
-    float total = 0.0f;
-    if (rect_traced) total = window_weight(st.cone, normal, &all_above);
-    float blocked = 0.0f;
-    uint32_t todo = __ballot_sync(0xffffffffu, rect_traced && !last_empty);
-    while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const float b = warp_blocked(st.cone, normal, all_above, ws->cov + j, ws->cone, j, lane);
-      if (lane == j) blocked = b;
-    }
-    if (traced) {
-      const Cone& cn = st.cone;
-      if (is_sphere(L)) {
-        // sphere_open_share (:957-972)
-        float total = 0.0f, open = 0.0f;
-        const float g = float(kGrid);
-        for (int b = 0; b < kBins; ++b) {
-          const float mfrac = info.wide_clipped ? 1.0f : c_disk[b];
-          if (mfrac <= 0.0f) continue;
-          f3 d = direction(cn, (float(b % kGrid) + 0.5f) / g, (float(b / kGrid) + 0.5f) / g);
-          float l2 = dot(d, d);
-          float w = mfrac * fmaxf(dot(normal, d), 0.0f) / (l2 * l2);
-          total += w;
-          open += w * (1.0f - st.cov[32 * b]);
-        }
-        const float share = total <= 0.0f ? 1.0f : open / total;
-        value = sphere_unshadowed(point, normal, L) * share;
-      } else {
-        // cone_visible (:1244-1272) and wide_visible (:1070-1073)
-        float visible = fmaxf(total - blocked, 0.0f);
-        if (info.wide_clipped) visible = (total > 1e-9f ? visible / total : 1.0f) * rect_open(point, normal, L);
-        value = visible;
-      }
-    }
-    value *= spot;
-    // The lighting cache's ratio (vc_bake :3453-3510, static light).
-    const float open = unshadowed(point, normal, L);
-    ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
-    if (open > 0.0f && last_empty) ratio = 1.0f;
-    if (open > 0.0f && last_full) ratio = 0.0f;
-    }
-
-    // A walk again keeps the reasons its packet pass listed the cone for.
-    if (valid && list && out_work) st.status |= out_work[c].w & (4u | kStatusAccOverflow);
-    if (list) st.status |= 8u;
-    const bool redo = !list && o.redo_list &&
-                      (((st.status & 4u) && (st.status & (1u | 16u))) || (st.status & kStatusAccOverflow));
-    if (redo) {
-      const uint32_t at = atomicAdd(o.redo_count, 1u);
-      if (at < o.redo_capacity) o.redo_list[at] = (uint32_t)(cone_start + c);
-      else atomicOr(o.error, 1u);
-    }
-    if (st.status & 2u) atomicOr(o.error, 2u);
-    if (valid && redo && out_work) out_work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
-    if (valid && !redo) {
-      if (out_full) out_full[c] = make_uint2(fw0, fw1);
-      if (out_any) out_any[c] = make_uint2(aw0, aw1);
-      if (out_irradiance) out_irradiance[c] = value;
-      if (out_fraction) out_fraction[c] = ratio;
-      if (out_work) out_work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
-      if (out_partial) {
-        float4* dst = reinterpret_cast<float4*>(out_partial + 64 * c);
-#pragma unroll 4
-        for (int k = 0; k < 16; ++k)
-          dst[k] = make_float4(st.cov[32 * (4 * k)], st.cov[32 * (4 * k + 1)], st.cov[32 * (4 * k + 2)],
-                               st.cov[32 * (4 * k + 3)]);
-      }
-    }
-    __syncwarp();
-  }
-}
 
 // ---- host-side launchers --------------------------------------------------------
 
 cudaError_t upload_disk_table(const float* table64) {
-  return cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
+  cudaError_t e = cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
+  if (e != cudaSuccess) return e;
+  return upload_disk_table_splat(table64);  // the prefiltering unit's copy
 }
 
-// Whether the large dynamic shared memory size was allowed, per device and
-// kernel variant (the attribute is set per device).
-static uint64_t g_attr_set[32] = {};
-
-template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false>
-static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
+// The exact cones' plain pass (packet or solo) of the variant the flags pick;
+// prefiltering cones' passes are compiled in visibility_splat.cu.
+template <bool kWide>
+static cudaError_t exact_pass(bool count, bool inst, bool sky, const DevScene& s, const DevQuery& q, const DevOut& o,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * (kWide ? sizeof(WideShared<kSky>) : sizeof(NarrowShared<kSky>));
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const uint64_t bit = 1ull << (dev & 63);
-  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0) + (kSky ? 16 : 0);
-  if (!(g_attr_set[variant] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide, kSky>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    g_attr_set[variant] |= bit;
-  }
-  visibility_kernel<kCount, kBatch, kInst, kWide, kSky>
-      <<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
-  return cudaGetLastError();
-}
-
-// A plain (not batched) pass of the variant the flags pick.
-template <bool kWide, bool kSky>
-static cudaError_t plain_pass(bool count, bool inst, const DevScene& s, const DevQuery& q, const DevOut& o,
-                              const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
-                              cudaStream_t stream) {
-  const BatchLaunch none{};
-  if (inst)
-    return count ? launch_one<true, false, true, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream)
-                 : launch_one<false, false, true, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream);
-  return count ? launch_one<true, false, false, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream)
-               : launch_one<false, false, false, kWide, kSky>(s, q, o, none, list, list_count, pw, blocks, stream);
+  return sky ? plain_pass<kWide, true, false>(count, inst, s, q, o, list, list_count, pw, blocks, stream)
+             : plain_pass<kWide, false, false>(count, inst, s, q, o, list, list_count, pw, blocks, stream);
 }
 
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t pw, bool count,
@@ -925,14 +66,15 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
   const bool inst = s.xforms != nullptr;
   const bool sky = (q.sky & kSkyCones) != 0u;
+  const bool splat = q.prefilter > 0.0f;
   // The packet pass with 32-bit accumulator cells, the solo pass with 64-bit.
   auto packets_pass = [&](uint32_t p, uint32_t nb) {
-    return sky ? plain_pass<false, true>(count, inst, s, q, o, nullptr, nullptr, p, nb, stream)
-               : plain_pass<false, false>(count, inst, s, q, o, nullptr, nullptr, p, nb, stream);
+    return splat ? launch_splat_pass(false, count, inst, sky, s, q, o, nullptr, nullptr, p, nb, stream)
+                 : exact_pass<false>(count, inst, sky, s, q, o, nullptr, nullptr, p, nb, stream);
   };
   auto solo_pass = [&](uint32_t nb) {
-    return sky ? plain_pass<true, true>(count, inst, s, q, o, o.redo_list, o.redo_count, 1, nb, stream)
-               : plain_pass<true, false>(count, inst, s, q, o, o.redo_list, o.redo_count, 1, nb, stream);
+    return splat ? launch_splat_pass(true, count, inst, sky, s, q, o, o.redo_list, o.redo_count, 1, nb, stream)
+                 : exact_pass<true>(count, inst, sky, s, q, o, o.redo_list, o.redo_count, 1, nb, stream);
   };
   cudaError_t e = packets_pass(pw, blocks);
   if (marks) cudaEventRecord(marks[1], stream);

@@ -188,6 +188,18 @@ class Scene:
         keys = ("ntris", "nmeshes", "nblas", "nblas_items", "nnodes", "nitems")
         return {k: int(v) for k, v in zip(keys, out)}
 
+    def coverage(self) -> tuple:
+        """The prefiltered cones' coverage samples: (triangle-hierarchy nodes
+        (n, 27), object nodes (m, 27) for an instanced scene, else None)."""
+        sz = self.sizes()
+        blas = np.zeros((max(sz["nblas"], 1), 27), np.float32)
+        inst = self.transforms().shape[0] > 0
+        obj = np.zeros((max(sz["nnodes"], 1), 27), np.float32) if inst else None
+        n = load().cc_scene_coverage(self.handle, ptr(blas), sz["nblas"], ptr(obj), sz["nnodes"] if inst else 0)
+        if n < 0:
+            check(int(-n))
+        return blas[: sz["nblas"]], (obj[: sz["nnodes"]] if inst else None)
+
     def arrays(self) -> dict:
         """The host layouts (hierarchy.rs Flat + mesh_hierarchy), for checking the builder."""
         sz = self.sizes()
@@ -283,7 +295,9 @@ class MaskConeKernel:
 
     Like the reference's kernel it is used from one thread at a time. The walk
     parameters the reference keeps in cells (``wide_extent``,
-    ``light_cone_cap``, ``wide_cone_cap``; lib.rs:1211-1213) are attributes.
+    ``light_cone_cap``, ``wide_cone_cap``; lib.rs:1211-1213; ``prefilter``,
+    set_prefilter, lib.rs:1508; ``object_prefilter``, lib.rs:1595) are
+    attributes.
     """
 
     def __init__(self, device: int = 0):
@@ -296,6 +310,8 @@ class MaskConeKernel:
         self.light_cone_cap = 4096
         self.wide_cone_cap = 512
         self.points_per_warp = 32
+        self.prefilter = 0.0
+        self.object_prefilter = True
 
     @classmethod
     def new(cls, device: int = 0) -> Optional["MaskConeKernel"]:
@@ -414,7 +430,8 @@ class MaskConeKernel:
         o.light_cone_cap = int(self.light_cone_cap)
         o.wide_cone_cap = int(self.wide_cone_cap)
         o.points_per_warp = int(points_per_warp or self.points_per_warp)
-        o.flags = int(flags)
+        o.flags = int(flags) | (0 if self.object_prefilter else _lib.CC_NO_OBJECT_PREFILTER)
+        o.prefilter = float(self.prefilter)
         return o
 
     def visibility(self, scene: Scene, receivers, lights, hierarchy=Hierarchy.TRIANGLES,

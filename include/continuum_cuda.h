@@ -62,6 +62,7 @@ extern "C" {
 #define CC_DEVICE_POINTERS 1u /* receivers, lights and outputs are device pointers */
 #define CC_NO_REDO 2u         /* skip the solo re-walk (diagnostic): order-diverged and overflowed cones keep their packet results */
 #define CC_KEEP_ORDER 4u      /* walk points in the given order (default: Morton order of their positions) */
+#define CC_NO_OBJECT_PREFILTER 8u /* with prefilter: splat triangle-hierarchy nodes only (set_object_prefilter(false)) */
 
 /* Status bits in cc_outputs.work[4 * c + 3] */
 #define CC_CONE_CAPPED 1u     /* the walk stopped at its cap (LIGHT_CONE_CAP / WIDE_CONE_CAP) */
@@ -184,10 +185,16 @@ typedef struct cc_options {
   uint32_t light_cone_cap;   /* LIGHT_CONE_CAP, mask_cones.wgsl:1052 (4096) */
   uint32_t wide_cone_cap;    /* WIDE_CONE_CAP, mask_cones.wgsl:1056 (512) */
   uint32_t points_per_warp;  /* cones walked together per warp: 1..32 (32); results do not depend on it */
-  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO, CC_KEEP_ORDER */
+  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO, CC_KEEP_ORDER, CC_NO_OBJECT_PREFILTER */
+  float prefilter;           /* prefiltered cones (MaskConeKernel::set_prefilter, lib.rs:1508): a hierarchy node
+                                wholly between the near and far planes projecting to at most this many bins is
+                                splatted with its directional coverage instead of descended into
+                                (node_cone_test, mask_cones.wgsl:519-574; object nodes of instanced scenes:
+                                splat_object_node, :1096-1150). 0: exact cones. Needs hierarchy 2; cc_visibility
+                                and cc_sky_visibility only */
 } cc_options;
 
-/* Defaults: hierarchy 2, 8.0, 4096, 512, 32, 0. */
+/* Defaults: hierarchy 2, 8.0, 4096, 512, 32, 0, prefilter 0. */
 CC_API void cc_options_default(cc_options* opt);
 
 typedef struct cc_outputs {
@@ -208,6 +215,15 @@ typedef struct cc_outputs {
 CC_API int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
                   const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                   void* stream);
+
+/* The prefiltered cones' coverage samples of a scene's nodes (27 per node,
+ * hierarchy.rs:710-723): of every triangle-hierarchy node (blas27, nullable,
+ * up to max_blas nodes) and, for an instanced scene, of every object-hierarchy
+ * node (obj27, nullable; sample 13 is 1 for a node without prefiltered
+ * coverage, 0 otherwise). Host scenes too. Returns the triangle-hierarchy
+ * node count, or minus a status code. */
+CC_API int64_t cc_scene_coverage(const cc_scene* scene, float* blas27, uint64_t max_blas, float* obj27,
+                                 uint64_t max_obj);
 
 /* cc_sky_visibility flags */
 #define CC_SKY_COMBINE_MAX 1u      /* meshes combine by the maximum, as light cones do (MaskConeKernel::set_sky_combination_max) */

@@ -152,7 +152,97 @@ struct Scene {
   // nodes from first_node, items from first_item, in `movers` order.
   uint32_t first_node = 0, mover_nodes = 0, first_item = 0;
   std::vector<uint32_t> movers;
+  // Prefiltered cones: 27 coverage samples per triangle-hierarchy node and
+  // (instanced scenes) per object-hierarchy node, built on first use.
+  std::vector<float> blas_cov, obj_cov;
+  bool coverage_built = false;
 };
+
+// COVERAGE_SAMPLES and coverage_directions (hierarchy.rs:710-723): directions
+// (i, j, k) in {-1, 0, 1}^3 at index 9(i+1) + 3(j+1) + (k+1), normalized as
+// glam's normalize_or_zero (times 1 / length; zero stays zero).
+constexpr uint32_t COV = 27;
+static void cov_directions(float d[COV][3]) {
+  for (uint32_t n = 0; n < COV; ++n) {
+    const float v[3] = {float(n / 9) - 1.0f, float(n / 3 % 3) - 1.0f, float(n % 3) - 1.0f};
+    const float r = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int k = 0; k < 3; ++k) d[n][k] = (std::isfinite(r) && r > 0.0f) ? v[k] * r : 0.0f;
+  }
+}
+
+// front_area (hierarchy.rs:625-652): bilinear on the sample cube's face,
+// with Rust's lerp (a + (b - a) t).
+static float host_front_area(const float* cov, const float v[3]) {
+  const float ax = std::fabs(v[0]), ay = std::fabs(v[1]), az = std::fabs(v[2]);
+  const int axis = (ay > ax && ay >= az) ? 1 : ((az > ax && az > ay) ? 2 : 0);
+  const float main = axis == 0 ? v[0] : (axis == 1 ? v[1] : v[2]);
+  const float div = axis == 0 ? ax : (axis == 1 ? ay : az);
+  const float s = (axis == 0 ? v[1] : v[0]) / div;
+  const float t = (axis == 2 ? v[1] : v[2]) / div;
+  const int m = main >= 0.0f ? 1 : -1, s0 = s < 0.0f ? -1 : 0, t0 = t < 0.0f ? -1 : 0;
+  const float fs = s - float(s0), ft = t - float(t0);
+  float f[4];
+  for (int c = 0; c < 4; ++c) {
+    const int gs = s0 + (c & 1), gt = t0 + (c >> 1);
+    int i = gs, j = gt, k = m;
+    if (axis == 0) i = m, j = gs, k = gt;
+    else if (axis == 1) i = gs, j = m, k = gt;
+    f[c] = cov[9 * (i + 1) + 3 * (j + 1) + (k + 1)];
+  }
+  auto lerp = [](float a, float b, float u) { return a + (b - a) * u; };
+  return lerp(lerp(f[0], f[1], fs), lerp(f[2], f[3], fs), ft);
+}
+
+// triangle_hierarchy's coverage (hierarchy.rs:546-569) over every mesh's
+// triangle hierarchy, and object_coverage (:661-707) for instanced scenes.
+static void build_coverage(Scene& sc) {
+  if (sc.coverage_built) return;
+  float d[COV][3];
+  cov_directions(d);
+  sc.blas_cov.assign(sc.blas.size() * COV, 0.0f);
+  for (size_t n = sc.blas.size(); n-- > 0;) {
+    float* out = &sc.blas_cov[n * COV];
+    const uint32_t x = sc.blas[n].info[0], count = sc.blas[n].info[1];
+    if (count > 0) {
+      for (uint32_t k = x; k < x + count; ++k) {
+        const float* t = &sc.tris[12 * (size_t)sc.blas_items[k]];
+        const F3 a{t[0], t[1], t[2]}, b{t[4], t[5], t[6]}, c{t[8], t[9], t[10]};
+        const F3 an = cross(b - a, c - a) * 0.5f;
+        for (uint32_t i = 0; i < COV; ++i) out[i] += std::max(an.x * d[i][0] + an.y * d[i][1] + an.z * d[i][2], 0.0f);
+      }
+    } else {
+      for (uint32_t i = 0; i < COV; ++i) out[i] = sc.blas_cov[(size_t)x * COV + i] + sc.blas_cov[((size_t)x + 1) * COV + i];
+    }
+  }
+  if (!sc.xforms.empty()) {
+    std::vector<float> per((size_t)sc.nmeshes * COV, 0.0f);
+    for (uint32_t m = 0; m < sc.nmeshes; ++m) {
+      const uint32_t root = sc.ranges[4 * m + 2], xi = sc.ranges[4 * m + 3];
+      if (root == NONE || xi == NONE) continue;
+      const float* X = &sc.xforms[16 * (size_t)xi];
+      for (uint32_t i = 0; i < COV; ++i) {
+        if (d[i][0] == 0.0f && d[i][1] == 0.0f && d[i][2] == 0.0f) continue;
+        // rotation^T d (glam: columns of the transpose, the rotation's rows, summed in order)
+        const float v[3] = {X[0] * d[i][0] + X[4] * d[i][1] + X[8] * d[i][2],
+                            X[1] * d[i][0] + X[5] * d[i][1] + X[9] * d[i][2],
+                            X[2] * d[i][0] + X[6] * d[i][1] + X[10] * d[i][2]};
+        per[(size_t)m * COV + i] = X[12] * X[12] * host_front_area(&sc.blas_cov[(size_t)root * COV], v);
+      }
+    }
+    sc.obj_cov.assign(sc.nodes.size() * COV, 0.0f);
+    for (size_t n = sc.nodes.size(); n-- > 0;) {
+      float* out = &sc.obj_cov[n * COV];
+      const uint32_t x = sc.nodes[n].info[0], count = sc.nodes[n].info[1];
+      if (count > 0) {
+        for (uint32_t k = x; k < x + count; ++k)
+          for (uint32_t i = 0; i < COV; ++i) out[i] += per[(size_t)sc.items[k] * COV + i];
+      } else {
+        for (uint32_t i = 0; i < COV; ++i) out[i] = sc.obj_cov[(size_t)x * COV + i] + sc.obj_cov[((size_t)x + 1) * COV + i];
+      }
+    }
+  }
+  sc.coverage_built = true;
+}
 
 static void mesh_bounds(const float* tris, uint32_t first, uint32_t count, F3& lo, F3& hi) {
   lo = {FLT_MAX, FLT_MAX, FLT_MAX};
@@ -442,6 +532,8 @@ template <class R> struct Params {
   R wide_extent;
   uint32_t light_cone_cap;
   uint32_t wide_cone_cap;
+  R prefilter = 0;               // prefilter_bins (0: exact cones)
+  bool object_prefilter = true;  // object-level splats in instanced scenes
 };
 
 template <class R> constexpr R NEAR = R(1e-4);
@@ -734,6 +826,117 @@ template <class R> bool cover_triangle(const Scene& s, const Cone<R>& c, Acc<R>&
   return rasterize(c, acc, v0, v1, v2);
 }
 
+// --- Prefiltered cones (:453-574, :1090-1150) ---
+
+// node_front_area (:462-486) over a node's 27 samples, with WGSL's mix
+// (a (1 - t) + b t).
+template <class R> R node_front_area(const float* cov, V3<R> v) {
+  const R ax = std::fabs(v.x), ay = std::fabs(v.y), az = std::fabs(v.z);
+  uint32_t axis = 0;
+  if (ay > ax && ay >= az) axis = 1;
+  else if (az > ax && az > ay) axis = 2;
+  R main, s, t;
+  if (axis == 0) { main = v.x; s = v.y / ax; t = v.z / ax; }
+  else if (axis == 1) { main = v.y; s = v.x / ay; t = v.z / ay; }
+  else { main = v.z; s = v.x / az; t = v.y / az; }
+  const int m = main >= 0 ? 1 : -1, s0 = s < 0 ? -1 : 0, t0 = t < 0 ? -1 : 0;
+  const R fs = s - R(s0), ft = t - R(t0);
+  R f[4];
+  for (int c = 0; c < 4; ++c) {
+    const int gs = s0 + (c & 1), gt = t0 + (c >> 1);
+    int i, j, k;
+    if (axis == 0) { i = m; j = gs; k = gt; }
+    else if (axis == 1) { i = gs; j = m; k = gt; }
+    else { i = gs; j = gt; k = m; }
+    f[c] = R(cov[9 * (i + 1) + 3 * (j + 1) + (k + 1)]);
+  }
+  auto mix = [](R a, R b, R u) { return a * (R(1) - u) + b * u; };
+  return mix(mix(f[0], f[1], fs), mix(f[2], f[3], fs), ft);
+}
+
+// hull8 (:488-511): clockwise convex hull of 8 points by gift wrapping.
+template <class R> Poly2<R> hull8(const V2<R> (&pts)[8]) {
+  int start = 0;
+  for (int k = 1; k < 8; ++k)
+    if (pts[k].x < pts[start].x || (pts[k].x == pts[start].x && pts[k].y < pts[start].y)) start = k;
+  Poly2<R> out;
+  int cur = start;
+  for (;;) {
+    out.v[out.n++] = pts[cur];
+    int next = (cur + 1) % 8;
+    for (int k = 0; k < 8; ++k) {
+      const R ex = pts[next].x - pts[cur].x, ey = pts[next].y - pts[cur].y;
+      const R fx = pts[k].x - pts[cur].x, fy = pts[k].y - pts[cur].y;
+      const R cr = ex * fy - ey * fx;
+      if (cr > 0 || (cr == 0 && fx * fx + fy * fy > ex * ex + ey * ey)) next = k;
+    }
+    cur = next;
+    if (cur == start || out.n >= 8) break;
+  }
+  return out;
+}
+
+// The hull clipped to the square and drawn with weight alpha (:564-573).
+template <class R> bool draw_hull(Acc<R>& acc, const V2<R> (&pts)[8], R alpha) {
+  const R g = R(GRID);
+  Poly2<R> q = hull8(pts);
+  q = clip_line2(q, V2<R>{-1, 0}, R(0));
+  q = clip_line2(q, V2<R>{1, 0}, g);
+  q = clip_line2(q, V2<R>{0, -1}, R(0));
+  q = clip_line2(q, V2<R>{0, 1}, g);
+  if (q.n < 3) return false;
+  for (int i = 0; i < q.n; ++i) {
+    V2<R> a = q.v[i], b = q.v[(i + 1) % q.n];
+    a = {clampv(a.x, R(0), g), clampv(a.y, R(0), g)};
+    b = {clampv(b.x, R(0), g), clampv(b.y, R(0), g)};
+    draw_edge(acc, a, b, alpha);
+  }
+  return true;
+}
+
+// node_cone_test (:519-574): 0 cannot touch, 1 splatted with nothing drawn,
+// 2 splatted and drawn, 3 descend. With prefilter 0 it is may_touch_box.
+template <class R> int node_cone_test(const Cone<R>& c, Acc<R>& acc, const float* cov, V3<R> lo, V3<R> hi,
+                                      R prefilter) {
+  const R g = R(GRID);
+  V2<R> pts[8];
+  R mnx = R(3.4e38), mny = R(3.4e38), mxx = R(-3.4e38), mxy = R(-3.4e38);
+  bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true, below = true;
+  bool inside = prefilter > 0;
+  const R* w = c.window;
+  for (uint32_t k = 0; k < 8; ++k) {
+    V3<R> corner{(k & 1u) ? hi.x : lo.x, (k & 2u) ? hi.y : lo.y, (k & 4u) ? hi.z : lo.z};
+    if (dot(c.horizon, corner - c.apex) >= 0) below = false;
+    const bool in_far = c.far_offset - dot(c.far_normal, corner) >= 0;
+    if (in_far) far_out = false; else inside = false;
+    V3<R> p = to_local(c, corner);
+    if (p.z >= NEAR<R>) near_out = false; else inside = false;
+    if (p.x - w[0] * p.z >= 0) out_u0 = false;
+    if (w[2] * p.z - p.x >= 0) out_u1 = false;
+    if (p.y - w[1] * p.z >= 0) out_v0 = false;
+    if (w[3] * p.z - p.y >= 0) out_v1 = false;
+    if (inside) {
+      const V2<R> q{(p.x / p.z - w[0]) / (w[2] - w[0]) * g, (p.y / p.z - w[1]) / (w[3] - w[1]) * g};
+      pts[k] = q;
+      mnx = std::min(mnx, q.x);
+      mny = std::min(mny, q.y);
+      mxx = std::max(mxx, q.x);
+      mxy = std::max(mxy, q.y);
+    }
+  }
+  if (far_out || near_out || out_u0 || out_u1 || out_v0 || out_v1 || below) return 0;
+  if (!in_bound(c, (lo + hi) * R(0.5), R(0.5) * length(hi - lo))) return 0;
+  if (!inside || std::max(mxx - mnx, mxy - mny) > prefilter) return 3;
+  if (mxx <= 0 || mxy <= 0 || mnx >= g || mny >= g) return 1;
+  const V3<R> e = hi - lo;
+  const V3<R> v = normalize(c.apex - (lo + hi) * R(0.5));
+  const R silhouette = std::fabs(v.x) * e.y * e.z + std::fabs(v.y) * e.x * e.z + std::fabs(v.z) * e.x * e.y;
+  if (silhouette <= R(1e-30)) return 1;
+  const R alpha = node_front_area(cov, v) / silhouette;
+  if (alpha <= 0) return 1;
+  return draw_hull(acc, pts, alpha) ? 2 : 1;
+}
+
 template <class R> inline V3<R> node_lo(const Node& n) { return {R(n.lo[0]), R(n.lo[1]), R(n.lo[2])}; }
 template <class R> inline V3<R> node_hi(const Node& n) { return {R(n.hi[0]), R(n.hi[1]), R(n.hi[2])}; }
 
@@ -743,8 +946,56 @@ template <class R> struct Walk {
   uint32_t cone_work = 0;
   uint32_t cone_cap = NONE;
   bool independent = false;  // sky cones: meshes combine as independent occluders (:819-821)
+  R prefilter = 0;           // prefilter_bins (0: exact cones)
+  bool object_prefilter = false;
   Work work;
 };
+
+// splat_object_node (:1096-1150): an object node small in the cone splatted
+// into the mask as one more mesh (opacity 1 - exp(-front area / silhouette),
+// no whole-bin snap). Returns whether it was splatted (or found empty).
+template <class R> bool splat_object_node(const Scene& s, const Cone<R>& c, uint32_t n, V3<R> lo, V3<R> hi,
+                                          Walk<R>& wk) {
+  if (!wk.object_prefilter || s.obj_cov.empty() || wk.prefilter <= 0) return false;
+  const R g = R(GRID);
+  const R* w = c.window;
+  V2<R> pts[8];
+  R mnx = R(3.4e38), mny = R(3.4e38), mxx = R(-3.4e38), mxy = R(-3.4e38);
+  for (uint32_t k = 0; k < 8; ++k) {
+    V3<R> corner{(k & 1u) ? hi.x : lo.x, (k & 2u) ? hi.y : lo.y, (k & 4u) ? hi.z : lo.z};
+    if (c.far_offset - dot(c.far_normal, corner) < 0) return false;
+    V3<R> p = to_local(c, corner);
+    if (p.z < NEAR<R>) return false;
+    const V2<R> q{(p.x / p.z - w[0]) / (w[2] - w[0]) * g, (p.y / p.z - w[1]) / (w[3] - w[1]) * g};
+    pts[k] = q;
+    mnx = std::min(mnx, q.x);
+    mny = std::min(mny, q.y);
+    mxx = std::max(mxx, q.x);
+    mxy = std::max(mxy, q.y);
+  }
+  if (std::max(mxx - mnx, mxy - mny) > wk.prefilter) return false;
+  if (mxx <= 0 || mxy <= 0 || mnx >= g || mny >= g) return true;
+  const V3<R> e = hi - lo;
+  const V3<R> v = normalize(c.apex - (lo + hi) * R(0.5));
+  const R silhouette = std::fabs(v.x) * e.y * e.z + std::fabs(v.y) * e.x * e.z + std::fabs(v.z) * e.x * e.y;
+  if (silhouette <= R(1e-30)) return true;
+  const R alpha = R(1) - std::exp(-node_front_area(&s.obj_cov[(size_t)n * COV], v) / silhouette);
+  if (alpha <= 0) return true;
+  Acc<R> acc;
+  acc.reset();
+  if (!draw_hull(acc, pts, alpha)) return true;
+  R running = 0;
+  for (uint32_t b = acc.span_lo; b < std::min(acc.span_hi, BINS); ++b) {
+    running += acc.cell[b];
+    const R covered = std::min(std::fabs(running), R(1));
+    if (covered > R(1e-6)) {
+      const R before = wk.cov[b];
+      wk.cov[b] = wk.independent ? R(1) - (R(1) - before) * (R(1) - covered) : std::max(before, covered);
+      if (before < R(1) && wk.cov[b] >= R(1)) wk.full++;
+    }
+  }
+  return true;
+}
 
 constexpr int STACK = 64;
 
@@ -788,7 +1039,10 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
         wk.cone_work++;
         const Node& node = s.blas[n];
         wk.work.blas_nodes++;
-        if (!may_touch_box(c, node_lo<R>(node), node_hi<R>(node))) continue;
+        const float* cov = s.blas_cov.empty() ? nullptr : &s.blas_cov[(size_t)n * COV];
+        const int test = node_cone_test(c, acc, cov, node_lo<R>(node), node_hi<R>(node), wk.prefilter);
+        if (test == 2) touched = true;
+        if (test != 3) continue;
         if (node.info[1] > 0) {
           wk.cone_work += node.info[1];
           for (uint32_t k = node.info[0]; k < node.info[0] + node.info[1]; ++k)
@@ -841,6 +1095,9 @@ template <class R> void scene_coverage(const Scene& s, const Cone<R>& c, Walk<R>
       const Node& node = s.nodes[n];
       wk.work.object_nodes++;
       if (!may_touch_box(c, node_lo<R>(node), node_hi<R>(node))) continue;
+      // info.z 1: no prefiltered coverage (the root over movers and the
+      // movers' subtree, whose boxes change).
+      if (node.info[2] == 0 && splat_object_node(s, c, n, node_lo<R>(node), node_hi<R>(node), wk)) continue;
       if (node.info[1] > 0) {
         for (uint32_t k = node.info[0]; k < node.info[0] + node.info[1]; ++k)
           add_mesh_coverage(s, c, s.items[k], wk, hierarchy);
@@ -1170,6 +1427,8 @@ template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> norma
   Walk<R> wk;
   std::fill(wk.cov, wk.cov + BINS, R(0));
   wk.cone_cap = lc.wide_window ? prm.wide_cone_cap : prm.light_cone_cap;
+  wk.prefilter = prm.prefilter;
+  wk.object_prefilter = prm.object_prefilter;
   if (traced) scene_coverage(s, lc.c, wk, prm.hierarchy);
   if (wk.cone_work >= wk.cone_cap && traced) wk.work.flags |= 1;
   if (traced && wk.cone_work >= wk.cone_cap && lc.wide_window && !lc.wide_clipped) {
@@ -1240,12 +1499,15 @@ template <class R> bool sky_face(uint32_t f, V3<R> apex, V3<R> normal, bool hori
 // coverage (no walk cap; independent occluders unless `combine_max`) and its
 // light per unit sky radiance.
 template <class R> R sky_face_irradiance(const Scene& s, uint32_t f, V3<R> point, V3<R> normal, uint32_t hierarchy,
-                                         bool combine_max, bool horizon_cull, R* cov_out, Work* work) {
+                                         bool combine_max, bool horizon_cull, R prefilter, bool object_prefilter,
+                                         R* cov_out, Work* work) {
   Cone<R> c;
   const bool above = sky_face(f, point, normal, horizon_cull, c);
   Walk<R> wk;
   std::fill(wk.cov, wk.cov + BINS, R(0));
   wk.independent = !combine_max;
+  wk.prefilter = prefilter;
+  wk.object_prefilter = object_prefilter;
   if (above) scene_coverage(s, c, wk, hierarchy);
   if (cov_out) std::copy(wk.cov, wk.cov + BINS, cov_out);
   if (work) *work = wk.work;
@@ -1780,6 +2042,15 @@ uint64_t oracle_scene_transforms(void* sp, float* out) {
 
 void oracle_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
 
+// The prefiltered cones' coverage samples (27 per node) of the triangle-
+// hierarchy nodes and, for instanced scenes, the object-hierarchy nodes.
+void oracle_scene_coverage(void* sp, float* blas27, float* obj27) {
+  Scene* s = static_cast<Scene*>(sp);
+  build_coverage(*s);
+  if (blas27) std::copy(s->blas_cov.begin(), s->blas_cov.end(), blas27);
+  if (obj27) std::copy(s->obj_cov.begin(), s->obj_cov.end(), obj27);
+}
+
 // Sizes of the flattened arrays: ntris, nmeshes, nblas, nblas_items, nnodes, nitems.
 void oracle_scene_sizes(void* sp, uint64_t* out6) {
   Scene* s = static_cast<Scene*>(sp);
@@ -1806,6 +2077,8 @@ struct OracleParams {
   float wide_extent;
   uint32_t light_cone_cap;
   uint32_t wide_cone_cap;
+  float prefilter;            // prefilter_bins (0: exact cones)
+  uint32_t object_prefilter;  // object-level splats (instanced scenes)
 };
 
 // Visibility of cones (light l, receiver p), cone id c = l * npoints + p,
@@ -1821,9 +2094,11 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
   if (!s || !prm_in) return 1;
   uint64_t total = npoints * nlights;
   uint64_t n = cone_ids ? ncones : total;
+  if (prm_in->prefilter > 0.0f) build_coverage(*s);
   auto run = [&](auto zero) {
     using R = decltype(zero);
-    Params<R> prm{prm_in->hierarchy, R(prm_in->wide_extent), prm_in->light_cone_cap, prm_in->wide_cone_cap};
+    Params<R> prm{prm_in->hierarchy, R(prm_in->wide_extent), prm_in->light_cone_cap, prm_in->wide_cone_cap,
+                  R(prm_in->prefilter), prm_in->object_prefilter != 0};
     parallel_for(n, threads, [&](uint64_t i) {
       uint64_t c = cone_ids ? cone_ids[i] : i;
       uint64_t l = c / npoints, p = c % npoints;
@@ -1865,10 +2140,11 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
 // npoints + point: its light, FULL/ANY words, coverage and work counters.
 // flags: 1 combine by the maximum, 2 no horizon cull.
 int oracle_sky_visibility(void* sp, const float* receivers, uint64_t npoints, uint32_t hierarchy, uint32_t flags,
-                          int precision, float* irradiance, float* face_light, uint32_t* full, uint32_t* any,
-                          float* partial, uint32_t* work, int threads) {
+                          float prefilter, int precision, float* irradiance, float* face_light, uint32_t* full,
+                          uint32_t* any, float* partial, uint32_t* work, int threads) {
   Scene* s = static_cast<Scene*>(sp);
   if (!s || !irradiance) return 1;
+  if (prefilter > 0.0f) build_coverage(*s);
   auto run = [&](auto zero) {
     using R = decltype(zero);
     parallel_for(npoints, threads, [&](uint64_t p) {
@@ -1878,7 +2154,8 @@ int oracle_sky_visibility(void* sp, const float* receivers, uint64_t npoints, ui
       for (uint32_t f = 0; f < 6; ++f) {
         R cov[BINS];
         Work wk;
-        const R v = sky_face_irradiance(*s, f, point, normal, hierarchy, (flags & 1u) != 0, (flags & 2u) == 0, cov, &wk);
+        const R v = sky_face_irradiance(*s, f, point, normal, hierarchy, (flags & 1u) != 0, (flags & 2u) == 0,
+                                        R(prefilter), (flags & 4u) == 0, cov, &wk);
         total += v;
         const uint64_t c = f * npoints + p;
         if (face_light) face_light[c] = float(v);

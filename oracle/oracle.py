@@ -19,7 +19,7 @@ NODE_DTYPE = np.dtype([("lo", "<f4", 4), ("hi", "<f4", 4), ("info", "<u4", 4)])
 
 class _Params(C.Structure):
     _fields_ = [("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
-                ("wide_cone_cap", C.c_uint32)]
+                ("wide_cone_cap", C.c_uint32), ("prefilter", C.c_float), ("object_prefilter", C.c_uint32)]
 
 
 def load():
@@ -36,8 +36,9 @@ def load():
         lib.oracle_scene_arrays.argtypes = [P, P, P, P, P, P]
         lib.oracle_visibility.restype = I
         lib.oracle_visibility.argtypes = [P, P, U64, P, U32, C.POINTER(_Params), P, U64, I, P, P, P, P, P, P, P, I]
+        lib.oracle_scene_coverage.argtypes = [P, P, P]
         lib.oracle_sky_visibility.restype = I
-        lib.oracle_sky_visibility.argtypes = [P, P, U64, U32, U32, I, P, P, P, P, P, P, I]
+        lib.oracle_sky_visibility.argtypes = [P, P, U64, U32, U32, C.c_float, I, P, P, P, P, P, P, I]
         lib.oracle_cpu_masked.restype = I
         lib.oracle_cpu_masked.argtypes = [P, P, U64, P, I, P, P, P, I]
         lib.oracle_disk_table.argtypes = [P]
@@ -130,7 +131,8 @@ class OracleScene:
 
     def visibility(self, receivers: np.ndarray, lights: np.ndarray, hierarchy: int = 2, precision: int = 4,
                    cone_ids: np.ndarray | None = None, threads: int | None = None, wide_extent: float = 8.0,
-                   light_cone_cap: int = 4096, wide_cone_cap: int = 512, partial: bool = True) -> dict:
+                   light_cone_cap: int = 4096, wide_cone_cap: int = 512, partial: bool = True, prefilter: float = 0.0,
+                   object_prefilter: bool = True) -> dict:
         """Per-cone results (cone c = light * npoints + point), for all cones or
         the `cone_ids` subset (outputs in subset order)."""
         rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
@@ -144,7 +146,7 @@ class OracleScene:
         frac = np.zeros(n, np.float32)
         work = np.zeros((n, 4), np.uint32)
         unsh = np.zeros(n, np.float32)
-        prm = _Params(hierarchy, wide_extent, light_cone_cap, wide_cone_cap)
+        prm = _Params(hierarchy, wide_extent, light_cone_cap, wide_cone_cap, prefilter, 1 if object_prefilter else 0)
         rc = load().oracle_visibility(self._h, _p(rec), rec.shape[0], _p(lig), lig.shape[0], C.byref(prm), _p(ids),
                                       0 if ids is None else len(ids), precision, _p(full), _p(any_), _p(part),
                                       _p(irr), _p(frac), _p(work), _p(unsh), threads or default_threads())
@@ -153,8 +155,16 @@ class OracleScene:
         return dict(full=full.view(np.uint64).reshape(n), any=any_.view(np.uint64).reshape(n), partial=part,
                     irradiance=irr, fraction=frac, work=work, unshadowed=unsh)
 
+    def coverage(self) -> tuple:
+        """(triangle-hierarchy nodes' samples (n, 27), object nodes' (m, 27) or None)."""
+        sizes = self.sizes()
+        blas = np.zeros((sizes["nblas"], 27), np.float32)
+        obj = np.zeros((sizes["nnodes"], 27), np.float32) if getattr(self, "instances", None) is not None else None
+        load().oracle_scene_coverage(self._h, _p(blas), _p(obj))
+        return blas, obj
+
     def sky_visibility(self, receivers: np.ndarray, hierarchy: int = 2, flags: int = 0, precision: int = 4,
-                       threads: int | None = None, faces: bool = True) -> dict:
+                       threads: int | None = None, faces: bool = True, prefilter: float = 0.0) -> dict:
         """Sky cones (six cube faces per receiver): irradiance per unit sky
         radiance per receiver, and per face cone c = face * npoints + point its
         light, FULL/ANY words, coverage and work counters. flags: 1 combine
@@ -168,7 +178,8 @@ class OracleScene:
                        any=np.zeros((6 * n, 2), np.uint32), partial=np.zeros((6 * n, 64), np.float32),
                        work=np.zeros((6 * n, 4), np.uint32))
         g = out.get
-        rc = load().oracle_sky_visibility(self._h, _p(rec), n, hierarchy, flags, precision, _p(irr), _p(g("face_light")),
+        rc = load().oracle_sky_visibility(self._h, _p(rec), n, hierarchy, flags, prefilter, precision, _p(irr),
+                                          _p(g("face_light")),
                                           _p(g("full")), _p(g("any")), _p(g("partial")), _p(g("work")),
                                           threads or default_threads())
         if rc != 0:
