@@ -488,10 +488,11 @@ int cc_scene_primary_hits(const cc_scene* s, const float camera[10], uint32_t wi
 }  // extern "C"
 
 // cc_visibility's body; `sky` (kSkyCones and its flags) makes the cones the
-// receivers' six sky faces (nlights = 6, no lights).
-static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
-                           const float* lights, uint32_t nlights, const cc_options* opt_in, const cc_outputs* out,
-                           void* stream_in, uint32_t sky) {
+// receivers' six sky faces (nlights = 6, no lights); `cones` (device, with
+// its count in device memory) walks only the listed cones, in that order.
+int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                             const float* lights, uint32_t nlights, const cc_options* opt_in, const cc_outputs* out,
+                             void* stream_in, uint32_t sky, const uint32_t* cones, const uint32_t* cones_count) {
   if (!ctx || !scene || !out) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
   if ((npoints && !receivers) || (nlights && !lights && !sky)) return fail(CC_ERR_INVALID, "null inputs");
@@ -518,6 +519,8 @@ static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* 
   q.wide_cone_cap = opt.wide_cone_cap;
   q.sky = sky;
   q.prefilter = opt.prefilter;
+  q.cones = cones;
+  q.cones_count = cones_count;
   cc::DevScene sd = scene->dev();
   if (opt.prefilter > 0.0f) {
     int rc2 = ensure_coverage(const_cast<cc_scene*>(scene));
@@ -572,7 +575,7 @@ static int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* 
   CC_CUDA(cudaMemsetAsync(counters, 0, cc::kCounterWords * sizeof(uint32_t), stream), "counter reset");
   // Walk the points in Morton order of their positions (coherent packets).
   q.order = nullptr;
-  if (!(opt.flags & CC_KEEP_ORDER) && npoints > 64 && !scene->flat.nodes.empty()) {
+  if (!(opt.flags & CC_KEEP_ORDER) && !cones && npoints > 64 && !scene->flat.nodes.empty()) {
     CC_CUDA(ctx->order.reserve(npoints * sizeof(uint32_t)), "walk order");
     const size_t need = cc::walk_order_scratch_bytes(npoints);
     CC_CUDA(ctx->sort_scratch.reserve(need), "walk order scratch");
@@ -627,7 +630,8 @@ extern "C" {
 int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
                   const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                   void* stream) {
-  return visibility_impl(ctx, scene, receivers, npoints, lights, nlights, opt, out, stream, 0u);
+  return cc_host::visibility_impl(ctx, scene, receivers, npoints, lights, nlights, opt, out, stream, 0u, nullptr,
+                                  nullptr);
 }
 
 int64_t cc_scene_coverage(const cc_scene* scene, float* blas27, uint64_t max_blas, float* obj27, uint64_t max_obj) {
@@ -690,7 +694,7 @@ int cc_sky_visibility(cc_context* ctx, const cc_scene* scene, const float* recei
   }
   cc_options vo = opt;
   vo.flags |= CC_DEVICE_POINTERS;
-  rc = visibility_impl(ctx, scene, d_rec, npoints, nullptr, 6, &vo, &fo, stream, sky);
+  rc = cc_host::visibility_impl(ctx, scene, d_rec, npoints, nullptr, 6, &vo, &fo, stream, sky, nullptr, nullptr);
   if (rc) return rc;
   if (npoints) {
     sum_sky_faces<<<(unsigned)((npoints + 255) / 256), 256, 0, stream>>>(fo.irradiance, npoints, d_sum);

@@ -47,6 +47,12 @@ struct DevBuf {
 
 int set_device(cc_context* ctx);
 
+// cc_visibility's body (capi.cu): `sky` makes the cones sky faces (0: light
+// cones); `cones` / `cones_count` (device, nullable) walk only listed cones.
+int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                    const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
+                    void* stream, uint32_t sky, const uint32_t* cones, const uint32_t* cones_count);
+
 }  // namespace cc_host
 
 struct cc_context {

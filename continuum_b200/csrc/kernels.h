@@ -32,6 +32,11 @@ struct DevQuery {
   // Prefiltering cones: nodes projecting to at most this many bins are
   // splatted (0: exact cones). Hierarchy level 2 only.
   float prefilter = 0.0f;
+  // A cone list (null: every cone): slot s walks cone cones[s] for s below
+  // *cones_count (device memory), in the list's order; outputs stay indexed
+  // by cone (light * npoints + point).
+  const uint32_t* cones = nullptr;
+  const uint32_t* cones_count = nullptr;
 };
 constexpr uint32_t kSkyCones = 1u;
 constexpr uint32_t kSkyCombineMax = 2u;      // combine meshes by the maximum, as light cones do (a diagnostic)

@@ -13,6 +13,9 @@
 
 #include <cfloat>
 #include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
 
 #include "capi_internal.h"
 
@@ -160,25 +163,14 @@ __global__ void stale_kernel(const float4* __restrict__ receivers, uint64_t npoi
   if (hit) atomicAdd(count, 1ull);
 }
 
-__global__ void gather_points(const float4* __restrict__ receivers, const uint32_t* __restrict__ idx, uint64_t n,
-                              float4* __restrict__ out) {
+// Moved objects' transforms into place: transform index in slot[i].x (its
+// bits), the 4 rows at rows[4 i ..].
+__global__ void scatter_xforms(const float4* __restrict__ slot, const float4* __restrict__ rows, uint64_t n,
+                               float4* __restrict__ xforms) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint32_t p = idx[i];
-  out[2 * i] = receivers[2 * p];
-  out[2 * i + 1] = receivers[2 * p + 1];
-}
-
-__global__ void scatter_results(const uint32_t* __restrict__ idx, uint64_t n, uint64_t base, const uint2* full_in,
-                                const uint2* any_in, const float* irr_in, const float* frac_in, uint2* full,
-                                uint2* any, float* irr, float* frac) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t c = base + idx[i];
-  if (full) full[c] = full_in[i];
-  if (any) any[c] = any_in[i];
-  if (irr) irr[c] = irr_in[i];
-  if (frac) frac[c] = frac_in[i];
+  const uint32_t x = __float_as_uint(slot[i].x);
+  for (int r = 0; r < 4; ++r) xforms[4 * (size_t)x + r] = rows[4 * i + r];
 }
 
 __global__ void iota_kernel(uint32_t* out, uint64_t n) {
@@ -186,7 +178,30 @@ __global__ void iota_kernel(uint32_t* out, uint64_t n) {
   if (i < n) out[i] = (uint32_t)i;
 }
 
+// Slot k = l * npoints + i walks cone l * npoints + order[i] (the points'
+// walk order within each light); its flag is that cone's staleness.
+__global__ void stale_in_order(const uint32_t* __restrict__ order, const uint8_t* __restrict__ stale, uint64_t npoints,
+                               uint64_t ncones, uint32_t* __restrict__ perm, uint8_t* __restrict__ flags) {
+  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncones) return;
+  const uint64_t l = k / npoints;
+  const uint32_t c = (uint32_t)(l * npoints + order[k - l * npoints]);
+  perm[k] = c;
+  flags[k] = stale[c];
+}
+
 // A hierarchy over boxes (two per leaf), for the region tables.
+inline uint32_t float_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+inline float bits_float(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
 struct BoxTree {
   std::vector<float4> nodes;
   std::vector<uint32_t> items;
@@ -265,11 +280,32 @@ int cc_scene_move(cc_scene* s, const cc_instance* placements, uint32_t n, float*
   if (!s->ctx) return CC_OK;
   int rc = set_device(s->ctx);
   if (rc) return rc;
-  // The movers' transforms, the root, the movers' subtree and their items.
+  // The movers' transforms (gathered, sent at once and scattered into place
+  // on the device), the root, the movers' subtree and their items.
   const cc::MoverTree& t = f.movers;
-  for (uint32_t m : t.objects) {
-    const uint32_t x = f.ranges[4 * m + 3];
-    CC_CUDA(cudaMemcpy(s->xforms + 4 * (size_t)x, &f.xforms[16 * (size_t)x], 64, cudaMemcpyHostToDevice), "move transforms");
+  if (!t.objects.empty()) {
+    const size_t nm = t.objects.size();
+    std::vector<float4> packed(5 * nm);
+    for (size_t i = 0; i < nm; ++i) {
+      const uint32_t x = f.ranges[4 * t.objects[i] + 3];
+      float xi;
+      std::memcpy(&xi, &x, 4);
+      packed[i] = make_float4(xi, 0.f, 0.f, 0.f);
+      for (int r = 0; r < 4; ++r) {
+        const float* row = &f.xforms[16 * (size_t)x + 4 * r];
+        packed[nm + 4 * i + r] = make_float4(row[0], row[1], row[2], row[3]);
+      }
+    }
+    float4* d = nullptr;
+    CC_CUDA(cudaMalloc(&d, packed.size() * sizeof(float4)), "move transforms");
+    cudaError_t e = cudaMemcpy(d, packed.data(), packed.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      cc::scatter_xforms<<<(unsigned)((nm + 127) / 128), 128>>>(d, d + nm, nm, s->xforms);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "move transforms");
   }
   auto put_nodes = [&](uint32_t first, uint32_t count) -> int {
     std::vector<float4> packed(2 * (size_t)count);
@@ -314,14 +350,17 @@ int cc_stale_cones(cc_context* ctx, const cc_scene* scene, const float* receiver
   std::vector<float4> nodes;
   std::vector<uint32_t> roots(nlights, cc::kNone), items, region_box;
   std::vector<float> region_boxes;
-  for (uint32_t l = 0; l < nlights; ++l) {
+  // Each light's regions and their hierarchy on a host thread of its own
+  // (numbered from 0), then joined in light order, renumbered.
+  std::vector<std::vector<cc::Box3>> regions(nlights);
+  std::vector<std::vector<uint32_t>> which(nlights);
+  std::vector<cc::BoxTree> trees(nlights);
+  auto per_light = [&](uint32_t l) {
     const cc::Box3 lb = cc::light_box(lights16 + 16 * (size_t)l);
     for (int k = 0; k < 3; ++k) {
       lboxes[6 * l + k] = lb.lo[k];
       lboxes[6 * l + 3 + k] = lb.hi[k];
     }
-    std::vector<cc::Box3> regions;
-    std::vector<uint32_t> which;
     for (uint32_t b = 0; b < 2 * nmovers; ++b) {
       cc::Box3 m, r;
       for (int k = 0; k < 3; ++k) {
@@ -329,21 +368,35 @@ int cc_stale_cones(cc_context* ctx, const cc_scene* scene, const float* receiver
         m.hi[k] = boxes[6 * b + 3 + k];
       }
       if (cc::shadow_region(m, lb, sbox, r)) {
-        regions.push_back(r);
-        which.push_back(b);
+        regions[l].push_back(r);
+        which[l].push_back(b);
       }
     }
-    if (regions.empty()) continue;
-    cc::BoxTree tree;
+    if (!regions[l].empty()) cc::box_tree(regions[l], 0, 0, trees[l]);
+  };
+  {
+    std::vector<std::thread> pool;
+    for (uint32_t l = 1; l < nlights; ++l) pool.emplace_back(per_light, l);
+    if (nlights) per_light(0);
+    for (std::thread& th : pool) th.join();
+  }
+  for (uint32_t l = 0; l < nlights; ++l) {
+    if (regions[l].empty()) continue;
     const uint32_t node_base = (uint32_t)(nodes.size() / 2);
     const uint32_t item_base = (uint32_t)items.size();
-    cc::box_tree(regions, node_base, item_base, tree);
     roots[l] = node_base;
-    nodes.insert(nodes.end(), tree.nodes.begin(), tree.nodes.end());
+    std::vector<float4>& tn = trees[l].nodes;
+    for (size_t i = 0; i < tn.size(); i += 2) {
+      uint32_t a = cc::float_bits(tn[i].w), b = cc::float_bits(tn[i + 1].w);
+      a += b == 0 ? node_base : item_base;  // interior: left child; leaf: first item
+      tn[i].w = cc::bits_float(a);
+    }
+    nodes.insert(nodes.end(), tn.begin(), tn.end());
     const uint32_t region_base = (uint32_t)region_box.size();
-    for (uint32_t k : tree.items) items.push_back(region_base + k);
-    region_box.insert(region_box.end(), which.begin(), which.end());
-    for (const cc::Box3& r : regions) region_boxes.insert(region_boxes.end(), {r.lo[0], r.lo[1], r.lo[2], r.hi[0], r.hi[1], r.hi[2]});
+    for (uint32_t k : trees[l].items) items.push_back(region_base + k);
+    region_box.insert(region_box.end(), which[l].begin(), which[l].end());
+    for (const cc::Box3& r : regions[l])
+      region_boxes.insert(region_boxes.end(), {r.lo[0], r.lo[1], r.lo[2], r.hi[0], r.hi[1], r.hi[2]});
   }
   // Tables to the device (one allocation, freed after the call).
   auto bytes_of = [](size_t n, size_t each) { return (n * each + 255) & ~size_t(255); };
@@ -392,69 +445,73 @@ int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const float* re
   if (!ctx || !scene || !out || (npoints && !receivers) || (nlights && !lights) || !stale)
     return fail(CC_ERR_INVALID, "null argument");
   if (out->partial || out->work) return fail(CC_ERR_INVALID, "an update writes full, any, irradiance and fraction only");
+  if (scene->ctx != ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   int rc = set_device(ctx);
   if (rc) return rc;
   cudaStream_t stream = stream_in ? (cudaStream_t)stream_in : ctx->stream;
-  // Per light: the stale points' indices (ordered), their receivers gathered,
-  // their cones solved, the results scattered to their cones.
-  uint32_t* seq = nullptr;
-  uint32_t* idx = nullptr;
-  uint32_t* nsel = nullptr;
-  float4* gathered = nullptr;
-  uint8_t* tmp = nullptr;
-  void* sel_temp = nullptr;
+  const uint64_t ncones = npoints * (uint64_t)nlights;
+  if (ncones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one call");
+  if (recomputed) *recomputed = 0;
+  if (ncones == 0) return CC_OK;
+  // The stale cones of every light as one list, each light's in the walk
+  // order (Morton order of the points), so one launch walks them all in
+  // coherent packets and writes each result at its own cone.
+  uint32_t* perm = nullptr;
+  uint8_t* flags = nullptr;
+  uint32_t* list = nullptr;
+  uint32_t* count = nullptr;
+  uint32_t* order = nullptr;
+  void* temp = nullptr;
   size_t sel_bytes = 0;
   cub::DeviceSelect::Flagged(nullptr, sel_bytes, (const uint32_t*)nullptr, (const uint8_t*)nullptr, (uint32_t*)nullptr,
-                             (uint32_t*)nullptr, (int)npoints);
-  cudaError_t e = cudaMalloc(&seq, std::max<uint64_t>(npoints, 1) * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&idx, std::max<uint64_t>(npoints, 1) * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&nsel, 4);
-  if (e == cudaSuccess) e = cudaMalloc(&gathered, std::max<uint64_t>(npoints, 1) * 32);
-  if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<uint64_t>(npoints, 1) * 24);
-  if (e == cudaSuccess) e = cudaMalloc(&sel_temp, std::max<size_t>(sel_bytes, 256));
-  uint64_t total = 0;
+                             (uint32_t*)nullptr, (int)ncones);
+  const size_t sort_bytes = cc::walk_order_scratch_bytes(npoints);
+  cudaError_t e = cudaMalloc(&perm, ncones * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&flags, ncones);
+  if (e == cudaSuccess) e = cudaMalloc(&list, ncones * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&count, 4);
+  if (e == cudaSuccess) e = cudaMalloc(&order, npoints * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&temp, std::max<size_t>(std::max(sel_bytes, sort_bytes), 256));
   const unsigned threads = 256;
-  if (e == cudaSuccess && npoints) {
-    cc::iota_kernel<<<(unsigned)((npoints + threads - 1) / threads), threads, 0, stream>>>(seq, npoints);
+  if (e == cudaSuccess) {
+    if (npoints > 64 && !scene->flat.nodes.empty()) {
+      e = cc::walk_order(reinterpret_cast<const float4*>(receivers), npoints, scene->flat.nodes[0].lo,
+                         scene->flat.nodes[0].hi, temp, std::max(sel_bytes, sort_bytes), order, stream);
+    } else {
+      cc::iota_kernel<<<(unsigned)((npoints + threads - 1) / threads), threads, 0, stream>>>(order, npoints);
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) {
+    cc::stale_in_order<<<(unsigned)((ncones + threads - 1) / threads), threads, 0, stream>>>(order, stale, npoints,
+                                                                                             ncones, perm, flags);
     e = cudaGetLastError();
   }
-  for (uint32_t l = 0; l < nlights && e == cudaSuccess && rc == CC_OK && npoints; ++l) {
-    size_t bytes = sel_bytes;
-    e = cub::DeviceSelect::Flagged(sel_temp, bytes, seq, stale + (size_t)l * npoints, idx, nsel, (int)npoints, stream);
-    uint32_t n = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&n, nsel, 4, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess || n == 0) continue;
-    total += n;
-    cc::gather_points<<<(n + threads - 1) / threads, threads, 0, stream>>>(reinterpret_cast<const float4*>(receivers),
-                                                                            idx, n, gathered);
-    cc_outputs o{};
-    o.full = reinterpret_cast<uint32_t*>(tmp);
-    o.any = reinterpret_cast<uint32_t*>(tmp + 8 * (size_t)n);
-    o.irradiance = reinterpret_cast<float*>(tmp + 16 * (size_t)n);
-    o.fraction = reinterpret_cast<float*>(tmp + 20 * (size_t)n);
+  size_t bytes = std::max(sel_bytes, sort_bytes);
+  if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(temp, bytes, perm, flags, list, count, (int)ncones, stream);
+  if (e == cudaSuccess) {
     cc_options lo = opt;
     lo.flags |= CC_DEVICE_POINTERS;
-    rc = cc_visibility(ctx, scene, reinterpret_cast<const float*>(gathered), n, lights + 16 * (size_t)l, 1, &lo, &o,
-                       stream);
-    if (rc) break;
-    cc::scatter_results<<<(n + threads - 1) / threads, threads, 0, stream>>>(
-        idx, n, (uint64_t)l * npoints, reinterpret_cast<const uint2*>(o.full), reinterpret_cast<const uint2*>(o.any),
-        o.irradiance, o.fraction, reinterpret_cast<uint2*>(out->full), reinterpret_cast<uint2*>(out->any),
-        out->irradiance, out->fraction);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the scratch is reused by the next light
+    cc_outputs o{};
+    o.full = out->full;
+    o.any = out->any;
+    o.irradiance = out->irradiance;
+    o.fraction = out->fraction;
+    rc = cc_host::visibility_impl(ctx, scene, receivers, npoints, lights, nlights, &lo, &o, stream, 0u, list, count);
   }
-  cudaFree(seq);
-  cudaFree(idx);
-  cudaFree(nsel);
-  cudaFree(gathered);
-  cudaFree(tmp);
-  cudaFree(sel_temp);
+  uint32_t n = 0;
+  if (e == cudaSuccess && rc == CC_OK) e = cudaMemcpyAsync(&n, count, 4, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess && rc == CC_OK) e = cudaStreamSynchronize(stream);
+  cudaFree(perm);
+  cudaFree(flags);
+  cudaFree(list);
+  cudaFree(count);
+  cudaFree(order);
+  cudaFree(temp);
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "visibility update");
-  if (recomputed) *recomputed = total;
+  if (recomputed) *recomputed = n;
   return CC_OK;
 }

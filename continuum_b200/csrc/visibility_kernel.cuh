@@ -768,7 +768,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
   ws->span_lo[lane] = 68u;
   ws->span_hi[lane] = 0u;
 
-  const uint64_t plain_cones = q_plain.npoints * (uint64_t)q_plain.nlights;
+  const uint64_t plain_cones =
+      q_plain.cones ? (uint64_t)*q_plain.cones_count : q_plain.npoints * (uint64_t)q_plain.nlights;
   uint64_t npackets;
   if (list) npackets = (uint64_t)min(*list_count, o.redo_capacity);  // one cone per packet
   else npackets = kBatch ? batch.packets : (plain_cones + pw - 1) / pw;
@@ -818,6 +819,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     if (valid) {
       if (list) {
         c = listed - cone_start;
+      } else if (q.cones) {
+        c = __ldg(&q.cones[slot]);
       } else if (q.order) {
         const uint64_t light_base = (slot / q.npoints) * q.npoints;
         c = light_base + __ldg(&q.order[slot - light_base]);
