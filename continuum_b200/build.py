@@ -15,7 +15,7 @@ LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libcontinuum_cuda.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["visibility.cu", "visibility_splat.cu", "order.cu", "capi.cu", "batch.cu", "server.cu", "movers.cu", "cache.cu", "static_scratch.cu", "bvh.cpp",
+SOURCES = ["visibility.cu", "visibility_splat.cu", "visibility_split.cu", "order.cu", "capi.cu", "batch.cu", "server.cu", "movers.cu", "cache.cu", "static_scratch.cu", "bvh.cpp",
            "raycast.cpp", "cache_plan.cpp"]
 # The cone geometry is evaluated without fused multiply-adds: the reference's
 # clip and cull decisions are ill-conditioned in f32 for receivers lifted
@@ -23,7 +23,7 @@ SOURCES = ["visibility.cu", "visibility_splat.cu", "order.cu", "capi.cu", "batch
 # and contracting a*b+c there changes which side a vertex falls on. Plain
 # IEEE multiplies and adds (with IEEE division and square root, nvcc's
 # defaults) reproduce the reference arithmetic's rounding.
-PER_SOURCE = {"visibility.cu": ["-fmad=false"], "visibility_splat.cu": ["-fmad=false"]}
+PER_SOURCE = {"visibility.cu": ["-fmad=false"], "visibility_splat.cu": ["-fmad=false"], "visibility_split.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-fvisibility=hidden",
               "--cudart", "static", "-Xptxas", "-warn-spills"]

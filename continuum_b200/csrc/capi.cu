@@ -274,7 +274,8 @@ int cc_context_destroy(cc_context* ctx) {
   if (!ctx) return CC_OK;
   cudaSetDevice(ctx->device);
   for (DevBuf* b : {&ctx->receivers, &ctx->lights, &ctx->full, &ctx->any, &ctx->partial, &ctx->irradiance,
-                    &ctx->fraction, &ctx->work, &ctx->redo, &ctx->order, &ctx->sort_scratch, &ctx->counters})
+                    &ctx->fraction, &ctx->work, &ctx->redo, &ctx->order, &ctx->sort_scratch, &ctx->records, &ctx->masks,
+                    &ctx->counters})
     b->release();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -573,6 +574,14 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
     o.redo_capacity = (uint32_t)std::max<uint64_t>(ncones, 1);
   }
   CC_CUDA(cudaMemsetAsync(counters, 0, cc::kCounterWords * sizeof(uint32_t), stream), "counter reset");
+  if (!sky && opt.prefilter <= 0.0f) {
+    // The split path's scratch: one chunk of cone records and masks.
+    const uint64_t slots = std::max<uint64_t>(std::min<uint64_t>(ncones, cc::kSplitChunk), 1);
+    CC_CUDA(ctx->records.reserve(slots * sizeof(cc::ConeRecord)), "cone records");
+    CC_CUDA(ctx->masks.reserve(slots * 256), "cone masks");
+    q.records = static_cast<const cc::ConeRecord*>(ctx->records.ptr);
+    o.cov_out = static_cast<float*>(ctx->masks.ptr);
+  }
   // Walk the points in Morton order of their positions (coherent packets).
   q.order = nullptr;
   if (!(opt.flags & CC_KEEP_ORDER) && !cones && npoints > 64 && !scene->flat.nodes.empty()) {
@@ -784,6 +793,9 @@ int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t
             "walk order");
     q.order = order;
   }
+  // The split path's records and masks, over the sort scratch (used up by now).
+  q.records = reinterpret_cast<const cc::ConeRecord*>(scratch + cc::kStaticRecordsOffset);
+  o.cov_out = reinterpret_cast<float*>(scratch + cc::kStaticMasksOffset);
   CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
                                 nullptr),
           "visibility launch");

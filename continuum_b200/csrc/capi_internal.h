@@ -65,6 +65,8 @@ struct cc_context {
   DevBuf redo;      // redo list
   DevBuf order;     // walk order of the points
   DevBuf sort_scratch;
+  DevBuf records;   // the split path's cone records, one chunk
+  DevBuf masks;     // the split path's masks (64 floats a slot), one chunk
   DevBuf counters;  // [redo count, error word]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Kernel timing: three events per visibility call (before the packet pass,

@@ -37,7 +37,28 @@ struct DevQuery {
   // by cone (light * npoints + point).
   const uint32_t* cones = nullptr;
   const uint32_t* cones_count = nullptr;
+  // The split plain path (exact light cones): slots slot_base .. + slot_count
+  // of this call's walk, each set up beforehand in records[slot - slot_base].
+  const struct ConeRecord* records = nullptr;
+  uint64_t slot_base = 0;
+  uint64_t slot_count = 0;
 };
+
+// A light cone set up before its walk (the split plain path): frame, window,
+// far plane and bounding cone, its walk cap, flags and spot factor, and its
+// cone number.
+struct ConeRecord {
+  float4 a;  // apex.xyz, far_offset
+  float4 b;  // right.xyz, u0
+  float4 c;  // up.xyz, v0
+  float4 d;  // fwd.xyz, u1
+  float4 e;  // baxis.xyz, v1
+  float4 f;  // bcos, bsin, spot, flags (bits: 1 traced, 2 wide window, 4 wide window clipped)
+  uint4 g;   // cone number (low, high words), walk cap, 0
+};
+// Slots per split chunk (records and masks: 368 bytes a slot).
+static_assert(sizeof(ConeRecord) == 112, "cone record layout");
+constexpr uint64_t kSplitChunk = 1ull << 23;
 constexpr uint32_t kSkyCones = 1u;
 constexpr uint32_t kSkyCombineMax = 2u;      // combine meshes by the maximum, as light cones do (a diagnostic)
 constexpr uint32_t kSkyNoHorizonCull = 4u;   // walk geometry below the receiver's horizon too
@@ -65,6 +86,9 @@ struct DevOut {
   // Work counters: the next packet of the packet pass and of the solo pass.
   uint32_t* next_packet;
   uint32_t* next_solo;
+  // The split plain path: each slot's mask (64 coverages), for the
+  // integration after the walk; the solo pass lists slots, not cones.
+  float* cov_out = nullptr;
 };
 
 // Scratch words per call: redo count, error word, packet and solo counters.
@@ -118,12 +142,17 @@ cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count_work,
 // Scratch of cc_visibility_static: a file-scope device array of
 // kStaticScratchBytes per device, laid out as the counters (256 bytes), the
 // redo list (4 bytes per cone), the walk order (4 bytes per point) and the
-// walk order's sort scratch (the rest).
+// rest, which holds the walk order's sort scratch while the order is made,
+// then the split path's cone records (112 bytes per cone) and masks (256).
 constexpr uint32_t kStaticMaxCones = 1u << 17;  // cones (and points) per call: 131,072
-constexpr size_t kStaticScratchBytes = size_t(8) << 20;
 constexpr size_t kStaticRedoOffset = 256;
 constexpr size_t kStaticOrderOffset = kStaticRedoOffset + 4 * size_t(kStaticMaxCones);
 constexpr size_t kStaticSortOffset = kStaticOrderOffset + 4 * size_t(kStaticMaxCones);
+constexpr size_t kStaticRecordsOffset = kStaticSortOffset;
+constexpr size_t kStaticMasksOffset = kStaticRecordsOffset + sizeof(ConeRecord) * size_t(kStaticMaxCones);
+constexpr size_t kStaticScratchBytes = size_t(48) << 20;
+static_assert(kStaticMasksOffset + 256 * size_t(kStaticMaxCones) <= kStaticScratchBytes, "static scratch too small");
+static_assert(kStaticMaxCones <= kSplitChunk, "a static call is one split chunk");
 // The array's device address on `device` (the current device). The first
 // call per device looks it up; later calls return the cached address.
 cudaError_t static_scratch(int device, void** ptr);
@@ -136,10 +165,21 @@ cudaError_t launch_splat_pass(bool wide, bool count, bool inst, bool sky, const 
                               const DevOut& o, const uint32_t* list, const uint32_t* list_count, uint32_t pw,
                               uint32_t blocks, cudaStream_t stream);
 
+// The split plain path's kernels (visibility_split.cu): the unit's copy of
+// the table; slots base .. base + n - 1 set up into records[0 .. n - 1]; and
+// their masks (o.cov_out) integrated into o.irradiance and o.fraction.
+cudaError_t upload_disk_table_split(const float* table64);
+cudaError_t launch_cone_setup(const DevQuery& q, uint64_t base, uint64_t n, ConeRecord* records, cudaStream_t stream);
+cudaError_t launch_integrate(const DevQuery& q, const DevOut& o, uint64_t base, uint64_t n, const ConeRecord* records,
+                             cudaStream_t stream);
+
 // The packet pass over every cone, then (with o.redo_list) the solo pass over
-// the cones it listed. o.redo_count and o.error must be zero on entry.
+// the cones it listed. o.redo_count and o.error must be zero on entry. Exact
+// light cones take the split path: per chunk of kSplitChunk slots, setup,
+// the two passes and the integration; q.records and o.cov_out then hold
+// min(cones, kSplitChunk) slots.
 // `marks` (nullable): three events recorded before the packet pass, between
-// the passes and after the solo pass.
+// the passes and after the solo pass (after the integration, split).
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t points_per_warp,
                               bool count_work, int sm_count, cudaStream_t stream, const cudaEvent_t* marks);
 

@@ -32,6 +32,7 @@ namespace cc {
 
 cudaError_t upload_disk_table(const float* table64) {
   cudaError_t e = cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
+  if (e == cudaSuccess) e = upload_disk_table_split(table64);  // the integrating unit's copy
   if (e != cudaSuccess) return e;
   return upload_disk_table_splat(table64);  // the prefiltering unit's copy
 }
@@ -44,6 +45,48 @@ static cudaError_t exact_pass(bool count, bool inst, bool sky, const DevScene& s
                               cudaStream_t stream) {
   return sky ? plain_pass<kWide, true, false>(count, inst, s, q, o, list, list_count, pw, blocks, stream)
              : plain_pass<kWide, false, false>(count, inst, s, q, o, list, list_count, pw, blocks, stream);
+}
+
+// The split plain path (exact light cones): per chunk of at most kSplitChunk
+// slots, the cones set up, walked (the packet pass, then the solo pass over
+// the slots it listed) and integrated. For a call of several chunks the
+// middle mark follows the last chunk's packet pass.
+static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const DevOut& o, uint32_t pw, bool count,
+                                    bool inst, int sm_count, cudaStream_t stream, const cudaEvent_t* marks) {
+  if (!q0.records || !o.cov_out) return cudaErrorInvalidValue;
+  const uint64_t ncones = q0.npoints * (uint64_t)q0.nlights;
+  cudaError_t e = cudaSuccess;
+  for (uint64_t base = 0; base < ncones; base += kSplitChunk) {
+    const uint64_t n = ncones - base < kSplitChunk ? ncones - base : kSplitChunk;
+    DevQuery q = q0;
+    q.slot_base = base;
+    q.slot_count = n;
+    if (base > 0) {
+      // Each chunk's passes count from zero again; the error word carries on.
+      e = cudaMemsetAsync(o.redo_count, 0, sizeof(uint32_t), stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(o.next_packet, 0, sizeof(uint32_t), stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(o.next_solo, 0, sizeof(uint32_t), stream);
+      if (e != cudaSuccess) return e;
+    }
+    e = launch_cone_setup(q, base, n, const_cast<ConeRecord*>(q.records), stream);
+    if (e != cudaSuccess) return e;
+    const uint64_t packets = (n + pw - 1) / pw;
+    const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
+    const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
+    e = plain_pass<false, false, false>(count, inst, s, q, o, nullptr, nullptr, pw, blocks, stream);
+    if (e != cudaSuccess) return e;
+    if (marks && base + kSplitChunk >= ncones) cudaEventRecord(marks[1], stream);
+    if (o.redo_list) {
+      e = plain_pass<true, false, false>(count, inst, s, q, o, o.redo_list, o.redo_count, 1,
+                                         (uint32_t)sm_count * kSoloBlocksPerSm, stream);
+      if (e != cudaSuccess) return e;
+    }
+    e = launch_integrate(q, o, base, n, q.records, stream);
+    if (e != cudaSuccess) return e;
+  }
+  if (marks) cudaEventRecord(marks[2], stream);
+  return e;
 }
 
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t pw, bool count,
@@ -59,14 +102,15 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
     }
     return cudaSuccess;
   }
+  const bool inst = s.xforms != nullptr;
+  const bool sky = (q.sky & kSkyCones) != 0u;
+  const bool splat = q.prefilter > 0.0f;
+  if (!sky && !splat) return split_visibility(s, q, o, pw, count, inst, sm_count, stream, marks);
   const uint64_t packets = (ncones + pw - 1) / pw;
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
   // One resident wave: warps take packets from the shared counter.
   const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-  const bool inst = s.xforms != nullptr;
-  const bool sky = (q.sky & kSkyCones) != 0u;
-  const bool splat = q.prefilter > 0.0f;
   // The packet pass with 32-bit accumulator cells, the solo pass with 64-bit.
   auto packets_pass = [&](uint32_t p, uint32_t nb) {
     return splat ? launch_splat_pass(false, count, inst, sky, s, q, o, nullptr, nullptr, p, nb, stream)

@@ -731,6 +731,62 @@ static __device__ __noinline__ float warp_blocked(const Cone& mine, f3 my_normal
   return sum;
 }
 
+// The light a light cone's mask lets through (cone_irradiance_rect,
+// :1286-1321: rect lights' Lambert bin weights, one cone at a time across the
+// warp; sphere_open_share, :957-972), times the spot factor, and the lighting
+// cache's ratio (vc_bake :3453-3510, static light). Warp-collective: every
+// lane calls it. `cov` is the warp's coverage table (bin b of lane j at
+// cov[32 b + j]); `scratch` holds 387 floats the warp may overwrite.
+__device__ __forceinline__ void light_integral(const Cone& cone, f3 point, f3 normal, const DevLight& L, float spot,
+                                               bool traced, const LightConeInfo& info, bool last_empty,
+                                               bool last_full, const float* cov, float* scratch, int lane,
+                                               float& value_out, float& ratio_out) {
+  const float* mine = cov + lane;
+  const bool rect_traced = traced && !is_sphere(L);
+  bool all_above = true;
+  float total = 0.0f;
+  if (rect_traced) total = window_weight(cone, normal, &all_above);
+  float blocked = 0.0f;
+  uint32_t todo = __ballot_sync(0xffffffffu, rect_traced && !last_empty);
+  while (todo) {
+    const int j = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const float b = warp_blocked(cone, normal, all_above, cov + j, scratch, j, lane);
+    if (lane == j) blocked = b;
+  }
+  float value = 0.0f;
+  if (traced) {
+    if (is_sphere(L)) {
+      // sphere_open_share (:957-972)
+      float total_w = 0.0f, open_w = 0.0f;
+      const float g = float(kGrid);
+      for (int b = 0; b < kBins; ++b) {
+        const float mfrac = info.wide_clipped ? 1.0f : c_disk[b];
+        if (mfrac <= 0.0f) continue;
+        f3 d = direction(cone, (float(b % kGrid) + 0.5f) / g, (float(b / kGrid) + 0.5f) / g);
+        float l2 = dot(d, d);
+        float w = mfrac * fmaxf(dot(normal, d), 0.0f) / (l2 * l2);
+        total_w += w;
+        open_w += w * (1.0f - mine[32 * b]);
+      }
+      const float share = total_w <= 0.0f ? 1.0f : open_w / total_w;
+      value = sphere_unshadowed(point, normal, L) * share;
+    } else {
+      // cone_visible (:1244-1272) and wide_visible (:1070-1073)
+      float visible = fmaxf(total - blocked, 0.0f);
+      if (info.wide_clipped) visible = (total > 1e-9f ? visible / total : 1.0f) * rect_open(point, normal, L);
+      value = visible;
+    }
+  }
+  value *= spot;
+  const float open = unshadowed(point, normal, L);
+  float ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
+  if (open > 0.0f && last_empty) ratio = 1.0f;
+  if (open > 0.0f && last_full) ratio = 0.0f;
+  value_out = value;
+  ratio_out = ratio;
+}
+
 // The job of a batch that holds `key` (a packet or a cone number): the last
 // job whose start is at most `key`. Warp-uniform.
 __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, uint32_t njobs, uint64_t key,
@@ -768,8 +824,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
   ws->span_lo[lane] = 68u;
   ws->span_hi[lane] = 0u;
 
-  const uint64_t plain_cones =
-      q_plain.cones ? (uint64_t)*q_plain.cones_count : q_plain.npoints * (uint64_t)q_plain.nlights;
+  // The split plain path (exact light cones, not batched): the walk takes
+  // each slot's cone from its record, set up by cone_setup_kernel, and
+  // leaves its mask to integrate_kernel.
+  constexpr bool kSplit = !kBatch && !kSky && !kSplat;
+  uint64_t plain_cones;
+  if constexpr (kSplit) {
+    plain_cones = q_plain.slot_count;
+    if (q_plain.cones) {
+      const uint64_t listed_cones = *q_plain.cones_count;
+      const uint64_t left = listed_cones > q_plain.slot_base ? listed_cones - q_plain.slot_base : 0;
+      plain_cones = left < plain_cones ? left : plain_cones;
+    }
+  } else {
+    plain_cones = q_plain.cones ? (uint64_t)*q_plain.cones_count : q_plain.npoints * (uint64_t)q_plain.nlights;
+  }
   uint64_t npackets;
   if (list) npackets = (uint64_t)min(*list_count, o.redo_capacity);  // one cone per packet
   else npackets = kBatch ? batch.packets : (plain_cones + pw - 1) / pw;
@@ -816,7 +885,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     const uint64_t slot = wbase + lane;
     const bool valid = list ? lane == 0 : ((uint32_t)lane < pw && slot < ncones);
     uint64_t c = 0;
-    if (valid) {
+    [[maybe_unused]] uint64_t slot_local = 0;
+    [[maybe_unused]] ConeRecord rec;
+    if constexpr (kSplit) {
+      slot_local = valid ? (list ? listed : slot) : 0;
+      rec = q.records[slot_local];
+      c = valid ? ((uint64_t)rec.g.x | ((uint64_t)rec.g.y << 32)) : 0;
+    } else if (valid) {
       if (list) {
         c = listed - cone_start;
       } else if (q.cones) {
@@ -851,7 +926,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     float spot = 1.0f;
     LightConeInfo info{true, false, false};
     bool traced;
-    if constexpr (WS::kSky) {
+    if constexpr (kSplit) {
+      // The cone as cone_setup_kernel set it up.
+      st.cone.apex = mk(rec.a.x, rec.a.y, rec.a.z);
+      st.cone.far_offset = rec.a.w;
+      st.cone.right = mk(rec.b.x, rec.b.y, rec.b.z);
+      st.cone.u0 = rec.b.w;
+      st.cone.up = mk(rec.c.x, rec.c.y, rec.c.z);
+      st.cone.v0 = rec.c.w;
+      st.cone.fwd = mk(rec.d.x, rec.d.y, rec.d.z);
+      st.cone.u1 = rec.d.w;
+      st.cone.baxis = mk(rec.e.x, rec.e.y, rec.e.z);
+      st.cone.v1 = rec.e.w;
+      st.cone.bcos = rec.f.x;
+      st.cone.bsin = rec.f.y;
+      const uint32_t flags = __float_as_uint(rec.f.w);
+      traced = valid && (flags & 1u);
+      info.wide_window = (flags & 2u) != 0u;
+      info.wide_clipped = (flags & 4u) != 0u;
+      st.cap = rec.g.z;
+    } else if constexpr (WS::kSky) {
       // Sky face l of the receiver (sky_face, :1444-1478); walked without a
       // cap (:1059, :1305).
       traced = valid && sky_face(l, point, normal, st.cone);
@@ -910,51 +1004,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
         value = fmaxf(open - blocked, 0.0f);
         ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
       }
-    } else {
-    // Rect light cones with coverage: the bins' Lambert weights, one cone at
-    // a time across the warp (the cone table is free now: it is the scratch).
-    const bool rect_traced = traced && !is_sphere(L);
-    bool all_above = true;
-    float total = 0.0f;
-    if (rect_traced) total = window_weight(st.cone, normal, &all_above);
-    float blocked = 0.0f;
-    uint32_t todo = __ballot_sync(0xffffffffu, rect_traced && !last_empty);
-    while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const float b = warp_blocked(st.cone, normal, all_above, ws->cov + j, ws->cone, j, lane);
-      if (lane == j) blocked = b;
-    }
-    if (traced) {
-      const Cone& cn = st.cone;
-      if (is_sphere(L)) {
-        // sphere_open_share (:957-972)
-        float total = 0.0f, open = 0.0f;
-        const float g = float(kGrid);
-        for (int b = 0; b < kBins; ++b) {
-          const float mfrac = info.wide_clipped ? 1.0f : c_disk[b];
-          if (mfrac <= 0.0f) continue;
-          f3 d = direction(cn, (float(b % kGrid) + 0.5f) / g, (float(b / kGrid) + 0.5f) / g);
-          float l2 = dot(d, d);
-          float w = mfrac * fmaxf(dot(normal, d), 0.0f) / (l2 * l2);
-          total += w;
-          open += w * (1.0f - st.cov[32 * b]);
-        }
-        const float share = total <= 0.0f ? 1.0f : open / total;
-        value = sphere_unshadowed(point, normal, L) * share;
-      } else {
-        // cone_visible (:1244-1272) and wide_visible (:1070-1073)
-        float visible = fmaxf(total - blocked, 0.0f);
-        if (info.wide_clipped) visible = (total > 1e-9f ? visible / total : 1.0f) * rect_open(point, normal, L);
-        value = visible;
-      }
-    }
-    value *= spot;
-    // The lighting cache's ratio (vc_bake :3453-3510, static light).
-    const float open = unshadowed(point, normal, L);
-    ratio = open > 0.0f ? clampf(value / open, 0.0f, 1.0f) : 1.0f;
-    if (open > 0.0f && last_empty) ratio = 1.0f;
-    if (open > 0.0f && last_full) ratio = 0.0f;
+    } else if constexpr (!kSplit) {
+      // The cone table is free now: it is the integration's scratch.
+      light_integral(st.cone, point, normal, L, spot, traced, info, last_empty, last_full, ws->cov, ws->cone, lane,
+                     value, ratio);
     }
 
     // A walk again keeps the reasons its packet pass listed the cone for.
@@ -964,7 +1017,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
                       (((st.status & 4u) && (st.status & (1u | 16u))) || (st.status & kStatusAccOverflow));
     if (redo) {
       const uint32_t at = atomicAdd(o.redo_count, 1u);
-      if (at < o.redo_capacity) o.redo_list[at] = (uint32_t)(cone_start + c);
+      if (at < o.redo_capacity) o.redo_list[at] = kSplit ? (uint32_t)slot_local : (uint32_t)(cone_start + c);
       else atomicOr(o.error, 1u);
     }
     if (st.status & 2u) atomicOr(o.error, 2u);
@@ -972,8 +1025,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     if (valid && !redo) {
       if (out_full) out_full[c] = make_uint2(fw0, fw1);
       if (out_any) out_any[c] = make_uint2(aw0, aw1);
-      if (out_irradiance) out_irradiance[c] = value;
-      if (out_fraction) out_fraction[c] = ratio;
+      if constexpr (kSplit) {
+        // The mask, for the integration after the walk.
+        float4* dst = reinterpret_cast<float4*>(o.cov_out + 64 * slot_local);
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k)
+          dst[k] = make_float4(st.cov[32 * (4 * k)], st.cov[32 * (4 * k + 1)], st.cov[32 * (4 * k + 2)],
+                               st.cov[32 * (4 * k + 3)]);
+      } else {
+        if (out_irradiance) out_irradiance[c] = value;
+        if (out_fraction) out_fraction[c] = ratio;
+      }
       if (out_work) out_work[c] = make_uint4(st.n_obj, st.n_blas, st.n_tris, st.status);
       if (out_partial) {
         float4* dst = reinterpret_cast<float4*>(out_partial + 64 * c);

@@ -1,0 +1,147 @@
+// The split plain path's kernels before and after the walk: each slot's light
+// cone set up (cone_setup_kernel) and each walked mask integrated into the
+// cone's light and the cache's ratio (integrate_kernel), with the same
+// functions the fused kernels use, so every result is the same. Kept out of
+// the walk kernel, whose speed follows the size of its code (instruction
+// fetch): without them it is a third smaller.
+#include "visibility_kernel.cuh"
+
+namespace cc {
+
+// The cone a slot walks: the listed cone, else its light's walk order.
+__device__ __forceinline__ bool slot_cone(const DevQuery& q, uint64_t slot, uint64_t* c) {
+  if (q.cones) {
+    if (slot >= (uint64_t)*q.cones_count) return false;
+    *c = __ldg(&q.cones[slot]);
+    return true;
+  }
+  if (slot >= q.npoints * (uint64_t)q.nlights) return false;
+  if (q.order) {
+    const uint64_t light_base = (slot / q.npoints) * q.npoints;
+    *c = light_base + __ldg(&q.order[slot - light_base]);
+  } else {
+    *c = slot;
+  }
+  return true;
+}
+
+// One slot per thread: the spot factor and facing test that gate the cone,
+// and the cone itself (hit_irradiance_rect, :2125-2128; light_cone).
+__global__ void cone_setup_kernel(DevQuery q, uint64_t base, uint64_t n, ConeRecord* __restrict__ records) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t c = 0;
+  const bool valid = slot_cone(q, base + i, &c);
+  const uint32_t l = valid ? (uint32_t)(c / q.npoints) : 0u;
+  const uint64_t p = valid ? c - (uint64_t)l * q.npoints : 0u;
+  const f3 point = xyz(__ldg(&q.receivers[2 * p + 0])), normal = xyz(__ldg(&q.receivers[2 * p + 1]));
+  const DevLight L = load_light(q.lights, l);
+  const float spot = spot_falloff(L, normalize(point - light_center(L)));
+  const bool on = valid && spot > 0.0f && faces_light(L, point, normal);
+  Cone cone{};
+  const LightConeInfo info = light_cone(point, L, q.wide_extent, cone);
+  const bool traced = on && info.ok;
+  const uint32_t flags = (traced ? 1u : 0u) | (info.wide_window ? 2u : 0u) | (info.wide_clipped ? 4u : 0u);
+  ConeRecord r;
+  r.a = make_float4(cone.apex.x, cone.apex.y, cone.apex.z, cone.far_offset);
+  r.b = make_float4(cone.right.x, cone.right.y, cone.right.z, cone.u0);
+  r.c = make_float4(cone.up.x, cone.up.y, cone.up.z, cone.v0);
+  r.d = make_float4(cone.fwd.x, cone.fwd.y, cone.fwd.z, cone.u1);
+  r.e = make_float4(cone.baxis.x, cone.baxis.y, cone.baxis.z, cone.v1);
+  r.f = make_float4(cone.bcos, cone.bsin, spot, __uint_as_float(flags));
+  r.g = make_uint4((uint32_t)c, (uint32_t)(c >> 32), info.wide_window ? q.wide_cone_cap : q.light_cone_cap, 0u);
+  records[i] = r;
+}
+
+// Shared memory of one integrating warp: its 32 slots' masks (bin b of lane
+// j at cov[32 b + j]) and the integration's scratch.
+struct IntegrateShared {
+  float cov[kBins * 32];
+  float scratch[kConeFields * 32];
+};
+
+// One warp per 32 slots: each walked mask integrated as the fused kernels
+// integrate it (light_integral), the results written at each slot's cone.
+__global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, uint64_t base, uint64_t n,
+                                                      const ConeRecord* __restrict__ records) {
+  __shared__ IntegrateShared sh[2];
+  const int lane = threadIdx.x & 31;
+  IntegrateShared* ws = sh + (threadIdx.x >> 5);
+  const uint64_t first = ((uint64_t)blockIdx.x * 2 + (threadIdx.x >> 5)) * 32;
+  if (first >= n) return;  // the whole warp leaves together
+  uint64_t limit = n;
+  if (q.cones) {
+    const uint64_t listed = *q.cones_count;
+    const uint64_t left = listed > base ? listed - base : 0;
+    limit = left < limit ? left : limit;
+  }
+  const uint64_t slot = first + lane;
+  const bool valid = slot < limit;
+  const ConeRecord r = records[valid ? slot : first];
+  const uint64_t c = (uint64_t)r.g.x | ((uint64_t)r.g.y << 32);
+  const uint32_t flags = __float_as_uint(r.f.w);
+  const bool traced = valid && (flags & 1u);
+  LightConeInfo info;
+  info.ok = true;
+  info.wide_window = (flags & 2u) != 0u;
+  info.wide_clipped = (flags & 4u) != 0u;
+  Cone cone{};
+  cone.apex = mk(r.a.x, r.a.y, r.a.z);
+  cone.far_offset = r.a.w;
+  cone.right = mk(r.b.x, r.b.y, r.b.z);
+  cone.u0 = r.b.w;
+  cone.up = mk(r.c.x, r.c.y, r.c.z);
+  cone.v0 = r.c.w;
+  cone.fwd = mk(r.d.x, r.d.y, r.d.z);
+  cone.u1 = r.d.w;
+  cone.baxis = mk(r.e.x, r.e.y, r.e.z);
+  cone.v1 = r.e.w;
+  cone.bcos = r.f.x;
+  cone.bsin = r.f.y;
+  const uint32_t l = (uint32_t)(c / q.npoints);
+  const uint64_t p = c - (uint64_t)l * q.npoints;
+  const f3 point = xyz(__ldg(&q.receivers[2 * p + 0])), normal = xyz(__ldg(&q.receivers[2 * p + 1]));
+  const DevLight L = load_light(q.lights, l);
+  // The mask, and whether it is empty or whole.
+  bool any = false, all = true;
+  const float4* src = reinterpret_cast<const float4*>(o.cov_out + 64 * (valid ? slot : first));
+#pragma unroll 4
+  for (int k = 0; k < 16; ++k) {
+    const float4 v = src[k];
+    const float vs[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float x = valid ? vs[j] : 0.0f;
+      ws->cov[32 * (4 * k + j) + lane] = x;
+      any = any || x > 0.0f;
+      all = all && x >= 1.0f;
+    }
+  }
+  __syncwarp();
+  float value, ratio;
+  light_integral(cone, point, normal, L, r.f.z, traced, info, !any, all, ws->cov, ws->scratch, lane, value, ratio);
+  if (valid) {
+    if (o.irradiance) o.irradiance[c] = value;
+    if (o.fraction) o.fraction[c] = ratio;
+  }
+}
+
+cudaError_t upload_disk_table_split(const float* table64) {
+  return cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
+}
+
+cudaError_t launch_cone_setup(const DevQuery& q, uint64_t base, uint64_t n, ConeRecord* records, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  cone_setup_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(q, base, n, records);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_integrate(const DevQuery& q, const DevOut& o, uint64_t base, uint64_t n,
+                             const ConeRecord* records, cudaStream_t stream) {
+  if (n == 0 || (!o.irradiance && !o.fraction)) return cudaSuccess;
+  const uint64_t warps = (n + 31) / 32;
+  integrate_kernel<<<(unsigned)((warps + 1) / 2), 64, 0, stream>>>(q, o, base, n, records);
+  return cudaGetLastError();
+}
+
+}  // namespace cc
