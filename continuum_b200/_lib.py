@@ -40,7 +40,7 @@ CC_SKY_NO_HORIZON_CULL = 2
 
 #: Every symbol include/continuum_cuda.h declares.
 EXPORTS = (
-    "cc_context_create", "cc_context_destroy", "cc_last_error", "cc_scene_upload", "cc_scene_build",
+    "cc_context_create", "cc_context_destroy", "cc_context_set_split_chunk", "cc_last_error", "cc_scene_upload", "cc_scene_build",
     "cc_scene_destroy", "cc_scene_sizes", "cc_scene_arrays", "cc_scene_device_bytes", "cc_options_default",
     "cc_visibility", "cc_irradiance", "cc_coverage", "cc_scene_primary_hits", "cc_context_kernel_times",
     "cc_visibility_static", "cc_batch_options_default", "cc_batch_create", "cc_batch_destroy", "cc_batch_clear",
@@ -144,6 +144,7 @@ def load() -> C.CDLL:
     sig = {
         "cc_context_create": (I, [I, C.POINTER(P)]),
         "cc_context_destroy": (I, [P]),
+        "cc_context_set_split_chunk": (I, [P, C.c_uint64]),
         "cc_last_error": (C.c_char_p, []),
         "cc_scene_upload": (I, [P, C.POINTER(FlatScene), C.POINTER(P)]),
         "cc_scene_build": (I, [P, P, P, U32, C.POINTER(P)]),

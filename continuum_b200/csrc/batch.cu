@@ -16,10 +16,13 @@ struct cc_batch {
   uint64_t points = 0, cones = 0;
   // Device state, sized by prepare().
   DevBuf job_table, redo, order, sort_scratch, counters;
+  DevBuf records, masks;               // the split path's scratch, one chunk
+  std::vector<cc::BatchChunk> chunks;  // the split path's chunks, set by prepare()
   uint32_t* status = nullptr;    // pinned: the counters copied back after each submission
   cudaEvent_t done = nullptr;
   bool prepared = false;
   uint32_t prepared_pw = 0;
+  uint64_t prepared_chunk = 0;
   uint64_t packets = 0;
   // The captured graph and the options it was captured with.
   cudaGraphExec_t graph = nullptr;
@@ -50,11 +53,13 @@ int check_options(const cc_batch_options& o) {
 // sizes the device buffers and uploads the job table. The previous
 // submission has finished.
 int prepare(cc_batch* b, uint32_t pw) {
-  if (b->prepared && b->prepared_pw == pw) return CC_OK;
+  if (b->prepared && b->prepared_pw == pw && b->prepared_chunk == b->ctx->split_chunk) return CC_OK;
   drop_graph(b);
   uint64_t packet = 0, cone = 0, point = 0;
+  std::vector<uint64_t> job_cones;
   for (cc::JobGpu& j : b->jobs) {
     const uint64_t c = j.query.npoints * (uint64_t)j.query.nlights;
+    job_cones.push_back(c);
     j.packet_start = packet;
     j.cone_start = cone;
     j.point_start = point;
@@ -63,6 +68,11 @@ int prepare(cc_batch* b, uint32_t pw) {
     point += j.query.npoints;
   }
   b->packets = packet;
+  b->chunks = cc::batch_chunks(job_cones, pw, b->ctx->split_chunk);
+  uint64_t slots = 1;
+  for (const cc::BatchChunk& k : b->chunks) slots = std::max(slots, k.cone_count);
+  CC_CUDA(b->records.reserve(slots * sizeof(cc::ConeRecord)), "batch cone records");
+  CC_CUDA(b->masks.reserve(slots * 256), "batch cone masks");
   CC_CUDA(b->job_table.reserve(std::max<size_t>(b->jobs.size(), 1) * sizeof(cc::JobGpu)), "batch job table");
   CC_CUDA(b->redo.reserve(std::max<uint64_t>(cone, 1) * 4), "batch redo list");
   CC_CUDA(b->order.reserve(std::max<uint64_t>(point, 1) * 4), "batch walk order");
@@ -73,6 +83,7 @@ int prepare(cc_batch* b, uint32_t pw) {
             "batch job table upload");
   b->prepared = true;
   b->prepared_pw = pw;
+  b->prepared_chunk = b->ctx->split_chunk;
   return CC_OK;
 }
 
@@ -88,6 +99,7 @@ int enqueue(cc_batch* b, const cc_batch_options& opt, cudaStream_t stream) {
   L.points = b->points;
   L.pw = opt.points_per_warp;
   L.order = nullptr;
+  L.records = static_cast<cc::ConeRecord*>(b->records.ptr);
   if (!(opt.flags & CC_KEEP_ORDER) && b->points > 0) {
     CC_CUDA(cc::batch_order(L, b->sort_scratch.ptr, b->sort_scratch.size, static_cast<uint32_t*>(b->order.ptr),
                             stream),
@@ -103,7 +115,10 @@ int enqueue(cc_batch* b, const cc_batch_options& opt, cudaStream_t stream) {
     o.redo_list = static_cast<uint32_t*>(b->redo.ptr);
     o.redo_capacity = (uint32_t)std::max<uint64_t>(b->cones, 1);
   }
-  CC_CUDA(cc::launch_batch(L, o, b->count_work, b->ctx->sm_count, (int)opt.blocks_per_sm, stream), "batch launch");
+  o.cov_out = static_cast<float*>(b->masks.ptr);
+  CC_CUDA(cc::launch_batch(L, o, b->chunks.data(), b->chunks.size(), b->count_work, b->ctx->sm_count,
+                           (int)opt.blocks_per_sm, stream),
+          "batch launch");
   CC_CUDA(cudaMemcpyAsync(b->status, counters, cc::kCounterWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
           "batch status copy");
   return CC_OK;
@@ -195,7 +210,8 @@ int cc_batch_destroy(cc_batch* b) {
   cudaSetDevice(b->ctx->device);
   if (b->submitted && b->done) cudaEventSynchronize(b->done);
   drop_graph(b);
-  for (DevBuf* d : {&b->job_table, &b->redo, &b->order, &b->sort_scratch, &b->counters}) d->release();
+  for (DevBuf* d : {&b->job_table, &b->redo, &b->order, &b->sort_scratch, &b->counters, &b->records, &b->masks})
+    d->release();
   if (b->status) cudaFreeHost(b->status);
   if (b->done) cudaEventDestroy(b->done);
   delete b;

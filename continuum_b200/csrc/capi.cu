@@ -270,6 +270,13 @@ int cc_context_create(int device, cc_context** out) {
   return CC_OK;
 }
 
+int cc_context_set_split_chunk(cc_context* ctx, uint64_t cones) {
+  if (!ctx) return fail(CC_ERR_INVALID, "null context");
+  if (cones < 32 || cones > (1ull << 31)) return fail(CC_ERR_INVALID, "split chunk must hold 32 .. 2^31 cones");
+  ctx->split_chunk = cones;
+  return CC_OK;
+}
+
 int cc_context_destroy(cc_context* ctx) {
   if (!ctx) return CC_OK;
   cudaSetDevice(ctx->device);
@@ -576,7 +583,7 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
   CC_CUDA(cudaMemsetAsync(counters, 0, cc::kCounterWords * sizeof(uint32_t), stream), "counter reset");
   if (!sky && opt.prefilter <= 0.0f) {
     // The split path's scratch: one chunk of cone records and masks.
-    const uint64_t slots = std::max<uint64_t>(std::min<uint64_t>(ncones, cc::kSplitChunk), 1);
+    const uint64_t slots = std::max<uint64_t>(std::min<uint64_t>(ncones, ctx->split_chunk), 1);
     CC_CUDA(ctx->records.reserve(slots * sizeof(cc::ConeRecord)), "cone records");
     CC_CUDA(ctx->masks.reserve(slots * 256), "cone masks");
     q.records = static_cast<const cc::ConeRecord*>(ctx->records.ptr);
@@ -603,8 +610,8 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
   }
   const int slot = (ctx->timed_first + ctx->timed_count) % ring;
   ctx->timed_count++;
-  CC_CUDA(cc::launch_visibility(sd, q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
-                                &ctx->marks[3 * slot]),
+  CC_CUDA(cc::launch_visibility(sd, q, o, opt.points_per_warp, o.work != nullptr, ctx->split_chunk, ctx->sm_count,
+                                stream, &ctx->marks[3 * slot]),
           "visibility launch");
   if (device_ptrs) return CC_OK;
 
@@ -796,8 +803,8 @@ int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t
   // The split path's records and masks, over the sort scratch (used up by now).
   q.records = reinterpret_cast<const cc::ConeRecord*>(scratch + cc::kStaticRecordsOffset);
   o.cov_out = reinterpret_cast<float*>(scratch + cc::kStaticMasksOffset);
-  CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, ctx->sm_count, stream,
-                                nullptr),
+  CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, cc::kStaticMaxCones,
+                                ctx->sm_count, stream, nullptr),
           "visibility launch");
   return CC_OK;
 }

@@ -59,6 +59,7 @@ struct cc_context {
   using DevBuf = cc_host::DevBuf;
   int device = 0;
   int sm_count = 148;
+  uint64_t split_chunk = cc::kSplitChunk;  // cones a split chunk holds at most
   cudaStream_t stream = nullptr;
   DevBuf receivers, lights, full, any, partial, irradiance, fraction, work;
   DevBuf sky_sum;   // sky irradiance per receiver before its download

@@ -1,6 +1,7 @@
 // Launch interface between the host library and the device kernels.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "cone_device.cuh"
@@ -54,9 +55,9 @@ struct ConeRecord {
   float4 d;  // fwd.xyz, u1
   float4 e;  // baxis.xyz, v1
   float4 f;  // bcos, bsin, spot, flags (bits: 1 traced, 2 wide window, 4 wide window clipped)
-  uint4 g;   // cone number (low, high words), walk cap, 0
+  uint4 g;   // cone number (low, high words), walk cap, job (batched; else 0)
 };
-// Slots per split chunk (records and masks: 368 bytes a slot).
+// Slots per split chunk by default (records and masks: 368 bytes a slot).
 static_assert(sizeof(ConeRecord) == 112, "cone record layout");
 constexpr uint64_t kSplitChunk = 1ull << 23;
 constexpr uint32_t kSkyCones = 1u;
@@ -123,7 +124,22 @@ struct BatchLaunch {
   // The walk order of every job's points (job j's at order + point_start,
   // job-local indices), or null: each job's points in their given order.
   const uint32_t* order;
+  // The split path's chunk (set by launch_batch): packets packet_base ..
+  // + packet_count, whose cones are batch cones cone_base .. + cone_count,
+  // each set up in records[cone - cone_base].
+  ConeRecord* records = nullptr;
+  uint64_t packet_base = 0, packet_count = 0;
+  uint64_t cone_base = 0, cone_count = 0;
 };
+
+// A chunk of a batch for the split path: whole packets, at most the chunk's
+// slot count of cones.
+struct BatchChunk {
+  uint64_t packet_base, packet_count, cone_base, cone_count;
+};
+// The chunks of a batch whose jobs (in order) hold `cones[j]` cones, at `pw`
+// cones a packet and at most `max_slots` cones a chunk (max_slots >= pw).
+std::vector<BatchChunk> batch_chunks(const std::vector<uint64_t>& cones, uint32_t pw, uint64_t max_slots);
 
 // Morton walk order of every job's points in one sort: keys are the job index
 // above each point's 30-bit code, values the job-local point index; job j's
@@ -132,12 +148,13 @@ size_t batch_order_scratch_bytes(uint64_t points);
 cudaError_t batch_order(const BatchLaunch& b, void* scratch, size_t scratch_bytes, uint32_t* order,
                         cudaStream_t stream);
 
-// The packet pass over every job's cones, then the solo pass over the cones
-// it listed (batch cone numbers). o.redo_count, o.error and the two packet
-// counters must be zero on entry. blocks_per_sm: resident blocks per SM to
-// launch (1..kBlocksPerSm).
-cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count_work, int sm_count, int blocks_per_sm,
-                         cudaStream_t stream);
+// Per chunk (batch_chunks), the cones set up into b.records, the packet pass,
+// the solo pass over the slots it listed, and the masks (o.cov_out, one
+// chunk's) integrated into each job's irradiance and fraction.
+// o.redo_count, o.error and the two packet counters must be zero on entry.
+// blocks_per_sm: resident blocks per SM to launch (1..kBlocksPerSm).
+cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, const BatchChunk* chunks, size_t nchunks,
+                         bool count_work, int sm_count, int blocks_per_sm, cudaStream_t stream);
 
 // Scratch of cc_visibility_static: a file-scope device array of
 // kStaticScratchBytes per device, laid out as the counters (256 bytes), the
@@ -172,15 +189,19 @@ cudaError_t upload_disk_table_split(const float* table64);
 cudaError_t launch_cone_setup(const DevQuery& q, uint64_t base, uint64_t n, ConeRecord* records, cudaStream_t stream);
 cudaError_t launch_integrate(const DevQuery& q, const DevOut& o, uint64_t base, uint64_t n, const ConeRecord* records,
                              cudaStream_t stream);
+// Batched: the batch cones of chunk b (b.cone_base .. + b.cone_count).
+cudaError_t launch_batch_setup(const BatchLaunch& b, cudaStream_t stream);
+cudaError_t launch_batch_integrate(const BatchLaunch& b, const DevOut& o, cudaStream_t stream);
 
 // The packet pass over every cone, then (with o.redo_list) the solo pass over
 // the cones it listed. o.redo_count and o.error must be zero on entry. Exact
-// light cones take the split path: per chunk of kSplitChunk slots, setup,
+// light cones take the split path: per chunk of chunk_slots slots, setup,
 // the two passes and the integration; q.records and o.cov_out then hold
-// min(cones, kSplitChunk) slots.
+// min(cones, chunk_slots) slots.
 // `marks` (nullable): three events recorded before the packet pass, between
 // the passes and after the solo pass (after the integration, split).
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t points_per_warp,
-                              bool count_work, int sm_count, cudaStream_t stream, const cudaEvent_t* marks);
+                              bool count_work, uint64_t chunk_slots, int sm_count, cudaStream_t stream,
+                              const cudaEvent_t* marks);
 
 }  // namespace cc

@@ -99,6 +99,7 @@ struct cc_server {
   std::list<CacheEntry*> lru;        // front: least recently used
   std::multimap<uint64_t, std::unique_ptr<CacheEntry>> cache;  // by key
   uint64_t in_use = 0, peak = 0;
+  uint64_t chunk = 1ull << 22;  // cones a launch's split chunk holds at most
 
   uint64_t completed = 0, refused = 0, launches = 0, cached_lights = 0, traced_lights = 0;
 };
@@ -113,6 +114,12 @@ uint64_t request_bytes(const cc_request& r, uint64_t traced) {
   const uint64_t P = r.npoints;
   return P * 32 + traced * 64 + traced * P * kResultBytes + traced * P * 4 /* redo */ + P * 4 /* order */ +
          cc::batch_order_scratch_bytes(std::max<uint64_t>(P, 1)) + traced * sizeof(cc::JobGpu) + 4096;
+}
+
+// A launch's split-path scratch (cone records and masks) for its largest
+// chunk, when it traces `cones` cones: chunks hold at most s->chunk.
+uint64_t split_bytes(const cc_server* s, uint64_t cones) {
+  return std::min(cones, s->chunk) * (sizeof(cc::ConeRecord) + 256);
 }
 
 void* pool_alloc(cc_server* s, uint64_t bytes, cudaStream_t stream, cudaError_t* e) {
@@ -251,6 +258,7 @@ void abandon(cc_server* s, Slot& slot, int status, const std::string& error) {
 void launch(cc_server* s, Slot& slot) {
   cudaStream_t st = slot.stream;
   std::vector<cc::JobGpu> jobs;
+  std::vector<uint64_t> job_cones;
   uint64_t points = 0, cones = 0, packet = 0;
   const uint32_t pw = s->opt.points_per_warp;
   cc_options d;
@@ -304,10 +312,12 @@ void launch(cc_server* s, Slot& slot) {
       cones += P;
       points += P;
       jobs.push_back(j);
+      job_cones.push_back(P);
       ++t;
     }
   }
-  // Launch scratch: job table, redo list, walk order and its sort, counters.
+  // Launch scratch: job table, redo list, walk order and its sort, counters,
+  // and the split path's records and masks for one chunk.
   if (!jobs.empty()) {
     cudaError_t e = cudaSuccess;
     if (slot.host_jobs_cap < jobs.size()) {
@@ -334,6 +344,15 @@ void launch(cc_server* s, Slot& slot) {
     void* d_counters = pool_alloc(s, cc::kCounterWords * 4, st, &e);
     SRV_CUDA(e, "counters");
     slot.scratch.push_back(d_counters);
+    const std::vector<cc::BatchChunk> chunks = cc::batch_chunks(job_cones, pw, s->chunk);
+    uint64_t slots = 1;
+    for (const cc::BatchChunk& k : chunks) slots = std::max(slots, k.cone_count);
+    void* d_records = pool_alloc(s, slots * sizeof(cc::ConeRecord), st, &e);
+    SRV_CUDA(e, "cone records");
+    slot.scratch.push_back(d_records);
+    void* d_masks = pool_alloc(s, slots * 256, st, &e);
+    SRV_CUDA(e, "cone masks");
+    slot.scratch.push_back(d_masks);
     SRV_CUDA(cudaMemcpyAsync(d_jobs, slot.host_jobs, jobs.size() * sizeof(cc::JobGpu), cudaMemcpyHostToDevice, st),
              "job table upload");
     SRV_CUDA(cudaMemsetAsync(d_counters, 0, cc::kCounterWords * 4, st), "counter reset");
@@ -343,6 +362,7 @@ void launch(cc_server* s, Slot& slot) {
     L.packets = packet;
     L.points = points;
     L.pw = pw;
+    L.records = static_cast<cc::ConeRecord*>(d_records);
     SRV_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
     L.order = static_cast<const uint32_t*>(d_order);
     uint32_t* counters = static_cast<uint32_t*>(d_counters);
@@ -353,7 +373,10 @@ void launch(cc_server* s, Slot& slot) {
     o.next_solo = counters + 3;
     o.redo_list = static_cast<uint32_t*>(d_redo);
     o.redo_capacity = (uint32_t)std::max<uint64_t>(cones, 1);
-    SRV_CUDA(cc::launch_batch(L, o, false, s->ctx->sm_count, (int)s->opt.blocks_per_sm, st), "launch");
+    o.cov_out = static_cast<float*>(d_masks);
+    SRV_CUDA(cc::launch_batch(L, o, chunks.data(), chunks.size(), false, s->ctx->sm_count, (int)s->opt.blocks_per_sm,
+                              st),
+             "launch");
     SRV_CUDA(cudaMemcpyAsync(slot.status, counters, cc::kCounterWords * 4, cudaMemcpyDeviceToHost, st), "status");
   } else {
     std::fill(slot.status, slot.status + cc::kCounterWords, 0u);
@@ -398,7 +421,8 @@ std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_
     if (!taken.empty() && cones + c > s->opt.max_launch_cones) break;
     for (CacheEntry* e : hit)
       if (e) e->refs++;  // keep them through make_room
-    const uint64_t need = request_bytes(q, traced);
+    // The request's bytes, and what it adds to the launch's split scratch.
+    const uint64_t need = request_bytes(q, traced) + split_bytes(s, cones + c) - split_bytes(s, cones);
     if (!make_room(s, need, stream)) {
       for (CacheEntry* e : hit)
         if (e) e->refs--;
@@ -505,6 +529,7 @@ int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server
   cc_server* s = new cc_server;
   s->ctx = ctx;
   s->opt = opt;
+  s->chunk = std::min<uint64_t>(s->chunk, ctx->split_chunk);
   cudaMemPoolProps props{};
   props.allocType = cudaMemAllocationTypePinned;
   props.location.type = cudaMemLocationTypeDevice;
@@ -582,7 +607,7 @@ int cc_server_submit(cc_server* s, const cc_request* req, uint64_t* ticket) {
     s->refused++;
     return fail(CC_ERR_BUSY, "the server's queue is full");
   }
-  if (request_bytes(*req, req->nlights) > s->opt.hbm_budget) {
+  if (request_bytes(*req, req->nlights) + split_bytes(s, request_cones(*req)) > s->opt.hbm_budget) {
     s->refused++;
     return fail(CC_ERR_BUSY, "the request alone exceeds the server's memory budget");
   }

@@ -47,17 +47,18 @@ static cudaError_t exact_pass(bool count, bool inst, bool sky, const DevScene& s
              : plain_pass<kWide, false, false>(count, inst, s, q, o, list, list_count, pw, blocks, stream);
 }
 
-// The split plain path (exact light cones): per chunk of at most kSplitChunk
+// The split plain path (exact light cones): per chunk of at most `chunk`
 // slots, the cones set up, walked (the packet pass, then the solo pass over
 // the slots it listed) and integrated. For a call of several chunks the
 // middle mark follows the last chunk's packet pass.
 static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const DevOut& o, uint32_t pw, bool count,
-                                    bool inst, int sm_count, cudaStream_t stream, const cudaEvent_t* marks) {
-  if (!q0.records || !o.cov_out) return cudaErrorInvalidValue;
+                                    bool inst, uint64_t chunk, int sm_count, cudaStream_t stream,
+                                    const cudaEvent_t* marks) {
+  if (!q0.records || !o.cov_out || chunk == 0) return cudaErrorInvalidValue;
   const uint64_t ncones = q0.npoints * (uint64_t)q0.nlights;
   cudaError_t e = cudaSuccess;
-  for (uint64_t base = 0; base < ncones; base += kSplitChunk) {
-    const uint64_t n = ncones - base < kSplitChunk ? ncones - base : kSplitChunk;
+  for (uint64_t base = 0; base < ncones; base += chunk) {
+    const uint64_t n = ncones - base < chunk ? ncones - base : chunk;
     DevQuery q = q0;
     q.slot_base = base;
     q.slot_count = n;
@@ -76,7 +77,7 @@ static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const
     const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
     e = plain_pass<false, false, false>(count, inst, s, q, o, nullptr, nullptr, pw, blocks, stream);
     if (e != cudaSuccess) return e;
-    if (marks && base + kSplitChunk >= ncones) cudaEventRecord(marks[1], stream);
+    if (marks && base + chunk >= ncones) cudaEventRecord(marks[1], stream);
     if (o.redo_list) {
       e = plain_pass<true, false, false>(count, inst, s, q, o, o.redo_list, o.redo_count, 1,
                                          (uint32_t)sm_count * kSoloBlocksPerSm, stream);
@@ -90,7 +91,7 @@ static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const
 }
 
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t pw, bool count,
-                              int sm_count, cudaStream_t stream, const cudaEvent_t* marks) {
+                              uint64_t chunk, int sm_count, cudaStream_t stream, const cudaEvent_t* marks) {
   if (pw < 1) pw = 1;
   if (pw > 32) pw = 32;
   const uint64_t ncones = q.npoints * (uint64_t)q.nlights;
@@ -105,7 +106,7 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   const bool inst = s.xforms != nullptr;
   const bool sky = (q.sky & kSkyCones) != 0u;
   const bool splat = q.prefilter > 0.0f;
-  if (!sky && !splat) return split_visibility(s, q, o, pw, count, inst, sm_count, stream, marks);
+  if (!sky && !splat) return split_visibility(s, q, o, pw, count, inst, chunk, sm_count, stream, marks);
   const uint64_t packets = (ncones + pw - 1) / pw;
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
   // One resident wave: warps take packets from the shared counter.
@@ -132,22 +133,46 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   return e;
 }
 
-cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, bool count, int sm_count, int blocks_per_sm,
-                         cudaStream_t stream) {
-  if (b.njobs == 0 || b.packets == 0) return cudaSuccess;
+cudaError_t launch_batch(const BatchLaunch& b0, const DevOut& o, const BatchChunk* chunks, size_t nchunks, bool count,
+                         int sm_count, int blocks_per_sm, cudaStream_t stream) {
+  if (b0.njobs == 0 || b0.packets == 0) return cudaSuccess;
+  if (!b0.records || !o.cov_out) return cudaErrorInvalidValue;
   if (blocks_per_sm < 1) blocks_per_sm = 1;
   if (blocks_per_sm > kBlocksPerSm) blocks_per_sm = kBlocksPerSm;
   const DevScene s{};
   const DevQuery q{};
-  const uint64_t want = (b.packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  const uint64_t cap = (uint64_t)sm_count * blocks_per_sm;
-  const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-  cudaError_t e = count ? launch_one<true, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
-                        : launch_one<false, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
-  if (e != cudaSuccess || !o.redo_list) return e;
-  const uint32_t solo_blocks = (uint32_t)sm_count * kSoloBlocksPerSm;
-  return count ? launch_one<true, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
-               : launch_one<false, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+  cudaError_t e = cudaSuccess;
+  for (size_t k = 0; k < nchunks; ++k) {
+    BatchLaunch b = b0;
+    b.packet_base = chunks[k].packet_base;
+    b.packet_count = chunks[k].packet_count;
+    b.cone_base = chunks[k].cone_base;
+    b.cone_count = chunks[k].cone_count;
+    if (k > 0) {
+      // Each chunk's passes count from zero again; the error word carries on.
+      e = cudaMemsetAsync(o.redo_count, 0, sizeof(uint32_t), stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(o.next_packet, 0, sizeof(uint32_t), stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(o.next_solo, 0, sizeof(uint32_t), stream);
+      if (e != cudaSuccess) return e;
+    }
+    e = launch_batch_setup(b, stream);
+    if (e != cudaSuccess) return e;
+    const uint64_t want = (b.packet_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const uint64_t cap = (uint64_t)sm_count * blocks_per_sm;
+    const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
+    e = count ? launch_one<true, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
+              : launch_one<false, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+    if (e != cudaSuccess) return e;
+    if (o.redo_list) {
+      const uint32_t solo_blocks = (uint32_t)sm_count * kSoloBlocksPerSm;
+      e = count ? launch_one<true, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+                : launch_one<false, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+      if (e != cudaSuccess) return e;
+    }
+    e = launch_batch_integrate(b, o, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return e;
 }
 
 }  // namespace cc

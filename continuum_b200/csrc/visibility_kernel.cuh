@@ -824,24 +824,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
   ws->span_lo[lane] = 68u;
   ws->span_hi[lane] = 0u;
 
-  // The split plain path (exact light cones, not batched): the walk takes
-  // each slot's cone from its record, set up by cone_setup_kernel, and
-  // leaves its mask to integrate_kernel.
-  constexpr bool kSplit = !kBatch && !kSky && !kSplat;
-  uint64_t plain_cones;
-  if constexpr (kSplit) {
+  // The split path (exact light cones): the walk takes each slot's cone from
+  // its record, set up by cone_setup_kernel, and leaves its mask to
+  // integrate_kernel. Slots are this chunk's: plain, slots slot_base ..;
+  // batched, the cones of packets packet_base .. (from batch cone cone_base).
+  constexpr bool kSplit = !kSky && !kSplat;
+  const ConeRecord* __restrict__ records = kBatch ? batch.records : q_plain.records;
+  uint64_t plain_cones = 0;  // unused when batched
+  if constexpr (!kBatch && kSplit) {
     plain_cones = q_plain.slot_count;
     if (q_plain.cones) {
       const uint64_t listed_cones = *q_plain.cones_count;
       const uint64_t left = listed_cones > q_plain.slot_base ? listed_cones - q_plain.slot_base : 0;
       plain_cones = left < plain_cones ? left : plain_cones;
     }
-  } else {
+  } else if constexpr (!kBatch) {
     plain_cones = q_plain.cones ? (uint64_t)*q_plain.cones_count : q_plain.npoints * (uint64_t)q_plain.nlights;
   }
   uint64_t npackets;
   if (list) npackets = (uint64_t)min(*list_count, o.redo_capacity);  // one cone per packet
-  else npackets = kBatch ? batch.packets : (plain_cones + pw - 1) / pw;
+  else npackets = kBatch ? batch.packet_count : (plain_cones + pw - 1) / pw;
   // Packets are taken from a shared counter as warps finish: their costs
   // differ by two orders of magnitude, so a fixed assignment leaves most
   // warps idle behind the slowest.
@@ -866,8 +868,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     uint64_t listed = 0;
     if (list) listed = list[packet];
     if constexpr (kBatch) {
-      const uint32_t j = list ? find_job(batch.jobs, batch.njobs, listed, true)
-                              : find_job(batch.jobs, batch.njobs, packet, false);
+      // The packet's job; a listed slot's is in its record.
+      const uint64_t packet_abs = batch.packet_base + packet;
+      const uint32_t j = list ? records[listed].g.w : find_job(batch.jobs, batch.njobs, packet_abs, false);
       const JobGpu* J = batch.jobs + j;
       s = J->scene;
       q = J->query;
@@ -880,7 +883,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
       out_work = J->work;
       cone_start = J->cone_start;
       ncones = q.npoints * (uint64_t)q.nlights;
-      if (!list) wbase = (packet - J->packet_start) * (uint64_t)pw;
+      if (!list) wbase = (packet_abs - J->packet_start) * (uint64_t)pw;
     }
     const uint64_t slot = wbase + lane;
     const bool valid = list ? lane == 0 : ((uint32_t)lane < pw && slot < ncones);
@@ -888,8 +891,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     [[maybe_unused]] uint64_t slot_local = 0;
     [[maybe_unused]] ConeRecord rec;
     if constexpr (kSplit) {
-      slot_local = valid ? (list ? listed : slot) : 0;
-      rec = q.records[slot_local];
+      if (valid) slot_local = list ? listed : (kBatch ? cone_start + slot - batch.cone_base : slot);
+      rec = records[slot_local];
       c = valid ? ((uint64_t)rec.g.x | ((uint64_t)rec.g.y << 32)) : 0;
     } else if (valid) {
       if (list) {

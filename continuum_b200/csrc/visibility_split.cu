@@ -1,4 +1,4 @@
-// The split plain path's kernels before and after the walk: each slot's light
+// The split path's kernels before and after the walk: each slot's light
 // cone set up (cone_setup_kernel) and each walked mask integrated into the
 // cone's light and the cache's ratio (integrate_kernel), with the same
 // functions the fused kernels use, so every result is the same. Kept out of
@@ -25,13 +25,9 @@ __device__ __forceinline__ bool slot_cone(const DevQuery& q, uint64_t slot, uint
   return true;
 }
 
-// One slot per thread: the spot factor and facing test that gate the cone,
-// and the cone itself (hit_irradiance_rect, :2125-2128; light_cone).
-__global__ void cone_setup_kernel(DevQuery q, uint64_t base, uint64_t n, ConeRecord* __restrict__ records) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint64_t c = 0;
-  const bool valid = slot_cone(q, base + i, &c);
+// A slot's record: the spot factor and facing test that gate its cone, and
+// the cone itself (hit_irradiance_rect, :2125-2128; light_cone).
+__device__ __forceinline__ ConeRecord make_record(const DevQuery& q, bool valid, uint64_t c, uint32_t job) {
   const uint32_t l = valid ? (uint32_t)(c / q.npoints) : 0u;
   const uint64_t p = valid ? c - (uint64_t)l * q.npoints : 0u;
   const f3 point = xyz(__ldg(&q.receivers[2 * p + 0])), normal = xyz(__ldg(&q.receivers[2 * p + 1]));
@@ -49,8 +45,32 @@ __global__ void cone_setup_kernel(DevQuery q, uint64_t base, uint64_t n, ConeRec
   r.d = make_float4(cone.fwd.x, cone.fwd.y, cone.fwd.z, cone.u1);
   r.e = make_float4(cone.baxis.x, cone.baxis.y, cone.baxis.z, cone.v1);
   r.f = make_float4(cone.bcos, cone.bsin, spot, __uint_as_float(flags));
-  r.g = make_uint4((uint32_t)c, (uint32_t)(c >> 32), info.wide_window ? q.wide_cone_cap : q.light_cone_cap, 0u);
-  records[i] = r;
+  r.g = make_uint4((uint32_t)c, (uint32_t)(c >> 32), info.wide_window ? q.wide_cone_cap : q.light_cone_cap, job);
+  return r;
+}
+
+// One slot per thread. Plain: slots base .. base + n - 1 of q's walk.
+// Batched: batch cones b.cone_base .. + b.cone_count, each in its job's walk.
+template <bool kBatch>
+__global__ void cone_setup_kernel(DevQuery q, BatchLaunch b, uint64_t base, uint64_t n,
+                                  ConeRecord* __restrict__ records) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t c = 0;
+  uint32_t j = 0;
+  if constexpr (kBatch) {
+    const uint64_t bc = base + i;
+    j = find_job(b.jobs, b.njobs, bc, true);
+    const JobGpu* J = b.jobs + j;
+    q = J->query;
+    q.order = b.order ? b.order + J->point_start : nullptr;
+    q.cones = nullptr;
+    const bool valid = slot_cone(q, bc - J->cone_start, &c);
+    records[i] = make_record(q, valid, c, j);
+  } else {
+    const bool valid = slot_cone(q, base + i, &c);
+    records[i] = make_record(q, valid, c, 0u);
+  }
 }
 
 // Shared memory of one integrating warp: its 32 slots' masks (bin b of lane
@@ -60,17 +80,20 @@ struct IntegrateShared {
   float scratch[kConeFields * 32];
 };
 
-// One warp per 32 slots: each walked mask integrated as the fused kernels
-// integrate it (light_integral), the results written at each slot's cone.
-__global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, uint64_t base, uint64_t n,
-                                                      const ConeRecord* __restrict__ records) {
+// One warp per 32 slots (n of them, from slot 0 of the chunk's records and
+// masks; plain calls with a cone list stop at the list's end): each walked
+// mask integrated as the fused kernels integrate it (light_integral), the
+// results written at each slot's cone, in its job's outputs when batched.
+template <bool kBatch>
+__global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, BatchLaunch b, uint64_t base,
+                                                      uint64_t n, const ConeRecord* __restrict__ records) {
   __shared__ IntegrateShared sh[2];
   const int lane = threadIdx.x & 31;
   IntegrateShared* ws = sh + (threadIdx.x >> 5);
   const uint64_t first = ((uint64_t)blockIdx.x * 2 + (threadIdx.x >> 5)) * 32;
   if (first >= n) return;  // the whole warp leaves together
   uint64_t limit = n;
-  if (q.cones) {
+  if (!kBatch && q.cones) {
     const uint64_t listed = *q.cones_count;
     const uint64_t left = listed > base ? listed - base : 0;
     limit = left < limit ? left : limit;
@@ -79,6 +102,16 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, uin
   const bool valid = slot < limit;
   const ConeRecord r = records[valid ? slot : first];
   const uint64_t c = (uint64_t)r.g.x | ((uint64_t)r.g.y << 32);
+  float* irradiance = o.irradiance;
+  float* fraction = o.fraction;
+  if constexpr (kBatch) {
+    const JobGpu* J = b.jobs + r.g.w;
+    q.receivers = J->query.receivers;
+    q.lights = J->query.lights;
+    q.npoints = J->query.npoints;
+    irradiance = J->irradiance;
+    fraction = J->fraction;
+  }
   const uint32_t flags = __float_as_uint(r.f.w);
   const bool traced = valid && (flags & 1u);
   LightConeInfo info;
@@ -121,8 +154,8 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, uin
   float value, ratio;
   light_integral(cone, point, normal, L, r.f.z, traced, info, !any, all, ws->cov, ws->scratch, lane, value, ratio);
   if (valid) {
-    if (o.irradiance) o.irradiance[c] = value;
-    if (o.fraction) o.fraction[c] = ratio;
+    if (irradiance) irradiance[c] = value;
+    if (fraction) fraction[c] = ratio;
   }
 }
 
@@ -132,7 +165,7 @@ cudaError_t upload_disk_table_split(const float* table64) {
 
 cudaError_t launch_cone_setup(const DevQuery& q, uint64_t base, uint64_t n, ConeRecord* records, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  cone_setup_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(q, base, n, records);
+  cone_setup_kernel<false><<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(q, BatchLaunch{}, base, n, records);
   return cudaGetLastError();
 }
 
@@ -140,8 +173,48 @@ cudaError_t launch_integrate(const DevQuery& q, const DevOut& o, uint64_t base, 
                              const ConeRecord* records, cudaStream_t stream) {
   if (n == 0 || (!o.irradiance && !o.fraction)) return cudaSuccess;
   const uint64_t warps = (n + 31) / 32;
-  integrate_kernel<<<(unsigned)((warps + 1) / 2), 64, 0, stream>>>(q, o, base, n, records);
+  integrate_kernel<false><<<(unsigned)((warps + 1) / 2), 64, 0, stream>>>(q, o, BatchLaunch{}, base, n, records);
   return cudaGetLastError();
+}
+
+cudaError_t launch_batch_setup(const BatchLaunch& b, cudaStream_t stream) {
+  const uint64_t n = b.cone_count;
+  if (n == 0) return cudaSuccess;
+  cone_setup_kernel<true><<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(DevQuery{}, b, b.cone_base, n, b.records);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_integrate(const BatchLaunch& b, const DevOut& o, cudaStream_t stream) {
+  const uint64_t n = b.cone_count;
+  if (n == 0) return cudaSuccess;
+  const uint64_t warps = (n + 31) / 32;
+  integrate_kernel<true><<<(unsigned)((warps + 1) / 2), 64, 0, stream>>>(DevQuery{}, o, b, b.cone_base, n, b.records);
+  return cudaGetLastError();
+}
+
+std::vector<BatchChunk> batch_chunks(const std::vector<uint64_t>& cones, uint32_t pw, uint64_t max_slots) {
+  std::vector<BatchChunk> out;
+  BatchChunk cur{0, 0, 0, 0};
+  for (const uint64_t c : cones) {
+    const uint64_t packets = (c + pw - 1) / pw;
+    uint64_t done = 0;  // the job's packets taken
+    while (done < packets) {
+      const uint64_t room = max_slots - cur.cone_count;
+      if (room < pw) {
+        out.push_back(cur);
+        cur = BatchChunk{cur.packet_base + cur.packet_count, 0, cur.cone_base + cur.cone_count, 0};
+        continue;
+      }
+      uint64_t take = room / pw;
+      if (take > packets - done) take = packets - done;
+      const uint64_t end = (done + take) * pw < c ? (done + take) * pw : c;  // a job's last packet may be short
+      cur.packet_count += take;
+      cur.cone_count += end - done * pw;
+      done += take;
+    }
+  }
+  if (cur.packet_count) out.push_back(cur);
+  return out;
 }
 
 }  // namespace cc

@@ -313,6 +313,12 @@ class MaskConeKernel:
         self.prefilter = 0.0
         self.object_prefilter = True
 
+    def set_split_chunk(self, cones: int) -> None:
+        """Cones one chunk of the split path holds at most (its device scratch
+        is 368 bytes a slot); results do not depend on it
+        (cc_context_set_split_chunk)."""
+        check(load().cc_context_set_split_chunk(self.handle, int(cones)))
+
     @classmethod
     def new(cls, device: int = 0) -> Optional["MaskConeKernel"]:
         """None without a CUDA device, as MaskConeKernel::new (lib.rs:1155-1175)."""

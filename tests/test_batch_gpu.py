@@ -125,6 +125,30 @@ def test_every_tuned_configuration_gives_the_same_results(kernel):
     jobs.close()
 
 
+def test_small_split_chunks_give_the_same_results(kernel):
+    """A batch split into chunks of whole packets that end inside jobs (and
+    jobs spread over several chunks) gives every job's results alone."""
+    import torch
+
+    stream = torch.cuda.Stream()
+    jobs = Jobs(kernel, torch)
+    alone = jobs.alone(kernel, stream)
+    b = jobs.batch(kernel)
+    try:
+        for chunk in (1000, 20000):
+            kernel.set_split_chunk(chunk)
+            for opt in (Batch.options(32, 5, _lib.CC_BATCH_GRAPH), Batch.options(8, 3, 0)):
+                jobs.zero()
+                torch.cuda.synchronize()
+                b.submit(opt, stream=stream.cuda_stream)
+                b.wait()
+                jobs.check(alone, KEYS[:5])
+    finally:
+        kernel.set_split_chunk(1 << 23)
+        b.close()
+        jobs.close()
+
+
 def test_batch_rejects_bad_jobs_and_options(kernel):
     import torch
 

@@ -88,3 +88,42 @@ def test_moved_objects_mark_the_oracle_stale_cones_and_the_update_equals_a_full_
     parity.compare(full, o, o["unshadowed"])
     scene.close()
     orc.close()
+
+
+def test_update_in_small_chunks_equals_the_default(kernel, world):
+    """The incremental update walks its listed cones a chunk at a time; small
+    chunks give the same cache as the default."""
+    import torch
+
+    movable = np.arange(0, len(world.instances) - 1, 10, dtype=np.uint32)
+    scene = kernel.scene_instanced(world.geometries, world.instances, movable)
+    dev = torch.device("cuda:0")
+    rec = torch.from_numpy(world.receivers).to(dev)
+    lig = torch.from_numpy(world.lights).to(dev)
+    P, L = rec.shape[0], lig.shape[0]
+    n = P * L
+
+    def cache():
+        return {"full": torch.zeros(n, dtype=torch.int64, device=dev), "any": torch.zeros(n, dtype=torch.int64, device=dev),
+                "irradiance": torch.zeros(n, device=dev), "fraction": torch.zeros(n, device=dev)}
+
+    caches = [cache(), cache()]
+    for c in caches:
+        kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, {k: v.data_ptr() for k, v in c.items()})
+    torch.cuda.synchronize()
+    boxes = scene.move(scenes.moved_placements(world, movable, 1))
+    stale = torch.zeros(n, dtype=torch.uint8, device=dev)
+    count = kernel.stale_cones(scene, rec.data_ptr(), P, world.lights, boxes, stale.data_ptr())
+    assert count > 1000
+    try:
+        for c, chunk in zip(caches, (1 << 23, 1000)):
+            kernel.set_split_chunk(chunk)
+            solved = kernel.visibility_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(),
+                                              {k: v.data_ptr() for k, v in c.items()})
+            assert solved == count
+        torch.cuda.synchronize()
+        for k in caches[0]:
+            assert torch.equal(caches[0][k], caches[1][k]), k
+    finally:
+        kernel.set_split_chunk(1 << 23)
+        scene.close()

@@ -106,6 +106,25 @@ def test_walk_order_changes_no_result(kernel):
         assert np.array_equal(a[k], b[k]), k
 
 
+def test_split_chunks_change_no_result(kernel):
+    """Exact cones are set up, walked and integrated a chunk at a time; chunks
+    of any size (whole packets or not) give identical results."""
+    w = small_field(seed=13, n=8, sub=3, width=96, height=54)
+    scene = kernel.scene(w.meshes)
+    base = parity.flat(kernel.visibility(scene, w.receivers, w.lights, outputs=ALL))
+    try:
+        for chunk in (32, 1000, 4099):
+            kernel.set_split_chunk(chunk)
+            got = parity.flat(kernel.visibility(scene, w.receivers, w.lights, outputs=ALL))
+            for k in ("full", "any", "partial", "irradiance", "fraction"):
+                assert np.array_equal(got[k], base[k]), (chunk, k)
+        with pytest.raises(_lib.CCError):
+            kernel.set_split_chunk(31)
+    finally:
+        kernel.set_split_chunk(1 << 23)
+        scene.close()
+
+
 def small_field(seed=5, n=12, sub=4, width=160, height=90):
     return scenes.icosphere_field(seed=seed, n_spheres=n, subdivisions=sub, width=width, height=height)
 

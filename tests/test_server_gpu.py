@@ -38,9 +38,17 @@ def fields(kernel):
         s.close()
 
 
-def test_each_request_is_the_same_alone_and_in_the_mix(kernel, fields):
+@pytest.mark.parametrize("chunk", [None, 3000])
+def test_each_request_is_the_same_alone_and_in_the_mix(kernel, fields, chunk):
+    """(chunk: launches split into chunks of at most that many cones, which
+    end inside requests.)"""
     ws, sc = fields
-    srv = Server(kernel, max_inflight=3, max_launch_cones=40_000)
+    if chunk:
+        kernel.set_split_chunk(chunk)
+    try:
+        srv = Server(kernel, max_inflight=3, max_launch_cones=40_000)
+    finally:
+        kernel.set_split_chunk(1 << 23)
     ids = [srv.add_scene(s) for s in sc]
     rng = np.random.default_rng(4)
     reqs = []
@@ -96,8 +104,9 @@ def test_admission_stays_under_the_budget(kernel, fields):
     rec, lig = w.receivers, w.lights
     P, L = rec.shape[0], lig.shape[0]
     # Room for two or three requests in flight, but not for every request's
-    # cached results besides: admission must evict cache entries.
-    budget = P * 32 + L * 64 + L * P * 28 + P * 4 + 64 * P + (4 << 20)
+    # cached results besides: admission must evict cache entries. A launch
+    # also holds 368 bytes of split-path scratch per traced cone.
+    budget = P * 32 + L * 64 + L * P * (28 + 368) + P * 4 + 64 * P + (4 << 20)
     srv = Server(kernel, hbm_budget=budget, max_inflight=4)
     sid = srv.add_scene(sc[0])
     outs = [host_outputs(P, L) for _ in range(4)]
