@@ -44,7 +44,7 @@ void drop_graph(cc_batch* b) {
 int check_options(const cc_batch_options& o) {
   if (o.points_per_warp < 1 || o.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
   if (o.blocks_per_sm < 1 || o.blocks_per_sm > (uint32_t)cc::kBlocksPerSm)
-    return fail(CC_ERR_INVALID, "blocks_per_sm must be 1..5");
+    return fail(CC_ERR_INVALID, "blocks_per_sm must be 1..8");
   if (o.flags & ~(CC_KEEP_ORDER | CC_NO_REDO | CC_BATCH_GRAPH)) return fail(CC_ERR_INVALID, "unknown batch flag");
   return CC_OK;
 }
@@ -320,7 +320,7 @@ int cc_batch_tune(cc_batch* b, const cc_batch_options* base, uint32_t reps, cc_b
   std::vector<cc_batch_options> cands;
   for (uint32_t pw : {8u, 16u, 32u})
     for (uint32_t order : {0u, (uint32_t)CC_KEEP_ORDER})
-      for (uint32_t bps : {3u, 5u}) cands.push_back({pw, bps, (keep & CC_NO_REDO) | order});
+      for (uint32_t bps : {4u, 8u}) cands.push_back({pw, bps, (keep & CC_NO_REDO) | order});
   cudaStream_t stream = b->ctx->stream;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   CC_CUDA(cudaEventCreate(&t0), "tune event");

@@ -282,7 +282,8 @@ int cc_context_destroy(cc_context* ctx) {
   cudaSetDevice(ctx->device);
   for (DevBuf* b : {&ctx->receivers, &ctx->lights, &ctx->full, &ctx->any, &ctx->partial, &ctx->irradiance,
                     &ctx->fraction, &ctx->work, &ctx->redo, &ctx->order, &ctx->sort_scratch, &ctx->records, &ctx->masks,
-                    &ctx->counters})
+                    &ctx->counters, &ctx->move_xforms, &ctx->stale_tables, &ctx->upd_perm, &ctx->upd_flags,
+                    &ctx->upd_list, &ctx->upd_count, &ctx->upd_order, &ctx->upd_temp})
     b->release();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);

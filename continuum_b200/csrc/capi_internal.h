@@ -66,6 +66,9 @@ struct cc_context {
   DevBuf redo;      // redo list
   DevBuf order;     // walk order of the points
   DevBuf sort_scratch;
+  // Moving frames' scratch, kept between frames: the movers' transforms, the
+  // stale-cone tables, and the update's cone order, flags, list and count.
+  DevBuf move_xforms, stale_tables, upd_perm, upd_flags, upd_list, upd_count, upd_order, upd_temp;
   DevBuf records;   // the split path's cone records, one chunk
   DevBuf masks;     // the split path's masks (64 floats a slot), one chunk
   DevBuf counters;  // [redo count, error word]

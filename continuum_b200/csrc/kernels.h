@@ -9,11 +9,15 @@
 namespace cc {
 
 constexpr int kWarpsPerBlock = 2;
-// Resident blocks per SM the shared memory allows: the packet pass (32-bit
-// accumulator cells, 38 KB per block) fits 5, the solo pass (64-bit cells,
-// 55 KB) 4.
-constexpr int kBlocksPerSm = 5;
-constexpr int kSoloBlocksPerSm = 4;
+// Resident blocks per SM the shared memory allows. The split path's passes
+// keep each cone's coverages in thread-local memory: its packet pass (32-bit
+// accumulator cells, 22 KB per block) fits 8, its solo pass (64-bit cells,
+// 38 KB) 5. Sky and prefiltering passes keep them in shared memory, where
+// the integration in the same kernel reads every lane's: 5 and 4.
+constexpr int kBlocksPerSm = 8;
+constexpr int kSoloBlocksPerSm = 5;
+constexpr int kFusedBlocksPerSm = 5;
+constexpr int kFusedSoloBlocksPerSm = 4;
 
 struct DevQuery {
   const float4* receivers;  // 2 per point: point, normal

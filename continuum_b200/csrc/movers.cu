@@ -296,15 +296,14 @@ int cc_scene_move(cc_scene* s, const cc_instance* placements, uint32_t n, float*
         packed[nm + 4 * i + r] = make_float4(row[0], row[1], row[2], row[3]);
       }
     }
-    float4* d = nullptr;
-    CC_CUDA(cudaMalloc(&d, packed.size() * sizeof(float4)), "move transforms");
+    CC_CUDA(s->ctx->move_xforms.reserve(packed.size() * sizeof(float4)), "move transforms");
+    float4* d = static_cast<float4*>(s->ctx->move_xforms.ptr);
     cudaError_t e = cudaMemcpy(d, packed.data(), packed.size() * sizeof(float4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
       cc::scatter_xforms<<<(unsigned)((nm + 127) / 128), 128>>>(d, d + nm, nm, s->xforms);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    cudaFree(d);
     if (e != cudaSuccess) return cuda_fail(e, "move transforms");
   }
   auto put_nodes = [&](uint32_t first, uint32_t count) -> int {
@@ -398,15 +397,15 @@ int cc_stale_cones(cc_context* ctx, const cc_scene* scene, const float* receiver
     for (const cc::Box3& r : regions[l])
       region_boxes.insert(region_boxes.end(), {r.lo[0], r.lo[1], r.lo[2], r.hi[0], r.hi[1], r.hi[2]});
   }
-  // Tables to the device (one allocation, freed after the call).
+  // Tables to the device (one buffer, kept for the next frame).
   auto bytes_of = [](size_t n, size_t each) { return (n * each + 255) & ~size_t(255); };
   const size_t b_nodes = bytes_of(nodes.size(), sizeof(float4)), b_roots = bytes_of(roots.size(), 4),
                b_items = bytes_of(items.size(), 4), b_rbox = bytes_of(region_box.size(), 4),
                b_boxes = bytes_of(boxes.size(), 4), b_lbox = bytes_of(lboxes.size(), 4), b_count = 256,
                b_regions = bytes_of(region_boxes.size(), 4);
-  uint8_t* dev = nullptr;
-  CC_CUDA(cudaMalloc(&dev, b_nodes + b_roots + b_items + b_rbox + b_boxes + b_lbox + b_regions + b_count), "stale tables");
-  uint8_t* at = dev;
+  CC_CUDA(ctx->stale_tables.reserve(b_nodes + b_roots + b_items + b_rbox + b_boxes + b_lbox + b_regions + b_count),
+          "stale tables");
+  uint8_t* at = static_cast<uint8_t*>(ctx->stale_tables.ptr);
   auto put = [&](const void* src, size_t n, size_t padded) {
     uint8_t* p = at;
     if (n) cudaMemcpyAsync(p, src, n, cudaMemcpyHostToDevice, stream);
@@ -433,7 +432,6 @@ int cc_stale_cones(cc_context* ctx, const cc_scene* scene, const float* receiver
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(&host_count, d_count, 8, cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-  cudaFree(dev);
   if (e != cudaSuccess) return cuda_fail(e, "stale cones");
   *count = host_count;
   return CC_OK;
@@ -458,22 +456,24 @@ int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const float* re
   // The stale cones of every light as one list, each light's in the walk
   // order (Morton order of the points), so one launch walks them all in
   // coherent packets and writes each result at its own cone.
-  uint32_t* perm = nullptr;
-  uint8_t* flags = nullptr;
-  uint32_t* list = nullptr;
-  uint32_t* count = nullptr;
-  uint32_t* order = nullptr;
-  void* temp = nullptr;
   size_t sel_bytes = 0;
   cub::DeviceSelect::Flagged(nullptr, sel_bytes, (const uint32_t*)nullptr, (const uint8_t*)nullptr, (uint32_t*)nullptr,
                              (uint32_t*)nullptr, (int)ncones);
   const size_t sort_bytes = cc::walk_order_scratch_bytes(npoints);
-  cudaError_t e = cudaMalloc(&perm, ncones * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&flags, ncones);
-  if (e == cudaSuccess) e = cudaMalloc(&list, ncones * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&count, 4);
-  if (e == cudaSuccess) e = cudaMalloc(&order, npoints * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&temp, std::max<size_t>(std::max(sel_bytes, sort_bytes), 256));
+  // Scratch kept in the context between frames.
+  cudaError_t e = ctx->upd_perm.reserve(ncones * 4);
+  if (e == cudaSuccess) e = ctx->upd_flags.reserve(ncones);
+  if (e == cudaSuccess) e = ctx->upd_list.reserve(ncones * 4);
+  if (e == cudaSuccess) e = ctx->upd_count.reserve(4);
+  if (e == cudaSuccess) e = ctx->upd_order.reserve(npoints * 4);
+  if (e == cudaSuccess) e = ctx->upd_temp.reserve(std::max<size_t>(std::max(sel_bytes, sort_bytes), 256));
+  if (e != cudaSuccess) return cuda_fail(e, "update scratch");
+  uint32_t* perm = static_cast<uint32_t*>(ctx->upd_perm.ptr);
+  uint8_t* flags = static_cast<uint8_t*>(ctx->upd_flags.ptr);
+  uint32_t* list = static_cast<uint32_t*>(ctx->upd_list.ptr);
+  uint32_t* count = static_cast<uint32_t*>(ctx->upd_count.ptr);
+  uint32_t* order = static_cast<uint32_t*>(ctx->upd_order.ptr);
+  void* temp = ctx->upd_temp.ptr;
   const unsigned threads = 256;
   if (e == cudaSuccess) {
     if (npoints > 64 && !scene->flat.nodes.empty()) {
@@ -504,12 +504,6 @@ int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const float* re
   uint32_t n = 0;
   if (e == cudaSuccess && rc == CC_OK) e = cudaMemcpyAsync(&n, count, 4, cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess && rc == CC_OK) e = cudaStreamSynchronize(stream);
-  cudaFree(perm);
-  cudaFree(flags);
-  cudaFree(list);
-  cudaFree(count);
-  cudaFree(order);
-  cudaFree(temp);
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "visibility update");
   if (recomputed) *recomputed = n;

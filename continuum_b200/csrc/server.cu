@@ -521,7 +521,7 @@ int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server
   if (opt.max_inflight < 1 || opt.max_inflight > 8) return fail(CC_ERR_INVALID, "max_inflight must be 1..8");
   if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
   if (opt.blocks_per_sm < 1 || opt.blocks_per_sm > (uint32_t)cc::kBlocksPerSm)
-    return fail(CC_ERR_INVALID, "blocks_per_sm must be 1..5");
+    return fail(CC_ERR_INVALID, "blocks_per_sm must be 1..8");
   if (opt.max_queue < 1 || opt.hbm_budget == 0 || opt.max_launch_cones == 0)
     return fail(CC_ERR_INVALID, "zero queue, budget or launch size");
   int rc = set_device(ctx);

@@ -31,12 +31,15 @@ __device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) 
 
 // Shared memory of one warp; Cell is the accumulator's cell: 32 bits in the
 // packet pass, 64 in the solo pass. Sky: the warp walks sky cones, whose
-// horizons are kept beside their frames.
-template <class CellT, bool Sky>
+// horizons are kept beside their frames. SmemCov: each cone's coverages are
+// kept here, where the integration in the same kernel reads every lane's
+// (else each lane keeps its own in thread-local memory, and the smaller
+// block lets more warps be resident).
+template <class CellT, bool Sky, bool SmemCov>
 struct WarpShared {
   using Cell = CellT;
   static constexpr bool kSky = Sky;
-  float cov[kBins * 32];                // each cone's 64 coverages, bin-major, lane innermost
+  static constexpr bool kSmemCov = SmemCov;
   Cell acc[kBins * 32];                 // each cone's accumulator (fixed point, units of kFixUnit)
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
   uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
@@ -44,18 +47,33 @@ struct WarpShared {
   uint32_t general[kQueueCap];          // pairs that need rasterize's general path, waiting for it
   uint32_t overflow[4];                 // word 0: cones whose 32-bit accumulation overflowed in the current mesh
   float horizon[Sky ? 3 * 32 : 4];      // sky cones: each cone's horizon, field-major
+  float cov[SmemCov ? kBins * 32 : 4];  // each cone's 64 coverages, bin-major, lane innermost
 };
-static_assert(sizeof(WarpShared<unsigned int, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-static_assert(sizeof(WarpShared<unsigned long long, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-static_assert(sizeof(WarpShared<unsigned int, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-template <bool kSky>
-using NarrowShared = WarpShared<unsigned int, kSky>;
-template <bool kSky>
-using WideShared = WarpShared<unsigned long long, kSky>;
-// Resident blocks per SM the shared memory allows: 5 x 38 KB with 32-bit
-// cells, 4 x 55 KB with 64-bit ones.
-template <class WS>
-constexpr int blocks_per_sm() { return sizeof(typename WS::Cell) == 4 ? 5 : 4; }
+static_assert(sizeof(WarpShared<unsigned int, false, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned long long, false, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned int, true, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+static_assert(sizeof(WarpShared<unsigned int, false, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
+template <bool kSky, bool kSmemCov>
+using NarrowShared = WarpShared<unsigned int, kSky, kSmemCov>;
+template <bool kSky, bool kSmemCov>
+using WideShared = WarpShared<unsigned long long, kSky, kSmemCov>;
+// The shared memory of a kernel variant's warps, and the blocks per SM it
+// fits: the split path (neither sky nor prefiltering cones) keeps coverages
+// in thread-local memory.
+template <bool kWide, bool kSky, bool kSplat>
+using KernelShared = typename std::conditional<kWide, WideShared<kSky, kSky || kSplat>,
+                                               NarrowShared<kSky, kSky || kSplat>>::type;
+template <bool kWide, bool kSky, bool kSplat>
+constexpr int resident_blocks() {
+  return (kSky || kSplat) ? (kWide ? kFusedSoloBlocksPerSm : kFusedBlocksPerSm)
+                          : (kWide ? kSoloBlocksPerSm : kBlocksPerSm);
+}
+// Per SM (228 KB): 8 x 22.8 KB and 5 x 38.9 KB split, 5 x 38.9 KB and
+// 4 x 55.3 KB otherwise, with 1 KB reserved per block.
+static_assert(8 * (kWarpsPerBlock * sizeof(KernelShared<false, false, false>) + 1024) <= 233472, "split packet pass");
+static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<true, false, false>) + 1024) <= 233472, "split solo pass");
+static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<false, true, false>) + 1024) <= 233472, "sky packet pass");
+static_assert(4 * (kWarpsPerBlock * sizeof(KernelShared<true, true, false>) + 1024) <= 233472, "sky solo pass");
 constexpr uint32_t kStatusAccOverflow = 32u;
 static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
 
@@ -111,7 +129,9 @@ struct LaneState {
   Cone cone;   // the cone in the space of the object being walked (the world's elsewhere)
   Cone world;  // instanced scenes: the cone in world space
   WS* ws;
-  float* cov;  // &ws->cov[lane]; bin b at cov[32 * b]
+  // The cone's coverages: bin b at cov[32 * b] in the warp's shared table
+  // (&ws->cov[lane]), or at cov[b] in a thread-local array.
+  float* cov;
   uint32_t full;
   uint32_t queued;  // both queues' lengths (queue_lens; the same in every lane)
   uint32_t cone_work;
@@ -121,6 +141,8 @@ struct LaneState {
   bool independent;  // sky cones: meshes combine as independent occluders (else by the maximum)
   f3 horizon;        // sky cones: the horizon in the space of the object being walked (the world's elsewhere)
   f3 world_horizon;  // sky cones in instanced scenes: the horizon in world space
+  // The cone's coverage of bin b.
+  __device__ __forceinline__ float& cov_at(int b) { return cov[(WS::kSmemCov ? 32 : 1) * b]; }
 };
 
 __device__ __forceinline__ f3 node_lo(float4 a) { return mk(a.x, a.y, a.z); }
@@ -316,7 +338,7 @@ __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState<WS>& s
     if (splat) covered = fminf(covered, 1.0f);
     else if (covered >= 1.0f - 1e-5f) covered = 1.0f;
     if (covered > 1e-6f) {
-      const float before = st.cov[32 * b];
+      const float before = st.cov_at(b);
       float after;
       if constexpr (WS::kSky) {
         after = st.independent ? 1.0f - (1.0f - before) * (1.0f - fminf(covered, 1.0f))
@@ -324,7 +346,7 @@ __device__ __forceinline__ void resolve_mesh(const DevScene& s, LaneState<WS>& s
       } else {
         after = fmaxf(before, fminf(covered, 1.0f));
       }
-      st.cov[32 * b] = after;
+      st.cov_at(b) = after;
       if (before < 1.0f && after >= 1.0f) st.full++;
     }
   }
@@ -811,14 +833,15 @@ __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, ui
 template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSplat>
 // The blocks the shared memory fits per SM; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm : kBlocksPerSm)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kSky, kSplat>())
     visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
                       const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
-  using WS = typename std::conditional<kWide, WideShared<kSky>, NarrowShared<kSky>>::type;
+  using WS = KernelShared<kWide, kSky, kSplat>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   WS* ws = reinterpret_cast<WS*>(smem_raw) + wib;
+  float cov_local[WS::kSmemCov ? 1 : kBins];  // the lane's cone's coverages, unless the warp's table holds them
   for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0;
   if (lane == 0) ws->overflow[0] = 0u;
   ws->span_lo[lane] = 68u;
@@ -911,7 +934,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
 
     LaneState<WS> st;
     st.ws = ws;
-    st.cov = ws->cov + lane;
+    st.cov = WS::kSmemCov ? ws->cov + lane : cov_local;
     st.full = 0;
     st.queued = 0;
     st.cone_work = 0;
@@ -919,7 +942,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     st.n_obj = st.n_blas = st.n_tris = 0;
     st.independent = false;
     st.horizon = st.world_horizon = mk(0.f, 0.f, 0.f);
-    for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 0.0f;
+    for (int k = 0; k < kBins; ++k) st.cov_at(k) = 0.0f;
 
     const float4 pt4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 0]);
     const float4 nm4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 1]);
@@ -978,14 +1001,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
     const bool capped = traced && st.cone_work >= st.cap;
     if (capped) st.status |= 1u;
     if (capped && info.wide_window && !info.wide_clipped) {
-      for (int k = 0; k < kBins; ++k) st.cov[32 * k] = 1.0f;
+      for (int k = 0; k < kBins; ++k) st.cov_at(k) = 1.0f;
       st.full = kBins;
     }
     if (traced && st.full >= (uint32_t)kBins) st.status |= 16u;
 
     uint32_t fw0 = 0, fw1 = 0, aw0 = 0, aw1 = 0;
     for (int k = 0; k < kBins; ++k) {
-      const float v = st.cov[32 * k];
+      const float v = st.cov_at(k);
       const uint32_t bit = 1u << (k & 31);
       if (v >= 1.0f) { if (k < 32) fw0 |= bit; else fw1 |= bit; }
       if (v > 0.0f) { if (k < 32) aw0 |= bit; else aw1 |= bit; }
@@ -1000,7 +1023,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
       if (traced) {
         float blocked = 0.0f;
         for (int b = 0; b < kBins; ++b) {
-          const float cv = st.cov[32 * b];
+          const float cv = st.cov_at(b);
           if (cv > 0.0f) blocked += cv * clipped_bin_weight(st.cone, normal, b);
         }
         const float open = clipped_window_weight(st.cone, normal);
@@ -1033,8 +1056,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
         float4* dst = reinterpret_cast<float4*>(o.cov_out + 64 * slot_local);
 #pragma unroll 4
         for (int k = 0; k < 16; ++k)
-          dst[k] = make_float4(st.cov[32 * (4 * k)], st.cov[32 * (4 * k + 1)], st.cov[32 * (4 * k + 2)],
-                               st.cov[32 * (4 * k + 3)]);
+          dst[k] = make_float4(st.cov_at(4 * k), st.cov_at(4 * k + 1), st.cov_at(4 * k + 2), st.cov_at(4 * k + 3));
       } else {
         if (out_irradiance) out_irradiance[c] = value;
         if (out_fraction) out_fraction[c] = ratio;
@@ -1044,8 +1066,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWide ? kSoloBlocksPerSm 
         float4* dst = reinterpret_cast<float4*>(out_partial + 64 * c);
 #pragma unroll 4
         for (int k = 0; k < 16; ++k)
-          dst[k] = make_float4(st.cov[32 * (4 * k)], st.cov[32 * (4 * k + 1)], st.cov[32 * (4 * k + 2)],
-                               st.cov[32 * (4 * k + 3)]);
+          dst[k] = make_float4(st.cov_at(4 * k), st.cov_at(4 * k + 1), st.cov_at(4 * k + 2), st.cov_at(4 * k + 3));
       }
     }
     __syncwarp();
@@ -1063,7 +1084,7 @@ template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false, b
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * (kWide ? sizeof(WideShared<kSky>) : sizeof(NarrowShared<kSky>));
+  const size_t smem = (size_t)kWarpsPerBlock * sizeof(KernelShared<kWide, kSky, kSplat>);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);

@@ -557,7 +557,7 @@ class Batch:
         return int(job.value)
 
     @staticmethod
-    def options(points_per_warp: int = 32, blocks_per_sm: int = 5, flags: int = _lib.CC_BATCH_GRAPH):
+    def options(points_per_warp: int = 32, blocks_per_sm: int = 8, flags: int = _lib.CC_BATCH_GRAPH):
         return _lib.BatchOptions(int(points_per_warp), int(blocks_per_sm), int(flags))
 
     def submit(self, options=None, stream: int = 0) -> None:
@@ -606,7 +606,7 @@ class Server:
 
     def __init__(self, kernel: MaskConeKernel, hbm_budget: int = 8 << 30, max_inflight: int = 4,
                  max_queue: int = 256, max_launch_cones: int = 8 << 20, points_per_warp: int = 32,
-                 blocks_per_sm: int = 5):
+                 blocks_per_sm: int = 8):
         opt = _lib.ServerOptions(int(hbm_budget), int(max_inflight), int(max_queue), int(max_launch_cones),
                                  int(points_per_warp), int(blocks_per_sm))
         h = C.c_void_p()

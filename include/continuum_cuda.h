@@ -307,7 +307,7 @@ typedef struct cc_batch cc_batch;
 
 typedef struct cc_batch_options {
   uint32_t points_per_warp; /* cones per packet: 1..32 (32) */
-  uint32_t blocks_per_sm;   /* resident blocks per SM launched: 1..5 (5) */
+  uint32_t blocks_per_sm;   /* resident blocks per SM launched: 1..8 (8) */
   uint32_t flags;           /* CC_KEEP_ORDER, CC_NO_REDO, CC_BATCH_GRAPH */
 } cc_batch_options;
 
@@ -372,10 +372,10 @@ typedef struct cc_server_options {
   uint32_t max_queue;        /* queued requests before submissions are refused with CC_ERR_BUSY (256) */
   uint64_t max_launch_cones; /* cones one launch takes at most (8M); one larger request runs alone */
   uint32_t points_per_warp;  /* 1..32 (32) */
-  uint32_t blocks_per_sm;    /* 1..5 (5) */
+  uint32_t blocks_per_sm;    /* 1..8 (8) */
 } cc_server_options;
 
-/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 8M cones per launch, 32, 5. */
+/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 8M cones per launch, 32, 8. */
 CC_API void cc_server_options_default(cc_server_options* opt);
 
 typedef struct cc_request {

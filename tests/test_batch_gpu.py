@@ -112,7 +112,7 @@ def test_every_tuned_configuration_gives_the_same_results(kernel):
     b = jobs.batch(kernel)
     best, ms = b.tune(reps=1)
     assert len(ms) == 12 and np.all(ms > 0)
-    assert best.points_per_warp in (8, 16, 32) and best.blocks_per_sm in (3, 5)
+    assert best.points_per_warp in (8, 16, 32) and best.blocks_per_sm in (4, 8)
     assert best.flags & _lib.CC_BATCH_GRAPH
     for opt in (best, Batch.options(1, 1, 0), Batch.options(32, 5, _lib.CC_KEEP_ORDER)):
         jobs.zero()
@@ -162,7 +162,7 @@ def test_batch_rejects_bad_jobs_and_options(kernel):
         b.add(scene, r.data_ptr() + 4, r.shape[0], l.data_ptr(), 1, ptrs(outs))
     assert e.value.code == _lib.CC_ERR_INVALID
     b.add(scene, r.data_ptr(), r.shape[0], l.data_ptr(), 1, ptrs(outs))
-    for bad in (Batch.options(0, 4), Batch.options(33, 4), Batch.options(32, 6), Batch.options(32, 4, 1 << 10)):
+    for bad in (Batch.options(0, 4), Batch.options(33, 4), Batch.options(32, 9), Batch.options(32, 4, 1 << 10)):
         with pytest.raises(_lib.CCError) as e:
             b.submit(bad)
         assert e.value.code == _lib.CC_ERR_INVALID
