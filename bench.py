@@ -608,9 +608,11 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, ptrs, stream=stream.cuda_stream)
 
     # This library's kernels per step: morton_keys (Morton walk order, when
-    # there are more than 64 points), the packet pass and the solo pass.
+    # there are more than 64 points), and per split chunk the cone setup, the
+    # packet pass, the solo pass and the integration.
     morton = P > 64
-    launches_per_step = 2 + (1 if morton else 0)
+    chunks = (C + (1 << 23) - 1) >> 23
+    launches_per_step = 4 * chunks + (1 if morton else 0)
 
     # Work counters (an untimed counted run): the algorithmic bytes per cone.
     work = torch.empty(C, 4, dtype=torch.int32, device=dev)
@@ -705,7 +707,8 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": (tpc * C) if tpc else None, "peak_source": peak_src,
-                     "kernel": "visibility_kernel (packet pass)", "kernel_ms": packet_ms, "solo_pass_ms": solo_ms,
+                     "kernel": "visibility_kernel (packet pass)", "kernel_ms": packet_ms,
+                     "solo_pass_and_integration_ms": solo_ms,
                      "algorithmic_bytes_per_launch": algo_bytes,
                      "bytes_model": "per cone: 32 B receiver + 16 B light + 24 B outputs + 48 B x (object + "
                                     "triangle-hierarchy nodes tested) + 48 B x triangles tested",

@@ -202,8 +202,9 @@ cudaError_t launch_batch_integrate(const BatchLaunch& b, const DevOut& o, cudaSt
 // light cones take the split path: per chunk of chunk_slots slots, setup,
 // the two passes and the integration; q.records and o.cov_out then hold
 // min(cones, chunk_slots) slots.
-// `marks` (nullable): three events recorded before the packet pass, between
-// the passes and after the solo pass (after the integration, split).
+// `marks` (nullable): three events recorded before the packet pass (split:
+// after the first chunk's setup), between the passes and after the solo pass
+// (split: after the last integration).
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t points_per_warp,
                               bool count_work, uint64_t chunk_slots, int sm_count, cudaStream_t stream,
                               const cudaEvent_t* marks);

@@ -49,8 +49,9 @@ static cudaError_t exact_pass(bool count, bool inst, bool sky, const DevScene& s
 
 // The split plain path (exact light cones): per chunk of at most `chunk`
 // slots, the cones set up, walked (the packet pass, then the solo pass over
-// the slots it listed) and integrated. For a call of several chunks the
-// middle mark follows the last chunk's packet pass.
+// the slots it listed) and integrated. The marks: after the first chunk's
+// setup, after the last chunk's packet pass, after the last integration (a
+// call of one chunk: its packet pass, then its solo pass and integration).
 static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const DevOut& o, uint32_t pw, bool count,
                                     bool inst, uint64_t chunk, int sm_count, cudaStream_t stream,
                                     const cudaEvent_t* marks) {
@@ -71,6 +72,7 @@ static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const
     }
     e = launch_cone_setup(q, base, n, const_cast<ConeRecord*>(q.records), stream);
     if (e != cudaSuccess) return e;
+    if (marks && base == 0) cudaEventRecord(marks[0], stream);
     const uint64_t packets = (n + pw - 1) / pw;
     const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const uint64_t cap = (uint64_t)sm_count * kBlocksPerSm;
@@ -95,9 +97,9 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   if (pw < 1) pw = 1;
   if (pw > 32) pw = 32;
   const uint64_t ncones = q.npoints * (uint64_t)q.nlights;
-  if (marks) cudaEventRecord(marks[0], stream);
   if (ncones == 0) {
     if (marks) {
+      cudaEventRecord(marks[0], stream);
       cudaEventRecord(marks[1], stream);
       cudaEventRecord(marks[2], stream);
     }
@@ -107,6 +109,7 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   const bool sky = (q.sky & kSkyCones) != 0u;
   const bool splat = q.prefilter > 0.0f;
   if (!sky && !splat) return split_visibility(s, q, o, pw, count, inst, chunk, sm_count, stream, marks);
+  if (marks) cudaEventRecord(marks[0], stream);
   const uint64_t packets = (ncones + pw - 1) / pw;
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
   // One resident wave: warps take packets from the shared counter.
