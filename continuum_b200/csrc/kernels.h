@@ -9,11 +9,11 @@
 namespace cc {
 
 constexpr int kWarpsPerBlock = 2;
-// Resident blocks per SM the shared memory allows. The split path's passes
-// keep each cone's coverages in thread-local memory: its packet pass (32-bit
-// accumulator cells, 22 KB per block) fits 8, its solo pass (64-bit cells,
-// 38 KB) 5. Sky and prefiltering passes keep them in shared memory, where
-// the integration in the same kernel reads every lane's: 5 and 4.
+// Resident blocks per SM the shared memory allows. Passes that keep each
+// cone's coverages in thread-local memory (the split path's, exact sky
+// cones'): the packet pass (32-bit accumulator cells, 22 KB per block) fits
+// 8, the solo pass (64-bit cells, 38 KB) 5. Prefiltering cones keep them in
+// shared memory: 5 and 4.
 constexpr int kBlocksPerSm = 8;
 constexpr int kSoloBlocksPerSm = 5;
 constexpr int kFusedBlocksPerSm = 5;
