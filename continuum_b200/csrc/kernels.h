@@ -12,12 +12,14 @@ constexpr int kWarpsPerBlock = 2;
 // Resident blocks per SM the shared memory allows. Passes that keep each
 // cone's coverages in thread-local memory (the split path's, exact sky
 // cones'): the packet pass (32-bit accumulator cells, 22 KB per block) fits
-// 8, the solo pass (64-bit cells, 38 KB) 5. Prefiltering cones keep them in
+// 8, the solo pass (64-bit cells, 38 KB) 5; prefiltering sky cones, whose
+// walk needs more registers, 6 and 5. Prefiltering light cones keep them in
 // shared memory: 5 and 4.
 constexpr int kBlocksPerSm = 8;
 constexpr int kSoloBlocksPerSm = 5;
 constexpr int kFusedBlocksPerSm = 5;
 constexpr int kFusedSoloBlocksPerSm = 4;
+constexpr int kSkySplatBlocksPerSm = 6;  // prefiltering sky cones' packet pass (thread-local coverages)
 
 struct DevQuery {
   const float4* receivers;  // 2 per point: point, normal

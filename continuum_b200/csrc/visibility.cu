@@ -112,11 +112,9 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   if (marks) cudaEventRecord(marks[0], stream);
   const uint64_t packets = (ncones + pw - 1) / pw;
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  // One resident wave: warps take packets from the shared counter. Exact sky
-  // cones keep coverages in thread-local memory, prefiltering cones in
-  // shared memory (fewer blocks fit).
-  const bool smem_table = splat;
-  const uint64_t cap = (uint64_t)sm_count * (smem_table ? kFusedBlocksPerSm : kBlocksPerSm);
+  // One resident wave: warps take packets from the shared counter; the
+  // blocks per SM follow where the variant keeps its coverages.
+  const uint64_t cap = (uint64_t)sm_count * resident_blocks_for(false, sky, splat);
   const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
   // The packet pass with 32-bit accumulator cells, the solo pass with 64-bit.
   auto packets_pass = [&](uint32_t p, uint32_t nb) {
@@ -133,7 +131,7 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   if (o.redo_list) {
     // The listed cones, each walked alone (one cone per warp; the warp still
     // shares its leaves' triangles).
-    e = solo_pass((uint32_t)sm_count * (smem_table ? kFusedSoloBlocksPerSm : kSoloBlocksPerSm));
+    e = solo_pass((uint32_t)sm_count * resident_blocks_for(true, sky, splat));
   }
   if (marks) cudaEventRecord(marks[2], stream);
   return e;

@@ -59,29 +59,32 @@ template <bool kSky, bool kSmemCov>
 using WideShared = WarpShared<unsigned long long, kSky, kSmemCov>;
 // The shared memory of a kernel variant's warps, and the blocks per SM it
 // fits. Prefiltering light cones integrate in the walk kernel, reading every
-// lane's coverages (warp_blocked), and the prefiltering walk needs more
-// registers than 8 blocks per SM leave: prefiltering cones keep the table in
-// shared memory. The split path's cones and exact sky cones (whose
-// integration reads only the lane's own) keep coverages in thread-local
-// memory.
+// lane's coverages (warp_blocked): their table stays in shared memory. The
+// split path's cones and sky cones (whose integration reads only the lane's
+// own) keep coverages in thread-local memory; the prefiltering walk of sky
+// cones needs about 165 registers, so its packet pass takes 6 blocks per SM
+// (8 would cap registers at 128 and spill).
 template <bool kSky, bool kSplat>
-constexpr bool smem_cov() { return kSplat; }
+constexpr bool smem_cov() { return kSplat && !kSky; }
 template <bool kWide, bool kSky, bool kSplat>
 using KernelShared = typename std::conditional<kWide, WideShared<kSky, smem_cov<kSky, kSplat>()>,
                                                NarrowShared<kSky, smem_cov<kSky, kSplat>()>>::type;
-template <bool kWide, bool kSky, bool kSplat>
-constexpr int resident_blocks() {
-  return smem_cov<kSky, kSplat>() ? (kWide ? kFusedSoloBlocksPerSm : kFusedBlocksPerSm)
-                                  : (kWide ? kSoloBlocksPerSm : kBlocksPerSm);
+constexpr int resident_blocks_for(bool wide, bool sky, bool splat) {
+  return (splat && !sky) ? (wide ? kFusedSoloBlocksPerSm : kFusedBlocksPerSm)
+                         : (wide ? kSoloBlocksPerSm : (splat ? kSkySplatBlocksPerSm : kBlocksPerSm));
 }
+template <bool kWide, bool kSky, bool kSplat>
+constexpr int resident_blocks() { return resident_blocks_for(kWide, kSky, kSplat); }
 // Per SM (228 KB): 8 x 22.8 KB and 5 x 38.9 KB with thread-local coverages,
 // 5 x 38.9 KB and 4 x 55.3 KB with shared ones, 1 KB reserved per block.
 static_assert(8 * (kWarpsPerBlock * sizeof(KernelShared<false, false, false>) + 1024) <= 233472, "split packet pass");
 static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<true, false, false>) + 1024) <= 233472, "split solo pass");
 static_assert(8 * (kWarpsPerBlock * sizeof(KernelShared<false, true, false>) + 1024) <= 233472, "sky packet pass");
 static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<true, true, false>) + 1024) <= 233472, "sky solo pass");
-static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<false, true, true>) + 1024) <= 233472, "prefiltering packet pass");
-static_assert(4 * (kWarpsPerBlock * sizeof(KernelShared<true, true, true>) + 1024) <= 233472, "prefiltering solo pass");
+static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<false, false, true>) + 1024) <= 233472, "prefiltering packet pass");
+static_assert(4 * (kWarpsPerBlock * sizeof(KernelShared<true, false, true>) + 1024) <= 233472, "prefiltering solo pass");
+static_assert(6 * (kWarpsPerBlock * sizeof(KernelShared<false, true, true>) + 1024) <= 233472, "prefiltering sky packet pass");
+static_assert(5 * (kWarpsPerBlock * sizeof(KernelShared<true, true, true>) + 1024) <= 233472, "prefiltering sky solo pass");
 constexpr uint32_t kStatusAccOverflow = 32u;
 static_assert(kConeFields * 32 >= 387, "the integration scratch fits in the cone table");
 
