@@ -508,7 +508,7 @@ void cc_server_options_default(cc_server_options* opt) {
   opt->hbm_budget = 8ull << 30;
   opt->max_inflight = 4;
   opt->max_queue = 256;
-  opt->max_launch_cones = 8ull << 20;
+  opt->max_launch_cones = 2ull << 20;
   opt->points_per_warp = 32;
   opt->blocks_per_sm = cc::kBlocksPerSm;
 }

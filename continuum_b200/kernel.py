@@ -605,7 +605,7 @@ class Server:
     copies overlap with other launches)."""
 
     def __init__(self, kernel: MaskConeKernel, hbm_budget: int = 8 << 30, max_inflight: int = 4,
-                 max_queue: int = 256, max_launch_cones: int = 8 << 20, points_per_warp: int = 32,
+                 max_queue: int = 256, max_launch_cones: int = 2 << 20, points_per_warp: int = 32,
                  blocks_per_sm: int = 8):
         opt = _lib.ServerOptions(int(hbm_budget), int(max_inflight), int(max_queue), int(max_launch_cones),
                                  int(points_per_warp), int(blocks_per_sm))

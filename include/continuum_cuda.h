@@ -370,12 +370,12 @@ typedef struct cc_server_options {
   uint64_t hbm_budget;       /* device bytes for requests in flight and cached results */
   uint32_t max_inflight;     /* launches in flight at once: 1..8 (4) */
   uint32_t max_queue;        /* queued requests before submissions are refused with CC_ERR_BUSY (256) */
-  uint64_t max_launch_cones; /* cones one launch takes at most (8M); one larger request runs alone */
+  uint64_t max_launch_cones; /* cones one launch takes at most (2M); one larger request runs alone */
   uint32_t points_per_warp;  /* 1..32 (32) */
   uint32_t blocks_per_sm;    /* 1..8 (8) */
 } cc_server_options;
 
-/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 8M cones per launch, 32, 8. */
+/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 2M cones per launch, 32, 8. */
 CC_API void cc_server_options_default(cc_server_options* opt);
 
 typedef struct cc_request {
