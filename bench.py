@@ -611,7 +611,7 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
     # there are more than 64 points), and per split chunk the cone setup, the
     # packet pass, the solo pass and the integration.
     morton = P > 64
-    chunks = (C + (1 << 23) - 1) >> 23
+    chunks = (C + (1 << 25) - 1) >> 25
     launches_per_step = 4 * chunks + (1 if morton else 0)
 
     # Work counters (an untimed counted run): the algorithmic bytes per cone.

@@ -65,7 +65,7 @@ struct ConeRecord {
 };
 // Slots per split chunk by default (records and masks: 368 bytes a slot).
 static_assert(sizeof(ConeRecord) == 112, "cone record layout");
-constexpr uint64_t kSplitChunk = 1ull << 23;
+constexpr uint64_t kSplitChunk = 1ull << 25;
 constexpr uint32_t kSkyCones = 1u;
 constexpr uint32_t kSkyCombineMax = 2u;      // combine meshes by the maximum, as light cones do (a diagnostic)
 constexpr uint32_t kSkyNoHorizonCull = 4u;   // walk geometry below the receiver's horizon too

@@ -82,7 +82,7 @@ CC_API int cc_context_create(int device, cc_context** out);
 CC_API int cc_context_destroy(cc_context* ctx);
 
 /* Cones one chunk of the split path holds at most (32 .. 2^31; default
- * 8,388,608). Exact light cones are set up, walked and integrated a chunk at
+ * 33,554,432). Exact light cones are set up, walked and integrated a chunk at
  * a time, with 368 bytes of device scratch per slot of one chunk (cone
  * records and masks): cc_visibility, batches submitted after the call, and
  * servers created after it (which hold at most 4,194,304) take the bound.

@@ -144,7 +144,7 @@ def test_small_split_chunks_give_the_same_results(kernel):
                 b.wait()
                 jobs.check(alone, KEYS[:5])
     finally:
-        kernel.set_split_chunk(1 << 23)
+        kernel.set_split_chunk(1 << 25)
         b.close()
         jobs.close()
 

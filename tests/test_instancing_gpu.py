@@ -116,7 +116,7 @@ def test_update_in_small_chunks_equals_the_default(kernel, world):
     count = kernel.stale_cones(scene, rec.data_ptr(), P, world.lights, boxes, stale.data_ptr())
     assert count > 1000
     try:
-        for c, chunk in zip(caches, (1 << 23, 1000)):
+        for c, chunk in zip(caches, (1 << 25, 1000)):
             kernel.set_split_chunk(chunk)
             solved = kernel.visibility_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(),
                                               {k: v.data_ptr() for k, v in c.items()})
@@ -125,5 +125,5 @@ def test_update_in_small_chunks_equals_the_default(kernel, world):
         for k in caches[0]:
             assert torch.equal(caches[0][k], caches[1][k]), k
     finally:
-        kernel.set_split_chunk(1 << 23)
+        kernel.set_split_chunk(1 << 25)
         scene.close()

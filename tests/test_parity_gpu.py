@@ -121,7 +121,7 @@ def test_split_chunks_change_no_result(kernel):
         with pytest.raises(_lib.CCError):
             kernel.set_split_chunk(31)
     finally:
-        kernel.set_split_chunk(1 << 23)
+        kernel.set_split_chunk(1 << 25)
         scene.close()
 
 

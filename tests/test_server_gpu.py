@@ -48,7 +48,7 @@ def test_each_request_is_the_same_alone_and_in_the_mix(kernel, fields, chunk):
     try:
         srv = Server(kernel, max_inflight=3, max_launch_cones=40_000)
     finally:
-        kernel.set_split_chunk(1 << 23)
+        kernel.set_split_chunk(1 << 25)
     ids = [srv.add_scene(s) for s in sc]
     rng = np.random.default_rng(4)
     reqs = []
