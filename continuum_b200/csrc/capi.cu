@@ -254,6 +254,9 @@ int cc_context_create(int device, cc_context** out) {
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->walked, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->copied, cudaEventDisableTiming);
   float disk[64];
   disk_table(disk);
   if (e == cudaSuccess) e = cc::upload_disk_table(disk);
@@ -287,6 +290,9 @@ int cc_context_destroy(cc_context* ctx) {
     b->release();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->walked) cudaEventDestroy(ctx->walked);
+  if (ctx->copied) cudaEventDestroy(ctx->copied);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   for (auto ev : ctx->marks)
     if (ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -611,13 +617,25 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
   }
   const int slot = (ctx->timed_first + ctx->timed_count) % ring;
   ctx->timed_count++;
+  // Host buffers: FULL/ANY are final once the walk passes end, so they go
+  // down on the copy stream while the integration runs.
+  const bool early = !device_ptrs && (out->full || out->any) && o.cov_out != nullptr;
   CC_CUDA(cc::launch_visibility(sd, q, o, opt.points_per_warp, o.work != nullptr, ctx->split_chunk, ctx->sm_count,
-                                stream, &ctx->marks[3 * slot]),
+                                stream, &ctx->marks[3 * slot], early ? ctx->walked : nullptr),
           "visibility launch");
   if (device_ptrs) return CC_OK;
 
-  if (out->full) CC_CUDA(cudaMemcpyAsync(out->full, o.full, ncones * 8, cudaMemcpyDeviceToHost, stream), "download");
-  if (out->any) CC_CUDA(cudaMemcpyAsync(out->any, o.any, ncones * 8, cudaMemcpyDeviceToHost, stream), "download");
+  cudaStream_t words = stream;
+  if (early) {
+    CC_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->walked, 0), "download order");
+    words = ctx->copy_stream;
+  }
+  if (out->full) CC_CUDA(cudaMemcpyAsync(out->full, o.full, ncones * 8, cudaMemcpyDeviceToHost, words), "download");
+  if (out->any) CC_CUDA(cudaMemcpyAsync(out->any, o.any, ncones * 8, cudaMemcpyDeviceToHost, words), "download");
+  if (early) {
+    CC_CUDA(cudaEventRecord(ctx->copied, ctx->copy_stream), "download order");
+    CC_CUDA(cudaStreamWaitEvent(stream, ctx->copied, 0), "download order");
+  }
   if (out->partial) CC_CUDA(cudaMemcpyAsync(out->partial, o.partial, ncones * 256, cudaMemcpyDeviceToHost, stream), "download");
   if (out->irradiance) CC_CUDA(cudaMemcpyAsync(out->irradiance, o.irradiance, ncones * 4, cudaMemcpyDeviceToHost, stream), "download");
   if (out->fraction) CC_CUDA(cudaMemcpyAsync(out->fraction, o.fraction, ncones * 4, cudaMemcpyDeviceToHost, stream), "download");
@@ -805,7 +823,7 @@ int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t
   q.records = reinterpret_cast<const cc::ConeRecord*>(scratch + cc::kStaticRecordsOffset);
   o.cov_out = reinterpret_cast<float*>(scratch + cc::kStaticMasksOffset);
   CC_CUDA(cc::launch_visibility(scene->dev(), q, o, opt.points_per_warp, o.work != nullptr, cc::kStaticMaxCones,
-                                ctx->sm_count, stream, nullptr),
+                                ctx->sm_count, stream, nullptr, nullptr),
           "visibility launch");
   return CC_OK;
 }

@@ -73,6 +73,10 @@ struct cc_context {
   DevBuf masks;     // the split path's masks (64 floats a slot), one chunk
   DevBuf counters;  // [redo count, error word]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Host-buffer calls download FULL/ANY on copy_stream once the walk is done
+  // (walked), while the integration runs; copied marks that download's end.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t walked = nullptr, copied = nullptr;
   // Kernel timing: three events per visibility call (before the packet pass,
   // between the passes, after the solo pass) in a ring of kTimingRing calls.
   static constexpr int kTimingRing = 256;

@@ -207,8 +207,10 @@ cudaError_t launch_batch_integrate(const BatchLaunch& b, const DevOut& o, cudaSt
 // `marks` (nullable): three events recorded before the packet pass (split:
 // after the first chunk's setup), between the passes and after the solo pass
 // (split: after the last integration).
+// `walked` (nullable, split path): recorded once every walk pass has run,
+// when FULL, ANY and the per-bin coverages are final.
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t points_per_warp,
                               bool count_work, uint64_t chunk_slots, int sm_count, cudaStream_t stream,
-                              const cudaEvent_t* marks);
+                              const cudaEvent_t* marks, cudaEvent_t walked);
 
 }  // namespace cc

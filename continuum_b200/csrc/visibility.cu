@@ -54,7 +54,7 @@ static cudaError_t exact_pass(bool count, bool inst, bool sky, const DevScene& s
 // call of one chunk: its packet pass, then its solo pass and integration).
 static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const DevOut& o, uint32_t pw, bool count,
                                     bool inst, uint64_t chunk, int sm_count, cudaStream_t stream,
-                                    const cudaEvent_t* marks) {
+                                    const cudaEvent_t* marks, cudaEvent_t walked) {
   if (!q0.records || !o.cov_out || chunk == 0) return cudaErrorInvalidValue;
   const uint64_t ncones = q0.npoints * (uint64_t)q0.nlights;
   cudaError_t e = cudaSuccess;
@@ -85,6 +85,10 @@ static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const
                                          (uint32_t)sm_count * kSoloBlocksPerSm, stream);
       if (e != cudaSuccess) return e;
     }
+    if (walked && base + chunk >= ncones) {
+      e = cudaEventRecord(walked, stream);
+      if (e != cudaSuccess) return e;
+    }
     e = launch_integrate(q, o, base, n, q.records, stream);
     if (e != cudaSuccess) return e;
   }
@@ -93,7 +97,8 @@ static cudaError_t split_visibility(const DevScene& s, const DevQuery& q0, const
 }
 
 cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut& o, uint32_t pw, bool count,
-                              uint64_t chunk, int sm_count, cudaStream_t stream, const cudaEvent_t* marks) {
+                              uint64_t chunk, int sm_count, cudaStream_t stream, const cudaEvent_t* marks,
+                              cudaEvent_t walked) {
   if (pw < 1) pw = 1;
   if (pw > 32) pw = 32;
   const uint64_t ncones = q.npoints * (uint64_t)q.nlights;
@@ -108,7 +113,7 @@ cudaError_t launch_visibility(const DevScene& s, const DevQuery& q, const DevOut
   const bool inst = s.xforms != nullptr;
   const bool sky = (q.sky & kSkyCones) != 0u;
   const bool splat = q.prefilter > 0.0f;
-  if (!sky && !splat) return split_visibility(s, q, o, pw, count, inst, chunk, sm_count, stream, marks);
+  if (!sky && !splat) return split_visibility(s, q, o, pw, count, inst, chunk, sm_count, stream, marks, walked);
   if (marks) cudaEventRecord(marks[0], stream);
   const uint64_t packets = (ncones + pw - 1) / pw;
   const uint64_t want = (packets + kWarpsPerBlock - 1) / kWarpsPerBlock;
