@@ -10,12 +10,17 @@ hits of a 1280 x 720 camera: 3,686,400 cones. Synthetic, seeded data.
 
 The CUDA arm prints one JSON line with the device-resident throughput
 (`value`), the end-to-end throughput through the C ABI with host buffers
-(`e2e`), the dominant kernel's roofline, a timed CPU baseline (the oracle's
-FP32 restatement of the reference's path on the host cores, a bounded
-sample), the SM clocks seen during the timed region and the kernel launch
-count. The reference arm times the reference's algorithm on the host cores
+(`e2e`), the dominant kernel's roofline, timed CPU baselines (the oracle's
+FP32 restatement of the reference's GPU path on every host core, and its
+restatement of the reference's CPU path on one and on every core), the SM
+clocks seen during the timed region and the kernel launch count. Beside it:
+the small plain workload's line (65,536 cones), the batched, served,
+instanced, lighting-cache and sky forms, and an untimed accuracy report of
+every workload against the oracle (FP32 for the parity bar, FP64 for the
+error). The reference arm times the reference's algorithm on the host cores
 (the reference is Rust + WGSL and cannot be built or run here; its FP32
-restatement in oracle/ stands in for it).
+restatement in oracle/ stands in for it) and loads nothing of this library:
+its inputs come from the oracle's own camera pass.
 Under torchrun each rank solves its own copy of the workload on its own GPU
 (weak scaling); `value` is the whole job's cones per second over the slowest
 rank's time.
@@ -43,10 +48,22 @@ NODE_BYTES = 48  # reference NodeGpu (hierarchy.rs:68-76)
 TRI_BYTES = 48   # three vec4 vertices (hierarchy.rs:12-13)
 
 
-def workload(points: int = 0):
+def workload(points: int = 0, caster: str = "library"):
+    """The plain-at-scale workload. caster "oracle": the receivers come from
+    the oracle's camera pass (the same receivers, bit for bit), so that the
+    reference arm never loads this library."""
     from continuum_b200 import scenes
 
-    w = scenes.icosphere_field(seed=2)
+    if caster == "oracle":
+        from oracle.oracle import OracleScene
+
+        w = scenes.icosphere_field(seed=2, with_receivers=False)
+        osc = OracleScene(w.meshes)
+        rec, hit = osc.primary_hits(w.camera, *w.size)
+        osc.close()
+        w.receivers = np.ascontiguousarray(rec[hit.astype(bool)])
+    else:
+        w = scenes.icosphere_field(seed=2)
     if points and points < w.receivers.shape[0]:
         width, height = w.size
         if w.receivers.shape[0] == width * height:
@@ -72,13 +89,56 @@ def cpu_threads() -> int:
     return max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
 
 
-def cpu_sample(w, target_seconds: float, offset: int = 0):
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_path_baseline(w, oscene, light_ids, max_points: int = 0, repeats: int = 5) -> dict:
+    """The reference's CPU path (cone3 + coverage + the leaf-4 BVH of bvh.rs,
+    Receiver::masked; oracle/ restates it) timed on the host cores as the
+    reference times it: one thread, and every thread taking rows in chunks of
+    64 (par_map), best of `repeats` after one warm run, the BVH's build timed
+    apart. Rect lights only (the reference's CPU path has no sphere lights);
+    `max_points` > 0 takes an evenly strided sample of the receivers."""
+    rec = w.receivers
+    if max_points and rec.shape[0] > max_points:
+        rec = np.ascontiguousarray(rec[:: rec.shape[0] // max_points][:max_points])
+    t0 = time.perf_counter()
+    bvh = oscene.cpu_bvh()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    lights9 = [np.concatenate([w.lights[l][0:3], w.lights[l][4:7], w.lights[l][8:11]]) for l in light_ids]
+    out = {"kind": "port", "code": "restatement of the reference's CPU path (cone3.rs, coverage.rs, bvh.rs; "
+                                   "Receiver::masked), not the reference binary",
+           "lights": [int(l) for l in light_ids], "points": int(rec.shape[0]),
+           "cones": int(rec.shape[0] * len(light_ids)), "bvh_build_ms": build_ms, "cpu_model": cpu_model()}
+    for key, threads in (("threads_1", 1), ("threads_all", cpu_threads())):
+        best = None
+        for rep in range(repeats + 1):
+            t0 = time.perf_counter()
+            for l9 in lights9:
+                oscene.cpu_masked_with(bvh, rec, l9, threads=threads)
+            dt = time.perf_counter() - t0
+            if rep and (best is None or dt < best):
+                best = dt
+        out[key] = {"value": out["cones"] / best, "unit": UNIT, "threads": threads, "seconds": best}
+    out["cores"] = cpu_threads()
+    bvh.close()
+    return out
+
+
+def cpu_sample(w, target_seconds: float, offset: int = 0, oscene=None):
     """Times the oracle (FP32, all host threads) on a strided sample of cones
     sized for about `target_seconds` of wall time. Returns (cones/s, cones, threads)."""
     from oracle.oracle import OracleScene
 
     threads = cpu_threads()
-    scene = OracleScene(w.meshes)
+    scene = oscene if oscene is not None else OracleScene(w.meshes)
     total = w.receivers.shape[0] * w.lights.shape[0]
     probe = np.arange(offset % 97, total, max(1, total // 16384), dtype=np.uint64)[:16384]
     t0 = time.perf_counter()
@@ -90,7 +150,8 @@ def cpu_sample(w, target_seconds: float, offset: int = 0):
     t0 = time.perf_counter()
     scene.visibility(w.receivers, w.lights, cone_ids=ids, threads=threads, partial=False)
     dt = time.perf_counter() - t0
-    scene.close()
+    if oscene is None:
+        scene.close()
     return len(ids) / dt, len(ids), threads, dt
 
 
@@ -144,21 +205,6 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def traffic_per_cone():
-    """DRAM bytes per cone of the packet kernel from the committed ncu summary
-    (profiles/visibility_kernel_icosphere_field.md), or None."""
-    p = ROOT / "profiles" / "visibility_kernel_icosphere_field.md"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_cone:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
-
-
 def max_over_ranks(x: float, world: int, device) -> float:
     """The largest of every rank's `x` (all ranks call it, in the same order);
     x itself with one rank. Each rank of a multi-GPU run solves its own replica
@@ -192,6 +238,192 @@ def timed_steps(torch, dev, stream, flush, fn, warmup, steps):
         e1.record(stream)
     torch.cuda.synchronize(dev)
     return [e0.elapsed_time(e1) for e0, e1 in ev]
+
+
+def solve_on_device(kernel, scene, rec, lig, dev, stream, partial: bool = True, work: bool = False) -> dict:
+    """One untimed plain solve with every output on the device (for checks)."""
+    import torch
+
+    P, L = rec.shape[0], lig.shape[0]
+    C = P * L
+    outs = {"full": torch.empty(C, dtype=torch.int64, device=dev), "any": torch.empty(C, dtype=torch.int64, device=dev),
+            "irradiance": torch.empty(C, device=dev), "fraction": torch.empty(C, device=dev)}
+    if partial:
+        outs["partial"] = torch.empty(C, 64, device=dev)
+    if work:
+        outs["work"] = torch.empty(C, 4, dtype=torch.int32, device=dev)
+    kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, {k: v.data_ptr() for k, v in outs.items()},
+                             stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    return outs
+
+
+def host_results(outs: dict, ids=None) -> dict:
+    """Device results (full, any, irradiance, fraction) as host arrays, for
+    every cone or the `ids` subset."""
+    import torch
+
+    sel = None if ids is None else torch.from_numpy(np.asarray(ids, np.int64)).to(outs["full"].device)
+    res = {}
+    for k in ("full", "any", "irradiance", "fraction"):
+        v = outs[k].reshape(-1)
+        v = v if sel is None else v[sel]
+        a = v.cpu().numpy()
+        res[k] = a.view(np.uint64) if k in ("full", "any") else a
+    return res
+
+
+def partial_rows(partial, ids=None):
+    """A function giving the device coverages (C, 64) of positions into `ids`
+    (or of cones), as the oracle's trace asks for them."""
+    import torch
+
+    def rows(pos):
+        cones = np.asarray(pos, np.int64) if ids is None else np.asarray(ids, np.int64)[np.asarray(pos, np.int64)]
+        return partial[torch.from_numpy(cones).to(partial.device)].cpu().numpy()
+    return rows
+
+
+def same_bits(a, b) -> np.ndarray:
+    """Per element: the same bits (mask words as integers, floats as bits)."""
+    a, b = np.asarray(a), np.asarray(b)
+    if a.dtype == np.float32:
+        return a.view(np.uint32) == b.view(np.uint32)
+    return a == b
+
+
+def strided_ids(total: int, n: int, offset: int = 0) -> np.ndarray:
+    """At most n cone numbers evenly strided over [0, total)."""
+    if n <= 0 or n >= total:
+        return np.arange(total, dtype=np.uint64)
+    stride = total // n
+    return np.arange(offset % stride, total, stride, dtype=np.uint64)[:n]
+
+
+def plain_accuracy(kernel, scene, oscene, receivers, lights, dev, stream, max_cones: int = 0,
+                   label: str = "every cone") -> dict:
+    """The accuracy report of one plain solve (untimed) against the oracle:
+    every cone, or an evenly strided sample of `max_cones`."""
+    import torch
+
+    from oracle.parity import check_against
+
+    rec = torch.from_numpy(np.ascontiguousarray(receivers)).to(dev)
+    lig = torch.from_numpy(np.ascontiguousarray(lights)).to(dev)
+    C = rec.shape[0] * lig.shape[0]
+    outs = solve_on_device(kernel, scene, rec, lig, dev, stream)
+    ids = None if not max_cones or max_cones >= C else strided_ids(C, max_cones)
+    gpu = host_results(outs, ids)
+    t0 = time.perf_counter()
+    rep = check_against(oscene, receivers, lights, gpu, partial_rows(outs["partial"], ids), cone_ids=ids,
+                        threads=cpu_threads(), sample=label if ids is None else f"{len(ids)} strided cones of {C}")
+    rep["oracle_seconds"] = time.perf_counter() - t0
+    del outs
+    return rep
+
+
+def merge_reports(reports: list, sample: str) -> dict:
+    """One accuracy report over several checked parts (jobs, requests)."""
+    n = sum(r["cones"] for r in reports)
+    out = {"cones": n, "sample": sample, "parts": len(reports),
+           "word_agreement": sum(r["word_agreement"] * r["cones"] for r in reports) / max(n, 1),
+           "max_dfraction": max((r["max_dfraction"] or 0.0) for r in reports) if reports else None,
+           "max_dirradiance_rel": max((r["max_dirradiance_rel"] or 0.0) for r in reports) if reports else None,
+           "mismatched_cones": sum(r["mismatched_cones"] for r in reports),
+           "untraced_bits": sum(max(r["untraced_bits"], 0) for r in reports)
+           if all(r["untraced_bits"] >= 0 for r in reports) else -1,
+           "meets_bar": all(r["meets_bar"] for r in reports)}
+    refs = [r["reference_summation"] for r in reports if "reference_summation" in r]
+    if refs:
+        m = sum(r["cones"] for r in reports if "reference_summation" in r)
+        out["reference_summation"] = {
+            "word_agreement": sum(x["word_agreement"] * r["cones"] for x, r in zip(refs, reports)) / max(m, 1),
+            "mismatched_cones": sum(x["mismatched_cones"] for x in refs),
+            "untraced_bits": sum(max(x["untraced_bits"], 0) for x in refs)
+            if all(x["untraced_bits"] >= 0 for x in refs) else -1,
+            "max_dfraction": max(x["max_dfraction"] for x in refs),
+            "cones_dfraction_over_1e-3": sum(x["cones_dfraction_over_1e-3"] for x in refs),
+            "exact_sums_word_agreement": {
+                k: sum(x["exact_sums_word_agreement"][k] * r["cones"] for x, r in zip(refs, reports)) / max(m, 1)
+                for k in ("reference_summation", "library")}}
+    errs = [r["fp64_max_abs_err"] for r in reports if "fp64_max_abs_err" in r]
+    if errs:
+        out["fp64_max_abs_err"] = {k: max(e.get(k, 0.0) for e in errs) for k in errs[0]
+                                   if k not in ("word_agreement", "cones_dfraction_over_1e-3")}
+        out["fp64_max_abs_err"]["cones_dfraction_over_1e-3"] = sum(e.get("cones_dfraction_over_1e-3", 0) for e in errs)
+        out["fp64_max_abs_err"]["word_agreement"] = min(e["word_agreement"] for e in errs)
+    return out
+
+
+def small_leg(args, kernel, dev, stream, flush) -> dict:
+    """The small plain workload (the ground and 64 boxes, 770 triangles; one
+    1 x 1 m rect light at 4 m; 256 x 256 receivers on the ground): 65,536
+    cones per step, device-timed (CUDA events, L2 flushed) and end to end
+    through cc_visibility with pinned host buffers; beside it the reference's
+    CPU path and the restatement of its GPU path on the host cores, and the
+    accuracy of every cone against the oracle (FP32 and FP64)."""
+    import ctypes as Cc
+
+    import torch
+
+    from continuum_b200 import _lib, scenes
+    from oracle.oracle import OracleScene
+
+    w = scenes.box_field(seed=1, grid=256)
+    scene = kernel.scene(w.meshes)
+    P, L = w.receivers.shape[0], w.lights.shape[0]
+    C = P * L
+    rec = torch.from_numpy(w.receivers).to(dev)
+    lig = torch.from_numpy(w.lights).to(dev)
+    outs = {"full": torch.empty(C, dtype=torch.int64, device=dev), "any": torch.empty(C, dtype=torch.int64, device=dev),
+            "irradiance": torch.empty(C, device=dev), "fraction": torch.empty(C, device=dev)}
+    ptrs = {k: v.data_ptr() for k, v in outs.items()}
+
+    def step():
+        kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, ptrs, stream=stream.cuda_stream)
+
+    steps = max(3, args.steps)
+    ms = float(np.mean(timed_steps(torch, dev, stream, flush, step, max(3, args.warmup), steps)))
+    rec_h = torch.from_numpy(w.receivers).pin_memory().numpy()
+    lig_h = np.ascontiguousarray(w.lights)
+    host_out = {k: torch.empty(C, dtype=dt).pin_memory().numpy() for k, dt in
+                (("full", torch.int64), ("any", torch.int64), ("irradiance", torch.float32), ("fraction", torch.float32))}
+    opt = kernel.options()
+    o = _lib.Outputs(host_out["full"].ctypes.data, host_out["any"].ctypes.data, None,
+                     host_out["irradiance"].ctypes.data, host_out["fraction"].ctypes.data, None)
+
+    def e2e_step():
+        _lib.check(_lib.load().cc_visibility(kernel.handle, scene.handle, rec_h.ctypes.data, P, lig_h.ctypes.data, L,
+                                             Cc.byref(opt), Cc.byref(o), None))
+
+    for _ in range(3):
+        e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / steps
+    out = {"workload": "small plain: a 40 x 40 m ground quad and 64 boxes (770 triangles), one 1 x 1 m one-sided rect "
+                       "light at 4 m facing down, 256 x 256 receivers on the ground over [-10, 10]^2",
+           "cones_per_step": C, "triangles": int(w.ntris), "steps": steps,
+           "value": C / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "timing": "CUDA events; L2 flushed between steps (the scene is 60 KB: cache-resident)",
+           "e2e": {"value": C / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+                   "h2d_bytes_per_step": int(rec_h.nbytes + lig_h.nbytes),
+                   "d2h_bytes_per_step": int(sum(v.nbytes for v in host_out.values()) + 8),
+                   "path": "cc_visibility with host buffers (pinned), scene resident, wall clock"}}
+    oscene = OracleScene(w.meshes)
+    if not args.no_cpu_baseline:
+        rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds, oscene=oscene)
+        out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"{n} strided cones of {C} ({dt:.2f} s wall); FP32 restatement of the "
+                                         "reference's GPU path (oracle/)"}
+    if not args.no_cpu_path:
+        out["cpu_path"] = cpu_path_baseline(w, oscene, [0])
+    if not args.no_accuracy:
+        out["accuracy"] = plain_accuracy(kernel, scene, oscene, w.receivers, w.lights, dev, stream)
+    oscene.close()
+    scene.close()
+    return out
 
 
 def batched_leg(args, kernel, dev, stream, flush) -> dict:
@@ -241,6 +473,28 @@ def batched_leg(args, kernel, dev, stream, flush) -> dict:
     # The first submission runs directly and captures the graph; later ones replay it.
     batched_ms = timed_steps(torch, dev, stream, flush, batched, 2, steps)
     b.wait()
+    acc = None
+    if not args.no_accuracy:
+        # Untimed: every 8th job's batched results (a strided sample of its
+        # cones) against the oracle, and against the plain path's.
+        from oracle.oracle import OracleScene
+        from oracle.parity import check_against
+
+        reports, same = [], True
+        for j in range(0, len(jobs), 8):
+            ids = strided_ids(cones[j], args.accuracy_cones // 8)
+            gpu = host_results(outs[j], ids)
+            alone = solve_on_device(kernel, sc[j], rec[j], lig[j], dev, stream)
+            solo = host_results(alone, ids)
+            same = same and all(same_bits(gpu[k], solo[k]).all() for k in gpu)
+            osc = OracleScene(jobs[j].meshes)
+            reports.append(check_against(osc, jobs[j].receivers, jobs[j].lights, gpu,
+                                         partial_rows(alone["partial"], ids), cone_ids=ids, threads=cpu_threads()))
+            osc.close()
+            del alone
+        acc = merge_reports(reports, f"every 8th job ({len(reports)} jobs), at most "
+                                     f"{args.accuracy_cones // 8} strided cones each")
+        acc["batched_equals_plain"] = bool(same)
     plain_ms = timed_steps(torch, dev, stream, flush, plain, 1, steps)
     kernel_times(kernel)
     b.close()
@@ -260,7 +514,7 @@ def batched_leg(args, kernel, dev, stream, flush) -> dict:
                       "graph_replay": bool(best.flags & _lib.CC_BATCH_GRAPH)},
             "tune_ms_per_candidate": [round(float(x), 3) for x in tune_ms],
             "tune_sample": "every 16th point of every job",
-            "l2": "flushed between timed steps (256 MB write)"}
+            "l2": "flushed between timed steps (256 MB write)", "accuracy": acc}
 
 
 def served_leg(args, kernel) -> dict:
@@ -365,9 +619,44 @@ def served_leg(args, kernel) -> dict:
             "plain_per_request": {"p50_ms": pct(lat_plain, 50), "p99_ms": pct(lat_plain, 99),
                                   "queries_per_s": sum(cones) / plain_span},
         })
+    acc = None
+    if not args.no_accuracy:
+        # Untimed: every 6th request's served results (from the last rate; a
+        # strided sample of its cones) against the oracle and the plain path.
+        import torch
+
+        from oracle.oracle import OracleScene
+        from oracle.parity import check_against
+
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.current_stream(dev)
+        oscenes, reports, same = {}, [], True
+        for i in range(0, len(reqs), 6):
+            si, pi, l = reqs[i]
+            if si not in oscenes:
+                oscenes[si] = OracleScene(pool[si].meshes)
+            recv = poses[si][pi].numpy()
+            C = recv.shape[0] * l.shape[0]
+            ids = strided_ids(C, args.accuracy_cones // 8)
+            gpu = {k: np.asarray(outs[i][k]).reshape(-1)[ids.astype(np.int64)] for k in
+                   ("full", "any", "irradiance", "fraction")}
+            gpu["full"], gpu["any"] = gpu["full"].view(np.uint64), gpu["any"].view(np.uint64)
+            alone = solve_on_device(kernel, sc[si], torch.from_numpy(recv).to(dev), torch.from_numpy(l).to(dev), dev,
+                                    stream)
+            solo = host_results(alone, ids)
+            same = same and all(same_bits(gpu[k], solo[k]).all() for k in gpu)
+            reports.append(check_against(oscenes[si], recv, l, gpu, partial_rows(alone["partial"], ids), cone_ids=ids,
+                                         threads=cpu_threads()))
+            del alone
+        for o_ in oscenes.values():
+            o_.close()
+        acc = merge_reports(reports, f"every 6th request ({len(reports)}) of the last rate, at most "
+                                     f"{args.accuracy_cones // 8} strided cones each")
+        acc["served_equals_plain"] = bool(same)
     for s_ in sc:
         s_.close()
-    return {"workload": "8 resident displaced-icosphere scenes (50k-3M triangles, log-uniform), 3 seeded camera poses "
+    return {"accuracy": acc,
+            "workload": "8 resident displaced-icosphere scenes (50k-3M triangles, log-uniform), 3 seeded camera poses "
                         "each (16k-2M primary hits, log-uniform); requests of 1-8 lights, each a base light recoloured "
                         "or a moved light (1:1)",
             "scene_triangles": [p.ntris for p in pool], "requests_per_rate": len(reqs),
@@ -408,6 +697,35 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
 
     steps = max(1, min(args.steps, 2))
     full_ms = float(np.mean(timed_steps(torch, dev, stream, flush, full, 1, steps)))
+    acc = {}
+    oscene = None
+    ids = strided_ids(C, args.accuracy_cones)
+
+    def check(label):
+        """Untimed: the cached results (a strided sample) against the oracle
+        and against a fresh plain solve of the scene as it now is."""
+        from oracle.parity import check_against
+
+        from continuum_b200 import _lib
+
+        gpu = host_results(cache, ids)
+        fresh = solve_on_device(kernel, scene, rec, lig, dev, stream, work=True)
+        solo = host_results(fresh, ids)
+        capped = (fresh["work"][:, 3].cpu().numpy()[ids.astype(np.int64)] & _lib.CC_CONE_CAPPED) != 0
+        differ = np.zeros(len(ids), bool)
+        for k in gpu:
+            differ |= ~same_bits(gpu[k], solo[k])
+        rep = check_against(oscene, w.receivers, w.lights, solo, partial_rows(fresh["partial"], ids), cone_ids=ids,
+                            threads=cpu_threads(), sample=f"{len(ids)} strided cones of {C}")
+        rep["cache_vs_full_solve"] = {"differing_cones": int(differ.sum()), "differing_uncapped": int((differ & ~capped).sum()),
+                                      "capped": int(capped.sum())}
+        acc[label] = rep
+
+    if not args.no_accuracy:
+        from oracle.oracle import OracleScene
+
+        oscene = OracleScene.instanced(w.geometries, w.instances, movable)
+        check("full_solve")
     stale = torch.empty(C, dtype=torch.uint8, device=dev)
     frames = []
     # Frame 0 untimed (the update path's first-call costs), then the timed frames.
@@ -424,11 +742,16 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
         ms = (time.perf_counter() - t0) * 1e3
         if f > 0:
             frames.append({"ms": ms, "stale_cones": count, "recomputed": solved, "stale_share": count / C})
+        last_placements = pl
+    if oscene is not None:
+        oscene.move(last_placements)
+        check(f"after_{args.frames + 1}_moving_frames")
+        oscene.close()
     scene.close()
     upd = float(np.mean([fr["ms"] for fr in frames])) if frames else None
     return {"workload": f"{n_obj - 1} boulder instances (10 displaced UV spheres, 10,240 triangles each) on a ground "
                         f"quad, {L} lights, 1280x720 primary hits; 1% of the instances move per frame",
-            "instanced_triangles": w.instanced_tris, "points": P, "cones": C,
+            "instanced_triangles": w.instanced_tris, "points": P, "cones": C, "accuracy": acc or None,
             "full_solve": {"value": C / (full_ms * 1e-3), "unit": UNIT, "ms": full_ms, "steps": steps,
                            "timing": "CUDA events, L2 flushed"},
             "frames": frames,
@@ -555,14 +878,21 @@ def sky_leg(args, kernel, dev, stream, flush, prefiltered_scene) -> dict:
 
 
 def reference_arm(args, rank: int) -> None:
+    """The reference's algorithm on the host cores: the oracle's FP32
+    restatement of the reference's light-cone path on every host thread, each
+    step a bounded strided sample of the workload's cones. Nothing of this
+    library is loaded (the receivers come from the oracle's camera pass)."""
     if rank != 0:
         return
-    w = workload()
+    from oracle.oracle import OracleScene
+
+    w = workload(caster="oracle")
+    oscene = OracleScene(w.meshes)
     rates = []
     total_cones, total_time = 0, 0.0
     threads = cpu_threads()
     for step in range(args.warmup + args.steps):
-        rate, n, threads, dt = cpu_sample(w, target_seconds=args.reference_seconds, offset=step)
+        rate, n, threads, dt = cpu_sample(w, target_seconds=args.reference_seconds, offset=step, oscene=oscene)
         if step >= args.warmup:
             rates.append(rate)
             total_cones += n
@@ -573,12 +903,19 @@ def reference_arm(args, rank: int) -> None:
         "warmup": args.warmup, "ms_per_step": 1e3 * total_time / max(args.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
         "config": config(1, w),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                          "sample": f"{total_cones} cones in {args.steps} strided samples of the workload's "
                                    f"{w.receivers.shape[0] * w.lights.shape[0]}; the reference (Rust/WGSL) "
                                    "cannot be built here, its FP32 restatement (oracle/) runs on all host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "inputs": "receivers from the oracle's camera pass (no library loaded)",
     }
+    if not args.no_cpu_path:
+        # The reference's CPU path (rect lights only) on the same workload:
+        # slower than the restatement of its GPU path timed above.
+        line["cpu_path"] = cpu_path_baseline(w, oscene, [i for i in range(w.lights.shape[0]) if w.lights[i][3] < 1.5],
+                                             max_points=args.cpu_path_points)
+    oscene.close()
     print(json.dumps(line), flush=True)
 
 
@@ -698,7 +1035,6 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         except Exception:
             pass
     achieved = algo_bytes / (packet_ms * 1e-3) / 1e9 if packet_ms else None
-    tpc = traffic_per_cone()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -708,7 +1044,7 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
                 "steps": e2e_steps, "path": "cc_visibility with host buffers (pinned), scene resident"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "traffic": (tpc * C) if tpc else None, "peak_source": peak_src,
+                     "traffic": None, "peak_source": peak_src,
                      "kernel": "visibility_kernel (packet pass)", "kernel_ms": packet_ms,
                      "solo_pass_and_integration_ms": solo_ms,
                      "algorithmic_bytes_per_launch": algo_bytes,
@@ -739,6 +1075,20 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         if host_empty is not None:
             host_empty()
 
+    oscene = None
+    if world == 1 and not (args.no_accuracy and args.no_cpu_baseline and args.no_cpu_path):
+        from oracle.oracle import OracleScene
+
+        oscene = OracleScene(w.meshes)
+    if world == 1 and not args.no_accuracy:
+        # Untimed: every cone of the step against the oracle (FP32 bar, FP64 error).
+        settle()
+        line["accuracy"] = {"plain_at_scale": plain_accuracy(kernel, scene, oscene, w.receivers, w.lights, dev, stream)}
+    if "small" in forms:
+        settle()
+        line["small"] = small_leg(args, kernel, dev, stream, flush)
+        if line["small"].get("accuracy") is not None:
+            line.setdefault("accuracy", {})["small"] = line["small"]["accuracy"]
     if "batched" in forms:
         settle()
         line["batched"] = batched_leg(args, kernel, dev, stream, flush)
@@ -754,11 +1104,21 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
     if "sky" in forms:
         settle()
         line["sky"] = sky_leg(args, kernel, dev, stream, flush, (scene, w))
+    for form in ("batched", "served"):
+        if line.get(form, {}).get("accuracy") is not None:
+            line.setdefault("accuracy", {})[form] = line[form]["accuracy"]
+    if line.get("instanced", {}).get("accuracy") is not None:
+        line.setdefault("accuracy", {})["instanced"] = line["instanced"]["accuracy"]
     if world == 1 and not args.no_cpu_baseline:
-        rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+        rate, n, threads, dt = cpu_sample(w, target_seconds=args.cpu_seconds, oscene=oscene)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                                 "sample": f"{n} strided cones of {C} ({dt:.1f} s wall); FP32 restatement "
-                                          "of the reference's path (oracle/)"}
+                                          "of the reference's GPU path (oracle/) on every host thread"}
+        if not args.no_cpu_path:
+            line["cpu_baseline"]["cpu_path"] = cpu_path_baseline(
+                w, oscene, [i for i in range(L) if w.lights[i][3] < 1.5], max_points=args.cpu_path_points)
+    if oscene is not None:
+        oscene.close()
     print(json.dumps(line), flush=True)
     scene.close()
     kernel.close()
@@ -773,10 +1133,16 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=1.5)
     ap.add_argument("--reference-seconds", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-path", action="store_true", help="skip the reference CPU path's 1- and all-thread timings")
+    ap.add_argument("--cpu-path-points", type=int, default=8192,
+                    help="receivers per rect light of the plain-at-scale workload's CPU-path sample")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the untimed accuracy report (profiling runs)")
+    ap.add_argument("--accuracy-cones", type=int, default=65536,
+                    help="cones checked per sampled form (batched and served: an eighth per job or request)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--forms", default="batched,served,instanced,bake,sky",
-                    help="systems forms measured beside the plain line (comma list of batched, served, instanced, "
-                         "bake, sky; none)")
+    ap.add_argument("--forms", default="small,batched,served,instanced,bake,sky",
+                    help="workloads and forms measured beside the plain line (comma list of small, batched, served, "
+                         "instanced, bake, sky; none)")
     ap.add_argument("--bake-budget", type=int, default=1 << 20, help="cones a frame of the bake leg's fixed budget")
     ap.add_argument("--instances", type=int, default=1_000_000)
     ap.add_argument("--frames", type=int, default=3, help="moving frames of the instanced leg")

@@ -13,9 +13,11 @@
  *    are host pointers; with CC_DEVICE_POINTERS in cc_options.flags the
  *    receivers, lights and every output of cc_visibility are device pointers
  *    and the call is asynchronous on the given stream.
- *  - A context is used from one host thread at a time (the reference's
- *    MaskConeKernel is !Sync for the same reason); scenes belong to the
- *    context that built them.
+ *  - A context is used from one host thread at a time and serves one call at
+ *    a time (the reference's MaskConeKernel is !Sync for the same reason):
+ *    its buffers, copy stream and events are shared by its calls, so two
+ *    calls on one context must not overlap, even on different streams.
+ *    Scenes belong to the context that built them.
  *  - Cone c = light * npoints + point (light-major). Mask words: bin b of a
  *    cone is bit (b % 32) of word (b / 32); bin b = row * 8 + col.
  *
@@ -267,9 +269,12 @@ CC_API int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const fl
  * cc_visibility without allocation: the same results as cc_visibility with
  * CC_DEVICE_POINTERS, for at most CC_STATIC_MAX_CONES cones and as many points
  * per call (larger calls are rejected with CC_ERR_INVALID), with its scratch
- * (the work counters, the re-walk list, the walk order and its sort space) in
- * one fixed 8 MiB device array of the library per device instead of context
- * buffers. It calls no cudaMalloc, cudaFree or allocating library routine, so
+ * in one fixed 48 MiB device array of the library per device instead of
+ * context buffers: the counters (256 B), the re-walk list (4 B per cone), the
+ * walk order (4 B per point), then the walk order's sort space, which the
+ * split path's cone records (112 B per cone) and masks (256 B per cone) reuse
+ * once the order is made. Every GPU that loads the library holds the 48 MiB
+ * until the process exits. It calls no cudaMalloc, cudaFree or allocating library routine, so
  * it suits callers that cannot let the library allocate: a server that admits
  * scenes against a fixed device-memory budget or whose memory a caching
  * allocator owns (cc_visibility grows its context's buffers with cudaMalloc
@@ -286,7 +291,11 @@ CC_API int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const fl
  *  - All calls on one device share the array: calls whose work can overlap on
  *    the device (on different streams, or from several host threads) race and
  *    corrupt each other's results. Issue them on one stream, or order them.
- *  - No kernel times are recorded (cc_context_kernel_times does not see it). */
+ *  - No kernel times are recorded (cc_context_kernel_times does not see it).
+ *  - The call does not wait, so it cannot return CC_ERR_STACK: a cone whose
+ *    traversal stack overflowed is flagged only in its status word
+ *    (CC_CONE_STACK in out->work's fourth word); ask for `work` to see it.
+ *    The array's error word is cleared by the next call. */
 #define CC_STATIC_MAX_CONES 131072u
 CC_API int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
                                 uint32_t nlights, const cc_options* opt, const cc_outputs* out, void* stream);
@@ -311,7 +320,7 @@ typedef struct cc_batch_options {
   uint32_t flags;           /* CC_KEEP_ORDER, CC_NO_REDO, CC_BATCH_GRAPH */
 } cc_batch_options;
 
-/* Defaults: 32 cones per packet, 5 blocks per SM, CC_BATCH_GRAPH. */
+/* Defaults: 32 cones per packet, 8 blocks per SM, CC_BATCH_GRAPH. */
 CC_API void cc_batch_options_default(cc_batch_options* opt);
 
 CC_API int cc_batch_create(cc_context* ctx, cc_batch** out);

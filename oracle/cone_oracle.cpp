@@ -527,6 +527,14 @@ template <class R> struct Light {  // LightRect (mask_cones.wgsl:843-848), Light
   R edge_v_w;
 };
 
+// How a mesh's cells are summed. kSumWalkOrder is the reference's: each
+// add rounded into the scalar type in walk order (mask_cones.wgsl:297-348,
+// 809-812). kSumFixed adds each value rounded to a multiple of 2^-24 of a bin
+// into exact integer cells (the CUDA library's accumulator: its sums do not
+// depend on the order of the adds). kSumExact sums the same values in double.
+// Only the summation differs: every value added is the same.
+enum AccumulateMode : uint32_t { kSumWalkOrder = 0, kSumFixed = 1, kSumExact = 2 };
+
 template <class R> struct Params {
   uint32_t hierarchy;  // 0 every triangle, 1 mesh hierarchy, 2 + triangle hierarchies
   R wide_extent;
@@ -534,6 +542,7 @@ template <class R> struct Params {
   uint32_t wide_cone_cap;
   R prefilter = 0;               // prefilter_bins (0: exact cones)
   bool object_prefilter = true;  // object-level splats in instanced scenes
+  uint32_t accumulate = kSumWalkOrder;  // AccumulateMode
 };
 
 template <class R> constexpr R NEAR = R(1e-4);
@@ -669,11 +678,43 @@ template <class R> Poly2<R> clip_line2(const Poly2<R>& p, V2<R> normal, R offset
 
 template <class R> struct Acc {
   R cell[68];
+  int64_t fix[68];
+  double wide[68];
+  uint32_t mode = kSumWalkOrder;
   uint32_t span_lo, span_hi;
   void reset() {
     std::fill(cell, cell + 68, R(0));
+    std::fill(fix, fix + 68, int64_t(0));
+    std::fill(wide, wide + 68, 0.0);
     span_lo = 68;
     span_hi = 0;
+  }
+  void add(uint32_t i, R v) {
+    if (mode == kSumFixed)
+      fix[i] += (int64_t)std::nearbyint(float(v) * 16777216.0f);
+    else if (mode == kSumExact)
+      wide[i] += double(v);
+    else
+      cell[i] += v;
+  }
+};
+
+// The running sum of a mesh's cells (:809-812) in the accumulator's mode.
+template <class R> struct Running {
+  R r = 0;
+  int64_t f = 0;
+  double w = 0;
+  R next(const Acc<R>& a, uint32_t b) {
+    if (a.mode == kSumFixed) {
+      f += a.fix[b];
+      return R(std::fabs(float(f) * (1.0f / 16777216.0f)));
+    }
+    if (a.mode == kSumExact) {
+      w += a.wide[b];
+      return R(std::fabs(w));
+    }
+    r += a.cell[b];
+    return std::fabs(r);
   }
 };
 
@@ -705,25 +746,25 @@ template <class R> void draw_edge(Acc<R>& acc, V2<R> q0, V2<R> q1, R weight) {
     uint32_t x1i = (uint32_t)x1_ceil;
     if (x1i <= x0i + 1) {
       R xmf = R(0.5) * (x + x_next) - x0_floor;
-      acc.cell[row + x0i] += d - d * xmf;
-      acc.cell[row + x0i + 1] += d * xmf;
+      acc.add(row + x0i, d - d * xmf);
+      acc.add(row + x0i + 1, d * xmf);
     } else {
       R s = R(1) / (x1 - x0);
       R x0f = x0 - x0_floor;
       R a0 = R(0.5) * s * (R(1) - x0f) * (R(1) - x0f);
       R x1f = x1 - x1_ceil + R(1);
       R am = R(0.5) * s * x1f * x1f;
-      acc.cell[row + x0i] += d * a0;
+      acc.add(row + x0i, d * a0);
       if (x1i == x0i + 2) {
-        acc.cell[row + x0i + 1] += d * (R(1) - a0 - am);
+        acc.add(row + x0i + 1, d * (R(1) - a0 - am));
       } else {
         R a1 = s * (R(1.5) - x0f);
-        acc.cell[row + x0i + 1] += d * (a1 - a0);
-        for (uint32_t xi = x0i + 2; xi < x1i - 1; ++xi) acc.cell[row + xi] += d * s;
+        acc.add(row + x0i + 1, d * (a1 - a0));
+        for (uint32_t xi = x0i + 2; xi < x1i - 1; ++xi) acc.add(row + xi, d * s);
         R a2 = a1 + R(x1i - x0i - 3) * s;
-        acc.cell[row + x1i - 1] += d * (R(1) - a2 - am);
+        acc.add(row + x1i - 1, d * (R(1) - a2 - am));
       }
-      acc.cell[row + x1i] += d * am;
+      acc.add(row + x1i, d * am);
     }
     x = x_next;
   }
@@ -948,6 +989,7 @@ template <class R> struct Walk {
   bool independent = false;  // sky cones: meshes combine as independent occluders (:819-821)
   R prefilter = 0;           // prefilter_bins (0: exact cones)
   bool object_prefilter = false;
+  uint32_t accumulate = kSumWalkOrder;  // how each mesh's cells are summed (AccumulateMode)
   Work work;
 };
 
@@ -983,11 +1025,11 @@ template <class R> bool splat_object_node(const Scene& s, const Cone<R>& c, uint
   if (alpha <= 0) return true;
   Acc<R> acc;
   acc.reset();
+  acc.mode = wk.accumulate;
   if (!draw_hull(acc, pts, alpha)) return true;
-  R running = 0;
+  Running<R> running;
   for (uint32_t b = acc.span_lo; b < std::min(acc.span_hi, BINS); ++b) {
-    running += acc.cell[b];
-    const R covered = std::min(std::fabs(running), R(1));
+    const R covered = std::min(running.next(acc, b), R(1));
     if (covered > R(1e-6)) {
       const R before = wk.cov[b];
       wk.cov[b] = wk.independent ? R(1) - (R(1) - before) * (R(1) - covered) : std::max(before, covered);
@@ -1025,6 +1067,7 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
                                           uint32_t hierarchy) {
   Acc<R> acc;
   acc.reset();
+  acc.mode = wk.accumulate;
   bool touched = false;
   const uint32_t* range = s.ranges.data() + 4 * m;
   const Cone<R> c = range[3] != NONE ? cone_to_object(s, world, range[3]) : world;
@@ -1062,10 +1105,9 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
       if (cover_triangle(s, c, acc, t, wk.work)) touched = true;
   }
   if (touched) {
-    R running = 0;
+    Running<R> running;
     for (uint32_t b = acc.span_lo; b < std::min(acc.span_hi, BINS); ++b) {
-      running += acc.cell[b];
-      R covered = std::fabs(running);
+      R covered = running.next(acc, b);
       if (covered >= R(1) - R(1e-5)) covered = 1;
       if (covered > R(1e-6)) {
         R before = wk.cov[b];
@@ -1429,6 +1471,7 @@ template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> norma
   wk.cone_cap = lc.wide_window ? prm.wide_cone_cap : prm.light_cone_cap;
   wk.prefilter = prm.prefilter;
   wk.object_prefilter = prm.object_prefilter;
+  wk.accumulate = prm.accumulate;
   if (traced) scene_coverage(s, lc.c, wk, prm.hierarchy);
   if (wk.cone_work >= wk.cone_cap && traced) wk.work.flags |= 1;
   if (traced && wk.cone_work >= wk.cone_cap && lc.wide_window && !lc.wide_clipped) {
@@ -1914,11 +1957,166 @@ template <class F> static void parallel_for(uint64_t n, int threads, F fn) {
   for (auto& th : pool) th.join();
 }
 
+// ---------------------------------------------------------------------------
+// Camera pass: the receivers at a pinhole camera's primary hits. Input
+// preparation, restated from the reference's camera pass (camera_dir
+// mask_cones.wgsl:1724-1729, primary_hit :1732-1760, the lifted hit point
+// surface_offset :2062-2064 and the facing normal of per_pixel_hit_color
+// :2275-2277) over this file's own hierarchies, so that the CPU legs can build
+// their inputs without the library. Every operation is the FP32 one the
+// library's host caster performs, in the same order, with the same
+// traversal order (right child popped first), so the two give the same
+// receivers bit for bit.
+// ---------------------------------------------------------------------------
+namespace camera {
+
+using V = V3<float>;
+
+// The ray (origin o, inverse direction inv) meets the box nearer than limit.
+inline bool slab(V o, V inv, const Node& n, float limit) {
+  float near_t = 0.0f, far_t = limit;
+  const float oc[3] = {o.x, o.y, o.z}, ic[3] = {inv.x, inv.y, inv.z};
+  for (int k = 0; k < 3; ++k) {
+    float a = (n.lo[k] - oc[k]) * ic[k];
+    float b = (n.hi[k] - oc[k]) * ic[k];
+    if (a > b) std::swap(a, b);
+    near_t = std::max(near_t, a);
+    far_t = std::min(far_t, b);
+    if (near_t > far_t) return false;
+  }
+  return true;
+}
+
+// Moller and Trumbore's ray-triangle test: the distance, or -1 for a miss.
+inline float hit_distance(V o, V d, V v0, V v1, V v2) {
+  const V e1 = v1 - v0, e2 = v2 - v0;
+  const V p = cross(d, e2);
+  const float det = dot(e1, p);
+  if (std::fabs(det) < 1e-12f) return -1.0f;
+  const float inv = 1.0f / det;
+  const V s = o - v0;
+  const float u = dot(s, p) * inv;
+  if (u < 0.0f || u > 1.0f) return -1.0f;
+  const V q = cross(s, e1);
+  const float v = dot(d, q) * inv;
+  if (v < 0.0f || u + v > 1.0f) return -1.0f;
+  const float t = dot(e2, q) * inv;
+  return t > 0.0f ? t : -1.0f;
+}
+
+struct Nearest {
+  float t = FLT_MAX;
+  uint32_t tri = NONE;
+  uint32_t xform = NONE;
+};
+
+inline V tri_at(const Scene& s, uint32_t t, int k) {
+  const float* p = &s.tris[12 * (size_t)t + 4 * k];
+  return V{p[0], p[1], p[2]};
+}
+
+void nearest_hit(const Scene& s, V o, V d, Nearest& h) {
+  const V inv{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  std::vector<uint32_t> objects{0};
+  std::vector<uint32_t> tri_nodes;
+  while (!objects.empty()) {
+    const Node& n = s.nodes[objects.back()];
+    objects.pop_back();
+    if (!slab(o, inv, n, h.t)) continue;
+    if (n.info[1] == 0) {
+      objects.push_back(n.info[0]);
+      objects.push_back(n.info[0] + 1);
+      continue;
+    }
+    for (uint32_t k = n.info[0]; k < n.info[0] + n.info[1]; ++k) {
+      const uint32_t* r = &s.ranges[4 * s.items[k]];
+      if (r[2] == NONE) continue;
+      V ro = o, rd = d, rinv = inv;
+      if (r[3] != NONE) {  // the ray in the placed object's space: R^T (o - t) / s, R^T d / s
+        const float* x = &s.xforms[16 * (size_t)r[3]];
+        const V a{x[0], x[1], x[2]}, b{x[4], x[5], x[6]}, c{x[8], x[9], x[10]}, tr{x[3], x[7], x[11]};
+        const float inv_scale = x[13];
+        const V q = o - tr;
+        ro = (a * q.x + b * q.y + c * q.z) * inv_scale;
+        rd = (a * d.x + b * d.y + c * d.z) * inv_scale;
+        rinv = V{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
+      }
+      tri_nodes.assign(1, r[2]);
+      while (!tri_nodes.empty()) {
+        const Node& b = s.blas[tri_nodes.back()];
+        tri_nodes.pop_back();
+        if (!slab(ro, rinv, b, h.t)) continue;
+        if (b.info[1] == 0) {
+          tri_nodes.push_back(b.info[0]);
+          tri_nodes.push_back(b.info[0] + 1);
+          continue;
+        }
+        for (uint32_t j = b.info[0]; j < b.info[0] + b.info[1]; ++j) {
+          const uint32_t t = s.blas_items[j];
+          const float dist = hit_distance(ro, rd, tri_at(s, t, 0), tri_at(s, t, 1), tri_at(s, t, 2));
+          if (dist > 0.0f && dist < h.t) {
+            h.t = dist;
+            h.tri = t;
+            h.xform = r[3];
+          }
+        }
+      }
+    }
+  }
+}
+
+// camera: eye.xyz, target.xyz, up.xyz, vertical fov in degrees. Per pixel
+// (row-major) a receiver (point.xyz 0, normal.xyz 0) and 1 if the ray hit.
+void primary_hits(const Scene& s, const float* camera, uint32_t width, uint32_t height, float* out8, uint8_t* hit,
+                  int threads) {
+  const V eye{camera[0], camera[1], camera[2]}, target{camera[3], camera[4], camera[5]};
+  const V up_world{camera[6], camera[7], camera[8]};
+  const float tan_half = std::tan(camera[9] * 3.14159265358979f / 360.0f);
+  const V fwd = normalize(target - eye);
+  const V right = normalize(cross(fwd, up_world));
+  const V up = cross(right, fwd);
+  const float aspect = float(width) / float(height);
+  parallel_for(height, threads, [&](uint64_t row) {
+    for (uint32_t x = 0; x < width; ++x) {
+      const float sx = ((float(x) + 0.5f) / float(width) * 2.0f - 1.0f) * tan_half * aspect;
+      const float sy = (1.0f - (float(row) + 0.5f) / float(height) * 2.0f) * tan_half;
+      const V d = normalize(fwd + right * sx + up * sy);
+      Nearest h;
+      nearest_hit(s, eye, d, h);
+      const size_t i = (size_t)row * width + x;
+      float* o = out8 + 8 * i;
+      std::fill(o, o + 8, 0.0f);
+      hit[i] = h.tri != NONE;
+      if (h.tri == NONE) continue;
+      const V v0 = tri_at(s, h.tri, 0), v1 = tri_at(s, h.tri, 1), v2 = tri_at(s, h.tri, 2);
+      V n = normalize(cross(v1 - v0, v2 - v0));
+      if (h.xform != NONE) {  // the object's normal in world space: R n
+        const float* x = &s.xforms[16 * (size_t)h.xform];
+        n = normalize(V{x[0] * n.x + x[1] * n.y + x[2] * n.z, x[4] * n.x + x[5] * n.y + x[6] * n.z,
+                        x[8] * n.x + x[9] * n.y + x[10] * n.z});
+      }
+      if (dot(n, d) > 0.0f) n = n * -1.0f;
+      const V point = (eye + d * h.t) + n * std::max(1e-4f, 2e-6f * h.t);
+      o[0] = point.x;
+      o[1] = point.y;
+      o[2] = point.z;
+      o[4] = n.x;
+      o[5] = n.y;
+      o[6] = n.z;
+    }
+  });
+}
+
+}  // namespace camera
+
 }  // namespace oracle
 
 using namespace oracle;
 
 extern "C" {
+
+int oracle_cpu_masked_with(void* sp, void* bvh_p, const float* receivers, uint64_t npoints, const float* light9,
+                           float* visible, float* total, uint32_t* visited, int threads);
 
 // Builds the reference's host layouts from meshes given as 9 floats per
 // triangle, `mesh_counts[m]` triangles each, consecutive.
@@ -2079,6 +2277,7 @@ struct OracleParams {
   uint32_t wide_cone_cap;
   float prefilter;            // prefilter_bins (0: exact cones)
   uint32_t object_prefilter;  // object-level splats (instanced scenes)
+  uint32_t accumulate;        // AccumulateMode: 0 the reference's walk-order sums, 1 fixed point, 2 double
 };
 
 // Visibility of cones (light l, receiver p), cone id c = l * npoints + p,
@@ -2098,7 +2297,7 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
   auto run = [&](auto zero) {
     using R = decltype(zero);
     Params<R> prm{prm_in->hierarchy, R(prm_in->wide_extent), prm_in->light_cone_cap, prm_in->wide_cone_cap,
-                  R(prm_in->prefilter), prm_in->object_prefilter != 0};
+                  R(prm_in->prefilter), prm_in->object_prefilter != 0, prm_in->accumulate};
     parallel_for(n, threads, [&](uint64_t i) {
       uint64_t c = cone_ids ? cone_ids[i] : i;
       uint64_t l = c / npoints, p = c % npoints;
@@ -2193,6 +2392,23 @@ int oracle_cpu_masked(void* sp, const float* receivers, uint64_t npoints, const 
                       float* visible, float* total, uint32_t* visited, int threads) {
   Scene* s = static_cast<Scene*>(sp);
   cpu::Bvh* bvh = use_bvh ? cpu::build_bvh(*s) : nullptr;
+  oracle_cpu_masked_with(sp, bvh, receivers, npoints, light9, visible, total, visited, threads);
+  delete bvh;
+  return 0;
+}
+
+// The reference CPU path's leaf-4 BVH (bvh.rs) alone, so that its build time
+// is measured apart from the cones (lib.rs:3497-3510 reports them apart).
+void* oracle_cpu_bvh_create(void* sp) { return cpu::build_bvh(*static_cast<Scene*>(sp)); }
+void oracle_cpu_bvh_destroy(void* bvh) { delete static_cast<cpu::Bvh*>(bvh); }
+
+// oracle_cpu_masked over a BVH made by oracle_cpu_bvh_create (null: brute
+// force). Threads take rows in chunks of 64 from a shared counter, as the
+// reference's par_map does (experiments/flatland/src/incremental.rs:124-154).
+int oracle_cpu_masked_with(void* sp, void* bvh_p, const float* receivers, uint64_t npoints, const float* light9,
+                           float* visible, float* total, uint32_t* visited, int threads) {
+  Scene* s = static_cast<Scene*>(sp);
+  const cpu::Bvh* bvh = static_cast<const cpu::Bvh*>(bvh_p);
   cpu::V corner{light9[0], light9[1], light9[2]}, eu{light9[3], light9[4], light9[5]}, ev{light9[6], light9[7], light9[8]};
   parallel_for(npoints, threads, [&](uint64_t p) {
     const float* rc = receivers + 8 * p;
@@ -2203,8 +2419,13 @@ int oracle_cpu_masked(void* sp, const float* receivers, uint64_t npoints, const 
     if (total) total[p] = t;
     if (visited) visited[p] = vis;
   });
-  delete bvh;
   return 0;
+}
+
+// Receivers at a pinhole camera's primary hits (camera::primary_hits).
+void oracle_primary_hits(void* sp, const float* camera10, uint32_t width, uint32_t height, float* out8, uint8_t* hit,
+                         int threads) {
+  camera::primary_hits(*static_cast<const Scene*>(sp), camera10, width, height, out8, hit, threads);
 }
 
 // The DISK table as this file computes it (64 doubles).

@@ -19,7 +19,13 @@ NODE_DTYPE = np.dtype([("lo", "<f4", 4), ("hi", "<f4", 4), ("info", "<u4", 4)])
 
 class _Params(C.Structure):
     _fields_ = [("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
-                ("wide_cone_cap", C.c_uint32), ("prefilter", C.c_float), ("object_prefilter", C.c_uint32)]
+                ("wide_cone_cap", C.c_uint32), ("prefilter", C.c_float), ("object_prefilter", C.c_uint32),
+                ("accumulate", C.c_uint32)]
+
+#: How each mesh's cells are summed: the reference's sums in walk order in
+#: the run's precision; each add rounded to 2^-24 of a bin into exact integer
+#: cells (the CUDA library's accumulator); exact sums in double.
+SUM_WALK_ORDER, SUM_FIXED, SUM_EXACT = 0, 1, 2
 
 
 def load():
@@ -42,6 +48,12 @@ def load():
         lib.oracle_cpu_masked.restype = I
         lib.oracle_cpu_masked.argtypes = [P, P, U64, P, I, P, P, P, I]
         lib.oracle_disk_table.argtypes = [P]
+        lib.oracle_cpu_masked_with.restype = I
+        lib.oracle_cpu_masked_with.argtypes = [P, P, P, U64, P, P, P, P, I]
+        lib.oracle_cpu_bvh_create.restype = P
+        lib.oracle_cpu_bvh_create.argtypes = [P]
+        lib.oracle_cpu_bvh_destroy.argtypes = [P]
+        lib.oracle_primary_hits.argtypes = [P, P, U32, U32, P, P, I]
         lib.oracle_cpu_weights.restype = I
         lib.oracle_cpu_weights.argtypes = [P, P, P, P]
         lib.oracle_poly_overflows.restype = U64
@@ -132,7 +144,7 @@ class OracleScene:
     def visibility(self, receivers: np.ndarray, lights: np.ndarray, hierarchy: int = 2, precision: int = 4,
                    cone_ids: np.ndarray | None = None, threads: int | None = None, wide_extent: float = 8.0,
                    light_cone_cap: int = 4096, wide_cone_cap: int = 512, partial: bool = True, prefilter: float = 0.0,
-                   object_prefilter: bool = True) -> dict:
+                   object_prefilter: bool = True, accumulate: int = 0) -> dict:
         """Per-cone results (cone c = light * npoints + point), for all cones or
         the `cone_ids` subset (outputs in subset order)."""
         rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
@@ -146,7 +158,8 @@ class OracleScene:
         frac = np.zeros(n, np.float32)
         work = np.zeros((n, 4), np.uint32)
         unsh = np.zeros(n, np.float32)
-        prm = _Params(hierarchy, wide_extent, light_cone_cap, wide_cone_cap, prefilter, 1 if object_prefilter else 0)
+        prm = _Params(hierarchy, wide_extent, light_cone_cap, wide_cone_cap, prefilter, 1 if object_prefilter else 0,
+                      int(accumulate))
         rc = load().oracle_visibility(self._h, _p(rec), rec.shape[0], _p(lig), lig.shape[0], C.byref(prm), _p(ids),
                                       0 if ids is None else len(ids), precision, _p(full), _p(any_), _p(part),
                                       _p(irr), _p(frac), _p(work), _p(unsh), threads or default_threads())
@@ -200,9 +213,54 @@ class OracleScene:
                                  _p(visited), threads or default_threads())
         return vis, tot
 
+    def cpu_bvh(self) -> "CpuBvh":
+        """The reference CPU path's leaf-4 BVH (bvh.rs), built alone so that
+        its build time can be measured apart from the cones."""
+        return CpuBvh(self)
+
+    def cpu_masked_with(self, bvh: "CpuBvh | None", receivers: np.ndarray, light9, threads: int | None = None):
+        """cpu_masked over a prebuilt BVH (None: every triangle tested)."""
+        rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
+        l9 = np.ascontiguousarray(light9, np.float32).reshape(9)
+        vis = np.zeros(rec.shape[0], np.float32)
+        tot = np.zeros(rec.shape[0], np.float32)
+        load().oracle_cpu_masked_with(self._h, None if bvh is None else bvh._h, _p(rec), rec.shape[0], _p(l9),
+                                      _p(vis), _p(tot), None, threads or default_threads())
+        return vis, tot
+
+    def primary_hits(self, camera, width: int, height: int, threads: int | None = None):
+        """Receivers (H*W, 8) at a pinhole camera's primary hits and the hit
+        mask, cast over this scene's own hierarchies (the same receivers as
+        the library's host caster, bit for bit)."""
+        cam = np.ascontiguousarray(np.asarray(camera, np.float32).reshape(10))
+        out = np.zeros((width * height, 8), np.float32)
+        hit = np.zeros(width * height, np.uint8)
+        load().oracle_primary_hits(self._h, _p(cam), int(width), int(height), _p(out), _p(hit),
+                                   int(threads or default_threads()))
+        return out, hit
+
     def close(self):
         if self._h:
             load().oracle_scene_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CpuBvh:
+    """The reference CPU path's BVH over an OracleScene's triangles."""
+
+    def __init__(self, scene: OracleScene):
+        self.scene = scene
+        self._h = C.c_void_p(load().oracle_cpu_bvh_create(scene._h))
+
+    def close(self):
+        if self._h:
+            load().oracle_cpu_bvh_destroy(self._h)
             self._h = C.c_void_p(None)
 
     def __del__(self):
