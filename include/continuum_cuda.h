@@ -345,7 +345,7 @@ CC_API int cc_batch_submit(cc_batch* batch, const cc_batch_options* opt, void* s
  * not finished, CC_ERR_STACK if a traversal stack overflowed, else CC_OK. */
 CC_API int cc_batch_wait(cc_batch* batch, uint32_t timeout_ms);
 /* The autotuner: times every candidate launch configuration (cones per
- * packet 8, 16, 32 x Morton or given walk order x 3 or 5 blocks per SM) on
+ * packet 8, 16, 32 x Morton or given walk order x 4 or 8 blocks per SM) on
  * this batch, `reps` runs each, and writes the fastest to *best (keeping
  * base->flags' CC_BATCH_GRAPH and CC_NO_REDO; base nullable). ms_out
  * (nullable, max_candidates entries) receives each candidate's best time in
