@@ -37,6 +37,7 @@ CC_CONE_ACC_WIDE = 32
 CC_NO_OBJECT_PREFILTER = 8
 CC_SKY_COMBINE_MAX = 1
 CC_SKY_NO_HORIZON_CULL = 2
+CC_SKY_OBJECT_FRAME = 4
 
 #: Every symbol include/continuum_cuda.h declares.
 EXPORTS = (

@@ -688,7 +688,8 @@ int cc_sky_visibility(cc_context* ctx, const cc_scene* scene, const float* recei
   if (!ctx || !scene || !irradiance) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
   if (npoints && !receivers) return fail(CC_ERR_INVALID, "null inputs");
-  if (sky_flags & ~(CC_SKY_COMBINE_MAX | CC_SKY_NO_HORIZON_CULL)) return fail(CC_ERR_INVALID, "unknown sky flags");
+  if (sky_flags & ~(CC_SKY_COMBINE_MAX | CC_SKY_NO_HORIZON_CULL | CC_SKY_OBJECT_FRAME))
+    return fail(CC_ERR_INVALID, "unknown sky flags");
   if (npoints >= (0xffffffffull / 6)) return fail(CC_ERR_INVALID, "too many receivers in one call");
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
@@ -700,6 +701,7 @@ int cc_sky_visibility(cc_context* ctx, const cc_scene* scene, const float* recei
   uint32_t sky = cc::kSkyCones;
   if (sky_flags & CC_SKY_COMBINE_MAX) sky |= cc::kSkyCombineMax;
   if (sky_flags & CC_SKY_NO_HORIZON_CULL) sky |= cc::kSkyNoHorizonCull;
+  if (sky_flags & CC_SKY_OBJECT_FRAME) sky |= cc::kSkyObjectFrame;
   // The face cones run on device buffers: the caller's with device pointers,
   // else the context's.
   cc_outputs fo{};

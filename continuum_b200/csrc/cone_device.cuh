@@ -689,17 +689,32 @@ __device__ __forceinline__ float clipped_window_weight(const Cone& c, f3 n) {
                              direction(c, 0.f, 1.f));
 }
 
-// sky_face (:1444-1478) in world axes: cube face f (axis f / 2, negative for
-// odd f) around `apex`, reaching kSkyFar past it (its horizon, the
-// receiver's normal or zero, is the caller's). Returns whether any of its
+// rotate_to_world (:65-67): a direction of the space of the object placed by
+// transform X, in world space.
+__device__ __forceinline__ f3 rotate_to_world(f3 d, const float4* __restrict__ X) {
+  const float4 r0 = __ldg(X), r1 = __ldg(X + 1), r2 = __ldg(X + 2);
+  return mk(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
+            r2.x * d.x + r2.y * d.y + r2.z * d.z);
+}
+
+// sky_face (:1444-1478): cube face f (axis f / 2, negative for odd f) around
+// `apex`, reaching kSkyFar past it (its horizon, the receiver's normal or
+// zero, is the caller's), in world axes or, with `frame` (the transform of
+// the object the receiver lies on: the reference's sky_frame, :1432-1456),
+// in that object's axes turned to world space. Returns whether any of its
 // directions lies above the horizon of `normal`.
-__device__ __forceinline__ bool sky_face(uint32_t f, f3 apex, f3 normal, Cone& c) {
+__device__ __forceinline__ bool sky_face(uint32_t f, f3 apex, f3 normal, Cone& c,
+                                         const float4* __restrict__ frame = nullptr) {
   const uint32_t axis = f / 2u;
   const float sign = (f & 1u) ? -1.0f : 1.0f;
   f3 forward = mk(0.f, 0.f, 0.f), right = mk(0.f, 0.f, 0.f);
   if (axis == 0u) forward.x = sign; else if (axis == 1u) forward.y = sign; else forward.z = sign;
   const uint32_t r = (axis + 1u) % 3u;
   if (r == 0u) right.x = 1.0f; else if (r == 1u) right.y = 1.0f; else right.z = 1.0f;
+  if (frame) {
+    forward = rotate_to_world(forward, frame);
+    right = rotate_to_world(right, frame);
+  }
   c.apex = apex;
   c.right = right;
   c.up = cross(forward, right);

@@ -69,6 +69,7 @@ constexpr uint64_t kSplitChunk = 1ull << 25;
 constexpr uint32_t kSkyCones = 1u;
 constexpr uint32_t kSkyCombineMax = 2u;      // combine meshes by the maximum, as light cones do (a diagnostic)
 constexpr uint32_t kSkyNoHorizonCull = 4u;   // walk geometry below the receiver's horizon too
+constexpr uint32_t kSkyObjectFrame = 8u;     // faces turn with the object each receiver lies on (point.w)
 
 // Scratch bytes walk_order needs for `npoints` receivers.
 size_t walk_order_scratch_bytes(uint64_t npoints);

@@ -984,8 +984,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
       st.cap = rec.g.z;
     } else if constexpr (WS::kSky) {
       // Sky face l of the receiver (sky_face, :1444-1478); walked without a
-      // cap (:1059, :1305).
-      traced = valid && sky_face(l, point, normal, st.cone);
+      // cap (:1059, :1305). With kSkyObjectFrame the receiver's point.w holds
+      // (as bits) the object it lies on, whose transform turns the faces
+      // (sky_frame = meshes[m].w, :2286, :3602); objects without one, and
+      // NONE, keep world axes.
+      const float4* frame = nullptr;
+      if ((q.sky & kSkyObjectFrame) && s.xforms) {
+        const uint32_t m = __float_as_uint(pt4.w);
+        if (m < s.nmeshes) {
+          const uint32_t x = __ldg(&s.meshes[m]).w;
+          if (x != kNoneU) frame = s.xforms + 4 * (size_t)x;
+        }
+      }
+      traced = valid && sky_face(l, point, normal, st.cone, frame);
       st.cap = 0xffffffffu;
       st.independent = (q.sky & kSkyCombineMax) == 0u;
       st.horizon = (q.sky & kSkyNoHorizonCull) == 0u ? normal : mk(0.f, 0.f, 0.f);

@@ -26,6 +26,7 @@ pub const CC_BATCH_GRAPH: u32 = 8;
 /// cc_sky_visibility flags
 pub const CC_SKY_COMBINE_MAX: u32 = 1;
 pub const CC_SKY_NO_HORIZON_CULL: u32 = 2;
+pub const CC_SKY_OBJECT_FRAME: u32 = 4;
 
 /// Status bits of a cone (the fourth word of cc_outputs.work).
 pub const CC_CONE_CAPPED: u32 = 1;

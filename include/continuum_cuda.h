@@ -239,6 +239,11 @@ CC_API int64_t cc_scene_coverage(const cc_scene* scene, float* blas27, uint64_t 
 /* cc_sky_visibility flags */
 #define CC_SKY_COMBINE_MAX 1u      /* meshes combine by the maximum, as light cones do (MaskConeKernel::set_sky_combination_max) */
 #define CC_SKY_NO_HORIZON_CULL 2u  /* walk geometry below the receiver's horizon too (set_sky_horizon_cull(false)) */
+#define CC_SKY_OBJECT_FRAME 4u     /* faces turn with the object each receiver lies on (set_sky_object_frame(true)):
+                                      the receiver's point.w holds that object's index among the scene's meshes as
+                                      the bits of a uint32 (0xffffffff, or an object without a transform: world
+                                      axes); the cube's axes are the object's, turned to world space (sky_frame,
+                                      mask_cones.wgsl:1432-1456, :2286) */
 
 /* A uniform sky through six cube-face mask cones per receiver (the sky light
  * of mask_cones.wgsl:1323-1511, sky_irradiance :1411-1426, for a uniform sky

@@ -1513,13 +1513,26 @@ constexpr float SKY_FAR = 1e7f;  // :1326
 
 // sky_face (:1444-1478): cube face f around `apex`; returns whether any of its
 // window's corner directions lies above the horizon of `normal`.
-template <class R> bool sky_face(uint32_t f, V3<R> apex, V3<R> normal, bool horizon_cull, Cone<R>& c) {
+// `frame` (nullable): the rotation rows of the transform of the object the
+// receiver lies on (sky_frame, :1432-1456): the face's axes are turned to
+// world space by rotate_to_world (:65-67).
+template <class R> bool sky_face(uint32_t f, V3<R> apex, V3<R> normal, bool horizon_cull, Cone<R>& c,
+                                 const float* frame = nullptr) {
   const uint32_t axis = f / 2;
   const R sign = (f & 1u) ? R(-1) : R(1);
   R fw[3] = {0, 0, 0}, rt[3] = {0, 0, 0};
   fw[axis] = sign;
   rt[(axis + 1) % 3] = 1;
-  const V3<R> forward{fw[0], fw[1], fw[2]}, right{rt[0], rt[1], rt[2]};
+  V3<R> forward{fw[0], fw[1], fw[2]}, right{rt[0], rt[1], rt[2]};
+  if (frame) {
+    auto to_world = [&](V3<R> d) {
+      return V3<R>{R(frame[0]) * d.x + R(frame[1]) * d.y + R(frame[2]) * d.z,
+                   R(frame[4]) * d.x + R(frame[5]) * d.y + R(frame[6]) * d.z,
+                   R(frame[8]) * d.x + R(frame[9]) * d.y + R(frame[10]) * d.z};
+    };
+    forward = to_world(forward);
+    right = to_world(right);
+  }
   c.apex = apex;
   c.right = right;
   c.up = cross(forward, right);
@@ -1543,10 +1556,12 @@ template <class R> bool sky_face(uint32_t f, V3<R> apex, V3<R> normal, bool hori
 // light per unit sky radiance.
 template <class R> R sky_face_irradiance(const Scene& s, uint32_t f, V3<R> point, V3<R> normal, uint32_t hierarchy,
                                          bool combine_max, bool horizon_cull, R prefilter, bool object_prefilter,
-                                         R* cov_out, Work* work) {
+                                         R* cov_out, Work* work, const float* frame = nullptr,
+                                         uint32_t accumulate = kSumWalkOrder) {
   Cone<R> c;
-  const bool above = sky_face(f, point, normal, horizon_cull, c);
+  const bool above = sky_face(f, point, normal, horizon_cull, c, frame);
   Walk<R> wk;
+  wk.accumulate = accumulate;
   std::fill(wk.cov, wk.cov + BINS, R(0));
   wk.independent = !combine_max;
   wk.prefilter = prefilter;
@@ -2337,10 +2352,12 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
 // Sky irradiance per unit radiance per receiver (sky_irradiance, :1411-1426:
 // the six faces summed in order) and, nullable, per face cone c = face *
 // npoints + point: its light, FULL/ANY words, coverage and work counters.
-// flags: 1 combine by the maximum, 2 no horizon cull.
+// flags: 1 combine by the maximum, 2 no horizon cull, 4 no object-level
+// splats, 8 faces in the frame of the object each receiver lies on (its
+// point.w holds the object's index as bits; sky_frame, :1432-1456, :2286).
 int oracle_sky_visibility(void* sp, const float* receivers, uint64_t npoints, uint32_t hierarchy, uint32_t flags,
                           float prefilter, int precision, float* irradiance, float* face_light, uint32_t* full,
-                          uint32_t* any, float* partial, uint32_t* work, int threads) {
+                          uint32_t* any, float* partial, uint32_t* work, int threads, uint32_t accumulate) {
   Scene* s = static_cast<Scene*>(sp);
   if (!s || !irradiance) return 1;
   if (prefilter > 0.0f) build_coverage(*s);
@@ -2349,12 +2366,18 @@ int oracle_sky_visibility(void* sp, const float* receivers, uint64_t npoints, ui
     parallel_for(npoints, threads, [&](uint64_t p) {
       const float* rc = receivers + 8 * p;
       const V3<R> point{R(rc[0]), R(rc[1]), R(rc[2])}, normal{R(rc[4]), R(rc[5]), R(rc[6])};
+      const float* frame = nullptr;
+      if (flags & 8u) {
+        uint32_t m;
+        std::memcpy(&m, rc + 3, 4);
+        if (m < s->nmeshes && s->ranges[4 * m + 3] != NONE) frame = &s->xforms[16 * (size_t)s->ranges[4 * m + 3]];
+      }
       R total = 0;
       for (uint32_t f = 0; f < 6; ++f) {
         R cov[BINS];
         Work wk;
         const R v = sky_face_irradiance(*s, f, point, normal, hierarchy, (flags & 1u) != 0, (flags & 2u) == 0,
-                                        R(prefilter), (flags & 4u) == 0, cov, &wk);
+                                        R(prefilter), (flags & 4u) == 0, cov, &wk, frame, accumulate);
         total += v;
         const uint64_t c = f * npoints + p;
         if (face_light) face_light[c] = float(v);

@@ -44,7 +44,7 @@ def load():
         lib.oracle_visibility.argtypes = [P, P, U64, P, U32, C.POINTER(_Params), P, U64, I, P, P, P, P, P, P, P, I]
         lib.oracle_scene_coverage.argtypes = [P, P, P]
         lib.oracle_sky_visibility.restype = I
-        lib.oracle_sky_visibility.argtypes = [P, P, U64, U32, U32, C.c_float, I, P, P, P, P, P, P, I]
+        lib.oracle_sky_visibility.argtypes = [P, P, U64, U32, U32, C.c_float, I, P, P, P, P, P, P, I, U32]
         lib.oracle_cpu_masked.restype = I
         lib.oracle_cpu_masked.argtypes = [P, P, U64, P, I, P, P, P, I]
         lib.oracle_disk_table.argtypes = [P]
@@ -177,11 +177,14 @@ class OracleScene:
         return blas, obj
 
     def sky_visibility(self, receivers: np.ndarray, hierarchy: int = 2, flags: int = 0, precision: int = 4,
-                       threads: int | None = None, faces: bool = True, prefilter: float = 0.0) -> dict:
+                       threads: int | None = None, faces: bool = True, prefilter: float = 0.0,
+                       accumulate: int = 0) -> dict:
         """Sky cones (six cube faces per receiver): irradiance per unit sky
         radiance per receiver, and per face cone c = face * npoints + point its
         light, FULL/ANY words, coverage and work counters. flags: 1 combine
-        meshes by the maximum, 2 walk geometry below the horizon too."""
+        meshes by the maximum, 2 walk geometry below the horizon too, 8 faces
+        in the frame of the object each receiver lies on (its point.w holds
+        the object's index as the bits of a uint32)."""
         rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
         n = rec.shape[0]
         irr = np.zeros(n, np.float32)
@@ -194,7 +197,7 @@ class OracleScene:
         rc = load().oracle_sky_visibility(self._h, _p(rec), n, hierarchy, flags, prefilter, precision, _p(irr),
                                           _p(g("face_light")),
                                           _p(g("full")), _p(g("any")), _p(g("partial")), _p(g("work")),
-                                          threads or default_threads())
+                                          threads or default_threads(), int(accumulate))
         if rc != 0:
             raise RuntimeError(f"oracle_sky_visibility failed: {rc}")
         if faces:

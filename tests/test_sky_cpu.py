@@ -59,3 +59,35 @@ def test_float_matches_double_and_flags_change_what_they_should():
     face_light = r32["face_light"].reshape(6, -1)
     assert np.all(face_light[3] == 0.0)
     assert np.allclose(face_light.sum(0), r32["irradiance"], atol=1e-5)
+
+
+def test_open_sky_is_pi_in_any_objects_frame():
+    """Faces turned with the receiver's object (flag 8: sky_frame,
+    mask_cones.wgsl:1432-1456) still tile the hemisphere: a uniform open sky
+    gives pi whatever the object's rotation; the turned faces see a wall
+    differently from world-axis faces, but their light sums to the same
+    total where nothing blocks it."""
+    from continuum_b200._lib import INSTANCE_DTYPE
+
+    rng = np.random.default_rng(6)
+    geo = [scenes.box_mesh((-1.0, -1.0, -1.0), (1.0, 1.0, 1.0))]
+    inst = np.zeros(5, INSTANCE_DTYPE)
+    for i in range(5):
+        a = rng.normal(size=3)
+        a /= np.linalg.norm(a)
+        ang = rng.uniform(0, 2 * math.pi)
+        k = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        rot = np.eye(3) + math.sin(ang) * k + (1 - math.cos(ang)) * k @ k  # Rodrigues
+        inst[i] = (0, rot.astype(np.float32).reshape(9), 1.0, (i * 10.0, -1e4, 0.0))
+    o = OracleScene.instanced(geo, inst)
+    normals = rng.normal(size=(40, 3))
+    normals[:, 1] = np.abs(normals[:, 1]) + 0.3
+    rec = ground_receivers(normals)
+    rec[:, 3] = (np.arange(40, dtype=np.uint32) % 5).view(np.float32)  # the object each receiver lies on
+    for precision, tol in ((8, 1e-7), (4, 2e-5)):
+        framed = o.sky_visibility(rec, precision=precision, flags=8)
+        assert np.abs(framed["irradiance"] - math.pi).max() <= tol * math.pi
+    world = o.sky_visibility(rec, precision=8)
+    framed = o.sky_visibility(rec, precision=8, flags=8)
+    assert not np.allclose(world["face_light"], framed["face_light"])  # the faces did turn
+    o.close()

@@ -2,12 +2,15 @@
 the FULL/ANY words and coverage, per face and per receiver the light within
 2e-3 of the open sky's (pi); the open sky is pi.
 
-Mask words: every disagreeing bit must be explained by coverage within 2e-5
-of whole (or of nothing) on both sides, as for light cones, and at least 99 %
-of face cones agree word for word (light cones: 99.9 %). A face's window is
-90 degrees wide and reaches past the whole scene, so far more bins end
-within rounding of whole or of nothing than a light cone's do (on the small
-icosphere field 0.27 % of face cones, whichever way meshes combine)."""
+Mask words are held to the light cones' bar (99.9 % of face cones word for
+word, every disagreeing bit traced to coverage within 2e-5 of whole or of
+nothing on both sides) against the oracle summing each mesh's cells as the
+library does (fixed point, 2^-24 of a bin per add). Against the oracle
+summing in walk order in f32, as the reference does, every disagreeing bit
+is traced the same way and at least 99 % of face cones agree: a face's
+window is 90 degrees wide and reaches past the whole scene, so far more bins
+end within the reference's rounding of whole or of nothing than a light
+cone's do."""
 import math
 
 import numpy as np
@@ -16,10 +19,16 @@ import pytest
 import kat
 import parity
 from continuum_b200 import _lib, scenes
-from oracle.oracle import OracleScene
+from oracle.oracle import SUM_FIXED, OracleScene
 
 pytestmark = pytest.mark.gpu
 SKY_TOL = 2e-3 * math.pi
+
+
+def oracle_flags(sky_flags):
+    """The oracle's sky flags for cc_sky_visibility's."""
+    return ((1 if sky_flags & _lib.CC_SKY_COMBINE_MAX else 0) | (2 if sky_flags & _lib.CC_SKY_NO_HORIZON_CULL else 0) |
+            (8 if sky_flags & _lib.CC_SKY_OBJECT_FRAME else 0))
 
 
 def check_against_oracle(kernel, meshes, rec, sky_flags=0, instanced=None):
@@ -30,11 +39,15 @@ def check_against_oracle(kernel, meshes, rec, sky_flags=0, instanced=None):
     finally:
         scene.close()
     orc = OracleScene(meshes) if instanced is None else OracleScene.instanced(*instanced)
-    o = orc.sky_visibility(rec, flags=sky_flags)
     g = {"full": faces.full.reshape(-1), "any": faces.any.reshape(-1), "partial": faces.partial.reshape(-1, 64)}
-    stats = parity.compare(g, o, None, check=False)
+    fixed = orc.sky_visibility(rec, flags=oracle_flags(sky_flags), accumulate=SUM_FIXED)
+    stats = parity.compare(g, fixed, None, check=False)
     assert stats["untraced_bits"] == 0, stats
-    assert stats["word_agreement"] >= 0.99, stats
+    assert stats["word_agreement"] >= parity.WORD_AGREEMENT, stats
+    o = orc.sky_visibility(rec, flags=oracle_flags(sky_flags))
+    walk = parity.compare(g, o, None, check=False)
+    assert walk["untraced_bits"] == 0, walk
+    assert walk["word_agreement"] >= 0.99, walk
     assert np.abs(faces.irradiance.reshape(-1) - o["face_light"]).max() <= SKY_TOL
     assert np.abs(irr - o["irradiance"]).max() <= SKY_TOL
     # The per-receiver sum is the faces' light summed in face order.
@@ -113,3 +126,45 @@ def test_sky_instanced_world(kernel):
                                segments=24, rings=18)
     rec = np.ascontiguousarray(w.receivers[::3])
     check_against_oracle(kernel, None, rec, instanced=(w.geometries, w.instances))
+
+
+def receivers_on_objects(w, count, seed=7):
+    """Receivers on the boulders of an instanced world: a triangle's centroid
+    of a random instance, placed and lifted 1e-3 along its world normal, with
+    the instance's index in point.w (as bits) for CC_SKY_OBJECT_FRAME."""
+    rng = np.random.default_rng(seed)
+    inst = w.instances
+    rec = np.zeros((count, 8), np.float32)
+    objects = rng.integers(0, len(inst) - 1, count)  # the last instance is the ground
+    for i, m in enumerate(objects):
+        g = w.geometries[inst["geometry"][m]].reshape(-1, 3, 3).astype(np.float64)
+        t = g[rng.integers(0, len(g))]
+        rot = inst["rotation"][m].reshape(3, 3).astype(np.float64)
+        c = rot @ t.mean(axis=0) * inst["scale"][m] + inst["translation"][m]
+        n = rot @ np.cross(t[1] - t[0], t[2] - t[0])
+        n /= np.linalg.norm(n)
+        rec[i, 0:3] = c + n * 1e-3 * inst["scale"][m]
+        rec[i, 4:7] = n
+    rec[:, 3] = objects.astype(np.uint32).view(np.float32)
+    rec[-4:, 3] = np.array([0xFFFFFFFF] * 4, np.uint32).view(np.float32)  # world axes
+    return rec
+
+
+def test_sky_faces_in_the_receivers_object_frame(kernel):
+    """CC_SKY_OBJECT_FRAME (the reference's sky_frame, set_sky_object_frame):
+    each receiver's cube of faces turns with the object it lies on. Against
+    the oracle, and different from world axes where the objects are turned."""
+    w = scenes.instanced_world(seed=3, n_instances=300, n_boulders=3, half=40.0, n_lights=4, width=96, height=54,
+                               segments=24, rings=18)
+    rec = receivers_on_objects(w, 1024)
+    irr, faces, o, stats = check_against_oracle(kernel, None, rec, sky_flags=_lib.CC_SKY_OBJECT_FRAME,
+                                                instanced=(w.geometries, w.instances))
+    assert stats["cones"] == 6 * 1024
+    scene = kernel.scene_instanced(w.geometries, w.instances)
+    try:
+        world_irr, world_faces = kernel.sky_visibility(scene, rec, outputs=("full",))
+    finally:
+        scene.close()
+    # Receivers on turned objects see their faces' masks change; NONE keeps world axes.
+    assert (world_faces.full.reshape(6, -1)[:, :-4] != faces.full.reshape(6, -1)[:, :-4]).any()
+    assert np.array_equal(world_faces.full.reshape(6, -1)[:, -4:], faces.full.reshape(6, -1)[:, -4:])
