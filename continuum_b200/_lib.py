@@ -35,6 +35,7 @@ CC_CONE_REWALKED = 8
 CC_CONE_FULL_STOP = 16
 CC_CONE_ACC_WIDE = 32
 CC_NO_OBJECT_PREFILTER = 8
+CC_BACK_FACING = 16
 CC_SKY_COMBINE_MAX = 1
 CC_SKY_NO_HORIZON_CULL = 2
 CC_SKY_OBJECT_FRAME = 4

@@ -5,7 +5,9 @@
 // the visible fraction of the unshadowed light (`light_ratio`, :3505-3510,
 // 1 for an empty cone, 0 for a full one, the kernel's `fraction`) or the
 // shadowed light (:3527-3531), 0 for a texel without a surface, nothing for
-// one outside its chart's grid.
+// one outside its chart's grid. A light below a texel's horizon gives the
+// share seen past the texel's own triangle (`back`, :3476-3494;
+// CC_BACK_FACING) and no light.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -332,7 +334,7 @@ int cc_cache_frame(cc_cache* c, const cc_page_request* requests, uint32_t nreque
           if (flag >= 1.5f) {
             float* d = c->host_receivers + 8 * (size_t)npoints;
             d[0] = r[0], d[1] = r[1], d[2] = r[2], d[3] = 0.0f;
-            d[4] = r[4], d[5] = r[5], d[6] = r[6], d[7] = 0.0f;
+            d[4] = r[4], d[5] = r[5], d[6] = r[6], d[7] = r[7];  // the texel's own triangle + 1 (bits)
             e.receiver = npoints++;
           }
         }
@@ -349,6 +351,10 @@ int cc_cache_frame(cc_cache* c, const cc_page_request* requests, uint32_t nreque
         cc_options vo;
         cc_options_default(&vo);
         vo.flags = CC_DEVICE_POINTERS;
+        // A light below a texel's horizon: the share seen past the texel's
+        // own triangle (vc_bake's `back`, :3476-3494), for texels that name
+        // it, in scenes without instancing.
+        if (c->scene->flat.xforms.empty()) vo.flags |= CC_BACK_FACING;
         cc_outputs out{};
         float* v = static_cast<float*>(c->value.ptr);
         if (c->opt.light_ratio) out.fraction = v; else out.irradiance = v;

@@ -91,6 +91,8 @@ void free_scene_device(cc_scene* s) {
   cudaFree(s->xforms);
   cudaFree(s->blas_cov);
   cudaFree(s->obj_cov);
+  cudaFree(s->tri_slot);
+  s->tri_slot = nullptr;
   s->blas_cov = nullptr;
   s->obj_cov = nullptr;
   s->coverage_ready = false;
@@ -151,6 +153,20 @@ int ensure_coverage(cc_scene* s) {
   }
   s->coverage_ready = true;
   return CC_OK;
+}
+
+// Each triangle's slot on the device (the inverse of the leaf order in which
+// upload_scene stores the triangles), for CC_BACK_FACING's own triangles.
+int ensure_slots(cc_scene* s) {
+  if (s->tri_slot) return CC_OK;
+  const cc::FlatScene& f = s->flat;
+  const size_t ntris = f.tris.size() / 12;
+  std::vector<uint32_t> slot(std::max<size_t>(ntris, 1), 0u);
+  for (size_t k = 0; k < ntris; ++k) {
+    const size_t t = (!f.blas.empty() && k < f.blas_items.size()) ? f.blas_items[k] : k;
+    slot[t] = (uint32_t)k;
+  }
+  return upload(slot, &s->tri_slot, s->bytes, "triangle slots");
 }
 
 int validate_flat(const cc::FlatScene& f) {
@@ -517,6 +533,11 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
   if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
   if (!(opt.prefilter >= 0.0f)) return fail(CC_ERR_INVALID, "prefilter must be >= 0");
   if (opt.prefilter > 0.0f && opt.hierarchy != 2) return fail(CC_ERR_INVALID, "prefiltered cones need hierarchy 2");
+  const bool back = (opt.flags & CC_BACK_FACING) != 0;
+  if (back && (sky || opt.prefilter > 0.0f))
+    return fail(CC_ERR_INVALID, "CC_BACK_FACING takes exact light cones only");
+  if (back && !scene->flat.xforms.empty())
+    return fail(CC_ERR_INVALID, "CC_BACK_FACING takes scenes without instancing");
   const uint64_t ncones = npoints * (uint64_t)nlights;
   if (ncones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one call");
   if (npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one call");
@@ -536,6 +557,13 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
   q.prefilter = opt.prefilter;
   q.cones = cones;
   q.cones_count = cones_count;
+  if (back) {
+    int rc2 = ensure_slots(const_cast<cc_scene*>(scene));
+    if (rc2) return rc2;
+    q.back = 1u;
+    q.ntris = (uint32_t)(scene->flat.tris.size() / 12);
+    q.tri_slot = scene->tri_slot;
+  }
   cc::DevScene sd = scene->dev();
   if (opt.prefilter > 0.0f) {
     int rc2 = ensure_coverage(const_cast<cc_scene*>(scene));
@@ -767,6 +795,7 @@ int cc_visibility_static(const cc_scene* scene, const float* receivers, uint64_t
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
   if (opt.points_per_warp < 1 || opt.points_per_warp > 32) return fail(CC_ERR_INVALID, "points_per_warp must be 1..32");
   if (opt.prefilter != 0.0f) return fail(CC_ERR_INVALID, "cc_visibility_static takes exact cones only (prefilter 0)");
+  if (opt.flags & CC_BACK_FACING) return fail(CC_ERR_INVALID, "CC_BACK_FACING is cc_visibility's");
   if (npoints > CC_STATIC_MAX_CONES || npoints * (uint64_t)nlights > CC_STATIC_MAX_CONES)
     return fail(CC_ERR_INVALID, "more than CC_STATIC_MAX_CONES cones (or points) in one cc_visibility_static call");
   const uint64_t ncones = npoints * (uint64_t)nlights;

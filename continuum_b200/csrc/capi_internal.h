@@ -98,6 +98,8 @@ struct cc_scene {
   float* blas_cov = nullptr;
   float* obj_cov = nullptr;
   bool coverage_ready = false;
+  // CC_BACK_FACING: each triangle's slot on the device, uploaded on first use.
+  uint32_t* tri_slot = nullptr;
   uint64_t bytes = 0;
   cc::DevScene dev() const {
     cc::DevScene s;

@@ -49,6 +49,14 @@ struct DevQuery {
   const struct ConeRecord* records = nullptr;
   uint64_t slot_base = 0;
   uint64_t slot_count = 0;
+  // CC_BACK_FACING (exact light cones of a world-space scene): a cone whose
+  // light lies below its receiver's horizon is traced with a horizon facing
+  // the light, past the receiver's own triangle, whose index + 1 the
+  // receiver's normal.w holds as bits (0: none); tri_slot maps a triangle's
+  // index to its slot on the device (ntris of them).
+  uint32_t back = 0;
+  uint32_t ntris = 0;
+  const uint32_t* tri_slot = nullptr;
 };
 
 // A light cone set up before its walk (the split plain path): frame, window,
@@ -60,7 +68,8 @@ struct ConeRecord {
   float4 c;  // up.xyz, v0
   float4 d;  // fwd.xyz, u1
   float4 e;  // baxis.xyz, v1
-  float4 f;  // bcos, bsin, spot, flags (bits: 1 traced, 2 wide window, 4 wide window clipped)
+  float4 f;  // bcos, bsin, spot, flags (bits: 1 traced, 2 wide window, 4 wide window clipped, 8 traced past
+             // the receiver's own triangle toward a light below its horizon; bits 4-31: that triangle's slot + 1)
   uint4 g;   // cone number (low, high words), walk cap, job (batched; else 0)
 };
 // Slots per split chunk by default (records and masks: 368 bytes a slot).

@@ -9,6 +9,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -67,6 +68,7 @@ struct Hit {
   float t = FLT_MAX;
   uint32_t tri = kNone;
   uint32_t xform = kNone;  // the hit object's transform (instanced scenes)
+  uint32_t object = kNone; // the hit mesh (object)
 };
 
 void trace(const FlatScene& s, V o, V d, Hit& hit) {
@@ -108,6 +110,7 @@ void trace(const FlatScene& s, V o, V d, Hit& hit) {
                 hit.t = dist;
                 hit.tri = t;
                 hit.xform = r[3];
+                hit.object = s.items[k];
               }
             }
           } else if (bp + 2 <= 128) {
@@ -126,7 +129,8 @@ void trace(const FlatScene& s, V o, V d, Hit& hit) {
 }  // namespace
 
 // camera: eye.xyz, target.xyz, up.xyz, vertical fov (degrees). Writes per
-// pixel (row-major) a receiver (8 floats: point, normal) and 1 if the ray hit.
+// pixel (row-major) a receiver (8 floats: point, hit object's index as bits;
+// normal, hit triangle's index + 1 as bits) and 1 if the ray hit.
 void primary_hits(const FlatScene& s, const float* camera, uint32_t width, uint32_t height, float* out8,
                   uint8_t* hit_mask, int threads) {
   V eye{camera[0], camera[1], camera[2]}, target{camera[3], camera[4], camera[5]}, upw{camera[6], camera[7], camera[8]};
@@ -164,14 +168,17 @@ void primary_hits(const FlatScene& s, const float* camera, uint32_t width, uint3
         if (dot(n, d) > 0.0f) n = n * -1.0f;
         V surface = eye + d * h.t;
         V point = surface + n * std::max(1e-4f, 2e-6f * h.t);
+        // w: the hit object (point) and the hit triangle + 1 (normal), as
+        // bits: CC_SKY_OBJECT_FRAME's object and CC_BACK_FACING's own triangle.
+        const uint32_t own = h.tri + 1u;
         o[0] = point.x;
         o[1] = point.y;
         o[2] = point.z;
-        o[3] = 0.0f;
+        std::memcpy(&o[3], &h.object, 4);
         o[4] = n.x;
         o[5] = n.y;
         o[6] = n.z;
-        o[7] = 0.0f;
+        std::memcpy(&o[7], &own, 4);
         hit_mask[i] = 1;
       }
     }

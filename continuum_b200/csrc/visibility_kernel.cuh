@@ -35,11 +35,14 @@ __device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) 
 // kept here, where the integration in the same kernel reads every lane's
 // (else each lane keeps its own in thread-local memory, and the smaller
 // block lets more warps be resident).
-template <class CellT, bool Sky, bool SmemCov>
+// Back: the launch's cones may skip their receiver's own triangle
+// (CC_BACK_FACING); other launches compile without the check.
+template <class CellT, bool Sky, bool SmemCov, bool Back = false>
 struct WarpShared {
   using Cell = CellT;
   static constexpr bool kSky = Sky;
   static constexpr bool kSmemCov = SmemCov;
+  static constexpr bool kBack = Back;
   Cell acc[kBins * 32];                 // each cone's accumulator (fixed point, units of kFixUnit)
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
   uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
@@ -53,10 +56,10 @@ static_assert(sizeof(WarpShared<unsigned int, false, true>) % 16 == 0, "warp sha
 static_assert(sizeof(WarpShared<unsigned long long, false, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(sizeof(WarpShared<unsigned int, true, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(sizeof(WarpShared<unsigned int, false, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-template <bool kSky, bool kSmemCov>
-using NarrowShared = WarpShared<unsigned int, kSky, kSmemCov>;
-template <bool kSky, bool kSmemCov>
-using WideShared = WarpShared<unsigned long long, kSky, kSmemCov>;
+template <bool kSky, bool kSmemCov, bool kBack = false>
+using NarrowShared = WarpShared<unsigned int, kSky, kSmemCov, kBack>;
+template <bool kSky, bool kSmemCov, bool kBack = false>
+using WideShared = WarpShared<unsigned long long, kSky, kSmemCov, kBack>;
 // The shared memory of a kernel variant's warps, and the blocks per SM it
 // fits. Prefiltering light cones integrate in the walk kernel, reading every
 // lane's coverages (warp_blocked): their table stays in shared memory. The
@@ -66,9 +69,9 @@ using WideShared = WarpShared<unsigned long long, kSky, kSmemCov>;
 // (8 would cap registers at 128 and spill).
 template <bool kSky, bool kSplat>
 constexpr bool smem_cov() { return kSplat && !kSky; }
-template <bool kWide, bool kSky, bool kSplat>
-using KernelShared = typename std::conditional<kWide, WideShared<kSky, smem_cov<kSky, kSplat>()>,
-                                               NarrowShared<kSky, smem_cov<kSky, kSplat>()>>::type;
+template <bool kWide, bool kSky, bool kSplat, bool kBack = false>
+using KernelShared = typename std::conditional<kWide, WideShared<kSky, smem_cov<kSky, kSplat>(), kBack>,
+                                               NarrowShared<kSky, smem_cov<kSky, kSplat>(), kBack>>::type;
 constexpr int resident_blocks_for(bool wide, bool sky, bool splat) {
   return (splat && !sky) ? (wide ? kFusedSoloBlocksPerSm : kFusedBlocksPerSm)
                          : (wide ? kSoloBlocksPerSm : (splat ? kSkySplatBlocksPerSm : kBlocksPerSm));
@@ -149,6 +152,8 @@ struct LaneState {
   uint32_t cap;
   uint32_t status;
   uint32_t n_obj, n_blas, n_tris;
+  uint32_t skip;     // the cone's own triangle slot, which it does not draw (kNoneU: none)
+  bool skips;        // some lane of the warp has one (warp-uniform)
   bool independent;  // sky cones: meshes combine as independent occluders (else by the maximum)
   f3 horizon;        // sky cones: the horizon in the space of the object being walked (the world's elsewhere)
   f3 world_horizon;  // sky cones in instanced scenes: the horizon in world space
@@ -287,9 +292,11 @@ __device__ __noinline__ uint32_t raster_queue(const DevScene& s, WS* ws, uint32_
 // join the warp's queue, and every 32 queued pairs are rasterized by the
 // whole warp at once, so lanes whose pair was culled do not sit idle while
 // the others rasterize. `queues` and the result are both queues' lengths.
+// `skip` is the lane's cone's own triangle slot (kNoneU: none), which it
+// does not draw; `skips` (warp-uniform) says some lane has one.
 template <class WS>
 __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t owners, uint32_t t0,
-                                            uint32_t nt, uint32_t queues, int lane) {
+                                            uint32_t nt, uint32_t queues, int lane, uint32_t skip, bool skips) {
   uint32_t queued = fast_len(queues), general = general_len(queues);
   const uint32_t n_owners = __popc(owners);
   const uint32_t n_pairs = n_owners * nt;
@@ -297,12 +304,19 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t 
     const uint32_t pair = base + lane;
     bool pass = false;
     uint32_t entry = 0;
+    int owner = 0;
+    uint32_t t = kNoneU;
     if (pair < n_pairs) {
       const uint32_t k = pair / n_owners;
       const uint32_t r = pair - k * n_owners;
-      const int owner = (int)__fns(owners, 0, r + 1);
-      pass = pair_survives(s, ws, owner, t0 + k);
-      entry = ((uint32_t)owner << kQueueOwnerShift) | (t0 + k);
+      owner = (int)__fns(owners, 0, r + 1);
+      t = t0 + k;
+      pass = pair_survives(s, ws, owner, t);
+      entry = ((uint32_t)owner << kQueueOwnerShift) | t;
+    }
+    // The owner's own triangle is not drawn (cover_triangle's cover_skip, :595).
+    if constexpr (WS::kBack) {
+      if (skips && __shfl_sync(0xffffffffu, skip, owner) == t) pass = false;
     }
     const uint32_t m = __ballot_sync(0xffffffffu, pass);
     if (pass) ws->queue[queued + __popc(m & ((1u << lane) - 1u))] = entry;
@@ -392,7 +406,8 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& 
   }
   if (kCount && on) st.n_tris += range.y;
   for (uint32_t t = range.x; t < range.x + range.y; t += 8)
-    st.queued = cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), st.queued, lane);
+    st.queued = cover_leaf(s, st.ws, owners, t, min(8u, range.x + range.y - t), st.queued, lane, st.skip,
+                           st.skips);
   resolve_mesh(s, st, lane);
   if (placed) {
     st.cone = st.world;
@@ -479,7 +494,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
         st.cone_work += ib;
         if (kCount) st.n_tris += ib;
       }
-      st.queued = cover_leaf(s, st.ws, owners, ia, ib, st.queued, lane);
+      st.queued = cover_leaf(s, st.ws, owners, ia, ib, st.queued, lane, st.skip, st.skips);
     } else if (ib > 0) {
       // An object leaf: its meshes.
       if (hierarchy == 1) {
@@ -664,7 +679,7 @@ __device__ __forceinline__ void scene_walk_splat(const DevScene& s, float prefil
         st.cone_work += ib;
         if (kCount) st.n_tris += ib;
       }
-      st.queued = cover_leaf(s, ws, owners, ia, ib, st.queued, lane);
+      st.queued = cover_leaf(s, ws, owners, ia, ib, st.queued, lane, st.skip, st.skips);
     } else {
       if (sp + 2 > kStack) {
         if (descend) st.status |= 2u;
@@ -841,13 +856,15 @@ __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, ui
 // kSky: sky cones, the six cube faces around each receiver in place of its
 // lights (cone c = face * npoints + point).
 // kSplat: prefiltering cones (q.prefilter bins), walking hierarchy level 2.
-template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSplat>
+// kBack: cones may skip their receiver's own triangle (CC_BACK_FACING; the
+// split path's plain cones of scenes without instancing).
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSplat, bool kBack = false>
 // The blocks the shared memory fits per SM; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kSky, kSplat>())
     visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
                       const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
-  using WS = KernelShared<kWide, kSky, kSplat>;
+  using WS = KernelShared<kWide, kSky, kSplat, kBack>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -952,6 +969,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
     st.status = 0;
     st.n_obj = st.n_blas = st.n_tris = 0;
     st.independent = false;
+    st.skip = kNoneU;
     st.horizon = st.world_horizon = mk(0.f, 0.f, 0.f);
     for (int k = 0; k < kBins; ++k) st.cov_at(k) = 0.0f;
 
@@ -979,6 +997,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
       st.cone.bsin = rec.f.y;
       const uint32_t flags = __float_as_uint(rec.f.w);
       traced = valid && (flags & 1u);
+      st.skip = valid ? (flags >> 4) - 1u : kNoneU;
       info.wide_window = (flags & 2u) != 0u;
       info.wide_clipped = (flags & 4u) != 0u;
       st.cap = rec.g.z;
@@ -1011,6 +1030,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
       traced = on && info.ok;
       st.cap = info.wide_window ? q.wide_cone_cap : q.light_cone_cap;
     }
+    st.skips = __any_sync(0xffffffffu, st.skip != kNoneU);
     if (kInst) st.world = st.cone;
     store_cone(ws, st.cone, lane);
     store_horizon(ws, st.horizon, lane);
@@ -1100,35 +1120,45 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
 // Whether the large dynamic shared memory size was allowed, per device and
 // kernel variant (the attribute is set per device); per unit, for the
 // variants it launches.
-static uint64_t g_attr_set[64] = {};
+static uint64_t g_attr_set[128] = {};
 
-template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false, bool kSplat = false>
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false, bool kSplat = false,
+          bool kBack = false>
 static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * sizeof(KernelShared<kWide, kSky, kSplat>);
+  const size_t smem = (size_t)kWarpsPerBlock * sizeof(KernelShared<kWide, kSky, kSplat, kBack>);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
-  const int variant =
-      (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0) + (kSky ? 16 : 0) + (kSplat ? 32 : 0);
+  const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0) + (kSky ? 16 : 0) +
+                      (kSplat ? 32 : 0) + (kBack ? 64 : 0);
   if (!(g_attr_set[variant] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat>,
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     g_attr_set[variant] |= bit;
   }
-  visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat>
+  visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack>
       <<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
   return cudaGetLastError();
 }
 
-// A plain (not batched) pass of the variant the flags pick.
+// A plain (not batched) pass of the variant the flags pick; q.back (the split
+// path's exact cones of a scene without instancing) takes the variant that
+// skips each cone's own triangle.
 template <bool kWide, bool kSky, bool kSplat>
 static cudaError_t plain_pass(bool count, bool inst, const DevScene& s, const DevQuery& q, const DevOut& o,
                               const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                               cudaStream_t stream) {
   const BatchLaunch none{};
+  if constexpr (!kSky && !kSplat) {
+    if (q.back && !inst)
+      return count ? launch_one<true, false, false, kWide, false, false, true>(s, q, o, none, list, list_count, pw,
+                                                                               blocks, stream)
+                   : launch_one<false, false, false, kWide, false, false, true>(s, q, o, none, list, list_count, pw,
+                                                                                blocks, stream);
+  }
   if (inst)
     return count ? launch_one<true, false, true, kWide, kSky, kSplat>(s, q, o, none, list, list_count, pw, blocks,
                                                                       stream)

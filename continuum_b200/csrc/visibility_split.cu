@@ -27,17 +27,40 @@ __device__ __forceinline__ bool slot_cone(const DevQuery& q, uint64_t slot, uint
 
 // A slot's record: the spot factor and facing test that gate its cone, and
 // the cone itself (hit_irradiance_rect, :2125-2128; light_cone).
+// vc_bake's `back` (:3476-3494): the light gives the receiver no unshadowed
+// light, yet lies in front of a horizon facing it; the direction to the
+// light's centre is that horizon's normal.
+__device__ __forceinline__ bool back_facing(const DevLight& L, f3 point, f3 normal, f3& toward) {
+  toward = normalize(light_center(L) - point);
+  return unshadowed(point, normal, L) <= 0.0f && faces_light(L, point, toward);
+}
+
 __device__ __forceinline__ ConeRecord make_record(const DevQuery& q, bool valid, uint64_t c, uint32_t job) {
   const uint32_t l = valid ? (uint32_t)(c / q.npoints) : 0u;
   const uint64_t p = valid ? c - (uint64_t)l * q.npoints : 0u;
-  const f3 point = xyz(__ldg(&q.receivers[2 * p + 0])), normal = xyz(__ldg(&q.receivers[2 * p + 1]));
+  const float4 normal4 = __ldg(&q.receivers[2 * p + 1]);
+  const f3 point = xyz(__ldg(&q.receivers[2 * p + 0]));
+  f3 normal = xyz(normal4);
   const DevLight L = load_light(q.lights, l);
+  // CC_BACK_FACING: the cone of a light below the horizon is traced with a
+  // horizon facing the light, past the receiver's own triangle (its slot + 1
+  // goes in the flags' top bits).
+  uint32_t back = 0u;
+  const uint32_t own = __float_as_uint(normal4.w);  // the receiver's own triangle + 1 (0: none)
+  if (q.back && valid && own != 0u) {
+    f3 toward;
+    if (back_facing(L, point, normal, toward)) {
+      normal = toward;
+      const uint32_t slot = own <= q.ntris ? __ldg(&q.tri_slot[own - 1u]) + 1u : 0u;
+      back = 8u | (slot << 4);
+    }
+  }
   const float spot = spot_falloff(L, normalize(point - light_center(L)));
   const bool on = valid && spot > 0.0f && faces_light(L, point, normal);
   Cone cone{};
   const LightConeInfo info = light_cone(point, L, q.wide_extent, cone);
   const bool traced = on && info.ok;
-  const uint32_t flags = (traced ? 1u : 0u) | (info.wide_window ? 2u : 0u) | (info.wide_clipped ? 4u : 0u);
+  const uint32_t flags = (traced ? 1u : 0u) | (info.wide_window ? 2u : 0u) | (info.wide_clipped ? 4u : 0u) | back;
   ConeRecord r;
   r.a = make_float4(cone.apex.x, cone.apex.y, cone.apex.z, cone.far_offset);
   r.b = make_float4(cone.right.x, cone.right.y, cone.right.z, cone.u0);
@@ -133,8 +156,14 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, Bat
   cone.bsin = r.f.y;
   const uint32_t l = (uint32_t)(c / q.npoints);
   const uint64_t p = c - (uint64_t)l * q.npoints;
-  const f3 point = xyz(__ldg(&q.receivers[2 * p + 0])), normal = xyz(__ldg(&q.receivers[2 * p + 1]));
+  const f3 point = xyz(__ldg(&q.receivers[2 * p + 0]));
+  f3 normal = xyz(__ldg(&q.receivers[2 * p + 1]));
   const DevLight L = load_light(q.lights, l);
+  // A cone traced toward a light below the receiver's horizon (CC_BACK_FACING)
+  // is integrated with the horizon facing the light: its ratio is the share
+  // seen past the receiver's own triangle, its light 0 (vc_bake :3476-3531).
+  const bool back = (flags & 8u) != 0u;
+  if (back) normal = normalize(light_center(L) - point);
   // The mask, and whether it is empty or whole.
   bool any = false, all = true;
   const float4* src = reinterpret_cast<const float4*>(o.cov_out + 64 * (valid ? slot : first));
@@ -154,7 +183,7 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, Bat
   float value, ratio;
   light_integral(cone, point, normal, L, r.f.z, traced, info, !any, all, ws->cov, ws->scratch, lane, value, ratio);
   if (valid) {
-    if (irradiance) irradiance[c] = value;
+    if (irradiance) irradiance[c] = back ? 0.0f : value;
     if (fraction) fraction[c] = ratio;
   }
 }

@@ -698,8 +698,9 @@ TEXEL_OUTSIDE, TEXEL_EMPTY, TEXEL_SURFACE = 0.0, 1.0, 2.0
 class PageRequest:
     """A page a view wants (vcache.rs: a request with its priority): `key` of
     3 u32, `priority` (lower first), `inside` texels per axis (0..9) and
-    `texels`, 81 x 8 floats (point.xyz, flag, normal.xyz, 0), row-major 9 x 9,
-    needed only when the page is not resident."""
+    `texels`, 81 x 8 floats (point.xyz, flag, normal.xyz, own triangle + 1
+    as uint32 bits or 0), row-major 9 x 9, needed only when the page is not
+    resident."""
 
     key: Sequence[int]
     priority: int

@@ -559,7 +559,8 @@ def grid_pages(grid: np.ndarray, surface: Optional[np.ndarray] = None, object_id
     library): page (px, py) holds the grid points [py * 8 + y, px * 8 + x]
     for x, y in 0..8 (8 x 8 texels stored 9 x 9, vcache.rs:32-35); `inside`
     counts those within the grid; a texel's flag is 2 where `surface` is true
-    (all by default), 1 where it is not, 0 past the grid. Keys are
+    (all by default), 1 where it is not, 0 past the grid; the grid's own
+    triangles (normal.w, as the camera pass writes them) are kept. Keys are
     (object_id, py, px); priorities 0."""
     from .kernel import PageRequest
     rows, cols = grid.shape[:2]
@@ -573,6 +574,5 @@ def grid_pages(grid: np.ndarray, surface: Optional[np.ndarray] = None, object_id
             ins = (min(9, cols - c0), min(9, rows - r0))
             t[: ins[1], : ins[0]] = grid[r0:r0 + ins[1], c0:c0 + ins[0]]
             t[: ins[1], : ins[0], 3] = np.where(surface[r0:r0 + ins[1], c0:c0 + ins[0]], 2.0, 1.0)
-            t[: ins[1], : ins[0], 7] = 0.0
             pages.append(PageRequest((object_id, py, px), 0, ins, t.reshape(81, 8)))
     return pages

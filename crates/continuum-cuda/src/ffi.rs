@@ -21,6 +21,7 @@ pub const CC_DEVICE_POINTERS: u32 = 1;
 pub const CC_NO_REDO: u32 = 2;
 pub const CC_KEEP_ORDER: u32 = 4;
 pub const CC_NO_OBJECT_PREFILTER: u32 = 8;
+pub const CC_BACK_FACING: u32 = 16;
 /// cc_batch_options.flags
 pub const CC_BATCH_GRAPH: u32 = 8;
 /// cc_sky_visibility flags

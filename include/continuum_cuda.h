@@ -185,7 +185,9 @@ CC_API uint64_t cc_scene_device_bytes(const cc_scene* scene);
  * camera, as the reference's camera pass forms them (camera_dir, primary_hit,
  * surface_offset: mask_cones.wgsl:1724-1760, 2062-2064, 2275-2277). Host
  * threads; for preparing inputs. camera: eye.xyz, target.xyz, up.xyz,
- * vertical fov in degrees. out8: 8 floats per pixel (receiver layout);
+ * vertical fov in degrees. out8: 8 floats per pixel (receiver layout; point.w
+ * holds the hit object's index and normal.w the hit triangle's index + 1, as
+ * the bits of uint32s: the inputs of CC_SKY_OBJECT_FRAME and CC_BACK_FACING);
  * hit: 1 per pixel, 0 where the ray misses (its receiver is zero). */
 CC_API int cc_scene_primary_hits(const cc_scene* scene, const float camera[10], uint32_t width, uint32_t height,
                                  float* out8, uint8_t* hit);
@@ -196,7 +198,7 @@ typedef struct cc_options {
   uint32_t light_cone_cap;   /* LIGHT_CONE_CAP, mask_cones.wgsl:1052 (4096) */
   uint32_t wide_cone_cap;    /* WIDE_CONE_CAP, mask_cones.wgsl:1056 (512) */
   uint32_t points_per_warp;  /* cones walked together per warp: 1..32 (32); results do not depend on it */
-  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO, CC_KEEP_ORDER, CC_NO_OBJECT_PREFILTER */
+  uint32_t flags;            /* CC_DEVICE_POINTERS, CC_NO_REDO, CC_KEEP_ORDER, CC_NO_OBJECT_PREFILTER, CC_BACK_FACING */
   float prefilter;           /* prefiltered cones (MaskConeKernel::set_prefilter, lib.rs:1508): a hierarchy node
                                 wholly between the near and far planes projecting to at most this many bins is
                                 splatted with its directional coverage instead of descended into
@@ -204,6 +206,20 @@ typedef struct cc_options {
                                 splat_object_node, :1096-1150). 0: exact cones. Needs hierarchy 2; cc_visibility
                                 and cc_sky_visibility only */
 } cc_options;
+
+/* cc_options.flags: the lighting cache's estimator for a light below a
+ * receiver's horizon (vc_bake's `back`, mask_cones.wgsl:3476-3494): a cone
+ * whose light gives the receiver no unshadowed light (its normal turns away)
+ * but which faces the light is traced with a horizon facing the light (the
+ * normal replaced by the direction to the light's centre), past the
+ * receiver's own triangle, so its fraction is the light's share seen past
+ * that triangle (1 on a convex object's terminator, the shadow's where
+ * something else covers it); its irradiance is 0. The receiver's normal.w
+ * holds its own triangle's index in the scene's triangle order plus one, as
+ * the bits of a uint32 (cc_scene_primary_hits writes it); a receiver without
+ * one (0) keeps its normal. cc_visibility only, exact cones of a scene
+ * without instancing. */
+#define CC_BACK_FACING 16u
 
 /* Defaults: hierarchy 2, 8.0, 4096, 512, 32, 0, prefilter 0. */
 CC_API void cc_options_default(cc_options* opt);
@@ -496,8 +512,11 @@ typedef struct cc_page_request {
   uint32_t key[3];        /* the page's identity (object, chart and mip, page coordinates: the caller's packing) */
   uint32_t priority;      /* lower first */
   uint32_t inside[2];     /* texels of the page inside its chart's grid along x and y (0..9) */
-  const float* texels;    /* 81 receiver records of 8 floats (point.xyz, flag, normal.xyz, 0), row-major 9 x 9;
-                             flag 0: outside the chart's grid, 1: inside without a surface, 2: a surface to bake.
+  const float* texels;    /* 81 receiver records of 8 floats (point.xyz, flag, normal.xyz, own), row-major 9 x 9;
+                             flag 0: outside the chart's grid, 1: inside without a surface, 2: a surface to bake;
+                             own: the texel's triangle's index + 1 as the bits of a uint32 (0: not named), so that
+                             a light below the texel's horizon bakes the share seen past that triangle (vc_bake's
+                             `back`, mask_cones.wgsl:3476-3494; scenes without instancing), else ratio 1.
                              Host memory, read during cc_cache_frame; may be null for pages that are resident */
 } cc_page_request;
 

@@ -543,6 +543,7 @@ template <class R> struct Params {
   R prefilter = 0;               // prefilter_bins (0: exact cones)
   bool object_prefilter = true;  // object-level splats in instanced scenes
   uint32_t accumulate = kSumWalkOrder;  // AccumulateMode
+  bool back_facing = false;  // vc_bake's estimator for a light below the horizon (:3476-3494)
 };
 
 template <class R> constexpr R NEAR = R(1e-4);
@@ -852,11 +853,13 @@ struct Work {  // the reference's work counters (mask_cones.wgsl:655-665), per c
   uint32_t blas_nodes = 0;    // triangle-hierarchy nodes tested
   uint32_t tris = 0;          // triangles tested
   uint32_t flags = 0;         // bit 0: walk capped; bit 1: stack overflow
+  uint32_t skip = NONE;       // a triangle not drawn (cover_skip, :588-595): the receiver's own
 };
 
 // cover_triangle (:594-616)
 template <class R> bool cover_triangle(const Scene& s, const Cone<R>& c, Acc<R>& acc, uint32_t t, Work& wk) {
   wk.tris++;
+  if (t == wk.skip) return false;
   V3<R> v0 = tri_vertex<R>(s, t, 0), v1 = tri_vertex<R>(s, t, 1), v2 = tri_vertex<R>(s, t, 2);
   V3<R> n = cross(v1 - v0, v2 - v0);
   if (dot(n, c.apex - v0) <= 0) return false;
@@ -1460,8 +1463,23 @@ template <class R> struct ConeResult {
 // plus the lighting cache's ratio (vc_bake, :3453-3510, static light): the
 // visible fraction of the unshadowed light, exactly 1 for an empty cone and 0
 // for a full one.
+// `own`: the receiver's own triangle + 1 (0: none). With prm.back_facing, a
+// light that gives the receiver no unshadowed light but lies in front of a
+// horizon facing it is traced with that horizon (the normal replaced by the
+// direction to the light's centre) past the receiver's own triangle; the
+// ratio is then the share seen past it and the light 0 (vc_bake :3476-3531).
 template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> normal, const Light<R>& r,
-                                        const Params<R>& prm, ConeResult<R>& out) {
+                                        const Params<R>& prm, ConeResult<R>& out, uint32_t own = 0) {
+  bool back = false;
+  uint32_t skip = NONE;
+  if (prm.back_facing && own != 0) {
+    const V3<R> toward = normalize(light_center(r) - point);
+    if (unshadowed_rect(point, normal, r) <= 0 && faces_light(r, point, toward)) {
+      back = true;
+      normal = toward;
+      skip = own - 1;
+    }
+  }
   R spot = spot_falloff(r, normalize(point - light_center(r)));
   bool on = spot > 0 && faces_light(r, point, normal);
   LightCone<R> lc = light_cone_rect(point, r, prm.wide_extent);
@@ -1472,6 +1490,7 @@ template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> norma
   wk.prefilter = prm.prefilter;
   wk.object_prefilter = prm.object_prefilter;
   wk.accumulate = prm.accumulate;
+  wk.work.skip = skip;
   if (traced) scene_coverage(s, lc.c, wk, prm.hierarchy);
   if (wk.cone_work >= wk.cone_cap && traced) wk.work.flags |= 1;
   if (traced && wk.cone_work >= wk.cone_cap && lc.wide_window && !lc.wide_clipped) {
@@ -1502,7 +1521,7 @@ template <class R> void visibility_cone(const Scene& s, V3<R> point, V3<R> norma
   if (open > 0 && last_empty) ratio = 1;
   if (open > 0 && last_full) ratio = 0;
   std::copy(wk.cov, wk.cov + BINS, out.cov);
-  out.irradiance = value;
+  out.irradiance = back ? R(0) : value;
   out.fraction = ratio;
   out.unshadowed = open;
   out.work = wk.work;
@@ -2023,6 +2042,7 @@ struct Nearest {
   float t = FLT_MAX;
   uint32_t tri = NONE;
   uint32_t xform = NONE;
+  uint32_t object = NONE;
 };
 
 inline V tri_at(const Scene& s, uint32_t t, int k) {
@@ -2073,6 +2093,7 @@ void nearest_hit(const Scene& s, V o, V d, Nearest& h) {
             h.t = dist;
             h.tri = t;
             h.xform = r[3];
+            h.object = s.items[k];
           }
         }
       }
@@ -2081,7 +2102,8 @@ void nearest_hit(const Scene& s, V o, V d, Nearest& h) {
 }
 
 // camera: eye.xyz, target.xyz, up.xyz, vertical fov in degrees. Per pixel
-// (row-major) a receiver (point.xyz 0, normal.xyz 0) and 1 if the ray hit.
+// (row-major) a receiver (point.xyz, the hit object's index as bits;
+// normal.xyz, the hit triangle's index + 1 as bits) and 1 if the ray hit.
 void primary_hits(const Scene& s, const float* camera, uint32_t width, uint32_t height, float* out8, uint8_t* hit,
                   int threads) {
   const V eye{camera[0], camera[1], camera[2]}, target{camera[3], camera[4], camera[5]};
@@ -2112,12 +2134,15 @@ void primary_hits(const Scene& s, const float* camera, uint32_t width, uint32_t 
       }
       if (dot(n, d) > 0.0f) n = n * -1.0f;
       const V point = (eye + d * h.t) + n * std::max(1e-4f, 2e-6f * h.t);
+      const uint32_t own = h.tri + 1u;  // w: the hit object, and the hit triangle + 1, as bits
       o[0] = point.x;
       o[1] = point.y;
       o[2] = point.z;
+      std::memcpy(&o[3], &h.object, 4);
       o[4] = n.x;
       o[5] = n.y;
       o[6] = n.z;
+      std::memcpy(&o[7], &own, 4);
     }
   });
 }
@@ -2293,6 +2318,7 @@ struct OracleParams {
   float prefilter;            // prefilter_bins (0: exact cones)
   uint32_t object_prefilter;  // object-level splats (instanced scenes)
   uint32_t accumulate;        // AccumulateMode: 0 the reference's walk-order sums, 1 fixed point, 2 double
+  uint32_t back_facing;       // 1: vc_bake's estimator for a light below the horizon (receiver normal.w: own triangle + 1)
 };
 
 // Visibility of cones (light l, receiver p), cone id c = l * npoints + p,
@@ -2312,7 +2338,8 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
   auto run = [&](auto zero) {
     using R = decltype(zero);
     Params<R> prm{prm_in->hierarchy, R(prm_in->wide_extent), prm_in->light_cone_cap, prm_in->wide_cone_cap,
-                  R(prm_in->prefilter), prm_in->object_prefilter != 0, prm_in->accumulate};
+                  R(prm_in->prefilter), prm_in->object_prefilter != 0, prm_in->accumulate,
+                  prm_in->back_facing != 0};
     parallel_for(n, threads, [&](uint64_t i) {
       uint64_t c = cone_ids ? cone_ids[i] : i;
       uint64_t l = c / npoints, p = c % npoints;
@@ -2321,7 +2348,10 @@ int oracle_visibility(void* sp, const float* receivers, uint64_t npoints, const 
       Light<R> L{{R(lt[0]), R(lt[1]), R(lt[2])}, R(lt[3]), {R(lt[4]), R(lt[5]), R(lt[6])}, R(lt[7]),
                  {R(lt[8]), R(lt[9]), R(lt[10])}, R(lt[11])};
       ConeResult<R> res;
-      visibility_cone<R>(*s, V3<R>{R(rc[0]), R(rc[1]), R(rc[2])}, V3<R>{R(rc[4]), R(rc[5]), R(rc[6])}, L, prm, res);
+      uint32_t own;
+      std::memcpy(&own, rc + 7, 4);
+      visibility_cone<R>(*s, V3<R>{R(rc[0]), R(rc[1]), R(rc[2])}, V3<R>{R(rc[4]), R(rc[5]), R(rc[6])}, L, prm, res,
+                         own);
       uint32_t f[2] = {0, 0}, a[2] = {0, 0};
       for (uint32_t b = 0; b < BINS; ++b) {
         if (res.cov[b] >= R(1)) f[b >> 5] |= 1u << (b & 31);

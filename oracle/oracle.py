@@ -20,7 +20,7 @@ NODE_DTYPE = np.dtype([("lo", "<f4", 4), ("hi", "<f4", 4), ("info", "<u4", 4)])
 class _Params(C.Structure):
     _fields_ = [("hierarchy", C.c_uint32), ("wide_extent", C.c_float), ("light_cone_cap", C.c_uint32),
                 ("wide_cone_cap", C.c_uint32), ("prefilter", C.c_float), ("object_prefilter", C.c_uint32),
-                ("accumulate", C.c_uint32)]
+                ("accumulate", C.c_uint32), ("back_facing", C.c_uint32)]
 
 #: How each mesh's cells are summed: the reference's sums in walk order in
 #: the run's precision; each add rounded to 2^-24 of a bin into exact integer
@@ -144,7 +144,7 @@ class OracleScene:
     def visibility(self, receivers: np.ndarray, lights: np.ndarray, hierarchy: int = 2, precision: int = 4,
                    cone_ids: np.ndarray | None = None, threads: int | None = None, wide_extent: float = 8.0,
                    light_cone_cap: int = 4096, wide_cone_cap: int = 512, partial: bool = True, prefilter: float = 0.0,
-                   object_prefilter: bool = True, accumulate: int = 0) -> dict:
+                   object_prefilter: bool = True, accumulate: int = 0, back_facing: bool = False) -> dict:
         """Per-cone results (cone c = light * npoints + point), for all cones or
         the `cone_ids` subset (outputs in subset order)."""
         rec = np.ascontiguousarray(receivers, np.float32).reshape(-1, 8)
@@ -159,7 +159,7 @@ class OracleScene:
         work = np.zeros((n, 4), np.uint32)
         unsh = np.zeros(n, np.float32)
         prm = _Params(hierarchy, wide_extent, light_cone_cap, wide_cone_cap, prefilter, 1 if object_prefilter else 0,
-                      int(accumulate))
+                      int(accumulate), 1 if back_facing else 0)
         rc = load().oracle_visibility(self._h, _p(rec), rec.shape[0], _p(lig), lig.shape[0], C.byref(prm), _p(ids),
                                       0 if ids is None else len(ids), precision, _p(full), _p(any_), _p(part),
                                       _p(irr), _p(frac), _p(work), _p(unsh), threads or default_threads())

@@ -7,7 +7,7 @@ import pytest
 
 import parity
 from continuum_b200 import Light, LightingCache, RectLight, SphereLight, light_gpu, scenes
-from oracle.oracle import OracleScene
+from oracle.oracle import SUM_FIXED, OracleScene
 
 pytestmark = pytest.mark.gpu
 
@@ -121,3 +121,76 @@ def test_jobs_and_pool_layout(kernel):
         cache.close()
     finally:
         scene.close()
+
+
+def terminator_workload():
+    """A convex sphere (an undisplaced icosphere) lit from its side by a rect
+    light, with a wall between the light and part of its far side, and a
+    sphere light above; one texel per sphere triangle (its centroid lifted
+    1e-4 along its normal, naming the triangle), laid out as a 40 x 32 grid."""
+    sphere = scenes.displaced_icosphere((0.0, 0.0, 0.0), 1.0, seed=1, subdivisions=3, amplitude=0.0)
+    wall = scenes.box_mesh((2.0, -3.0, 0.2), (2.2, 3.0, 3.0))
+    tris = sphere.reshape(-1, 3, 3).astype(np.float64)
+    n = np.cross(tris[:, 1] - tris[:, 0], tris[:, 2] - tris[:, 0])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    c = tris.mean(axis=1) + 1e-4 * n
+    rec = np.zeros((len(tris), 8), np.float32)
+    rec[:, 0:3], rec[:, 4:7] = c, n
+    rec[:, 7] = (np.arange(len(tris), dtype=np.uint32) + 1).view(np.float32)  # own triangle + 1
+    rect = light_gpu(Light.rect(RectLight((6.0, -0.5, -0.5), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), one_sided=False)))
+    lights = np.stack([rect, light_gpu(Light(SphereLight((0.3, 6.0, 0.2), 0.5), (1.0, 1.0, 1.0)))])
+    return [sphere, wall], np.ascontiguousarray(rec[:1280]), lights
+
+
+@pytest.mark.parametrize("light_ratio", [True, False])
+def test_back_facing_texels_bake_the_share_past_their_own_triangle(kernel, light_ratio):
+    """vc_bake's `back` (mask_cones.wgsl:3476-3494): a light below a texel's
+    horizon bakes the share seen past the texel's own triangle (1 on the
+    convex sphere's terminator, less where the wall covers the light) and no
+    light; the pool equals cc_visibility with CC_BACK_FACING bit for bit and
+    the oracle's estimator within the parity bar."""
+    from continuum_b200 import _lib
+
+    meshes, rec, lights = terminator_workload()
+    grid = rec.reshape(40, 32, 8)
+    pages = scenes.grid_pages(grid)
+    scene = kernel.scene(meshes)
+    try:
+        cache, frames = bake_all(kernel, scene, lights, pages, pages=256, bake_budget=1 << 16, light_ratio=light_ratio)
+        got = kernel.visibility(scene, rec, lights, outputs=("irradiance", "fraction", "full", "any"),
+                                flags=_lib.CC_BACK_FACING)
+        want = (got.fraction if light_ratio else got.irradiance).reshape(2, 40, 32)
+        for p in pages:
+            vals = cache.read(p.key).reshape(9, 9, 2)
+            _, py, px = p.key
+            for y in range(min(9, 40 - py * 8)):
+                for x in range(min(9, 32 - px * 8)):
+                    assert np.array_equal(vals[y, x], want[:, py * 8 + y, px * 8 + x]), (p.key, y, x)
+        cache.close()
+        o = OracleScene(meshes)
+        orc = o.visibility(rec, lights, back_facing=True, accumulate=SUM_FIXED)
+        g = {"full": got.full.reshape(-1), "any": got.any.reshape(-1), "fraction": got.fraction.reshape(-1),
+             "irradiance": got.irradiance.reshape(-1)}
+        parity.compare(g, orc, orc["unshadowed"])
+        plain = kernel.visibility(scene, rec, lights, outputs=("fraction",))
+        open_light = o.visibility(rec, lights, partial=False)["unshadowed"].reshape(2, -1)[0]
+        o.close()
+    finally:
+        scene.close()
+    # Texels below the rect light's horizon: without the estimator their
+    # ratio is 1; with it, 1 where only their own sphere turns away, less
+    # where the wall covers the light, and their light is 0.
+    below = open_light <= 0.0
+    frac = got.fraction.reshape(2, -1)[0]
+    assert below.sum() > 500
+    assert np.all(plain.fraction.reshape(2, -1)[0][below] == 1.0)
+    assert np.all(got.irradiance.reshape(2, -1)[0][below] == 0.0)
+    assert (frac[below] == 1.0).mean() > 0.3 and (frac[below] < 0.9).sum() > 100  # the wall's shadow
+    # The sphere alone: every texel below the light's horizon sees all of it
+    # past its own triangle (a convex object's terminator).
+    alone = kernel.scene(meshes[:1])
+    try:
+        v = kernel.visibility(alone, rec, lights, outputs=("fraction",), flags=_lib.CC_BACK_FACING)
+    finally:
+        alone.close()
+    assert np.all(v.fraction.reshape(2, -1)[0][below] == 1.0)
