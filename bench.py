@@ -498,6 +498,35 @@ def batched_leg(args, kernel, dev, stream, flush) -> dict:
     plain_ms = timed_steps(torch, dev, stream, flush, plain, 1, steps)
     kernel_times(kernel)
     b.close()
+    # The gain by job size: each class's jobs batched alone against the same
+    # jobs through the plain path one at a time (same options, same timing).
+    classes = []
+    bounds = [(0, 100_000, "under 100k cones"), (100_000, 1_000_000, "100k-1M cones"),
+              (1_000_000, 1 << 62, "1M cones or more")]
+    for lo, hi, name in bounds:
+        members = [j for j, c in enumerate(cones) if lo <= c < hi]
+        if not members:
+            continue
+        cb = Batch(kernel)
+        for j in members:
+            cb.add(sc[j], rec[j].data_ptr(), rec[j].shape[0], lig[j].data_ptr(), lig[j].shape[0], ptrs[j])
+
+        def class_batched():
+            cb.submit(best, stream=stream.cuda_stream)
+
+        def class_plain():
+            for j in members:
+                kernel.visibility_device(sc[j], rec[j].data_ptr(), rec[j].shape[0], lig[j].data_ptr(),
+                                         lig[j].shape[0], ptrs[j], stream=stream.cuda_stream)
+
+        cbt = float(np.mean(timed_steps(torch, dev, stream, flush, class_batched, 2, steps)))
+        cb.wait()
+        cpt = float(np.mean(timed_steps(torch, dev, stream, flush, class_plain, 1, steps)))
+        kernel_times(kernel)
+        cb.close()
+        n = int(sum(cones[j] for j in members))
+        classes.append({"class": name, "jobs": len(members), "cones": n, "batched_ms": cbt, "plain_per_job_ms": cpt,
+                        "batched_value": n / (cbt * 1e-3), "plain_value": n / (cpt * 1e-3), "speedup": cpt / cbt})
     for s_ in sc:
         s_.close()
     bt, pt = float(np.mean(batched_ms)), float(np.mean(plain_ms))
@@ -509,6 +538,7 @@ def batched_leg(args, kernel, dev, stream, flush) -> dict:
             "plain_per_job": {"value": total / (pt * 1e-3), "ms_per_step": pt,
                               "path": "cc_visibility with device pointers, once per job, same stream"},
             "speedup_vs_plain_per_job": pt / bt,
+            "by_job_size": classes,
             "tuned": {"points_per_warp": best.points_per_warp, "blocks_per_sm": best.blocks_per_sm,
                       "walk_order": "given" if best.flags & _lib.CC_KEEP_ORDER else "morton",
                       "graph_replay": bool(best.flags & _lib.CC_BATCH_GRAPH)},
@@ -553,6 +583,7 @@ def served_leg(args, kernel) -> dict:
         t0 = time.perf_counter()
         kernel.visibility(sc[si], poses[si][pi].numpy(), l)
         service.append(time.perf_counter() - t0)
+    service_alone = service
 
     def pct(x, q):
         return float(np.percentile(np.asarray(x) * 1e3, q)) if len(x) else None
@@ -606,13 +637,20 @@ def served_leg(args, kernel) -> dict:
         st = srv.stats()
         srv.close()
         lat = [x["total_ms"] / 1e3 for x in stats]
+        service = [(x["total_ms"] - x["queued_ms"]) / 1e3 for x in stats]
         big = [x["total_ms"] / 1e3 for x, p in zip(stats, [p for p, t in zip(pts, tickets) if t is not None])
                if p >= 1_000_000]
+        big_service = [(x["total_ms"] - x["queued_ms"]) / 1e3
+                       for x, p in zip(stats, [p for p, t in zip(pts, tickets) if t is not None]) if p >= 1_000_000]
         served_cones = sum(c for c, t in zip(cones, tickets) if t is not None)
         results.append({
             "rate_req_s": rate, "requests": len(reqs), "completed": len(stats), "refused": int(sum(refused)),
             "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
             "p99_ms_requests_of_1M_points_or_more": pct(big, 99) if big else None,
+            "p50_ms_requests_of_1M_points_or_more": pct(big, 50) if big else None,
+            "service_p50_ms": pct(service, 50), "service_p99_ms": pct(service, 99),
+            "service_p99_ms_requests_of_1M_points_or_more": pct(big_service, 99) if big_service else None,
+            "offered_load": rate * float(np.mean(service_alone)) if service_alone else None,
             "queries_per_s": served_cones / span, "requests_per_s": len(stats) / span,
             "launches": st["launches"], "lights_from_cache": st["cached_lights"], "lights_traced": st["traced_lights"],
             "peak_device_bytes": st["peak_bytes"],
@@ -665,6 +703,12 @@ def served_leg(args, kernel) -> dict:
                        "cache_key": "scene and camera pose (recoloured lights are served from the lighting cache)"},
             "plain_per_request_path": "cc_visibility with pinned host buffers, one request at a time; latency under "
                                       "the same arrivals from each request's measured time alone, first come first served",
+            "latency_terms": "total: submission to results in the host buffers; service: admission to results; "
+                             "offered_load: arrival rate x mean time of a request alone (above 1: over capacity)",
+            "requests_of_1M_points_or_more": int(sum(1 for p in pts if p >= 1_000_000)),
+            "kernel_rate_for_16ms_at_1M_points": {
+                "cones_per_s_needed_per_light": 1_000_000 / 0.016,
+                "note": "a 1M-point request with L lights is L M cones: 16 ms needs 62.5 M x L cones/s"},
             "rates": results}
 
 
@@ -1149,7 +1193,7 @@ def main() -> None:
     ap.add_argument("--batch-jobs", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3, help="timed steps of the batched leg (at most --steps)")
     ap.add_argument("--serve-requests", type=int, default=48)
-    ap.add_argument("--serve-rates", default="50,200,2000", help="Poisson arrival rates (requests/s)")
+    ap.add_argument("--serve-rates", default="5,10,20,50,200,2000", help="Poisson arrival rates (requests/s)")
     ap.add_argument("--serve-budget-gib", type=int, default=16)
     ap.add_argument("--points", type=int, default=0,
                     help="keep a strided subset of this many receivers (profiling runs; not a bench line)")

@@ -19,7 +19,7 @@
 //    rasterize them into the owning cone's accumulator — cones whose
 //    triangles take the long clip path no longer hold 31 lanes idle.
 // Results depend on the walk order only through the walk caps: the packet
-// takes its child order from its first lane that descends; a lane whose own
+// takes the child order most of its descending lanes prefer; a lane whose own
 // nearest-first order differs somewhere on its walk, and whose walk then
 // stopped early (capped, or every bin full), is listed and walked again
 // alone by a second launch, so every cone's result is the one its own walk

@@ -550,7 +550,10 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
         const float da = dot(c.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - c.apex);
         const float db = dot(c.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - c.apex);
         const bool pref = db < da;  // this lane's own order: right child nearer
-        swap = __shfl_sync(0xffffffffu, pref, __ffs(owners) - 1);
+        // The packet takes the order most of its descending lanes prefer;
+        // the others are flagged (their walk is redone alone if its order
+        // could matter).
+        swap = 2u * __popc(__ballot_sync(0xffffffffu, descend && pref)) > __popc(owners);
         if (descend && pref != swap) st.status |= 4u;
       } else if (!is_obj) {
         swap = true;  // triangle hierarchies pop the right child first (:783-787)
@@ -694,7 +697,7 @@ __device__ __forceinline__ void scene_walk_splat(const DevScene& s, float prefil
         const float da = dot(st.cone.baxis, (node_lo(la) + node_lo(lb)) * 0.5f - st.cone.apex);
         const float db = dot(st.cone.baxis, (node_lo(xa) + node_lo(xb)) * 0.5f - st.cone.apex);
         const bool pref = db < da;
-        swap = __shfl_sync(0xffffffffu, pref, __ffs(owners) - 1);
+        swap = 2u * __popc(__ballot_sync(0xffffffffu, descend && pref)) > __popc(owners);  // the majority's order
         if (descend && pref != swap) st.status |= 4u;
       }
       const uint32_t l = (kind << kRefKindShift) | ia, r = (kind << kRefKindShift) | (ia + 1u);
