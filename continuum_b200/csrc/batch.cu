@@ -100,6 +100,8 @@ int enqueue(cc_batch* b, const cc_batch_options& opt, cudaStream_t stream) {
   L.pw = opt.points_per_warp;
   L.order = nullptr;
   L.records = static_cast<cc::ConeRecord*>(b->records.ptr);
+  for (const cc::JobGpu& j : b->jobs)
+    if (j.query.hierarchy < 2) L.flat_levels = 1;
   if (!(opt.flags & CC_KEEP_ORDER) && b->points > 0) {
     CC_CUDA(cc::batch_order(L, b->sort_scratch.ptr, b->sort_scratch.size, static_cast<uint32_t*>(b->order.ptr),
                             stream),

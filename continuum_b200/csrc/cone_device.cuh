@@ -263,10 +263,13 @@ __device__ __forceinline__ f3 rotate_to_object(f3 v, const float4* __restrict__ 
 // kHorizon: sky cones, whose horizon `horizon` (the receiver's normal, in the
 // cone's space) also culls a box wholly below it (:245); a light cone's
 // horizon is zero (:146-147), which culls nothing, so light cones skip it.
-template <bool kHorizon = false>
+// kUnrolled: the eight corners side by side (the walk's hot test of a node's
+// children); else one at a time, in a fifth of the code (the tests of a
+// walk's root and of meshes' roots, which run far less often).
+template <bool kHorizon = false, bool kUnrolled = true>
 __device__ __forceinline__ bool may_touch_box(const Cone& c, f3 lo, f3 hi, f3 horizon = f3{0.f, 0.f, 0.f}) {
   bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true, below = kHorizon;
-#pragma unroll
+#pragma unroll (kUnrolled ? 8 : 1)
   for (int k = 0; k < 8; ++k) {
     f3 corner = mk((k & 1) ? hi.x : lo.x, (k & 2) ? hi.y : lo.y, (k & 4) ? hi.z : lo.z);
     if (c.far_offset - dot(c.fwd, corner) >= 0.0f) far_out = false;
@@ -368,6 +371,7 @@ __device__ __forceinline__ void draw_edge(Acc& acc, float q0x, float q0y, float 
   const float dxdy = (p1x - p0x) / (p1y - p0y);
   float x = p0x;
   const uint32_t y_end = min((uint32_t)ceilf(p1y), (uint32_t)kGrid);
+#pragma unroll 1
   for (uint32_t y = (uint32_t)p0y; y < y_end; ++y) {
     const uint32_t row = y * kGrid;
     acc.span_lo = min(acc.span_lo, row);
@@ -380,27 +384,32 @@ __device__ __forceinline__ void draw_edge(Acc& acc, float q0x, float q0y, float 
     uint32_t x0i = (uint32_t)x0_floor;
     float x1_ceil = ceilf(x1);
     uint32_t x1i = (uint32_t)x1_ceil;
-    if (x1i <= x0i + 1) {
-      float xmf = 0.5f * (x + x_next) - x0_floor;
-      acc.add(row + x0i, d - d * xmf);
-      acc.add(row + x0i + 1, d * xmf);
-    } else {
-      float s = 1.0f / (x1 - x0);
-      float x0f = x0 - x0_floor;
-      float a0 = 0.5f * s * (1.0f - x0f) * (1.0f - x0f);
-      float x1f = x1 - x1_ceil + 1.0f;
-      float am = 0.5f * s * x1f * x1f;
-      acc.add(row + x0i, d * a0);
-      if (x1i == x0i + 2) {
-        acc.add(row + x0i + 1, d * (1.0f - a0 - am));
-      } else {
-        float a1 = s * (1.5f - x0f);
-        acc.add(row + x0i + 1, d * (a1 - a0));
-        for (uint32_t xi = x0i + 2; xi < x1i - 1; ++xi) acc.add(row + xi, d * s);
-        float a2 = a1 + float(x1i - x0i - 3) * s;
-        acc.add(row + x1i - 1, d * (1.0f - a2 - am));
-      }
-      acc.add(row + x1i, d * am);
+    // The row's cells x0i .. last and their shares (the WGSL's cases), all
+    // added from one site.
+    const bool narrow = x1i <= x0i + 1;
+    const float xmf = 0.5f * (x + x_next) - x0_floor;
+    float s = 0.f, a0 = 0.f, am = 0.f, a1 = 0.f, a2 = 0.f;
+    if (!narrow) {
+      s = 1.0f / (x1 - x0);
+      const float x0f = x0 - x0_floor;
+      a0 = 0.5f * s * (1.0f - x0f) * (1.0f - x0f);
+      const float x1f = x1 - x1_ceil + 1.0f;
+      am = 0.5f * s * x1f * x1f;
+      a1 = s * (1.5f - x0f);
+      a2 = a1 + float(x1i - x0i - 3) * s;
+    }
+    const uint32_t last = narrow ? x0i + 1 : x1i;
+#pragma unroll 1
+    for (uint32_t xi = x0i; xi <= last; ++xi) {
+      float v;
+      if (narrow) v = xi == x0i ? d - d * xmf : d * xmf;
+      else if (xi == x0i) v = d * a0;
+      else if (xi == x1i) v = d * am;
+      else if (x1i == x0i + 2) v = d * (1.0f - a0 - am);
+      else if (xi == x0i + 1) v = d * (a1 - a0);
+      else if (xi == x1i - 1) v = d * (1.0f - a2 - am);
+      else v = d * s;
+      acc.add(row + xi, v);
     }
     x = x_next;
   }
@@ -416,12 +425,19 @@ constexpr int kPolyCap = 16;
 // clip_plane3 (:264-277), in place through a scratch copy.
 __device__ __forceinline__ int clip_plane3(const f3* in, int n, f3* out, f3 normal, float offset) {
   int m = 0;
+#pragma unroll 1
   for (int i = 0; i < n; ++i) {
     f3 a = in[i], b = in[(i + 1) % n];
     float da = offset - dot(normal, a), db = offset - dot(normal, b);
     if (da >= 0.0f && m < kPolyCap) out[m++] = a;
-    if (da >= 0.0f && db < 0.0f && m < kPolyCap) out[m++] = a + (b - a) * (da / (da - db));
-    if (da < 0.0f && db >= 0.0f && m < kPolyCap) out[m++] = b + (a - b) * (db / (db - da));
+    // The crossing, from the vertex inside (a, leaving) or outside (b,
+    // entering): one division site for both.
+    const bool leaves = da >= 0.0f && db < 0.0f, enters = da < 0.0f && db >= 0.0f;
+    if ((leaves || enters) && m < kPolyCap) {
+      const f3 from = leaves ? a : b, to = leaves ? b : a;
+      const float d_from = leaves ? da : db, d_to = leaves ? db : da;
+      out[m++] = from + (to - from) * (d_from / (d_from - d_to));
+    }
   }
   return m;
 }
@@ -429,18 +445,18 @@ __device__ __forceinline__ int clip_plane3(const f3* in, int n, f3* out, f3 norm
 // clip_line2 (:280-294)
 __device__ __forceinline__ int clip_line2(const float2* in, int n, float2* out, float nx, float ny, float offset) {
   int m = 0;
+#pragma unroll 1
   for (int i = 0; i < n; ++i) {
     float2 a = in[i], b = in[(i + 1) % n];
     float da = offset - (nx * a.x + ny * a.y);
     float db = offset - (nx * b.x + ny * b.y);
     if (da >= 0.0f && m < kPolyCap) out[m++] = a;
-    if (da >= 0.0f && db < 0.0f && m < kPolyCap) {
-      float f = da / (da - db);
-      out[m++] = make_float2(a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f);
-    }
-    if (da < 0.0f && db >= 0.0f && m < kPolyCap) {
-      float f = db / (db - da);
-      out[m++] = make_float2(b.x + (a.x - b.x) * f, b.y + (a.y - b.y) * f);
+    const bool leaves = da >= 0.0f && db < 0.0f, enters = da < 0.0f && db >= 0.0f;
+    if ((leaves || enters) && m < kPolyCap) {
+      const float2 from = leaves ? a : b, to = leaves ? b : a;
+      const float d_from = leaves ? da : db, d_to = leaves ? db : da;
+      const float f = d_from / (d_from - d_to);
+      out[m++] = make_float2(from.x + (to.x - from.x) * f, from.y + (to.y - from.y) * f);
     }
   }
   return m;
@@ -449,6 +465,7 @@ __device__ __forceinline__ int clip_line2(const float2* in, int n, float2* out, 
 template <class Acc>
 __device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n) {
   const float g = float(kGrid);
+#pragma unroll 1
   for (int i = 0; i < n; ++i) {
     float2 a = q[i], b = q[(i + 1) % n];
     draw_edge(acc, clampf(a.x, 0.f, g), clampf(a.y, 0.f, g), clampf(b.x, 0.f, g), clampf(b.y, 0.f, g), 1.0f);
@@ -459,6 +476,9 @@ __device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n) {
 // :350-451): far and near clips, then either the projected corners or, for a
 // polygon reaching outside the window, the window square clipped to the
 // planes through the apex and each edge; finally the square's sides.
+// Every loop here stays rolled and each clip has one call site: the walk
+// kernel is bound by instruction fetch, and the unrolled path (1,832
+// instructions against 1,069) made the packet pass 13 % slower.
 template <class Acc>
 static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2, bool far_clip) {
   f3 pa[kPolyCap], pb[kPolyCap];
@@ -468,24 +488,25 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f
   int n = 3;
   f3* p = pa;
   f3* other = pb;
-  if (far_clip) {
-    n = clip_plane3(p, n, other, c.fwd, c.far_offset);
-    f3* t = p;
-    p = other;
-    other = t;
-  }
+  // Pass 0: the far clip (world space), then the corners in the cone's
+  // frame; pass 1: the near clip there. One clip call site for both.
   bool all_near_ok = true, all_in_window = true;
-  for (int i = 0; i < n; ++i) {
-    f3 v = to_local(c, p[i]);
-    p[i] = v;
-    if (v.z < kNear) all_near_ok = false;
-    if (v.x < c.u0 * v.z || v.x > c.u1 * v.z || v.y < c.v0 * v.z || v.y > c.v1 * v.z) all_in_window = false;
-  }
-  if (!all_near_ok) {
-    n = clip_plane3(p, n, other, mk(0.f, 0.f, -1.f), -kNear);
-    f3* t = p;
-    p = other;
-    other = t;
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 0 ? far_clip : !all_near_ok) {
+      n = clip_plane3(p, n, other, pass == 0 ? c.fwd : mk(0.f, 0.f, -1.f), pass == 0 ? c.far_offset : -kNear);
+      f3* t = p;
+      p = other;
+      other = t;
+    }
+    if (pass == 1) break;
+#pragma unroll 1
+    for (int i = 0; i < n; ++i) {
+      f3 v = to_local(c, p[i]);
+      p[i] = v;
+      if (v.z < kNear) all_near_ok = false;
+      if (v.x < c.u0 * v.z || v.x > c.u1 * v.z || v.y < c.v0 * v.z || v.y > c.v1 * v.z) all_in_window = false;
+    }
   }
   if (n < 3) return false;
   const float su = float(kGrid) / (c.u1 - c.u0);
@@ -499,6 +520,7 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f
   float side = 1.0f;
   if (projected) {
     m = n;
+#pragma unroll 1
     for (int i = 0; i < n; ++i) q[i] = make_float2((p[i].x / p[i].z - c.u0) * su, (p[i].y / p[i].z - c.v0) * sv);
   } else {
     f3 l0 = to_local(c, v0), l1 = to_local(c, v1), l2 = to_local(c, v2);
@@ -539,6 +561,7 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f
       off = k.x * c.u0 + k.y * c.v0 + k.z;
     } else if (stage == 1) {
       bool inside = true;
+#pragma unroll 1
       for (int j = 0; j < m; ++j)
         if (q[j].x < 0.f || q[j].y < 0.f || q[j].x > g || q[j].y > g) inside = false;
       if (inside) break;
@@ -585,9 +608,19 @@ __device__ __forceinline__ bool rasterize_fast(const Cone& c, Acc& acc, f3 v0, f
       const float su = float(kGrid) / (c.u1 - c.u0);
       const float sv = float(kGrid) / (c.v1 - c.v0);
       const float g = float(kGrid);
-      float ax = (p0.x / p0.z - c.u0) * su, ay = (p0.y / p0.z - c.v0) * sv;
-      float bx = (p1.x / p1.z - c.u0) * su, by = (p1.y / p1.z - c.v0) * sv;
-      float cx = (p2.x / p2.z - c.u0) * su, cy = (p2.y / p2.z - c.v0) * sv;
+      // The corners projected in turn (one site for each division).
+      float ax = 0.f, ay = 0.f, bx = 0.f, by = 0.f, cx = 0.f, cy = 0.f;
+      f3 pk = p0;
+#pragma unroll 1
+      for (int k = 0; k < 3; ++k) {
+        ax = bx;
+        ay = by;
+        bx = cx;
+        by = cy;
+        cx = (pk.x / pk.z - c.u0) * su;
+        cy = (pk.y / pk.z - c.v0) * sv;
+        pk = k == 0 ? p1 : p2;
+      }
       bool inside = ax >= 0.f && ay >= 0.f && ax <= g && ay <= g && bx >= 0.f && by >= 0.f && bx <= g &&
                     by <= g && cx >= 0.f && cy >= 0.f && cx <= g && cy <= g;
       if (inside) {

@@ -146,6 +146,9 @@ struct BatchLaunch {
   ConeRecord* records = nullptr;
   uint64_t packet_base = 0, packet_count = 0;
   uint64_t cone_base = 0, cone_count = 0;
+  // Some job walks hierarchy level 0 or 1 (the kernel variant that carries
+  // those levels' code is launched).
+  uint32_t flat_levels = 0;
 };
 
 // A chunk of a batch for the split path: whole packets, at most the chunk's

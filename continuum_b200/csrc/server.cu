@@ -363,6 +363,8 @@ void launch(cc_server* s, Slot& slot) {
     L.points = points;
     L.pw = pw;
     L.records = static_cast<cc::ConeRecord*>(d_records);
+    for (const cc::JobGpu& j : jobs)
+      if (j.query.hierarchy < 2) L.flat_levels = 1;
     SRV_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
     L.order = static_cast<const uint32_t*>(d_order);
     uint32_t* counters = static_cast<uint32_t*>(d_counters);

@@ -430,20 +430,23 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& 
 // first (:783-787) with no full check, as in the reference; every popped node
 // a lane needs counts toward its walk cap, though its box was tested when its
 // parent was visited. Levels 0 and 1 keep the reference's loops over meshes
-// and triangles.
-template <bool kCount, bool kInst, class WS>
+// and triangles; they are compiled only into the kernels of kFlat, which
+// launches at those levels take, so the level-2 walk's code stays small.
+template <bool kCount, bool kInst, bool kFlat, class WS>
 __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy, LaneState<WS>& st, bool traced,
                                            int lane) {
   const Cone& c = st.cone;
-  if (hierarchy == 0) {
-    for (uint32_t m = 0; m < s.nmeshes; ++m)
-      add_mesh_flat<kCount, kInst, WS>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
-    return;
+  if constexpr (kFlat) {
+    if (hierarchy == 0) {
+      for (uint32_t m = 0; m < s.nmeshes; ++m)
+        add_mesh_flat<kCount, kInst, WS>(s, st, traced && st.full < (uint32_t)kBins, m, lane);
+      return;
+    }
   }
   WarpStack stk;
   const float4 ra = __ldg(&s.nodes[0]);
   const float4 rb = __ldg(&s.nodes[1]);
-  const bool root_pass = traced && may_touch_box<WS::kSky>(c, node_lo(ra), node_lo(rb), st.horizon);
+  const bool root_pass = traced && may_touch_box<WS::kSky, false>(c, node_lo(ra), node_lo(rb), st.horizon);
   stk.push(0, node_ref(ra, rb, kObjNode), traced, root_pass, lane);
   int sp = 1;
   while (sp > 0) {
@@ -497,10 +500,12 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       st.queued = cover_leaf(s, st.ws, owners, ia, ib, st.queued, lane, st.skip, st.skips);
     } else if (ib > 0) {
       // An object leaf: its meshes.
-      if (hierarchy == 1) {
-        for (uint32_t k = ia; k < ia + ib; ++k)
-          add_mesh_flat<kCount, kInst, WS>(s, st, descend, __ldg(&s.items[k]), lane);
-        continue;
+      if constexpr (kFlat) {
+        if (hierarchy == 1) {
+          for (uint32_t k = ia; k < ia + ib; ++k)
+            add_mesh_flat<kCount, kInst, WS>(s, st, descend, __ldg(&s.items[k]), lane);
+          continue;
+        }
       }
       for (int k = (int)(ia + ib) - 1; k >= (int)ia; --k) {
         const uint4 range = __ldg(&s.meshes[__ldg(&s.items[k])]);
@@ -522,7 +527,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
           stk.push(sp, (kResolve << kRefKindShift) | 1u, false, false, lane);
           stk.push(sp + 1, (kObjRoot << kRefKindShift) | m, descend, mesh_pass, lane);
         } else {
-          const bool mesh_pass = descend && may_touch_box<WS::kSky>(c, node_lo(ma), node_lo(mb), st.horizon);
+          const bool mesh_pass = descend && may_touch_box<WS::kSky, false>(c, node_lo(ma), node_lo(mb), st.horizon);
           stk.push(sp, kResolve << kRefKindShift, false, false, lane);
           stk.push(sp + 1, node_ref(ma, mb, kTriNode), descend, mesh_pass, lane);
         }
@@ -861,7 +866,9 @@ __device__ __forceinline__ uint32_t find_job(const JobGpu* __restrict__ jobs, ui
 // kSplat: prefiltering cones (q.prefilter bins), walking hierarchy level 2.
 // kBack: cones may skip their receiver's own triangle (CC_BACK_FACING; the
 // split path's plain cones of scenes without instancing).
-template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSplat, bool kBack = false>
+// kFlat: the launch's cones may walk hierarchy levels 0 or 1 (else level 2).
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSplat, bool kBack = false,
+          bool kFlat = false>
 // The blocks the shared memory fits per SM; saying so bounds the registers
 // per thread the allocator may use without lowering occupancy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kSky, kSplat>())
@@ -873,6 +880,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
   const int wib = threadIdx.x >> 5;
   WS* ws = reinterpret_cast<WS*>(smem_raw) + wib;
   float cov_local[WS::kSmemCov ? 1 : kBins];  // the lane's cone's coverages, unless the warp's table holds them
+  // The per-packet loops over the 64 bins stay rolled: unrolled, they are
+  // a tenth of the kernel's code, which competes for the instruction caches
+  // with the walk.
+#pragma unroll 1
   for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0;
   if (lane == 0) ws->overflow[0] = 0u;
   ws->span_lo[lane] = 68u;
@@ -974,6 +985,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
     st.independent = false;
     st.skip = kNoneU;
     st.horizon = st.world_horizon = mk(0.f, 0.f, 0.f);
+#pragma unroll 1
     for (int k = 0; k < kBins; ++k) st.cov_at(k) = 0.0f;
 
     const float4 pt4 = __ldg(&q.receivers[2 * (valid ? p : 0) + 0]);
@@ -1040,18 +1052,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
     __syncwarp();
 
     if constexpr (kSplat) scene_walk_splat<kCount, kInst>(s, q.prefilter, st, traced, lane);
-    else scene_walk<kCount, kInst>(s, q.hierarchy, st, traced, lane);
+    else scene_walk<kCount, kInst, kFlat>(s, q.hierarchy, st, traced, lane);
 
     // A grazing sliver stopped at its cap counts as blocked (:1295-1305).
     const bool capped = traced && st.cone_work >= st.cap;
     if (capped) st.status |= 1u;
     if (capped && info.wide_window && !info.wide_clipped) {
+#pragma unroll 1
       for (int k = 0; k < kBins; ++k) st.cov_at(k) = 1.0f;
       st.full = kBins;
     }
     if (traced && st.full >= (uint32_t)kBins) st.status |= 16u;
 
     uint32_t fw0 = 0, fw1 = 0, aw0 = 0, aw1 = 0;
+#pragma unroll 1
     for (int k = 0; k < kBins; ++k) {
       const float v = st.cov_at(k);
       const uint32_t bit = 1u << (k & 31);
@@ -1123,28 +1137,43 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
 // Whether the large dynamic shared memory size was allowed, per device and
 // kernel variant (the attribute is set per device); per unit, for the
 // variants it launches.
-static uint64_t g_attr_set[128] = {};
+static uint64_t g_attr_set[256] = {};
 
-template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false, bool kSplat = false,
-          bool kBack = false>
-static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
-                              const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
-                              cudaStream_t stream) {
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSplat, bool kBack, bool kFlat>
+static cudaError_t launch_variant(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
+                                  const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
+                                  cudaStream_t stream) {
   const size_t smem = (size_t)kWarpsPerBlock * sizeof(KernelShared<kWide, kSky, kSplat, kBack>);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
   const int variant = (kCount ? 1 : 0) + (kBatch ? 2 : 0) + (kInst ? 4 : 0) + (kWide ? 8 : 0) + (kSky ? 16 : 0) +
-                      (kSplat ? 32 : 0) + (kBack ? 64 : 0);
+                      (kSplat ? 32 : 0) + (kBack ? 64 : 0) + (kFlat ? 128 : 0);
   if (!(g_attr_set[variant] & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack>,
+    cudaError_t e = cudaFuncSetAttribute(visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack, kFlat>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     g_attr_set[variant] |= bit;
   }
-  visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack>
+  visibility_kernel<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack, kFlat>
       <<<blocks, kWarpsPerBlock * 32, smem, stream>>>(s, q, o, b, list, list_count, pw);
   return cudaGetLastError();
+}
+
+// The variant for the launch's hierarchy levels: levels 0 and 1 (a plain
+// query's, or some job's of a batch) take the kernel that carries their code.
+template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky = false, bool kSplat = false,
+          bool kBack = false>
+static cudaError_t launch_one(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
+                              const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
+                              cudaStream_t stream) {
+  if constexpr (!kSplat) {
+    if (kBatch ? b.flat_levels != 0u : q.hierarchy < 2u)
+      return launch_variant<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack, true>(s, q, o, b, list, list_count,
+                                                                                     pw, blocks, stream);
+  }
+  return launch_variant<kCount, kBatch, kInst, kWide, kSky, kSplat, kBack, false>(s, q, o, b, list, list_count, pw,
+                                                                                  blocks, stream);
 }
 
 // A plain (not batched) pass of the variant the flags pick; q.back (the split
