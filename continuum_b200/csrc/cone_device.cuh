@@ -427,7 +427,7 @@ __device__ __forceinline__ int clip_plane3(const f3* in, int n, f3* out, f3 norm
   int m = 0;
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
-    f3 a = in[i], b = in[(i + 1) % n];
+    f3 a = in[i], b = in[i + 1 == n ? 0 : i + 1];
     float da = offset - dot(normal, a), db = offset - dot(normal, b);
     if (da >= 0.0f && m < kPolyCap) out[m++] = a;
     // The crossing, from the vertex inside (a, leaving) or outside (b,
@@ -447,7 +447,7 @@ __device__ __forceinline__ int clip_line2(const float2* in, int n, float2* out, 
   int m = 0;
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
-    float2 a = in[i], b = in[(i + 1) % n];
+    float2 a = in[i], b = in[i + 1 == n ? 0 : i + 1];
     float da = offset - (nx * a.x + ny * a.y);
     float db = offset - (nx * b.x + ny * b.y);
     if (da >= 0.0f && m < kPolyCap) out[m++] = a;
@@ -467,7 +467,7 @@ __device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n) {
   const float g = float(kGrid);
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
-    float2 a = q[i], b = q[(i + 1) % n];
+    float2 a = q[i], b = q[i + 1 == n ? 0 : i + 1];
     draw_edge(acc, clampf(a.x, 0.f, g), clampf(a.y, 0.f, g), clampf(b.x, 0.f, g), clampf(b.y, 0.f, g), 1.0f);
   }
 }
@@ -551,7 +551,7 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f
         stage = 1;
         continue;
       }
-      const f3 e = cross(p[i], p[(i + 1) % n]);
+      const f3 e = cross(p[i], p[i + 1 == n ? 0 : i + 1]);
       ++i;
       const float l = len(e);
       if (l == 0.0f) continue;

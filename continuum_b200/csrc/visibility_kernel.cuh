@@ -300,6 +300,11 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t 
   uint32_t queued = fast_len(queues), general = general_len(queues);
   const uint32_t n_owners = __popc(owners);
   const uint32_t n_pairs = n_owners * nt;
+  // pair / n_owners as a multiply and a shift: pairs stay below 32 x 15 and
+  // there are 1 to 32 owners, so (pair * magic) >> 16 with magic =
+  // 65536 / n_owners + 1 exceeds the quotient by under 480 / 65536, less than
+  // the 1 / n_owners a quotient's fraction stays below 1 by.
+  const uint32_t magic = 65536u / n_owners + 1u;
   for (uint32_t base = 0; base < n_pairs; base += 32) {
     const uint32_t pair = base + lane;
     bool pass = false;
@@ -307,7 +312,7 @@ __device__ __noinline__ uint32_t cover_leaf(const DevScene& s, WS* ws, uint32_t 
     int owner = 0;
     uint32_t t = kNoneU;
     if (pair < n_pairs) {
-      const uint32_t k = pair / n_owners;
+      const uint32_t k = (pair * magic) >> 16;
       const uint32_t r = pair - k * n_owners;
       owner = (int)__fns(owners, 0, r + 1);
       t = t0 + k;
