@@ -46,7 +46,7 @@ EXPORTS = (
     "cc_scene_destroy", "cc_scene_sizes", "cc_scene_arrays", "cc_scene_device_bytes", "cc_options_default",
     "cc_visibility", "cc_irradiance", "cc_coverage", "cc_scene_primary_hits", "cc_context_kernel_times",
     "cc_visibility_static", "cc_batch_options_default", "cc_batch_create", "cc_batch_destroy", "cc_batch_clear",
-    "cc_batch_add", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
+    "cc_batch_add", "cc_batch_add_update", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
     "cc_server_options_default", "cc_server_create", "cc_server_destroy", "cc_server_add_scene", "cc_server_submit",
     "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms", "cc_scene_move",
     "cc_stale_cones", "cc_visibility_update", "cc_cache_options_default", "cc_cache_create", "cc_cache_destroy",
@@ -166,6 +166,7 @@ def load() -> C.CDLL:
         "cc_batch_destroy": (I, [P]),
         "cc_batch_clear": (I, [P]),
         "cc_batch_add": (I, [P, P, P, U64, P, U32, C.POINTER(Options), C.POINTER(Outputs), C.POINTER(U32)]),
+        "cc_batch_add_update": (I, [P, P, P, U64, P, U32, P, C.POINTER(Options), C.POINTER(Outputs), C.POINTER(U32)]),
         "cc_batch_submit": (I, [P, C.POINTER(BatchOptions), P]),
         "cc_batch_wait": (I, [P, U32]),
         "cc_batch_tune": (I, [P, C.POINTER(BatchOptions), U32, C.POINTER(BatchOptions), P, U32]),

@@ -13,6 +13,17 @@ struct cc_batch {
   cc_context* ctx = nullptr;
   std::vector<cc::JobGpu> jobs;  // host copy; the starts are set by prepare()
   bool count_work = false;       // some job wants work counters
+  bool instanced = false;        // some job's scene is instanced
+  // Update jobs (cc_batch_add_update): the job and its stale bytes. Each
+  // submission lists the stale cones of the job's grid in its walk order
+  // (its slice of upd_list at the job's first cone, its length in
+  // upd_count[k]) and walks only those.
+  struct Update {
+    uint32_t job;
+    const uint8_t* stale;
+  };
+  std::vector<Update> updates;
+  DevBuf upd_perm, upd_flags, upd_list, upd_count, upd_temp;
   uint64_t points = 0, cones = 0;
   // Device state, sized by prepare().
   DevBuf job_table, redo, order, sort_scratch, counters;
@@ -69,6 +80,23 @@ int prepare(cc_batch* b, uint32_t pw) {
   }
   b->packets = packet;
   b->chunks = cc::batch_chunks(job_cones, pw, b->ctx->split_chunk);
+  if (!b->updates.empty()) {
+    size_t temp = 256;
+    for (const cc_batch::Update& u : b->updates)
+      temp = std::max(temp, cc::stale_list_scratch_bytes(job_cones[u.job]));
+    CC_CUDA(b->upd_perm.reserve(std::max<uint64_t>(cone, 1) * 4), "batch update scratch");
+    CC_CUDA(b->upd_flags.reserve(std::max<uint64_t>(cone, 1)), "batch update scratch");
+    CC_CUDA(b->upd_list.reserve(std::max<uint64_t>(cone, 1) * 4), "batch update lists");
+    CC_CUDA(b->upd_count.reserve(b->updates.size() * 4), "batch update counts");
+    CC_CUDA(b->upd_temp.reserve(temp), "batch update scratch");
+    uint32_t* list = static_cast<uint32_t*>(b->upd_list.ptr);
+    uint32_t* count = static_cast<uint32_t*>(b->upd_count.ptr);
+    for (size_t k = 0; k < b->updates.size(); ++k) {
+      cc::JobGpu& j = b->jobs[b->updates[k].job];
+      j.query.cones = list + j.cone_start;
+      j.query.cones_count = count + k;
+    }
+  }
   uint64_t slots = 1;
   for (const cc::BatchChunk& k : b->chunks) slots = std::max(slots, k.cone_count);
   CC_CUDA(b->records.reserve(slots * sizeof(cc::ConeRecord)), "batch cone records");
@@ -102,11 +130,22 @@ int enqueue(cc_batch* b, const cc_batch_options& opt, cudaStream_t stream) {
   L.records = static_cast<cc::ConeRecord*>(b->records.ptr);
   for (const cc::JobGpu& j : b->jobs)
     if (j.query.hierarchy < 2) L.flat_levels = 1;
+  L.inst = b->instanced ? 1u : 0u;
   if (!(opt.flags & CC_KEEP_ORDER) && b->points > 0) {
     CC_CUDA(cc::batch_order(L, b->sort_scratch.ptr, b->sort_scratch.size, static_cast<uint32_t*>(b->order.ptr),
                             stream),
             "batch walk order");
     L.order = static_cast<const uint32_t*>(b->order.ptr);
+  }
+  // Update jobs: their stale cones as lists, each light's in the walk order.
+  for (size_t k = 0; k < b->updates.size(); ++k) {
+    const cc::JobGpu& j = b->jobs[b->updates[k].job];
+    const uint64_t at = j.cone_start;
+    CC_CUDA(cc::stale_list(L.order ? L.order + j.point_start : nullptr, b->updates[k].stale, j.query.npoints,
+                           j.query.nlights, static_cast<uint32_t*>(b->upd_perm.ptr) + at,
+                           static_cast<uint8_t*>(b->upd_flags.ptr) + at, static_cast<uint32_t*>(b->upd_list.ptr) + at,
+                           static_cast<uint32_t*>(b->upd_count.ptr) + k, b->upd_temp.ptr, b->upd_temp.size, stream),
+            "batch update list");
   }
   cc::DevOut o{};
   o.redo_count = counters;
@@ -227,18 +266,24 @@ int cc_batch_clear(cc_batch* b) {
   if (b->submitted) CC_CUDA(cudaEventSynchronize(b->done), "batch");
   drop_graph(b);
   b->jobs.clear();
+  b->updates.clear();
+  b->instanced = false;
   b->count_work = false;
   b->points = b->cones = 0;
   b->prepared = false;
   return CC_OK;
 }
 
-int cc_batch_add(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
-                 uint32_t nlights, const cc_options* opt_in, const cc_outputs* out, uint32_t* job) {
+namespace {
+
+// A job of every cone of its grid, or (stale non-null) an update job.
+int add_job(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
+            uint32_t nlights, const uint8_t* stale, const cc_options* opt_in, const cc_outputs* out, uint32_t* job) {
   if (!b || !scene || !out) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != b->ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
-  if (scene->xforms) return fail(CC_ERR_INVALID, "instanced scenes are solved by cc_visibility, not in batches");
   if ((npoints && !receivers) || (nlights && !lights)) return fail(CC_ERR_INVALID, "null inputs");
+  if (stale && (out->partial || out->work))
+    return fail(CC_ERR_INVALID, "an update job writes full, any, irradiance and fraction only");
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
@@ -281,13 +326,29 @@ int cc_batch_add(cc_batch* b, const cc_scene* scene, const float* receivers, uin
     }
   }
   if (job) *job = (uint32_t)b->jobs.size();
+  if (stale) b->updates.push_back({(uint32_t)b->jobs.size(), stale});
   b->jobs.push_back(j);
+  b->instanced = b->instanced || scene->xforms != nullptr;
   b->count_work = b->count_work || out->work != nullptr;
   b->points += npoints;
   b->cones += cones;
   b->prepared = false;
   drop_graph(b);
   return CC_OK;
+}
+
+}  // namespace
+
+int cc_batch_add(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t npoints, const float* lights,
+                 uint32_t nlights, const cc_options* opt_in, const cc_outputs* out, uint32_t* job) {
+  return add_job(b, scene, receivers, npoints, lights, nlights, nullptr, opt_in, out, job);
+}
+
+int cc_batch_add_update(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                        const float* lights, uint32_t nlights, const uint8_t* stale, const cc_options* opt_in,
+                        const cc_outputs* out, uint32_t* job) {
+  if (!stale) return fail(CC_ERR_INVALID, "null stale flags");
+  return add_job(b, scene, receivers, npoints, lights, nlights, stale, opt_in, out, job);
 }
 
 int cc_batch_submit(cc_batch* b, const cc_batch_options* opt_in, void* stream_in) {

@@ -87,6 +87,16 @@ size_t walk_order_scratch_bytes(uint64_t npoints);
 cudaError_t walk_order(const float4* receivers, uint64_t npoints, const float* scene_lo, const float* scene_hi,
                        void* scratch, size_t scratch_bytes, uint32_t* order, cudaStream_t stream);
 
+// The stale cones of a (light, point) grid as one list, each light's in the
+// points' walk order (`order`, or their own order when null): `stale` holds a
+// byte per cone (light-major), `perm` and `flags` take a word and a byte per
+// cone, `count` the list's length; `temp` (stale_list_scratch_bytes) is the
+// selection's scratch. On `stream`.
+size_t stale_list_scratch_bytes(uint64_t ncones);
+cudaError_t stale_list(const uint32_t* order, const uint8_t* stale, uint64_t npoints, uint32_t nlights, uint32_t* perm,
+                       uint8_t* flags, uint32_t* list, uint32_t* count, void* temp, size_t temp_bytes,
+                       cudaStream_t stream);
+
 struct DevOut {
   uint2* full;
   uint2* any;
@@ -149,6 +159,8 @@ struct BatchLaunch {
   // Some job walks hierarchy level 0 or 1 (the kernel variant that carries
   // those levels' code is launched).
   uint32_t flat_levels = 0;
+  // Some job's scene is instanced (the instanced variant is launched).
+  uint32_t inst = 0;
 };
 
 // A chunk of a batch for the split path: whole packets, at most the chunk's

@@ -179,16 +179,19 @@ __global__ void iota_kernel(uint32_t* out, uint64_t n) {
 }
 
 // Slot k = l * npoints + i walks cone l * npoints + order[i] (the points'
-// walk order within each light); its flag is that cone's staleness.
+// walk order within each light; no order: the points' own); its flag is that
+// cone's staleness.
 __global__ void stale_in_order(const uint32_t* __restrict__ order, const uint8_t* __restrict__ stale, uint64_t npoints,
                                uint64_t ncones, uint32_t* __restrict__ perm, uint8_t* __restrict__ flags) {
   const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ncones) return;
   const uint64_t l = k / npoints;
-  const uint32_t c = (uint32_t)(l * npoints + order[k - l * npoints]);
+  const uint64_t i = k - l * npoints;
+  const uint32_t c = (uint32_t)(l * npoints + (order ? order[i] : i));
   perm[k] = c;
   flags[k] = stale[c];
 }
+
 
 // A hierarchy over boxes (two per leaf), for the region tables.
 inline uint32_t float_bits(float f) {
@@ -263,6 +266,27 @@ void box_tree(const std::vector<Box3>& boxes, uint32_t node_base, uint32_t item_
 }
 
 }  // namespace
+
+size_t stale_list_scratch_bytes(uint64_t ncones) {
+  size_t sel_bytes = 0;
+  cub::DeviceSelect::Flagged(nullptr, sel_bytes, (const uint32_t*)nullptr, (const uint8_t*)nullptr, (uint32_t*)nullptr,
+                             (uint32_t*)nullptr, (int)ncones);
+  return std::max<size_t>(sel_bytes, 256);
+}
+
+cudaError_t stale_list(const uint32_t* order, const uint8_t* stale, uint64_t npoints, uint32_t nlights, uint32_t* perm,
+                       uint8_t* flags, uint32_t* list, uint32_t* count, void* temp, size_t temp_bytes,
+                       cudaStream_t stream) {
+  const uint64_t ncones = npoints * (uint64_t)nlights;
+  if (ncones == 0) return cudaMemsetAsync(count, 0, sizeof(uint32_t), stream);
+  const unsigned threads = 256;
+  stale_in_order<<<(unsigned)((ncones + threads - 1) / threads), threads, 0, stream>>>(order, stale, npoints, ncones,
+                                                                                       perm, flags);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(temp, temp_bytes, perm, flags, list, count, (int)ncones, stream);
+  return e;
+}
+
 }  // namespace cc
 
 int cc_scene_move(cc_scene* s, const cc_instance* placements, uint32_t n, float* boxes12) {
@@ -484,13 +508,9 @@ int cc_visibility_update(cc_context* ctx, const cc_scene* scene, const float* re
       e = cudaGetLastError();
     }
   }
-  if (e == cudaSuccess) {
-    cc::stale_in_order<<<(unsigned)((ncones + threads - 1) / threads), threads, 0, stream>>>(order, stale, npoints,
-                                                                                             ncones, perm, flags);
-    e = cudaGetLastError();
-  }
-  size_t bytes = std::max(sel_bytes, sort_bytes);
-  if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(temp, bytes, perm, flags, list, count, (int)ncones, stream);
+  if (e == cudaSuccess)
+    e = cc::stale_list(order, stale, npoints, nlights, perm, flags, list, count, temp, std::max(sel_bytes, sort_bytes),
+                       stream);
   if (e == cudaSuccess) {
     cc_options lo = opt;
     lo.flags |= CC_DEVICE_POINTERS;

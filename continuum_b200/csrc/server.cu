@@ -363,8 +363,10 @@ void launch(cc_server* s, Slot& slot) {
     L.points = points;
     L.pw = pw;
     L.records = static_cast<cc::ConeRecord*>(d_records);
-    for (const cc::JobGpu& j : jobs)
+    for (const cc::JobGpu& j : jobs) {
       if (j.query.hierarchy < 2) L.flat_levels = 1;
+      if (j.scene.xforms) L.inst = 1;  // an instanced scene: the instanced kernel for the launch
+    }
     SRV_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
     L.order = static_cast<const uint32_t*>(d_order);
     uint32_t* counters = static_cast<uint32_t*>(d_counters);
@@ -585,7 +587,6 @@ int cc_server_destroy(cc_server* s) {
 int cc_server_add_scene(cc_server* s, const cc_scene* scene, uint32_t* id) {
   if (!s || !scene) return fail(CC_ERR_INVALID, "null argument");
   if (scene->ctx != s->ctx) return fail(CC_ERR_INVALID, "scene belongs to another context (or to none)");
-  if (scene->xforms) return fail(CC_ERR_INVALID, "instanced scenes are solved by cc_visibility, not by the server");
   std::lock_guard<std::mutex> g(s->mu);
   if (id) *id = (uint32_t)s->scenes.size();
   s->scenes.push_back(scene);

@@ -169,13 +169,25 @@ cudaError_t launch_batch(const BatchLaunch& b0, const DevOut& o, const BatchChun
     const uint64_t want = (b.packet_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const uint64_t cap = (uint64_t)sm_count * blocks_per_sm;
     const uint32_t blocks = (uint32_t)(want < cap ? want : cap);
-    e = count ? launch_one<true, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
-              : launch_one<false, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+    // Batches with an instanced scene take the instanced variant, which
+    // walks world-space scenes too.
+    if (b.inst) {
+      e = count ? launch_one<true, true, true, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
+                : launch_one<false, true, true, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+    } else {
+      e = count ? launch_one<true, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream)
+                : launch_one<false, true, false, false>(s, q, o, b, nullptr, nullptr, b.pw, blocks, stream);
+    }
     if (e != cudaSuccess) return e;
     if (o.redo_list) {
       const uint32_t solo_blocks = (uint32_t)sm_count * kSoloBlocksPerSm;
-      e = count ? launch_one<true, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
-                : launch_one<false, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+      if (b.inst) {
+        e = count ? launch_one<true, true, true, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+                  : launch_one<false, true, true, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+      } else {
+        e = count ? launch_one<true, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream)
+                  : launch_one<false, true, false, true>(s, q, o, b, o.redo_list, o.redo_count, 1, solo_blocks, stream);
+      }
       if (e != cudaSuccess) return e;
     }
     e = launch_batch_integrate(b, o, stream);

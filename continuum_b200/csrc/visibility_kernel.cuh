@@ -956,13 +956,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
       if (!list) wbase = (packet_abs - J->packet_start) * (uint64_t)pw;
     }
     const uint64_t slot = wbase + lane;
-    const bool valid = list ? lane == 0 : ((uint32_t)lane < pw && slot < ncones);
+    bool valid = list ? lane == 0 : ((uint32_t)lane < pw && slot < ncones);
     uint64_t c = 0;
     [[maybe_unused]] uint64_t slot_local = 0;
     [[maybe_unused]] ConeRecord rec;
     if constexpr (kSplit) {
       if (valid) slot_local = list ? listed : (kBatch ? cone_start + slot - batch.cone_base : slot);
       rec = records[slot_local];
+      // A batched job with a cone list (an update) has fewer cones than
+      // slots: the setup marks the slots past its list.
+      if constexpr (kBatch) valid = valid && !(rec.g.x == 0xffffffffu && rec.g.y == 0xffffffffu);
       c = valid ? ((uint64_t)rec.g.x | ((uint64_t)rec.g.y << 32)) : 0;
     } else if (valid) {
       if (list) {

@@ -68,7 +68,9 @@ __device__ __forceinline__ ConeRecord make_record(const DevQuery& q, bool valid,
   r.d = make_float4(cone.fwd.x, cone.fwd.y, cone.fwd.z, cone.u1);
   r.e = make_float4(cone.baxis.x, cone.baxis.y, cone.baxis.z, cone.v1);
   r.f = make_float4(cone.bcos, cone.bsin, spot, __uint_as_float(flags));
-  r.g = make_uint4((uint32_t)c, (uint32_t)(c >> 32), info.wide_window ? q.wide_cone_cap : q.light_cone_cap, job);
+  // A slot past its cone list holds no cone (both words all ones).
+  const uint64_t cn = valid ? c : ~0ull;
+  r.g = make_uint4((uint32_t)cn, (uint32_t)(cn >> 32), info.wide_window ? q.wide_cone_cap : q.light_cone_cap, job);
   return r;
 }
 
@@ -87,7 +89,6 @@ __global__ void cone_setup_kernel(DevQuery q, BatchLaunch b, uint64_t base, uint
     const JobGpu* J = b.jobs + j;
     q = J->query;
     q.order = b.order ? b.order + J->point_start : nullptr;
-    q.cones = nullptr;
     const bool valid = slot_cone(q, bc - J->cone_start, &c);
     records[i] = make_record(q, valid, c, j);
   } else {
@@ -122,9 +123,10 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, Bat
     limit = left < limit ? left : limit;
   }
   const uint64_t slot = first + lane;
-  const bool valid = slot < limit;
-  const ConeRecord r = records[valid ? slot : first];
+  const ConeRecord r = records[slot < limit ? slot : first];
   const uint64_t c = (uint64_t)r.g.x | ((uint64_t)r.g.y << 32);
+  // Batched: a slot past its job's cone list holds no cone.
+  const bool valid = slot < limit && (!kBatch || c != ~0ull);
   float* irradiance = o.irradiance;
   float* fraction = o.fraction;
   if constexpr (kBatch) {
@@ -154,8 +156,9 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, Bat
   cone.v1 = r.e.w;
   cone.bcos = r.f.x;
   cone.bsin = r.f.y;
-  const uint32_t l = (uint32_t)(c / q.npoints);
-  const uint64_t p = c - (uint64_t)l * q.npoints;
+  const uint64_t cv = valid ? c : 0;  // an invalid slot reads cone 0's inputs and writes nothing
+  const uint32_t l = (uint32_t)(cv / q.npoints);
+  const uint64_t p = cv - (uint64_t)l * q.npoints;
   const f3 point = xyz(__ldg(&q.receivers[2 * p + 0]));
   f3 normal = xyz(__ldg(&q.receivers[2 * p + 1]));
   const DevLight L = load_light(q.lights, l);

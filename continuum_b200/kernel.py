@@ -556,6 +556,19 @@ class Batch:
                                   C.c_void_p(d_lights), int(nlights), C.byref(opt), C.byref(o), C.byref(job)))
         return int(job.value)
 
+    def add_update(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int, d_stale: int,
+                   outputs: dict, hierarchy=Hierarchy.TRIANGLES) -> int:
+        """An update job (cc_batch_add_update): each submission recomputes the
+        cones whose byte in the device array `d_stale` (light-major) is set,
+        in place in the device outputs (full, any, irradiance, fraction)."""
+        o = _lib.Outputs(*(outputs.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
+        opt = self.kernel.options(hierarchy)
+        job = C.c_uint32()
+        check(load().cc_batch_add_update(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints),
+                                         C.c_void_p(d_lights), int(nlights), C.c_void_p(d_stale), C.byref(opt),
+                                         C.byref(o), C.byref(job)))
+        return int(job.value)
+
     @staticmethod
     def options(points_per_warp: int = 32, blocks_per_sm: int = 8, flags: int = _lib.CC_BATCH_GRAPH):
         return _lib.BatchOptions(int(points_per_warp), int(blocks_per_sm), int(flags))

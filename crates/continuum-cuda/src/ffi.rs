@@ -246,6 +246,9 @@ unsafe extern "C" {
     pub fn cc_batch_add(batch: *mut cc_batch, scene: *const cc_scene, receivers: *const f32, npoints: u64,
                         lights: *const f32, nlights: u32, opt: *const cc_options, out: *const cc_outputs,
                         job: *mut u32) -> c_int;
+    pub fn cc_batch_add_update(batch: *mut cc_batch, scene: *const cc_scene, receivers: *const f32, npoints: u64,
+                               lights: *const f32, nlights: u32, stale: *const u8, opt: *const cc_options,
+                               out: *const cc_outputs, job: *mut u32) -> c_int;
     pub fn cc_batch_submit(batch: *mut cc_batch, opt: *const cc_batch_options, stream: *mut c_void) -> c_int;
     pub fn cc_batch_wait(batch: *mut cc_batch, timeout_ms: u32) -> c_int;
     pub fn cc_batch_tune(batch: *mut cc_batch, base: *const cc_batch_options, reps: u32,

@@ -352,10 +352,22 @@ CC_API int cc_batch_clear(cc_batch* batch);
  * stay valid while the batch is submitted; opt gives the job's hierarchy,
  * wide extent and walk caps (its points_per_warp and flags are ignored: the
  * batch's options apply). `job` (nullable) receives the job's index. At most
- * 2^32 - 1 cones over all jobs. */
+ * 2^32 - 1 cones over all jobs. The scene may be instanced
+ * (cc_scene_build_instanced); a batch with such a job runs the instanced
+ * kernel for all its jobs. */
 CC_API int cc_batch_add(cc_batch* batch, const cc_scene* scene, const float* receivers, uint64_t npoints,
                         const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                         uint32_t* job);
+/* Appends an update job: cc_visibility_update's work inside the batch (the
+ * reference has no batched form; its view cache re-bakes the stale entries of
+ * moved objects' shadows, vcache.rs). `stale` (device, one byte per cone,
+ * light-major, nonzero = stale) is read at each submission: only those cones
+ * are walked, in the walk order, and written to out (full, any, irradiance,
+ * fraction; partial and work are refused); every other cone's outputs keep
+ * their contents. Each result equals cc_visibility_update's. */
+CC_API int cc_batch_add_update(cc_batch* batch, const cc_scene* scene, const float* receivers, uint64_t npoints,
+                               const float* lights, uint32_t nlights, const uint8_t* stale, const cc_options* opt,
+                               const cc_outputs* out, uint32_t* job);
 /* Enqueues the whole batch on `stream` (NULL: the context's stream) and
  * returns. The first submission after a change of jobs or options sizes the
  * batch's buffers and uploads the job table; with CC_BATCH_GRAPH it runs the
@@ -432,8 +444,8 @@ typedef struct cc_request_stats {
 CC_API int cc_server_create(cc_context* ctx, const cc_server_options* opt, cc_server** out);
 /* Finishes every queued and running request, then stops the loop. */
 CC_API int cc_server_destroy(cc_server* server);
-/* Makes a scene of the server's context resident for requests; `id`
- * receives its index. The scene must outlive the server. */
+/* Makes a scene of the server's context resident for requests (instanced or
+ * not); `id` receives its index. The scene must outlive the server. */
 CC_API int cc_server_add_scene(cc_server* server, const cc_scene* scene, uint32_t* id);
 /* Queues a request (its receivers are read, and its outputs written, by the
  * server's thread: they must stay valid until the request completes; its

@@ -125,6 +125,25 @@ def test_split_chunks_change_no_result(kernel):
         scene.close()
 
 
+def test_host_buffers_with_full_and_any_only(kernel):
+    """Host-buffer calls download FULL and ANY on a second stream while the
+    integration runs; asked for alone (no irradiance or fraction), over one
+    chunk or several, they equal the words of a call that asks for all."""
+    w = small_field(seed=17, n=8, sub=3, width=96, height=54)
+    scene = kernel.scene(w.meshes)
+    base = kernel.visibility(scene, w.receivers, w.lights, outputs=ALL)
+    try:
+        for chunk in (1 << 25, 1000):
+            kernel.set_split_chunk(chunk)
+            got = kernel.visibility(scene, w.receivers, w.lights, outputs=("full", "any"))
+            assert np.array_equal(got.full, base.full), chunk
+            assert np.array_equal(got.any, base.any), chunk
+            assert not hasattr(got, "irradiance") or got.irradiance is None
+    finally:
+        kernel.set_split_chunk(1 << 25)
+        scene.close()
+
+
 def small_field(seed=5, n=12, sub=4, width=160, height=90):
     return scenes.icosphere_field(seed=seed, n_spheres=n, subdivisions=sub, width=width, height=height)
 
