@@ -719,7 +719,11 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
     (device-timed, L2 flushed), then frames in which 1% of the instances (a
     fixed movable set) move: each frame's move (host subtree rebuild and
     upload), stale-cone marking and incremental recompute, wall-clock timed
-    as one update of the cached results, after one untimed frame."""
+    as one update of the cached results, after one untimed frame. The stale
+    cones are recomputed through the batched form (an update job,
+    cc_batch_add_update, replayed from its captured graph); the plain update
+    (cc_visibility_update) recomputes a second copy of the cache beside it,
+    device-timed, and the two copies must be equal."""
     import torch
 
     from continuum_b200 import scenes
@@ -770,9 +774,16 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
 
         oscene = OracleScene.instanced(w.geometries, w.instances, movable)
         check("full_solve")
+    from continuum_b200 import Batch
+
     stale = torch.empty(C, dtype=torch.uint8, device=dev)
+    plain_cache = {k: v.clone() for k, v in cache.items()}
+    plain_ptrs = {k: v.data_ptr() for k, v in plain_cache.items()}
+    batch = Batch(kernel)
+    batch.add_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(), ptrs)
     frames = []
-    # Frame 0 untimed (the update path's first-call costs), then the timed frames.
+    # Frame 0 untimed (first-call costs and the batch's graph capture), then
+    # the timed frames.
     for f in range(0, args.frames + 1):
         pl = scenes.moved_placements(w, movable, f)
         torch.cuda.synchronize(dev)
@@ -780,19 +791,31 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
         boxes = scene.move(pl)
         count = kernel.stale_cones(scene, rec.data_ptr(), P, w.lights, boxes, stale.data_ptr(),
                                    stream=stream.cuda_stream)
-        solved = kernel.visibility_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(), ptrs,
-                                          stream=stream.cuda_stream)
-        torch.cuda.synchronize(dev)
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        e0.record(stream)
+        batch.submit(stream=stream.cuda_stream)
+        e1.record(stream)
+        batch.wait()
         ms = (time.perf_counter() - t0) * 1e3
+        e2.record(stream)
+        solved = kernel.visibility_update(scene, rec.data_ptr(), P, lig.data_ptr(), L, stale.data_ptr(), plain_ptrs,
+                                          stream=stream.cuda_stream)
+        e3.record(stream)
+        torch.cuda.synchronize(dev)
         if f > 0:
-            frames.append({"ms": ms, "stale_cones": count, "recomputed": solved, "stale_share": count / C})
+            frames.append({"ms": ms, "stale_cones": count, "recomputed": solved, "stale_share": count / C,
+                           "batched_recompute_ms": e0.elapsed_time(e1), "plain_update_ms": e2.elapsed_time(e3)})
         last_placements = pl
+    batched_equals_plain = all(torch.equal(cache[k], plain_cache[k]) for k in cache)
+    batch.close()
+    del plain_cache
     if oscene is not None:
         oscene.move(last_placements)
         check(f"after_{args.frames + 1}_moving_frames")
         oscene.close()
     scene.close()
     upd = float(np.mean([fr["ms"] for fr in frames])) if frames else None
+    mean = lambda key: float(np.mean([fr[key] for fr in frames])) if frames else None
     return {"workload": f"{n_obj - 1} boulder instances (10 displaced UV spheres, 10,240 triangles each) on a ground "
                         f"quad, {L} lights, 1280x720 primary hits; 1% of the instances move per frame",
             "instanced_triangles": w.instanced_tris, "points": P, "cones": C, "accuracy": acc or None,
@@ -801,8 +824,12 @@ def instanced_leg(args, kernel, dev, stream, flush) -> dict:
             "frames": frames,
             "update": {"ms_per_frame": upd, "cones_per_s_served": (C / (upd * 1e-3)) if upd else None,
                        "timing": "wall clock: host move of the movers' subtree and upload, stale-cone marking, "
-                                 "recompute of the stale cones",
-                       "speedup_vs_full_solve": (full_ms / upd) if upd else None}}
+                                 "recompute of the stale cones through the batched form (an update job, graph "
+                                 "replay)",
+                       "speedup_vs_full_solve": (full_ms / upd) if upd else None,
+                       "batched_recompute_ms": mean("batched_recompute_ms"),
+                       "plain_update_ms": mean("plain_update_ms"),
+                       "batched_equals_plain_update": batched_equals_plain}}
 
 
 def bake_leg(args, kernel, scene, w) -> dict:
