@@ -48,7 +48,7 @@ EXPORTS = (
     "cc_visibility_static", "cc_batch_options_default", "cc_batch_create", "cc_batch_destroy", "cc_batch_clear",
     "cc_batch_add", "cc_batch_add_update", "cc_batch_submit", "cc_batch_wait", "cc_batch_tune", "cc_batch_sizes",
     "cc_server_options_default", "cc_server_create", "cc_server_destroy", "cc_server_add_scene", "cc_server_submit",
-    "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms", "cc_scene_move",
+    "cc_server_wait", "cc_server_stats", "cc_scene_build_instanced", "cc_scene_transforms", "cc_scene_move", "cc_scene_set_clear",
     "cc_stale_cones", "cc_visibility_update", "cc_cache_options_default", "cc_cache_create", "cc_cache_destroy",
     "cc_cache_frame", "cc_cache_read", "cc_cache_pool", "cc_cache_jobs", "cc_planner_create", "cc_planner_destroy",
     "cc_planner_frame", "cc_planner_jobs", "cc_planner_slot", "cc_sky_visibility", "cc_scene_coverage",
@@ -180,6 +180,7 @@ def load() -> C.CDLL:
         "cc_server_stats": (I, [P, P]),
         "cc_scene_build_instanced": (I, [P, P, P, U32, P, U32, P, U32, C.POINTER(P)]),
         "cc_scene_move": (I, [P, P, U32, P]),
+        "cc_scene_set_clear": (I, [P, P, U32]),
         "cc_stale_cones": (I, [P, P, P, U64, P, U32, P, U32, P, C.POINTER(U64), P]),
         "cc_visibility_update": (I, [P, P, P, U64, P, U32, P, C.POINTER(Options), C.POINTER(Outputs), C.POINTER(U64), P]),
         "cc_scene_transforms": (U64, [P, P, U64]),

@@ -347,6 +347,8 @@ void build_instanced_scene(const float* tri9, const uint32_t* geometry_counts, u
   // Each geometry's triangles and hierarchy once (flatten, triangle_hierarchy).
   build_flat_scene(tri9, geometry_counts, ngeometries, out, threads);
   const std::vector<uint32_t> geometry_ranges = out.ranges;
+  out.geometry_roots.assign(ngeometries, kNone);
+  for (uint32_t g = 0; g < ngeometries; ++g) out.geometry_roots[g] = geometry_ranges[4 * g + 2];
   std::vector<Box> local(ngeometries);
   for (uint32_t g = 0; g < ngeometries; ++g)
     local[g] = bounds_of(out.tris.data(), geometry_ranges[4 * g], geometry_ranges[4 * g + 1]);
@@ -440,8 +442,9 @@ void move_instances(FlatScene& s, const Instance* placements, float* boxes12) {
     const Instance& o = placements[i];
     const float* R = o.rotation;
     const float* tr = o.translation;
+    // The object keeps its `clear` (row 3's z) where it moves.
     const float row[16] = {R[0], R[1], R[2], tr[0], R[3], R[4], R[5], tr[1], R[6], R[7], R[8], tr[2],
-                           o.scale, 1.0f / o.scale, 0.0f, 0.0f};
+                           o.scale, 1.0f / o.scale, X[14], 0.0f};
     std::memcpy(X, row, sizeof(row));
     mover_bounds[i] = world_bounds(local, o);
     if (boxes12) {
@@ -468,6 +471,19 @@ static void coverage_directions(float d[kCoverageSamples][3]) {
   }
 }
 
+// A placed object's opacity for its geometry's coverage samples: blended
+// (clear in (0, 1)), transmissive at normal incidence (clear below 0), a
+// volume's two surfaces (clear at most -2) (flatten_instanced,
+// hierarchy.rs:488-497).
+static float clear_opacity(float clear) {
+  if (clear > 0.0f) return 1.0f - clear;
+  if (clear <= -2.0f) {
+    const float t = 0.96f * (-2.0f - clear);
+    return 1.0f - t * t;
+  }
+  return 1.0f - 0.96f * -clear;
+}
+
 std::vector<float> blas_coverage(const FlatScene& s) {
   float dirs[kCoverageSamples][3];
   coverage_directions(dirs);
@@ -491,6 +507,29 @@ std::vector<float> blas_coverage(const FlatScene& s) {
       const float* a = cov.data() + (size_t)x * kCoverageSamples;
       const float* b = a + kCoverageSamples;
       for (uint32_t d = 0; d < kCoverageSamples; ++d) out[d] = a[d] + b[d];
+    }
+  }
+  // Instanced scenes: a geometry whose first placing object is blended or
+  // transmissive has its nodes' samples (its root's and those after it, up
+  // to the next geometry's root) scaled by that object's opacity
+  // (hierarchy.rs:469-503).
+  if (!s.xforms.empty()) {
+    const uint32_t ngeom = (uint32_t)s.geometry_roots.size();
+    std::vector<uint32_t> first_object(ngeom, kNone);
+    for (uint32_t m = (uint32_t)s.object_geometry.size(); m-- > 0;)
+      if (s.object_geometry[m] < ngeom) first_object[s.object_geometry[m]] = m;
+    std::vector<std::pair<uint32_t, uint32_t>> roots;  // (root, geometry) of every geometry with triangles
+    for (uint32_t g = 0; g < ngeom; ++g)
+      if (s.geometry_roots[g] != kNone) roots.push_back({s.geometry_roots[g], g});
+    std::sort(roots.begin(), roots.end());
+    for (size_t k = 0; k < roots.size(); ++k) {
+      const uint32_t m = first_object[roots[k].second];
+      if (m == kNone) continue;
+      const float clear = s.xforms[16 * (size_t)s.ranges[4 * m + 3] + 14];
+      if (clear == 0.0f) continue;
+      const float opacity = clear_opacity(clear);
+      const size_t end = k + 1 < roots.size() ? roots[k + 1].first : n;
+      for (size_t i = (size_t)roots[k].first * kCoverageSamples; i < end * kCoverageSamples; ++i) cov[i] *= opacity;
     }
   }
   return cov;

@@ -49,6 +49,7 @@ struct FlatScene {
   std::vector<float> xforms;
   std::vector<uint32_t> object_geometry;  // instanced scenes: each object's geometry
   std::vector<float> geometry_bounds;     // instanced scenes: each geometry's object-space box (lo, hi)
+  std::vector<uint32_t> geometry_roots;   // instanced scenes: each geometry's triangle-hierarchy root (kNone: none)
   MoverTree movers;                       // instanced scenes built with movable objects
 };
 

@@ -697,6 +697,35 @@ int cc_visibility(cc_context* ctx, const cc_scene* scene, const float* receivers
                                   nullptr);
 }
 
+int cc_scene_set_clear(cc_scene* s, const float* clear, uint32_t nobjects) {
+  if (!s || (nobjects && !clear)) return fail(CC_ERR_INVALID, "null argument");
+  cc::FlatScene& f = s->flat;
+  if (f.xforms.empty() || f.object_geometry.empty())
+    return fail(CC_ERR_INVALID, "blended and transmissive objects are placed objects: the scene is not instanced");
+  if (nobjects != f.object_geometry.size()) return fail(CC_ERR_INVALID, "one value per object, in their order");
+  for (uint32_t m = 0; m < nobjects; ++m)
+    if (!std::isfinite(clear[m]) || clear[m] >= 1.0f) return fail(CC_ERR_INVALID, "clear must be finite and below 1");
+  for (uint32_t m = 0; m < nobjects; ++m) f.xforms[16 * (size_t)f.ranges[4 * m + 3] + 14] = clear[m];
+  if (!s->ctx) return CC_OK;
+  int rc = set_device(s->ctx);
+  if (rc) return rc;
+  CC_CUDA(cudaMemcpy(s->xforms, f.xforms.data(), f.xforms.size() * sizeof(float), cudaMemcpyHostToDevice),
+          "object transforms");
+  if (s->coverage_ready) {
+    // The prefiltered cones' samples scale with the objects' opacity: the
+    // same buffers, refilled.
+    const std::vector<float> blas = cc::blas_coverage(f);
+    if (!blas.empty())
+      CC_CUDA(cudaMemcpy(s->blas_cov, blas.data(), blas.size() * sizeof(float), cudaMemcpyHostToDevice),
+              "triangle-node coverage");
+    const std::vector<float> obj = cc::object_coverage(f, blas);
+    if (!obj.empty() && s->obj_cov)
+      CC_CUDA(cudaMemcpy(s->obj_cov, obj.data(), obj.size() * sizeof(float), cudaMemcpyHostToDevice),
+              "object-node coverage");
+  }
+  return CC_OK;
+}
+
 int64_t cc_scene_coverage(const cc_scene* scene, float* blas27, uint64_t max_blas, float* obj27, uint64_t max_obj) {
   if (!scene) return -(int64_t)fail(CC_ERR_INVALID, "null scene");
   const std::vector<float> blas = cc::blas_coverage(scene->flat);

@@ -463,12 +463,12 @@ __device__ __forceinline__ int clip_line2(const float2* in, int n, float2* out, 
 }
 
 template <class Acc>
-__device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n) {
+__device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n, float weight) {
   const float g = float(kGrid);
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
     float2 a = q[i], b = q[i + 1 == n ? 0 : i + 1];
-    draw_edge(acc, clampf(a.x, 0.f, g), clampf(a.y, 0.f, g), clampf(b.x, 0.f, g), clampf(b.y, 0.f, g), 1.0f);
+    draw_edge(acc, clampf(a.x, 0.f, g), clampf(a.y, 0.f, g), clampf(b.x, 0.f, g), clampf(b.y, 0.f, g), weight);
   }
 }
 
@@ -479,8 +479,11 @@ __device__ __forceinline__ void draw_polygon(Acc& acc, const float2* q, int n) {
 // Every loop here stays rolled and each clip has one call site: the walk
 // kernel is bound by instruction fetch, and the unrolled path (1,832
 // instructions against 1,069) made the packet pass 13 % slower.
-template <class Acc>
-static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2, bool far_clip) {
+// kWeighted: the triangle is drawn with `weight` (tri_weight: a blended or
+// transmissive object's); else whole.
+template <class Acc, bool kWeighted = false>
+static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2, bool far_clip,
+                                                      float weight = 1.0f) {
   f3 pa[kPolyCap], pb[kPolyCap];
   pa[0] = v0;
   pa[1] = v1;
@@ -581,7 +584,7 @@ static __device__ __noinline__ bool rasterize_general(const Cone& c, Acc& acc, f
     q2 = t;
   }
   if (m < 3) return false;
-  draw_polygon(acc, q, m);
+  draw_polygon(acc, q, m, kWeighted ? weight : 1.0f);
   return true;
 }
 
@@ -598,7 +601,7 @@ __device__ __forceinline__ bool crosses_far(const Cone& c, f3 v0, f3 v1, f3 v2) 
 // from registers. Returns false, having drawn nothing, for every other
 // triangle: those take rasterize_general.
 template <class Acc>
-__device__ __forceinline__ bool rasterize_fast(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2) {
+__device__ __forceinline__ bool rasterize_fast(const Cone& c, Acc& acc, f3 v0, f3 v1, f3 v2, float weight = 1.0f) {
   if (!crosses_far(c, v0, v1, v2)) {
     f3 p0 = to_local(c, v0), p1 = to_local(c, v1), p2 = to_local(c, v2);
     auto in_win = [&](f3 v) {
@@ -630,7 +633,7 @@ __device__ __forceinline__ bool rasterize_fast(const Cone& c, Acc& acc, f3 v0, f
         for (int e = 0; e < 3; ++e) {
           const float sx = e == 0 ? ax : (e == 1 ? bx : cx), sy = e == 0 ? ay : (e == 1 ? by : cy);
           const float tx = e == 0 ? bx : (e == 1 ? cx : ax), ty = e == 0 ? by : (e == 1 ? cy : ay);
-          draw_edge(acc, sx, sy, tx, ty, 1.0f);
+          draw_edge(acc, sx, sy, tx, ty, weight);
         }
         return true;
       }

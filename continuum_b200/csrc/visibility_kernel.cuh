@@ -37,12 +37,16 @@ __device__ __forceinline__ uint32_t queue_lens(uint32_t fast, uint32_t general) 
 // block lets more warps be resident).
 // Back: the launch's cones may skip their receiver's own triangle
 // (CC_BACK_FACING); other launches compile without the check.
-template <class CellT, bool Sky, bool SmemCov, bool Back = false>
+// Weighted: instanced scenes, whose placed objects may be alpha-blended or
+// transmissive (the transform's `clear`): triangles are drawn with the
+// current object's weight; other launches draw every triangle whole.
+template <class CellT, bool Sky, bool SmemCov, bool Back = false, bool Weighted = false>
 struct WarpShared {
   using Cell = CellT;
   static constexpr bool kSky = Sky;
   static constexpr bool kSmemCov = SmemCov;
   static constexpr bool kBack = Back;
+  static constexpr bool kWeighted = Weighted;
   Cell acc[kBins * 32];                 // each cone's accumulator (fixed point, units of kFixUnit)
   float cone[kConeFields * 32];         // each cone's frame, field-major; the integration's scratch after the walk
   uint32_t span_lo[32], span_hi[32];    // each cone's accumulator rows written (the WGSL's span)
@@ -51,15 +55,20 @@ struct WarpShared {
   uint32_t overflow[4];                 // word 0: cones whose 32-bit accumulation overflowed in the current mesh
   float horizon[Sky ? 3 * 32 : 4];      // sky cones: each cone's horizon, field-major
   float cov[SmemCov ? kBins * 32 : 4];  // each cone's 64 coverages, bin-major, lane innermost
+  // The placed object being walked (Weighted): its triangles' weight and its
+  // transmission (add_mesh_coverage_if's tri_weight / tri_transmit /
+  // tri_volume, :725-741); weight 1 and no transmission elsewhere.
+  float object_weight, object_transmit;
+  uint32_t object_volume, object_pad;
 };
 static_assert(sizeof(WarpShared<unsigned int, false, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(sizeof(WarpShared<unsigned long long, false, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(sizeof(WarpShared<unsigned int, true, true>) % 16 == 0, "warp shared block keeps 16-byte alignment");
 static_assert(sizeof(WarpShared<unsigned int, false, false>) % 16 == 0, "warp shared block keeps 16-byte alignment");
-template <bool kSky, bool kSmemCov, bool kBack = false>
-using NarrowShared = WarpShared<unsigned int, kSky, kSmemCov, kBack>;
-template <bool kSky, bool kSmemCov, bool kBack = false>
-using WideShared = WarpShared<unsigned long long, kSky, kSmemCov, kBack>;
+template <bool kSky, bool kSmemCov, bool kBack = false, bool kWeighted = false>
+using NarrowShared = WarpShared<unsigned int, kSky, kSmemCov, kBack, kWeighted>;
+template <bool kSky, bool kSmemCov, bool kBack = false, bool kWeighted = false>
+using WideShared = WarpShared<unsigned long long, kSky, kSmemCov, kBack, kWeighted>;
 // The shared memory of a kernel variant's warps, and the blocks per SM it
 // fits. Prefiltering light cones integrate in the walk kernel, reading every
 // lane's coverages (warp_blocked): their table stays in shared memory. The
@@ -69,9 +78,9 @@ using WideShared = WarpShared<unsigned long long, kSky, kSmemCov, kBack>;
 // (8 would cap registers at 128 and spill).
 template <bool kSky, bool kSplat>
 constexpr bool smem_cov() { return kSplat && !kSky; }
-template <bool kWide, bool kSky, bool kSplat, bool kBack = false>
-using KernelShared = typename std::conditional<kWide, WideShared<kSky, smem_cov<kSky, kSplat>(), kBack>,
-                                               NarrowShared<kSky, smem_cov<kSky, kSplat>(), kBack>>::type;
+template <bool kWide, bool kSky, bool kSplat, bool kBack = false, bool kInst = false>
+using KernelShared = typename std::conditional<kWide, WideShared<kSky, smem_cov<kSky, kSplat>(), kBack, kInst>,
+                                               NarrowShared<kSky, smem_cov<kSky, kSplat>(), kBack, kInst>>::type;
 constexpr int resident_blocks_for(bool wide, bool sky, bool splat) {
   return (splat && !sky) ? (wide ? kFusedSoloBlocksPerSm : kFusedBlocksPerSm)
                          : (wide ? kSoloBlocksPerSm : (splat ? kSkySplatBlocksPerSm : kBlocksPerSm));
@@ -232,6 +241,56 @@ __device__ __forceinline__ void load_pair(const DevScene& s, const WS* ws, uint3
   v2 = xyz(__ldg(&s.tris[3 * (size_t)t + 2]));
 }
 
+// The weight a (triangle, cone) pair is drawn with: the current object's
+// (1 - clear for a blended one), or for a transmissive object one less what
+// passes through the triangle at the cone's central direction, Schlick's
+// Fresnel with F0 0.04, twice for a volume (cover_triangle, :608-614). The
+// fifth power is taken by multiplications.
+template <class WS>
+__device__ __forceinline__ float pair_weight(const WS* ws, const Cone& c, f3 v0, f3 v1, f3 v2) {
+  const float transmit = ws->object_transmit;
+  if (!(transmit > 0.0f)) return ws->object_weight;
+  const f3 n = cross(v1 - v0, v2 - v0);
+  const float cos_t = fabsf(dot(normalize(n), normalize(direction(c, 0.5f, 0.5f))));
+  const float x = 1.0f - cos_t;
+  const float x2 = x * x;
+  const float f = 0.04f + 0.96f * (x2 * x2 * x);
+  float passes = transmit * (1.0f - f);
+  if (ws->object_volume) passes *= 1.0f - f;
+  return 1.0f - passes;
+}
+
+// Entering placed object X's triangles: its weight and transmission from
+// its transform's `clear` (row 3's z; add_mesh_coverage_if, :733-741); and
+// leaving it. The caller syncs the warp before the values are read.
+template <class WS>
+__device__ __forceinline__ void enter_object(WS* ws, const float4* __restrict__ X, int lane) {
+  if constexpr (WS::kWeighted) {
+    const float clear = __ldg(&X[3]).z;
+    if (lane == 0) {
+      float transmit = fmaxf(-clear, 0.0f);
+      uint32_t volume = 0u;
+      if (clear <= -2.0f) {  // a volume: two surfaces
+        transmit = -2.0f - clear;
+        volume = 1u;
+      }
+      ws->object_weight = 1.0f - fmaxf(clear, 0.0f);
+      ws->object_transmit = transmit;
+      ws->object_volume = volume;
+    }
+  }
+}
+template <class WS>
+__device__ __forceinline__ void leave_object(WS* ws, int lane) {
+  if constexpr (WS::kWeighted) {
+    if (lane == 0) {
+      ws->object_weight = 1.0f;
+      ws->object_transmit = 0.0f;
+      ws->object_volume = 0u;
+    }
+  }
+}
+
 template <class WS, class Acc>
 __device__ __forceinline__ void note_span(WS* ws, int owner, const Acc& acc) {
   if (acc.span_lo < acc.span_hi) {
@@ -250,7 +309,9 @@ __device__ __noinline__ void raster_general(const DevScene& s, WS* ws, uint32_t 
     f3 v0, v1, v2;
     load_pair(s, ws, ws->general[first + lane], owner, c, v0, v1, v2);
     LaneAcc<typename WS::Cell> acc{ws->acc + owner, 68u, 0u, &ws->overflow[0], 1u << owner};
-    rasterize_general(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2));
+    float weight = 1.0f;
+    if constexpr (WS::kWeighted) weight = pair_weight(ws, c, v0, v1, v2);
+    rasterize_general<decltype(acc), WS::kWeighted>(c, acc, v0, v1, v2, crosses_far(c, v0, v1, v2), weight);
     note_span(ws, owner, acc);
   }
   __syncwarp();
@@ -272,7 +333,9 @@ __device__ __noinline__ uint32_t raster_queue(const DevScene& s, WS* ws, uint32_
     f3 v0, v1, v2;
     load_pair(s, ws, e, owner, c, v0, v1, v2);
     LaneAcc<typename WS::Cell> acc{ws->acc + owner, 68u, 0u, &ws->overflow[0], 1u << owner};
-    defer = !rasterize_fast(c, acc, v0, v1, v2);
+    float weight = 1.0f;
+    if constexpr (WS::kWeighted) weight = pair_weight(ws, c, v0, v1, v2);
+    defer = !rasterize_fast(c, acc, v0, v1, v2, weight);
     note_span(ws, owner, acc);
   }
   const uint32_t m = __ballot_sync(0xffffffffu, defer);
@@ -403,6 +466,7 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& 
   if (placed) {
     st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);  // cone_to_object (:623-638)
     store_cone(st.ws, st.cone, lane);
+    enter_object(st.ws, s.xforms + 4 * (size_t)range.w, lane);
     if constexpr (WS::kSky) {
       st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
       store_horizon(st.ws, st.horizon, lane);
@@ -417,6 +481,7 @@ __device__ __forceinline__ void add_mesh_flat(const DevScene& s, LaneState<WS>& 
   if (placed) {
     st.cone = st.world;
     store_cone(st.ws, st.cone, lane);
+    leave_object(st.ws, lane);
     if constexpr (WS::kSky) {
       st.horizon = st.world_horizon;
       store_horizon(st.ws, st.horizon, lane);
@@ -463,6 +528,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       if (kInst && ref_index(ref) == 1) {  // back to world space
         st.cone = st.world;
         store_cone(st.ws, st.cone, lane);
+        leave_object(st.ws, lane);
         if constexpr (WS::kSky) {
           st.horizon = st.world_horizon;
           store_horizon(st.ws, st.horizon, lane);
@@ -477,6 +543,7 @@ __device__ __forceinline__ void scene_walk(const DevScene& s, uint32_t hierarchy
       const uint4 range = __ldg(&s.meshes[ref_index(ref)]);
       st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
       store_cone(st.ws, st.cone, lane);
+      enter_object(st.ws, s.xforms + 4 * (size_t)range.w, lane);
       if constexpr (WS::kSky) {
         // The horizon turns with the cone (:634).
         st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
@@ -607,6 +674,7 @@ __device__ __forceinline__ void scene_walk_splat(const DevScene& s, float prefil
       if (kInst && idx == 1) {  // back to world space
         st.cone = st.world;
         store_cone(ws, st.cone, lane);
+        leave_object(ws, lane);
         if constexpr (WS::kSky) {
           st.horizon = st.world_horizon;
           store_horizon(ws, st.horizon, lane);
@@ -621,6 +689,7 @@ __device__ __forceinline__ void scene_walk_splat(const DevScene& s, float prefil
       const uint4 range = __ldg(&s.meshes[idx]);
       st.cone = cone_to_object(st.world, s.xforms + 4 * (size_t)range.w);
       store_cone(ws, st.cone, lane);
+      enter_object(ws, s.xforms + 4 * (size_t)range.w, lane);
       if constexpr (WS::kSky) {
         st.horizon = rotate_to_object(st.world_horizon, s.xforms + 4 * (size_t)range.w);
         store_horizon(ws, st.horizon, lane);
@@ -879,7 +948,7 @@ template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSpl
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kSky, kSplat>())
     visibility_kernel(DevScene s_plain, DevQuery q_plain, DevOut o, BatchLaunch batch,
                       const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count, uint32_t pw) {
-  using WS = KernelShared<kWide, kSky, kSplat, kBack>;
+  using WS = KernelShared<kWide, kSky, kSplat, kBack, kInst>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -891,6 +960,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
 #pragma unroll 1
   for (int k = 0; k < kBins; ++k) ws->acc[32 * k + lane] = 0;
   if (lane == 0) ws->overflow[0] = 0u;
+  leave_object(ws, lane);  // the world's weight until a placed object is entered
   ws->span_lo[lane] = 68u;
   ws->span_hi[lane] = 0u;
 
@@ -1151,7 +1221,7 @@ template <bool kCount, bool kBatch, bool kInst, bool kWide, bool kSky, bool kSpl
 static cudaError_t launch_variant(const DevScene& s, const DevQuery& q, const DevOut& o, const BatchLaunch& b,
                                   const uint32_t* list, const uint32_t* list_count, uint32_t pw, uint32_t blocks,
                                   cudaStream_t stream) {
-  const size_t smem = (size_t)kWarpsPerBlock * sizeof(KernelShared<kWide, kSky, kSplat, kBack>);
+  const size_t smem = (size_t)kWarpsPerBlock * sizeof(KernelShared<kWide, kSky, kSplat, kBack, kInst>);
   int dev = 0;
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);

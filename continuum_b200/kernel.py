@@ -219,6 +219,12 @@ class Scene:
         check(load().cc_scene_move(self.handle, ptr(inst), len(inst), ptr(boxes)))
         return boxes
 
+    def set_clear(self, clear) -> None:
+        """Each object's `clear` (cc_scene_set_clear): 0 opaque, (0, 1)
+        alpha-blended, below 0 transmissive (at most -2 a volume)."""
+        c = np.ascontiguousarray(clear, np.float32)
+        check(load().cc_scene_set_clear(self.handle, ptr(c), len(c)))
+
     def transforms(self) -> np.ndarray:
         """The objects' transforms, 16 floats each (instanced scenes; else empty)."""
         n = int(load().cc_scene_transforms(self.handle, None, 0))

@@ -212,6 +212,7 @@ unsafe extern "C" {
                                     movable: *const u32, nmovable: u32, out: *mut *mut cc_scene) -> c_int;
     pub fn cc_scene_move(scene: *mut cc_scene, placements: *const cc_instance, nplacements: u32,
                          boxes12: *mut f32) -> c_int;
+    pub fn cc_scene_set_clear(scene: *mut cc_scene, clear: *const f32, nobjects: u32) -> c_int;
     pub fn cc_stale_cones(ctx: *mut cc_context, scene: *const cc_scene, receivers: *const f32, npoints: u64,
                           lights: *const f32, nlights: u32, boxes12: *const f32, nmovers: u32, stale: *mut u8,
                           count: *mut u64, stream: *mut c_void) -> c_int;

@@ -145,7 +145,8 @@ typedef struct cc_instance {
  * (object_hierarchy, :198-253). Cones are walked into each object's space as
  * the reference's cone_to_object does (mask_cones.wgsl:623-638). The
  * transforms are stored as the reference's shader reads them: rows 0-2 of the
- * rotation with the translation in w, then (scale, 1 / scale, 0, 0). With ctx
+ * rotation with the translation in w, then (scale, 1 / scale, clear, 0)
+ * (clear 0: see cc_scene_set_clear). With ctx
  * NULL the scene stays on the host. */
 CC_API int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const uint32_t* geometry_counts,
                                     uint32_t ngeometries, const cc_instance* instances, uint32_t ninstances,
@@ -158,6 +159,18 @@ CC_API int cc_scene_build_instanced(cc_context* ctx, const float* tri9, const ui
  * (nullable) receives per mover its padded world bounds before and after
  * (lo.xyz, hi.xyz each): the input of cc_stale_cones. */
 CC_API int cc_scene_move(cc_scene* scene, const cc_instance* placements, uint32_t nplacements, float* boxes12);
+/* Each object's `clear` (Placement::clear, hierarchy.rs:266-270; one value per
+ * object, in build order): 0 opaque; in (0, 1) alpha-blended, its shadows
+ * keeping that share of the light (its triangles drawn with weight 1 - clear);
+ * below 0 transmissive, thin glass passing -clear of the light less Schlick's
+ * Fresnel reflectance at the cone's central direction; at most -2 a volume
+ * passing -2 - clear through two surfaces (add_mesh_coverage_if and
+ * cover_triangle, mask_cones.wgsl:600-614, :725-741). Stored in each
+ * transform's row 3 (its z) as the reference stores it, kept by
+ * cc_scene_move; prefiltered cones' coverage samples scale by the opacity of
+ * the first object placing each geometry (hierarchy.rs:469-503). Values of
+ * 1 and more, and non-finite ones, are refused. */
+CC_API int cc_scene_set_clear(cc_scene* scene, const float* clear, uint32_t nobjects);
 /* The cones that moved objects may have changed: cone (light l, point p) is
  * stale when a mover's box, old or new, meets the convex hull of p and the
  * light's box (hull_meets, mask_cones.wgsl:3903-3917, after the shadow-region

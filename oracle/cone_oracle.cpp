@@ -147,6 +147,7 @@ struct Scene {
   // hierarchy.rs:272-285); ranges[4 * m + 3] names object m's.
   std::vector<float> xforms;
   std::vector<uint32_t> object_geometry;  // instanced scenes: each object's geometry
+  std::vector<uint32_t> geometry_root;    // instanced scenes: each geometry's triangle-hierarchy root (NONE: none)
   std::vector<std::pair<F3, F3>> geometry_box;  // instanced scenes: each geometry's object-space box
   // The movers' subtree (MoverTree, hierarchy.rs:309-327): root node 2, other
   // nodes from first_node, items from first_item, in `movers` order.
@@ -212,6 +213,38 @@ static void build_coverage(Scene& sc) {
       }
     } else {
       for (uint32_t i = 0; i < COV; ++i) out[i] = sc.blas_cov[(size_t)x * COV + i] + sc.blas_cov[((size_t)x + 1) * COV + i];
+    }
+  }
+  // flatten_instanced (hierarchy.rs:469-503): a geometry's node samples
+  // (from its root up to the next geometry's root, in root order) scale by
+  // the opacity of the first object placing it, if that object is blended
+  // or transmissive.
+  if (!sc.geometry_root.empty()) {
+    std::vector<std::pair<uint32_t, uint32_t>> roots;
+    for (uint32_t g = 0; g < sc.geometry_root.size(); ++g)
+      if (sc.geometry_root[g] != NONE) roots.push_back({sc.geometry_root[g], g});
+    std::sort(roots.begin(), roots.end());
+    for (size_t k = 0; k < roots.size(); ++k) {
+      uint32_t first = NONE;
+      for (uint32_t m = 0; m < sc.object_geometry.size(); ++m)
+        if (sc.object_geometry[m] == roots[k].second) {
+          first = m;
+          break;
+        }
+      if (first == NONE) continue;
+      const float clear = sc.xforms[16 * (size_t)sc.ranges[4 * first + 3] + 14];
+      if (clear == 0.0f) continue;
+      float opacity;
+      if (clear > 0.0f) {
+        opacity = 1.0f - clear;
+      } else if (clear <= -2.0f) {
+        const float t = 0.96f * (-2.0f - clear);
+        opacity = 1.0f - t * t;
+      } else {
+        opacity = 1.0f - 0.96f * -clear;
+      }
+      const size_t end = k + 1 < roots.size() ? roots[k + 1].first : sc.blas.size();
+      for (size_t i = (size_t)roots[k].first * COV; i < end * COV; ++i) sc.blas_cov[i] *= opacity;
     }
   }
   if (!sc.xforms.empty()) {
@@ -417,6 +450,8 @@ static Scene* build_instanced(const float* tri9, const uint32_t* geometry_counts
   for (uint32_t g = 0; g < ngeometries; ++g) mesh_bounds(s->tris.data(), geometry[4 * g], geometry[4 * g + 1], local[g].first, local[g].second);
   s->ranges.clear();
   s->geometry_box = local;
+  s->geometry_root.assign(ngeometries, NONE);
+  for (uint32_t g = 0; g < ngeometries; ++g) s->geometry_root[g] = geometry[4 * g + 2];
   s->object_geometry.assign(ninstances, 0);
   std::vector<std::pair<F3, F3>> box(ninstances);
   for (uint32_t k = 0; k < ninstances; ++k) {
@@ -487,7 +522,7 @@ static void move_objects(Scene* s, const Instance* placements, float* boxes12) {
     const float* R = o.rotation;
     const float* t = o.translation;
     const float row[16] = {R[0], R[1], R[2], t[0], R[3], R[4], R[5], t[1], R[6], R[7], R[8], t[2],
-                           o.scale, 1.0f / o.scale, 0.0f, 0.0f};
+                           o.scale, 1.0f / o.scale, X[14], 0.0f};  // the object keeps its clear
     std::memcpy(X, row, sizeof(row));
     mb[i] = world_bounds(s->geometry_box[old.geometry], o);
     if (boxes12) {
@@ -772,7 +807,7 @@ template <class R> void draw_edge(Acc<R>& acc, V2<R> q0, V2<R> q1, R weight) {
 }
 
 // rasterize (:350-451)
-template <class R> bool rasterize(const Cone<R>& c, Acc<R>& acc, V3<R> v0, V3<R> v1, V3<R> v2) {
+template <class R> bool rasterize(const Cone<R>& c, Acc<R>& acc, V3<R> v0, V3<R> v1, V3<R> v2, R weight = R(1)) {
   Poly3<R> p;
   p.v[0] = v0;
   p.v[1] = v1;
@@ -838,7 +873,7 @@ template <class R> bool rasterize(const Cone<R>& c, Acc<R>& acc, V3<R> v0, V3<R>
     V2<R> a = q.v[i], b = q.v[(i + 1) % q.n];
     a = {clampv(a.x, R(0), g), clampv(a.y, R(0), g)};
     b = {clampv(b.x, R(0), g), clampv(b.y, R(0), g)};
-    draw_edge(acc, a, b, R(1));
+    draw_edge(acc, a, b, weight);
   }
   return true;
 }
@@ -857,7 +892,33 @@ struct Work {  // the reference's work counters (mask_cones.wgsl:655-665), per c
 };
 
 // cover_triangle (:594-616)
-template <class R> bool cover_triangle(const Scene& s, const Cone<R>& c, Acc<R>& acc, uint32_t t, Work& wk) {
+// The placed object a mesh's triangles belong to: its triangles' weight and
+// its transmission, from its transform's `clear` (row 3's z;
+// add_mesh_coverage_if, :725-741). World-space meshes: weight 1.
+template <class R> struct ObjectLight {
+  R weight = R(1);
+  R transmit = R(0);
+  bool volume = false;
+};
+template <class R> ObjectLight<R> object_light(const Scene& s, uint32_t x) {
+  ObjectLight<R> o;
+  if (x == NONE || s.xforms.empty()) return o;
+  const R clear = R(s.xforms[16 * (size_t)x + 14]);
+  o.weight = R(1) - std::max(clear, R(0));
+  o.transmit = std::max(-clear, R(0));
+  if (clear <= R(-2)) {  // a volume: two surfaces
+    o.transmit = R(-2) - clear;
+    o.volume = true;
+  }
+  return o;
+}
+
+// cover_triangle (:594-616): the culls, then the triangle drawn with its
+// object's weight, or for a transmissive object one less what passes through
+// it at the cone's central direction (Schlick's Fresnel, F0 0.04; twice for
+// a volume; the fifth power by multiplications).
+template <class R> bool cover_triangle(const Scene& s, const Cone<R>& c, Acc<R>& acc, uint32_t t, Work& wk,
+                                       const ObjectLight<R>& ol = ObjectLight<R>{}) {
   wk.tris++;
   if (t == wk.skip) return false;
   V3<R> v0 = tri_vertex<R>(s, t, 0), v1 = tri_vertex<R>(s, t, 1), v2 = tri_vertex<R>(s, t, 2);
@@ -867,7 +928,17 @@ template <class R> bool cover_triangle(const Scene& s, const Cone<R>& c, Acc<R>&
       dot(n, direction(c, R(0), R(1))) >= 0 && dot(n, direction(c, R(1), R(1))) >= 0)
     return false;
   if (!may_touch(c, v0, v1, v2)) return false;
-  return rasterize(c, acc, v0, v1, v2);
+  R weight = ol.weight;
+  if (ol.transmit > R(0)) {
+    const R cos_t = std::fabs(dot(normalize(n), normalize(direction(c, R(0.5), R(0.5)))));
+    const R x = R(1) - cos_t;
+    const R x2 = x * x;
+    const R f = R(0.04) + R(0.96) * (x2 * x2 * x);
+    R passes = ol.transmit * (R(1) - f);
+    if (ol.volume) passes *= R(1) - f;
+    weight = R(1) - passes;
+  }
+  return rasterize(c, acc, v0, v1, v2, weight);
 }
 
 // --- Prefiltered cones (:453-574, :1090-1150) ---
@@ -1074,6 +1145,7 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
   bool touched = false;
   const uint32_t* range = s.ranges.data() + 4 * m;
   const Cone<R> c = range[3] != NONE ? cone_to_object(s, world, range[3]) : world;
+  const ObjectLight<R> ol = object_light<R>(s, range[3]);
   if (hierarchy == 2) {
     if (range[2] != NONE) {
       uint32_t stack[STACK];
@@ -1092,7 +1164,7 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
         if (node.info[1] > 0) {
           wk.cone_work += node.info[1];
           for (uint32_t k = node.info[0]; k < node.info[0] + node.info[1]; ++k)
-            if (cover_triangle(s, c, acc, s.blas_items[k], wk.work)) touched = true;
+            if (cover_triangle(s, c, acc, s.blas_items[k], wk.work, ol)) touched = true;
         } else {
           if (sp + 2 > STACK) {
             wk.work.flags |= 2;
@@ -1105,7 +1177,7 @@ template <class R> void add_mesh_coverage(const Scene& s, const Cone<R>& world, 
     }
   } else {
     for (uint32_t t = range[0]; t < range[0] + range[1]; ++t)
-      if (cover_triangle(s, c, acc, t, wk.work)) touched = true;
+      if (cover_triangle(s, c, acc, t, wk.work, ol)) touched = true;
   }
   if (touched) {
     Running<R> running;
@@ -2171,6 +2243,14 @@ void* oracle_scene_create_instanced(const float* tri9, const uint32_t* geometry_
                                     uint32_t nmovable) {
   return build_instanced(tri9, geometry_counts, ngeometries, static_cast<const Instance*>(instances), ninstances,
                          movable, nmovable);
+}
+
+// Each object's clear (Placement::clear), in its transform's row 3 z; the
+// prefiltered samples are rebuilt on their next use.
+void oracle_scene_set_clear(void* sp, const float* clear, uint32_t n) {
+  Scene* s = static_cast<Scene*>(sp);
+  for (uint32_t m = 0; m < n && m < s->object_geometry.size(); ++m) s->xforms[16 * (size_t)s->ranges[4 * m + 3] + 14] = clear[m];
+  s->coverage_built = false;
 }
 
 void oracle_scene_move(void* sp, const void* placements, float* boxes12) {

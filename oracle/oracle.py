@@ -60,6 +60,7 @@ def load():
         lib.oracle_scene_create_instanced.restype = P
         lib.oracle_scene_create_instanced.argtypes = [P, P, U32, P, U32, P, U32]
         lib.oracle_scene_move.argtypes = [P, P, P]
+        lib.oracle_scene_set_clear.argtypes = [P, P, C.c_uint32]
         lib.oracle_stale_cones.argtypes = [P, P, U64, P, U32, P, U32, P, I]
         lib.oracle_scene_transforms.restype = U64
         lib.oracle_scene_transforms.argtypes = [P, P]
@@ -101,6 +102,12 @@ class OracleScene:
             _p(self.tri9), _p(self.counts), len(self.counts), _p(self.instances), len(self.instances),
             _p(self.movable), 0 if self.movable is None else len(self.movable)))
         return self
+
+    def set_clear(self, clear) -> None:
+        """Each object's clear (Placement::clear, hierarchy.rs:266-270): 0 opaque,
+        (0, 1) alpha-blended, below 0 transmissive (at most -2 a volume)."""
+        c = np.ascontiguousarray(clear, np.float32)
+        load().oracle_scene_set_clear(self._h, _p(c), len(c))
 
     def move(self, placements: np.ndarray) -> np.ndarray:
         """Places the movers anew (in their order); per mover its bounds before and after."""

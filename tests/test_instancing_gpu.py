@@ -127,3 +127,52 @@ def test_update_in_small_chunks_equals_the_default(kernel, world):
     finally:
         kernel.set_split_chunk(1 << 25)
         scene.close()
+
+
+def clear_values(world):
+    """Some boulders alpha-blended (clear 0.5), some thin glass (-0.7), some
+    solid glass volumes (-2.5); the ground stays opaque."""
+    clear = np.zeros(len(world.instances), np.float32)
+    clear[0:-1:7] = 0.5
+    clear[3:-1:11] = -0.7
+    clear[5:-1:13] = -2.5
+    return clear
+
+
+def test_blended_and_transmissive_objects_match_the_oracle(kernel, world):
+    """Placed objects' `clear` (Placement::clear; add_mesh_coverage_if and
+    cover_triangle, mask_cones.wgsl:600-614, :725-741): blended objects'
+    triangles drawn with 1 - clear, transmissive ones with one less the
+    Fresnel-weighted share passing through, against the oracle at the parity
+    bar; their shadows let light through where opaque ones would not."""
+    clear = clear_values(world)
+    scene = kernel.scene_instanced(world.geometries, world.instances)
+    opaque = parity.flat(kernel.visibility(scene, world.receivers, world.lights, outputs=ALL))
+    scene.set_clear(clear)
+    g = parity.flat(kernel.visibility(scene, world.receivers, world.lights, outputs=ALL))
+    scene.close()
+    orc = OracleScene.instanced(world.geometries, world.instances)
+    orc.set_clear(clear)
+    o = orc.visibility(world.receivers, world.lights)
+    orc.close()
+    parity.compare(g, o, o["unshadowed"])
+    lit = g["fraction"] > opaque["fraction"] + 1e-3
+    assert lit.sum() > 50
+    assert np.all(g["fraction"] >= opaque["fraction"] - 1e-6)
+
+
+def test_prefiltered_cones_through_blended_objects_match_the_oracle(kernel, world):
+    clear = clear_values(world)
+    scene = kernel.scene_instanced(world.geometries, world.instances)
+    scene.set_clear(clear)
+    kernel.prefilter = 2.0
+    try:
+        g = parity.flat(kernel.visibility(scene, world.receivers, world.lights, outputs=ALL))
+    finally:
+        kernel.prefilter = 0.0
+        scene.close()
+    orc = OracleScene.instanced(world.geometries, world.instances)
+    orc.set_clear(clear)
+    o = orc.visibility(world.receivers, world.lights, prefilter=2.0)
+    orc.close()
+    parity.compare(g, o, o["unshadowed"])
