@@ -636,6 +636,14 @@ int cc_host::visibility_impl(cc_context* ctx, const cc_scene* scene, const float
             "walk order");
     q.order = static_cast<const uint32_t*>(ctx->order.ptr);
   }
+  // Lights with wider cones first (the split path; results do not depend on
+  // the order).
+  if (!(opt.flags & CC_KEEP_ORDER) && !cones && q.records && nlights >= 2 && nlights <= cc::kMaxOrderedLights &&
+      npoints > 0) {
+    CC_CUDA(ctx->light_order.reserve(nlights * sizeof(uint32_t)), "light order");
+    CC_CUDA(cc::launch_light_order(q, static_cast<uint32_t*>(ctx->light_order.ptr), stream), "light order");
+    q.light_order = static_cast<const uint32_t*>(ctx->light_order.ptr);
+  }
   // The call's slot in the timing ring (the oldest unread call is dropped
   // when the ring is full).
   const int ring = cc_context::kTimingRing;

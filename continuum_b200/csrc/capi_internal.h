@@ -65,6 +65,7 @@ struct cc_context {
   DevBuf sky_sum;   // sky irradiance per receiver before its download
   DevBuf redo;      // redo list
   DevBuf order;     // walk order of the points
+  DevBuf light_order;  // the split path's light order
   DevBuf sort_scratch;
   // Moving frames' scratch, kept between frames: the movers' transforms, the
   // stale-cone tables, and the update's cone order, flags, list and count.

@@ -57,6 +57,11 @@ struct DevQuery {
   uint32_t back = 0;
   uint32_t ntris = 0;
   const uint32_t* tri_slot = nullptr;
+  // The split path's light order (null: the given order): slots of light
+  // rank r walk light light_order[r]'s cones. Results do not depend on it;
+  // lights whose cones are wider go first, so their costlier packets do not
+  // start last (light_order_kernel).
+  const uint32_t* light_order = nullptr;
 };
 
 // A light cone set up before its walk (the split plain path): frame, window,
@@ -218,6 +223,10 @@ cudaError_t launch_splat_pass(bool wide, bool count, bool inst, bool sky, const 
 // their masks (o.cov_out) integrated into o.irradiance and o.fraction.
 cudaError_t upload_disk_table_split(const float* table64);
 cudaError_t launch_cone_setup(const DevQuery& q, uint64_t base, uint64_t n, ConeRecord* records, cudaStream_t stream);
+// The query's lights in decreasing order of the mean window of their cones
+// over a sample of the points (at most 1024 lights), into `out`.
+constexpr uint32_t kMaxOrderedLights = 1024;
+cudaError_t launch_light_order(const DevQuery& q, uint32_t* out, cudaStream_t stream);
 cudaError_t launch_integrate(const DevQuery& q, const DevOut& o, uint64_t base, uint64_t n, const ConeRecord* records,
                              cudaStream_t stream);
 // Batched: the batch cones of chunk b (b.cone_base .. + b.cone_count).

@@ -16,12 +16,10 @@ __device__ __forceinline__ bool slot_cone(const DevQuery& q, uint64_t slot, uint
     return true;
   }
   if (slot >= q.npoints * (uint64_t)q.nlights) return false;
-  if (q.order) {
-    const uint64_t light_base = (slot / q.npoints) * q.npoints;
-    *c = light_base + __ldg(&q.order[slot - light_base]);
-  } else {
-    *c = slot;
-  }
+  const uint64_t rank = slot / q.npoints;
+  const uint64_t i = slot - rank * q.npoints;
+  const uint64_t light = q.light_order ? (uint64_t)__ldg(&q.light_order[rank]) : rank;
+  *c = light * q.npoints + (q.order ? (uint64_t)__ldg(&q.order[i]) : i);
   return true;
 }
 
@@ -193,6 +191,52 @@ __global__ void __launch_bounds__(64) integrate_kernel(DevQuery q, DevOut o, Bat
 
 cudaError_t upload_disk_table_split(const float* table64) {
   return cudaMemcpyToSymbol(c_disk, table64, kBins * sizeof(float));
+}
+
+// One block: per light, the windows of its traced cones summed over the same
+// sample of points (at most 1024, evenly strided), then the lights ranked
+// by that sum, largest first (ties by index). Packet costs follow the
+// cone's window (a wider cone meets more of the scene), and the packets of
+// the light walked last end the pass.
+__global__ void __launch_bounds__(256) light_order_kernel(DevQuery q, uint32_t* __restrict__ out) {
+  __shared__ float sum[kMaxOrderedLights];
+  __shared__ float part[8];
+  const uint32_t L = q.nlights;
+  const uint64_t samples = q.npoints < 1024 ? q.npoints : 1024;
+  const uint64_t stride = samples ? q.npoints / samples : 1;
+  for (uint32_t l = 0; l < L; ++l) {
+    const DevLight light = load_light(q.lights, l);
+    float acc = 0.0f;
+    for (uint64_t k = threadIdx.x; k < samples; k += blockDim.x) {
+      const uint64_t p = k * stride;
+      const f3 point = xyz(__ldg(&q.receivers[2 * p + 0]));
+      const f3 normal = xyz(__ldg(&q.receivers[2 * p + 1]));
+      if (!(spot_falloff(light, normalize(point - light_center(light))) > 0.0f) || !faces_light(light, point, normal))
+        continue;
+      Cone cone{};
+      if (light_cone(point, light, q.wide_extent, cone).ok) acc += (cone.u1 - cone.u0) * (cone.v1 - cone.v0);
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float total = 0.0f;
+      for (int w = 0; w < 8; ++w) total += part[w];
+      sum[l] = total;
+    }
+    __syncthreads();
+  }
+  for (uint32_t l = threadIdx.x; l < L; l += blockDim.x) {
+    uint32_t rank = 0;
+    for (uint32_t k = 0; k < L; ++k) rank += (sum[k] > sum[l] || (sum[k] == sum[l] && k < l)) ? 1u : 0u;
+    out[rank] = l;
+  }
+}
+
+cudaError_t launch_light_order(const DevQuery& q, uint32_t* out, cudaStream_t stream) {
+  if (q.nlights == 0 || q.nlights > kMaxOrderedLights) return cudaErrorInvalidValue;
+  light_order_kernel<<<1, 256, 0, stream>>>(q, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_cone_setup(const DevQuery& q, uint64_t base, uint64_t n, ConeRecord* records, cudaStream_t stream) {
