@@ -24,12 +24,20 @@ struct cc_batch {
   };
   std::vector<Update> updates;
   DevBuf upd_perm, upd_flags, upd_list, upd_count, upd_temp;
+  // Prefiltering jobs (cc_options.prefilter > 0): a table of their own,
+  // walked by the prefiltering kernel (which integrates in the walk) in a
+  // second launch after the exact jobs' split path, with its own walk order,
+  // re-walk list and counters (words 4-7).
+  std::vector<cc::JobGpu> splat_jobs;
+  bool splat_instanced = false;
+  uint64_t splat_points = 0, splat_cones = 0, splat_packets = 0;
+  DevBuf splat_table, splat_redo, splat_order, splat_sort_scratch;
   uint64_t points = 0, cones = 0;
   // Device state, sized by prepare().
   DevBuf job_table, redo, order, sort_scratch, counters;
   DevBuf records, masks;               // the split path's scratch, one chunk
   std::vector<cc::BatchChunk> chunks;  // the split path's chunks, set by prepare()
-  uint32_t* status = nullptr;    // pinned: the counters copied back after each submission
+  uint32_t* status = nullptr;    // pinned: the counters (both launches') copied back after each submission
   cudaEvent_t done = nullptr;
   bool prepared = false;
   uint32_t prepared_pw = 0;
@@ -105,10 +113,31 @@ int prepare(cc_batch* b, uint32_t pw) {
   CC_CUDA(b->redo.reserve(std::max<uint64_t>(cone, 1) * 4), "batch redo list");
   CC_CUDA(b->order.reserve(std::max<uint64_t>(point, 1) * 4), "batch walk order");
   CC_CUDA(b->sort_scratch.reserve(cc::batch_order_scratch_bytes(std::max<uint64_t>(point, 1))), "batch sort scratch");
-  CC_CUDA(b->counters.reserve(cc::kCounterWords * sizeof(uint32_t)), "batch counters");
+  CC_CUDA(b->counters.reserve(2 * cc::kCounterWords * sizeof(uint32_t)), "batch counters");
   if (!b->jobs.empty())
     CC_CUDA(cudaMemcpy(b->job_table.ptr, b->jobs.data(), b->jobs.size() * sizeof(cc::JobGpu), cudaMemcpyHostToDevice),
             "batch job table upload");
+  if (!b->splat_jobs.empty()) {
+    uint64_t sp = 0, sc = 0, spt = 0;
+    for (cc::JobGpu& j : b->splat_jobs) {
+      const uint64_t c = j.query.npoints * (uint64_t)j.query.nlights;
+      j.packet_start = sp;
+      j.cone_start = sc;
+      j.point_start = spt;
+      sp += (c + pw - 1) / pw;
+      sc += c;
+      spt += j.query.npoints;
+    }
+    b->splat_packets = sp;
+    CC_CUDA(b->splat_table.reserve(b->splat_jobs.size() * sizeof(cc::JobGpu)), "batch prefiltering job table");
+    CC_CUDA(b->splat_redo.reserve(std::max<uint64_t>(sc, 1) * 4), "batch prefiltering redo list");
+    CC_CUDA(b->splat_order.reserve(std::max<uint64_t>(spt, 1) * 4), "batch prefiltering walk order");
+    CC_CUDA(b->splat_sort_scratch.reserve(cc::batch_order_scratch_bytes(std::max<uint64_t>(spt, 1))),
+            "batch prefiltering sort scratch");
+    CC_CUDA(cudaMemcpy(b->splat_table.ptr, b->splat_jobs.data(), b->splat_jobs.size() * sizeof(cc::JobGpu),
+                       cudaMemcpyHostToDevice),
+            "batch prefiltering job table upload");
+  }
   b->prepared = true;
   b->prepared_pw = pw;
   b->prepared_chunk = b->ctx->split_chunk;
@@ -119,7 +148,7 @@ int prepare(cc_batch* b, uint32_t pw) {
 // and solo passes, and the counters' copy to pinned host memory.
 int enqueue(cc_batch* b, const cc_batch_options& opt, cudaStream_t stream) {
   uint32_t* counters = static_cast<uint32_t*>(b->counters.ptr);
-  CC_CUDA(cudaMemsetAsync(counters, 0, cc::kCounterWords * sizeof(uint32_t), stream), "batch counter reset");
+  CC_CUDA(cudaMemsetAsync(counters, 0, 2 * cc::kCounterWords * sizeof(uint32_t), stream), "batch counter reset");
   cc::BatchLaunch L{};
   L.jobs = static_cast<const cc::JobGpu*>(b->job_table.ptr);
   L.njobs = (uint32_t)b->jobs.size();
@@ -157,10 +186,39 @@ int enqueue(cc_batch* b, const cc_batch_options& opt, cudaStream_t stream) {
     o.redo_capacity = (uint32_t)std::max<uint64_t>(b->cones, 1);
   }
   o.cov_out = static_cast<float*>(b->masks.ptr);
-  CC_CUDA(cc::launch_batch(L, o, b->chunks.data(), b->chunks.size(), b->count_work, b->ctx->sm_count,
-                           (int)opt.blocks_per_sm, stream),
-          "batch launch");
-  CC_CUDA(cudaMemcpyAsync(b->status, counters, cc::kCounterWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
+  if (!b->jobs.empty())
+    CC_CUDA(cc::launch_batch(L, o, b->chunks.data(), b->chunks.size(), b->count_work, b->ctx->sm_count,
+                             (int)opt.blocks_per_sm, stream),
+            "batch launch");
+  if (!b->splat_jobs.empty()) {
+    cc::BatchLaunch S{};
+    S.jobs = static_cast<const cc::JobGpu*>(b->splat_table.ptr);
+    S.njobs = (uint32_t)b->splat_jobs.size();
+    S.packets = b->splat_packets;
+    S.points = b->splat_points;
+    S.pw = opt.points_per_warp;
+    S.inst = b->splat_instanced ? 1u : 0u;
+    if (!(opt.flags & CC_KEEP_ORDER) && b->splat_points > 0) {
+      CC_CUDA(cc::batch_order(S, b->splat_sort_scratch.ptr, b->splat_sort_scratch.size,
+                              static_cast<uint32_t*>(b->splat_order.ptr), stream),
+              "batch prefiltering walk order");
+      S.order = static_cast<const uint32_t*>(b->splat_order.ptr);
+    }
+    cc::DevOut so{};
+    uint32_t* sc = counters + cc::kCounterWords;
+    so.redo_count = sc;
+    so.error = sc + 1;
+    so.next_packet = sc + 2;
+    so.next_solo = sc + 3;
+    if (!(opt.flags & CC_NO_REDO)) {
+      so.redo_list = static_cast<uint32_t*>(b->splat_redo.ptr);
+      so.redo_capacity = (uint32_t)std::max<uint64_t>(b->splat_cones, 1);
+    }
+    CC_CUDA(cc::launch_batch_splat(S, so, b->count_work, b->ctx->sm_count, (int)opt.blocks_per_sm, stream),
+            "batch prefiltering launch");
+  }
+  CC_CUDA(cudaMemcpyAsync(b->status, counters, 2 * cc::kCounterWords * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                          stream),
           "batch status copy");
   return CC_OK;
 }
@@ -213,8 +271,9 @@ int wait_done(cc_batch* b, uint32_t timeout_ms) {
     if (std::chrono::steady_clock::now() >= until) return fail(CC_ERR_TIMEOUT, "the batch has not finished");
     std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
-  if (b->status[1] & 2u) return fail(CC_ERR_STACK, "a traversal stack overflowed");
-  if (b->status[1] & 1u) return fail(CC_ERR_INVALID, "solo re-walk list overflowed");
+  const uint32_t error = b->status[1] | b->status[cc::kCounterWords + 1];
+  if (error & 2u) return fail(CC_ERR_STACK, "a traversal stack overflowed");
+  if (error & 1u) return fail(CC_ERR_INVALID, "solo re-walk list overflowed");
   return CC_OK;
 }
 
@@ -234,14 +293,14 @@ int cc_batch_create(cc_context* ctx, cc_batch** out) {
   if (rc) return rc;
   cc_batch* b = new cc_batch;
   b->ctx = ctx;
-  cudaError_t e = cudaMallocHost(&b->status, cc::kCounterWords * sizeof(uint32_t));
+  cudaError_t e = cudaMallocHost(&b->status, 2 * cc::kCounterWords * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     rc = cuda_fail(e, "batch setup");
     cc_batch_destroy(b);
     return rc;
   }
-  std::fill(b->status, b->status + cc::kCounterWords, 0u);
+  std::fill(b->status, b->status + 2 * cc::kCounterWords, 0u);
   *out = b;
   return CC_OK;
 }
@@ -268,6 +327,9 @@ int cc_batch_clear(cc_batch* b) {
   b->jobs.clear();
   b->updates.clear();
   b->instanced = false;
+  b->splat_jobs.clear();
+  b->splat_instanced = false;
+  b->splat_points = b->splat_cones = b->splat_packets = 0;
   b->count_work = false;
   b->points = b->cones = 0;
   b->prepared = false;
@@ -287,10 +349,14 @@ int add_job(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t
   cc_options opt;
   if (opt_in) opt = *opt_in; else cc_options_default(&opt);
   if (opt.hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
-  if (opt.prefilter != 0.0f) return fail(CC_ERR_INVALID, "batched jobs take exact cones only (prefilter 0)");
+  if (!(opt.prefilter >= 0.0f)) return fail(CC_ERR_INVALID, "prefilter must be >= 0");
+  const bool splat = opt.prefilter > 0.0f;
+  if (splat && opt.hierarchy != 2) return fail(CC_ERR_INVALID, "prefiltered cones need hierarchy 2");
+  if (splat && stale) return fail(CC_ERR_INVALID, "update jobs take exact cones (prefilter 0)");
   if (npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one job");
   const uint64_t cones = npoints * (uint64_t)nlights;
-  if (b->cones + cones >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one batch");
+  if (b->cones + b->splat_cones + cones >= 0xffffffffull)
+    return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one batch");
   if (b->jobs.size() >= 0xfffffffeull) return fail(CC_ERR_INVALID, "too many jobs");
   auto misaligned = [](const void* p, uintptr_t a) { return p && (reinterpret_cast<uintptr_t>(p) % a) != 0; };
   if (misaligned(receivers, 16) || misaligned(lights, 16) || misaligned(out->partial, 16) ||
@@ -302,8 +368,17 @@ int add_job(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t
     if (rc) return rc;
     CC_CUDA(cudaEventSynchronize(b->done), "batch");
   }
+  if (splat) {
+    // The scene's coverage samples on the device (as a prefiltered
+    // cc_visibility call makes them).
+    int rc = set_device(b->ctx);
+    if (rc) return rc;
+    if ((rc = cc_host::scene_coverage(const_cast<cc_scene*>(scene)))) return rc;
+  }
   cc::JobGpu j{};
   j.scene = scene->dev();
+  if (splat && (opt.flags & CC_NO_OBJECT_PREFILTER)) j.scene.obj_cov = nullptr;
+  j.query.prefilter = opt.prefilter;
   j.query.receivers = reinterpret_cast<const float4*>(receivers);
   j.query.lights = reinterpret_cast<const float4*>(lights);
   j.query.npoints = npoints;
@@ -325,14 +400,22 @@ int add_job(cc_batch* b, const cc_scene* scene, const float* receivers, uint64_t
       j.hi[k] = scene->flat.nodes[0].hi[k];
     }
   }
-  if (job) *job = (uint32_t)b->jobs.size();
+  if (job) *job = (uint32_t)(b->jobs.size() + b->splat_jobs.size());
+  b->count_work = b->count_work || out->work != nullptr;
+  b->prepared = false;
+  if (splat) {
+    b->splat_jobs.push_back(j);
+    b->splat_instanced = b->splat_instanced || scene->xforms != nullptr;
+    b->splat_points += npoints;
+    b->splat_cones += cones;
+    drop_graph(b);
+    return CC_OK;
+  }
   if (stale) b->updates.push_back({(uint32_t)b->jobs.size(), stale});
   b->jobs.push_back(j);
   b->instanced = b->instanced || scene->xforms != nullptr;
-  b->count_work = b->count_work || out->work != nullptr;
   b->points += npoints;
   b->cones += cones;
-  b->prepared = false;
   drop_graph(b);
   return CC_OK;
 }
@@ -426,9 +509,11 @@ int cc_batch_tune(cc_batch* b, const cc_batch_options* base, uint32_t reps, cc_b
 
 int cc_batch_sizes(const cc_batch* b, uint64_t out4[4]) {
   if (!b || !out4) return fail(CC_ERR_INVALID, "null argument");
-  out4[0] = b->jobs.size();
-  out4[1] = b->points;
-  out4[2] = b->cones;
-  out4[3] = b->job_table.size + b->redo.size + b->order.size + b->sort_scratch.size + b->counters.size;
+  out4[0] = b->jobs.size() + b->splat_jobs.size();
+  out4[1] = b->points + b->splat_points;
+  out4[2] = b->cones + b->splat_cones;
+  out4[3] = b->job_table.size + b->redo.size + b->order.size + b->sort_scratch.size + b->counters.size +
+            b->records.size + b->masks.size + b->splat_table.size + b->splat_redo.size + b->splat_order.size +
+            b->splat_sort_scratch.size;
   return CC_OK;
 }

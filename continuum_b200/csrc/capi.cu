@@ -234,6 +234,8 @@ int threads_for_build() {
 
 }  // namespace
 
+int cc_host::scene_coverage(cc_scene* s) { return ensure_coverage(s); }
+
 extern "C" {
 
 const char* cc_last_error(void) { return g_error.c_str(); }

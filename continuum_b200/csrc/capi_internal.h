@@ -53,6 +53,10 @@ int visibility_impl(cc_context* ctx, const cc_scene* scene, const float* receive
                     const float* lights, uint32_t nlights, const cc_options* opt, const cc_outputs* out,
                     void* stream, uint32_t sky, const uint32_t* cones, const uint32_t* cones_count);
 
+// The scene's prefiltered coverage samples on the device (built and uploaded
+// on first use; capi.cu). The scene's device is current.
+int scene_coverage(cc_scene* s);
+
 }  // namespace cc_host
 
 struct cc_context {

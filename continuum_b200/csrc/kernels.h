@@ -189,6 +189,11 @@ cudaError_t batch_order(const BatchLaunch& b, void* scratch, size_t scratch_byte
 // chunk's) integrated into each job's irradiance and fraction.
 // o.redo_count, o.error and the two packet counters must be zero on entry.
 // blocks_per_sm: resident blocks per SM to launch (1..kBlocksPerSm).
+// A batch's prefiltering jobs (visibility_splat.cu): one persistent launch of
+// the prefiltering kernel over their packets (walk and integration), then
+// their listed cones alone.
+cudaError_t launch_batch_splat(const BatchLaunch& b, const DevOut& o, bool count, int sm_count, int blocks_per_sm,
+                               cudaStream_t stream);
 cudaError_t launch_batch(const BatchLaunch& b, const DevOut& o, const BatchChunk* chunks, size_t nchunks,
                          bool count_work, int sm_count, int blocks_per_sm, cudaStream_t stream);
 

@@ -1008,9 +1008,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
     uint64_t listed = 0;
     if (list) listed = list[packet];
     if constexpr (kBatch) {
-      // The packet's job; a listed slot's is in its record.
+      // The packet's job; a listed slot's is in its record (split path), or
+      // found from its batch cone number (the prefiltering kernel keeps no
+      // records).
       const uint64_t packet_abs = batch.packet_base + packet;
-      const uint32_t j = list ? records[listed].g.w : find_job(batch.jobs, batch.njobs, packet_abs, false);
+      uint32_t j;
+      if (list) j = kSplit ? records[listed].g.w : find_job(batch.jobs, batch.njobs, listed, true);
+      else j = find_job(batch.jobs, batch.njobs, packet_abs, false);
       const JobGpu* J = batch.jobs + j;
       s = J->scene;
       q = J->query;

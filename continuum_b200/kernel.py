@@ -554,9 +554,13 @@ class Batch:
         return self._h
 
     def add(self, scene: Scene, d_receivers: int, npoints: int, d_lights: int, nlights: int, outputs: dict,
-            hierarchy=Hierarchy.TRIANGLES) -> int:
+            hierarchy=Hierarchy.TRIANGLES, prefilter: Optional[float] = None) -> int:
+        """A job (cc_batch_add); prefilter (bins; None: the kernel's setting)
+        makes it a prefiltering job."""
         o = _lib.Outputs(*(outputs.get(k) for k in ("full", "any", "partial", "irradiance", "fraction", "work")))
         opt = self.kernel.options(hierarchy)
+        if prefilter is not None:
+            opt.prefilter = float(prefilter)
         job = C.c_uint32()
         check(load().cc_batch_add(self.handle, scene.handle, C.c_void_p(d_receivers), int(npoints),
                                   C.c_void_p(d_lights), int(nlights), C.byref(opt), C.byref(o), C.byref(job)))

@@ -156,3 +156,52 @@ def test_served_requests_on_an_instanced_scene_equal_the_plain_call(kernel, worl
     srv.close()
     inst.close()
     flat.close()
+
+
+def test_prefiltered_jobs_share_a_batch_with_exact_ones(kernel, world):
+    """Prefiltering jobs (prefilter 1 and 2 bins; instanced with and without
+    object splats, and world-space) run in the batch's second launch beside
+    an exact job: each equals its prefiltered cc_visibility call alone, on the
+    first submission and on graph replays."""
+    import torch
+
+    inst = kernel.scene_instanced(world.geometries, world.instances)
+    ico = scenes.icosphere_field(seed=8, n_spheres=6, subdivisions=3, width=64, height=36)
+    flat = kernel.scene(ico.meshes)
+    specs = [(inst, world.receivers, world.lights, 2.0, True), (flat, ico.receivers, ico.lights, 0.0, True),
+             (flat, ico.receivers[::3], ico.lights[:2], 1.0, True), (inst, world.receivers[::4], world.lights[1:], 2.0, False)]
+    jobs = []
+    for scene, rec, lig, pf, obj in specs:
+        r = torch.from_numpy(np.ascontiguousarray(rec)).cuda()
+        l = torch.from_numpy(np.ascontiguousarray(lig)).cuda()
+        jobs.append((scene, r, l, pf, obj, outputs(torch, r.shape[0] * l.shape[0], with_all=True)))
+    alone = []
+    for scene, r, l, pf, obj, outs in jobs:
+        ref = {k: torch.zeros_like(v) for k, v in outs.items()}
+        kernel.prefilter, kernel.object_prefilter = pf, obj
+        try:
+            kernel.visibility_device(scene, r.data_ptr(), r.shape[0], l.data_ptr(), l.shape[0], ptrs(ref))
+        finally:
+            kernel.prefilter, kernel.object_prefilter = 0.0, True
+        alone.append(ref)
+    torch.cuda.synchronize()
+    b = Batch(kernel)
+    for scene, r, l, pf, obj, outs in jobs:
+        kernel.object_prefilter = obj
+        try:
+            b.add(scene, r.data_ptr(), r.shape[0], l.data_ptr(), l.shape[0], ptrs(outs), prefilter=pf)
+        finally:
+            kernel.object_prefilter = True
+    assert b.sizes()["jobs"] == 4
+    for submission in range(3):
+        for *_, outs in jobs:
+            for v in outs.values():
+                v.zero_()
+        torch.cuda.synchronize()
+        b.submit()
+        b.wait()
+        for (*_, outs), ref in zip(jobs, alone):
+            same(outs, ref, KEYS + ("partial",))
+    b.close()
+    inst.close()
+    flat.close()
