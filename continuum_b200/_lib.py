@@ -116,7 +116,8 @@ class CacheStats(C.Structure):
 class Request(C.Structure):
     _fields_ = [("scene", C.c_uint32), ("receivers", C.c_void_p), ("npoints", C.c_uint64), ("lights", C.c_void_p),
                 ("nlights", C.c_uint32), ("hierarchy", C.c_uint32), ("cache_key", C.c_uint64),
-                ("full", C.c_void_p), ("any", C.c_void_p), ("irradiance", C.c_void_p), ("fraction", C.c_void_p)]
+                ("full", C.c_void_p), ("any", C.c_void_p), ("irradiance", C.c_void_p), ("fraction", C.c_void_p),
+                ("prefilter", C.c_float)]
 
 
 class RequestStats(C.Structure):

@@ -42,6 +42,7 @@ struct CacheEntry {
   float geometry[12] = {};  // the light record without its radiance
   uint64_t npoints = 0;
   uint32_t scene = 0, hierarchy = 0;
+  float prefilter = 0.0f;
   uint8_t* dev = nullptr;   // npoints x (full | any | irradiance | fraction)
   uint64_t bytes = 0;
   int refs = 0;             // launches in flight reading it
@@ -133,7 +134,7 @@ CacheEntry* find_entry(cc_server* s, const cc_request& r, const float* light) {
   for (auto it = range.first; it != range.second; ++it) {
     CacheEntry* e = it->second.get();
     if (e->npoints == r.npoints && e->scene == r.scene && e->hierarchy == r.hierarchy &&
-        std::memcmp(e->geometry, light, sizeof(e->geometry)) == 0)
+        e->prefilter == r.prefilter && std::memcmp(e->geometry, light, sizeof(e->geometry)) == 0)
       return e;
   }
   return nullptr;
@@ -191,7 +192,7 @@ void release_slot(cc_server* s, Slot& slot) {
 // Retires a finished launch: traced results become cache entries (or are
 // freed), inputs and scratch are freed, and its requests complete. (s->mu held.)
 void retire(cc_server* s, Slot& slot) {
-  const bool stack = (slot.status[1] & 2u) != 0;
+  const bool stack = ((slot.status[1] | slot.status[cc::kCounterWords + 1]) & 2u) != 0;
   for (Request* r : slot.reqs) {
     for (size_t l = 0; l < r->result.size(); ++l) {
       if (r->hit[l]) r->hit[l]->refs--;
@@ -206,6 +207,7 @@ void retire(cc_server* s, Slot& slot) {
         e->npoints = r->req.npoints;
         e->scene = r->req.scene;
         e->hierarchy = r->req.hierarchy;
+        e->prefilter = r->req.prefilter;
         e->dev = block;
         e->bytes = bytes;
         e->lru = s->lru.insert(s->lru.end(), e.get());
@@ -255,11 +257,115 @@ void abandon(cc_server* s, Slot& slot, int status, const std::string& error) {
 // Builds and enqueues one launch on `slot` from the requests admitted to it
 // (their memory already counted in in_use). Called without s->mu: the
 // requests and the slot belong to the loop thread until the launch retires.
+// A launch's jobs of one kind with their starts (packets, cones, points).
+struct JobGroup {
+  std::vector<cc::JobGpu> jobs;
+  std::vector<uint64_t> cones_of;
+  uint64_t points = 0, cones = 0, packets = 0;
+  void add(cc::JobGpu j, uint64_t P, uint32_t pw) {
+    j.packet_start = packets;
+    j.cone_start = cones;
+    j.point_start = points;
+    packets += (P + pw - 1) / pw;
+    cones += P;
+    points += P;
+    jobs.push_back(j);
+    cones_of.push_back(P);
+  }
+};
+
+#define GROUP_CUDA(call, what)                                                     \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      abandon(s, slot, e_ == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA, \
+              std::string(what) + ": " + cudaGetErrorString(e_));                  \
+      return false;                                                                \
+    }                                                                              \
+  } while (0)
+
+// Enqueues one group on the slot's stream: exact jobs through the split path
+// (cone setup, packet and solo passes, integration, per chunk), prefiltering
+// jobs through the prefiltering kernel (walk and integration in one pass).
+// Its job table goes up from `staging` (pinned); its counters land in
+// `status` (kCounterWords). Returns false once it has abandoned the launch.
+bool enqueue_group(cc_server* s, Slot& slot, JobGroup& g, bool splat, cc::JobGpu* staging, uint32_t* status) {
+  cudaStream_t st = slot.stream;
+  const uint32_t pw = s->opt.points_per_warp;
+  cudaError_t e = cudaSuccess;
+  std::memcpy(staging, g.jobs.data(), g.jobs.size() * sizeof(cc::JobGpu));
+  const uint64_t sort_bytes = cc::batch_order_scratch_bytes(g.points);
+  void* d_jobs = pool_alloc(s, g.jobs.size() * sizeof(cc::JobGpu), st, &e);
+  GROUP_CUDA(e, "job table");
+  slot.scratch.push_back(d_jobs);
+  void* d_redo = pool_alloc(s, g.cones * 4, st, &e);
+  GROUP_CUDA(e, "redo list");
+  slot.scratch.push_back(d_redo);
+  void* d_order = pool_alloc(s, g.points * 4, st, &e);
+  GROUP_CUDA(e, "walk order");
+  slot.scratch.push_back(d_order);
+  void* d_sort = pool_alloc(s, sort_bytes, st, &e);
+  GROUP_CUDA(e, "sort scratch");
+  slot.scratch.push_back(d_sort);
+  void* d_counters = pool_alloc(s, cc::kCounterWords * 4, st, &e);
+  GROUP_CUDA(e, "counters");
+  slot.scratch.push_back(d_counters);
+  std::vector<cc::BatchChunk> chunks;
+  void* d_records = nullptr;
+  void* d_masks = nullptr;
+  if (!splat) {
+    chunks = cc::batch_chunks(g.cones_of, pw, s->chunk);
+    uint64_t slots = 1;
+    for (const cc::BatchChunk& k : chunks) slots = std::max(slots, k.cone_count);
+    d_records = pool_alloc(s, slots * sizeof(cc::ConeRecord), st, &e);
+    GROUP_CUDA(e, "cone records");
+    slot.scratch.push_back(d_records);
+    d_masks = pool_alloc(s, slots * 256, st, &e);
+    GROUP_CUDA(e, "cone masks");
+    slot.scratch.push_back(d_masks);
+  }
+  GROUP_CUDA(cudaMemcpyAsync(d_jobs, staging, g.jobs.size() * sizeof(cc::JobGpu), cudaMemcpyHostToDevice, st),
+             "job table upload");
+  GROUP_CUDA(cudaMemsetAsync(d_counters, 0, cc::kCounterWords * 4, st), "counter reset");
+  cc::BatchLaunch L{};
+  L.jobs = static_cast<const cc::JobGpu*>(d_jobs);
+  L.njobs = (uint32_t)g.jobs.size();
+  L.packets = g.packets;
+  L.points = g.points;
+  L.pw = pw;
+  L.records = static_cast<cc::ConeRecord*>(d_records);
+  for (const cc::JobGpu& j : g.jobs) {
+    if (j.query.hierarchy < 2) L.flat_levels = 1;
+    if (j.scene.xforms) L.inst = 1;  // an instanced scene: the instanced kernel for the launch
+  }
+  GROUP_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
+  L.order = static_cast<const uint32_t*>(d_order);
+  uint32_t* counters = static_cast<uint32_t*>(d_counters);
+  cc::DevOut o{};
+  o.redo_count = counters;
+  o.error = counters + 1;
+  o.next_packet = counters + 2;
+  o.next_solo = counters + 3;
+  o.redo_list = static_cast<uint32_t*>(d_redo);
+  o.redo_capacity = (uint32_t)std::max<uint64_t>(g.cones, 1);
+  o.cov_out = static_cast<float*>(d_masks);
+  if (splat) {
+    GROUP_CUDA(cc::launch_batch_splat(L, o, false, s->ctx->sm_count, (int)s->opt.blocks_per_sm, st), "launch");
+  } else {
+    GROUP_CUDA(cc::launch_batch(L, o, chunks.data(), chunks.size(), false, s->ctx->sm_count,
+                                (int)s->opt.blocks_per_sm, st),
+               "launch");
+  }
+  GROUP_CUDA(cudaMemcpyAsync(status, counters, cc::kCounterWords * 4, cudaMemcpyDeviceToHost, st), "status");
+  return true;
+}
+
+// Builds and enqueues one launch on `slot` from the requests admitted to it
+// (their memory already counted in in_use). Called without s->mu: the
+// requests and the slot belong to the loop thread until the launch retires.
 void launch(cc_server* s, Slot& slot) {
   cudaStream_t st = slot.stream;
-  std::vector<cc::JobGpu> jobs;
-  std::vector<uint64_t> job_cones;
-  uint64_t points = 0, cones = 0, packet = 0;
+  JobGroup exact, splat;  // exact cones; prefiltering cones
   const uint32_t pw = s->opt.points_per_warp;
   cc_options d;
   cc_options_default(&d);
@@ -287,12 +393,13 @@ void launch(cc_server* s, Slot& slot) {
       SRV_CUDA(e, "request results");
       r->result[l] = block;
       cc::JobGpu j{};
-      j.scene = sc->dev();
+      j.scene = sc->dev();  // prefiltering requests: coverage made at submission
       j.query.receivers = r->d_receivers;
       j.query.lights = r->d_lights + 4 * t;
       j.query.npoints = P;
       j.query.nlights = 1;
       j.query.hierarchy = q.hierarchy;
+      j.query.prefilter = q.prefilter;
       j.query.wide_extent = d.wide_extent;
       j.query.light_cone_cap = d.light_cone_cap;
       j.query.wide_cone_cap = d.wide_cone_cap;
@@ -305,86 +412,26 @@ void launch(cc_server* s, Slot& slot) {
           j.lo[k] = sc->flat.nodes[0].lo[k];
           j.hi[k] = sc->flat.nodes[0].hi[k];
         }
-      j.packet_start = packet;
-      j.cone_start = cones;
-      j.point_start = points;
-      packet += (P + pw - 1) / pw;
-      cones += P;
-      points += P;
-      jobs.push_back(j);
-      job_cones.push_back(P);
+      (q.prefilter > 0.0f ? splat : exact).add(j, P, pw);
       ++t;
     }
   }
-  // Launch scratch: job table, redo list, walk order and its sort, counters,
-  // and the split path's records and masks for one chunk.
-  if (!jobs.empty()) {
-    cudaError_t e = cudaSuccess;
-    if (slot.host_jobs_cap < jobs.size()) {
-      if (slot.host_jobs) cudaFreeHost(slot.host_jobs);
-      slot.host_jobs = nullptr;
-      slot.host_jobs_cap = 0;
-      SRV_CUDA(cudaMallocHost(&slot.host_jobs, jobs.size() * 2 * sizeof(cc::JobGpu)), "job table staging");
-      slot.host_jobs_cap = jobs.size() * 2;
-    }
-    std::memcpy(slot.host_jobs, jobs.data(), jobs.size() * sizeof(cc::JobGpu));
-    const uint64_t sort_bytes = cc::batch_order_scratch_bytes(points);
-    void* d_jobs = pool_alloc(s, jobs.size() * sizeof(cc::JobGpu), st, &e);
-    SRV_CUDA(e, "job table");
-    slot.scratch.push_back(d_jobs);
-    void* d_redo = pool_alloc(s, cones * 4, st, &e);
-    SRV_CUDA(e, "redo list");
-    slot.scratch.push_back(d_redo);
-    void* d_order = pool_alloc(s, points * 4, st, &e);
-    SRV_CUDA(e, "walk order");
-    slot.scratch.push_back(d_order);
-    void* d_sort = pool_alloc(s, sort_bytes, st, &e);
-    SRV_CUDA(e, "sort scratch");
-    slot.scratch.push_back(d_sort);
-    void* d_counters = pool_alloc(s, cc::kCounterWords * 4, st, &e);
-    SRV_CUDA(e, "counters");
-    slot.scratch.push_back(d_counters);
-    const std::vector<cc::BatchChunk> chunks = cc::batch_chunks(job_cones, pw, s->chunk);
-    uint64_t slots = 1;
-    for (const cc::BatchChunk& k : chunks) slots = std::max(slots, k.cone_count);
-    void* d_records = pool_alloc(s, slots * sizeof(cc::ConeRecord), st, &e);
-    SRV_CUDA(e, "cone records");
-    slot.scratch.push_back(d_records);
-    void* d_masks = pool_alloc(s, slots * 256, st, &e);
-    SRV_CUDA(e, "cone masks");
-    slot.scratch.push_back(d_masks);
-    SRV_CUDA(cudaMemcpyAsync(d_jobs, slot.host_jobs, jobs.size() * sizeof(cc::JobGpu), cudaMemcpyHostToDevice, st),
-             "job table upload");
-    SRV_CUDA(cudaMemsetAsync(d_counters, 0, cc::kCounterWords * 4, st), "counter reset");
-    cc::BatchLaunch L{};
-    L.jobs = static_cast<const cc::JobGpu*>(d_jobs);
-    L.njobs = (uint32_t)jobs.size();
-    L.packets = packet;
-    L.points = points;
-    L.pw = pw;
-    L.records = static_cast<cc::ConeRecord*>(d_records);
-    for (const cc::JobGpu& j : jobs) {
-      if (j.query.hierarchy < 2) L.flat_levels = 1;
-      if (j.scene.xforms) L.inst = 1;  // an instanced scene: the instanced kernel for the launch
-    }
-    SRV_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
-    L.order = static_cast<const uint32_t*>(d_order);
-    uint32_t* counters = static_cast<uint32_t*>(d_counters);
-    cc::DevOut o{};
-    o.redo_count = counters;
-    o.error = counters + 1;
-    o.next_packet = counters + 2;
-    o.next_solo = counters + 3;
-    o.redo_list = static_cast<uint32_t*>(d_redo);
-    o.redo_capacity = (uint32_t)std::max<uint64_t>(cones, 1);
-    o.cov_out = static_cast<float*>(d_masks);
-    SRV_CUDA(cc::launch_batch(L, o, chunks.data(), chunks.size(), false, s->ctx->sm_count, (int)s->opt.blocks_per_sm,
-                              st),
-             "launch");
-    SRV_CUDA(cudaMemcpyAsync(slot.status, counters, cc::kCounterWords * 4, cudaMemcpyDeviceToHost, st), "status");
-  } else {
-    std::fill(slot.status, slot.status + cc::kCounterWords, 0u);
+  // Each group's scratch: job table, redo list, walk order and its sort,
+  // counters, and for exact jobs the split path's records and masks for one
+  // chunk. The job tables go up from one pinned staging area.
+  const size_t njobs = exact.jobs.size() + splat.jobs.size();
+  if (njobs && slot.host_jobs_cap < njobs) {
+    if (slot.host_jobs) cudaFreeHost(slot.host_jobs);
+    slot.host_jobs = nullptr;
+    slot.host_jobs_cap = 0;
+    SRV_CUDA(cudaMallocHost(&slot.host_jobs, njobs * 2 * sizeof(cc::JobGpu)), "job table staging");
+    slot.host_jobs_cap = njobs * 2;
   }
+  std::fill(slot.status, slot.status + 2 * cc::kCounterWords, 0u);
+  if (!exact.jobs.empty() && !enqueue_group(s, slot, exact, false, slot.host_jobs, slot.status)) return;
+  if (!splat.jobs.empty() &&
+      !enqueue_group(s, slot, splat, true, slot.host_jobs + exact.jobs.size(), slot.status + cc::kCounterWords))
+    return;
   // Results to the requests' host buffers, light-major.
   for (Request* r : slot.reqs) {
     const cc_request& q = r->req;
@@ -547,7 +594,7 @@ int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server
   for (Slot& slot : s->slots) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaMallocHost(&slot.status, cc::kCounterWords * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMallocHost(&slot.status, 2 * cc::kCounterWords * sizeof(uint32_t));
   }
   if (e != cudaSuccess) {
     rc = cuda_fail(e, "server setup");
@@ -598,6 +645,8 @@ int cc_server_submit(cc_server* s, const cc_request* req, uint64_t* ticket) {
   if ((req->npoints && !req->receivers) || (req->nlights && !req->lights))
     return fail(CC_ERR_INVALID, "null inputs");
   if (req->hierarchy > 2) return fail(CC_ERR_INVALID, "hierarchy must be 0, 1 or 2");
+  if (!(req->prefilter >= 0.0f)) return fail(CC_ERR_INVALID, "prefilter must be >= 0");
+  if (req->prefilter > 0.0f && req->hierarchy != 2) return fail(CC_ERR_INVALID, "prefiltered cones need hierarchy 2");
   if (req->npoints >= (1ull << 31)) return fail(CC_ERR_INVALID, "more than 2^31 - 1 points in one request");
   if (request_cones(*req) >= 0xffffffffull) return fail(CC_ERR_INVALID, "more than 2^32 - 1 cones in one request");
   auto r = std::make_unique<Request>();
@@ -606,6 +655,14 @@ int cc_server_submit(cc_server* s, const cc_request* req, uint64_t* ticket) {
   r->t_submit = Clock::now();
   std::lock_guard<std::mutex> g(s->mu);
   if (req->scene >= s->scenes.size()) return fail(CC_ERR_INVALID, "unknown scene");
+  if (req->prefilter > 0.0f) {
+    // The scene's coverage samples, made before the request can be launched
+    // (submissions are serialized by the lock; exact launches never read
+    // them).
+    int rc = set_device(s->ctx);
+    if (rc) return rc;
+    if ((rc = cc_host::scene_coverage(const_cast<cc_scene*>(s->scenes[req->scene])))) return rc;
+  }
   if (s->queue.size() >= s->opt.max_queue) {
     s->refused++;
     return fail(CC_ERR_BUSY, "the server's queue is full");

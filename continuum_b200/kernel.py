@@ -650,7 +650,7 @@ class Server:
         return int(i.value)
 
     def submit(self, scene_id: int, receivers: np.ndarray, lights: np.ndarray, outputs: dict,
-               hierarchy=Hierarchy.TRIANGLES, cache_key: int = 0) -> int:
+               hierarchy=Hierarchy.TRIANGLES, cache_key: int = 0, prefilter: float = 0.0) -> int:
         """Queues a request; outputs maps full/any (uint64 [L, P]) and
         irradiance/fraction (float32 [L, P]) to host arrays. Raises CCError
         (CC_ERR_BUSY) when the queue is full."""
@@ -661,7 +661,8 @@ class Server:
                 raise ValueError(f"output {k} must be C-contiguous with a value per cone")
         req = _lib.Request(int(scene_id), ptr(rec), rec.shape[0], ptr(lig), lig.shape[0],
                            int(Hierarchy.of(hierarchy)), int(cache_key),
-                           *(ptr(outputs.get(k)) for k in ("full", "any", "irradiance", "fraction")))
+                           *(ptr(outputs.get(k)) for k in ("full", "any", "irradiance", "fraction")),
+                           float(prefilter))
         t = C.c_uint64()
         check(load().cc_server_submit(self.handle, C.byref(req), C.byref(t)))
         self._live[int(t.value)] = (rec, lig, outputs)

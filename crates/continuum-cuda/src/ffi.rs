@@ -146,6 +146,7 @@ pub struct cc_request {
     pub any: *mut u32,
     pub irradiance: *mut f32,
     pub fraction: *mut f32,
+    pub prefilter: f32,
 }
 
 #[repr(C)]

@@ -445,6 +445,7 @@ typedef struct cc_request {
   uint32_t* any;
   float* irradiance;
   float* fraction;
+  float prefilter;           /* prefiltered cones, as cc_options.prefilter (bins; 0: exact cones; needs hierarchy 2) */
 } cc_request;
 
 typedef struct cc_request_stats {

@@ -205,3 +205,42 @@ def test_prefiltered_jobs_share_a_batch_with_exact_ones(kernel, world):
     b.close()
     inst.close()
     flat.close()
+
+
+def test_served_prefiltered_requests_equal_the_plain_call(kernel, world):
+    """Prefiltering requests (cc_request.prefilter) beside exact ones, on an
+    instanced and a world-space scene: each launch runs its exact jobs
+    through the split path and its prefiltering jobs through the
+    prefiltering kernel; every result equals the plain call's. The lighting
+    cache keeps exact and prefiltered results of the same light apart."""
+    inst = kernel.scene_instanced(world.geometries, world.instances)
+    ico = scenes.icosphere_field(seed=8, n_spheres=6, subdivisions=3, width=64, height=36)
+    flat = kernel.scene(ico.meshes)
+    srv = Server(kernel, max_inflight=2, max_launch_cones=30_000)
+    ids = {id(inst): srv.add_scene(inst), id(flat): srv.add_scene(flat)}
+    specs = [(inst, world.receivers, world.lights, 2.0), (flat, ico.receivers, ico.lights[:2], 1.0),
+             (inst, world.receivers[1::3], world.lights[2:], 0.0), (flat, ico.receivers, ico.lights[:2], 0.0)]
+    reqs = []
+    for scene, rec, lig, pf in specs:
+        rec = np.ascontiguousarray(rec)
+        lig = np.ascontiguousarray(lig)
+        out = {"full": np.zeros((lig.shape[0], rec.shape[0]), np.uint64),
+               "any": np.zeros((lig.shape[0], rec.shape[0]), np.uint64),
+               "irradiance": np.zeros((lig.shape[0], rec.shape[0]), np.float32),
+               "fraction": np.zeros((lig.shape[0], rec.shape[0]), np.float32)}
+        t = srv.submit(ids[id(scene)], rec, lig, out, cache_key=5, prefilter=pf)
+        reqs.append((scene, rec, lig, pf, out, t))
+    for scene, rec, lig, pf, out, t in reqs:
+        srv.wait(t)
+        kernel.prefilter = pf
+        try:
+            v = kernel.visibility(scene, rec, lig, outputs=KEYS)
+        finally:
+            kernel.prefilter = 0.0
+        for key in KEYS:
+            assert np.array_equal(out[key], getattr(v, key).reshape(lig.shape[0], rec.shape[0])), (pf, key)
+    with pytest.raises(_lib.CCError):
+        srv.submit(ids[id(flat)], ico.receivers, ico.lights[:1], {}, hierarchy=1, prefilter=1.0)
+    srv.close()
+    inst.close()
+    flat.close()
