@@ -1018,11 +1018,12 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
         kernel.visibility_device(scene, rec.data_ptr(), P, lig.data_ptr(), L, ptrs, stream=stream.cuda_stream)
 
     # This library's kernels per step: morton_keys (Morton walk order, when
-    # there are more than 64 points), and per split chunk the cone setup, the
-    # packet pass, the solo pass and the integration.
+    # there are more than 64 points), light_order_kernel (two lights or
+    # more), and per split chunk the cone setup, the packet pass, the solo
+    # pass and the integration.
     morton = P > 64
     chunks = (C + (1 << 25) - 1) >> 25
-    launches_per_step = 4 * chunks + (1 if morton else 0)
+    launches_per_step = 4 * chunks + (1 if morton else 0) + (1 if L >= 2 else 0)
 
     # Work counters (an untimed counted run): the algorithmic bytes per cone.
     work = torch.empty(C, 4, dtype=torch.int32, device=dev)
