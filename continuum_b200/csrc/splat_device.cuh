@@ -45,13 +45,15 @@ __device__ __forceinline__ float node_front_area(const float* __restrict__ cov, 
 // space, so splats add to them. Returns its vertex count (at most 8).
 __device__ __forceinline__ int hull8(const float2* pts, float2* out) {
   int start = 0;
+#pragma unroll 1
   for (int k = 1; k < 8; ++k)
     if (pts[k].x < pts[start].x || (pts[k].x == pts[start].x && pts[k].y < pts[start].y)) start = k;
   int n = 0, cur = start;
 #pragma unroll 1
   for (;;) {
     out[n++] = pts[cur];
-    int next = (cur + 1) % 8;
+    int next = (cur + 1) & 7;
+#pragma unroll 1
     for (int k = 0; k < 8; ++k) {
       const float ex = pts[next].x - pts[cur].x, ey = pts[next].y - pts[cur].y;
       const float fx = pts[k].x - pts[cur].x, fy = pts[k].y - pts[cur].y;
@@ -66,21 +68,27 @@ __device__ __forceinline__ int hull8(const float2* pts, float2* out) {
 
 // The hull of 8 projected corners clipped to the window's square and drawn
 // with weight `alpha` (:564-573, :1123-1133). Returns whether anything was
-// drawn.
+// drawn. Out of line, with the square's four clips from one call site and
+// rolled loops: the prefiltering walk, like the exact one, is bound by
+// instruction fetch.
 template <class Acc>
-__device__ __forceinline__ bool draw_hull(Acc& acc, const float2* pts, float alpha) {
+static __device__ __noinline__ bool draw_hull(Acc& acc, const float2* pts, float alpha) {
   const float g = float(kGrid);
   float2 qa[kPolyCap], qb[kPolyCap];
   int n = hull8(pts, qa);
-  n = clip_line2(qa, n, qb, -1.0f, 0.0f, 0.0f);
-  n = clip_line2(qb, n, qa, 1.0f, 0.0f, g);
-  n = clip_line2(qa, n, qb, 0.0f, -1.0f, 0.0f);
-  n = clip_line2(qb, n, qa, 0.0f, 1.0f, g);
-  if (n < 3) return false;
-  for (int i = 0; i < n; ++i) {
-    const float2 a = qa[i], b = qa[(i + 1) % n];
-    draw_edge(acc, clampf(a.x, 0.f, g), clampf(a.y, 0.f, g), clampf(b.x, 0.f, g), clampf(b.y, 0.f, g), alpha);
+  float2* q = qa;
+  float2* q2 = qb;
+#pragma unroll 1
+  for (int side = 0; side < 4; ++side) {
+    const float nx = side == 0 ? -1.0f : (side == 1 ? 1.0f : 0.0f);
+    const float ny = side == 2 ? -1.0f : (side == 3 ? 1.0f : 0.0f);
+    n = clip_line2(q, n, q2, nx, ny, (side & 1) ? g : 0.0f);
+    float2* t = q;
+    q = q2;
+    q2 = t;
   }
+  if (n < 3) return false;
+  draw_polygon(acc, q, n, alpha);
   return true;
 }
 
@@ -106,7 +114,7 @@ __device__ __noinline__ int node_cone_test(const Cone& c, f3 horizon, Acc& acc, 
   bool far_out = true, near_out = true, out_u0 = true, out_u1 = true, out_v0 = true, out_v1 = true;
   bool below = kHorizon;
   bool inside = prefilter > 0.0f;  // splattable: every corner between the near and far planes
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < 8; ++k) {
     const f3 corner = mk((k & 1) ? hi.x : lo.x, (k & 2) ? hi.y : lo.y, (k & 4) ? hi.z : lo.z);
     if constexpr (kHorizon) {
@@ -154,7 +162,7 @@ __device__ __noinline__ bool splat_object_node(const Cone& c, Acc& acc, const fl
   const float g = float(kGrid);
   float2 pts[8];
   float mnx = 3.4e38f, mny = 3.4e38f, mxx = -3.4e38f, mxy = -3.4e38f;
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < 8; ++k) {
     const f3 corner = mk((k & 1) ? hi.x : lo.x, (k & 2) ? hi.y : lo.y, (k & 4) ? hi.z : lo.z);
     if (c.far_offset - dot(c.fwd, corner) < 0.0f) return false;
