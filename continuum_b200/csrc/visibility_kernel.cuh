@@ -890,6 +890,7 @@ __device__ __forceinline__ void light_integral(const Cone& cone, f3 point, f3 no
       // sphere_open_share (:957-972)
       float total_w = 0.0f, open_w = 0.0f;
       const float g = float(kGrid);
+#pragma unroll 1
       for (int b = 0; b < kBins; ++b) {
         const float mfrac = info.wide_clipped ? 1.0f : c_disk[b];
         if (mfrac <= 0.0f) continue;
@@ -1163,6 +1164,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
       // horizon, less its covered bins' clipped weights.
       if (traced) {
         float blocked = 0.0f;
+#pragma unroll 1
         for (int b = 0; b < kBins; ++b) {
           const float cv = st.cov_at(b);
           if (cv > 0.0f) blocked += cv * clipped_bin_weight(st.cone, normal, b);
