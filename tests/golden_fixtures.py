@@ -31,18 +31,46 @@ def cases() -> dict:
     return out
 
 
+def instanced_cases() -> dict:
+    """name -> (world, per-object clear, prefilter bins, partial cones): placed
+    boulders, some alpha-blended (clear 0.5), some thin glass (-0.7), some
+    solid glass volumes (-2.5), with exact and prefiltered cones."""
+    w = scenes.instanced_world(seed=7, n_instances=120, n_boulders=2, half=30.0, n_lights=3, width=48, height=27,
+                               segments=16, rings=10)
+    clear = np.zeros(len(w.instances), np.float32)
+    clear[0:-1:5] = 0.5
+    clear[1:-1:7] = -0.7
+    clear[2:-1:9] = -2.5
+    return {"clear_objects_48x27": (w, clear, 0.0, 256), "clear_objects_prefiltered_48x27": (w, clear, 8.0, 256)}
+
+
+def oracle_instanced(w, clear, prefilter):
+    from oracle.oracle import OracleScene
+
+    orc = OracleScene.instanced(w.geometries, w.instances)
+    orc.set_clear(clear)
+    r = orc.visibility(w.receivers, w.lights, prefilter=prefilter)
+    orc.close()
+    return r
+
+
+def save(name: str, r: dict, npart: int, h: int) -> None:
+    n = r["full"].size
+    pick = np.linspace(0, n - 1, min(npart, n)).astype(np.int64)
+    np.savez_compressed(GOLDEN / f"{name}.npz", full=r["full"], any=r["any"], irradiance=r["irradiance"],
+                        fraction=r["fraction"], unshadowed=r["unshadowed"], partial_ids=pick,
+                        partial=r["partial"][pick], hierarchy=np.int64(h))
+    print(name, n, "cones")
+
+
 def make() -> None:
     from oracle.oracle import OracleScene
 
     GOLDEN.mkdir(exist_ok=True)
     for name, (meshes, rec, lights, h, npart) in cases().items():
-        r = OracleScene(meshes).visibility(rec, lights, hierarchy=h)
-        n = r["full"].size
-        pick = np.linspace(0, n - 1, min(npart, n)).astype(np.int64)
-        np.savez_compressed(GOLDEN / f"{name}.npz", full=r["full"], any=r["any"], irradiance=r["irradiance"],
-                            fraction=r["fraction"], unshadowed=r["unshadowed"], partial_ids=pick,
-                            partial=r["partial"][pick], hierarchy=np.int64(h))
-        print(name, n, "cones")
+        save(name, OracleScene(meshes).visibility(rec, lights, hierarchy=h), npart, h)
+    for name, (w, clear, pf, npart) in instanced_cases().items():
+        save(name, oracle_instanced(w, clear, pf), npart, 2)
 
 
 def load(name: str) -> dict:
@@ -70,11 +98,21 @@ def check(name: str, got: dict) -> dict:
 
 
 def check_all(kernel) -> None:
+    outputs = ("full", "any", "partial", "irradiance", "fraction")
     for name, (meshes, rec, lights, h, _) in cases().items():
         scene = kernel.scene(meshes)
-        v = kernel.visibility(scene, rec, lights, hierarchy=h, outputs=("full", "any", "partial", "irradiance",
-                                                                          "fraction"))
+        v = kernel.visibility(scene, rec, lights, hierarchy=h, outputs=outputs)
         scene.close()
+        check(name, parity.flat(v))
+    for name, (w, clear, pf, _) in instanced_cases().items():
+        scene = kernel.scene_instanced(w.geometries, w.instances)
+        scene.set_clear(clear)
+        kernel.prefilter = pf
+        try:
+            v = kernel.visibility(scene, w.receivers, w.lights, outputs=outputs)
+        finally:
+            kernel.prefilter = 0.0
+            scene.close()
         check(name, parity.flat(v))
 
 

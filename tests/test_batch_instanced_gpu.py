@@ -159,7 +159,7 @@ def test_served_requests_on_an_instanced_scene_equal_the_plain_call(kernel, worl
 
 
 def test_prefiltered_jobs_share_a_batch_with_exact_ones(kernel, world):
-    """Prefiltering jobs (prefilter 1 and 2 bins; instanced with and without
+    """Prefiltering jobs (prefilter 4 and 8 bins; instanced with and without
     object splats, and world-space) run in the batch's second launch beside
     an exact job: each equals its prefiltered cc_visibility call alone, on the
     first submission and on graph replays."""
@@ -168,8 +168,8 @@ def test_prefiltered_jobs_share_a_batch_with_exact_ones(kernel, world):
     inst = kernel.scene_instanced(world.geometries, world.instances)
     ico = scenes.icosphere_field(seed=8, n_spheres=6, subdivisions=3, width=64, height=36)
     flat = kernel.scene(ico.meshes)
-    specs = [(inst, world.receivers, world.lights, 2.0, True), (flat, ico.receivers, ico.lights, 0.0, True),
-             (flat, ico.receivers[::3], ico.lights[:2], 1.0, True), (inst, world.receivers[::4], world.lights[1:], 2.0, False)]
+    specs = [(inst, world.receivers, world.lights, 8.0, True), (flat, ico.receivers, ico.lights, 0.0, True),
+             (flat, ico.receivers[::3], ico.lights[:2], 4.0, True), (inst, world.receivers[::4], world.lights[1:], 8.0, False)]
     jobs = []
     for scene, rec, lig, pf, obj in specs:
         r = torch.from_numpy(np.ascontiguousarray(rec)).cuda()
@@ -218,7 +218,7 @@ def test_served_prefiltered_requests_equal_the_plain_call(kernel, world):
     flat = kernel.scene(ico.meshes)
     srv = Server(kernel, max_inflight=2, max_launch_cones=30_000)
     ids = {id(inst): srv.add_scene(inst), id(flat): srv.add_scene(flat)}
-    specs = [(inst, world.receivers, world.lights, 2.0), (flat, ico.receivers, ico.lights[:2], 1.0),
+    specs = [(inst, world.receivers, world.lights, 8.0), (flat, ico.receivers, ico.lights[:2], 4.0),
              (inst, world.receivers[1::3], world.lights[2:], 0.0), (flat, ico.receivers, ico.lights[:2], 0.0)]
     reqs = []
     for scene, rec, lig, pf in specs:

@@ -162,17 +162,22 @@ def test_blended_and_transmissive_objects_match_the_oracle(kernel, world):
 
 
 def test_prefiltered_cones_through_blended_objects_match_the_oracle(kernel, world):
+    """At 8 bins some nodes of this world are splatted (their coverage samples
+    scaled by their geometry's opacity): the results differ from exact cones
+    and meet the bar against the oracle's prefiltered walk."""
     clear = clear_values(world)
     scene = kernel.scene_instanced(world.geometries, world.instances)
     scene.set_clear(clear)
-    kernel.prefilter = 2.0
+    exact = parity.flat(kernel.visibility(scene, world.receivers, world.lights, outputs=ALL))
+    kernel.prefilter = 8.0
     try:
         g = parity.flat(kernel.visibility(scene, world.receivers, world.lights, outputs=ALL))
     finally:
         kernel.prefilter = 0.0
         scene.close()
+    assert (g["fraction"] != exact["fraction"]).sum() > 10
     orc = OracleScene.instanced(world.geometries, world.instances)
     orc.set_clear(clear)
-    o = orc.visibility(world.receivers, world.lights, prefilter=2.0)
+    o = orc.visibility(world.receivers, world.lights, prefilter=8.0)
     orc.close()
     parity.compare(g, o, o["unshadowed"])

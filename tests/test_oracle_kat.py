@@ -192,3 +192,6 @@ def test_oracle_reproduces_the_golden_fixtures():
         r = OracleScene(meshes).visibility(rec, lights, hierarchy=h)
         stats = golden_fixtures.check(name, r)
         assert stats["word_agreement"] == 1.0
+    for name, (w, clear, pf, _) in golden_fixtures.instanced_cases().items():
+        stats = golden_fixtures.check(name, golden_fixtures.oracle_instanced(w, clear, pf))
+        assert stats["word_agreement"] == 1.0
