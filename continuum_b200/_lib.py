@@ -92,7 +92,8 @@ class BatchOptions(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget", C.c_uint64), ("max_inflight", C.c_uint32), ("max_queue", C.c_uint32),
-                ("max_launch_cones", C.c_uint64), ("points_per_warp", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+                ("max_launch_cones", C.c_uint64), ("points_per_warp", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("deadline_ns_per_cone", C.c_uint32)]
 
 
 class CacheOptions(C.Structure):

@@ -6,7 +6,7 @@
 // Each launch slot owns a stream, an event and pinned host staging for its
 // job table and status words. The loop retires finished launches (results
 // become cache entries or are freed), then builds the next launch from the
-// queue's front: cache lookups first, then device memory for the traced
+// queued requests, earliest deadline first: cache lookups first, then device memory for the traced
 // lights (evicting unused cache entries least recently used), one job per
 // (request, traced light), the copies in, one batched launch, and the copies
 // out. Device memory comes from a pool owned by the server, allocated and
@@ -54,6 +54,7 @@ struct Request {
   cc_request req{};
   std::vector<float> lights;  // copied at submission
   Clock::time_point t_submit, t_admit, t_done;
+  Clock::time_point deadline;  // admission order: submission + the options' time per cone
   bool done = false;
   int status = CC_OK;
   std::string error;
@@ -71,6 +72,7 @@ struct Slot {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   bool busy = false;
+  bool large = false;                // the launch runs one request above the launch's cone limit
   std::vector<Request*> reqs;
   std::vector<void*> scratch;        // freed when the launch retires
   uint64_t scratch_bytes = 0;        // in_use held by the launch besides result blocks
@@ -451,15 +453,30 @@ void launch(cc_server* s, Slot& slot) {
   s->launches++;
 }
 
-// Takes requests off the queue's front for a launch while they fit: the
-// budget (after evicting unused cache entries) and the launch's cone limit.
+// Takes queued requests for a launch, earliest deadline first (arrival order
+// among equal deadlines), while they fit: the budget (after evicting unused
+// cache entries) and the launch's cone limit. The most urgent request that
+// does not fit the memory stops the admission (*blocked: it), so that later
+// ones cannot keep it waiting; one that does not fit the launch's cone limit
+// is left for the next launch (in arrival order: admission stops there).
+// Ordered by deadline, requests above the cone limit (each runs alone) hold
+// at most all slots but one, so that smaller requests always find a slot
+// instead of queueing behind long launches. *large: the launch takes one.
 // Returns the requests taken and the bytes their results hold. (s->mu held.)
-std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_bytes, uint64_t* total_bytes) {
+std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_bytes, uint64_t* total_bytes,
+                            Request** blocked, bool* large) {
   std::vector<Request*> taken;
   uint64_t cones = 0;
   *result_bytes = *total_bytes = 0;
-  while (!s->queue.empty()) {
-    Request* r = s->queue.front();
+  *blocked = nullptr;
+  *large = false;
+  uint32_t large_busy = 0;
+  for (const Slot& slot : s->slots) large_busy += slot.busy && slot.large;
+  std::vector<Request*> order(s->queue.begin(), s->queue.end());
+  std::stable_sort(order.begin(), order.end(),
+                   [](const Request* a, const Request* b) { return a->deadline < b->deadline; });
+  const bool arrival = s->opt.deadline_ns_per_cone == 0;
+  for (Request* r : order) {
     const cc_request& q = r->req;
     // Lighting-cache lookups (entries found stay referenced by this launch).
     std::vector<CacheEntry*> hit(q.nlights, nullptr);
@@ -469,7 +486,12 @@ std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_
       if (!hit[l]) ++traced;
     }
     const uint64_t c = traced * q.npoints;
-    if (!taken.empty() && cones + c > s->opt.max_launch_cones) break;
+    if (!taken.empty() && cones + c > s->opt.max_launch_cones) {
+      if (arrival) break;
+      continue;
+    }
+    const bool is_large = c > s->opt.max_launch_cones;
+    if (!arrival && is_large && s->opt.max_inflight > 1 && large_busy + 1 >= s->opt.max_inflight) continue;
     for (CacheEntry* e : hit)
       if (e) e->refs++;  // keep them through make_room
     // The request's bytes, and what it adds to the launch's split scratch.
@@ -477,11 +499,11 @@ std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_
     if (!make_room(s, need, stream)) {
       for (CacheEntry* e : hit)
         if (e) e->refs--;
+      *blocked = r;
       break;
     }
     for (CacheEntry* e : hit)
       if (e) touch(s, e);
-    s->queue.pop_front();
     r->hit = std::move(hit);
     r->result.assign(q.nlights, nullptr);
     r->t_admit = Clock::now();
@@ -495,6 +517,13 @@ std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_
     *total_bytes += need;
     taken.push_back(r);
     cones += c;
+    *large = is_large;
+  }
+  if (!taken.empty()) {
+    std::deque<Request*> rest;
+    for (Request* r : s->queue)
+      if (std::find(taken.begin(), taken.end(), r) == taken.end()) rest.push_back(r);
+    s->queue.swap(rest);
   }
   for (Request* r : taken) r->stats.launch_requests = (uint32_t)taken.size();
   return taken;
@@ -519,23 +548,26 @@ void run_loop(cc_server* s) {
       }
     if (free_slot && !s->queue.empty()) {
       uint64_t result_bytes = 0, total_bytes = 0;
-      std::vector<Request*> taken = admit(s, free_slot->stream, &result_bytes, &total_bytes);
+      Request* blocked = nullptr;
+      bool large = false;
+      std::vector<Request*> taken = admit(s, free_slot->stream, &result_bytes, &total_bytes, &blocked, &large);
       if (!taken.empty()) {
         // Result blocks are released one by one (or kept as cache entries);
         // the rest of the admitted bytes are released with the launch.
         free_slot->scratch_bytes = total_bytes - result_bytes;
         free_slot->reqs = std::move(taken);
         free_slot->busy = true;
+        free_slot->large = large;
         lk.unlock();
         launch(s, *free_slot);
         lk.lock();
         continue;
       }
-      if (!any_busy) {
-        // Nothing in flight and the cache emptied, yet the front request does
-        // not fit: it never will.
-        Request* r = s->queue.front();
-        s->queue.pop_front();
+      if (!any_busy && blocked) {
+        // Nothing in flight and the cache emptied, yet the most urgent request
+        // does not fit: it never will.
+        Request* r = blocked;
+        s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
         s->refused++;
         r->t_admit = Clock::now();
         complete_locked(s, r, CC_ERR_BUSY, "the request does not fit the server's memory budget");
@@ -562,6 +594,7 @@ void cc_server_options_default(cc_server_options* opt) {
   opt->max_launch_cones = 2ull << 20;
   opt->points_per_warp = 32;
   opt->blocks_per_sm = cc::kBlocksPerSm;
+  opt->deadline_ns_per_cone = 12;
 }
 
 int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server** out) {
@@ -653,6 +686,7 @@ int cc_server_submit(cc_server* s, const cc_request* req, uint64_t* ticket) {
   r->req = *req;
   r->lights.assign(req->lights, req->lights + 16 * (size_t)req->nlights);
   r->t_submit = Clock::now();
+  r->deadline = r->t_submit + std::chrono::nanoseconds(request_cones(*req) * s->opt.deadline_ns_per_cone);
   std::lock_guard<std::mutex> g(s->mu);
   if (req->scene >= s->scenes.size()) return fail(CC_ERR_INVALID, "unknown scene");
   if (req->prefilter > 0.0f) {

@@ -131,6 +131,7 @@ pub struct cc_server_options {
     pub max_launch_cones: u64,
     pub points_per_warp: u32,
     pub blocks_per_sm: u32,
+    pub deadline_ns_per_cone: u32,
 }
 
 #[repr(C)]

@@ -127,3 +127,88 @@ def test_admission_stays_under_the_budget(kernel, fields):
     assert e.value.code == _lib.CC_ERR_BUSY
     assert srv.stats()["refused"] == 1
     srv.close()
+
+
+@pytest.mark.parametrize("ns_per_cone", [12, 0])
+def test_small_requests_overtake_large_ones(kernel, fields, ns_per_cone):
+    """Earliest deadline first: while one launch runs (one slot, one request
+    a launch), a small request submitted just after a large one is admitted
+    first, and the large one after the small one has completed; with no time
+    per cone (arrival order) the small one waits for the large one. Results
+    are the same either way."""
+    import time
+
+    ws, sc = fields
+    w = ws[0]
+    srv = Server(kernel, max_inflight=1, max_launch_cones=1, deadline_ns_per_cone=ns_per_cone)
+    sid = srv.add_scene(sc[0])
+    busy = np.ascontiguousarray(np.concatenate([w.receivers] * 8))
+    big_rec, big_lig = w.receivers, w.lights
+    small_rec, small_lig = np.ascontiguousarray(w.receivers[:500]), np.ascontiguousarray(w.lights[:1])
+    outs = [host_outputs(busy.shape[0], big_lig.shape[0]), host_outputs(big_rec.shape[0], big_lig.shape[0]),
+            host_outputs(500, 1)]
+    t_busy = srv.submit(sid, busy, big_lig, outs[0])
+    t0 = time.perf_counter()
+    t_big = srv.submit(sid, big_rec, big_lig, outs[1])
+    t_small = srv.submit(sid, small_rec, small_lig, outs[2])
+    between_ms = 1e3 * (time.perf_counter() - t0)
+    srv.wait(t_busy)
+    big, small = srv.wait(t_big), srv.wait(t_small)
+    if ns_per_cone:
+        # The large request was admitted after the small one completed.
+        assert big["queued_ms"] >= small["total_ms"]
+    else:
+        assert small["queued_ms"] + between_ms >= big["total_ms"]
+    assert srv.stats()["launches"] == 3
+    for out, rec, lig in ((outs[1], big_rec, big_lig), (outs[2], small_rec, small_lig)):
+        ref = alone(kernel, sc[0], rec, lig)
+        for key in KEYS:
+            assert np.array_equal(out[key], ref[key]), key
+    srv.close()
+
+
+def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
+    """Two slots, a launch limit of 500 cones: while one request above the
+    limit runs, a second such request waits for it although a slot is free,
+    and a small request submitted later takes that slot at once. (Pinned
+    host buffers: a copy to pageable memory would hold the server's thread
+    until the launch before it is done.)"""
+    import time
+
+    import torch
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype).pin_memory()
+        t.numpy()[...] = a
+        return t.numpy()
+
+    ws, sc = fields
+    w = ws[0]
+    srv = Server(kernel, max_inflight=2, max_launch_cones=500)
+    sid = srv.add_scene(sc[0])
+    busy = pinned(np.concatenate([w.receivers] * 32))
+    rec, lig = pinned(w.receivers), w.lights
+    small_rec, small_lig = pinned(w.receivers[:500]), np.ascontiguousarray(w.lights[:1])
+    outs = [{k: pinned(v) for k, v in host_outputs(P, L).items()}
+            for P, L in ((busy.shape[0], lig.shape[0]), (rec.shape[0], lig.shape[0]), (500, 1))]
+    # A first request, so that the server's thread is up and idle before the
+    # sequence (a request queued before its first admission would be ordered
+    # with the later ones by deadline).
+    srv.wait(srv.submit(sid, small_rec, small_lig, outs[2]))
+    t0 = time.perf_counter()
+    t_a = srv.submit(sid, busy, lig, outs[0])
+    time.sleep(0.003)
+    t_b = srv.submit(sid, rec, lig, outs[1])
+    b_after_ms = 1e3 * (time.perf_counter() - t0)
+    time.sleep(0.002)
+    t_c = srv.submit(sid, small_rec, small_lig, outs[2])
+    a, b, c = srv.wait(t_a), srv.wait(t_b), srv.wait(t_c)
+    # b could not start before a completed.
+    assert b["queued_ms"] + b_after_ms >= a["total_ms"]
+    # c was admitted while a still ran.
+    assert c["queued_ms"] < a["total_ms"]
+    for out, r, li in ((outs[1], rec, lig), (outs[2], small_rec, small_lig)):
+        ref = alone(kernel, sc[0], r, li)
+        for key in KEYS:
+            assert np.array_equal(out[key], ref[key]), key
+    srv.close()
