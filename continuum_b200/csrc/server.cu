@@ -460,8 +460,9 @@ void launch(cc_server* s, Slot& slot) {
 // ones cannot keep it waiting; one that does not fit the launch's cone limit
 // is left for the next launch (in arrival order: admission stops there).
 // Ordered by deadline, requests above the cone limit (each runs alone) hold
-// at most all slots but one, so that smaller requests always find a slot
-// instead of queueing behind long launches. *large: the launch takes one.
+// at most all slots but one while a smaller request waits, so that smaller
+// requests find a slot instead of queueing behind long launches (with none
+// waiting, the last slot keeps the device busy). *large: the launch takes one.
 // Returns the requests taken and the bytes their results hold. (s->mu held.)
 std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_bytes, uint64_t* total_bytes,
                             Request** blocked, bool* large) {
@@ -472,6 +473,8 @@ std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_
   *large = false;
   uint32_t large_busy = 0;
   for (const Slot& slot : s->slots) large_busy += slot.busy && slot.large;
+  bool small_waits = false;  // a queued request within the cone limit (before cache hits)
+  for (const Request* r : s->queue) small_waits = small_waits || request_cones(r->req) <= s->opt.max_launch_cones;
   std::vector<Request*> order(s->queue.begin(), s->queue.end());
   std::stable_sort(order.begin(), order.end(),
                    [](const Request* a, const Request* b) { return a->deadline < b->deadline; });
@@ -491,7 +494,8 @@ std::vector<Request*> admit(cc_server* s, cudaStream_t stream, uint64_t* result_
       continue;
     }
     const bool is_large = c > s->opt.max_launch_cones;
-    if (!arrival && is_large && s->opt.max_inflight > 1 && large_busy + 1 >= s->opt.max_inflight) continue;
+    if (!arrival && is_large && small_waits && s->opt.max_inflight > 1 && large_busy + 1 >= s->opt.max_inflight)
+      continue;
     for (CacheEntry* e : hit)
       if (e) e->refs++;  // keep them through make_room
     // The request's bytes, and what it adds to the launch's split scratch.

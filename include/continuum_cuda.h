@@ -412,9 +412,9 @@ CC_API int cc_batch_sizes(const cc_batch* batch, uint64_t out4[4]);
  * request waits forever (0 per cone: arrival order). The most urgent queued
  * request that does not fit the memory left holds back the rest; one that
  * does not fit the current launch's cone limit waits for the next launch while
- * less urgent ones join this one, and requests above the limit (each launched
- * alone) run in at most max_inflight - 1 slots at once, so that smaller ones
- * always find a slot. Each launch takes every admitted request (continuous
+ * less urgent ones join this one, and while a request within the limit waits,
+ * requests above it (each launched alone) take at most max_inflight - 1 slots,
+ * so that smaller ones find a slot. Each launch takes every admitted request (continuous
  * batching: requests that arrive while earlier launches run join the next
  * one, and up to max_inflight launches overlap on the device on their own
  * streams); every (request, light) pair is one job of a batched launch.

@@ -168,11 +168,14 @@ def test_small_requests_overtake_large_ones(kernel, fields, ns_per_cone):
 
 
 def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
-    """Two slots, a launch limit of 500 cones: while one request above the
-    limit runs, a second such request waits for it although a slot is free,
-    and a small request submitted later takes that slot at once. (Pinned
-    host buffers: a copy to pageable memory would hold the server's thread
-    until the launch before it is done.)"""
+    """Two slots, a launch limit of 1M cones, 1 ns of deadline per cone. A
+    request above the limit (a) and one within it (s) hold both slots; then
+    a second request above the limit (b) and, 3 ms later, a small one (c)
+    queue, b with the earlier deadline. When s completes, c takes the slot
+    and b keeps waiting, since a slot stays free of requests above the limit
+    while a smaller one waits. (Pinned host buffers: a copy to pageable
+    memory would hold the server's thread until the launch before it is
+    done.)"""
     import time
 
     import torch
@@ -184,30 +187,29 @@ def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
 
     ws, sc = fields
     w = ws[0]
-    srv = Server(kernel, max_inflight=2, max_launch_cones=500)
+    srv = Server(kernel, max_inflight=2, max_launch_cones=1_000_000, deadline_ns_per_cone=1)
     sid = srv.add_scene(sc[0])
-    busy = pinned(np.concatenate([w.receivers] * 32))
-    rec, lig = pinned(w.receivers), w.lights
+    lig = w.lights
+    big = pinned(np.concatenate([w.receivers] * 32))      # 1.84 M cones with 4 lights
+    medium = pinned(np.concatenate([w.receivers] * 16))   # 0.92 M cones
     small_rec, small_lig = pinned(w.receivers[:500]), np.ascontiguousarray(w.lights[:1])
-    outs = [{k: pinned(v) for k, v in host_outputs(P, L).items()}
-            for P, L in ((busy.shape[0], lig.shape[0]), (rec.shape[0], lig.shape[0]), (500, 1))]
-    # A first request, so that the server's thread is up and idle before the
-    # sequence (a request queued before its first admission would be ordered
-    # with the later ones by deadline).
-    srv.wait(srv.submit(sid, small_rec, small_lig, outs[2]))
-    t0 = time.perf_counter()
-    t_a = srv.submit(sid, busy, lig, outs[0])
-    time.sleep(0.003)
-    t_b = srv.submit(sid, rec, lig, outs[1])
-    b_after_ms = 1e3 * (time.perf_counter() - t0)
+    shapes = ((big.shape[0], 4), (medium.shape[0], 4), (big.shape[0], 4), (500, 1))
+    outs = [{k: pinned(v) for k, v in host_outputs(P, L).items()} for P, L in shapes]
+    # A first request, so that the server's thread is up and idle.
+    srv.wait(srv.submit(sid, small_rec, small_lig, outs[3]))
+    t_a = srv.submit(sid, big, lig, outs[0])
     time.sleep(0.002)
-    t_c = srv.submit(sid, small_rec, small_lig, outs[2])
-    a, b, c = srv.wait(t_a), srv.wait(t_b), srv.wait(t_c)
-    # b could not start before a completed.
-    assert b["queued_ms"] + b_after_ms >= a["total_ms"]
-    # c was admitted while a still ran.
-    assert c["queued_ms"] < a["total_ms"]
-    for out, r, li in ((outs[1], rec, lig), (outs[2], small_rec, small_lig)):
+    t_s = srv.submit(sid, medium, lig, outs[1])
+    time.sleep(0.001)
+    t0 = time.perf_counter()
+    t_b = srv.submit(sid, big, lig, outs[2])
+    time.sleep(0.003)
+    t_c = srv.submit(sid, small_rec, small_lig, outs[3])
+    between_ms = 1e3 * (time.perf_counter() - t0)
+    a, s_, b, c = (srv.wait(t) for t in (t_a, t_s, t_b, t_c))
+    # c was admitted before b although b's deadline came first.
+    assert c["queued_ms"] + between_ms < b["queued_ms"]
+    for out, r, li in ((outs[2], big, lig), (outs[3], small_rec, small_lig)):
         ref = alone(kernel, sc[0], r, li)
         for key in KEYS:
             assert np.array_equal(out[key], ref[key]), key
