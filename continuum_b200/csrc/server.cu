@@ -6,7 +6,7 @@
 // Each launch slot owns a stream, an event and pinned host staging for its
 // job table and status words. The loop retires finished launches (results
 // become cache entries or are freed), then builds the next launch from the
-// queued requests, earliest deadline first: cache lookups first, then device memory for the traced
+// queued requests (in arrival order, or earliest deadline first): cache lookups first, then device memory for the traced
 // lights (evicting unused cache entries least recently used), one job per
 // (request, traced light), the copies in, one batched launch, and the copies
 // out. Device memory comes from a pool owned by the server, allocated and
@@ -36,6 +36,9 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 // Per-point bytes of one light's results: full and any words, irradiance, fraction.
 constexpr uint64_t kResultBytes = 8 + 8 + 4 + 4;
+// Jobs a launch slot's pinned job-table staging holds from the start: a
+// launch of 2M cones in requests of at least 16k points and 8 lights has 1,024.
+constexpr size_t kStagingJobs = 1024;
 
 struct CacheEntry {
   uint64_t key = 0;
@@ -598,7 +601,7 @@ void cc_server_options_default(cc_server_options* opt) {
   opt->max_launch_cones = 2ull << 20;
   opt->points_per_warp = 32;
   opt->blocks_per_sm = cc::kBlocksPerSm;
-  opt->deadline_ns_per_cone = 12;
+  opt->deadline_ns_per_cone = 0;
 }
 
 int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server** out) {
@@ -632,6 +635,11 @@ int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost(&slot.status, 2 * cc::kCounterWords * sizeof(uint32_t));
+    // Job-table staging for launches of up to kStagingJobs jobs, made here:
+    // a pinned allocation (or free) while launches run waits for the whole
+    // device, so the loop grows it only for a launch of more jobs.
+    if (e == cudaSuccess) e = cudaMallocHost(&slot.host_jobs, kStagingJobs * sizeof(cc::JobGpu));
+    if (e == cudaSuccess) slot.host_jobs_cap = kStagingJobs;
   }
   if (e != cudaSuccess) {
     rc = cuda_fail(e, "server setup");

@@ -405,16 +405,18 @@ CC_API int cc_batch_sizes(const cc_batch* batch, uint64_t out4[4]);
 /* ---- Served form --------------------------------------------------------
  * A request loop on its own host thread. Scenes stay resident; requests
  * (a scene, receivers, 1 or more lights) queue on submission and are admitted
- * earliest deadline first while launch slots and device memory under the
- * server's budget allow: a request's deadline is its submission time plus
- * deadline_ns_per_cone for each of its cones, so small requests overtake large
- * ones that have not waited about as long as the small ones take, and no
- * request waits forever (0 per cone: arrival order). The most urgent queued
- * request that does not fit the memory left holds back the rest; one that
- * does not fit the current launch's cone limit waits for the next launch while
- * less urgent ones join this one, and while a request within the limit waits,
- * requests above it (each launched alone) take at most max_inflight - 1 slots,
- * so that smaller ones find a slot. Each launch takes every admitted request (continuous
+ * in arrival order, or with deadline_ns_per_cone > 0 earliest deadline first,
+ * while launch slots and device memory under the server's budget allow: a
+ * request's deadline is its submission time plus deadline_ns_per_cone for each
+ * of its cones, so small requests overtake large ones that have not waited
+ * about as long as the small ones take, and no request waits forever. The
+ * first (most urgent) queued request that does not fit the memory left holds
+ * back the rest. In arrival order, admission into a launch stops at the first
+ * request that does not fit its cone limit. By deadline, such a request waits
+ * for the next launch while less urgent ones join this one, and while a
+ * request within the limit waits, requests above it (each launched alone)
+ * take at most max_inflight - 1 slots, so that smaller ones find a slot.
+ * Each launch takes every admitted request (continuous
  * batching: requests that arrive while earlier launches run join the next
  * one, and up to max_inflight launches overlap on the device on their own
  * streams); every (request, light) pair is one job of a batched launch.
@@ -436,11 +438,12 @@ typedef struct cc_server_options {
   uint64_t max_launch_cones; /* cones one launch takes at most (2M); one larger request runs alone */
   uint32_t points_per_warp;  /* 1..32 (32) */
   uint32_t blocks_per_sm;    /* 1..8 (8) */
-  uint32_t deadline_ns_per_cone; /* admission order: deadline = submission + this per cone (12, about one
-                                    B200's rate on a plain scene); 0: arrival order */
+  uint32_t deadline_ns_per_cone; /* 0: admission in arrival order (default); else earliest deadline first,
+                                    deadline = submission + this per cone (12: about one B200's rate on a
+                                    plain scene) */
 } cc_server_options;
 
-/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 2M cones per launch, 32, 8, 12 ns per cone. */
+/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 2M cones per launch, 32, 8, arrival order. */
 CC_API void cc_server_options_default(cc_server_options* opt);
 
 typedef struct cc_request {
