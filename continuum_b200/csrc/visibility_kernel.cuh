@@ -1007,7 +1007,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, resident_blocks<kWide, kS
     uint64_t ncones = plain_cones;
     uint64_t wbase = (uint64_t)packet * pw;
     uint64_t listed = 0;
-    if (list) listed = list[packet];
+    // The solo pass (64-bit cells) takes the re-walk list from its end: the
+    // packets that finish last, the heaviest, list their cones last, and
+    // walked first they no longer set the pass's end (4.99 -> 3.87 ms for the
+    // solo pass and integration on the plain workload at scale).
+    if (list) listed = list[kWide ? npackets - 1 - packet : packet];
     if constexpr (kBatch) {
       // The packet's job; a listed slot's is in its record (split path), or
       // found from its batch cone number (the prefiltering kernel keeps no
