@@ -646,17 +646,17 @@ def served_leg(args, kernel) -> dict:
                      if p < 100_000]
             return pct(small, 50) if small else None
 
-        deadline = None
+        arrival = None
         if rate * float(np.mean(service_alone)) > 1.0:
             # Over capacity, where the order matters: the same arrivals again,
-            # admitted earliest deadline first (12 ns per cone).
-            d_tickets, _, d_stats, d_span, _ = serve(12)
-            d_lat = [x["total_ms"] / 1e3 for x in d_stats]
-            deadline = {"deadline_ns_per_cone": 12,
-                        "queries_per_s": sum(c for c, t in zip(cones, d_tickets) if t is not None) / d_span,
-                        "p50_ms": pct(d_lat, 50), "p99_ms": pct(d_lat, 99),
-                        "p50_ms_requests_under_100k_points": small_p50(d_tickets, d_stats)}
-        tickets, refused, stats, span, st = serve(0)
+            # admitted in arrival order, beside the default deadline order.
+            a_tickets, _, a_stats, a_span, _ = serve(0)
+            a_lat = [x["total_ms"] / 1e3 for x in a_stats]
+            arrival = {"deadline_ns_per_cone": 0,
+                       "queries_per_s": sum(c for c, t in zip(cones, a_tickets) if t is not None) / a_span,
+                       "p50_ms": pct(a_lat, 50), "p99_ms": pct(a_lat, 99),
+                       "p50_ms_requests_under_100k_points": small_p50(a_tickets, a_stats)}
+        tickets, refused, stats, span, st = serve(12)
         lat = [x["total_ms"] / 1e3 for x in stats]
         served_service = [(x["total_ms"] - x["queued_ms"]) / 1e3 for x in stats]
         big = [x["total_ms"] / 1e3 for x, p in zip(stats, [p for p, t in zip(pts, tickets) if t is not None])
@@ -683,7 +683,8 @@ def served_leg(args, kernel) -> dict:
                          "queued_ms": round(x["queued_ms"], 1), "total_ms": round(x["total_ms"], 1),
                          "alone_ms": round(1e3 * service_alone[i], 1), "launch_requests": x["launch_requests"]}
                         for i, x in slowest],
-            "deadline_order": deadline,
+            "admission": "earliest deadline first, 12 ns per cone",
+            "arrival_order": arrival,
             "plain_per_request": {"p50_ms": pct(lat_plain, 50), "p99_ms": pct(lat_plain, 99),
                                   "queries_per_s": sum(cones) / plain_span},
         })

@@ -13,6 +13,8 @@
 // freed in stream order.
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <list>
@@ -76,6 +78,7 @@ struct Slot {
   cudaEvent_t done = nullptr;
   bool busy = false;
   bool large = false;                // the launch runs one request above the launch's cone limit
+  size_t trace_row = 0;              // the launch's row in the server's trace (when tracing)
   std::vector<Request*> reqs;
   std::vector<void*> scratch;        // freed when the launch retires
   uint64_t scratch_bytes = 0;        // in_use held by the launch besides result blocks
@@ -108,6 +111,20 @@ struct cc_server {
   uint64_t chunk = 1ull << 22;  // cones a launch's split chunk holds at most
 
   uint64_t completed = 0, refused = 0, launches = 0, cached_lights = 0, traced_lights = 0;
+  // CC_SERVER_TRACE set in the environment at creation: one row per launch
+  // (ms since creation: admitted, host time to build and enqueue it, retired;
+  // its requests and cones; slots busy when admitted), written to stderr
+  // when the server is destroyed.
+  bool tracing = false;
+  std::chrono::steady_clock::time_point t0;
+  struct TraceRow {
+    double admitted_ms, enqueue_ms, retired_ms;
+    uint64_t requests, cones;
+    uint32_t busy;
+    double part_ms[5];  // host time in: pool allocations, copies in, walk order, kernel launches, copies out
+  };
+  std::vector<TraceRow> trace;
+  double part_ms[5] = {};  // the launch being built (loop thread only)
 };
 
 namespace {
@@ -128,7 +145,19 @@ uint64_t split_bytes(const cc_server* s, uint64_t cones) {
   return std::min(cones, s->chunk) * (sizeof(cc::ConeRecord) + 256);
 }
 
+// Host time of a call, added to part `k` of the launch's trace row (when tracing).
+struct PartTimer {
+  cc_server* s;
+  int k;
+  Clock::time_point t;
+  PartTimer(cc_server* s_, int k_) : s(s_), k(k_), t(s_->tracing ? Clock::now() : Clock::time_point{}) {}
+  ~PartTimer() {
+    if (s->tracing) s->part_ms[k] += ms_between(t, Clock::now());
+  }
+};
+
 void* pool_alloc(cc_server* s, uint64_t bytes, cudaStream_t stream, cudaError_t* e) {
+  PartTimer timer(s, 0);
   void* p = nullptr;
   *e = cudaMallocFromPoolAsync(&p, std::max<uint64_t>(bytes, 256), s->pool, stream);
   return *e == cudaSuccess ? p : nullptr;
@@ -198,6 +227,8 @@ void release_slot(cc_server* s, Slot& slot) {
 // freed), inputs and scratch are freed, and its requests complete. (s->mu held.)
 void retire(cc_server* s, Slot& slot) {
   const bool stack = ((slot.status[1] | slot.status[cc::kCounterWords + 1]) & 2u) != 0;
+  if (s->tracing && slot.trace_row < s->trace.size())
+    s->trace[slot.trace_row].retired_ms = ms_between(s->t0, Clock::now());
   for (Request* r : slot.reqs) {
     for (size_t l = 0; l < r->result.size(); ++l) {
       if (r->hit[l]) r->hit[l]->refs--;
@@ -343,7 +374,11 @@ bool enqueue_group(cc_server* s, Slot& slot, JobGroup& g, bool splat, cc::JobGpu
     if (j.query.hierarchy < 2) L.flat_levels = 1;
     if (j.scene.xforms) L.inst = 1;  // an instanced scene: the instanced kernel for the launch
   }
-  GROUP_CUDA(cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st), "walk order");
+  {
+    PartTimer timer(s, 2);
+    e = cc::batch_order(L, d_sort, sort_bytes, static_cast<uint32_t*>(d_order), st);
+  }
+  GROUP_CUDA(e, "walk order");
   L.order = static_cast<const uint32_t*>(d_order);
   uint32_t* counters = static_cast<uint32_t*>(d_counters);
   cc::DevOut o{};
@@ -354,13 +389,13 @@ bool enqueue_group(cc_server* s, Slot& slot, JobGroup& g, bool splat, cc::JobGpu
   o.redo_list = static_cast<uint32_t*>(d_redo);
   o.redo_capacity = (uint32_t)std::max<uint64_t>(g.cones, 1);
   o.cov_out = static_cast<float*>(d_masks);
-  if (splat) {
-    GROUP_CUDA(cc::launch_batch_splat(L, o, false, s->ctx->sm_count, (int)s->opt.blocks_per_sm, st), "launch");
-  } else {
-    GROUP_CUDA(cc::launch_batch(L, o, chunks.data(), chunks.size(), false, s->ctx->sm_count,
-                                (int)s->opt.blocks_per_sm, st),
-               "launch");
+  {
+    PartTimer timer(s, 3);
+    e = splat ? cc::launch_batch_splat(L, o, false, s->ctx->sm_count, (int)s->opt.blocks_per_sm, st)
+              : cc::launch_batch(L, o, chunks.data(), chunks.size(), false, s->ctx->sm_count,
+                                 (int)s->opt.blocks_per_sm, st);
   }
+  GROUP_CUDA(e, "launch");
   GROUP_CUDA(cudaMemcpyAsync(status, counters, cc::kCounterWords * 4, cudaMemcpyDeviceToHost, st), "status");
   return true;
 }
@@ -380,13 +415,18 @@ void launch(cc_server* s, Slot& slot) {
     cudaError_t e = cudaSuccess;
     r->d_receivers = static_cast<float4*>(pool_alloc(s, P * 32, st, &e));
     SRV_CUDA(e, "request receivers");
-    SRV_CUDA(cudaMemcpyAsync(r->d_receivers, q.receivers, P * 32, cudaMemcpyHostToDevice, st), "request receivers");
+    {
+      PartTimer timer(s, 1);
+      e = cudaMemcpyAsync(r->d_receivers, q.receivers, P * 32, cudaMemcpyHostToDevice, st);
+    }
+    SRV_CUDA(e, "request receivers");
     r->traced.clear();
     for (size_t l = 0; l < r->result.size(); ++l)
       if (!r->hit[l]) r->traced.insert(r->traced.end(), r->lights.begin() + 16 * l, r->lights.begin() + 16 * (l + 1));
     if (!r->traced.empty()) {
       r->d_lights = static_cast<float4*>(pool_alloc(s, r->traced.size() * 4, st, &e));
       SRV_CUDA(e, "request lights");
+      PartTimer timer(s, 1);
       SRV_CUDA(cudaMemcpyAsync(r->d_lights, r->traced.data(), r->traced.size() * 4, cudaMemcpyHostToDevice, st),
                "request lights");
     }
@@ -438,6 +478,7 @@ void launch(cc_server* s, Slot& slot) {
       !enqueue_group(s, slot, splat, true, slot.host_jobs + exact.jobs.size(), slot.status + cc::kCounterWords))
     return;
   // Results to the requests' host buffers, light-major.
+  PartTimer copies_out(s, 4);
   for (Request* r : slot.reqs) {
     const cc_request& q = r->req;
     const uint64_t P = q.npoints;
@@ -565,9 +606,24 @@ void run_loop(cc_server* s) {
         free_slot->reqs = std::move(taken);
         free_slot->busy = true;
         free_slot->large = large;
+        const Clock::time_point t_launch = Clock::now();
+        if (s->tracing) {
+          uint32_t busy = 0;
+          uint64_t cones = 0;
+          for (const Slot& sl : s->slots) busy += sl.busy;
+          for (const Request* r : free_slot->reqs) cones += request_cones(r->req);
+          free_slot->trace_row = s->trace.size();
+          s->trace.push_back({ms_between(s->t0, t_launch), 0.0, 0.0, free_slot->reqs.size(), cones, busy, {}});
+        }
+        const size_t row = free_slot->trace_row;
+        std::fill(s->part_ms, s->part_ms + 5, 0.0);
         lk.unlock();
         launch(s, *free_slot);
         lk.lock();
+        if (s->tracing && row < s->trace.size()) {
+          s->trace[row].enqueue_ms = ms_between(t_launch, Clock::now());
+          std::copy(s->part_ms, s->part_ms + 5, s->trace[row].part_ms);
+        }
         continue;
       }
       if (!any_busy && blocked) {
@@ -601,7 +657,7 @@ void cc_server_options_default(cc_server_options* opt) {
   opt->max_launch_cones = 2ull << 20;
   opt->points_per_warp = 32;
   opt->blocks_per_sm = cc::kBlocksPerSm;
-  opt->deadline_ns_per_cone = 0;
+  opt->deadline_ns_per_cone = 12;
 }
 
 int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server** out) {
@@ -620,6 +676,8 @@ int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server
   cc_server* s = new cc_server;
   s->ctx = ctx;
   s->opt = opt;
+  s->tracing = std::getenv("CC_SERVER_TRACE") != nullptr;
+  s->t0 = Clock::now();
   s->chunk = std::min<uint64_t>(s->chunk, ctx->split_chunk);
   cudaMemPoolProps props{};
   props.allocType = cudaMemAllocationTypePinned;
@@ -645,6 +703,23 @@ int cc_server_create(cc_context* ctx, const cc_server_options* opt_in, cc_server
     rc = cuda_fail(e, "server setup");
     cc_server_destroy(s);
     return rc;
+  }
+  // The budget is reserved in the pool now (its memory stays in the pool,
+  // whose release threshold is unlimited): growing the pool while launches
+  // run stalled the loop thread inside cudaMallocFromPoolAsync for up to
+  // 1.4 s at a time, with the device idle. Without room for the whole budget
+  // the pool grows on demand, as before.
+  {
+    const Clock::time_point t = Clock::now();
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, opt.hbm_budget, s->pool, s->slots[0].stream) == cudaSuccess) {
+      cudaFreeAsync(p, s->slots[0].stream);
+      cudaStreamSynchronize(s->slots[0].stream);
+    } else {
+      cudaGetLastError();  // not an error of the server's
+    }
+    if (s->tracing) std::fprintf(stderr, "cc_server trace: reserved %.2f GiB in %.1f ms\n",
+                                 opt.hbm_budget / 1073741824.0, ms_between(t, Clock::now()));
   }
   s->loop = std::thread(run_loop, s);
   *out = s;
@@ -672,6 +747,15 @@ int cc_server_destroy(cc_server* s) {
     if (slot.stream) cudaStreamDestroy(slot.stream);
   }
   if (s->pool) cudaMemPoolDestroy(s->pool);
+  if (s->tracing) {
+    std::fprintf(stderr,
+                 "cc_server trace: admitted_ms enqueue_ms retired_ms requests cones slots_busy alloc_ms copy_in_ms "
+                 "order_ms kernels_ms copy_out_ms\n");
+    for (const auto& t : s->trace)
+      std::fprintf(stderr, "cc_server trace: %.2f %.2f %.2f %llu %llu %u %.2f %.2f %.2f %.2f %.2f\n", t.admitted_ms,
+                   t.enqueue_ms, t.retired_ms, (unsigned long long)t.requests, (unsigned long long)t.cones, t.busy,
+                   t.part_ms[0], t.part_ms[1], t.part_ms[2], t.part_ms[3], t.part_ms[4]);
+  }
   delete s;
   return CC_OK;
 }

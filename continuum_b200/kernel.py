@@ -629,7 +629,7 @@ class Server:
 
     def __init__(self, kernel: MaskConeKernel, hbm_budget: int = 8 << 30, max_inflight: int = 4,
                  max_queue: int = 256, max_launch_cones: int = 2 << 20, points_per_warp: int = 32,
-                 blocks_per_sm: int = 8, deadline_ns_per_cone: int = 0):
+                 blocks_per_sm: int = 8, deadline_ns_per_cone: int = 12):
         opt = _lib.ServerOptions(int(hbm_budget), int(max_inflight), int(max_queue), int(max_launch_cones),
                                  int(points_per_warp), int(blocks_per_sm), int(deadline_ns_per_cone))
         h = C.c_void_p()

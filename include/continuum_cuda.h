@@ -405,8 +405,9 @@ CC_API int cc_batch_sizes(const cc_batch* batch, uint64_t out4[4]);
 /* ---- Served form --------------------------------------------------------
  * A request loop on its own host thread. Scenes stay resident; requests
  * (a scene, receivers, 1 or more lights) queue on submission and are admitted
- * in arrival order, or with deadline_ns_per_cone > 0 earliest deadline first,
- * while launch slots and device memory under the server's budget allow: a
+ * earliest deadline first (deadline_ns_per_cone > 0, the default) or in
+ * arrival order (0), while launch slots and device memory under the server's
+ * budget allow: a
  * request's deadline is its submission time plus deadline_ns_per_cone for each
  * of its cones, so small requests overtake large ones that have not waited
  * about as long as the small ones take, and no request waits forever. The
@@ -432,18 +433,18 @@ CC_API int cc_batch_sizes(const cc_batch* batch, uint64_t out4[4]);
 typedef struct cc_server cc_server;
 
 typedef struct cc_server_options {
-  uint64_t hbm_budget;       /* device bytes for requests in flight and cached results */
+  uint64_t hbm_budget;       /* device bytes for requests in flight and cached results, reserved by the
+                                server at creation when the device has room (held until destroyed) */
   uint32_t max_inflight;     /* launches in flight at once: 1..8 (4) */
   uint32_t max_queue;        /* queued requests before submissions are refused with CC_ERR_BUSY (256) */
   uint64_t max_launch_cones; /* cones one launch takes at most (2M); one larger request runs alone */
   uint32_t points_per_warp;  /* 1..32 (32) */
   uint32_t blocks_per_sm;    /* 1..8 (8) */
-  uint32_t deadline_ns_per_cone; /* 0: admission in arrival order (default); else earliest deadline first,
-                                    deadline = submission + this per cone (12: about one B200's rate on a
-                                    plain scene) */
+  uint32_t deadline_ns_per_cone; /* admission earliest deadline first, deadline = submission + this per
+                                    cone (12: about one B200's rate on a plain scene); 0: arrival order */
 } cc_server_options;
 
-/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 2M cones per launch, 32, 8, arrival order. */
+/* Defaults: 8 GiB budget, 4 in flight, 256 queued, 2M cones per launch, 32, 8, 12 ns per cone. */
 CC_API void cc_server_options_default(cc_server_options* opt);
 
 typedef struct cc_request {

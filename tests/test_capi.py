@@ -162,7 +162,7 @@ def test_server_options_and_invalid_arguments():
     o = _lib.ServerOptions()
     lib.cc_server_options_default(C.byref(o))
     assert (o.hbm_budget, o.max_inflight, o.max_queue, o.max_launch_cones, o.points_per_warp, o.blocks_per_sm,
-            o.deadline_ns_per_cone) == (8 << 30, 4, 256, 2 << 20, 32, 8, 0)
+            o.deadline_ns_per_cone) == (8 << 30, 4, 256, 2 << 20, 32, 8, 12)
     h = C.c_void_p()
     assert lib.cc_server_create(None, C.byref(o), C.byref(h)) == _lib.CC_ERR_INVALID
     assert lib.cc_server_submit(None, None, None) == _lib.CC_ERR_INVALID
