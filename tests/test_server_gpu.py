@@ -168,14 +168,14 @@ def test_small_requests_overtake_large_ones(kernel, fields, ns_per_cone):
 
 
 def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
-    """Two slots, a launch limit of 1M cones, 1 ns of deadline per cone. A
-    request above the limit (a) and one within it (s) hold both slots; then
-    a second request above the limit (b) and, 3 ms later, a small one (c)
-    queue, b with the earlier deadline. When s completes, c takes the slot
-    and b keeps waiting, since a slot stays free of requests above the limit
-    while a smaller one waits. (Pinned host buffers: a copy to pageable
-    memory would hold the server's thread until the launch before it is
-    done.)"""
+    """Two slots, a launch limit of 6M cones, 1 ns of deadline per cone. A
+    request above the limit (a, 11.5M cones) and one within it (s, 5.8M)
+    hold both slots; then a second request above the limit (b, 6.3M) and,
+    8 ms later, a small one (c) queue, b with the earlier deadline. When s
+    completes, c takes the slot and b keeps waiting, since a slot stays free
+    of requests above the limit while a smaller one waits. (Pinned host
+    buffers: a copy to pageable memory would hold the server's thread until
+    the launch before it is done.)"""
     import time
 
     import torch
@@ -187,29 +187,31 @@ def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
 
     ws, sc = fields
     w = ws[0]
-    srv = Server(kernel, max_inflight=2, max_launch_cones=1_000_000, deadline_ns_per_cone=1)
-    sid = srv.add_scene(sc[0])
     lig = w.lights
-    big = pinned(np.concatenate([w.receivers] * 32))      # 1.84 M cones with 4 lights
-    medium = pinned(np.concatenate([w.receivers] * 16))   # 0.92 M cones
+    assert lig.shape[0] == 4
+    srv = Server(kernel, max_inflight=2, max_launch_cones=6_000_000, deadline_ns_per_cone=1)
+    sid = srv.add_scene(sc[0])
+    a_rec = pinned(np.concatenate([w.receivers] * 200))   # 11.5 M cones with 4 lights
+    s_rec = pinned(np.concatenate([w.receivers] * 100))   # 5.8 M cones
+    b_rec = pinned(np.concatenate([w.receivers] * 110))   # 6.3 M cones
     small_rec, small_lig = pinned(w.receivers[:500]), np.ascontiguousarray(w.lights[:1])
-    shapes = ((big.shape[0], 4), (medium.shape[0], 4), (big.shape[0], 4), (500, 1))
+    shapes = ((a_rec.shape[0], 4), (s_rec.shape[0], 4), (b_rec.shape[0], 4), (500, 1))
     outs = [{k: pinned(v) for k, v in host_outputs(P, L).items()} for P, L in shapes]
     # A first request, so that the server's thread is up and idle.
     srv.wait(srv.submit(sid, small_rec, small_lig, outs[3]))
-    t_a = srv.submit(sid, big, lig, outs[0])
-    time.sleep(0.002)
-    t_s = srv.submit(sid, medium, lig, outs[1])
+    t_a = srv.submit(sid, a_rec, lig, outs[0])
+    time.sleep(0.003)
+    t_s = srv.submit(sid, s_rec, lig, outs[1])
     time.sleep(0.001)
     t0 = time.perf_counter()
-    t_b = srv.submit(sid, big, lig, outs[2])
-    time.sleep(0.003)
+    t_b = srv.submit(sid, b_rec, lig, outs[2])
+    time.sleep(0.008)
     t_c = srv.submit(sid, small_rec, small_lig, outs[3])
     between_ms = 1e3 * (time.perf_counter() - t0)
     a, s_, b, c = (srv.wait(t) for t in (t_a, t_s, t_b, t_c))
     # c was admitted before b although b's deadline came first.
-    assert c["queued_ms"] + between_ms < b["queued_ms"]
-    for out, r, li in ((outs[2], big, lig), (outs[3], small_rec, small_lig)):
+    assert c["queued_ms"] + between_ms < b["queued_ms"], (a, s_, b, c, between_ms)
+    for out, r, li in ((outs[2], b_rec, lig), (outs[3], small_rec, small_lig)):
         ref = alone(kernel, sc[0], r, li)
         for key in KEYS:
             assert np.array_equal(out[key], ref[key]), key
