@@ -48,6 +48,13 @@ NODE_BYTES = 48  # reference NodeGpu (hierarchy.rs:68-76)
 TRI_BYTES = 48   # three vec4 vertices (hierarchy.rs:12-13)
 
 
+# The full plain workload's cones per step, and the DRAM bytes of one
+# packet-pass launch over them as ncu measured them (1.475 GB read + 1.453 GB
+# written, 39.19 ms).
+FULL_CONES = 3_686_400
+PACKET_PASS_DRAM_BYTES = 1_474_594_048 + 1_453_315_584
+
+
 def workload(points: int = 0, caster: str = "library"):
     """The plain-at-scale workload. caster "oracle": the receivers come from
     the oracle's camera pass (the same receivers, bit for bit), so that the
@@ -1147,7 +1154,13 @@ def cuda_arm(args, rank: int, world: int, local_rank: int) -> None:
                 "steps": e2e_steps, "path": "cc_visibility with host buffers (pinned), scene resident"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "traffic": None, "peak_source": peak_src,
+                     # DRAM bytes of one packet-pass launch of this workload at
+                     # full size (dram__bytes_read.sum + dram__bytes_write.sum),
+                     # from the ncu capture committed under profiles/, not from
+                     # this run; null for other sizes.
+                     "traffic": PACKET_PASS_DRAM_BYTES if C == FULL_CONES else None,
+                     "traffic_source": "ncu capture of the packet pass at full size (profiles/), not this run",
+                     "peak_source": peak_src,
                      "kernel": "visibility_kernel (packet pass)", "kernel_ms": packet_ms,
                      "solo_pass_and_integration_ms": solo_ms,
                      "algorithmic_bytes_per_launch": algo_bytes,
