@@ -6,11 +6,12 @@
 // Each launch slot owns a stream, an event and pinned host staging for its
 // job table and status words. The loop retires finished launches (results
 // become cache entries or are freed), then builds the next launch from the
-// queued requests (in arrival order, or earliest deadline first): cache lookups first, then device memory for the traced
-// lights (evicting unused cache entries least recently used), one job per
-// (request, traced light), the copies in, one batched launch, and the copies
-// out. Device memory comes from a pool owned by the server, allocated and
-// freed in stream order.
+// queued requests (earliest deadline first, or in arrival order): cache
+// lookups first, then device memory for the traced lights (evicting unused
+// cache entries least recently used), one job per (request, traced light),
+// the copies in, one batched launch, and the copies out. Device memory comes
+// from a pool owned by the server (the budget reserved in it at creation),
+// allocated and freed in stream order.
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>

@@ -622,10 +622,13 @@ class Batch:
 
 class Server:
     """The served form (cc_server_*): a native request loop with continuous
-    batching, admission against a device-memory budget and a resident
-    lighting cache. Requests take host arrays, which the server's thread
-    reads and writes until the request completes (pinned memory lets the
-    copies overlap with other launches)."""
+    batching, admission against a device-memory budget (reserved when the
+    server is made), earliest deadline first (deadline_ns_per_cone per cone
+    after submission; 0: arrival order), and a resident lighting cache.
+    Requests take host arrays, which the server's thread reads and writes
+    until the request completes (pinned memory lets the copies overlap with
+    other launches; a copy to pageable memory holds the server's thread until
+    its launch is done)."""
 
     def __init__(self, kernel: MaskConeKernel, hbm_budget: int = 8 << 30, max_inflight: int = 4,
                  max_queue: int = 256, max_launch_cones: int = 2 << 20, points_per_warp: int = 32,
