@@ -216,3 +216,47 @@ def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
         for key in KEYS:
             assert np.array_equal(out[key], ref[key]), key
     srv.close()
+
+
+def test_the_server_trace_lists_every_launch():
+    """CC_SERVER_TRACE set: the server reports its budget reservation at
+    creation and one line per launch (admitted, enqueue time, retired,
+    requests, cones, busy slots and the enqueue's parts) when destroyed.
+    Run in a child process, where the variable is set before the server is
+    made."""
+    import os
+    import subprocess
+    import sys
+    import textwrap
+
+    code = textwrap.dedent("""
+        import numpy as np
+        from continuum_b200 import MaskConeKernel, Server, scenes
+        w = scenes.box_field(grid=32)
+        k = MaskConeKernel(0)
+        sc = k.scene(w.meshes)
+        srv = Server(k, hbm_budget=1 << 30, max_inflight=2)
+        sid = srv.add_scene(sc)
+        P, L = w.receivers.shape[0], w.lights.shape[0]
+        outs = [{"full": np.zeros((L, P), np.uint64), "any": np.zeros((L, P), np.uint64),
+                 "irradiance": np.zeros((L, P), np.float32), "fraction": np.zeros((L, P), np.float32)}
+                for _ in range(3)]
+        for t in [srv.submit(sid, w.receivers, w.lights, o) for o in outs]:
+            srv.wait(t)
+        launches = srv.stats()["launches"]
+        srv.close()
+        print("launches", launches)
+    """)
+    env = dict(os.environ, CC_SERVER_TRACE="1")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    launches = int(r.stdout.split("launches")[1])
+    lines = [l for l in r.stderr.splitlines() if l.startswith("cc_server trace:")]
+    assert any("reserved 1.00 GiB" in l for l in lines)
+    rows = [l.split(":", 1)[1].split() for l in lines if "reserved" not in l and "admitted_ms" not in l]
+    assert len(rows) == launches >= 1
+    for row in rows:
+        admitted, enqueue, retired = (float(x) for x in row[:3])
+        assert len(row) == 11 and retired >= admitted and enqueue >= 0.0
+    assert sum(int(row[3]) for row in rows) == 3
