@@ -168,10 +168,10 @@ def test_small_requests_overtake_large_ones(kernel, fields, ns_per_cone):
 
 
 def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
-    """Two slots, a launch limit of 6M cones, 1 ns of deadline per cone. A
-    request above the limit (a, 11.5M cones) and one within it (s, 5.8M)
-    hold both slots; then a second request above the limit (b, 6.3M) and,
-    8 ms later, a small one (c) queue, b with the earlier deadline. When s
+    """Two slots, a launch limit of 9M cones, 1 ns of deadline per cone. A
+    request above the limit (a, 17.3M cones) and one within it (s, 8.6M)
+    hold both slots; then a second request above the limit (b, 9.2M) and,
+    12 ms later, a small one (c) queue, b with the earlier deadline. When s
     completes, c takes the slot and b keeps waiting, since a slot stays free
     of requests above the limit while a smaller one waits. (Pinned host
     buffers: a copy to pageable memory would hold the server's thread until
@@ -189,11 +189,11 @@ def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
     w = ws[0]
     lig = w.lights
     assert lig.shape[0] == 4
-    srv = Server(kernel, max_inflight=2, max_launch_cones=6_000_000, deadline_ns_per_cone=1)
+    srv = Server(kernel, max_inflight=2, max_launch_cones=9_000_000, deadline_ns_per_cone=1)
     sid = srv.add_scene(sc[0])
-    a_rec = pinned(np.concatenate([w.receivers] * 200))   # 11.5 M cones with 4 lights
-    s_rec = pinned(np.concatenate([w.receivers] * 100))   # 5.8 M cones
-    b_rec = pinned(np.concatenate([w.receivers] * 110))   # 6.3 M cones
+    a_rec = pinned(np.concatenate([w.receivers] * 300))   # 17.3 M cones with 4 lights
+    s_rec = pinned(np.concatenate([w.receivers] * 150))   # 8.6 M cones
+    b_rec = pinned(np.concatenate([w.receivers] * 160))   # 9.2 M cones
     small_rec, small_lig = pinned(w.receivers[:500]), np.ascontiguousarray(w.lights[:1])
     shapes = ((a_rec.shape[0], 4), (s_rec.shape[0], 4), (b_rec.shape[0], 4), (500, 1))
     outs = [{k: pinned(v) for k, v in host_outputs(P, L).items()} for P, L in shapes]
@@ -205,7 +205,7 @@ def test_a_slot_stays_free_of_requests_above_the_launch_limit(kernel, fields):
     time.sleep(0.001)
     t0 = time.perf_counter()
     t_b = srv.submit(sid, b_rec, lig, outs[2])
-    time.sleep(0.008)
+    time.sleep(0.012)
     t_c = srv.submit(sid, small_rec, small_lig, outs[3])
     between_ms = 1e3 * (time.perf_counter() - t0)
     a, s_, b, c = (srv.wait(t) for t in (t_a, t_s, t_b, t_c))
